@@ -1,0 +1,321 @@
+"""Benchmark of the B200 particle solver (prints one JSON line on rank 0).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pfsim|reference]
+                [--workload sort]
+
+Under torchrun (N > 1) each rank drives one GPU; work is sharded by
+independent units (scenes / sorts) with no data-path collective, timings are
+taken with CUDA events on the launching stream and the max over ranks is
+reported. `--impl reference` times the CPU restatement of the reference
+algorithm (the oracle) on this host's cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "threejs-particle-fluids_b200"
+for _p in (str(ROOT), str(PKG)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------ clocks ----
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# --------------------------------------------------------- workloads ----
+class SortWorkload:
+    """Standalone hash-grid counting sort, 16M float4 positions on a 128^3
+    linear grid (uniform distribution); one step = one stable sort."""
+
+    name = "grid_sort_16M_uniform_128cubed"
+    metric = "particles sorted/s"
+    unit = "particles/s"
+
+    def __init__(self, n: int = 16_000_000, dist: str = "uniform"):
+        self.n = n
+        self.dist = dist
+        self.cells = 128**3
+
+    def host_input(self, seed: int) -> np.ndarray:
+        from pfsim import workloads as W
+
+        return W.sort_uniform(self.n, seed) if self.dist == "uniform" else W.sort_blobs(self.n, seed)
+
+    def algorithmic_bytes(self) -> int:
+        # read x (16 B) + write perm (4 B) per particle; start + count (8 B) per cell
+        return 20 * self.n + 8 * self.cells
+
+    def grid(self):
+        from pfsim import hashgrid as H
+        from pfsim import workloads as W
+
+        return H.GridOptions(cell_size=W.SORT_CELL, kind="linear", dims=W.SORT_GRID_DIMS)
+
+    def run_gpu(self, steps: int, warmup: int, rank: int, world: int, dist_barrier) -> dict:
+        import ctypes as C
+
+        import torch
+
+        from pfsim import _native as N
+
+        L = N.lib()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        host = self.host_input(1000 + rank)
+        pos = torch.from_numpy(host).to(dev)
+        perm = torch.empty(self.n, dtype=torch.int32, device=dev)
+        start = torch.empty(self.cells, dtype=torch.int32, device=dev)
+        count = torch.empty(self.cells, dtype=torch.int32, device=dev)
+        desc = self.grid().desc(self.n)
+        stream = torch.cuda.current_stream(dev)
+        sp = C.c_void_p(stream.cuda_stream)
+
+        def one():
+            N.check(L.pf_sort(C.c_void_p(pos.data_ptr()), self.n, C.byref(desc), C.c_void_p(perm.data_ptr()),
+                              C.c_void_p(start.data_ptr()), C.c_void_p(count.data_ptr()), None, None, sp))
+
+        for _ in range(warmup):
+            one()
+        torch.cuda.synchronize()
+        dist_barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(dev.index)
+        clocks.start()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            one()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        dist_barrier()
+        ms = ev0.elapsed_time(ev1) / steps
+        clk = clocks.stop()
+        err = C.c_uint32(0)
+        N.check(L.pf_sort_device_errors(sp, C.byref(err)))
+        if err.value:
+            raise RuntimeError(f"device error word {err.value}")
+
+        # End to end through the host-buffer C ABI (H2D of positions and D2H of
+        # perm, start and count inside the timed region), pinned host memory.
+        h_pos = torch.from_numpy(host).pin_memory()
+        h_perm = torch.empty(self.n, dtype=torch.int32).pin_memory()
+        h_start = torch.empty(self.cells, dtype=torch.int32).pin_memory()
+        h_count = torch.empty(self.cells, dtype=torch.int32).pin_memory()
+        u32 = C.POINTER(C.c_uint32)
+
+        def one_host():
+            N.check(L.pf_sort_host(C.cast(C.c_void_p(h_pos.data_ptr()), C.POINTER(C.c_float)), self.n, C.byref(desc),
+                                   C.cast(C.c_void_p(h_perm.data_ptr()), u32), C.cast(C.c_void_p(h_start.data_ptr()), u32),
+                                   C.cast(C.c_void_p(h_count.data_ptr()), u32), None, None))
+
+        for _ in range(max(1, warmup)):
+            one_host()
+        e_steps = max(3, steps // 2)
+        legacy = torch.cuda.default_stream(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(legacy)
+        for _ in range(e_steps):
+            one_host()
+        e1.record(legacy)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e_steps
+        return {
+            "ms": ms,
+            "units_per_step": self.n,
+            "kernel_ms": ms,
+            "kernel_name": "grid sort pipeline (keys+hist, look-back scan, scatter, fix-up)",
+            "algorithmic_bytes": self.algorithmic_bytes(),
+            "gpu_launches_per_step": 10,
+            "clocks": clk,
+            "e2e_ms": e2e_ms,
+            "h2d": 16 * self.n,
+            "d2h": 4 * self.n + 8 * self.cells,
+        }
+
+    def run_cpu(self, threads: int) -> dict:
+        from oracle import oracle as O
+
+        O.set_threads(threads)
+        host = self.host_input(1000)
+        desc = self.grid().desc(self.n)
+        O.sort(host[:1000], desc)
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            O.sort(host, desc)
+            reps += 1
+            if time.perf_counter() - t0 > 3.0 or reps >= 3:
+                break
+        s = (time.perf_counter() - t0) / reps
+        return {"seconds_per_step": s, "units_per_step": self.n, "reps": reps,
+                "sample": f"{reps} full {self.n}-particle stable counting sorts", "cores": 1}
+
+
+WORKLOADS = {"sort": SortWorkload}
+
+
+# -------------------------------------------------------------- main ----
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pfsim", choices=["pfsim", "reference"])
+    ap.add_argument("--workload", default="sort", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = WORKLOADS[args.workload]()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        cpu = wl.run_cpu(threads)
+        value = cpu["units_per_step"] / cpu["seconds_per_step"]
+        line = {
+            "impl": "reference", "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": warmup, "ms_per_step": cpu["seconds_per_step"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": wl.name},
+            "cpu_baseline": {"value": value, "unit": wl.unit, "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]},
+            "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+        def barrier():
+            dist.barrier()
+    else:
+
+        def barrier():
+            pass
+
+    res = wl.run_gpu(args.steps, warmup, rank, world, barrier)
+    ms = res["ms"]
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms, res["e2e_ms"]], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    else:
+        e2e_ms = res["e2e_ms"]
+    peak, peak_kind = hbm_peak()
+    achieved = res["algorithmic_bytes"] / (res["kernel_ms"] * 1e-3) / 1e9
+    value = res["units_per_step"] * world / (ms * 1e-3)
+    line = {
+        "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
+        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {"workload": wl.name, "inputs_larger_than_l2": True, "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": res["kernel_name"], "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None},
+        "e2e": {"value": res["units_per_step"] * world / (e2e_ms * 1e-3), "unit": wl.unit,
+                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+        "gpu_launches": res["gpu_launches_per_step"] * args.steps,
+        "clocks": res["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = wl.run_cpu(1)
+        line["cpu_baseline"] = {"value": cpu["units_per_step"] / cpu["seconds_per_step"], "unit": wl.unit,
+                                "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,300 @@
+/*
+ * pfsim.h — C ABI of the B200 particle solver (libpfsim.so).
+ *
+ * The library replaces the WebGPU compute path of threejs-particle-fluids for
+ * one hot path: the neighbour-grid counting sort (src/core/hashGrid/) and the
+ * XPBD solver substep that uses it (src/core/loop.ts with the fluid, soft-body,
+ * cloth and collider materials). Every entry point below names the reference
+ * interface it stands in for. The signatures use plain C types, pointers and
+ * sizes only, so a Node N-API shim, Python ctypes or a C++ host can bind them.
+ *
+ * Conventions
+ *  - Every call returns pf_status. On failure pf_last_error() returns a
+ *    thread-local message prefixed like the reference's errors
+ *    ("<Class>: <reason>", e.g. src/core/loop.ts:270-272).
+ *  - Handles own their device memory; pf_*_destroy frees it, and any later use
+ *    of a destroyed handle is the caller's bug (the reference throws
+ *    "... has been disposed", src/core/particles.ts:255-257).
+ *  - Pointers documented as "host" are ordinary CPU memory copied in or out;
+ *    pointers documented as "device" are CUDA device pointers.
+ *  - Calls on one handle are not re-entrant (the reference's step() is
+ *    serialised by its promise, src/simulation/Simulation.ts:542-546).
+ *  - Vectors are xyzw float4 (16 bytes), as the reference's vec4 buffers.
+ */
+#ifndef PFSIM_H
+#define PFSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFSIM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PF_API __attribute__((visibility("default")))
+#else
+#define PF_API
+#endif
+
+typedef enum pf_status {
+  PF_OK = 0,
+  PF_ERR_INVALID = 1,   /* bad argument (the reference throws Error) */
+  PF_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  PF_ERR_STATE = 3,     /* call out of order (e.g. step before loop build) */
+  PF_ERR_OOM = 4,       /* device allocation failed */
+  PF_ERR_DEVICE = 5,    /* a kernel reported an error status (bounded wait expired) */
+  PF_ERR_BUDGET = 6     /* serving admission refused: HBM budget exhausted */
+} pf_status;
+
+/* Thread-local text of the last error on this thread ("" when none). */
+PF_API const char* pf_last_error(void);
+/* PFSIM_ABI_VERSION of the loaded library. */
+PF_API int pf_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Neighbour grid: standalone stable counting sort                          */
+/* ------------------------------------------------------------------------ */
+
+typedef enum pf_key_kind {
+  /* cell = clamp(floor((x - origin) / cell_size), 0, dims-1) per axis,
+   * key = ix + dims[0] * (iy + dims[1] * iz). */
+  PF_KEY_LINEAR = 0,
+  /* The reference bucket: Morton(cell + 512) & (table_size - 1) with the
+   * cell coordinate clamped to [-2^30, 2^30-1]
+   * (src/core/hashGrid/cellIndex.ts:113-170, mortonHash.ts:39-79). */
+  PF_KEY_MORTON = 1
+} pf_key_kind;
+
+typedef struct pf_grid_desc {
+  uint32_t key_kind;   /* pf_key_kind */
+  float origin[3];     /* HashGridOptions.hashOrigin (HashGrid.ts:47) */
+  float cell_size;     /* HashGridOptions.cellSize (HashGrid.ts:34) */
+  uint32_t dims[3];    /* PF_KEY_LINEAR: cells per axis */
+  uint32_t table_size; /* PF_KEY_MORTON: power-of-two bucket count (HashGrid.ts:40) */
+} pf_grid_desc;
+
+/* Number of cells (keys) the descriptor defines, or 0 if it is invalid. */
+PF_API uint64_t pf_grid_cells(const pf_grid_desc* grid);
+
+/*
+ * Stable counting sort of n particles by cell key.
+ * Replaces HashGrid.rebuild() (src/core/hashGrid/HashGrid.ts:219-222): the
+ * reset / cellIndexAndHistogram / blockScan / blockSumScan /
+ * finalizeCellRanges / scatter kernels (cellIndex.ts:101-170, sort.ts:72-192).
+ * Unlike the reference's atomic scatter the output is stable: particles of one
+ * cell appear in ascending index order.
+ *   d_pos4    device, n x float4 positions (w ignored)
+ *   d_perm    device, n entries: particle index at each sorted slot
+ *             (HashGridSnapshot.sortedIndices)
+ *   d_start   device, C entries: first slot of each cell (cellStart)
+ *   d_count   device, C entries: particles per cell (counts; cellEnd = start+count)
+ *   d_keys    device, n entries or NULL: each particle's key (cellIndex)
+ *   d_overflow device, 1 entry or NULL: 1 if a cell coordinate left the
+ *             Morton range or was clamped (HashGrid.overflowFlag)
+ *   stream    cudaStream_t or NULL for the legacy default stream
+ * Scratch memory comes from a per-device workspace owned by the library.
+ */
+PF_API pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* grid,
+                  uint32_t* d_perm, uint32_t* d_start, uint32_t* d_count,
+                  uint32_t* d_keys, uint32_t* d_overflow, void* stream);
+
+/* Synchronises `stream` and returns, then clears, the device error word of
+ * the most recent pf_sort on that stream (0 = no error; bit 0 = a bounded
+ * look-back wait expired, bit 1 = a fix-up list overflowed). */
+PF_API pf_status pf_sort_device_errors(void* stream, uint32_t* bits);
+
+/* pf_sort with host buffers: copies the positions in, sorts, copies the
+ * outputs back (any output pointer may be NULL). Synchronous. */
+PF_API pf_status pf_sort_host(const float* h_pos4, uint32_t n, const pf_grid_desc* grid,
+                       uint32_t* h_perm, uint32_t* h_start, uint32_t* h_count,
+                       uint32_t* h_keys, uint32_t* h_overflow);
+
+/* ------------------------------------------------------------------------ */
+/* Scene: ParticleSystem + materials + colliders + SimLoop                   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct pf_scene pf_scene;
+
+typedef struct pf_range {
+  uint32_t start;
+  uint32_t count;
+} pf_range;
+
+/* new ParticleSystem(renderer, capacity, particleRadius)
+ * (src/core/particles.ts:81-113). */
+typedef struct pf_scene_desc {
+  uint32_t capacity;
+  float particle_radius;
+} pf_scene_desc;
+
+
+/* ParticleSystem.uploadParticles(data, start) (particles.ts:121-160).
+ * Host arrays of n entries starting at slot `start`; vel4/inv_mass/group may
+ * be NULL for the reference defaults (0 velocity, invMass 1, group 0). */
+
+/* ParticleSystem.setInvMass(range, invMass) (particles.ts:163-173). */
+
+/* new FluidSystem(particles, options) and FluidSystem.addBoundary
+ * (src/fluids/FluidSystem.ts:31-54, 90-127, 171-183). Zero fields take the
+ * reference defaults: rest_density 1000, particle_spacing 2r,
+ * smoothing_radius 2*spacing. compliance < 0 selects the default 1e-4.
+ * XSPH viscosity runs only when PF_FLUID_VISCOSITY is set, as optional effects
+ * only compile in when given (FluidSystem.ts:111-115). */
+#define PF_FLUID_VISCOSITY 1u
+typedef struct pf_fluid_desc {
+  pf_range range;               /* count 0 = every particle */
+  float rest_density;
+  float particle_spacing;
+  float smoothing_radius;
+  float compliance;
+  float viscosity;
+  uint32_t flags;
+  uint32_t n_boundaries;
+  const pf_range* boundaries;   /* host, n_boundaries entries */
+  const uint8_t* boundary_static; /* host or NULL: 1 = static boundary (addBoundary dynamic:false) */
+} pf_fluid_desc;
+
+/* new SoftbodySystem(particles, {bodies, shapeMatching})
+ * (src/softbody/SoftbodySystem.ts:29-73, 132-199). */
+typedef struct pf_softbody_def {
+  pf_range range;
+  uint32_t surface_count;       /* UINT32_MAX = every particle */
+  float compliance;
+  const float* rest_positions;  /* host xyz x count, or NULL = uploaded positions */
+  const uint32_t* edges;        /* host pairs of body-local indices */
+  uint32_t n_edges;             /* number of pairs */
+} pf_softbody_def;
+enum { PF_SHAPE_MATCH_GLOBAL = 0, PF_SHAPE_MATCH_LOCAL = 1 };
+typedef struct pf_softbody_desc {
+  uint32_t n_bodies;
+  const pf_softbody_def* bodies;
+  uint32_t shape_matching;      /* PF_SHAPE_MATCH_* */
+} pf_softbody_desc;
+
+/* new ClothSystem(particles, {graph, offset, stretchCompliance})
+ * (src/cloth/ClothSystem.ts:37-70, 102-141, 190-202) with the graph produced
+ * by createClothGraph (src/cloth/graph.ts:130-342). Distance (stretch)
+ * constraints only; the cloth's particles are uploaded from the graph. */
+typedef struct pf_cloth_desc {
+  uint32_t offset;
+  uint32_t n_particles;
+  const float* positions;       /* host xyz x n_particles (graph.positions) */
+  const float* inv_mass;        /* host n_particles (graph.invMass) */
+  uint32_t n_pairs;
+  const uint32_t* pairs;        /* host cloth-local pairs (graph.distancePairs) */
+  const float* rest_lengths;    /* host n_pairs (graph.distanceRestLengths) */
+  float stretch_compliance;     /* < 0 selects the default 1e-7 */
+} pf_cloth_desc;
+
+/* PrimitiveSet.addPlane/addSphere/addBox/addCapsule and setSphere
+ * (src/core/collision/PrimitiveSet.ts:166-257), using the packed GPU record
+ * of the reference (primitives.ts:125-186, PrimitiveSet.ts:64-76). */
+enum { PF_PRIM_PLANE = 0, PF_PRIM_SPHERE = 1, PF_PRIM_BOX = 2, PF_PRIM_CAPSULE = 3 };
+enum { PF_PRIM_INVERT = 1, PF_PRIM_SWEEP = 2 };
+typedef struct pf_primitive {
+  uint32_t kind;
+  uint32_t flags;
+  float data0[4];     /* plane: normal; sphere/box: centre (w radius); capsule: a (w radius) */
+  float data1[4];     /* plane: point; box: half extents; capsule: b; w = muS */
+  float velocity[4];  /* w = muK */
+  float rotation[4];  /* unit quaternion xyzw (boxes) */
+  float spin[4];      /* angular velocity about the pivot, rad/s */
+} pf_primitive;
+
+/* new SimLoop(particles, {substeps, iterations, gravity, hashOrigin})
+ * (src/core/loop.ts:33-57, 117-243). Builds the substep pipeline for the
+ * materials and colliders added so far and allocates the device state. */
+typedef struct pf_loop_desc {
+  uint32_t substeps;
+  uint32_t iterations;
+  float gravity[3];
+  float hash_origin[3];
+  /* Bounds of the linear neighbour grid in metres; particles outside are
+   * clamped into the border cells. min >= max selects the bounds of the
+   * uploaded particles and primitives plus a margin. */
+  float grid_min[3];
+  float grid_max[3];
+} pf_loop_desc;
+
+/* SimLoop.step(dt) (loop.ts:267-279): one frame of `substeps` substeps. */
+
+/* ParticleSystem.readback() (particles.ts:192-227) and material outputs. */
+typedef enum pf_field {
+  PF_FIELD_POSITIONS = 0,          /* float4 x capacity, w = 0 */
+  PF_FIELD_PREDICTED = 1,          /* float4 x capacity, w = 0 */
+  PF_FIELD_VELOCITIES = 2,         /* float4 x capacity */
+  PF_FIELD_INV_MASS = 3,           /* float x capacity */
+  PF_FIELD_BOUNDARY_VOLUME = 4,    /* float x capacity */
+  PF_FIELD_DENSITY = 5,            /* float x capacity (FluidSystem.density) */
+  PF_FIELD_ROTATION = 6,           /* float4 x capacity */
+  PF_FIELD_PREDICTED_ROTATION = 7, /* float4 x capacity */
+  PF_FIELD_ANGULAR_VELOCITY = 8,   /* float4 x capacity */
+  PF_FIELD_LAMBDA = 9,             /* float x capacity (fluid lambda) */
+  PF_FIELD_NEIGHBOR_COUNT = 10,    /* uint32 x capacity (NeighborList.counts) */
+  PF_FIELD_NEIGHBORS = 11,         /* uint32 x capacity x 64, row i = particle i's neighbours */
+  PF_FIELD_CELL_PERM = 12          /* uint32 x capacity: particle index per sorted slot */
+} pf_field;
+
+/* SimLoop.readbackOverflow() (loop.ts:59-69, 286-295) plus the neighbour-list
+ * flag of FluidSystem.readbackOverflow(). */
+typedef struct pf_overflow {
+  uint32_t positions;
+  uint32_t velocities;
+  uint32_t grid;
+  uint32_t contacts;
+  uint32_t neighbors;
+  uint32_t device_error;
+} pf_overflow;
+
+/* Device milliseconds of the last pf_step (CUDA events on the scene stream). */
+
+/* ------------------------------------------------------------------------ */
+/* Batching: many scenes, one launch per stage, one CUDA graph per tick       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct pf_batch pf_batch;
+
+typedef struct pf_batch_opts {
+  uint32_t use_graph;        /* capture each tick as a CUDA graph */
+  uint32_t block_size;       /* 0 = autotuned */
+} pf_batch_opts;
+
+/* Pack the current state of `n` built scenes into one batch. The scenes stay
+ * valid and independent; the batch owns copies of their state. */
+/* One step of every scene; dt applies to all. */
+/* Move scene `index`'s primitive `slot` (PrimitiveSet.setSphere etc.). */
+
+/* ------------------------------------------------------------------------ */
+/* Serving: continuous batching under an HBM budget                           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct pf_server pf_server;
+
+typedef struct pf_server_opts {
+  uint64_t hbm_budget_bytes;  /* state budget for live scenes */
+  uint32_t max_scenes;
+  uint32_t use_graph;
+} pf_server_opts;
+
+typedef struct pf_server_stats {
+  uint32_t live;
+  uint32_t queued;
+  uint64_t ticks;
+  uint64_t particle_substeps;
+  uint64_t state_bytes;
+  float last_tick_ms;
+} pf_server_stats;
+
+/* Queue a built scene for admission. The server copies its state; `ticket`
+ * identifies the request. `lifetime_steps` steps later it retires. */
+/* Admit what fits, step every live scene once, retire finished scenes. */
+/* Copy a live or retired request's field (retired results are kept until read). */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFSIM_H */

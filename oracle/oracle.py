@@ -1,0 +1,153 @@
+"""ctypes loader of the CPU oracle (libpf_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA path. Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg may import this
+module. It restates the reference algorithm (see pf_oracle.cpp's header for
+the reference files each function follows) and is never part of the product.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libpf_oracle.so"
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (g++ only)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+        _bind(_lib)
+    return _lib
+
+
+def _bind(L: C.CDLL) -> None:
+    import sys
+
+    sys.path.insert(0, str(HERE.parent / "threejs-particle-fluids_b200"))
+    from pfsim import _native as N  # struct layouts only
+
+    P = C.c_void_p
+    u32p = C.POINTER(C.c_uint32)
+    f32p = C.POINTER(C.c_float)
+    sig = {
+        "or_last_error": (C.c_char_p, []),
+        "or_part1by2": (C.c_uint32, [C.c_uint32]),
+        "or_morton": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32]),
+        "or_set_threads": (None, [C.c_int]),
+        "or_max_threads": (C.c_int, []),
+        "or_hardware_threads": (C.c_int, []),
+        "or_grid_cells": (C.c_uint64, [C.POINTER(N.GridDesc)]),
+        "or_sort": (C.c_int, [f32p, C.c_uint32, C.POINTER(N.GridDesc), u32p, u32p, u32p, u32p, u32p]),
+        "or_walk": (C.c_int, [f32p, C.POINTER(N.GridDesc), u32p, u32p, u32p, u32p, C.c_uint32, u32p]),
+        "or_polar": (None, [f32p, f32p]),
+        "or_polar_f64": (None, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "or_color_constraints": (C.c_uint32, [u32p, C.c_uint32, u32p]),
+        "or_scene_create": (P, [C.POINTER(N.SceneDesc), C.c_int]),
+        "or_scene_destroy": (None, [P]),
+        "or_upload_particles": (C.c_int, [P, f32p, f32p, f32p, u32p, C.c_uint32, C.c_uint32]),
+        "or_set_inv_mass": (C.c_int, [P, N.Range, C.c_float]),
+        "or_add_fluid": (C.c_int, [P, C.POINTER(N.FluidDesc), u32p]),
+        "or_add_softbodies": (C.c_int, [P, C.POINTER(N.SoftbodyDesc), u32p]),
+        "or_add_cloth": (C.c_int, [P, C.POINTER(N.ClothDesc), u32p]),
+        "or_add_primitive": (C.c_int, [P, C.POINTER(N.Primitive), u32p]),
+        "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
+        "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
+        "or_step": (C.c_int, [P, C.c_float]),
+        "or_readback": (C.c_int, [P, C.c_uint32, P, C.c_size_t, C.c_int]),
+        "or_overflow_read": (C.c_int, [P, C.POINTER(N.Overflow)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise OracleError(lib().or_last_error().decode())
+
+
+def _p(a, t=C.c_float):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def set_threads(n: int) -> None:
+    lib().or_set_threads(int(n))
+
+
+def sort(positions: np.ndarray, desc) -> dict:
+    """Stable counting sort on the CPU (the oracle of pf_sort)."""
+    L = lib()
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    n = pos.shape[0]
+    cells = int(L.or_grid_cells(C.byref(desc)))
+    out = {
+        "keys": np.empty(n, np.uint32),
+        "perm": np.empty(n, np.uint32),
+        "start": np.empty(cells, np.uint32),
+        "count": np.empty(cells, np.uint32),
+        "overflow": np.zeros(1, np.uint32),
+    }
+    check(
+        L.or_sort(
+            _p(pos), n, C.byref(desc), _p(out["keys"], C.c_uint32), _p(out["perm"], C.c_uint32),
+            _p(out["start"], C.c_uint32), _p(out["count"], C.c_uint32), _p(out["overflow"], C.c_uint32),
+        )
+    )
+    return out
+
+
+def walk(query: np.ndarray, desc, perm, start, count, cap: int = 1 << 20) -> np.ndarray:
+    """Candidates of the 27-cell walk around one point (query.ts order)."""
+    L = lib()
+    q = np.ascontiguousarray(query, dtype=np.float32)
+    out = np.empty(cap, np.uint32)
+    n = C.c_uint32(0)
+    check(
+        L.or_walk(_p(q), C.byref(desc), _p(perm, C.c_uint32), _p(start, C.c_uint32),
+                  _p(count, C.c_uint32), _p(out, C.c_uint32), cap, C.byref(n))
+    )
+    return out[: min(n.value, cap)].copy()
+
+
+def polar(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32).reshape(9)
+    r = np.empty(9, np.float32)
+    lib().or_polar(_p(a), _p(r))
+    return r.reshape(3, 3)
+
+
+def polar_f64(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    r = np.empty(9, np.float64)
+    lib().or_polar_f64(_p(a, C.c_double), _p(r, C.c_double))
+    return r.reshape(3, 3)
+
+
+def color_constraints(pairs: np.ndarray) -> tuple[np.ndarray, int]:
+    p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1)
+    n = p.size // 2
+    g = np.empty(n, np.uint32)
+    k = lib().or_color_constraints(_p(p, C.c_uint32), n, _p(g, C.c_uint32))
+    return g, int(k)

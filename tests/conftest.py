@@ -1,0 +1,33 @@
+"""Shared pytest setup: import paths, the `gpu` marker and small helpers."""
+
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "threejs-particle-fluids_b200"
+for p in (str(ROOT), str(PKG)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the CUDA path through the C ABI")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+
+    O.build()
+    O.lib()
+    return O
+
+
+@pytest.fixture(scope="session")
+def pfsim():
+    import pfsim as P
+
+    P.lib()
+    return P

@@ -1,0 +1,40 @@
+"""The C ABI library loads and exports every symbol include/pfsim.h declares.
+
+CPU only: no compute call is made (there is no GPU here).
+"""
+
+import ctypes as C
+import re
+from pathlib import Path
+
+from pfsim import _native as N
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "pfsim.h"
+
+
+def declared_symbols() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^PF_API\s+[\w\s\*]+?\b(pf_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for must in ("pf_sort", "pf_sort_host", "pf_grid_cells", "pf_last_error"):
+        assert must in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = N.lib()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, f"libpfsim.so lacks {missing}"
+
+
+def test_abi_version_and_error_text():
+    lib = N.lib()
+    assert lib.pf_abi_version() == 1
+    # An invalid descriptor is rejected on the host before any device work.
+    d = N.GridDesc()
+    d.key_kind = N.PF_KEY_MORTON
+    d.cell_size = 0.1
+    d.table_size = 3
+    assert lib.pf_grid_cells(C.byref(d)) == 0
