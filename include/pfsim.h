@@ -101,6 +101,19 @@ PF_API pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* gr
                   uint32_t* d_perm, uint32_t* d_start, uint32_t* d_count,
                   uint32_t* d_keys, uint32_t* d_overflow, void* stream);
 
+/* pf_sort that allocates no device memory (no counterpart in the reference;
+ * added for callers that cannot allocate, such as hosts whose own pool owns
+ * the device memory or loops where an allocation would stall the frame).
+ * Same arguments and results as pf_sort. Its scratch is one fixed block
+ * compiled into the library (about 21 MB held on every GPU that loads it), so
+ * n <= 1,048,576 particles and at most 2,097,152 cells per call; larger sizes
+ * return PF_ERR_INVALID. The first call on a device looks up that block's
+ * device address, so make it before any stream capture. Calls share the
+ * block: calls whose GPU work overlaps race, so serialise them. */
+PF_API pf_status pf_sort_noalloc(const float* d_pos4, uint32_t n, const pf_grid_desc* grid,
+                                 uint32_t* d_perm, uint32_t* d_start, uint32_t* d_count,
+                                 uint32_t* d_keys, uint32_t* d_overflow, void* stream);
+
 /* Synchronises `stream` and returns, then clears, the device error word of
  * the most recent pf_sort on that stream (0 = no error; bit 0 = a bounded
  * look-back wait expired, bit 1 = a fix-up list overflowed). */

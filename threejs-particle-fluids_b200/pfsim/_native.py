@@ -186,6 +186,7 @@ SIGNATURES = {
     "pf_grid_cells": (C.c_uint64, [C.POINTER(GridDesc)]),
     "pf_sort": (C.c_int, [_P, C.c_uint32, C.POINTER(GridDesc), _P, _P, _P, _P, _P, _P]),
     "pf_sort_device_errors": (C.c_int, [_P, _u32p]),
+    "pf_sort_noalloc": (C.c_int, [_P, C.c_uint32, C.POINTER(GridDesc), _P, _P, _P, _P, _P, _P]),
     "pf_sort_host": (C.c_int, [_f32p, C.c_uint32, C.POINTER(GridDesc), _u32p, _u32p, _u32p, _u32p, _u32p]),
 }
 
