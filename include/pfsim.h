@@ -143,12 +143,19 @@ typedef struct pf_scene_desc {
   float particle_radius;
 } pf_scene_desc;
 
+PF_API pf_status pf_scene_create(const pf_scene_desc* desc, pf_scene** out);
+PF_API void pf_scene_destroy(pf_scene* scene);
+
 
 /* ParticleSystem.uploadParticles(data, start) (particles.ts:121-160).
  * Host arrays of n entries starting at slot `start`; vel4/inv_mass/group may
  * be NULL for the reference defaults (0 velocity, invMass 1, group 0). */
+PF_API pf_status pf_upload_particles(pf_scene* scene, const float* pos4, const float* vel4,
+                                     const float* inv_mass, const uint32_t* group,
+                                     uint32_t start, uint32_t n);
 
 /* ParticleSystem.setInvMass(range, invMass) (particles.ts:163-173). */
+PF_API pf_status pf_set_inv_mass(pf_scene* scene, pf_range range, float inv_mass);
 
 /* new FluidSystem(particles, options) and FluidSystem.addBoundary
  * (src/fluids/FluidSystem.ts:31-54, 90-127, 171-183). Zero fields take the
@@ -169,6 +176,7 @@ typedef struct pf_fluid_desc {
   const pf_range* boundaries;   /* host, n_boundaries entries */
   const uint8_t* boundary_static; /* host or NULL: 1 = static boundary (addBoundary dynamic:false) */
 } pf_fluid_desc;
+PF_API pf_status pf_add_fluid(pf_scene* scene, const pf_fluid_desc* desc, uint32_t* material_index);
 
 /* new SoftbodySystem(particles, {bodies, shapeMatching})
  * (src/softbody/SoftbodySystem.ts:29-73, 132-199). */
@@ -186,6 +194,8 @@ typedef struct pf_softbody_desc {
   const pf_softbody_def* bodies;
   uint32_t shape_matching;      /* PF_SHAPE_MATCH_* */
 } pf_softbody_desc;
+PF_API pf_status pf_add_softbodies(pf_scene* scene, const pf_softbody_desc* desc,
+                                   uint32_t* material_index);
 
 /* new ClothSystem(particles, {graph, offset, stretchCompliance})
  * (src/cloth/ClothSystem.ts:37-70, 102-141, 190-202) with the graph produced
@@ -201,6 +211,7 @@ typedef struct pf_cloth_desc {
   const float* rest_lengths;    /* host n_pairs (graph.distanceRestLengths) */
   float stretch_compliance;     /* < 0 selects the default 1e-7 */
 } pf_cloth_desc;
+PF_API pf_status pf_add_cloth(pf_scene* scene, const pf_cloth_desc* desc, uint32_t* material_index);
 
 /* PrimitiveSet.addPlane/addSphere/addBox/addCapsule and setSphere
  * (src/core/collision/PrimitiveSet.ts:166-257), using the packed GPU record
@@ -216,6 +227,8 @@ typedef struct pf_primitive {
   float rotation[4];  /* unit quaternion xyzw (boxes) */
   float spin[4];      /* angular velocity about the pivot, rad/s */
 } pf_primitive;
+PF_API pf_status pf_add_primitive(pf_scene* scene, const pf_primitive* prim, uint32_t* slot);
+PF_API pf_status pf_set_primitive(pf_scene* scene, uint32_t slot, const pf_primitive* prim);
 
 /* new SimLoop(particles, {substeps, iterations, gravity, hashOrigin})
  * (src/core/loop.ts:33-57, 117-243). Builds the substep pipeline for the
@@ -231,8 +244,12 @@ typedef struct pf_loop_desc {
   float grid_min[3];
   float grid_max[3];
 } pf_loop_desc;
+PF_API pf_status pf_loop_build(pf_scene* scene, const pf_loop_desc* desc);
 
-/* SimLoop.step(dt) (loop.ts:267-279): one frame of `substeps` substeps. */
+/* SimLoop.step(dt) (loop.ts:267-279): one frame of `substeps` substeps, dt in
+ * seconds (a double, as the reference's JavaScript number). Asynchronous. */
+PF_API pf_status pf_step(pf_scene* scene, double dt);
+
 
 /* ParticleSystem.readback() (particles.ts:192-227) and material outputs. */
 typedef enum pf_field {
@@ -250,6 +267,7 @@ typedef enum pf_field {
   PF_FIELD_NEIGHBORS = 11,         /* uint32 x capacity x 64, row i = particle i's neighbours */
   PF_FIELD_CELL_PERM = 12          /* uint32 x capacity: particle index per sorted slot */
 } pf_field;
+PF_API pf_status pf_readback(pf_scene* scene, uint32_t field, void* dst_host, size_t bytes);
 
 /* SimLoop.readbackOverflow() (loop.ts:59-69, 286-295) plus the neighbour-list
  * flag of FluidSystem.readbackOverflow(). */
@@ -261,8 +279,10 @@ typedef struct pf_overflow {
   uint32_t neighbors;
   uint32_t device_error;
 } pf_overflow;
+PF_API pf_status pf_overflow_read(pf_scene* scene, pf_overflow* out);
 
 /* Device milliseconds of the last pf_step (CUDA events on the scene stream). */
+PF_API pf_status pf_last_step_ms(pf_scene* scene, float* ms);
 
 /* ------------------------------------------------------------------------ */
 /* Batching: many scenes, one launch per stage, one CUDA graph per tick       */
@@ -277,8 +297,20 @@ typedef struct pf_batch_opts {
 
 /* Pack the current state of `n` built scenes into one batch. The scenes stay
  * valid and independent; the batch owns copies of their state. */
-/* One step of every scene; dt applies to all. */
+PF_API pf_status pf_batch_create(pf_scene* const* scenes, uint32_t n, const pf_batch_opts* opts,
+                                 pf_batch** out);
+PF_API void pf_batch_destroy(pf_batch* batch);
+/* One step of every scene; dt applies to all. Asynchronous. */
+PF_API pf_status pf_batch_step(pf_batch* batch, double dt);
 /* Move scene `index`'s primitive `slot` (PrimitiveSet.setSphere etc.). */
+PF_API pf_status pf_batch_set_primitive(pf_batch* batch, uint32_t index, uint32_t slot,
+                                        const pf_primitive* prim);
+PF_API pf_status pf_batch_readback(pf_batch* batch, uint32_t index, uint32_t field, void* dst_host,
+                                   size_t bytes);
+PF_API pf_status pf_batch_overflow_read(pf_batch* batch, uint32_t index, pf_overflow* out);
+PF_API pf_status pf_batch_last_step_ms(pf_batch* batch, float* ms);
+/* Particle-substeps one pf_batch_step advances (sum over scenes of N * substeps). */
+PF_API uint64_t pf_batch_particle_substeps(pf_batch* batch);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching under an HBM budget                           */

@@ -69,7 +69,7 @@ def _bind(L: C.CDLL) -> None:
         "or_add_primitive": (C.c_int, [P, C.POINTER(N.Primitive), u32p]),
         "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
         "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
-        "or_step": (C.c_int, [P, C.c_float]),
+        "or_step": (C.c_int, [P, C.c_double]),
         "or_readback": (C.c_int, [P, C.c_uint32, P, C.c_size_t, C.c_int]),
         "or_overflow_read": (C.c_int, [P, C.POINTER(N.Overflow)]),
     }
@@ -151,3 +151,96 @@ def color_constraints(pairs: np.ndarray) -> tuple[np.ndarray, int]:
     g = np.empty(n, np.uint32)
     k = lib().or_color_constraints(_p(p, C.c_uint32), n, _p(g, C.c_uint32))
     return g, int(k)
+
+
+# ----------------------------------------------------------- scene backend ----
+class OracleScene:
+    """A recipe replayed on the CPU oracle; same methods as pfsim's Scene."""
+
+    def __init__(self, handle, recipe, precision: int):
+        self.h = handle
+        self.recipe = recipe
+        self.capacity = recipe.capacity
+        self.precision = precision
+        self.steps = 0
+
+    def step(self, dt: float) -> None:
+        L = lib()
+        if self.recipe.motion is not None:
+            for slot, prim in self.recipe.motion(self.steps, dt).items():
+                p = prim.cstruct()
+                check(L.or_set_primitive(self.h, slot, C.byref(p)))
+        check(L.or_step(self.h, float(dt)))
+        self.steps += 1
+
+    def set_primitive(self, slot, prim) -> None:
+        p = prim.cstruct()
+        check(lib().or_set_primitive(self.h, slot, C.byref(p)))
+
+    def readback(self, field_id: int, as_f64: bool = False) -> "np.ndarray":
+        from pfsim import recipe as R
+
+        out = R.alloc_field(field_id, self.capacity)
+        if as_f64 and out.dtype == np.float32:
+            out = out.astype(np.float64)
+        check(lib().or_readback(self.h, field_id, out.ctypes.data_as(C.c_void_p), out.nbytes, 1 if as_f64 else 0))
+        return out
+
+    def overflow(self) -> dict:
+        from pfsim import _native as N
+
+        o = N.Overflow()
+        check(lib().or_overflow_read(self.h, C.byref(o)))
+        return {k: bool(getattr(o, k)) for k, _ in N.Overflow._fields_}
+
+    def close(self) -> None:
+        if self.h:
+            lib().or_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleBackend:
+    """Replays pfsim recipes on the oracle (FP32, or FP64 with precision=64)."""
+
+    def __init__(self, precision: int = 32, threads: int = 1, table_size: int = 0):
+        self.precision = precision
+        self.threads = threads
+        self.table_size = table_size
+        self.name = f"oracle-f{precision}"
+
+    def build(self, r) -> OracleScene:
+        from pfsim import _native as N
+        from pfsim import recipe as R
+
+        L = lib()
+        set_threads(self.threads)
+        desc = N.SceneDesc(r.capacity, r.radius)
+        h = L.or_scene_create(C.byref(desc), self.precision)
+        if not h:
+            raise OracleError(L.or_last_error().decode())
+        scene = OracleScene(h, r, self.precision)
+        keep = R._Keep()
+        for u in r.uploads:
+            p = R.pos4(u.pos)
+            v = None if u.vel is None else keep.f32(R.pos4(u.vel))
+            w = None if u.inv_mass is None else keep.f32(u.inv_mass)
+            check(L.or_upload_particles(h, keep.f32(p), v, w, None, u.start, p.shape[0]))
+        for kind, opts in r.materials:
+            if kind == "fluid":
+                check(L.or_add_fluid(h, C.byref(R.fluid_desc(opts, keep)), None))
+            elif kind == "soft":
+                check(L.or_add_softbodies(h, C.byref(R.softbody_desc(opts, keep)), None))
+            elif kind == "cloth":
+                check(L.or_add_cloth(h, C.byref(R.cloth_desc(opts, keep)), None))
+        for p in r.prims:
+            cs = p.cstruct()
+            check(L.or_add_primitive(h, C.byref(cs), None))
+        ld = R.loop_desc(r.loop)
+        check(L.or_loop_build(h, C.byref(ld), self.table_size))
+        return scene

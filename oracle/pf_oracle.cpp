@@ -1709,7 +1709,7 @@ int or_loop_build(void* h, const pf_loop_desc* d, uint32_t table_size) {
   return rc;
 }
 
-int or_step(void* h, float dt) {
+int or_step(void* h, double dt) {
   Scene* s = static_cast<Scene*>(h);
   if (!(dt > 0) || !std::isfinite(dt))
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number");
@@ -1719,7 +1719,7 @@ int or_step(void* h, float dt) {
       rc = fail(PF_ERR_STATE, "SimLoop: build the loop before stepping");
       return;
     }
-    e.step(static_cast<double>(dt));
+    e.step(dt);
   });
   return rc;
 }

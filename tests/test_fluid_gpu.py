@@ -1,0 +1,117 @@
+"""PBF fluid substep on the CUDA path against the oracle.
+
+Tolerances: positions after one step (one frame of substeps) within 1e-5 of
+the container extent (1 m here); neighbour lists, which are integer work,
+element for element; long runs by statistics because the dynamics are
+chaotic.
+"""
+
+import numpy as np
+import pytest
+
+from pfsim import _native as N
+from pfsim import recipe as R
+from pfsim import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+EXTENT = 1.0  # container extent of the dam break (x span), metres
+POS_TOL = 1e-5 * EXTENT
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    return R.NativeBackend()
+
+
+def test_neighbor_lists_bit_exact(oracle, cuda):
+    """Lists built from identical positions hold the same particles in the
+    same order (walk order dz, dy, dx; ascending index in a cell)."""
+    r = W.dam_break(5000, seed=1, gravity=(0.0, 0.0, 0.0), substeps=1, iterations=1)
+    a, b = cuda.build(r), oracle.OracleBackend().build(r)
+    a.step(DT)
+    b.step(DT)
+    na, nb = a.readback(N.PF_FIELD_NEIGHBOR_COUNT), b.readback(N.PF_FIELD_NEIGHBOR_COUNT)
+    assert np.array_equal(na, nb)
+    la, lb = a.readback(N.PF_FIELD_NEIGHBORS), b.readback(N.PF_FIELD_NEIGHBORS)
+    assert np.array_equal(la, lb)
+    da, db = a.readback(N.PF_FIELD_DENSITY), b.readback(N.PF_FIELD_DENSITY)
+    np.testing.assert_allclose(da, db, rtol=1e-5, atol=5e-3)
+    lam_a, lam_b = a.readback(N.PF_FIELD_LAMBDA), b.readback(N.PF_FIELD_LAMBDA)
+    np.testing.assert_allclose(lam_a, lam_b, rtol=1e-4, atol=1e-9)
+
+
+@pytest.mark.parametrize("seed", [0, 7])
+def test_one_frame_positions_within_tolerance(oracle, cuda, seed):
+    r = W.dam_break(5000, seed=seed)
+    a, b = cuda.build(r), oracle.OracleBackend().build(r)
+    a.step(DT)
+    b.step(DT)
+    xa, xb = a.readback(N.PF_FIELD_POSITIONS), b.readback(N.PF_FIELD_POSITIONS)
+    assert np.abs(xa - xb).max() <= POS_TOL
+    va, vb = a.readback(N.PF_FIELD_VELOCITIES), b.readback(N.PF_FIELD_VELOCITIES)
+    assert np.abs(va - vb).max() <= POS_TOL / (DT / r.loop.substeps)
+    assert not any(a.overflow().values())
+
+
+def test_one_frame_against_fp64_rerun(oracle, cuda):
+    r = W.dam_break(5000, seed=3)
+    a = cuda.build(r)
+    b = oracle.OracleBackend(precision=64).build(r)
+    a.step(DT)
+    b.step(DT)
+    xa = a.readback(N.PF_FIELD_POSITIONS).astype(np.float64)
+    xb = b.readback(N.PF_FIELD_POSITIONS, as_f64=True)
+    assert np.abs(xa - xb).max() <= POS_TOL
+
+
+def stats(scene, rho0):
+    x = scene.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
+    v = scene.readback(N.PF_FIELD_VELOCITIES)[:, :3].astype(np.float64)
+    d = scene.readback(N.PF_FIELD_DENSITY).astype(np.float64)
+    err = np.maximum(d / rho0 - 1.0, 0.0)
+    return {"com": x.mean(0), "ke": 0.5 * (v * v).sum(1).mean(), "mean_err": err.mean(), "max_err": err.max()}
+
+
+def test_long_run_statistics(oracle, cuda):
+    """100 frames: centre of mass, kinetic energy and density error agree."""
+    r = W.dam_break(5000, seed=5)
+    rho0 = r.materials[0][1].rest_density
+    a, b = cuda.build(r), oracle.OracleBackend().build(r)
+    for _ in range(100):
+        a.step(DT)
+        b.step(DT)
+    sa, sb = stats(a, rho0), stats(b, rho0)
+    assert np.abs(sa["com"] - sb["com"]).max() < 0.01
+    assert abs(sa["ke"] - sb["ke"]) <= 0.15 * max(sb["ke"], 1e-6)
+    assert abs(sa["mean_err"] - sb["mean_err"]) < 0.01
+    assert sa["max_err"] < 0.5
+    x = a.readback(N.PF_FIELD_POSITIONS)
+    assert np.isfinite(x).all()
+    assert x[:, 1].min() > -1e-3  # the floor holds
+
+
+def test_repeat_is_bit_identical(cuda):
+    r = W.dam_break(5000, seed=2)
+    a, b = cuda.build(r), cuda.build(r)
+    for _ in range(10):
+        a.step(DT)
+        b.step(DT)
+    assert np.array_equal(a.readback(N.PF_FIELD_POSITIONS), b.readback(N.PF_FIELD_POSITIONS))
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batched_equals_plain(cuda, use_graph):
+    """A scene stepped alone and inside a batch of uneven scenes agrees bit for bit."""
+    recipes = [W.dam_break(3000, seed=11), W.dam_break(8000, seed=12, scale=1.5, offset=(3.0, 0.0, 0.0)),
+               W.dam_break(1200, seed=13, scale=0.7)]
+    plain = [cuda.build(r) for r in recipes]
+    batch = R.Batch([cuda.build(r) for r in recipes], use_graph=use_graph)
+    for _ in range(5):
+        for s in plain:
+            s.step(DT)
+        batch.step(DT)
+    for i, s in enumerate(plain):
+        assert np.array_equal(s.readback(N.PF_FIELD_POSITIONS), batch.readback(i, N.PF_FIELD_POSITIONS))
+        assert np.array_equal(s.readback(N.PF_FIELD_VELOCITIES), batch.readback(i, N.PF_FIELD_VELOCITIES))

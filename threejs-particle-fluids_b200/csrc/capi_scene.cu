@@ -1,0 +1,505 @@
+// capi_scene.cu — C ABI of scenes (ParticleSystem + materials + colliders +
+// SimLoop) and of batches of scenes.
+//
+// The host-side set-up follows the reference constructors so that a scene
+// built through this ABI holds the same initial state the reference would:
+// FluidSystem sets its particles' inverse mass (FluidSystem.ts:90-127),
+// SoftbodySystem derives rest offsets, mass weights, the neighbour CSR and
+// rest centres from the uploaded particles (SoftbodySystem.ts:132-199,
+// 277-340, 366-514), ClothSystem uploads its graph and colours its distance
+// constraints greedily (ClothSystem.ts:102-141, types.ts:95-150).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "world.cuh"
+
+struct pf_scene {
+  pf::SceneSpec spec;
+  std::unique_ptr<pf::World> world;
+};
+
+struct pf_batch {
+  std::vector<std::unique_ptr<pf::SceneSpec>> specs;
+  std::unique_ptr<pf::World> world;
+};
+
+namespace pf {
+namespace {
+
+bool range_ok(const SceneSpec& s, RangeU r) { return r.count > 0 && (uint64_t)r.start + r.count <= s.cap; }
+bool overlaps(RangeU a, RangeU b) { return a.start < b.start + b.count && b.start < a.start + a.count; }
+
+pf_status not_built(const pf_scene* s, const char* what) {
+  if (!s) return fail(PF_ERR_INVALID, std::string(what) + ": scene is NULL");
+  if (s->spec.built)
+    return fail(PF_ERR_STATE, std::string(what) + ": add materials and colliders before building the SimLoop");
+  return PF_OK;
+}
+
+// Smallest eigenvalue of a symmetric 3x3 (xx, xy, xz, yy, yz, zz) by Jacobi
+// rotations on the largest off-diagonal entry (SoftbodySystem.ts:424-470).
+double smallest_eigenvalue(double a00, double a01, double a02, double a11, double a12, double a22) {
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    const double off = std::fabs(a01) + std::fabs(a02) + std::fabs(a12);
+    if (off < 1e-14) break;
+    const int pivot = (std::fabs(a01) >= std::fabs(a02) && std::fabs(a01) >= std::fabs(a12)) ? 0
+                      : (std::fabs(a02) >= std::fabs(a12))                                    ? 1
+                                                                                              : 2;
+    double apq, app, aqq;
+    if (pivot == 0) { apq = a01; app = a00; aqq = a11; }
+    else if (pivot == 1) { apq = a02; app = a00; aqq = a22; }
+    else { apq = a12; app = a11; aqq = a22; }
+    if (std::fabs(apq) < 1e-20) break;
+    const double theta = (aqq - app) / (2 * apq);
+    const double sgn = theta > 0 ? 1.0 : (theta < 0 ? -1.0 : 1.0);
+    const double t = sgn / (std::fabs(theta) + std::sqrt(1 + theta * theta));
+    const double c = 1 / std::sqrt(1 + t * t), s = t * c;
+    if (pivot == 0) {
+      const double n02 = c * a02 - s * a12, n12 = s * a02 + c * a12;
+      a00 = app - t * apq; a11 = aqq + t * apq; a01 = 0; a02 = n02; a12 = n12;
+    } else if (pivot == 1) {
+      const double n01 = c * a01 - s * a12, n12 = s * a01 + c * a12;
+      a00 = app - t * apq; a22 = aqq + t * apq; a02 = 0; a01 = n01; a12 = n12;
+    } else {
+      const double n01 = c * a01 - s * a02, n02 = s * a01 + c * a02;
+      a11 = app - t * apq; a22 = aqq + t * apq; a12 = 0; a01 = n01; a02 = n02;
+    }
+  }
+  return std::min(a00, std::min(a11, a22));
+}
+
+// Greedy colouring in constraint order: each constraint takes the lowest
+// colour none of its particles has yet (types.ts:95-150).
+std::vector<std::vector<uint32_t>> color_pairs(const std::vector<uint32_t>& pairs, uint32_t n, uint32_t cap) {
+  std::vector<std::vector<uint32_t>> owned(cap);
+  std::vector<std::vector<uint32_t>> colors;
+  for (uint32_t c = 0; c < n; ++c) {
+    const uint32_t a = pairs[2 * c], b = pairs[2 * c + 1];
+    uint32_t g = 0;
+    for (;;) {
+      const bool ca = std::find(owned[a].begin(), owned[a].end(), g) != owned[a].end();
+      const bool cb = std::find(owned[b].begin(), owned[b].end(), g) != owned[b].end();
+      if (!ca && !cb) break;
+      ++g;
+    }
+    if (g >= colors.size()) colors.resize(g + 1);
+    colors[g].push_back(c);
+    owned[a].push_back(g);
+    owned[b].push_back(g);
+  }
+  return colors;
+}
+
+}  // namespace
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" {
+
+pf_status pf_scene_create(const pf_scene_desc* d, pf_scene** out) {
+  if (!d || !out) return fail(PF_ERR_INVALID, "ParticleSystem: NULL argument");
+  if (d->capacity == 0) return fail(PF_ERR_INVALID, "ParticleSystem: capacity must be a positive integer, got 0");
+  if (!(d->particle_radius > 0) || !std::isfinite(d->particle_radius))
+    return fail(PF_ERR_INVALID, "ParticleSystem: particleRadius must be a positive finite number, got " +
+                                    std::to_string(d->particle_radius));
+  auto* s = new pf_scene;
+  SceneSpec& sp = s->spec;
+  sp.cap = d->capacity;
+  sp.radius = d->particle_radius;
+  sp.pos4.assign(4ull * sp.cap, 0.0f);
+  sp.vel4.assign(4ull * sp.cap, 0.0f);
+  sp.inv_mass.assign(sp.cap, 0.0f);
+  sp.bvol.assign(sp.cap, 0.0f);
+  sp.group.assign(sp.cap, 0u);
+  sp.rot4.assign(4ull * sp.cap, 0.0f);
+  sp.angv4.assign(4ull * sp.cap, 0.0f);
+  for (uint32_t i = 0; i < sp.cap; ++i) sp.rot4[4 * i + 3] = 1.0f;
+  *out = s;
+  return PF_OK;
+}
+
+void pf_scene_destroy(pf_scene* s) { delete s; }
+
+pf_status pf_upload_particles(pf_scene* s, const float* pos4, const float* vel4, const float* inv_mass,
+                              const uint32_t* group, uint32_t start, uint32_t n) {
+  if (!s) return fail(PF_ERR_INVALID, "ParticleSystem.uploadParticles: scene is NULL");
+  SceneSpec& sp = s->spec;
+  if ((uint64_t)start + n > sp.cap)
+    return fail(PF_ERR_INVALID, "ParticleSystem.uploadParticles: invalid particle range start=" + std::to_string(start) +
+                                    " count=" + std::to_string(n) + " (capacity " + std::to_string(sp.cap) + ")");
+  if (n && !pos4) return fail(PF_ERR_INVALID, "ParticleSystem.uploadParticles: positions are NULL");
+  if (s->world) return fail(PF_ERR_STATE, "ParticleSystem.uploadParticles: upload before building the SimLoop");
+  for (uint32_t k = 0; k < n; ++k) {
+    if (inv_mass && !(inv_mass[k] >= 0 && std::isfinite(inv_mass[k])))
+      return fail(PF_ERR_INVALID, "ParticleSystem.uploadParticles: invMass must be a finite number >= 0");
+  }
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t i = start + k;
+    for (int c = 0; c < 3; ++c) {
+      sp.pos4[4 * i + c] = pos4[4 * k + c];
+      sp.vel4[4 * i + c] = vel4 ? vel4[4 * k + c] : 0.0f;
+    }
+    sp.pos4[4 * i + 3] = sp.vel4[4 * i + 3] = 0.0f;
+    sp.inv_mass[i] = inv_mass ? inv_mass[k] : 1.0f;
+    sp.group[i] = group ? group[k] : 0u;
+  }
+  return PF_OK;
+}
+
+pf_status pf_set_inv_mass(pf_scene* s, pf_range r, float w) {
+  if (!s) return fail(PF_ERR_INVALID, "ParticleSystem.setInvMass: scene is NULL");
+  if (!range_ok(s->spec, {r.start, r.count}))
+    return fail(PF_ERR_INVALID, "ParticleSystem.setInvMass: invalid particle range");
+  if (!(w >= 0) || !std::isfinite(w)) return fail(PF_ERR_INVALID, "ParticleSystem.setInvMass: invMass must be >= 0");
+  if (s->world) return fail(PF_ERR_STATE, "ParticleSystem.setInvMass: set before building the SimLoop");
+  for (uint32_t i = r.start; i < r.start + r.count; ++i) s->spec.inv_mass[i] = w;
+  return PF_OK;
+}
+
+pf_status pf_add_fluid(pf_scene* s, const pf_fluid_desc* d, uint32_t* mat) {
+  PF_TRY(not_built(s, "FluidSystem"));
+  if (!d) return fail(PF_ERR_INVALID, "FluidSystem: options are NULL");
+  SceneSpec& sp = s->spec;
+  FluidSpec f;
+  f.range.start = d->range.count ? d->range.start : 0;
+  f.range.count = d->range.count ? d->range.count : sp.cap;
+  if (!range_ok(sp, f.range))
+    return fail(PF_ERR_INVALID, "FluidSystem: invalid particle range start=" + std::to_string(f.range.start) +
+                                    " count=" + std::to_string(f.range.count));
+  auto positive = [](double v, const char* name, double* out) -> pf_status {
+    if (!(v > 0) || !std::isfinite(v))
+      return fail(PF_ERR_INVALID, std::string("FluidSystem: ") + name + " must be positive, got " + std::to_string(v));
+    *out = v;
+    return PF_OK;
+  };
+  PF_TRY(positive(d->rest_density > 0 ? d->rest_density : 1000.0, "restDensity", &f.rho0));
+  PF_TRY(positive(d->particle_spacing > 0 ? (double)d->particle_spacing : 2.0 * sp.radius, "particleSpacing", &f.spacing));
+  PF_TRY(positive(d->smoothing_radius > 0 ? (double)d->smoothing_radius : 2.0 * f.spacing, "smoothingRadius", &f.h));
+  f.compliance = d->compliance >= 0 ? d->compliance : 1e-4;
+  if (!std::isfinite(f.compliance)) return fail(PF_ERR_INVALID, "FluidSystem: compliance must be >= 0");
+  f.has_visc = (d->flags & PF_FLUID_VISCOSITY) != 0;
+  f.viscosity = d->viscosity;
+  if (f.has_visc && !std::isfinite(f.viscosity))
+    return fail(PF_ERR_INVALID, "FluidSystem: viscosity must be finite");
+  for (uint32_t b = 0; b < d->n_boundaries; ++b) {
+    RangeU r{d->boundaries[b].start, d->boundaries[b].count};
+    if (!range_ok(sp, r)) return fail(PF_ERR_INVALID, "FluidSystem.addBoundary: invalid particle range");
+    if (overlaps(r, f.range)) return fail(PF_ERR_INVALID, "FluidSystem.addBoundary: a boundary cannot overlap the fluid");
+    for (auto& o : f.bnd)
+      if (overlaps(r, o)) return fail(PF_ERR_INVALID, "FluidSystem.addBoundary: boundaries cannot overlap each other");
+    f.bnd.push_back(r);
+    f.bnd_static.push_back(d->boundary_static ? d->boundary_static[b] : 0);
+  }
+  // FluidSystem.ts:117-118: the fluid owns its particles' mass.
+  const double mass = f.rho0 * f.spacing * f.spacing * f.spacing;
+  const float w = (float)(1.0 / mass);
+  for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) sp.inv_mass[i] = w;
+  sp.fluids.push_back(std::move(f));
+  sp.materials.push_back({MAT_FLUID, (uint32_t)sp.fluids.size() - 1});
+  if (mat) *mat = (uint32_t)sp.materials.size() - 1;
+  return PF_OK;
+}
+
+pf_status pf_add_softbodies(pf_scene* s, const pf_softbody_desc* d, uint32_t* mat) {
+  PF_TRY(not_built(s, "SoftbodySystem"));
+  if (!d || d->n_bodies == 0) return fail(PF_ERR_INVALID, "SoftbodySystem: at least one body is required");
+  SceneSpec& sp = s->spec;
+  SoftSpec ss;
+  ss.local = d->shape_matching == PF_SHAPE_MATCH_LOCAL;
+  ss.rest4.assign(4ull * sp.cap, 0.0f);
+  ss.weights.assign(sp.cap, 0.0f);
+  std::vector<uint8_t> used(sp.cap, 0);
+  uint32_t span_lo = UINT32_MAX, span_hi = 0;
+  for (uint32_t b = 0; b < d->n_bodies; ++b) {
+    const pf_softbody_def& def = d->bodies[b];
+    const std::string who = "SoftbodySystem: body " + std::to_string(b);
+    RangeU r{def.range.start, def.range.count};
+    if (r.count == 0) return fail(PF_ERR_INVALID, who + " has no particles");
+    if (!range_ok(sp, r)) return fail(PF_ERR_INVALID, who + ": invalid particle range");
+    for (uint32_t i = r.start; i < r.start + r.count; ++i) {
+      if (used[i]) return fail(PF_ERR_INVALID, "SoftbodySystem: particle " + std::to_string(i) + " belongs to two bodies");
+      used[i] = 1;
+    }
+    std::vector<float> restp(3ull * r.count);
+    for (uint32_t k = 0; k < r.count; ++k)
+      for (int c = 0; c < 3; ++c)
+        restp[3 * k + c] = def.rest_positions ? def.rest_positions[3 * k + c] : sp.pos4[4ull * (r.start + k) + c];
+    const uint32_t surface = def.surface_count == UINT32_MAX ? r.count : def.surface_count;
+    if (surface > r.count) return fail(PF_ERR_INVALID, who + " surfaceCount is out of range");
+    for (uint32_t e = 0; e < def.n_edges; ++e) {
+      const uint32_t i = def.edges[2 * e], j = def.edges[2 * e + 1];
+      if (!(i < r.count) || !(j < r.count) || i == j) return fail(PF_ERR_INVALID, who + " has an invalid edge");
+    }
+    if (ss.local && def.n_edges == 0 && r.count > 1)
+      return fail(PF_ERR_INVALID, who + " needs edges for local shape matching");
+    // massWeights (SoftbodySystem.ts:366-372)
+    std::vector<double> masses(r.count);
+    std::vector<double> dyn;
+    for (uint32_t k = 0; k < r.count; ++k) {
+      const double w = sp.inv_mass[r.start + k];
+      masses[k] = w > 0 ? 1.0 / w : 0.0;
+      if (masses[k] > 0) dyn.push_back(masses[k]);
+    }
+    bool all_eq = true;
+    for (double m : dyn) all_eq = all_eq && m == dyn[0];
+    std::vector<float> bw(r.count, 1.0f);
+    if (!all_eq) {
+      double mean = 0;
+      for (double m : dyn) mean += m;
+      mean /= (double)dyn.size();
+      for (uint32_t k = 0; k < r.count; ++k) bw[k] = (float)(masses[k] > 0 ? masses[k] / mean : 1.0);
+    }
+    double cx = 0, cy = 0, cz = 0, tot = 0;
+    for (uint32_t k = 0; k < r.count; ++k) {
+      cx += (double)restp[3 * k] * bw[k];
+      cy += (double)restp[3 * k + 1] * bw[k];
+      cz += (double)restp[3 * k + 2] * bw[k];
+      tot += bw[k];
+    }
+    cx /= tot;
+    cy /= tot;
+    cz /= tot;
+    // assertVolumetric (SoftbodySystem.ts:392-421)
+    double xx = 0, xy = 0, xz = 0, yy = 0, yz = 0, zz = 0;
+    for (uint32_t k = 0; k < r.count; ++k) {
+      const double x = restp[3 * k] - cx, y = restp[3 * k + 1] - cy, z = restp[3 * k + 2] - cz;
+      xx += x * x; xy += x * y; xz += x * z; yy += y * y; yz += y * z; zz += z * z;
+    }
+    const double smallest = std::sqrt(std::max(0.0, smallest_eigenvalue(xx, xy, xz, yy, yz, zz)));
+    if (smallest < sp.radius * 1e-3)
+      return fail(PF_ERR_INVALID, who + " is flat; shape matching needs a 3D particle cloud");
+    if (!(def.compliance >= 0) || !std::isfinite(def.compliance))
+      return fail(PF_ERR_INVALID, "SoftbodySystem: compliance must be >= 0");
+    for (uint32_t k = 0; k < r.count; ++k) {
+      const uint32_t i = r.start + k;
+      ss.weights[i] = bw[k];
+      ss.rest4[4 * i] = (float)(restp[3 * k] - cx);
+      ss.rest4[4 * i + 1] = (float)(restp[3 * k + 1] - cy);
+      ss.rest4[4 * i + 2] = (float)(restp[3 * k + 2] - cz);
+      ss.rest4[4 * i + 3] = def.compliance;
+    }
+    BodySpec body;
+    body.range = r;
+    body.surface = surface;
+    body.compliance = def.compliance;
+    ss.bodies.push_back(body);
+    span_lo = std::min(span_lo, r.start);
+    span_hi = std::max(span_hi, r.start + r.count);
+  }
+  ss.span = {span_lo, span_hi - span_lo};
+  if (ss.local) {
+    // buildNeighborGraph (SoftbodySystem.ts:489-514)
+    std::vector<uint32_t> degree(sp.cap, 0);
+    for (uint32_t b = 0; b < d->n_bodies; ++b) {
+      const pf_softbody_def& def = d->bodies[b];
+      for (uint32_t k = 0; k < def.range.count; ++k) degree[def.range.start + k] += 1;
+      for (uint32_t e = 0; e < def.n_edges; ++e) {
+        degree[def.range.start + def.edges[2 * e]] += 1;
+        degree[def.range.start + def.edges[2 * e + 1]] += 1;
+      }
+    }
+    ss.offsets.assign(sp.cap + 1ull, 0);
+    for (uint32_t i = 0; i < sp.cap; ++i) ss.offsets[i + 1] = ss.offsets[i] + degree[i];
+    ss.indices.assign(std::max<uint32_t>(1, ss.offsets[sp.cap]), 0);
+    std::vector<uint32_t> cursor(ss.offsets.begin(), ss.offsets.begin() + sp.cap);
+    for (uint32_t b = 0; b < d->n_bodies; ++b) {
+      const pf_softbody_def& def = d->bodies[b];
+      for (uint32_t i = def.range.start; i < def.range.start + def.range.count; ++i) ss.indices[cursor[i]++] = i;
+      for (uint32_t e = 0; e < def.n_edges; ++e) {
+        const uint32_t i = def.range.start + def.edges[2 * e], j = def.range.start + def.edges[2 * e + 1];
+        ss.indices[cursor[i]++] = j;
+        ss.indices[cursor[j]++] = i;
+      }
+    }
+    // rest centres accumulated into f32 storage (SoftbodySystem.ts:283-295)
+    ss.rest_centers4.assign(4ull * sp.cap, 0.0f);
+    for (auto& body : ss.bodies)
+      for (uint32_t i = body.range.start; i < body.range.start + body.range.count; ++i) {
+        const uint32_t from = ss.offsets[i], to = ss.offsets[i + 1];
+        for (uint32_t k = from; k < to; ++k) {
+          const uint32_t j = ss.indices[k];
+          for (int a = 0; a < 3; ++a)
+            ss.rest_centers4[4 * i + a] =
+                (float)((double)ss.rest_centers4[4 * i + a] + (double)ss.rest4[4 * j + a] / (double)(to - from));
+        }
+      }
+  }
+  sp.softs.push_back(std::move(ss));
+  sp.materials.push_back({MAT_SOFT, (uint32_t)sp.softs.size() - 1});
+  if (mat) *mat = (uint32_t)sp.materials.size() - 1;
+  return PF_OK;
+}
+
+pf_status pf_add_cloth(pf_scene* s, const pf_cloth_desc* d, uint32_t* mat) {
+  PF_TRY(not_built(s, "ClothSystem"));
+  if (!d) return fail(PF_ERR_INVALID, "ClothSystem: options are NULL");
+  SceneSpec& sp = s->spec;
+  if (!range_ok(sp, {d->offset, d->n_particles}))
+    return fail(PF_ERR_INVALID, "ClothSystem: invalid particle range start=" + std::to_string(d->offset) +
+                                    " count=" + std::to_string(d->n_particles));
+  if (d->n_pairs == 0) return fail(PF_ERR_INVALID, "createDistanceConstraints: pairs is empty");
+  const double comp = d->stretch_compliance >= 0 ? d->stretch_compliance : 1e-7;
+  if (!std::isfinite(comp)) return fail(PF_ERR_INVALID, "ClothSystem: stretchCompliance must be >= 0");
+  for (uint32_t q = 0; q < d->n_pairs; ++q) {
+    const uint32_t i = d->pairs[2 * q], j = d->pairs[2 * q + 1];
+    if (i >= d->n_particles || j >= d->n_particles)
+      return fail(PF_ERR_INVALID, "createDistanceConstraints: pair has out-of-range index");
+    if (i == j) return fail(PF_ERR_INVALID, "createDistanceConstraints: pair references the same particle");
+  }
+  // ClothSystem.ts:131-140: positions and masses from the graph, velocity 0.
+  for (uint32_t k = 0; k < d->n_particles; ++k) {
+    const uint32_t i = d->offset + k;
+    for (int c = 0; c < 3; ++c) {
+      sp.pos4[4 * i + c] = d->positions[3 * k + c];
+      sp.vel4[4 * i + c] = 0.0f;
+    }
+    sp.pos4[4 * i + 3] = sp.vel4[4 * i + 3] = 0.0f;
+    sp.inv_mass[i] = d->inv_mass[k];
+  }
+  ClothSpec cl;
+  cl.offset = d->offset;
+  cl.n = d->n_particles;
+  cl.pairs.resize(2ull * d->n_pairs);
+  for (size_t q = 0; q < cl.pairs.size(); ++q) cl.pairs[q] = d->offset + d->pairs[q];
+  cl.rest.assign(d->rest_lengths, d->rest_lengths + d->n_pairs);
+  cl.compliance = (float)comp;
+  cl.colors = color_pairs(cl.pairs, d->n_pairs, sp.cap);
+  sp.cloths.push_back(std::move(cl));
+  sp.materials.push_back({MAT_CLOTH, (uint32_t)sp.cloths.size() - 1});
+  if (mat) *mat = (uint32_t)sp.materials.size() - 1;
+  return PF_OK;
+}
+
+pf_status pf_add_primitive(pf_scene* s, const pf_primitive* p, uint32_t* slot) {
+  PF_TRY(not_built(s, "PrimitiveSet"));
+  if (!p || p->kind > PF_PRIM_CAPSULE) return fail(PF_ERR_INVALID, "PrimitiveSet: unknown primitive kind");
+  if (!(p->data1[3] >= 0) || !(p->velocity[3] >= 0))
+    return fail(PF_ERR_INVALID, "PrimitiveSet: friction coefficients must be non-negative");
+  s->spec.prims.push_back(*p);
+  if (slot) *slot = (uint32_t)s->spec.prims.size() - 1;
+  return PF_OK;
+}
+
+pf_status pf_set_primitive(pf_scene* s, uint32_t slot, const pf_primitive* p) {
+  if (!s || !p) return fail(PF_ERR_INVALID, "PrimitiveSet: NULL argument");
+  if (slot >= s->spec.prims.size()) return fail(PF_ERR_INVALID, "PrimitiveSet: no primitive in slot " + std::to_string(slot));
+  if (s->world) return s->world->set_primitive(0, slot, *p);
+  s->spec.prims[slot] = *p;
+  return PF_OK;
+}
+
+pf_status pf_loop_build(pf_scene* s, const pf_loop_desc* d) {
+  PF_TRY(not_built(s, "SimLoop"));
+  if (!d) return fail(PF_ERR_INVALID, "SimLoop: options are NULL");
+  if (d->substeps < 1) return fail(PF_ERR_INVALID, "SimLoop: substeps must be an integer >= 1, got 0");
+  s->spec.loop = *d;
+  s->spec.built = true;
+  auto w = std::make_unique<World>();
+  const pf_status st = w->build({&s->spec}, false);
+  if (st != PF_OK) {
+    s->spec.built = false;
+    return st;
+  }
+  s->world = std::move(w);
+  return PF_OK;
+}
+
+pf_status pf_step(pf_scene* s, double dt) {
+  if (!s) return fail(PF_ERR_INVALID, "SimLoop: scene is NULL");
+  if (!s->world) return fail(PF_ERR_STATE, "SimLoop: build the loop before stepping");
+  return s->world->step(dt);
+}
+
+pf_status pf_readback(pf_scene* s, uint32_t field, void* dst, size_t bytes) {
+  if (!s || !dst) return fail(PF_ERR_INVALID, "readback: NULL argument");
+  if (s->world) return s->world->readback(0, field, dst, bytes);
+  const SceneSpec& sp = s->spec;
+  auto copy = [&](const void* src, size_t b) -> pf_status {
+    if (bytes < b) return fail(PF_ERR_INVALID, "readback: destination too small");
+    std::memcpy(dst, src, b);
+    return PF_OK;
+  };
+  switch (field) {
+    case PF_FIELD_POSITIONS:
+    case PF_FIELD_PREDICTED: return copy(sp.pos4.data(), 16ull * sp.cap);
+    case PF_FIELD_VELOCITIES: return copy(sp.vel4.data(), 16ull * sp.cap);
+    case PF_FIELD_INV_MASS: return copy(sp.inv_mass.data(), 4ull * sp.cap);
+    case PF_FIELD_BOUNDARY_VOLUME: return copy(sp.bvol.data(), 4ull * sp.cap);
+    case PF_FIELD_ROTATION:
+    case PF_FIELD_PREDICTED_ROTATION: return copy(sp.rot4.data(), 16ull * sp.cap);
+    case PF_FIELD_ANGULAR_VELOCITY: return copy(sp.angv4.data(), 16ull * sp.cap);
+    default: return fail(PF_ERR_STATE, "readback: field is available once the SimLoop is built");
+  }
+}
+
+pf_status pf_overflow_read(pf_scene* s, pf_overflow* out) {
+  if (!s || !out) return fail(PF_ERR_INVALID, "readbackOverflow: NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  if (!s->world) return PF_OK;
+  return s->world->overflow(0, out);
+}
+
+pf_status pf_last_step_ms(pf_scene* s, float* ms) {
+  if (!s || !ms || !s->world) return fail(PF_ERR_STATE, "SimLoop: no step has run");
+  return s->world->elapsed_ms(ms);
+}
+
+// ----------------------------------------------------------------- batch ----
+
+pf_status pf_batch_create(pf_scene* const* scenes, uint32_t n, const pf_batch_opts* opts, pf_batch** out) {
+  if (!scenes || !n || !out) return fail(PF_ERR_INVALID, "batch: no scenes");
+  auto b = std::make_unique<pf_batch>();
+  std::vector<SceneSpec*> specs;
+  for (uint32_t i = 0; i < n; ++i) {
+    pf_scene* s = scenes[i];
+    if (!s || !s->world) return fail(PF_ERR_STATE, "batch: scene " + std::to_string(i) + " has no built SimLoop");
+    auto copy = std::make_unique<SceneSpec>(s->spec);
+    PF_TRY(s->world->pull_state(0, copy.get()));
+    specs.push_back(copy.get());
+    b->specs.push_back(std::move(copy));
+  }
+  b->world = std::make_unique<World>();
+  PF_TRY(b->world->build(specs, opts ? opts->use_graph != 0 : true));
+  *out = b.release();
+  return PF_OK;
+}
+
+void pf_batch_destroy(pf_batch* b) { delete b; }
+
+pf_status pf_batch_step(pf_batch* b, double dt) {
+  if (!b) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->step(dt);
+}
+
+pf_status pf_batch_set_primitive(pf_batch* b, uint32_t index, uint32_t slot, const pf_primitive* p) {
+  if (!b || !p) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->set_primitive(index, slot, *p);
+}
+
+pf_status pf_batch_readback(pf_batch* b, uint32_t index, uint32_t field, void* dst, size_t bytes) {
+  if (!b || !dst) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->readback(index, field, dst, bytes);
+}
+
+pf_status pf_batch_overflow_read(pf_batch* b, uint32_t index, pf_overflow* out) {
+  if (!b || !out) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->overflow(index, out);
+}
+
+pf_status pf_batch_last_step_ms(pf_batch* b, float* ms) {
+  if (!b || !ms) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->elapsed_ms(ms);
+}
+
+uint64_t pf_batch_particle_substeps(pf_batch* b) { return b ? b->world->particle_substeps_per_step() : 0; }
+
+}  // extern "C"

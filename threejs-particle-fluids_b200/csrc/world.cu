@@ -1,0 +1,1561 @@
+// world.cu — stage kernels of the solver substep and the World host engine.
+//
+// One substep follows the reference's stage order (src/core/loop.ts:175-242):
+//   predict -> [grid rebuild: keys+histogram, stable sort, permute state]
+//   -> preSolve (collider lambda reset, boundary volumes, neighbour lists,
+//      multiplier resets) -> iterations x [materials in order, colliders +
+//      position apply] -> advect -> postSolve (XSPH, orientations)
+//   -> friction + velocity apply -> clock tick.
+// Every kernel covers all scenes of the world; a 256-slot block belongs to
+// one scene. Colliders add to their own particle only, so the reference's
+// fixed-point accumulate-then-apply is done in registers (same integer sums).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "world.cuh"
+#include "world_kernels.cuh"
+
+namespace pf {
+
+namespace {
+
+// ---------------------------------------------------------- frame start ----
+__global__ void k_frame_start(WorldView V, uint32_t nscenes) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nscenes) return;
+  const DevScene& S = V.scenes[s];
+  for (uint32_t f = 0; f < kNumFlags; ++f) V.flags[s * kNumFlags + f] = 0;
+  // PrimitiveSet.ts:400-402: clock = dt * (substeps - 1)
+  V.clocks[s] = S.dt * (S.substeps_f - 1.0f);
+}
+
+// PrimitiveSet.ts:403-405, once per substep after friction.
+__global__ void k_tick(WorldView V, uint32_t nscenes, uint32_t sub) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nscenes) return;
+  const DevScene& S = V.scenes[s];
+  if (sub >= S.substeps || S.prim_count == 0) return;
+  V.clocks[s] = fmaxf(V.clocks[s] - S.dt, 0.0f);
+}
+
+// ------------------------------------------------------------ integrate ----
+// integrate.ts:25-34
+__global__ void __launch_bounds__(kBlock) k_predict(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 x = V.cur.x[k];
+  if (!(x.w > 0.0f)) return;
+  const float4 v = V.cur.v[k];
+  const float dt = S.dt;
+  const f3 vel = xyz(v) + mk(S.gx, S.gy, S.gz) * dt;
+  V.cur.v[k] = with_w(vel, 0.0f);
+  V.cur.xs[k] = with_w(xyz(x) + vel * dt, x.w);
+}
+
+// integrate.ts:36-44
+__global__ void __launch_bounds__(kBlock) k_advect(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 x = V.cur.x[k];
+  if (!(x.w > 0.0f)) return;
+  const float4 xs = V.cur.xs[k];
+  V.cur.v[k] = with_w((xyz(xs) - xyz(x)) / S.dt, 0.0f);
+  V.cur.x[k] = xs;
+}
+
+// ---------------------------------------------------------------- grid ----
+// Keys by particle id (cell of the predicted position in the scene's linear
+// grid, offset by the scene's key base; dead padding goes to the scene's
+// last key) with a warp-aggregated histogram.
+__global__ void __launch_bounds__(kBlock) k_keys(WorldView V) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = k < V.n;
+  uint32_t key = 0;
+  bool clamped = false;
+  uint32_t s = 0;
+  if (valid) {
+    s = scene_index(V, k);
+    const DevScene& S = V.scenes[s];
+    const uint32_t id = V.ids[k];
+    if (id >= S.seg_start + S.cap) {
+      key = S.cell_base + S.cells;
+    } else if (S.has_grid) {
+      int32_t cx, cy, cz;
+      local_cell(S, xyz(V.cur.xs[k]), &cx, &cy, &cz, &clamped);
+      key = S.cell_base + (uint32_t)cx + S.dims[0] * ((uint32_t)cy + S.dims[1] * (uint32_t)cz);
+    } else {
+      key = S.cell_base + (id - S.seg_start);
+    }
+    V.keys[id] = key;
+  }
+  const uint32_t active = __ballot_sync(0xffffffffu, valid);
+  if (valid) {
+    const uint32_t peers = __match_any_sync(active, key);
+    if (lane_of() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(V.ccount + key, (uint32_t)__popc(peers));
+    if (clamped) atomicOr(V.flags + s * kNumFlags + FLAG_GRID, 1u);
+  }
+}
+
+// Gather the per-slot state into cell order: new slot k takes particle
+// perm[k] from its old slot inv[perm[k]]; per-substep sums start at zero.
+__global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t id = V.perm[k];
+  const uint32_t o = V.inv[id];
+  V.nxt.x[k] = V.cur.x[o];
+  V.nxt.xs[k] = V.cur.xs[o];
+  V.nxt.v[k] = V.cur.v[o];
+  V.nxt.bv[k] = V.cur.bv[o];
+  V.nxt.tag[k] = V.cur.tag[o];
+  V.ids[k] = id;
+  V.inv[id] = k;
+  for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
+  if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
+  if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
+}
+
+// Without a grid the slots never move; only the per-substep sums reset.
+__global__ void __launch_bounds__(kBlock) k_reset_sums(WorldView V) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
+  if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
+  if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------- fluid ----
+// boundaryVolume.ts:36-52: V_i = 1 / max(sum_j W(x_i - x_j), 1e-12) over the
+// particle's own boundary range, walking the grid (not the neighbour list).
+__global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_t want_static, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t b = tag_bnd(V.cur.tag[k]);
+  if (!b) return;
+  const DevBoundary B = V.bnds[b - 1];
+  if (B.is_static != want_static) return;
+  const DevScene& S = scene_at(V, k);
+  if (!want_static && sub >= S.substeps) return;
+  const DevFluid& F = V.fluids[B.fluid];
+  const float4* pos = want_static ? V.cur.x : V.cur.xs;
+  const f3 xi = xyz(pos[k]);
+  float sum = 0.0f;
+  walk27(S, V.cstart, V.ccount, xi, [&](uint32_t j) {
+    const uint32_t idj = V.ids[j];
+    if (idj < B.start || idj >= B.start + B.count) return true;
+    const f3 off = xi - xyz(pos[j]);
+    const float rsq = dot(off, off);
+    if (rsq >= F.hsq) return true;
+    sum += poly6(rsq, F);
+    return true;
+  });
+  V.cur.bv[k] = 1.0f / fmaxf(sum, 1e-12f);
+}
+
+// neighborList.ts:48-71: up to 64 neighbours within h at the predicted
+// positions of this substep, in walk order, self included; stored as slots,
+// column-major so a warp reads its m-th neighbours contiguously.
+__global__ void __launch_bounds__(kBlock) k_neighbors(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const DevFluid& F = V.fluids[f - 1];
+  const f3 xi = xyz(V.cur.xs[k]);
+  uint32_t cnt = 0;
+  bool over = false;
+  const uint32_t n = V.n;
+  walk27(S, V.cstart, V.ccount, xi, [&](uint32_t j) {
+    const f3 off = xi - xyz(V.cur.xs[j]);
+    if (dot_rn(off) < F.hsq) {
+      if (cnt < kMaxNbr) {
+        V.nbr[(size_t)cnt * n + k] = j;
+        ++cnt;
+      } else {
+        over = true;
+        return false;
+      }
+    }
+    return true;
+  });
+  V.ncount[k] = cnt;
+  if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
+}
+
+// lambda.ts:41-71
+__global__ void __launch_bounds__(kBlock) k_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const float4 xi4 = V.cur.xs[k];
+  const f3 xi = xyz(xi4);
+  float rho = 0.0f, gss = 0.0f;
+  f3 gs = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const uint32_t n = V.n;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = V.nbr[(size_t)m * n + k];
+    const float4 xj = V.cur.xs[j];
+    const float mass = neighbor_mass(V.cur.bv[j], xj.w, F.rho0);
+    const f3 off = xi - xyz(xj);
+    rho += mass * poly6(dot(off, off), F);
+    const f3 g = spiky_grad(off, F) * mass;
+    gs = gs + g;
+    gss += dot(g, g) * xj.w;
+  }
+  V.density[k] = rho;
+  const float C = rho * F.inv_rho0 - 1.0f;
+  if (C <= 0.0f) {
+    V.lambda[k] = 0.0f;
+    return;
+  }
+  const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
+  const float at = F.compliance / (S.dt * S.dt);
+  V.lambda[k] = -C / fmaxf(gn + at, 1e-20f);
+}
+
+// positionDelta.ts:41-85 (with the reaction on dynamic boundary neighbours).
+__global__ void __launch_bounds__(kBlock) k_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const float4 xi4 = V.cur.xs[k];
+  const f3 xi = xyz(xi4);
+  const float li = V.lambda[k];
+  const bool react = F.react_lo != F.react_hi && li != 0.0f;
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const uint32_t n = V.n;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = V.nbr[(size_t)m * n + k];
+    const float4 xj = V.cur.xs[j];
+    const float bvj = V.cur.bv[j];
+    const float mass = neighbor_mass(bvj, xj.w, F.rho0);
+    const f3 g = spiky_grad(xi - xyz(xj), F);
+    sum = sum + g * ((li + V.lambda[j]) * mass);
+    if (react && bvj > 0.0f && xj.w > 0.0f) {
+      const uint32_t idj = V.ids[j];
+      bool in = false;
+      for (uint32_t b = 0; b < F.bnd_count; ++b) {
+        const DevBoundary B = V.bnds[F.bnd_first + b];
+        in = in || (idj >= B.start && idj < B.start + B.count);
+      }
+      if (in) acc_add(V.acc_react, j, g * (-(li / F.rho0) * (F.rho0 * bvj) * xj.w), F.react_scale);
+    }
+  }
+  V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
+}
+
+// positionDelta.ts:217-226, then the reaction accumulator's apply over the
+// covering range of the fluid's boundaries (FluidSystem.ts:280-287).
+__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  float4 x = V.cur.xs[k];
+  bool changed = false;
+  if (f && V.fluids[f - 1].rank == rank) {
+    const float4 d = V.dx[k];
+    x.x += d.x;
+    x.y += d.y;
+    x.z += d.z;
+    changed = true;
+  }
+  if (V.acc_react) {
+    const uint32_t id = V.ids[k];
+    for (uint32_t q = 0; q < S.fluid_count; ++q) {
+      const DevFluid& F = V.fluids[S.fluid_first + q];
+      if (F.rank != rank || F.react_lo == F.react_hi) continue;
+      if (id < F.react_lo || id >= F.react_hi) continue;
+      int4 t = V.acc_react[k];
+      bool sat = false;
+      const f3 c = ticks_change(t.x, t.y, t.z, F.react_inv, &sat);
+      V.acc_react[k] = make_int4(0, 0, 0, 0);
+      x.x += c.x;
+      x.y += c.y;
+      x.z += c.z;
+      changed = true;
+      if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_REACT, 1u);
+    }
+  }
+  if (changed) V.cur.xs[k] = x;
+}
+
+// velocity.ts:43-70 (XSPH part) and 99-120 (apply).
+__global__ void __launch_bounds__(kBlock) k_xsph(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_visc) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const f3 xi = xyz(V.cur.x[k]);
+  const f3 vi = xyz(V.cur.v[k]);
+  f3 sm = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const uint32_t n = V.n;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = V.nbr[(size_t)m * n + k];
+    const f3 off = xi - xyz(V.cur.x[j]);
+    const f3 vj = xyz(V.cur.v[j]);
+    const float bvj = V.cur.bv[j];
+    const float vol = bvj > 0.0f ? bvj : F.volume;
+    sm = sm + ((vj - vi) * poly6(dot(off, off), F)) * vol;
+  }
+  V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_visc) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 d = V.dv[k];
+  float4 v = V.cur.v[k];
+  v.x += 0.0f + d.x;
+  v.y += 0.0f + d.y;
+  v.z += 0.0f + d.z;
+  V.cur.v[k] = v;
+}
+
+// ------------------------------------------------------------ colliders ----
+// PrimitiveSet.ts:339-365 with collider.ts:53-89, fused with the position
+// accumulator's apply (loop.ts:225): a primitive contact only adds to its own
+// particle, so the sum of rounded ticks is formed in registers.
+__global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (S.prim_count == 0 || sub >= S.substeps || it >= S.iterations) return;
+  const float4 xs4 = V.cur.xs[k];
+  const float w = xs4.w;
+  if (!(w > 0.0f)) return;
+  const f3 xstar = xyz(xs4);
+  const f3 disp = xstar - xyz(V.cur.x[k]);
+  const float clock = V.clocks[s];
+  const float radius = S.radius;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  bool any = false;
+  for (uint32_t p = 0; p < S.prim_count; ++p) {
+    const pf_primitive& P = V.prims[S.prim_base + p];
+    float phi;
+    f3 nrm;
+    prim_sdf(P, xstar, clock, &phi, &nrm);
+    if (!(phi < radius)) continue;
+    const f3 coldisp = prim_surface_velocity(P, xstar, clock) * S.dt;
+    const float depth = radius - phi;
+    float2 lam = V.plam[(size_t)k * V.prim_stride + p];
+    const float ln = lam.x + depth / w;
+    const f3 slip = disp - coldisp;
+    const f3 tang = slip - nrm * dot(slip, nrm);
+    const float tl = len(tang);
+    const bool sticks = tl > 1e-10f && (tl / w <= P.data1[3] * ln - lam.y);
+    const f3 push = nrm * depth;
+    const f3 c = sticks ? push - tang : push;
+    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
+    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
+    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
+    lam.x = ln;
+    lam.y = lam.y + (sticks ? tl / w : 0.0f);
+    V.plam[(size_t)k * V.prim_stride + p] = lam;
+    any = true;
+  }
+  if (!any) return;
+  bool sat = false;
+  const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
+  V.cur.xs[k] = with_w(xstar + c, w);
+  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_POS, 1u);
+}
+
+// PrimitiveSet.ts:367-398 with collider.ts:96-118, fused with the velocity
+// accumulator's apply (loop.ts:226-230).
+__global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (S.prim_count == 0 || sub >= S.substeps) return;
+  const float4 xs4 = V.cur.xs[k];
+  const float w = xs4.w;
+  if (!(w > 0.0f)) return;
+  const f3 xstar = xyz(xs4);
+  const f3 vel = xyz(V.cur.v[k]);
+  const float clock = V.clocks[s];
+  uint32_t tx = 0, ty = 0, tz = 0;
+  bool any = false;
+  for (uint32_t p = 0; p < S.prim_count; ++p) {
+    const float ln = V.plam[(size_t)k * V.prim_stride + p].x;
+    if (!(ln > 0.0f)) continue;
+    const pf_primitive& P = V.prims[S.prim_base + p];
+    float phi;
+    f3 g;
+    prim_sdf(P, xstar, clock, &phi, &g);
+    const float gl = len(g);
+    if (!(gl > 1e-6f)) continue;
+    const f3 nrm = g / gl;
+    const f3 rel = vel - prim_surface_velocity(P, xstar, clock);
+    const f3 vt = rel - nrm * dot(nrm, rel);
+    const float vtl = len(vt);
+    if (vtl > 1e-6f) {
+      const float change = fminf(P.velocity[3] * ln * w / S.dt, vtl);
+      const f3 c = neg((vt / vtl) * change);
+      tx += (uint32_t)to_ticks(c.x, S.vel_scale);
+      ty += (uint32_t)to_ticks(c.y, S.vel_scale);
+      tz += (uint32_t)to_ticks(c.z, S.vel_scale);
+      any = true;
+    }
+  }
+  if (!any) return;
+  bool sat = false;
+  const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.vel_inv, &sat);
+  V.cur.v[k] = with_w(vel + c, 0.0f);
+  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_VEL, 1u);
+}
+
+// ---------------------------------------------------------------- cloth ----
+// distance.ts:264-288 for one colour of constraints (no two share a particle).
+__global__ void __launch_bounds__(kBlock) k_cloth(WorldView V, uint32_t begin, uint32_t end, uint32_t sub,
+                                                  uint32_t it) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const DevScene& S = V.scenes[V.c_scene[q]];
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const uint32_t i = V.inv[V.c_i[q]], j = V.inv[V.c_j[q]];
+  const float4 xi = V.cur.xs[i], xj = V.cur.xs[j];
+  const float wi = xi.w, wj = xj.w;
+  const float ws = wi + wj;
+  const f3 off = xyz(xi) - xyz(xj);
+  const float l = len(off);
+  if (ws <= 0.0f || l < 1e-12f) return;
+  const f3 nrm = off / l;
+  const float lc = V.c_lambda[q];
+  const float at = V.c_comp[q] / (S.dt * S.dt);
+  const float dl = (-(l - V.c_rest[q]) - at * lc) / (ws + at);
+  V.cur.xs[i] = with_w(xyz(xi) + nrm * (wi * dl), wi);
+  V.cur.xs[j] = with_w(xyz(xj) - nrm * (wj * dl), wj);
+  V.c_lambda[q] = lc + dl;
+}
+
+// ---------------------------------------------------------- soft bodies ----
+__device__ __forceinline__ bool group_active(const WorldView& V, uint32_t g, uint32_t rank, uint32_t sub,
+                                             uint32_t it, const DevSoft** D, const DevScene** S) {
+  *D = &V.softs[V.grp_soft[g]];
+  *S = &V.scenes[(*D)->scene];
+  return (*D)->rank == rank && sub < (*S)->substeps && it < (*S)->iterations;
+}
+
+// rotation.ts:297-314
+__global__ void __launch_bounds__(kBlock) k_rot_predict(WorldView V, uint32_t sub) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft& D = V.softs[V.grp_soft[g]];
+  const DevScene& S = V.scenes[D.scene];
+  if (sub >= S.substeps) return;
+  const uint32_t i = V.grp[g];
+  const float4 q = V.q[i];
+  const f3 om = xyz(V.omega[i]);
+  const float mag = len(om);
+  if (mag < 1e-8f) {
+    V.qp[i] = q;
+    return;
+  }
+  const float half = mag * S.dt * 0.5f;
+  float sh, ch;
+  sincosf(half, &sh, &ch);
+  const f3 sx = om * (sh / mag);
+  const f3 qx = xyz(q);
+  const f3 nx = qx * ch + sx * q.w + cross(sx, qx);
+  V.qp[i] = with_w(nx, ch * q.w - dot(sx, qx));
+}
+
+// rotation.ts:316-343
+__global__ void __launch_bounds__(kBlock) k_rot_advect(WorldView V, uint32_t sub) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft& D = V.softs[V.grp_soft[g]];
+  const DevScene& S = V.scenes[D.scene];
+  if (sub >= S.substeps) return;
+  const uint32_t i = V.grp[g];
+  const float4 q = V.q[i];
+  float4 qp = V.qp[i];
+  const float dd = qp.x * qp.x + qp.y * qp.y + qp.z * qp.z + qp.w * qp.w;
+  const float nrm = sqrtf(fmaxf(dd, 1e-12f));
+  qp = make_float4(qp.x / nrm, qp.y / nrm, qp.z / nrm, qp.w / nrm);
+  const f3 qi = mk(-q.x, -q.y, -q.z);
+  const f3 qpx = xyz(qp);
+  const f3 rpre = qpx * q.w + qi * qp.w + cross(qpx, qi);
+  const float rwpre = qp.w * q.w - dot(qpx, qi);
+  const float flip = rwpre < 0.0f ? -1.0f : 1.0f;
+  const f3 rx = rpre * flip;
+  const float rw = rwpre * flip;
+  const float hs = len(rx);
+  if (hs < 1e-8f) {
+    V.omega[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  } else {
+    const float angle = atan2f(hs, rw) * 2.0f;
+    const f3 om = rx * ((angle / hs) / S.dt);
+    const float sc = sqrtf(1.0e4f / fmaxf(dot(om, om), 1.0e4f));
+    V.omega[i] = with_w(om * sc, 0.0f);
+  }
+  V.q[i] = qp;
+}
+
+// shapeMatchImplicit.ts:46-71
+__global__ void __launch_bounds__(kBlock) k_sm_center(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft* D;
+  const DevScene* S;
+  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
+  const uint32_t i = V.grp[g];
+  const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  for (uint32_t m = s; m < e; ++m) sum = sum + xyz(V.cur.xs[V.inv[V.csr_idx[m]]]);
+  const uint32_t cnt = e - s;
+  const float inv = 1.0f / (float)max(cnt, 1u);
+  V.centers[i] = cnt == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : with_w(sum * inv, 0.0f);
+}
+
+// shapeMatchImplicit.ts:100-217
+__global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft* D;
+  const DevScene* S;
+  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
+  const uint32_t i = V.grp[g];
+  const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
+  float a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const f3 c = xyz(V.centers[i]);
+  const f3 cb = xyz(V.rest_c[i]);
+  const float ai = D->ai;
+  for (uint32_t m = s; m < e; ++m) {
+    const uint32_t j = V.csr_idx[m];
+    const float4 qj = V.qp[j];
+    const float xx = qj.x * qj.x, yy = qj.y * qj.y, zz = qj.z * qj.z, xy = qj.x * qj.y, xz = qj.x * qj.z,
+                yz = qj.y * qj.z, wx = qj.w * qj.x, wy = qj.w * qj.y, wz = qj.w * qj.z;
+    a[0] += ai * (1.0f - (yy + zz) * 2.0f);
+    a[1] += ai * ((xy - wz) * 2.0f);
+    a[2] += ai * ((xz + wy) * 2.0f);
+    a[3] += ai * ((xy + wz) * 2.0f);
+    a[4] += ai * (1.0f - (xx + zz) * 2.0f);
+    a[5] += ai * ((yz - wx) * 2.0f);
+    a[6] += ai * ((xz - wy) * 2.0f);
+    a[7] += ai * ((yz + wx) * 2.0f);
+    a[8] += ai * (1.0f - (xx + yy) * 2.0f);
+    const f3 xj = xyz(V.cur.xs[V.inv[j]]) - c;
+    const f3 xt = xyz(V.rest[j]) - cb;
+    a[0] += xj.x * xt.x;
+    a[1] += xj.x * xt.y;
+    a[2] += xj.x * xt.z;
+    a[3] += xj.y * xt.x;
+    a[4] += xj.y * xt.y;
+    a[5] += xj.y * xt.z;
+    a[6] += xj.z * xt.x;
+    a[7] += xj.z * xt.y;
+    a[8] += xj.z * xt.z;
+  }
+  float r[9];
+  polar3(a, r);
+  if (e == s) {
+    r[0] = 1; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 1; r[5] = 0; r[6] = 0; r[7] = 0; r[8] = 1;
+  }
+  V.rot3[3 * (size_t)i + 0] = make_float4(r[0], r[1], r[2], 0.0f);
+  V.rot3[3 * (size_t)i + 1] = make_float4(r[3], r[4], r[5], 0.0f);
+  V.rot3[3 * (size_t)i + 2] = make_float4(r[6], r[7], r[8], 0.0f);
+}
+
+// shapeMatchImplicit.ts:248-308
+__global__ void __launch_bounds__(kBlock) k_sm_scatter(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft* D;
+  const DevScene* S;
+  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
+  const uint32_t i = V.grp[g];
+  const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
+  const f3 R0 = xyz(V.rot3[3 * (size_t)i]), R1 = xyz(V.rot3[3 * (size_t)i + 1]), R2 = xyz(V.rot3[3 * (size_t)i + 2]);
+  const f3 c = xyz(V.centers[i]);
+  const f3 cb = xyz(V.rest_c[i]);
+  const float at = V.rest[i].w / (S->dt * S->dt);
+  for (uint32_t m = s; m < e; ++m) {
+    const uint32_t j = V.csr_idx[m];
+    const uint32_t sj = V.inv[j];
+    const f3 rr = xyz(V.rest[j]) - cb;
+    const f3 goal = mk(dot(R0, rr), dot(R1, rr), dot(R2, rr)) + c;
+    const float4 xj = V.cur.xs[sj];
+    const f3 C = xyz(xj) - goal;
+    const float wj = xj.w;
+    const float denom = wj + at;
+    const f3 lo = xyz(V.pair_lambda[m]);
+    const f3 dl = (neg(C) - lo * at) / denom;
+    V.pair_lambda[m] = with_w(lo + dl, 0.0f);
+    const float mj = fmaxf((float)(V.csr_off[j + 1] - V.csr_off[j]), 1.0f);
+    const f3 dx = (dl * wj) / mj;
+    const float sc = sqrtf(D->maxc2 / fmaxf(dot(dx, dx), D->maxc2));
+    acc_add(V.acc_soft, sj, dx * sc, S->sb_scale);
+  }
+}
+
+// accumulator.ts:148-178 over every particle of scenes with a local system at this rank.
+__global__ void __launch_bounds__(kBlock) k_soft_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (!((S.soft_local_ranks >> rank) & 1u) || sub >= S.substeps || it >= S.iterations) return;
+  const int4 t = V.acc_soft[k];
+  if (!(t.x | t.y | t.z)) return;
+  bool sat = false;
+  const f3 c = ticks_change(t.x, t.y, t.z, S.sb_inv, &sat);
+  V.acc_soft[k] = make_int4(0, 0, 0, 0);
+  const float4 x = V.cur.xs[k];
+  V.cur.xs[k] = with_w(xyz(x) + c, x.w);
+  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_SOFT, 1u);
+}
+
+// shapeMatchImplicit.ts:325-401
+__global__ void __launch_bounds__(kBlock) k_sm_qp(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_grp) return;
+  const DevSoft* D;
+  const DevScene* S;
+  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
+  const uint32_t i = V.grp[g];
+  if (V.csr_off[i + 1] <= V.csr_off[i]) return;
+  const float4 r0 = V.rot3[3 * (size_t)i], r1 = V.rot3[3 * (size_t)i + 1], r2 = V.rot3[3 * (size_t)i + 2];
+  const float m00 = r0.x, m01 = r0.y, m02 = r0.z, m10 = r1.x, m11 = r1.y, m12 = r1.z, m20 = r2.x, m21 = r2.y,
+              m22 = r2.z;
+  const float tr = m00 + m11 + m22;
+  float qx, qy, qz, qw;
+  if (tr > 0.0f) {
+    const float sq = 0.5f / sqrtf(tr + 1.0f);
+    qw = 0.25f / sq;
+    qx = (m21 - m12) * sq;
+    qy = (m02 - m20) * sq;
+    qz = (m10 - m01) * sq;
+  } else if (m00 > m11 && m00 > m22) {
+    const float sq = 2.0f * sqrtf(1.0f + m00 - m11 - m22);
+    qw = (m21 - m12) / sq;
+    qx = 0.25f * sq;
+    qy = (m01 + m10) / sq;
+    qz = (m02 + m20) / sq;
+  } else if (m11 > m22) {
+    const float sq = 2.0f * sqrtf(1.0f + m11 - m00 - m22);
+    qw = (m02 - m20) / sq;
+    qx = (m01 + m10) / sq;
+    qy = 0.25f * sq;
+    qz = (m12 + m21) / sq;
+  } else {
+    const float sq = 2.0f * sqrtf(1.0f + m22 - m00 - m11);
+    qw = (m10 - m01) / sq;
+    qx = (m02 + m20) / sq;
+    qy = (m12 + m21) / sq;
+    qz = 0.25f * sq;
+  }
+  const float4 q0 = V.q[i];
+  const float d = q0.x * qx + q0.y * qy + q0.z * qz + q0.w * qw;
+  const float fl = d < 0.0f ? -1.0f : 1.0f;
+  V.qp[i] = make_float4(qx * fl, qy * fl, qz * fl, qw * fl);
+}
+
+// shapeMatch.ts:53-229: one 256-thread block per body reduces the centre of
+// mass and A = sum m x r^T (strided partial sums, then a tree), and thread 0
+// takes the polar decomposition.
+__global__ void __launch_bounds__(256) k_body_frame(WorldView V, uint32_t rank, uint32_t sub, uint32_t it,
+                                                    uint32_t require_global) {
+  const uint32_t b = blockIdx.x;
+  if (b >= V.n_bodies) return;
+  const DevBody B = V.bodies[b];
+  const DevSoft& D = V.softs[B.soft];
+  const DevScene& S = V.scenes[B.scene];
+  if (D.rank != rank || sub >= S.substeps || it >= S.iterations) return;
+  if (require_global && D.local) return;
+  __shared__ float4 s4[256];
+  __shared__ float sr[9][256];
+  const uint32_t t = threadIdx.x;
+  float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t li = t; li < B.count; li += 256) {
+    const uint32_t id = B.start + li;
+    const float mi = V.weights[id];
+    const f3 xi = xyz(V.cur.xs[V.inv[id]]);
+    acc.x += xi.x * mi;
+    acc.y += xi.y * mi;
+    acc.z += xi.z * mi;
+    acc.w += mi;
+    const f3 xw = xi * mi;
+    const f3 ri = xyz(V.rest[id]);
+    r[0] += ri.x * xw.x; r[1] += ri.y * xw.x; r[2] += ri.z * xw.x;
+    r[3] += ri.x * xw.y; r[4] += ri.y * xw.y; r[5] += ri.z * xw.y;
+    r[6] += ri.x * xw.z; r[7] += ri.y * xw.z; r[8] += ri.z * xw.z;
+  }
+  s4[t] = acc;
+  for (int m = 0; m < 9; ++m) sr[m][t] = r[m];
+  __syncthreads();
+  for (uint32_t st = 128; st > 0; st >>= 1) {
+    if (t < st) {
+      const float4 o = s4[t + st];
+      s4[t] = make_float4(s4[t].x + o.x, s4[t].y + o.y, s4[t].z + o.z, s4[t].w + o.w);
+      for (int m = 0; m < 9; ++m) sr[m][t] += sr[m][t + st];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    const float4 tot = s4[0];
+    V.body_c[b] = make_float4(tot.x / tot.w, tot.y / tot.w, tot.z / tot.w, 0.0f);
+    float a[9], rr[9];
+    for (int m = 0; m < 9; ++m) a[m] = sr[m][0];
+    polar3(a, rr);
+    V.body_r[3 * b + 0] = make_float4(rr[0], rr[1], rr[2], 0.0f);
+    V.body_r[3 * b + 1] = make_float4(rr[3], rr[4], rr[5], 0.0f);
+    V.body_r[3 * b + 2] = make_float4(rr[6], rr[7], rr[8], 0.0f);
+  }
+}
+
+// shapeMatch.ts:277-351
+__global__ void __launch_bounds__(256) k_global_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t b = blockIdx.x;
+  if (b >= V.n_bodies) return;
+  const DevBody B = V.bodies[b];
+  const DevSoft& D = V.softs[B.soft];
+  const DevScene& S = V.scenes[B.scene];
+  if (D.local || D.rank != rank || sub >= S.substeps || it >= S.iterations) return;
+  const f3 R0 = xyz(V.body_r[3 * b]), R1 = xyz(V.body_r[3 * b + 1]), R2 = xyz(V.body_r[3 * b + 2]);
+  const f3 c = xyz(V.body_c[b]);
+  const float at = B.compliance / (S.dt * S.dt);
+  for (uint32_t li = threadIdx.x; li < B.count; li += 256) {
+    const uint32_t id = B.start + li;
+    const uint32_t sl = V.inv[id];
+    const f3 ri = xyz(V.rest[id]);
+    const f3 goal = mk(dot(R0, ri), dot(R1, ri), dot(R2, ri)) + c;
+    const float4 xs = V.cur.xs[sl];
+    const f3 C = xyz(xs) - goal;
+    const f3 lo = xyz(V.lambda_g[id]);
+    const f3 dl = (neg(C) - lo * at) / (xs.w + at);
+    V.lambda_g[id] = with_w(lo + dl, 0.0f);
+    V.cur.xs[sl] = with_w(xyz(xs) + dl * xs.w, xs.w);
+  }
+}
+
+template <typename K, typename... A>
+void launch_slots(K kernel, uint32_t n, cudaStream_t st, A... args) {
+  if (n == 0) return;
+  kernel<<<div_up(n, kBlock), kBlock, 0, st>>>(args...);
+}
+
+size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+// ================================================================ World ====
+
+World::~World() {
+  for (auto& g : graph_)
+    if (g) cudaGraphExecDestroy(g);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+  if (arena_) cudaFree(arena_);
+  if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
+  if (h_pinned_prims_) cudaFreeHost(h_pinned_prims_);
+}
+
+WorldView World::view(uint32_t parity) const {
+  WorldView v = base_;
+  v.cur = buf_[parity & 1];
+  v.nxt = buf_[(parity & 1) ^ 1];
+  return v;
+}
+
+uint64_t World::particle_substeps_per_step() const {
+  uint64_t t = 0;
+  for (auto* s : specs_) t += (uint64_t)s->cap * s->loop.substeps;
+  return t;
+}
+
+namespace {
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += al256(sizeof(T) * std::max<size_t>(count, 1));
+    return p;
+  }
+};
+
+float f32(double v) { return static_cast<float>(v); }
+}  // namespace
+
+pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
+  specs_ = specs;
+  use_graph_ = use_graph;
+  (void)sm_count();  // cache the SM count outside any stream capture
+  const uint32_t K = (uint32_t)specs.size();
+  if (K == 0) return fail(PF_ERR_INVALID, "SimLoop: no scenes to build");
+  // ---- segments, grids, materials -----------------------------------
+  uint64_t slot = 0, cell = 0;
+  h_scenes_.assign(K, DevScene{});
+  h_fluids_.clear();
+  h_bnds_.clear();
+  h_softs_.clear();
+  h_bodies_.clear();
+  h_prims_.clear();
+  max_rank_ = max_sub_ = max_iter_ = 0;
+  prim_stride_ = 1;
+  for (uint32_t s = 0; s < K; ++s) {
+    const SceneSpec& sp = *specs[s];
+    DevScene& S = h_scenes_[s];
+    S.seg_start = (uint32_t)slot;
+    S.cap = sp.cap;
+    S.seg_end = (uint32_t)(slot + ((sp.cap + kSegAlign - 1) / kSegAlign) * kSegAlign);
+    slot = S.seg_end;
+    S.substeps = sp.loop.substeps ? sp.loop.substeps : 4;
+    S.iterations = sp.loop.iterations;
+    S.substeps_f = (float)S.substeps;
+    S.gx = sp.loop.gravity[0];
+    S.gy = sp.loop.gravity[1];
+    S.gz = sp.loop.gravity[2];
+    S.radius = f32(sp.radius);
+    S.pos_scale = f32(std::floor(1073741824.0 / 10.0));
+    S.pos_inv = f32(1.0 / std::floor(1073741824.0 / 10.0));
+    S.vel_scale = f32(std::floor(1073741824.0 / 50.0));
+    S.vel_inv = f32(1.0 / std::floor(1073741824.0 / 50.0));
+    S.sb_scale = S.pos_scale;
+    S.sb_inv = S.pos_inv;
+    max_sub_ = std::max(max_sub_, S.substeps);
+    max_iter_ = std::max(max_iter_, S.iterations);
+    max_rank_ = std::max(max_rank_, (uint32_t)sp.materials.size());
+    // grid
+    double h = 0;
+    for (auto& f : sp.fluids) h = std::max(h, f.h);
+    S.has_grid = h > 0;
+    if (S.has_grid) {
+      const float cs = f32(h);
+      S.cell = cs;
+      S.ox = sp.loop.hash_origin[0];
+      S.oy = sp.loop.hash_origin[1];
+      S.oz = sp.loop.hash_origin[2];
+      double mn[3], mx[3];
+      bool auto_bounds = false;
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = sp.loop.grid_min[a];
+        mx[a] = sp.loop.grid_max[a];
+        auto_bounds = auto_bounds || !(mx[a] > mn[a]);
+      }
+      if (auto_bounds) {
+        for (int a = 0; a < 3; ++a) {
+          mn[a] = 1e30;
+          mx[a] = -1e30;
+        }
+        for (uint32_t i = 0; i < sp.cap; ++i)
+          for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(mn[a], (double)sp.pos4[4 * i + a]);
+            mx[a] = std::max(mx[a], (double)sp.pos4[4 * i + a]);
+          }
+        for (int a = 0; a < 3; ++a) {
+          const double ext = std::max(mx[a] - mn[a], 4 * h);
+          mn[a] -= 0.5 * ext;
+          mx[a] += 0.5 * ext;
+        }
+      }
+      const double org[3] = {S.ox, S.oy, S.oz};
+      uint64_t cells = 1;
+      for (int a = 0; a < 3; ++a) {
+        const int64_t lo = (int64_t)std::floor((mn[a] - org[a]) / cs) - 2;
+        const int64_t hi = (int64_t)std::floor((mx[a] - org[a]) / cs) + 2;
+        S.lo[a] = (int32_t)lo;
+        S.dims[a] = (uint32_t)(hi - lo + 1);
+        cells *= S.dims[a];
+      }
+      if (cells > (1ull << 27))
+        return fail(PF_ERR_INVALID, "SimLoop: neighbour grid over " + std::to_string(cells) +
+                                        " cells; give tighter grid bounds");
+      S.cells = (uint32_t)cells;
+    } else {
+      S.cells = sp.cap;
+    }
+    S.cell_base = (uint32_t)cell;
+    cell += (uint64_t)S.cells + 1;
+    // primitives
+    S.prim_base = (uint32_t)h_prims_.size();
+    S.prim_count = (uint32_t)sp.prims.size();
+    for (auto& p : sp.prims) h_prims_.push_back(p);
+    prim_stride_ = std::max(prim_stride_, S.prim_count);
+    // fluids
+    S.fluid_first = (uint32_t)h_fluids_.size();
+    S.fluid_count = (uint32_t)sp.fluids.size();
+    S.soft_local_ranks = 0;
+    for (uint32_t r = 0; r < sp.materials.size(); ++r) {
+      const MatKind kind = sp.materials[r].first;
+      const uint32_t idx = sp.materials[r].second;
+      if (kind == MAT_FLUID) {
+        const FluidSpec& fs = sp.fluids[idx];
+        DevFluid F{};
+        F.scene = s;
+        F.rank = r;
+        F.rho0 = f32(fs.rho0);
+        F.inv_rho0 = 1.0f / F.rho0;
+        F.volume = f32(fs.spacing * fs.spacing * fs.spacing);
+        F.h = f32(fs.h);
+        F.hsq = f32(fs.h * fs.h);
+        F.poly6 = f32(315.0 / (64.0 * M_PI * std::pow(fs.h, 9)));
+        F.spiky = f32(45.0 / (M_PI * std::pow(fs.h, 6)));
+        F.compliance = f32(fs.compliance);
+        F.c_xsph = f32(fs.viscosity);
+        F.has_visc = fs.has_visc ? 1u : 0u;
+        F.bnd_first = (uint32_t)h_bnds_.size();
+        F.bnd_count = (uint32_t)fs.bnd.size();
+        uint32_t lo = UINT32_MAX, hi = 0;
+        for (size_t b = 0; b < fs.bnd.size(); ++b) {
+          DevBoundary B{};
+          B.start = S.seg_start + fs.bnd[b].start;
+          B.count = fs.bnd[b].count;
+          B.fluid = (uint32_t)h_fluids_.size();
+          B.is_static = fs.bnd_static[b];
+          lo = std::min(lo, B.start);
+          hi = std::max(hi, B.start + B.count);
+          h_bnds_.push_back(B);
+          any_static_bnd_ = any_static_bnd_ || B.is_static;
+          any_dyn_bnd_ = any_dyn_bnd_ || !B.is_static;
+        }
+        F.react_lo = fs.bnd.empty() ? 0 : lo;
+        F.react_hi = fs.bnd.empty() ? 0 : hi;
+        any_react_ = any_react_ || !fs.bnd.empty();
+        F.react_scale = S.pos_scale;
+        F.react_inv = S.pos_inv;
+        any_fluid_ = true;
+        any_visc_ = any_visc_ || fs.has_visc;
+        h_fluids_.push_back(F);
+      } else if (kind == MAT_SOFT) {
+        const SoftSpec& ss = sp.softs[idx];
+        DevSoft D{};
+        D.scene = s;
+        D.rank = r;
+        D.local = ss.local ? 1u : 0u;
+        D.ai = f32(sp.radius * sp.radius / 5.0);
+        const double maxc = 5.0 * sp.radius;
+        D.maxc2 = f32(maxc * maxc);
+        const uint32_t di = (uint32_t)h_softs_.size();
+        h_softs_.push_back(D);
+        for (auto& b : ss.bodies) {
+          DevBody Bd{};
+          Bd.scene = s;
+          Bd.soft = di;
+          Bd.start = S.seg_start + b.range.start;
+          Bd.count = b.range.count;
+          Bd.compliance = f32(b.compliance);
+          h_bodies_.push_back(Bd);
+        }
+        if (ss.local) {
+          S.soft_local_ranks |= 1u << r;
+          any_soft_local_ = true;
+        } else {
+          any_soft_global_ = true;
+        }
+      }
+    }
+    any_grid_ = any_grid_ || S.has_grid;
+    any_prims_ = any_prims_ || S.prim_count > 0;
+  }
+  if (max_rank_ > 32) return fail(PF_ERR_INVALID, "SimLoop: at most 32 materials per scene");
+  n_ = (uint32_t)slot;
+  cells_ = (uint32_t)cell;
+  // ---- cloth constraints by (rank, colour) ----------------------------
+  std::vector<uint32_t> ci, cj, csc;
+  std::vector<float> crest, ccomp;
+  cloth_ranges_.assign(max_rank_, {});
+  for (uint32_t r = 0; r < max_rank_; ++r) {
+    uint32_t ncol = 0;
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      if (r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)
+        ncol = std::max(ncol, (uint32_t)sp.cloths[sp.materials[r].second].colors.size());
+    }
+    for (uint32_t c = 0; c < ncol; ++c) {
+      const uint32_t begin = (uint32_t)ci.size();
+      for (uint32_t s = 0; s < K; ++s) {
+        const SceneSpec& sp = *specs[s];
+        if (!(r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)) continue;
+        const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+        if (c >= cl.colors.size()) continue;
+        const uint32_t base = h_scenes_[s].seg_start;
+        for (uint32_t q : cl.colors[c]) {
+          ci.push_back(base + cl.pairs[2 * q]);
+          cj.push_back(base + cl.pairs[2 * q + 1]);
+          crest.push_back(cl.rest[q]);
+          ccomp.push_back(cl.compliance);
+          csc.push_back(s);
+        }
+      }
+      cloth_ranges_[r].push_back({begin, (uint32_t)ci.size()});
+    }
+  }
+  // ---- soft-body tables (global by id) ----------------------------------
+  std::vector<uint32_t> grp, grp_soft, csr_off(n_ + 1, 0), csr_idx;
+  std::vector<float> rest4(4ull * n_, 0.0f), restc4(4ull * n_, 0.0f), weights(n_, 0.0f);
+  {
+    uint32_t di = 0;
+    std::vector<uint32_t> deg(n_, 0);
+    std::vector<std::pair<uint32_t, const SoftSpec*>> locals;  // (scene, spec)
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      const uint32_t base = h_scenes_[s].seg_start;
+      for (uint32_t r = 0; r < sp.materials.size(); ++r) {
+        if (sp.materials[r].first != MAT_SOFT) continue;
+        const SoftSpec& ss = sp.softs[sp.materials[r].second];
+        for (uint32_t i = 0; i < sp.cap; ++i) {
+          if (ss.weights[i] != 0.0f || ss.rest4[4 * i + 3] != 0.0f || ss.rest4[4 * i] != 0.0f ||
+              ss.rest4[4 * i + 1] != 0.0f || ss.rest4[4 * i + 2] != 0.0f) {
+            for (int c = 0; c < 4; ++c) rest4[4ull * (base + i) + c] = ss.rest4[4 * i + c];
+            weights[base + i] = ss.weights[i];
+          }
+        }
+        if (ss.local) {
+          for (uint32_t i = ss.span.start; i < ss.span.start + ss.span.count; ++i) {
+            grp.push_back(base + i);
+            grp_soft.push_back(di);
+            deg[base + i] = ss.offsets[i + 1] - ss.offsets[i];
+            for (int c = 0; c < 4; ++c) restc4[4ull * (base + i) + c] = ss.rest_centers4[4 * i + c];
+          }
+          locals.push_back({s, &ss});
+        }
+        ++di;
+      }
+    }
+    for (uint32_t i = 0; i < n_; ++i) csr_off[i + 1] = csr_off[i] + deg[i];
+    csr_idx.assign(std::max<uint32_t>(1, csr_off[n_]), 0);
+    for (auto& [s, ss] : locals) {
+      const uint32_t base = h_scenes_[s].seg_start;
+      for (uint32_t i = ss->span.start; i < ss->span.start + ss->span.count; ++i) {
+        const uint32_t from = ss->offsets[i], to = ss->offsets[i + 1];
+        for (uint32_t k = from; k < to; ++k) csr_idx[csr_off[base + i] + (k - from)] = base + ss->indices[k];
+      }
+    }
+  }
+  // ---- chunk table and per-slot state ----------------------------------
+  std::vector<uint32_t> chunk(n_ / kSegAlign, 0);
+  for (uint32_t s = 0; s < K; ++s)
+    for (uint32_t c = h_scenes_[s].seg_start / kSegAlign; c < h_scenes_[s].seg_end / kSegAlign; ++c) chunk[c] = s;
+  std::vector<float4> x(n_), v(n_), q(n_), om(n_);
+  std::vector<float> bv(n_, 0.0f), dens(n_, 0.0f);
+  std::vector<uint32_t> tag(n_, 0), ids(n_);
+  for (uint32_t i = 0; i < n_; ++i) {
+    x[i] = make_float4(0, 0, 0, 0);
+    v[i] = make_float4(0, 0, 0, 0);
+    q[i] = make_float4(0, 0, 0, 1);
+    om[i] = make_float4(0, 0, 0, 0);
+    ids[i] = i;
+  }
+  for (uint32_t s = 0; s < K; ++s) {
+    const SceneSpec& sp = *specs[s];
+    const uint32_t base = h_scenes_[s].seg_start;
+    for (uint32_t i = 0; i < sp.cap; ++i) {
+      x[base + i] = make_float4(sp.pos4[4 * i], sp.pos4[4 * i + 1], sp.pos4[4 * i + 2], sp.inv_mass[i]);
+      v[base + i] = make_float4(sp.vel4[4 * i], sp.vel4[4 * i + 1], sp.vel4[4 * i + 2], 0.0f);
+      bv[base + i] = sp.bvol[i];
+      if (!sp.rot4.empty())
+        q[base + i] = make_float4(sp.rot4[4 * i], sp.rot4[4 * i + 1], sp.rot4[4 * i + 2], sp.rot4[4 * i + 3]);
+      if (!sp.angv4.empty()) om[base + i] = make_float4(sp.angv4[4 * i], sp.angv4[4 * i + 1], sp.angv4[4 * i + 2], 0.0f);
+    }
+    for (uint32_t f = 0; f < h_scenes_[s].fluid_count; ++f) {
+      const FluidSpec& fs = sp.fluids[f];
+      for (uint32_t i = fs.range.start; i < fs.range.start + fs.range.count; ++i) {
+        tag[base + i] = (tag[base + i] & 0xffff0000u) | (h_scenes_[s].fluid_first + f + 1);
+        dens[base + i] = f32(fs.rho0);
+      }
+    }
+  }
+  for (uint32_t b = 0; b < h_bnds_.size(); ++b) {
+    const DevBoundary& B = h_bnds_[b];
+    for (uint32_t i = B.start; i < B.start + B.count; ++i) tag[i] = (tag[i] & 0xffffu) | ((b + 1) << 16);
+  }
+  // ---- allocate one arena ----------------------------------------------
+  const size_t N = n_;
+  const size_t P = prim_stride_;
+  const bool need_soft = !grp.empty() || !h_bodies_.empty();
+  auto layout = [&](Carver& cv) {
+    base_.scenes_rw = cv.take<DevScene>(K);
+    base_.chunk_scene = cv.take<uint32_t>(chunk.size());
+    base_.flags = cv.take<uint32_t>(K * kNumFlags);
+    base_.clocks = cv.take<float>(K);
+    base_.fluids = cv.take<DevFluid>(h_fluids_.size());
+    base_.bnds = cv.take<DevBoundary>(h_bnds_.size());
+    base_.prims = cv.take<pf_primitive>(h_prims_.size());
+    for (int b = 0; b < 2; ++b) {
+      buf_[b].x = cv.take<float4>(N);
+      buf_[b].xs = cv.take<float4>(N);
+      buf_[b].v = cv.take<float4>(N);
+      buf_[b].bv = cv.take<float>(N);
+      buf_[b].tag = cv.take<uint32_t>(N);
+    }
+    base_.ids = cv.take<uint32_t>(N);
+    base_.inv = cv.take<uint32_t>(N);
+    base_.keys = cv.take<uint32_t>(N);
+    base_.perm = cv.take<uint32_t>(N);
+    base_.cstart = cv.take<uint32_t>(cells_);
+    base_.ccount = cv.take<uint32_t>(cells_);
+    base_.nbr = any_fluid_ ? cv.take<uint32_t>(N * kMaxNbr) : nullptr;
+    base_.ncount = cv.take<uint32_t>(N);
+    base_.lambda = cv.take<float>(N);
+    base_.density = cv.take<float>(N);
+    base_.dx = cv.take<float4>(N);
+    base_.dv = cv.take<float4>(N);
+    base_.plam = cv.take<float2>(N * P);
+    base_.acc_react = any_react_ ? cv.take<int4>(N) : nullptr;
+    base_.acc_soft = any_soft_local_ ? cv.take<int4>(N) : nullptr;
+    base_.softs = cv.take<DevSoft>(h_softs_.size());
+    base_.bodies = cv.take<DevBody>(h_bodies_.size());
+    base_.grp = cv.take<uint32_t>(grp.size());
+    base_.grp_soft = cv.take<uint32_t>(grp_soft.size());
+    base_.csr_off = need_soft ? cv.take<uint32_t>(N + 1) : nullptr;
+    base_.csr_idx = cv.take<uint32_t>(csr_idx.size());
+    base_.rest = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.rest_c = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.weights = need_soft ? cv.take<float>(N) : nullptr;
+    base_.centers = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.rot3 = need_soft ? cv.take<float4>(3 * N) : nullptr;
+    base_.q = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.qp = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.omega = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.pair_lambda = cv.take<float4>(csr_idx.size());
+    base_.lambda_g = need_soft ? cv.take<float4>(N) : nullptr;
+    base_.body_c = cv.take<float4>(h_bodies_.size());
+    base_.body_r = cv.take<float4>(3 * h_bodies_.size());
+    base_.c_i = cv.take<uint32_t>(ci.size());
+    base_.c_j = cv.take<uint32_t>(cj.size());
+    base_.c_rest = cv.take<float>(crest.size());
+    base_.c_comp = cv.take<float>(ccomp.size());
+    base_.c_scene = cv.take<uint32_t>(csc.size());
+    base_.c_lambda = cv.take<float>(ci.size());
+  };
+  Carver probe{nullptr};
+  layout(probe);
+  const size_t sort_bytes = sort_scratch_bytes(n_, cells_);
+  bytes_ = probe.off + al256(sort_bytes);
+  if (cudaMalloc(&arena_, bytes_) != cudaSuccess) {
+    cudaGetLastError();
+    arena_ = nullptr;
+    return fail(PF_ERR_OOM, "SimLoop: out of device memory (" + std::to_string(bytes_) + " bytes)");
+  }
+  Carver cv{static_cast<char*>(arena_)};
+  layout(cv);
+  sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, cells_, &sort_);
+  base_.scenes = base_.scenes_rw;
+  base_.n = n_;
+  base_.prim_stride = prim_stride_;
+  base_.n_grp = (uint32_t)grp.size();
+  base_.n_bodies = (uint32_t)h_bodies_.size();
+  base_.n_cons = (uint32_t)ci.size();
+  pair_entries_ = any_soft_local_ ? csr_idx.size() : 0;
+  PF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  PF_CUDA(cudaEventCreate(&ev0_));
+  PF_CUDA(cudaEventCreate(&ev1_));
+  PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
+  PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
+  // ---- upload ----------------------------------------------------------
+  auto up = [&](const void* dst, const void* src, size_t bytes) -> pf_status {
+    if (bytes == 0) return PF_OK;
+    PF_CUDA(cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, stream_));
+    return PF_OK;
+  };
+  PF_CUDA(cudaMemsetAsync(arena_, 0, probe.off, stream_));
+  PF_TRY(up(base_.scenes_rw, h_scenes_.data(), sizeof(DevScene) * K));
+  PF_TRY(up(base_.chunk_scene, chunk.data(), 4 * chunk.size()));
+  PF_TRY(up(base_.fluids, h_fluids_.data(), sizeof(DevFluid) * h_fluids_.size()));
+  PF_TRY(up(base_.bnds, h_bnds_.data(), sizeof(DevBoundary) * h_bnds_.size()));
+  PF_TRY(up(base_.prims, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size()));
+  PF_TRY(up(buf_[0].x, x.data(), 16 * N));
+  PF_TRY(up(buf_[0].xs, x.data(), 16 * N));
+  PF_TRY(up(buf_[0].v, v.data(), 16 * N));
+  PF_TRY(up(buf_[0].bv, bv.data(), 4 * N));
+  PF_TRY(up(buf_[0].tag, tag.data(), 4 * N));
+  PF_TRY(up(base_.ids, ids.data(), 4 * N));
+  PF_TRY(up(base_.inv, ids.data(), 4 * N));
+  PF_TRY(up(base_.density, dens.data(), 4 * N));
+  PF_TRY(up(base_.softs, h_softs_.data(), sizeof(DevSoft) * h_softs_.size()));
+  PF_TRY(up(base_.bodies, h_bodies_.data(), sizeof(DevBody) * h_bodies_.size()));
+  PF_TRY(up(base_.grp, grp.data(), 4 * grp.size()));
+  PF_TRY(up(base_.grp_soft, grp_soft.data(), 4 * grp_soft.size()));
+  if (need_soft) {
+    PF_TRY(up(base_.csr_off, csr_off.data(), 4 * csr_off.size()));
+    PF_TRY(up(base_.csr_idx, csr_idx.data(), 4 * csr_idx.size()));
+    PF_TRY(up(base_.rest, rest4.data(), 16 * N));
+    PF_TRY(up(base_.rest_c, restc4.data(), 16 * N));
+    PF_TRY(up(base_.weights, weights.data(), 4 * N));
+    PF_TRY(up(base_.q, q.data(), 16 * N));
+    PF_TRY(up(base_.qp, q.data(), 16 * N));
+    PF_TRY(up(base_.omega, om.data(), 16 * N));
+    std::vector<float4> ident(3 * h_bodies_.size());
+    for (size_t b = 0; b < h_bodies_.size(); ++b) {
+      ident[3 * b] = make_float4(1, 0, 0, 0);
+      ident[3 * b + 1] = make_float4(0, 1, 0, 0);
+      ident[3 * b + 2] = make_float4(0, 0, 1, 0);
+    }
+    PF_TRY(up(base_.body_r, ident.data(), 16 * ident.size()));
+  }
+  PF_TRY(up(base_.c_i, ci.data(), 4 * ci.size()));
+  PF_TRY(up(base_.c_j, cj.data(), 4 * cj.size()));
+  PF_TRY(up(base_.c_rest, crest.data(), 4 * crest.size()));
+  PF_TRY(up(base_.c_comp, ccomp.data(), 4 * ccomp.size()));
+  PF_TRY(up(base_.c_scene, csc.data(), 4 * csc.size()));
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  parity_ = 0;
+  inited_ = true;
+  for (auto* sp : specs_)
+    if (!sp->initialized) inited_ = false;
+  prims_dirty_ = false;
+  return PF_OK;
+}
+
+pf_status World::set_primitive(uint32_t scene, uint32_t slot, const pf_primitive& p) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "PrimitiveSet: no such scene");
+  const DevScene& S = h_scenes_[scene];
+  if (slot >= S.prim_count) return fail(PF_ERR_INVALID, "PrimitiveSet: no primitive in slot " + std::to_string(slot));
+  h_prims_[S.prim_base + slot] = p;
+  specs_[scene]->prims[slot] = p;
+  prims_dirty_ = true;
+  return PF_OK;
+}
+
+pf_status World::upload_params(double dt) {
+  const uint32_t K = (uint32_t)h_scenes_.size();
+  for (uint32_t s = 0; s < K; ++s) h_scenes_[s].dt = f32(dt / h_scenes_[s].substeps);
+  std::memcpy(h_pinned_scenes_, h_scenes_.data(), sizeof(DevScene) * K);
+  PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, h_pinned_scenes_, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
+  if (prims_dirty_ && !h_prims_.empty()) {
+    std::memcpy(h_pinned_prims_, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size());
+    PF_CUDA(cudaMemcpyAsync(const_cast<pf_primitive*>(base_.prims), h_pinned_prims_,
+                            sizeof(pf_primitive) * h_prims_.size(), cudaMemcpyHostToDevice, stream_));
+    prims_dirty_ = false;
+  }
+  return PF_OK;
+}
+
+void World::launch_frame_start_at(uint32_t parity) {
+  const uint32_t K = (uint32_t)h_scenes_.size();
+  k_frame_start<<<div_up(K, 128), 128, 0, stream_>>>(view(parity), K);
+}
+
+// Keys of the current predicted positions, stable sort, permute into the
+// other buffer; `parity` names the current buffer.
+void World::run_sort_and_permute(uint32_t parity, bool) {
+  const WorldView V = view(parity);
+  cudaMemsetAsync(V.ccount, 0, 4ull * cells_, stream_);
+  cudaMemsetAsync(sort_.counters, 0, 4ull * kNumCounters, stream_);
+  launch_slots(k_keys, n_, stream_, V);
+  launch_sort_from_hist(V.keys, n_, cells_, V.ccount, V.cstart, V.perm, sort_, stream_);
+  launch_slots(k_permute, n_, stream_, V);
+}
+
+void World::run_init_pass() {
+  // FluidSystem.ts:228-231 + loop.ts:237: static boundaries get their volume
+  // once, from committed positions, after a grid rebuild.
+  if (!any_static_bnd_) return;
+  run_sort_and_permute(parity_, true);
+  parity_ ^= 1;
+  launch_slots(k_boundary_volume, n_, stream_, view(parity_), 1u, 0u);
+}
+
+void World::run_substep(uint32_t s, uint32_t parity) {
+  WorldView V = view(parity);
+  launch_slots(k_predict, n_, stream_, V, s);
+  if (any_soft_local_) launch_slots(k_rot_predict, base_.n_grp, stream_, V, s);
+  if (any_grid_) {
+    run_sort_and_permute(parity, false);
+    V = view(parity ^ 1);
+  } else {
+    launch_slots(k_reset_sums, n_, stream_, V);
+  }
+  // preSolve
+  if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
+  if (any_fluid_) launch_slots(k_neighbors, n_, stream_, V, s);
+  // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
+  if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
+  if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
+  if (base_.n_cons) cudaMemsetAsync(base_.c_lambda, 0, 4ull * base_.n_cons, stream_);
+  // iterations
+  for (uint32_t it = 0; it < max_iter_; ++it) {
+    for (uint32_t r = 0; r < max_rank_; ++r) {
+      bool has_fluid = false, has_local = false, has_global = false;
+      for (auto& F : h_fluids_) has_fluid = has_fluid || F.rank == r;
+      for (auto& D : h_softs_) {
+        has_local = has_local || (D.rank == r && D.local);
+        has_global = has_global || (D.rank == r && !D.local);
+      }
+      if (has_fluid) {
+        launch_slots(k_lambda, n_, stream_, V, r, s, it);
+        launch_slots(k_delta, n_, stream_, V, r, s, it);
+        launch_slots(k_fluid_apply, n_, stream_, V, r, s, it);
+      }
+      if (has_local) {
+        launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
+        launch_slots(k_sm_moment, base_.n_grp, stream_, V, r, s, it);
+        launch_slots(k_sm_scatter, base_.n_grp, stream_, V, r, s, it);
+        launch_slots(k_soft_apply, n_, stream_, V, r, s, it);
+        launch_slots(k_sm_qp, base_.n_grp, stream_, V, r, s, it);
+      }
+      if (has_global && base_.n_bodies) {
+        k_body_frame<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it, 1u);
+        k_global_apply<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it);
+      }
+      if (r < cloth_ranges_.size())
+        for (auto& rg : cloth_ranges_[r])
+          if (rg.second > rg.first)
+            k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, stream_>>>(V, rg.first, rg.second, s, it);
+    }
+    if (any_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
+  }
+  launch_slots(k_advect, n_, stream_, V, s);
+  for (uint32_t r = 0; r < max_rank_; ++r) {
+    bool has_visc = false, has_local = false;
+    for (auto& F : h_fluids_) has_visc = has_visc || (F.rank == r && F.has_visc);
+    for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
+    if (has_visc) {
+      launch_slots(k_xsph, n_, stream_, V, r, s);
+      launch_slots(k_xsph_apply, n_, stream_, V, r, s);
+    }
+    if (has_local) {
+      launch_slots(k_rot_advect, base_.n_grp, stream_, V, s);
+      if (base_.n_bodies) k_body_frame<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, 0u, 0u);
+    }
+  }
+  if (any_prims_) {
+    launch_slots(k_friction, n_, stream_, V, s);
+    const uint32_t K = (uint32_t)h_scenes_.size();
+    k_tick<<<div_up(K, 128), 128, 0, stream_>>>(V, K, s);
+  }
+}
+
+pf_status World::step(double dt) {
+  if (!(dt > 0) || !std::isfinite(dt))
+    return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
+  PF_TRY(upload_params(dt));
+  PF_CUDA(cudaEventRecord(ev0_, stream_));
+  if (!inited_) {
+    run_init_pass();
+    inited_ = true;
+    for (auto* sp : specs_) sp->initialized = true;
+  }
+  const uint32_t flips = any_grid_ ? (max_sub_ & 1u) : 0u;
+  auto body = [&](uint32_t p0) {
+    launch_frame_start_at(p0);
+    uint32_t p = p0;
+    for (uint32_t s = 0; s < max_sub_; ++s) {
+      run_substep(s, p);
+      if (any_grid_) p ^= 1;
+    }
+  };
+  if (use_graph_) {
+    cudaGraphExec_t& g = graph_[parity_];
+    if (!g) {
+      cudaGraph_t graph;
+      PF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      body(parity_);
+      PF_CUDA(cudaStreamEndCapture(stream_, &graph));
+      const cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(PF_ERR_CUDA, std::string("SimLoop: graph instantiate: ") + cudaGetErrorString(e));
+    }
+    PF_CUDA(cudaGraphLaunch(g, stream_));
+  } else {
+    body(parity_);
+  }
+  parity_ ^= flips;
+  PF_CUDA(cudaEventRecord(ev1_, stream_));
+  PF_CUDA(cudaGetLastError());
+  return PF_OK;
+}
+
+
+pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t bytes) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "readback: no such scene");
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  const DevScene& S = h_scenes_[scene];
+  const uint32_t cap = S.cap, seg = S.seg_end - S.seg_start;
+  const StateBuf& B = buf_[parity_];
+  std::vector<uint32_t> ids(seg);
+  PF_CUDA(cudaMemcpy(ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+  auto need = [&](size_t b) -> pf_status {
+    if (bytes < b) return fail(PF_ERR_INVALID, "readback: destination holds " + std::to_string(bytes) +
+                                                   " bytes, need " + std::to_string(b));
+    return PF_OK;
+  };
+  auto by_slot4 = [&](const float4* src, bool zero_w, bool w_only) -> pf_status {
+    std::vector<float4> tmp(seg);
+    PF_CUDA(cudaMemcpy(tmp.data(), src + S.seg_start, 16ull * seg, cudaMemcpyDeviceToHost));
+    if (w_only) {
+      PF_TRY(need(4ull * cap));
+      float* o = static_cast<float*>(dst);
+      for (uint32_t k = 0; k < seg; ++k) {
+        const uint32_t id = ids[k] - S.seg_start;
+        if (id < cap) o[id] = tmp[k].w;
+      }
+      return PF_OK;
+    }
+    PF_TRY(need(16ull * cap));
+    float4* o = static_cast<float4*>(dst);
+    for (uint32_t k = 0; k < seg; ++k) {
+      const uint32_t id = ids[k] - S.seg_start;
+      if (id < cap) o[id] = zero_w ? make_float4(tmp[k].x, tmp[k].y, tmp[k].z, 0.0f) : tmp[k];
+    }
+    return PF_OK;
+  };
+  auto by_slot1 = [&](const float* src, bool fluid_only) -> pf_status {
+    PF_TRY(need(4ull * cap));
+    std::vector<float> tmp(seg);
+    std::vector<uint32_t> tag(seg);
+    PF_CUDA(cudaMemcpy(tmp.data(), src + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+    PF_CUDA(cudaMemcpy(tag.data(), B.tag + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+    float* o = static_cast<float*>(dst);
+    for (uint32_t k = 0; k < seg; ++k) {
+      const uint32_t id = ids[k] - S.seg_start;
+      if (id < cap) o[id] = (fluid_only && !tag_fluid(tag[k])) ? 0.0f : tmp[k];
+    }
+    return PF_OK;
+  };
+  auto by_id4 = [&](const float4* src) -> pf_status {
+    PF_TRY(need(16ull * cap));
+    if (!src) {
+      float4* o = static_cast<float4*>(dst);
+      for (uint32_t i = 0; i < cap; ++i) o[i] = make_float4(0, 0, 0, field == PF_FIELD_ANGULAR_VELOCITY ? 0.0f : 1.0f);
+      return PF_OK;
+    }
+    PF_CUDA(cudaMemcpy(dst, src + S.seg_start, 16ull * cap, cudaMemcpyDeviceToHost));
+    return PF_OK;
+  };
+  switch (field) {
+    case PF_FIELD_POSITIONS: return by_slot4(B.x, true, false);
+    case PF_FIELD_PREDICTED: return by_slot4(B.xs, true, false);
+    case PF_FIELD_VELOCITIES: return by_slot4(B.v, true, false);
+    case PF_FIELD_INV_MASS: return by_slot4(B.x, false, true);
+    case PF_FIELD_BOUNDARY_VOLUME: return by_slot1(B.bv, false);
+    case PF_FIELD_DENSITY: return by_slot1(base_.density, true);
+    case PF_FIELD_LAMBDA: return by_slot1(base_.lambda, true);
+    case PF_FIELD_ROTATION: return by_id4(base_.q);
+    case PF_FIELD_PREDICTED_ROTATION: return by_id4(base_.qp);
+    case PF_FIELD_ANGULAR_VELOCITY: return by_id4(base_.omega);
+    case PF_FIELD_CELL_PERM: {
+      PF_TRY(need(4ull * cap));
+      uint32_t* o = static_cast<uint32_t*>(dst);
+      uint32_t w = 0;
+      for (uint32_t k = 0; k < seg && w < cap; ++k) {
+        const uint32_t id = ids[k] - S.seg_start;
+        if (id < cap) o[w++] = id;
+      }
+      return PF_OK;
+    }
+    case PF_FIELD_NEIGHBOR_COUNT:
+    case PF_FIELD_NEIGHBORS: {
+      const bool lists = field == PF_FIELD_NEIGHBORS;
+      PF_TRY(need(4ull * cap * (lists ? kMaxNbr : 1)));
+      std::vector<uint32_t> cnt(seg), tag(seg);
+      PF_CUDA(cudaMemcpy(cnt.data(), base_.ncount + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+      PF_CUDA(cudaMemcpy(tag.data(), B.tag + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+      uint32_t* o = static_cast<uint32_t*>(dst);
+      if (!lists) {
+        for (uint32_t k = 0; k < seg; ++k) {
+          const uint32_t id = ids[k] - S.seg_start;
+          if (id < cap) o[id] = tag_fluid(tag[k]) ? cnt[k] : 0u;
+        }
+        return PF_OK;
+      }
+      std::fill(o, o + (size_t)cap * kMaxNbr, 0xffffffffu);
+      if (!base_.nbr) return PF_OK;
+      std::vector<uint32_t> col(seg), all_ids(n_);
+      PF_CUDA(cudaMemcpy(all_ids.data(), base_.ids, 4ull * n_, cudaMemcpyDeviceToHost));
+      for (uint32_t m = 0; m < kMaxNbr; ++m) {
+        PF_CUDA(cudaMemcpy(col.data(), base_.nbr + (size_t)m * n_ + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+        for (uint32_t k = 0; k < seg; ++k) {
+          const uint32_t id = ids[k] - S.seg_start;
+          if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k]) continue;
+          o[(size_t)id * kMaxNbr + m] = all_ids[col[k]] - S.seg_start;
+        }
+      }
+      return PF_OK;
+    }
+    default:
+      return fail(PF_ERR_INVALID, "readback: unknown field " + std::to_string(field));
+  }
+}
+
+pf_status World::pull_state(uint32_t scene, SceneSpec* sp) {
+  const uint32_t cap = h_scenes_[scene].cap;
+  std::vector<float4> t(cap);
+  PF_TRY(readback(scene, PF_FIELD_POSITIONS, t.data(), 16ull * cap));
+  for (uint32_t i = 0; i < cap; ++i) {
+    sp->pos4[4 * i] = t[i].x;
+    sp->pos4[4 * i + 1] = t[i].y;
+    sp->pos4[4 * i + 2] = t[i].z;
+  }
+  PF_TRY(readback(scene, PF_FIELD_VELOCITIES, t.data(), 16ull * cap));
+  for (uint32_t i = 0; i < cap; ++i) {
+    sp->vel4[4 * i] = t[i].x;
+    sp->vel4[4 * i + 1] = t[i].y;
+    sp->vel4[4 * i + 2] = t[i].z;
+  }
+  PF_TRY(readback(scene, PF_FIELD_INV_MASS, sp->inv_mass.data(), 4ull * cap));
+  PF_TRY(readback(scene, PF_FIELD_BOUNDARY_VOLUME, sp->bvol.data(), 4ull * cap));
+  sp->rot4.resize(4ull * cap);
+  sp->angv4.resize(4ull * cap);
+  PF_TRY(readback(scene, PF_FIELD_ROTATION, sp->rot4.data(), 16ull * cap));
+  PF_TRY(readback(scene, PF_FIELD_ANGULAR_VELOCITY, sp->angv4.data(), 16ull * cap));
+  return PF_OK;
+}
+
+pf_status World::overflow(uint32_t scene, pf_overflow* out) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "readbackOverflow: no such scene");
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  uint32_t f[kNumFlags];
+  PF_CUDA(cudaMemcpy(f, base_.flags + scene * kNumFlags, sizeof(f), cudaMemcpyDeviceToHost));
+  uint32_t err = 0;
+  PF_CUDA(cudaMemcpy(&err, sort_.counters + kCounterError, 4, cudaMemcpyDeviceToHost));
+  out->positions = f[FLAG_POS] | f[FLAG_SOFT] | f[FLAG_REACT];
+  out->velocities = f[FLAG_VEL];
+  out->grid = f[FLAG_GRID];
+  out->contacts = f[FLAG_CONTACTS];
+  out->neighbors = f[FLAG_NBR];
+  out->device_error = err | f[FLAG_DEVICE];
+  return PF_OK;
+}
+
+pf_status World::elapsed_ms(float* ms) {
+  PF_CUDA(cudaEventSynchronize(ev1_));
+  PF_CUDA(cudaEventElapsedTime(ms, ev0_, ev1_));
+  last_ms_ = *ms;
+  return PF_OK;
+}
+
+}  // namespace pf

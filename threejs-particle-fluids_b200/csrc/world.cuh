@@ -1,0 +1,291 @@
+// world.cuh — the solver engine: one "world" packs one or more independent
+// scenes (ParticleSystem + materials + colliders + SimLoop each) into shared
+// device arrays and steps all of them with one launch per solver stage.
+//
+// Layout (B200-first):
+//  * Each scene owns a segment of slots [seg_start, seg_end), 256-aligned, so
+//    every 256-thread block belongs to exactly one scene and reads its
+//    parameters uniformly. Particle ids equal slots at creation; after every
+//    grid rebuild the per-slot state is physically permuted into cell order
+//    (stable: ascending id inside a cell), so neighbour gathers and per-slot
+//    passes are coalesced float4 loads. ids[slot] and inv[id] map between the
+//    two orders; materials with topology (cloth pairs, shape-matching groups)
+//    address particles by id through inv[].
+//  * Scenes with a fluid get a bounded linear grid (cell = smoothing radius)
+//    at a private key offset; one stable counting sort covers every scene.
+//  * Per-slot state (x, x*, v, boundary volume, material tag) is
+//    double-buffered; the permutation gathers from one buffer into the other.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "grid_sort.cuh"
+#include "pfsim.h"
+
+namespace pf {
+
+constexpr uint32_t kSegAlign = 256;
+constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts:14)
+constexpr uint32_t kBlock = 256;
+
+// ------------------------------------------------------------- host spec ----
+struct RangeU {
+  uint32_t start = 0, count = 0;
+  bool contains(uint32_t i) const { return i >= start && i < start + count; }
+};
+
+struct FluidSpec {
+  RangeU range;
+  double rho0, spacing, h, compliance, viscosity;
+  bool has_visc;
+  std::vector<RangeU> bnd;
+  std::vector<uint8_t> bnd_static;
+};
+
+struct BodySpec {
+  RangeU range;
+  uint32_t surface;
+  double compliance;
+};
+
+struct SoftSpec {
+  bool local = true;
+  std::vector<BodySpec> bodies;
+  RangeU span;
+  std::vector<float> rest4;        // float4 per particle of the scene (cap)
+  std::vector<float> weights;      // per particle (cap)
+  std::vector<uint32_t> offsets;   // CSR by particle (cap + 1), local mode
+  std::vector<uint32_t> indices;   // CSR members (particle indices)
+  std::vector<float> rest_centers4;  // float4 per particle, local mode
+};
+
+struct ClothSpec {
+  uint32_t offset = 0, n = 0;
+  std::vector<uint32_t> pairs;  // absolute particle indices
+  std::vector<float> rest;
+  float compliance = 1e-7f;
+  std::vector<std::vector<uint32_t>> colors;  // constraint indices per colour
+};
+
+enum MatKind : uint32_t { MAT_FLUID = 0, MAT_SOFT = 1, MAT_CLOTH = 2 };
+
+struct SceneSpec {
+  uint32_t cap = 0;
+  double radius = 0;
+  std::vector<float> pos4, vel4, inv_mass, bvol;
+  std::vector<float> rot4, angv4;  // orientation state (identity / zero)
+  std::vector<uint32_t> group;
+  std::vector<std::pair<MatKind, uint32_t>> materials;
+  std::vector<FluidSpec> fluids;
+  std::vector<SoftSpec> softs;
+  std::vector<ClothSpec> cloths;
+  std::vector<pf_primitive> prims;
+  pf_loop_desc loop{};
+  bool built = false;
+  bool initialized = false;  // the one-time init pass (static boundaries) ran
+};
+
+// ----------------------------------------------------------- device data ----
+struct DevScene {
+  uint32_t seg_start, seg_end, cap;
+  uint32_t substeps, iterations;
+  float gx, gy, gz;
+  float dt;        // substep length (per step)
+  float substeps_f;
+  float radius;    // particle radius as an f32 literal
+  uint32_t has_grid;
+  uint32_t cell_base, cells;  // dead cell = cell_base + cells
+  float ox, oy, oz, cell;
+  int32_t lo[3];
+  uint32_t dims[3];
+  uint32_t prim_base, prim_count;
+  float pos_scale, pos_inv, vel_scale, vel_inv;
+  float sb_scale, sb_inv;
+  uint32_t fluid_first, fluid_count;  // this scene's fluids in the fluid table
+  uint32_t soft_local_ranks;          // bit r: a local shape-matching system at material rank r
+};
+
+struct DevFluid {
+  uint32_t scene, rank;
+  float rho0, inv_rho0, volume, h, hsq, poly6, spiky, compliance, c_xsph;
+  uint32_t has_visc;
+  uint32_t bnd_first, bnd_count;
+  uint32_t react_lo, react_hi;  // covering id range of the boundaries (lo == hi: no reaction)
+  float react_scale, react_inv;
+};
+
+struct DevBoundary {
+  uint32_t start, count;  // absolute ids
+  uint32_t fluid;
+  uint32_t is_static;
+};
+
+struct DevSoft {
+  uint32_t scene, rank, local;
+  float ai, maxc2;
+};
+
+struct DevBody {
+  uint32_t scene, soft;  // soft = index into DevSoft
+  uint32_t start, count; // absolute ids
+  float compliance;
+};
+
+// Per-scene overflow words (SimLoopOverflow + neighbour-list flag).
+enum FlagIdx : uint32_t {
+  FLAG_POS = 0,
+  FLAG_VEL = 1,
+  FLAG_GRID = 2,
+  FLAG_CONTACTS = 3,
+  FLAG_NBR = 4,
+  FLAG_SOFT = 5,
+  FLAG_REACT = 6,
+  FLAG_DEVICE = 7,
+  kNumFlags = 8
+};
+
+// Per-slot tag: low 16 bits fluid index + 1, high 16 bits boundary index + 1.
+__host__ __device__ inline uint32_t tag_fluid(uint32_t t) { return t & 0xffffu; }
+__host__ __device__ inline uint32_t tag_bnd(uint32_t t) { return t >> 16; }
+
+struct StateBuf {
+  float4* x = nullptr;   // committed positions, w = inverse mass
+  float4* xs = nullptr;  // predicted positions, w = inverse mass
+  float4* v = nullptr;   // velocities
+  float* bv = nullptr;   // boundary volume
+  uint32_t* tag = nullptr;
+};
+
+// Everything a stage kernel needs, passed by value.
+struct WorldView {
+  uint32_t n;            // total slots
+  uint32_t prim_stride;  // primitives per slot in the collider lambda array
+  const DevScene* scenes;
+  const uint32_t* chunk_scene;  // scene of each 256-slot chunk
+  DevScene* scenes_rw;
+  uint32_t* flags;              // kNumFlags per scene
+  float* clocks;                // collider sweep clock per scene (PrimitiveSet.motionClock)
+  const DevFluid* fluids;
+  const DevBoundary* bnds;
+  const pf_primitive* prims;
+  StateBuf cur, nxt;
+  uint32_t* ids;
+  uint32_t* inv;
+  uint32_t* keys;     // by id
+  uint32_t* perm;     // new slot -> id (sort output)
+  uint32_t* cstart;
+  uint32_t* ccount;
+  uint32_t* nbr;      // kMaxNbr * n, column-major
+  uint32_t* ncount;
+  float* lambda;
+  float* density;
+  float4* dx;
+  float4* dv;
+  float2* plam;       // (lambda_n, lambda_t) per slot x primitive
+  int4* acc_react;    // fixed-point reaction sums per slot
+  int4* acc_soft;     // fixed-point shape-matching sums per slot
+  // soft bodies (by id unless noted)
+  const DevSoft* softs;
+  const DevBody* bodies;
+  const uint32_t* grp;       // group ids (local shape matching)
+  const uint32_t* grp_soft;  // soft index per group
+  uint32_t n_grp;
+  const uint32_t* csr_off;   // by id, n + 1
+  const uint32_t* csr_idx;
+  const float4* rest;        // rest offsets, w = compliance
+  const float4* rest_c;      // neighbourhood rest centres
+  const float* weights;
+  float4* centers;
+  float4* rot3;              // 3 rows per id
+  float4* q;                 // orientation
+  float4* qp;                // predicted orientation
+  float4* omega;             // angular velocity
+  float4* pair_lambda;       // per CSR entry
+  float4* lambda_g;          // global matching multipliers per id
+  float4* body_c;            // per body
+  float4* body_r;            // 3 rows per body
+  uint32_t n_bodies;
+  // cloth
+  const uint32_t* c_i;
+  const uint32_t* c_j;
+  const float* c_rest;
+  const float* c_comp;
+  const uint32_t* c_scene;
+  float* c_lambda;
+  uint32_t n_cons;
+};
+
+class World {
+ public:
+  World() = default;
+  ~World();
+  World(const World&) = delete;
+  World& operator=(const World&) = delete;
+
+  // Pack `specs` (their current host state) into device arrays.
+  pf_status build(const std::vector<SceneSpec*>& specs, bool use_graph);
+  pf_status step(double dt);
+  pf_status set_primitive(uint32_t scene, uint32_t slot, const pf_primitive& p);
+  pf_status readback(uint32_t scene, uint32_t field, void* dst, size_t bytes);
+  // Copies the scene's state (by particle index) back into its spec.
+  pf_status pull_state(uint32_t scene, SceneSpec* spec);
+  pf_status overflow(uint32_t scene, pf_overflow* out);
+  // Device milliseconds between the start and end events of the last step.
+  pf_status elapsed_ms(float* ms);
+  cudaStream_t stream() const { return stream_; }
+  uint32_t scene_count() const { return (uint32_t)specs_.size(); }
+  uint64_t particle_substeps_per_step() const;
+  size_t device_bytes() const { return bytes_; }
+
+ private:
+  pf_status alloc_all();
+  void run_substep(uint32_t s, uint32_t parity);
+  void run_sort_and_permute(uint32_t parity, bool committed);
+  void run_init_pass();
+  void launch_frame_start_at(uint32_t parity);
+  pf_status upload_params(double dt);
+  WorldView view(uint32_t parity) const;
+
+  std::vector<SceneSpec*> specs_;
+  std::vector<DevScene> h_scenes_;
+  std::vector<DevFluid> h_fluids_;
+  std::vector<DevBoundary> h_bnds_;
+  std::vector<DevSoft> h_softs_;
+  std::vector<DevBody> h_bodies_;
+  std::vector<pf_primitive> h_prims_;
+  // stage plan
+  uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
+  bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false;
+  bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
+  bool any_react_ = false;
+  uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
+  // device memory: one arena
+  void* arena_ = nullptr;
+  size_t bytes_ = 0;
+  WorldView base_{};
+  StateBuf buf_[2];
+  SortScratch sort_{};
+  uint32_t parity_ = 0;
+  bool inited_ = false;
+  // graph
+  bool use_graph_ = false;
+  cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  double graph_dt_ = -1;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  float last_ms_ = 0;
+  // pinned staging for per-step parameters
+  DevScene* h_pinned_scenes_ = nullptr;
+  pf_primitive* h_pinned_prims_ = nullptr;
+  bool prims_dirty_ = true;
+  size_t pair_entries_ = 0;
+};
+
+}  // namespace pf

@@ -1,0 +1,311 @@
+// world_kernels.cuh — device helpers shared by the solver stage kernels:
+// SPH kernels, primitive SDFs, fixed-point accumulation, 3x3 polar
+// decomposition and the 27-cell stencil walk over the sorted slots.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "world.cuh"
+
+namespace pf {
+
+__device__ __forceinline__ uint32_t lane_of() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ const DevScene& scene_at(const WorldView& V, uint32_t slot) {
+  return V.scenes[V.chunk_scene[slot >> 8]];
+}
+__device__ __forceinline__ uint32_t scene_index(const WorldView& V, uint32_t slot) {
+  return V.chunk_scene[slot >> 8];
+}
+
+// ----------------------------------------------------------- vector math ----
+struct f3 {
+  float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 xyz(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ f3 neg(f3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ float4 with_w(f3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+// |a|^2 without fused multiply-add: the neighbour-list acceptance test must
+// round exactly like the reference's separately rounded products and sums.
+__device__ __forceinline__ float dot_rn(f3 a) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z));
+}
+
+// ------------------------------------------------------------ SPH kernels ----
+// sph/kernels.ts:254-298
+__device__ __forceinline__ float poly6(float rsq, const DevFluid& F) {
+  const float d = fmaxf(F.hsq - rsq, 0.0f);
+  return d * d * d * F.poly6;
+}
+__device__ __forceinline__ f3 spiky_grad(f3 r, const DevFluid& F) {
+  const float rl = sqrtf(dot(r, r));
+  const float t = fmaxf(F.h - rl, 0.0f);
+  const float rs = fmaxf(rl, 1e-20f);
+  const f3 rhat = r / rs;
+  const float mag = -(t * t * F.spiky);
+  return rhat * mag;
+}
+// shared.ts:52-62: the neighbour's SPH mass (boundary psi = rho0 * V).
+__device__ __forceinline__ float neighbor_mass(float bv, float w, float rho0) {
+  return bv > 0.0f ? rho0 * bv : (w > 0.0f ? 1.0f / w : 0.0f);
+}
+
+// ------------------------------------------------- fixed-point accumulation ----
+// accumulator.ts:108-115: round(v * scale) with ties to even, saturating.
+__device__ __forceinline__ int to_ticks(float v, float scale) { return __float2int_rn(v * scale); }
+__device__ __forceinline__ void acc_add(int4* acc, uint32_t slot, f3 v, float scale) {
+  int* p = reinterpret_cast<int*>(acc + slot);
+  atomicAdd(p + 0, to_ticks(v.x, scale));
+  atomicAdd(p + 1, to_ticks(v.y, scale));
+  atomicAdd(p + 2, to_ticks(v.z, scale));
+}
+// accumulator.ts:148-178: ticks -> float change, saturation test, clear.
+__device__ __forceinline__ f3 ticks_change(int tx, int ty, int tz, float inv, bool* sat) {
+  const float fx = (float)tx, fy = (float)ty, fz = (float)tz;
+  const float m = fmaxf(fmaxf(fabsf(fx), fabsf(fy)), fabsf(fz));
+  if (m >= 1073741824.0f) *sat = true;
+  return mk(fx * inv, fy * inv, fz * inv);
+}
+
+// --------------------------------------------------------- grid stencil ----
+__device__ __forceinline__ int32_t cell_of(float p, float o, float cell) {
+  return __float2int_rz(floorf(__fdiv_rn(__fsub_rn(p, o), cell)));
+}
+
+__device__ __forceinline__ int32_t clampi(int64_t v, int32_t lo, int32_t hi) {
+  return (int32_t)(v < lo ? lo : (v > hi ? hi : v));
+}
+
+// Local (grid) cell of a position, clamped into the grid.
+__device__ __forceinline__ void local_cell(const DevScene& S, f3 p, int32_t* cx, int32_t* cy, int32_t* cz,
+                                           bool* clamped) {
+  const int64_t ax = (int64_t)cell_of(p.x, S.ox, S.cell) - S.lo[0];
+  const int64_t ay = (int64_t)cell_of(p.y, S.oy, S.cell) - S.lo[1];
+  const int64_t az = (int64_t)cell_of(p.z, S.oz, S.cell) - S.lo[2];
+  *cx = clampi(ax, 0, (int32_t)S.dims[0] - 1);
+  *cy = clampi(ay, 0, (int32_t)S.dims[1] - 1);
+  *cz = clampi(az, 0, (int32_t)S.dims[2] - 1);
+  if (clamped) *clamped = (*cx != ax) || (*cy != ay) || (*cz != az);
+}
+
+// Visit the sorted slots of the 27 cells around p in the reference's order
+// (query.ts:37-66: dz, dy, dx; within a cell ascending particle index). With
+// linear keys the three cells of one (dy, dz) row are consecutive keys, so a
+// row is one contiguous slot range. fn(slot) returns false to stop early.
+template <typename F>
+__device__ __forceinline__ void walk27(const DevScene& S, const uint32_t* __restrict__ cstart,
+                                       const uint32_t* __restrict__ ccount, f3 p, F&& fn) {
+  int32_t cx, cy, cz;
+  local_cell(S, p, &cx, &cy, &cz, nullptr);
+  const int32_t x0 = max(cx - 1, 0), x1 = min(cx + 1, (int32_t)S.dims[0] - 1);
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int32_t z = cz + dz;
+    if (z < 0 || z >= (int32_t)S.dims[2]) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int32_t y = cy + dy;
+      if (y < 0 || y >= (int32_t)S.dims[1]) continue;
+      const uint32_t row = S.cell_base + S.dims[0] * ((uint32_t)y + S.dims[1] * (uint32_t)z);
+      const uint32_t k0 = row + (uint32_t)x0, k1 = row + (uint32_t)x1;
+      const uint32_t s0 = __ldg(cstart + k0);
+      const uint32_t s1 = __ldg(cstart + k1) + __ldg(ccount + k1);
+      for (uint32_t j = s0; j < s1; ++j)
+        if (!fn(j)) return;
+    }
+  }
+}
+
+// ------------------------------------------------------------ quaternions ----
+__device__ __forceinline__ f3 qrot(float4 q, f3 v) {
+  const f3 qv = mk(q.x, q.y, q.z);
+  const f3 t = cross(qv, v) * 2.0f;
+  return v + t * q.w + cross(qv, t);
+}
+
+// ------------------------------------------------------ primitive SDFs ----
+// primitives.ts:158-171
+__device__ __forceinline__ f3 prim_pivot(const pf_primitive& p) {
+  const f3 d0 = mk(p.data0[0], p.data0[1], p.data0[2]);
+  const f3 d1 = mk(p.data1[0], p.data1[1], p.data1[2]);
+  if (p.kind == PF_PRIM_PLANE) return d1;
+  if (p.kind == PF_PRIM_CAPSULE) return (d0 + d1) * 0.5f;
+  return d0;
+}
+
+// primitives.ts:203-335 with the PrimitiveSet fields (velocity and spin).
+__device__ __forceinline__ void prim_sdf(const pf_primitive& p, f3 xw, float rewind, float* phi_out, f3* grad_out) {
+  const float t = (p.flags & PF_PRIM_SWEEP) ? rewind : 0.0f;
+  const f3 shifted = xw + mk(p.velocity[0], p.velocity[1], p.velocity[2]) * t;
+  const f3 pivot = prim_pivot(p);
+  const f3 spin = mk(p.spin[0], p.spin[1], p.spin[2]);
+  const float rate = len(spin);
+  const float half = rate * t * 0.5f;
+  const f3 axis = spin / fmaxf(rate, 1e-8f);
+  float sh, ch;
+  sincosf(half, &sh, &ch);
+  const float4 turn = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, ch);
+  const f3 x = pivot + qrot(turn, shifted - pivot);
+  const float4 unturn = make_float4(-turn.x, -turn.y, -turn.z, turn.w);
+  const f3 d0 = mk(p.data0[0], p.data0[1], p.data0[2]);
+  const f3 d1 = mk(p.data1[0], p.data1[1], p.data1[2]);
+  float phi = 0.0f;
+  f3 g = mk(0.0f, 0.0f, 0.0f);
+  if (p.kind == PF_PRIM_PLANE) {
+    phi = dot(d0, x - d1);
+    g = d0;
+  } else if (p.kind == PF_PRIM_SPHERE) {
+    const f3 diff = x - d0;
+    const float l = len(diff);
+    phi = l - p.data0[3];
+    g = diff / fmaxf(l, 1e-8f);
+  } else if (p.kind == PF_PRIM_BOX) {
+    const float4 rot = make_float4(p.rotation[0], p.rotation[1], p.rotation[2], p.rotation[3]);
+    const float4 conj = make_float4(-rot.x, -rot.y, -rot.z, rot.w);
+    const f3 xl = qrot(conj, x - d0);
+    const f3 q = mk(fabsf(xl.x), fabsf(xl.y), fabsf(xl.z)) - d1;
+    const f3 qp = mk(fmaxf(q.x, 0.0f), fmaxf(q.y, 0.0f), fmaxf(q.z, 0.0f));
+    const float outside = len(qp);
+    const float inside = fminf(fmaxf(fmaxf(q.x, q.y), q.z), 0.0f);
+    phi = outside + inside;
+    const f3 sg = mk(xl.x >= 0.0f ? 1.0f : -1.0f, xl.y >= 0.0f ? 1.0f : -1.0f, xl.z >= 0.0f ? 1.0f : -1.0f);
+    const bool is_out = outside > 1e-8f;
+    const bool dx = q.x >= q.y && q.x >= q.z;
+    const bool dy = q.y >= q.x && q.y >= q.z;
+    const f3 in_dir = mk(dx ? sg.x : 0.0f, (!dx && dy) ? sg.y : 0.0f, (!dx && !dy) ? sg.z : 0.0f);
+    const f3 lg = is_out ? mk(qp.x * sg.x, qp.y * sg.y, qp.z * sg.z) / fmaxf(outside, 1e-8f) : in_dir;
+    g = qrot(rot, lg);
+  } else if (p.kind == PF_PRIM_CAPSULE) {
+    const f3 ab = d1 - d0;
+    const f3 ax = x - d0;
+    const float ab2 = fmaxf(dot(ab, ab), 1e-8f);
+    const float tt = fminf(fmaxf(dot(ax, ab) / ab2, 0.0f), 1.0f);
+    const f3 closest = d0 + ab * tt;
+    const f3 diff = x - closest;
+    const float l = len(diff);
+    phi = l - p.data0[3];
+    g = diff / fmaxf(l, 1e-8f);
+  }
+  if (p.flags & PF_PRIM_INVERT) {
+    phi = -phi;
+    g = neg(g);
+  }
+  *phi_out = phi;
+  *grad_out = qrot(unturn, g);
+}
+
+// primitives.ts:342-360
+__device__ __forceinline__ f3 prim_surface_velocity(const pf_primitive& p, f3 xw, float rewind) {
+  const f3 vel = mk(p.velocity[0], p.velocity[1], p.velocity[2]);
+  const float t = (p.flags & PF_PRIM_SWEEP) ? rewind : 0.0f;
+  const f3 arm = (xw - prim_pivot(p)) + vel * t;
+  return vel + cross(mk(p.spin[0], p.spin[1], p.spin[2]), arm);
+}
+
+// -------------------------------------------------- polar decomposition ----
+// polarDecomp.ts:34-264: Jacobi on A^T A (8 sweeps over the (0,1), (0,2),
+// (1,2) planes), S^-1 = Q diag(1/sqrt(lambda)) Q^T, R = A S^-1. All in
+// registers.
+__device__ __forceinline__ void jacobi_coeffs(float app, float aqq, float apq, float* t, float* c, float* s) {
+  const float tau = (aqq - app) / (apq * 2.0f);
+  const float sg = tau >= 0.0f ? 1.0f : -1.0f;
+  const float ta = fabsf(tau);
+  *t = sg / (ta + sqrtf(ta * ta + 1.0f));
+  *c = 1.0f / sqrtf(*t * *t + 1.0f);
+  *s = *t * *c;
+}
+
+__device__ __forceinline__ void polar3(const float a[9], float r[9]) {
+  float m00 = a[0] * a[0] + a[3] * a[3] + a[6] * a[6];
+  float m01 = a[0] * a[1] + a[3] * a[4] + a[6] * a[7];
+  float m02 = a[0] * a[2] + a[3] * a[5] + a[6] * a[8];
+  float m11 = a[1] * a[1] + a[4] * a[4] + a[7] * a[7];
+  float m12 = a[1] * a[2] + a[4] * a[5] + a[7] * a[8];
+  float m22 = a[2] * a[2] + a[5] * a[5] + a[8] * a[8];
+  float q00 = 1, q01 = 0, q02 = 0, q10 = 0, q11 = 1, q12 = 0, q20 = 0, q21 = 0, q22 = 1;
+  const float eps = 1e-12f;
+#pragma unroll 1
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    if (fabsf(m01) > eps) {
+      float t, c, s;
+      const float apq = m01, app = m00, aqq = m11;
+      jacobi_coeffs(app, aqq, apq, &t, &c, &s);
+      const float o02 = m02, o12 = m12, a0 = q00, a1 = q01, b0 = q10, b1 = q11, c0 = q20, c1 = q21;
+      m00 = app - t * apq;
+      m11 = aqq + t * apq;
+      m01 = 0.0f;
+      m02 = c * o02 - s * o12;
+      m12 = s * o02 + c * o12;
+      q00 = c * a0 - s * a1;
+      q01 = s * a0 + c * a1;
+      q10 = c * b0 - s * b1;
+      q11 = s * b0 + c * b1;
+      q20 = c * c0 - s * c1;
+      q21 = s * c0 + c * c1;
+    }
+    if (fabsf(m02) > eps) {
+      float t, c, s;
+      const float apq = m02, app = m00, aqq = m22;
+      jacobi_coeffs(app, aqq, apq, &t, &c, &s);
+      const float o01 = m01, o12 = m12, a0 = q00, a2 = q02, b0 = q10, b2 = q12, c0 = q20, c2 = q22;
+      m00 = app - t * apq;
+      m22 = aqq + t * apq;
+      m02 = 0.0f;
+      m01 = c * o01 - s * o12;
+      m12 = s * o01 + c * o12;
+      q00 = c * a0 - s * a2;
+      q02 = s * a0 + c * a2;
+      q10 = c * b0 - s * b2;
+      q12 = s * b0 + c * b2;
+      q20 = c * c0 - s * c2;
+      q22 = s * c0 + c * c2;
+    }
+    if (fabsf(m12) > eps) {
+      float t, c, s;
+      const float apq = m12, app = m11, aqq = m22;
+      jacobi_coeffs(app, aqq, apq, &t, &c, &s);
+      const float o01 = m01, o02 = m02, a1 = q01, a2 = q02, b1 = q11, b2 = q12, c1 = q21, c2 = q22;
+      m11 = app - t * apq;
+      m22 = aqq + t * apq;
+      m12 = 0.0f;
+      m01 = c * o01 - s * o02;
+      m02 = s * o01 + c * o02;
+      q01 = c * a1 - s * a2;
+      q02 = s * a1 + c * a2;
+      q11 = c * b1 - s * b2;
+      q12 = s * b1 + c * b2;
+      q21 = c * c1 - s * c2;
+      q22 = s * c1 + c * c2;
+    }
+  }
+  const float i0 = 1.0f / sqrtf(fmaxf(m00, 1e-20f));
+  const float i1 = 1.0f / sqrtf(fmaxf(m11, 1e-20f));
+  const float i2 = 1.0f / sqrtf(fmaxf(m22, 1e-20f));
+  const float s00 = q00 * q00 * i0 + q01 * q01 * i1 + q02 * q02 * i2;
+  const float s01 = q00 * q10 * i0 + q01 * q11 * i1 + q02 * q12 * i2;
+  const float s02 = q00 * q20 * i0 + q01 * q21 * i1 + q02 * q22 * i2;
+  const float s11 = q10 * q10 * i0 + q11 * q11 * i1 + q12 * q12 * i2;
+  const float s12 = q10 * q20 * i0 + q11 * q21 * i1 + q12 * q22 * i2;
+  const float s22 = q20 * q20 * i0 + q21 * q21 * i1 + q22 * q22 * i2;
+  r[0] = a[0] * s00 + a[1] * s01 + a[2] * s02;
+  r[1] = a[0] * s01 + a[1] * s11 + a[2] * s12;
+  r[2] = a[0] * s02 + a[1] * s12 + a[2] * s22;
+  r[3] = a[3] * s00 + a[4] * s01 + a[5] * s02;
+  r[4] = a[3] * s01 + a[4] * s11 + a[5] * s12;
+  r[5] = a[3] * s02 + a[4] * s12 + a[5] * s22;
+  r[6] = a[6] * s00 + a[7] * s01 + a[8] * s02;
+  r[7] = a[6] * s01 + a[7] * s11 + a[8] * s12;
+  r[8] = a[6] * s02 + a[7] * s12 + a[8] * s22;
+}
+
+}  // namespace pf

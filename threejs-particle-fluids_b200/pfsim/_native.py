@@ -188,6 +188,28 @@ SIGNATURES = {
     "pf_sort_device_errors": (C.c_int, [_P, _u32p]),
     "pf_sort_noalloc": (C.c_int, [_P, C.c_uint32, C.POINTER(GridDesc), _P, _P, _P, _P, _P, _P]),
     "pf_sort_host": (C.c_int, [_f32p, C.c_uint32, C.POINTER(GridDesc), _u32p, _u32p, _u32p, _u32p, _u32p]),
+    "pf_scene_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(_P)]),
+    "pf_scene_destroy": (None, [_P]),
+    "pf_upload_particles": (C.c_int, [_P, _f32p, _f32p, _f32p, _u32p, C.c_uint32, C.c_uint32]),
+    "pf_set_inv_mass": (C.c_int, [_P, Range, C.c_float]),
+    "pf_add_fluid": (C.c_int, [_P, C.POINTER(FluidDesc), _u32p]),
+    "pf_add_softbodies": (C.c_int, [_P, C.POINTER(SoftbodyDesc), _u32p]),
+    "pf_add_cloth": (C.c_int, [_P, C.POINTER(ClothDesc), _u32p]),
+    "pf_add_primitive": (C.c_int, [_P, C.POINTER(Primitive), _u32p]),
+    "pf_set_primitive": (C.c_int, [_P, C.c_uint32, C.POINTER(Primitive)]),
+    "pf_loop_build": (C.c_int, [_P, C.POINTER(LoopDesc)]),
+    "pf_step": (C.c_int, [_P, C.c_double]),
+    "pf_readback": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t]),
+    "pf_overflow_read": (C.c_int, [_P, C.POINTER(Overflow)]),
+    "pf_last_step_ms": (C.c_int, [_P, _f32p]),
+    "pf_batch_create": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(BatchOpts), C.POINTER(_P)]),
+    "pf_batch_destroy": (None, [_P]),
+    "pf_batch_step": (C.c_int, [_P, C.c_double]),
+    "pf_batch_set_primitive": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(Primitive)]),
+    "pf_batch_readback": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_size_t]),
+    "pf_batch_overflow_read": (C.c_int, [_P, C.c_uint32, C.POINTER(Overflow)]),
+    "pf_batch_last_step_ms": (C.c_int, [_P, _f32p]),
+    "pf_batch_particle_substeps": (C.c_uint64, [_P]),
 }
 
 _lib: C.CDLL | None = None

@@ -1,0 +1,411 @@
+"""Backend-neutral scene descriptions and the native (CUDA) backend.
+
+A ``Recipe`` is a plain description of one scene in the reference's terms: a
+ParticleSystem (capacity, radius, uploaded particles), materials in SimLoop
+order (FluidSystem, SoftbodySystem, ClothSystem), PrimitiveSet primitives and
+the SimLoop options. ``NativeBackend.build(recipe)`` replays it through the C
+ABI in the order the reference's constructors would run, and returns a
+``Scene`` handle. Any other object with the same methods (the CPU oracle in
+the test suite) can replay the same recipe.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+
+from . import _native as N
+
+# ---------------------------------------------------------------- recipe ----
+
+
+@dataclass
+class Upload:
+    start: int
+    pos: np.ndarray  # (n, 3) or (n, 4) float32
+    vel: np.ndarray | None = None
+    inv_mass: np.ndarray | None = None
+
+
+@dataclass
+class FluidOpts:
+    """FluidSystemOptions (src/fluids/FluidSystem.ts:31-54)."""
+
+    range: tuple[int, int] = (0, 0)  # (start, count); count 0 = every particle
+    rest_density: float = 0.0
+    particle_spacing: float = 0.0
+    smoothing_radius: float = 0.0
+    compliance: float = -1.0
+    viscosity: float | None = None
+    boundaries: list[tuple[int, int]] = field(default_factory=list)
+    boundary_static: list[bool] = field(default_factory=list)
+
+
+@dataclass
+class BodyDef:
+    """SoftbodyDef (src/softbody/SoftbodySystem.ts:29-60)."""
+
+    range: tuple[int, int]
+    surface_count: int | None = None
+    compliance: float = 0.0
+    rest_positions: np.ndarray | None = None
+    edges: np.ndarray | None = None  # (m, 2) body-local pairs
+
+
+@dataclass
+class SoftbodyOpts:
+    bodies: list[BodyDef]
+    shape_matching: str = "global"
+
+
+@dataclass
+class ClothOpts:
+    """ClothSystemOptions with a ClothGraph (src/cloth/ClothSystem.ts:37-70)."""
+
+    offset: int
+    positions: np.ndarray  # (n, 3)
+    inv_mass: np.ndarray  # (n,)
+    pairs: np.ndarray  # (m, 2) cloth-local
+    rest_lengths: np.ndarray  # (m,)
+    stretch_compliance: float = -1.0
+
+
+@dataclass
+class Prim:
+    kind: int
+    flags: int = 0
+    data0: tuple = (0.0, 0.0, 0.0, 0.0)
+    data1: tuple = (0.0, 0.0, 0.0, 0.0)
+    velocity: tuple = (0.0, 0.0, 0.0, 0.0)
+    rotation: tuple = (0.0, 0.0, 0.0, 1.0)
+    spin: tuple = (0.0, 0.0, 0.0, 0.0)
+
+    def cstruct(self) -> N.Primitive:
+        p = N.Primitive()
+        p.kind, p.flags = int(self.kind), int(self.flags)
+        p.data0[:] = [float(v) for v in self.data0]
+        p.data1[:] = [float(v) for v in self.data1]
+        p.velocity[:] = [float(v) for v in self.velocity]
+        p.rotation[:] = [float(v) for v in self.rotation]
+        p.spin[:] = [float(v) for v in self.spin]
+        return p
+
+
+def plane(normal, point, mu_s: float = 0.5, mu_k: float = 0.4) -> Prim:
+    """PrimitiveSet.addPlane (PrimitiveSet.ts:166-170): the normal is normalised."""
+    n = np.asarray(normal, np.float64)
+    n = n / np.linalg.norm(n)
+    return Prim(N.PF_PRIM_PLANE, 0, (*n, 0.0), (*point, mu_s), (0.0, 0.0, 0.0, mu_k))
+
+
+def sphere(center, radius, invert=False, mu_s=0.5, mu_k=0.4, velocity=(0.0, 0.0, 0.0)) -> Prim:
+    return Prim(N.PF_PRIM_SPHERE, N.PF_PRIM_INVERT if invert else 0, (*center, radius), (0.0, 0.0, 0.0, mu_s),
+                (*velocity, mu_k))
+
+
+def box(center, half, rotation=(0.0, 0.0, 0.0, 1.0), invert=False, mu_s=0.5, mu_k=0.4) -> Prim:
+    return Prim(N.PF_PRIM_BOX, N.PF_PRIM_INVERT if invert else 0, (*center, 0.0), (*half, mu_s), (0.0, 0.0, 0.0, mu_k),
+                tuple(rotation))
+
+
+def capsule(a, b, radius, mu_s=0.5, mu_k=0.4) -> Prim:
+    return Prim(N.PF_PRIM_CAPSULE, 0, (*a, radius), (*b, mu_s), (0.0, 0.0, 0.0, mu_k))
+
+
+def container_walls(lo, hi, closed: bool = False) -> list[Prim]:
+    """The Simulation façade's container planes (Simulation.ts:779-787)."""
+    walls = [
+        plane((0, 1, 0), lo),
+        plane((1, 0, 0), lo),
+        plane((-1, 0, 0), hi),
+        plane((0, 0, 1), lo),
+        plane((0, 0, -1), hi),
+    ]
+    if closed:
+        walls.append(plane((0, -1, 0), hi))
+    return walls
+
+
+@dataclass
+class LoopOpts:
+    """SimLoopOptions (src/core/loop.ts:33-57) plus the grid bounds."""
+
+    substeps: int = 4
+    iterations: int = 2
+    gravity: tuple = (0.0, -9.81, 0.0)
+    hash_origin: tuple = (0.0, 0.0, 0.0)
+    grid_min: tuple = (0.0, 0.0, 0.0)
+    grid_max: tuple = (0.0, 0.0, 0.0)
+
+
+@dataclass
+class Recipe:
+    capacity: int
+    radius: float
+    uploads: list[Upload] = field(default_factory=list)
+    materials: list[tuple[str, Any]] = field(default_factory=list)
+    prims: list[Prim] = field(default_factory=list)
+    loop: LoopOpts = field(default_factory=LoopOpts)
+    name: str = ""
+    # optional per-step primitive motion: fn(step_index, dt) -> {slot: Prim}
+    motion: Any = None
+
+    @property
+    def particle_substeps(self) -> int:
+        return self.capacity * self.loop.substeps
+
+
+# --------------------------------------------------- C struct conversion ----
+class _Keep:
+    """Keeps numpy buffers alive while a C call reads them."""
+
+    def __init__(self):
+        self.refs = []
+
+    def f32(self, a, shape_last=None):
+        arr = np.ascontiguousarray(a, dtype=np.float32)
+        self.refs.append(arr)
+        return arr.ctypes.data_as(C.POINTER(C.c_float))
+
+    def u32(self, a):
+        arr = np.ascontiguousarray(a, dtype=np.uint32)
+        self.refs.append(arr)
+        return arr.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def pos4(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a, np.float32)
+    if a.shape[1] == 4:
+        return np.ascontiguousarray(a)
+    out = np.zeros((a.shape[0], 4), np.float32)
+    out[:, :3] = a
+    return out
+
+
+def fluid_desc(o: FluidOpts, keep: _Keep) -> N.FluidDesc:
+    d = N.FluidDesc()
+    d.range.start, d.range.count = o.range
+    d.rest_density = o.rest_density
+    d.particle_spacing = o.particle_spacing
+    d.smoothing_radius = o.smoothing_radius
+    d.compliance = o.compliance
+    if o.viscosity is not None:
+        d.viscosity = o.viscosity
+        d.flags |= N.PF_FLUID_VISCOSITY
+    if o.boundaries:
+        arr = (N.Range * len(o.boundaries))(*[N.Range(s, c) for s, c in o.boundaries])
+        keep.refs.append(arr)
+        d.n_boundaries = len(o.boundaries)
+        d.boundaries = C.cast(arr, C.POINTER(N.Range))
+        st = np.array([1 if (i < len(o.boundary_static) and o.boundary_static[i]) else 0 for i in range(len(o.boundaries))], np.uint8)
+        keep.refs.append(st)
+        d.boundary_static = st.ctypes.data_as(C.POINTER(C.c_uint8))
+    return d
+
+
+def softbody_desc(o: SoftbodyOpts, keep: _Keep) -> N.SoftbodyDesc:
+    defs = (N.SoftbodyDef * len(o.bodies))()
+    for i, b in enumerate(o.bodies):
+        defs[i].range.start, defs[i].range.count = b.range
+        defs[i].surface_count = 0xFFFFFFFF if b.surface_count is None else int(b.surface_count)
+        defs[i].compliance = b.compliance
+        if b.rest_positions is not None:
+            defs[i].rest_positions = keep.f32(np.asarray(b.rest_positions, np.float32).reshape(-1))
+        if b.edges is not None and len(b.edges):
+            e = np.asarray(b.edges, np.uint32).reshape(-1)
+            defs[i].edges = keep.u32(e)
+            defs[i].n_edges = e.size // 2
+    keep.refs.append(defs)
+    d = N.SoftbodyDesc()
+    d.n_bodies = len(o.bodies)
+    d.bodies = C.cast(defs, C.POINTER(N.SoftbodyDef))
+    d.shape_matching = N.PF_SHAPE_MATCH_LOCAL if o.shape_matching == "local" else N.PF_SHAPE_MATCH_GLOBAL
+    return d
+
+
+def cloth_desc(o: ClothOpts, keep: _Keep) -> N.ClothDesc:
+    d = N.ClothDesc()
+    d.offset = o.offset
+    d.n_particles = len(o.positions)
+    d.positions = keep.f32(np.asarray(o.positions, np.float32).reshape(-1))
+    d.inv_mass = keep.f32(o.inv_mass)
+    pr = np.asarray(o.pairs, np.uint32).reshape(-1)
+    d.n_pairs = pr.size // 2
+    d.pairs = keep.u32(pr)
+    d.rest_lengths = keep.f32(o.rest_lengths)
+    d.stretch_compliance = o.stretch_compliance
+    return d
+
+
+def loop_desc(o: LoopOpts) -> N.LoopDesc:
+    d = N.LoopDesc()
+    d.substeps, d.iterations = o.substeps, o.iterations
+    d.gravity[:] = list(o.gravity)
+    d.hash_origin[:] = list(o.hash_origin)
+    d.grid_min[:] = list(o.grid_min)
+    d.grid_max[:] = list(o.grid_max)
+    return d
+
+
+# --------------------------------------------------------- native backend ----
+FIELD_SHAPES = {
+    N.PF_FIELD_POSITIONS: (np.float32, 4),
+    N.PF_FIELD_PREDICTED: (np.float32, 4),
+    N.PF_FIELD_VELOCITIES: (np.float32, 4),
+    N.PF_FIELD_INV_MASS: (np.float32, 1),
+    N.PF_FIELD_BOUNDARY_VOLUME: (np.float32, 1),
+    N.PF_FIELD_DENSITY: (np.float32, 1),
+    N.PF_FIELD_ROTATION: (np.float32, 4),
+    N.PF_FIELD_PREDICTED_ROTATION: (np.float32, 4),
+    N.PF_FIELD_ANGULAR_VELOCITY: (np.float32, 4),
+    N.PF_FIELD_LAMBDA: (np.float32, 1),
+    N.PF_FIELD_NEIGHBOR_COUNT: (np.uint32, 1),
+    N.PF_FIELD_NEIGHBORS: (np.uint32, N.MAX_NEIGHBORS),
+    N.PF_FIELD_CELL_PERM: (np.uint32, 1),
+}
+
+
+def alloc_field(field_id: int, capacity: int) -> np.ndarray:
+    dt, width = FIELD_SHAPES[field_id]
+    return np.empty((capacity, width) if width > 1 else (capacity,), dt)
+
+
+class Scene:
+    """A built scene on the native backend (pf_scene handle)."""
+
+    def __init__(self, handle, recipe: Recipe):
+        self.h = handle
+        self.recipe = recipe
+        self.capacity = recipe.capacity
+        self.steps = 0
+
+    def step(self, dt: float) -> None:
+        L = N.lib()
+        if self.recipe.motion is not None:
+            for slot, prim in self.recipe.motion(self.steps, dt).items():
+                p = prim.cstruct()
+                N.check(L.pf_set_primitive(self.h, slot, C.byref(p)))
+        N.check(L.pf_step(self.h, float(dt)))
+        self.steps += 1
+
+    def set_primitive(self, slot: int, prim: Prim) -> None:
+        p = prim.cstruct()
+        N.check(N.lib().pf_set_primitive(self.h, slot, C.byref(p)))
+
+    def readback(self, field_id: int) -> np.ndarray:
+        out = alloc_field(field_id, self.capacity)
+        N.check(N.lib().pf_readback(self.h, field_id, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def overflow(self) -> dict:
+        o = N.Overflow()
+        N.check(N.lib().pf_overflow_read(self.h, C.byref(o)))
+        return {k: bool(getattr(o, k)) for k, _ in N.Overflow._fields_}
+
+    def last_step_ms(self) -> float:
+        ms = C.c_float(0)
+        N.check(N.lib().pf_last_step_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def close(self) -> None:
+        if self.h:
+            N.lib().pf_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NativeBackend:
+    """Replays recipes through libpfsim (the CUDA path)."""
+
+    name = "cuda"
+
+    def build(self, r: Recipe) -> Scene:
+        L = N.lib()
+        desc = N.SceneDesc(r.capacity, r.radius)
+        h = C.c_void_p()
+        N.check(L.pf_scene_create(C.byref(desc), C.byref(h)))
+        scene = Scene(h, r)
+        keep = _Keep()
+        for u in r.uploads:
+            p = pos4(u.pos)
+            v = None if u.vel is None else keep.f32(pos4(u.vel))
+            w = None if u.inv_mass is None else keep.f32(u.inv_mass)
+            N.check(L.pf_upload_particles(h, keep.f32(p), v, w, None, u.start, p.shape[0]))
+        for kind, opts in r.materials:
+            if kind == "fluid":
+                N.check(L.pf_add_fluid(h, C.byref(fluid_desc(opts, keep)), None))
+            elif kind == "soft":
+                N.check(L.pf_add_softbodies(h, C.byref(softbody_desc(opts, keep)), None))
+            elif kind == "cloth":
+                N.check(L.pf_add_cloth(h, C.byref(cloth_desc(opts, keep)), None))
+            else:
+                raise ValueError(kind)
+        for p in r.prims:
+            cs = p.cstruct()
+            N.check(L.pf_add_primitive(h, C.byref(cs), None))
+        ld = loop_desc(r.loop)
+        N.check(L.pf_loop_build(h, C.byref(ld)))
+        return scene
+
+
+class Batch:
+    """Many built scenes stepped as one world (pf_batch): one launch per stage,
+    one CUDA graph per tick."""
+
+    def __init__(self, scenes: list[Scene], use_graph: bool = True):
+        L = N.lib()
+        arr = (C.c_void_p * len(scenes))(*[s.h for s in scenes])
+        opts = N.BatchOpts(1 if use_graph else 0, 0)
+        h = C.c_void_p()
+        N.check(L.pf_batch_create(arr, len(scenes), C.byref(opts), C.byref(h)))
+        self.h = h
+        self.recipes = [s.recipe for s in scenes]
+        self.capacities = [s.capacity for s in scenes]
+        self.steps = 0
+
+    def step(self, dt: float) -> None:
+        L = N.lib()
+        for i, r in enumerate(self.recipes):
+            if r.motion is not None:
+                for slot, prim in r.motion(self.steps, dt).items():
+                    p = prim.cstruct()
+                    N.check(L.pf_batch_set_primitive(self.h, i, slot, C.byref(p)))
+        N.check(L.pf_batch_step(self.h, float(dt)))
+        self.steps += 1
+
+    def readback(self, index: int, field_id: int) -> np.ndarray:
+        out = alloc_field(field_id, self.capacities[index])
+        N.check(N.lib().pf_batch_readback(self.h, index, field_id, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def overflow(self, index: int) -> dict:
+        o = N.Overflow()
+        N.check(N.lib().pf_batch_overflow_read(self.h, index, C.byref(o)))
+        return {k: bool(getattr(o, k)) for k, _ in N.Overflow._fields_}
+
+    def last_step_ms(self) -> float:
+        ms = C.c_float(0)
+        N.check(N.lib().pf_batch_last_step_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def particle_substeps(self) -> int:
+        return int(N.lib().pf_batch_particle_substeps(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            N.lib().pf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
