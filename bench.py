@@ -227,7 +227,248 @@ class SortWorkload:
                 "sample": f"{reps} full {self.n}-particle stable counting sorts", "cores": 1}
 
 
-WORKLOADS = {"sort": SortWorkload}
+class BatchWorkload:
+    """Batched solver over 256 uneven scenes: particle counts log-uniform on
+    [5k, 200k], 70% dam-break fluids (container scale U[0.5, 2]) and 30% cloth
+    sheets of 64^2-256^2 particles, 2 substeps x 4 iterations, dt = 1/60.
+    One step = one frame of every scene. The same scenes are also stepped the
+    plain way (each scene its own stream and launches, no graph) as the
+    baseline of the batched/plain ratio."""
+
+    name = "batch_256_scenes_5k-200k_fluid70_cloth30_S2_I4"
+    metric = "particle-substeps/s & p99 step latency: batched/served vs plain, 1\u00d7B200"
+    unit = "particle-substeps/s"
+    DT = 1.0 / 60.0
+    # algorithmic bytes per fluid particle of the density+lambda stage:
+    # read x* (16 B) and the boundary volume (4 B), write lambda and density (4 B each)
+    LAMBDA_BYTES = 28
+
+    def __init__(self, n_scenes: int = 256):
+        self.n_scenes = n_scenes
+
+    def recipes(self, seed: int):
+        from pfsim import workloads as W
+
+        return W.batch_stream(self.n_scenes, seed=seed)
+
+    def run_gpu(self, steps: int, warmup: int, rank: int, world: int, dist_barrier, plain_baseline=True) -> dict:
+        import ctypes as C
+
+        import torch
+
+        from pfsim import _native as N
+        from pfsim import recipe as R
+
+        L = N.lib()
+        backend = R.NativeBackend()
+        recipes = self.recipes(1000 + rank)
+        plain = [backend.build(r) for r in recipes]
+        psub = sum(r.particle_substeps for r in recipes)
+        # ---- plain baseline: per-scene streams and launches, no graph
+        for _ in range(warmup if plain_baseline else 0):
+            for sc in plain:
+                sc.step(self.DT)
+        torch.cuda.synchronize()
+        p_steps = max(2, steps // 2) if plain_baseline else 0
+        t0 = time.perf_counter()
+        for _ in range(p_steps):
+            for sc in plain:
+                sc.step(self.DT)
+        torch.cuda.synchronize()
+        plain_ms = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1) if plain_baseline else float("nan")
+        # ---- batched: one world, one launch per stage, one graph per tick
+        batch = R.Batch(plain, use_graph=True)
+        for sc in plain:
+            sc.close()
+        plain = None
+        stream = torch.cuda.ExternalStream(L.pf_batch_stream(batch.h))
+        for _ in range(warmup):
+            batch.step(self.DT)
+        torch.cuda.synchronize()
+        dist_barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        evs[0].record(stream)
+        for k in range(steps):
+            batch.step(self.DT)
+            evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+        dist_barrier()
+        clk = clocks.stop()
+        per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+        ms = evs[0].elapsed_time(evs[-1]) / steps
+        launches = int(L.pf_batch_launches_per_step(batch.h))
+        # ---- dominant stage, timed live on the batch stream
+        st_ms, items = C.c_float(0), C.c_uint64(0)
+        N.check(L.pf_batch_profile_stage(batch.h, 1, 20, C.byref(st_ms), C.byref(items)))
+        # ---- end to end: per step the scene parameters go host->device (pinned)
+        # and every scene's positions come back to pinned host memory
+        total = sum(r.capacity for r in recipes)
+        host = torch.empty(total * 4, dtype=torch.float32).pin_memory()
+        hp = C.cast(C.c_void_p(host.data_ptr()), C.POINTER(C.c_float))
+        e_steps = max(3, steps // 2)
+        for _ in range(2):
+            batch.step(self.DT)
+            N.check(L.pf_batch_read_positions(batch.h, hp, host.numel() * 4))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(e_steps):
+            batch.step(self.DT)
+            N.check(L.pf_batch_read_positions(batch.h, hp, host.numel() * 4))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e_steps
+        h2d = int(L.pf_batch_step_upload_bytes(batch.h))
+        ok = np.isfinite(host.numpy()).all()
+        batch.close()
+        if not ok:
+            raise RuntimeError("non-finite positions after the timed steps")
+        return {
+            "ms": ms,
+            "units_per_step": psub,
+            "kernel_ms": st_ms.value,
+            "kernel_name": "k_lambda (density + lambda, one solver iteration)",
+            "algorithmic_bytes": self.LAMBDA_BYTES * items.value,
+            "gpu_launches_per_step": launches,
+            "clocks": clk,
+            "e2e_ms": e2e_ms,
+            "h2d": h2d,
+            "d2h": 16 * total,
+            "extra": {
+                "p50_step_ms": float(np.percentile(per, 50)),
+                "p99_step_ms": float(np.percentile(per, 99)),
+                "plain_ms_per_step": plain_ms,
+                "plain_value": psub / (plain_ms * 1e-3),
+                "batched_over_plain": plain_ms / ms,
+                "scenes": len(recipes),
+                "particles": total,
+                "fluid_particles": int(items.value),
+            },
+        }
+
+    def run_cpu(self, threads: int, budget_particles: int = 150_000, steps: int = 3) -> dict:
+        """The oracle on a bounded sample of the same scene stream: the first
+        scenes of the stream up to `budget_particles`, stepped `steps` frames."""
+        from oracle import oracle as O
+
+        recipes = self.recipes(1000)
+        sample, n = [], 0
+        for r in recipes:
+            if n >= budget_particles:
+                break
+            sample.append(r)
+            n += r.capacity
+        be = O.OracleBackend(threads=threads)
+        scenes = [be.build(r) for r in sample]
+        for sc in scenes:
+            sc.step(self.DT)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for sc in scenes:
+                sc.step(self.DT)
+        s = (time.perf_counter() - t0) / steps
+        psub = sum(r.particle_substeps for r in sample)
+        return {"seconds_per_step": s, "units_per_step": psub, "cores": threads,
+                "sample": f"{len(sample)} scenes ({n} particles) of the same stream, {steps} frames each"}
+
+
+class ServeWorkload:
+    """Serving: a seeded Poisson stream of scene requests (N log-uniform on
+    [5k, 500k], fluid/soft/cloth 60/20/20, lifetime U[60, 600] ticks), admitted
+    under a 150 GB HBM budget and stepped every tick on device-resident
+    state. The run starts from a steady-state population (`live` scenes with
+    residual lifetimes) and keeps it by arrivals at live / mean lifetime per
+    tick. The same stream is served twice: batched (cohorts, graphs) and
+    plain (every scene its own world and stream)."""
+
+    name = "serve_poisson_5k-500k_fluid60_soft20_cloth20_budget150GB"
+    metric = BatchWorkload.metric
+    unit = "particle-substeps/s"
+    DT = 1.0 / 60.0
+    MEAN_LIFE = 330.0
+
+    def __init__(self, live: int = 96, seed: int = 7):
+        self.live = live
+        self.seed = seed
+
+    def stream(self, ticks: int):
+        """(tick, recipe, lifetime) in arrival order; tick 0 holds the
+        initial population with residual lifetimes."""
+        from pfsim import workloads as W
+
+        r = W.rng(self.seed)
+        out = []
+        idx = 0
+        for _ in range(self.live):
+            rec, life = W.serve_request(r, idx, self.seed)
+            rec.motion = None
+            out.append((0, rec, max(1, int(r.integers(1, life + 1)))))
+            idx += 1
+        rate = self.live / self.MEAN_LIFE
+        for t in range(1, ticks):
+            for _ in range(int(r.poisson(rate))):
+                rec, life = W.serve_request(r, idx, self.seed)
+                rec.motion = None
+                out.append((t, rec, life))
+                idx += 1
+        return out
+
+    def serve(self, stream, ticks: int, warmup: int, plain: bool):
+        import torch
+
+        from pfsim import recipe as R
+
+        srv = R.Server(budget_bytes=150 * 10**9, plain=plain, async_build=not plain, max_cohorts=4)
+        by_tick = {}
+        for t, rec, life in stream:
+            by_tick.setdefault(t, []).append((rec, life))
+        for rec, life in by_tick.get(0, []):
+            srv.submit(rec, life)
+        srv.drain()
+        tick_ms, ps0 = [], 0
+        clocks = ClockSampler(torch.cuda.current_device())
+        for t in range(warmup + ticks):
+            if t == warmup:
+                torch.cuda.synchronize()
+                ps0 = srv.stats()["particle_substeps"]
+                clocks.start()
+            for rec, life in by_tick.get(t + 1, []) if t > 0 else []:
+                srv.submit(rec, life)
+            t0 = time.perf_counter()
+            srv.tick(self.DT)
+            if t >= warmup:
+                tick_ms.append((time.perf_counter() - t0) * 1e3)
+        clk = clocks.stop()
+        st = srv.stats()
+        srv.close()
+        ps = st["particle_substeps"] - ps0
+        wall = sum(tick_ms)
+        return {"value": ps / (wall * 1e-3), "ms": wall / ticks, "p50": float(np.percentile(tick_ms, 50)),
+                "p99": float(np.percentile(tick_ms, 99)), "clocks": clk, "stats": st,
+                "ps_per_tick": ps / ticks}
+
+    def run_gpu(self, steps: int, warmup: int, rank: int, world: int, dist_barrier, plain_baseline=True) -> dict:
+        stream = self.stream(warmup + steps + 1)
+        b = self.serve(stream, steps, warmup, plain=False)
+        p = self.serve(stream, steps, warmup, plain=True) if plain_baseline else None
+        return {
+            "ms": b["ms"], "units_per_step": b["ps_per_tick"], "clocks": b["clocks"],
+            "extra": {
+                "p50_tick_ms": b["p50"], "p99_tick_ms": b["p99"],
+                "plain_value": p["value"] if p else None,
+                "plain_p50_tick_ms": p["p50"] if p else None,
+                "plain_p99_tick_ms": p["p99"] if p else None,
+                "served_over_plain": (b["value"] / p["value"]) if p else None,
+                "requests": len(stream), "cohort_builds": b["stats"]["rebuilds"],
+                "live_at_end": b["stats"]["live"], "queued_at_end": b["stats"]["queued"],
+            },
+        }
+
+
+WORKLOADS = {"sort": SortWorkload, "batch": BatchWorkload, "serve": ServeWorkload}
 
 
 # -------------------------------------------------------------- main ----
@@ -237,15 +478,23 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pfsim", choices=["pfsim", "reference"])
-    ap.add_argument("--workload", default="sort", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batch", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-scene baseline (profiling runs)")
+    ap.add_argument("--scenes", type=int, default=256, help="scenes of the batch workload (smaller for profiling)")
+    ap.add_argument("--live", type=int, default=96, help="steady-state live scenes of the serve workload")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    wl = WORKLOADS[args.workload]()
+    if args.workload == "batch":
+        wl = WORKLOADS["batch"](args.scenes)
+    elif args.workload == "serve":
+        wl = WORKLOADS["serve"](args.live)
+    else:
+        wl = WORKLOADS[args.workload]()
 
     if args.impl == "reference":
         if rank != 0:
@@ -256,7 +505,8 @@ def main() -> None:
         line = {
             "impl": "reference", "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": warmup, "ms_per_step": cpu["seconds_per_step"] * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.workload == "batch" else "u32", "data": "synthetic",
             "config": {"workload": wl.name},
             "cpu_baseline": {"value": value, "unit": wl.unit, "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]},
             "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -280,7 +530,21 @@ def main() -> None:
         def barrier():
             pass
 
-    res = wl.run_gpu(args.steps, warmup, rank, world, barrier)
+    if args.workload == "serve":
+        res = wl.run_gpu(args.steps, warmup, rank, world, barrier, plain_baseline=not args.no_plain)
+        line = {"metric": wl.metric, "value": res["units_per_step"] / (res["ms"] * 1e-3), "unit": wl.unit,
+                "n_gpus": world, "steps": args.steps, "warmup": warmup, "ms_per_step": res["ms"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded)", "config": {"workload": wl.name, "timing": "host wall clock per tick"},
+                "clocks": res["clocks"]}
+        line.update(res["extra"])
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    if args.workload == "batch":
+        res = wl.run_gpu(args.steps, warmup, rank, world, barrier, plain_baseline=not args.no_plain)
+    else:
+        res = wl.run_gpu(args.steps, warmup, rank, world, barrier)
     ms = res["ms"]
     if world > 1:
         import torch.distributed as dist
@@ -305,8 +569,10 @@ def main() -> None:
         "gpu_launches": res["gpu_launches_per_step"] * args.steps,
         "clocks": res["clocks"],
     }
+    line["dtype"] = "f32" if args.workload == "batch" else "u32"
+    line.update(res.get("extra", {}))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = wl.run_cpu(1)
+        cpu = wl.run_cpu(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": cpu["units_per_step"] / cpu["seconds_per_step"], "unit": wl.unit,
                                 "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]}
     if rank == 0:

@@ -230,6 +230,34 @@ typedef struct pf_primitive {
 PF_API pf_status pf_add_primitive(pf_scene* scene, const pf_primitive* prim, uint32_t* slot);
 PF_API pf_status pf_set_primitive(pf_scene* scene, uint32_t slot, const pf_primitive* prim);
 
+/* new SDFCollider(particles, sdf, {muS, muK, thickness, position, rotation,
+ * scale}) (src/core/collision/SDFCollider.ts:88-137): a signed-distance grid
+ * (one distance per voxel, x fastest; voxel (i, j, k) centred at
+ * origin + (i + 0.5, j + 0.5, k + 0.5) * voxel_size in the collider's local
+ * frame) stored as half floats (converted round-to-nearest-even), sampled
+ * trilinearly with clamp-to-edge, its gradient by central differences one
+ * voxel apart (sdf.ts:107-147). A particle touches it where
+ * phi < radius + thickness; contact and friction are those of the
+ * primitives (collider.ts:53-118) against a static surface. Colliders run
+ * in the order added: the primitives of the scene, then its SDF colliders. */
+typedef struct pf_sdf_desc {
+  uint32_t res[3];      /* >= 4 each */
+  const float* data;    /* res[0] * res[1] * res[2] distances */
+  float origin[3];      /* local-frame corner of voxel (0, 0, 0) */
+  float voxel_size[3];  /* > 0 */
+  float position[3];    /* world position of the local origin */
+  float rotation[4];    /* unit quaternion (x, y, z, w) */
+  float scale;          /* uniform, > 0 */
+  float thickness;      /* >= 0 */
+  float mu_s, mu_k;     /* >= 0 */
+} pf_sdf_desc;
+
+PF_API pf_status pf_add_sdf_collider(pf_scene* scene, const pf_sdf_desc* sdf, uint32_t* slot);
+/* SDFCollider.setPosition / setRotation / setScale (SDFCollider.ts:170-201):
+ * takes effect from the next step. */
+PF_API pf_status pf_set_sdf_transform(pf_scene* scene, uint32_t slot, const float position[3],
+                                      const float rotation[4], float scale);
+
 /* new SimLoop(particles, {substeps, iterations, gravity, hashOrigin})
  * (src/core/loop.ts:33-57, 117-243). Builds the substep pipeline for the
  * materials and colliders added so far and allocates the device state. */
@@ -311,6 +339,25 @@ PF_API pf_status pf_batch_overflow_read(pf_batch* batch, uint32_t index, pf_over
 PF_API pf_status pf_batch_last_step_ms(pf_batch* batch, float* ms);
 /* Particle-substeps one pf_batch_step advances (sum over scenes of N * substeps). */
 PF_API uint64_t pf_batch_particle_substeps(pf_batch* batch);
+/* Kernel launches of the batch's last step (counted when it was issued or
+ * captured), and the bytes of per-step parameters copied host-to-device. */
+PF_API uint64_t pf_batch_launches_per_step(pf_batch* batch);
+PF_API uint64_t pf_batch_step_upload_bytes(pf_batch* batch);
+/* The cudaStream_t the batch (or a built scene) runs on, for callers that
+ * order their own work after it or time it with events. */
+PF_API void* pf_batch_stream(pf_batch* batch);
+PF_API void* pf_scene_stream(pf_scene* scene);
+/* Positions of every scene of the batch, each scene's particles in particle
+ * order (w = 0), scenes concatenated in batch order: one device gather and
+ * one device-to-host copy (pinned host memory makes it fastest). Synchronous. */
+PF_API pf_status pf_batch_read_positions(pf_batch* batch, float* dst_host, size_t bytes);
+/* Average device milliseconds of one solver stage launched `reps` times on the
+ * batch's current state: 0 neighbour lists, 1 density + lambda, 2 position
+ * correction, 3 XSPH, 4 predict. `items` receives the particles the stage
+ * covers (fluid particles for 0-3). For measurement; it changes no state
+ * that the next pf_batch_step reads. */
+PF_API pf_status pf_batch_profile_stage(pf_batch* batch, uint32_t stage, uint32_t reps, float* ms,
+                                        uint64_t* items);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching under an HBM budget                           */
@@ -318,25 +365,65 @@ PF_API uint64_t pf_batch_particle_substeps(pf_batch* batch);
 
 typedef struct pf_server pf_server;
 
+/* Scheduling modes. BATCHED packs admitted scenes into cohorts (one world,
+ * one launch per solver stage, one CUDA graph per tick each); PLAIN gives
+ * every scene its own world stepped on its own stream without graphs, the
+ * per-scene loop of the reference's Simulation.step (Simulation.ts:542-634). */
+enum { PF_SERVER_BATCHED = 0, PF_SERVER_PLAIN = 1 };
+
 typedef struct pf_server_opts {
-  uint64_t hbm_budget_bytes;  /* state budget for live scenes */
-  uint32_t max_scenes;
-  uint32_t use_graph;
+  uint64_t hbm_budget_bytes;  /* device bytes live cohorts may hold (0: 150 GB) */
+  uint32_t max_scenes;        /* live + building scenes at most (0: 65536) */
+  uint32_t use_graph;         /* BATCHED: capture each cohort's tick as a CUDA graph */
+  uint32_t max_cohorts;       /* BATCHED: cohorts before the smallest is folded into the next (0: 4) */
+  uint32_t mode;              /* PF_SERVER_BATCHED or PF_SERVER_PLAIN */
+  uint32_t async_build;       /* build admitted cohorts on a host worker thread while ticks go on */
 } pf_server_opts;
 
 typedef struct pf_server_stats {
-  uint32_t live;
-  uint32_t queued;
+  uint32_t live;              /* scenes stepped each tick */
+  uint32_t queued;            /* submitted, waiting for memory or a slot */
+  uint32_t building;          /* admitted, their cohort is being built */
+  uint32_t finished;
+  uint32_t cohorts;
+  uint32_t reserved0;
   uint64_t ticks;
-  uint64_t particle_substeps;
-  uint64_t state_bytes;
+  uint64_t particle_substeps; /* sum over ticks of the live scenes' particles x substeps */
+  uint64_t state_bytes;       /* device bytes held by cohorts and the build in flight */
+  uint64_t rebuilds;          /* cohorts built (admission waves and folds) */
+  double busy_ms;             /* sum of tick wall times */
   float last_tick_ms;
+  float p50_tick_ms;
+  float p99_tick_ms;
+  float max_tick_ms;
 } pf_server_stats;
 
-/* Queue a built scene for admission. The server copies its state; `ticket`
- * identifies the request. `lifetime_steps` steps later it retires. */
-/* Admit what fits, step every live scene once, retire finished scenes. */
-/* Copy a live or retired request's field (retired results are kept until read). */
+/* Request states reported by pf_server_request_state. */
+enum { PF_REQ_QUEUED = 0, PF_REQ_BUILDING = 1, PF_REQ_LIVE = 2, PF_REQ_DONE = 3 };
+
+PF_API pf_status pf_server_create(const pf_server_opts* opts, pf_server** out);
+PF_API void pf_server_destroy(pf_server* server);
+/* Queue a scene for admission: materials and primitives added, and either a
+ * built SimLoop (loop == NULL: its current state is taken) or an unbuilt one
+ * with `loop` giving the SimLoop options. The server copies the scene; the
+ * caller keeps ownership of `scene`. The request retires after
+ * `lifetime_steps` ticks of stepping. */
+PF_API pf_status pf_server_submit(pf_server* server, pf_scene* scene, const pf_loop_desc* loop,
+                                  uint32_t lifetime_steps, uint64_t* ticket);
+/* Swap in a finished cohort build, admit what fits the budget (FIFO), step
+ * every live scene once by dt, retire scenes whose lifetime is over. */
+PF_API pf_status pf_server_tick(pf_server* server, double dt);
+/* Wait for a cohort build in flight (if any) and swap it in. */
+PF_API pf_status pf_server_drain_build(pf_server* server);
+PF_API pf_status pf_server_request_state(pf_server* server, uint64_t ticket, uint32_t* state,
+                                         uint32_t* steps_done);
+/* A live request's field (any pf_field), or a finished request's final state
+ * (positions, velocities, inverse mass, boundary volume, rotation, angular
+ * velocity). */
+PF_API pf_status pf_server_readback(pf_server* server, uint64_t ticket, uint32_t field, void* dst, size_t bytes);
+/* Device bytes a scene would hold alone in a cohort (the admission estimate). */
+PF_API pf_status pf_server_estimate_bytes(pf_scene* scene, const pf_loop_desc* loop, uint64_t* bytes);
+PF_API pf_status pf_server_stats_read(pf_server* server, pf_server_stats* out);
 
 #ifdef __cplusplus
 }

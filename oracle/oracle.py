@@ -67,6 +67,10 @@ def _bind(L: C.CDLL) -> None:
         "or_add_softbodies": (C.c_int, [P, C.POINTER(N.SoftbodyDesc), u32p]),
         "or_add_cloth": (C.c_int, [P, C.POINTER(N.ClothDesc), u32p]),
         "or_add_primitive": (C.c_int, [P, C.POINTER(N.Primitive), u32p]),
+        "or_add_sdf_collider": (C.c_int, [P, C.POINTER(N.SdfDesc), u32p]),
+        "or_set_sdf_transform": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float]),
+        "or_sdf_sample": (C.c_int, [C.POINTER(N.SdfDesc), C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]),
         "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
         "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
         "or_step": (C.c_int, [P, C.c_double]),
@@ -143,6 +147,19 @@ def polar_f64(a: np.ndarray) -> np.ndarray:
     r = np.empty(9, np.float64)
     lib().or_polar_f64(_p(a, C.c_double), _p(r, C.c_double))
     return r.reshape(3, 3)
+
+
+def sdf_sample(sdf, points: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """phi and world gradient of an SDF collider (pfsim.recipe.Sdf) at points."""
+    from pfsim import recipe as R
+
+    keep = R._Keep()
+    d = sdf.cstruct(keep)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    phi = np.empty(len(pts), np.float32)
+    grad = np.empty((len(pts), 3), np.float32)
+    check(lib().or_sdf_sample(C.byref(d), _p(pts), len(pts), _p(phi), _p(grad)))
+    return phi, grad
 
 
 def color_constraints(pairs: np.ndarray) -> tuple[np.ndarray, int]:
@@ -241,6 +258,8 @@ class OracleBackend:
         for p in r.prims:
             cs = p.cstruct()
             check(L.or_add_primitive(h, C.byref(cs), None))
+        for g in r.sdfs:
+            check(L.or_add_sdf_collider(h, C.byref(g.cstruct(keep)), None))
         ld = R.loop_desc(r.loop)
         check(L.or_loop_build(h, C.byref(ld), self.table_size))
         return scene

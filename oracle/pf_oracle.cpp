@@ -343,6 +343,55 @@ struct Prim {
   float data0[4], data1[4], velocity[4], rotation[4], spin[4];
 };
 
+// SDFCollider (src/core/collision/SDFCollider.ts:88-137): the grid holds the
+// half-float values the collider's texture holds (widened back to float),
+// the transform uniforms are f32.
+struct SdfGrid {
+  uint32_t res[3];
+  std::vector<float> phi;
+  float origin[3], voxel[3], invVoxel[3], position[3];
+  float R[9], invR[9];  // row-major
+  float scale, invScale, thickness, muS, muK;
+};
+
+// IEEE half rounding (nearest even) of a value clamped to +-65504, returned
+// as the float the half represents.
+inline float half_round(float f) {
+  f = std::min(std::max(f, -65504.0f), 65504.0f);
+  if (std::isnan(f)) return f;
+  const float a = std::fabs(f);
+  if (a < 6.103515625e-05f) {  // 2^-14: subnormal halves are multiples of 2^-24
+    return std::copysign(std::nearbyint(a * 16777216.0f) / 16777216.0f, f);
+  }
+  int e;
+  std::frexp(a, &e);                               // a in [2^(e-1), 2^e)
+  const float ulp = std::ldexp(1.0f, e - 1 - 10);  // 10 fraction bits
+  return std::copysign(std::nearbyint(a / ulp) * ulp, f);
+}
+
+inline void sdf_set_transform(SdfGrid& g, const float pos[3], const float rot[4], float scale) {
+  double q[4], n = 0;
+  for (int a = 0; a < 4; ++a) {
+    q[a] = rot[a];
+    n += q[a] * q[a];
+  }
+  n = std::sqrt(n);
+  for (int a = 0; a < 4; ++a) q[a] /= n;
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  // rotation matrix of a unit quaternion
+  const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                       2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                       2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      g.R[3 * r + c] = static_cast<float>(R[3 * r + c]);
+      g.invR[3 * r + c] = static_cast<float>(R[3 * c + r]);
+    }
+  for (int a = 0; a < 3; ++a) g.position[a] = pos[a];
+  g.scale = scale;
+  g.invScale = static_cast<float>(1.0 / scale);
+}
+
 enum MatKind { MAT_FLUID, MAT_SOFT, MAT_CLOTH };
 
 template <typename T>
@@ -359,6 +408,8 @@ struct Engine {
   std::vector<Softbodies<T>> softs;
   std::vector<Cloth<T>> cloths;
   std::vector<Prim> prims;
+  std::vector<SdfGrid> sdfs;
+  std::vector<T> sdfLambda;  // 2 * cap * sdfs
   // loop
   bool built = false, initialized = false;
   uint32_t substeps = 4, iterations = 2;
@@ -765,6 +816,111 @@ struct Engine {
       }
     });
   }
+  // sample.ts:12-53: trilinear filter at continuous grid coordinate g,
+  // clamp to the edge voxels.
+  static T sdf_trilinear(const SdfGrid& G, T gx, T gy, T gz) {
+    gx -= static_cast<T>(0.5);
+    gy -= static_cast<T>(0.5);
+    gz -= static_cast<T>(0.5);
+    const int nx = static_cast<int>(G.res[0]), ny = static_cast<int>(G.res[1]), nz = static_cast<int>(G.res[2]);
+    const int i0 = std::min(std::max(static_cast<int>(std::floor(gx)), 0), nx - 2);
+    const int j0 = std::min(std::max(static_cast<int>(std::floor(gy)), 0), ny - 2);
+    const int k0 = std::min(std::max(static_cast<int>(std::floor(gz)), 0), nz - 2);
+    auto c01 = [](T t) { return t < 0 ? static_cast<T>(0) : (t > 1 ? static_cast<T>(1) : t); };
+    const T tx = c01(gx - static_cast<T>(i0)), ty = c01(gy - static_cast<T>(j0)), tz = c01(gz - static_cast<T>(k0));
+    const size_t sy = static_cast<size_t>(nx), sz = static_cast<size_t>(nx) * ny;
+    const size_t b = static_cast<size_t>(i0) + j0 * sy + k0 * sz;
+    auto v = [&](size_t o) { return static_cast<T>(G.phi[b + o]); };
+    auto lerp = [](T a, T c, T t) { return a + (c - a) * t; };
+    const T c00 = lerp(v(0), v(1), tx), c10 = lerp(v(sy), v(sy + 1), tx);
+    const T c0z = lerp(v(sz), v(sz + 1), tx), c1z = lerp(v(sz + sy), v(sz + sy + 1), tx);
+    return lerp(lerp(c00, c10, ty), lerp(c0z, c1z, ty), tz);
+  }
+  // sdf.ts:107-147: world -> local, phi, central-difference gradient one
+  // voxel apart, back to world.
+  static void sdf_sample(const SdfGrid& G, V3<T> x, T* phi, V3<T>* grad) {
+    const V3<T> off = v3<T>(x.x - static_cast<T>(G.position[0]), x.y - static_cast<T>(G.position[1]),
+                            x.z - static_cast<T>(G.position[2]));
+    auto row = [&](const float* M, int r, V3<T> a) {
+      return static_cast<T>(M[3 * r]) * a.x + static_cast<T>(M[3 * r + 1]) * a.y + static_cast<T>(M[3 * r + 2]) * a.z;
+    };
+    const T is = static_cast<T>(G.invScale);
+    const V3<T> xl = v3<T>(row(G.invR, 0, off) * is, row(G.invR, 1, off) * is, row(G.invR, 2, off) * is);
+    const T gx = (xl.x - static_cast<T>(G.origin[0])) * static_cast<T>(G.invVoxel[0]);
+    const T gy = (xl.y - static_cast<T>(G.origin[1])) * static_cast<T>(G.invVoxel[1]);
+    const T gz = (xl.z - static_cast<T>(G.origin[2])) * static_cast<T>(G.invVoxel[2]);
+    const T one = static_cast<T>(1), two = static_cast<T>(2);
+    const T p0 = sdf_trilinear(G, gx, gy, gz);
+    const V3<T> gl = v3<T>(
+        (sdf_trilinear(G, gx + one, gy, gz) - sdf_trilinear(G, gx - one, gy, gz)) / (two * static_cast<T>(G.voxel[0])),
+        (sdf_trilinear(G, gx, gy + one, gz) - sdf_trilinear(G, gx, gy - one, gz)) / (two * static_cast<T>(G.voxel[1])),
+        (sdf_trilinear(G, gx, gy, gz + one) - sdf_trilinear(G, gx, gy, gz - one)) / (two * static_cast<T>(G.voxel[2])));
+    *phi = p0 * static_cast<T>(G.scale);
+    *grad = v3<T>(row(G.R, 0, gl), row(G.R, 1, gl), row(G.R, 2, gl));
+  }
+  // SDFCollider.ts:256-281 + collider.ts:53-89 (static surface)
+  void sdf_solve() {
+    const T radius = sizeof(T) == 8 ? static_cast<T>(this->radius)
+                                    : static_cast<T>(static_cast<float>(this->radius));
+    const uint32_t ns = static_cast<uint32_t>(sdfs.size());
+    parallel_for(0, static_cast<int64_t>(cap), [&](int64_t pi) {
+      const uint32_t p = static_cast<uint32_t>(pi);
+      const T w = invMass[p];
+      if (!(w > 0)) return;
+      const V3<T> xStar = p3(pred, p);
+      const V3<T> disp = xStar - p3(pos, p);
+      for (uint32_t q = 0; q < ns; ++q) {
+        const SdfGrid& G = sdfs[q];
+        T phi;
+        V3<T> g;
+        sdf_sample(G, xStar, &phi, &g);
+        const T gl = length(g);
+        if (!(gl > static_cast<T>(1e-6))) continue;
+        const T reach = radius + static_cast<T>(G.thickness);
+        if (!(phi < reach)) continue;
+        const V3<T> n = g / gl;
+        const T depth = reach - phi;
+        const size_t li = (static_cast<size_t>(p) * ns + q) * 2;
+        const T lambdaN = sdfLambda[li] + depth / w;
+        sdfLambda[li] = lambdaN;
+        const V3<T> tang = disp - n * dot(disp, n);
+        const T tl = length(tang);
+        const T lambdaT = sdfLambda[li + 1];
+        const bool sticks = tl > static_cast<T>(1e-10) && (tl / w <= static_cast<T>(G.muS) * lambdaN - lambdaT);
+        const V3<T> push = n * depth;
+        accPos.add(p, sticks ? push - tang : push);
+        sdfLambda[li + 1] = lambdaT + (sticks ? tl / w : static_cast<T>(0));
+      }
+    });
+  }
+  // SDFCollider.ts:283-299 + collider.ts:96-118 (static surface)
+  void sdf_friction() {
+    const uint32_t ns = static_cast<uint32_t>(sdfs.size());
+    parallel_for(0, static_cast<int64_t>(cap), [&](int64_t pi) {
+      const uint32_t p = static_cast<uint32_t>(pi);
+      const T w = invMass[p];
+      if (!(w > 0)) return;
+      const V3<T> xStar = p3(pred, p);
+      const V3<T> velocity = p3(vel, p);
+      for (uint32_t q = 0; q < ns; ++q) {
+        const T lambdaN = sdfLambda[(static_cast<size_t>(p) * ns + q) * 2];
+        if (!(lambdaN > 0)) continue;
+        const SdfGrid& G = sdfs[q];
+        T phi;
+        V3<T> g;
+        sdf_sample(G, xStar, &phi, &g);
+        const T len = length(g);
+        if (!(len > static_cast<T>(1e-6))) continue;
+        const V3<T> n = g / len;
+        const V3<T> vT = velocity - n * dot(n, velocity);
+        const T vTL = length(vT);
+        if (vTL > static_cast<T>(1e-6)) {
+          const T change = tmin(static_cast<T>(G.muK) * lambdaN * w / dt, vTL);
+          accVel.add(p, neg((vT / vTL) * change));
+        }
+      }
+    });
+  }
   void apply_acc(Accum<T>& a, std::vector<T>& target, uint32_t s, uint32_t e) {
     for (uint32_t i = s; i < e; ++i) {
       const V3<T> c = a.take(i, &a.flag);
@@ -1130,7 +1286,10 @@ struct Engine {
     // preSolve
     if (hasColliders) accPos.reset();
     if (hasGrid) rebuild_grid(pred);
-    if (hasColliders) std::fill(primLambda.begin(), primLambda.end(), static_cast<T>(0));
+    if (hasColliders) {
+      std::fill(primLambda.begin(), primLambda.end(), static_cast<T>(0));
+      std::fill(sdfLambda.begin(), sdfLambda.end(), static_cast<T>(0));
+    }
     for (auto& m : materials) {
       if (m.first == MAT_FLUID) {
         Fluid<T>& f = fluids[m.second];
@@ -1181,6 +1340,7 @@ struct Engine {
       }
       if (hasColliders) {
         collider_solve();
+        sdf_solve();
         apply_acc(accPos, pred, 0, cap);
       }
     }
@@ -1200,6 +1360,7 @@ struct Engine {
     if (hasColliders) {
       accVel.reset();
       collider_friction();
+      sdf_friction();
       apply_acc(accVel, vel, 0, cap);
       clock = tmax(clock - dt, static_cast<T>(0));
     }
@@ -1676,6 +1837,69 @@ int or_set_primitive(void* h, uint32_t slot, const pf_primitive* p) {
   return rc;
 }
 
+int or_add_sdf_collider(void* h, const pf_sdf_desc* d, uint32_t* slot) {
+  Scene* s = static_cast<Scene*>(h);
+  if (!d || !d->data) return fail(PF_ERR_INVALID, "SDFCollider: no distance data");
+  s->visit([&](auto& e) {
+    SdfGrid g;
+    const size_t n = static_cast<size_t>(d->res[0]) * d->res[1] * d->res[2];
+    for (int a = 0; a < 3; ++a) {
+      g.res[a] = d->res[a];
+      g.origin[a] = d->origin[a];
+      g.voxel[a] = d->voxel_size[a];
+      g.invVoxel[a] = static_cast<float>(1.0 / static_cast<double>(d->voxel_size[a]));
+    }
+    g.phi.resize(n);
+    for (size_t i = 0; i < n; ++i) g.phi[i] = half_round(d->data[i]);
+    g.thickness = d->thickness;
+    g.muS = d->mu_s;
+    g.muK = d->mu_k;
+    sdf_set_transform(g, d->position, d->rotation, d->scale);
+    e.sdfs.push_back(std::move(g));
+    if (slot) *slot = static_cast<uint32_t>(e.sdfs.size() - 1);
+  });
+  return PF_OK;
+}
+
+int or_set_sdf_transform(void* h, uint32_t slot, const float* pos, const float* rot, float scale) {
+  Scene* s = static_cast<Scene*>(h);
+  int rc = PF_OK;
+  s->visit([&](auto& e) {
+    if (slot >= e.sdfs.size()) {
+      rc = fail(PF_ERR_INVALID, "SDFCollider: no collider in slot");
+      return;
+    }
+    sdf_set_transform(e.sdfs[slot], pos, rot, scale);
+  });
+  return rc;
+}
+
+// SDF sample at points (tests): phi and the world gradient per point.
+int or_sdf_sample(const pf_sdf_desc* d, const float* pts, uint32_t n, float* phi, float* grad) {
+  SdfGrid g;
+  const size_t nv = static_cast<size_t>(d->res[0]) * d->res[1] * d->res[2];
+  for (int a = 0; a < 3; ++a) {
+    g.res[a] = d->res[a];
+    g.origin[a] = d->origin[a];
+    g.voxel[a] = d->voxel_size[a];
+    g.invVoxel[a] = static_cast<float>(1.0 / static_cast<double>(d->voxel_size[a]));
+  }
+  g.phi.resize(nv);
+  for (size_t i = 0; i < nv; ++i) g.phi[i] = half_round(d->data[i]);
+  g.thickness = d->thickness;
+  sdf_set_transform(g, d->position, d->rotation, d->scale);
+  for (uint32_t i = 0; i < n; ++i) {
+    float p;
+    V3<float> gr;
+    Engine<float>::sdf_sample(g, v3<float>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), &p, &gr);
+    phi[i] = p;
+    grad[3 * i] = gr.x;
+    grad[3 * i + 1] = gr.y;
+    grad[3 * i + 2] = gr.z;
+  }
+  return PF_OK;
+}
+
 int or_loop_build(void* h, const pf_loop_desc* d, uint32_t table_size) {
   Scene* s = static_cast<Scene*>(h);
   int rc = PF_OK;
@@ -1697,12 +1921,13 @@ int or_loop_build(void* h, const pf_loop_desc* d, uint32_t table_size) {
       e.grid.table_size = table_size ? table_size
                                      : std::min<uint32_t>(next_pow2(2ull * e.cap), 1u << 20);
     }
-    e.hasColliders = !e.prims.empty();
+    e.hasColliders = !e.prims.empty() || !e.sdfs.empty();
     if (e.hasColliders) {
       e.accPos.init(e.cap, 10.0);
       e.accVel.init(e.cap, 50.0);
       e.primCap = static_cast<uint32_t>(e.prims.size());
       e.primLambda.assign(2 * static_cast<size_t>(e.cap) * e.primCap, 0);
+      e.sdfLambda.assign(2 * static_cast<size_t>(e.cap) * e.sdfs.size(), 0);
     }
     e.built = true;
   });

@@ -1,0 +1,238 @@
+"""Scenes of the reference's analytical known-answer tests, as recipes that
+either backend (the CUDA path through the C ABI, or the oracle) replays.
+
+Each builder names the reference test it restates; the expected values and
+tolerances live in the tests that use these scenes.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from pfsim import recipe as R
+
+DT = 1.0 / 60.0
+G = 9.81
+
+
+def free_fall() -> R.Recipe:
+    """tests/analytical/integrate/integrate-free-fall.gpu.test.ts:8-24: one
+    particle at the origin, no material, no collider, one substep."""
+    return R.Recipe(
+        capacity=1,
+        radius=0.05,
+        uploads=[R.Upload(0, np.zeros((1, 3), np.float32), np.zeros((1, 3), np.float32), np.ones(1, np.float32))],
+        loop=R.LoopOpts(substeps=1),
+        name="free-fall",
+    )
+
+
+def free_fall_reference(steps: int) -> float:
+    """The test's own CPU reference (integrate-free-fall.gpu.test.ts:26-32):
+    semi-implicit Euler in double precision."""
+    v = y = 0.0
+    for _ in range(steps):
+        v -= G * DT
+        y += v * DT
+    return y
+
+
+def distance_pair(compliance: float, substeps: int, iterations: int, constrained: bool = True) -> R.Recipe:
+    """tests/analytical/xpbd/xpbd-limits.gpu.test.ts:44-56 and 80-106: particle 0
+    pinned at the origin, particle 1 at (0, -1, 0), joined by one distance
+    constraint of rest length 1 (a one-edge cloth graph carries it)."""
+    pos = np.array([[0.0, 0.0, 0.0], [0.0, -1.0, 0.0]], np.float32)
+    w = np.array([0.0, 1.0], np.float32)
+    r = R.Recipe(capacity=2, radius=0.02, loop=R.LoopOpts(substeps=substeps, iterations=iterations),
+                 name=f"distance-pair-{compliance:g}")
+    if constrained:
+        r.materials.append(("cloth", R.ClothOpts(offset=0, positions=pos, inv_mass=w,
+                                                 pairs=np.array([[0, 1]], np.uint32),
+                                                 rest_lengths=np.array([1.0], np.float32),
+                                                 stretch_compliance=compliance)))
+    else:
+        r.uploads.append(R.Upload(0, pos, np.zeros_like(pos), w))
+    return r
+
+
+LATTICE, SPACING, H, REST = 5, 0.025, 0.04, 1000.0
+
+
+def density_lattice() -> R.Recipe:
+    """tests/analytical/fluids/density-pair-list-cpu-parity.gpu.test.ts:33-86:
+    a 5x5x5 lattice at spacing 0.025, h = 0.04, rest density 1000, mass
+    rho0 * spacing^3; no gravity, so the first lambda pass sees the lattice."""
+    idx = np.arange(LATTICE ** 3)
+    x, y, z = idx % LATTICE, (idx // LATTICE) % LATTICE, idx // (LATTICE * LATTICE)
+    pos = (np.stack([x, y, z], -1) * SPACING).astype(np.float32)
+    m = REST * SPACING ** 3
+    w = np.full(pos.shape[0], np.float32(1.0 / m), np.float32)
+    r = R.Recipe(capacity=pos.shape[0], radius=SPACING * 0.5,
+                 uploads=[R.Upload(0, pos, np.zeros_like(pos), w)],
+                 loop=R.LoopOpts(substeps=1, iterations=1, gravity=(0.0, 0.0, 0.0)),
+                 name="density-lattice")
+    r.materials.append(("fluid", R.FluidOpts(range=(0, pos.shape[0]), rest_density=REST, particle_spacing=SPACING,
+                                             smoothing_radius=H, compliance=1e-6)))
+    return r
+
+
+def density_brute_force() -> np.ndarray:
+    """The test's CPU ground truth (density-pair-list-cpu-parity.gpu.test.ts:94-118):
+    rho_i = sum_j m W_poly6(|x_i - x_j|, h), double precision."""
+    idx = np.arange(LATTICE ** 3)
+    p = np.stack([idx % LATTICE, (idx // LATTICE) % LATTICE, idx // (LATTICE * LATTICE)], -1) * SPACING
+    p = p.astype(np.float32).astype(np.float64)
+    poly6 = 315.0 / (64.0 * math.pi * H ** 9)
+    m = REST * SPACING ** 3
+    d = ((p[:, None, :] - p[None, :, :]) ** 2).sum(-1)
+    t = np.where(d < H * H, (H * H - d) ** 3, 0.0)
+    return m * poly6 * t.sum(1)
+
+
+def plane_rest() -> R.Recipe:
+    """tests/analytical/collider/collider-plane-rest.gpu.test.ts:16-34: one
+    particle of radius 0.05 dropped from y = 0.5 onto the plane y = 0
+    (muS 0.5, muK 0.4), 4 substeps, 4 iterations."""
+    pos = np.array([[0.0, 0.5, 0.0]], np.float32)
+    return R.Recipe(capacity=1, radius=0.05,
+                    uploads=[R.Upload(0, pos, np.zeros_like(pos), np.ones(1, np.float32))],
+                    prims=[R.plane((0, 1, 0), (0, 0, 0), 0.5, 0.4)],
+                    loop=R.LoopOpts(substeps=4, iterations=4),
+                    name="plane-rest")
+
+
+def run_trace(scene, frames: int, every: int = 1, field=None):
+    """Step a built scene, reading positions (and velocities) every `every`
+    frames and on the last one."""
+    from pfsim import _native as N
+
+    out = []
+    for n in range(frames):
+        scene.step(DT)
+        if n % every == 0 or n == frames - 1:
+            out.append((scene.readback(N.PF_FIELD_POSITIONS).copy(), scene.readback(N.PF_FIELD_VELOCITIES).copy()))
+    return out
+
+
+# ---- the colouring test's graphs (xpbd-group-partition.test.ts:48-166) ----
+def chain_pairs(n: int = 10) -> np.ndarray:
+    return np.array([[i, i + 1] for i in range(n - 1)], np.uint32)
+
+
+def star_pairs(n: int = 8) -> np.ndarray:
+    return np.array([[0, leaf] for leaf in range(1, n + 1)], np.uint32)
+
+
+def random_graphs(trials: int = 10):
+    """The test's LCG (multiplier 1664525, increment 1013904223, seed
+    0xdeadc0de) drawing 10 random simple graphs (xpbd-group-partition.test.ts:102-127)."""
+    state = [0xDEADC0DE]
+
+    def nxt():
+        state[0] = (state[0] * 1664525 + 1013904223) & 0xFFFFFFFF
+        return state[0] / 0x100000000
+
+    graphs = []
+    for _ in range(trials):
+        n_particles = 20 + int(math.floor(nxt() * 30))
+        n_edges = 30 + int(math.floor(nxt() * 50))
+        seen = set()
+        pairs = []
+        attempts = 0
+        while len(pairs) < n_edges and attempts < n_edges * 10:
+            attempts += 1
+            i = int(math.floor(nxt() * n_particles))
+            j = int(math.floor(nxt() * n_particles))
+            if i == j:
+                continue
+            key = (min(i, j), max(i, j))
+            if key in seen:
+                continue
+            seen.add(key)
+            pairs.append((i, j))
+        graphs.append(np.array(pairs, np.uint32).reshape(-1, 2))
+    return graphs
+
+
+def rot_x(t):
+    c, s = math.cos(t), math.sin(t)
+    return np.array([[1, 0, 0], [0, c, -s], [0, s, c]])
+
+
+def rot_y(t):
+    c, s = math.cos(t), math.sin(t)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+
+
+def rot_z(t):
+    c, s = math.cos(t), math.sin(t)
+    return np.array([[c, -s, 0], [s, c, 0], [0, 0, 1]])
+
+
+def polar_cases():
+    """(A, expected R, tolerance) of softbody-polar-decomp.gpu.test.ts:119-200."""
+    I = np.eye(3)
+    Rk = rot_x(0.4) @ rot_z(-0.3)
+    S = np.array([[1.5, 0.2, 0.0], [0.2, 1.2, 0.0], [0.0, 0.0, 1.0]])
+    return [
+        ("identity", I, I, 1e-4),
+        ("rot-z", rot_z(math.pi / 4), rot_z(math.pi / 4), 1e-4),
+        ("rot-y", rot_y(math.pi / 3), rot_y(math.pi / 3), 1e-4),
+        ("rot-x", rot_x(-math.pi / 6), rot_x(-math.pi / 6), 1e-4),
+        ("composed", rot_z(0.3) @ rot_y(-0.7) @ rot_x(0.5), rot_z(0.3) @ rot_y(-0.7) @ rot_x(0.5), 1e-4),
+        ("uniform-stretch", np.diag([2.5, 2.5, 2.5]), I, 1e-4),
+        ("diag-stretch", np.diag([3.0, 1.5, 0.8]), I, 1e-4),
+        ("rot-stretch", rot_z(math.pi / 6) @ np.diag([2.0, 1.0, 0.5]), rot_z(math.pi / 6), 1e-4),
+        ("rot-shear", Rk @ S, Rk, 1e-4),
+        ("near-identity", rot_z(1e-3), rot_z(1e-3), 1e-5),
+    ]
+
+
+# ---- SDF collider (tests/analytical/sdf/*) ----
+def sdf_sphere_grid(res: int = 64, radius: float = 0.5, pad: float = 0.1):
+    """An exact sphere SDF baked at voxel centres (the reference bakes a UV
+    sphere mesh; the analytic field stands in for the bake)."""
+    from pfsim import recipe as R
+
+    return R.sphere_sdf((0.0, 0.0, 0.0), radius, res=res, pad=pad)
+
+
+def lcg_js(seed: int):
+    """The tests' `seed = (Math.imul(seed, 1664525) + 1013904223) | 0` and
+    `(seed >>> 0) / 2^32`."""
+    state = [seed & 0xFFFFFFFF]
+
+    def nxt():
+        state[0] = (state[0] * 1664525 + 1013904223) & 0xFFFFFFFF
+        return state[0] / 0x100000000
+
+    return nxt
+
+
+def sdf_rotated_scaled():
+    """sdf-rotated-scaled.gpu.test.ts:41-110: 100 particles (r = 0.04) inside a
+    sphere of mesh radius 0.5 placed at (0.3, 0, -0.2), scaled 2x and rotated
+    pi/3 about (1, 1, 0); one step of 1 substep x 4 iterations, no gravity."""
+    rand = lcg_js(0xC0FFEE42)
+    center = np.array([0.3, 0.0, -0.2])
+    scale, r = 2.0, 0.04
+    inner = scale * 0.5 - 2 * r
+    pts = []
+    while len(pts) < 100:
+        u = np.array([rand() * 2 - 1, rand() * 2 - 1, rand() * 2 - 1])
+        if (u * u).sum() > 1:
+            continue
+        pts.append(center + u * inner)
+    pos = np.array(pts, np.float32)
+    axis = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
+    q = (*(axis * np.sin(np.pi / 6)), np.cos(np.pi / 6))
+    g = sdf_sphere_grid()
+    g.position, g.rotation, g.scale = tuple(center), q, scale
+    from pfsim import recipe as R
+
+    rec = R.Recipe(capacity=100, radius=r, uploads=[R.Upload(0, pos, np.zeros_like(pos), np.ones(100, np.float32))],
+                   sdfs=[g], loop=R.LoopOpts(substeps=1, iterations=4, gravity=(0.0, 0.0, 0.0)),
+                   name="sdf-rotated-scaled")
+    return rec, center, scale * 0.5

@@ -38,3 +38,28 @@ def test_abi_version_and_error_text():
     d.cell_size = 0.1
     d.table_size = 3
     assert lib.pf_grid_cells(C.byref(d)) == 0
+
+
+def test_server_admission_estimate_is_host_only():
+    """pf_server_estimate_bytes plans a scene's world on the host (no GPU):
+    the estimate grows with the particle count and holds at least the
+    double-buffered per-particle state."""
+    from pfsim import recipe as R
+    from pfsim import workloads as W
+
+    small = R.Server.estimate_bytes(W.dam_break(4000, seed=1))
+    big = R.Server.estimate_bytes(W.dam_break(16000, seed=1))
+    n_small = W.dam_break(4000, seed=1).capacity
+    assert small > 2 * 56 * n_small
+    assert 2.5 < big / small < 5.5
+
+
+def test_unbuilt_scene_is_refused_without_loop_options():
+    from pfsim import recipe as R
+    from pfsim import workloads as W
+
+    scene = R.NativeBackend().build(W.dam_break(2000, seed=1), build_loop=False)
+    out = C.c_uint64(0)
+    rc = N.lib().pf_server_estimate_bytes(scene.h, None, C.byref(out))
+    assert rc == N.PF_ERR_STATE
+    assert b"SimLoop" in N.lib().pf_last_error()

@@ -1,0 +1,144 @@
+"""The oracle against the reference's analytical known-answer tests (CPU).
+
+Each test restates one reference test's scene, expected value and tolerance
+(tests/analytical/...), runs it on the oracle, and so pins the oracle's
+integrator, PBF density, XPBD distance constraint, collider contact, greedy
+colouring and polar decomposition to the reference's own expectations.
+The same scenes run on the CUDA path in test_kat_gpu.py.
+"""
+
+import numpy as np
+import pytest
+
+import kat_scenes as K
+from pfsim import _native as N
+
+
+@pytest.fixture(scope="module")
+def cpu(oracle):
+    return oracle.OracleBackend(precision=32)
+
+
+def test_free_fall(cpu):
+    """integrate-free-fall.gpu.test.ts:34-44: y after 60 steps within 1e-4 of
+    the semi-implicit Euler reference."""
+    s = cpu.build(K.free_fall())
+    for _ in range(60):
+        s.step(K.DT)
+    y = float(s.readback(N.PF_FIELD_POSITIONS)[0, 1])
+    assert y < 0
+    assert abs(y - K.free_fall_reference(60)) < 1e-4
+
+
+def test_xpbd_rigid_limit(cpu):
+    """xpbd-limits.gpu.test.ts:44-77 and 140-146: alpha = 0, 4 substeps x 4
+    iterations, |len - L0| < 1e-4 sampled every 25 of 1000 frames."""
+    s = cpu.build(K.distance_pair(0.0, 4, 4))
+    drift = 0.0
+    for p, _ in K.run_trace(s, 1000, every=25):
+        drift = max(drift, abs(float(np.linalg.norm(p[1, :3].astype(np.float64) - p[0, :3])) - 1.0))
+    assert drift < 1e-4
+
+
+def test_xpbd_soft_limit(cpu):
+    """xpbd-limits.gpu.test.ts:80-131 and 149-156: alpha = 1e12 matches the
+    unconstrained particle within 1e-6 over 120 frames (1 substep, 2 iterations)."""
+    a = cpu.build(K.distance_pair(1e12, 1, 2))
+    b = cpu.build(K.distance_pair(1e12, 1, 2, constrained=False))
+    ta, tb = K.run_trace(a, 120, every=20), K.run_trace(b, 120, every=20)
+    dev = max(float(np.abs(pa[1, :3] - pb[1, :3]).max()) for (pa, _), (pb, _) in zip(ta, tb))
+    assert dev < 1e-6
+
+
+def test_density_matches_brute_force(cpu):
+    """density-pair-list-cpu-parity.gpu.test.ts:120-146: |d rho| < 5e-3 and
+    |d rho| / max(rho, 1) < 1e-5 on the 5^3 lattice."""
+    s = cpu.build(K.density_lattice())
+    s.step(K.DT)
+    rho = s.readback(N.PF_FIELD_DENSITY).astype(np.float64)
+    ref = K.density_brute_force()
+    d = np.abs(rho - ref)
+    assert d.max() < 5e-3
+    assert (d / np.maximum(ref, 1.0)).max() < 1e-5
+
+
+def test_plane_rest(cpu):
+    """collider-plane-rest.gpu.test.ts:36-75: settles at y = r, never below
+    r - 1e-4, |vy| < 0.1 after 60 frames."""
+    s = cpu.build(K.plane_rest())
+    tr = K.run_trace(s, 60)
+    ys = [float(p[0, 1]) for p, _ in tr]
+    r = 0.05
+    assert r - 1e-4 < ys[-1] < r + 5e-3
+    assert abs(float(tr[-1][1][0, 1])) < 0.1
+    assert min(ys) > r - 1e-4
+
+
+@pytest.mark.parametrize("name,a,expected,tol", K.polar_cases(), ids=[c[0] for c in K.polar_cases()])
+def test_polar_decomposition(oracle, name, a, expected, tol):
+    """softbody-polar-decomp.gpu.test.ts:119-200 (FP32 oracle)."""
+    r = oracle.polar(a).astype(np.float64)
+    assert np.abs(r - expected).max() < tol
+    if name == "rot-shear":
+        assert np.abs(r @ r.T - np.eye(3)).max() < 1e-4
+        assert abs(np.linalg.det(r) - 1.0) < 1e-4
+
+
+def _no_conflict(pairs, groups, k):
+    for g in range(k):
+        sel = pairs[groups == g].reshape(-1)
+        assert np.unique(sel).size == sel.size, f"group {g} shares a particle"
+
+
+def test_colouring_empty(oracle):
+    g, k = oracle.color_constraints(np.zeros((0, 2), np.uint32))
+    assert k == 0 and g.size == 0
+
+
+def test_colouring_chain(oracle):
+    p = K.chain_pairs(10)
+    g, k = oracle.color_constraints(p)
+    assert k <= 2
+    _no_conflict(p, g, k)
+
+
+def test_colouring_star(oracle):
+    p = K.star_pairs(8)
+    g, k = oracle.color_constraints(p)
+    assert k == 8
+    _no_conflict(p, g, k)
+
+
+def test_colouring_random(oracle):
+    """xpbd-group-partition.test.ts:92-143: numGroups <= max(1, 2 maxDegree)."""
+    for p in K.random_graphs():
+        g, k = oracle.color_constraints(p)
+        _no_conflict(p, g, k)
+        deg = np.bincount(p.reshape(-1)).max()
+        assert k <= max(1, 2 * deg)
+
+
+def test_sdf_gradient_magnitude(oracle):
+    """sdf-gradient-sanity.test.ts:20-64: |grad phi| in [0.8, 1.2] at 1000
+    random points two voxels inside the grid's faces."""
+    g = K.sdf_sphere_grid()
+    res = g.data.shape[0]
+    vs = g.voxel_size[0]
+    lo = np.array(g.origin) + 2 * vs
+    hi = np.array(g.origin) + (res - 2) * vs
+    rand = K.lcg_js(0xDADA)
+    pts = np.array([[lo[a] + (hi[a] - lo[a]) * rand() for a in range(3)] for _ in range(1000)])
+    _, grad = oracle.sdf_sample(g, pts)
+    mag = np.linalg.norm(grad.astype(np.float64), axis=1)
+    assert mag.min() > 0.8 and mag.max() < 1.2
+
+
+def test_sdf_rotated_scaled_projection(cpu):
+    """sdf-rotated-scaled.gpu.test.ts:110-137: after one step no particle is
+    closer than R - 5e-3 to the scaled sphere's centre."""
+    rec, center, radius = K.sdf_rotated_scaled()
+    s = cpu.build(rec)
+    s.step(K.DT)
+    d = np.linalg.norm(s.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64) - center, axis=1)
+    assert (d < radius - 5e-3).sum() == 0
+    assert d.min() > radius - 5e-3

@@ -20,22 +20,52 @@
 
 #include "common.cuh"
 #include "world.cuh"
+#include "capi_handles.cuh"
 
-struct pf_scene {
-  pf::SceneSpec spec;
-  std::unique_ptr<pf::World> world;
-};
-
-struct pf_batch {
-  std::vector<std::unique_ptr<pf::SceneSpec>> specs;
-  std::unique_ptr<pf::World> world;
-};
 
 namespace pf {
 namespace {
 
 bool range_ok(const SceneSpec& s, RangeU r) { return r.count > 0 && (uint64_t)r.start + r.count <= s.cap; }
 bool overlaps(RangeU a, RangeU b) { return a.start < b.start + b.count && b.start < a.start + a.count; }
+
+// f32 -> IEEE half, round to nearest even, after clamping to +-65504 as the
+// SDFCollider's half-float upload does (SDFCollider.ts:101-103).
+uint16_t half_rn(float f) {
+  if (f > 65504.0f) f = 65504.0f;
+  if (f < -65504.0f) f = -65504.0f;
+  uint32_t x;
+  std::memcpy(&x, &f, 4);
+  const uint32_t sign = (x >> 16) & 0x8000u;
+  const uint32_t ax = x & 0x7fffffffu;
+  if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7e00u);  // NaN
+  if (ax < 0x38800000u) {                                    // below 2^-14: a half subnormal
+    float af;
+    std::memcpy(&af, &ax, 4);
+    return (uint16_t)(sign | (uint32_t)std::nearbyint(af * 16777216.0f));
+  }
+  uint32_t h = ((ax >> 23) - 112u) << 10 | ((ax & 0x7fffffu) >> 13);
+  const uint32_t rem = ax & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
+  return (uint16_t)(sign | h);
+}
+
+// SDFCollider.setPosition / setRotation / setScale checks (SDFCollider.ts:170-201).
+pf_status sdf_transform(const float pos[3], const float rot[4], float scale, SdfSpec* g) {
+  double q[4], n = 0;
+  for (int a = 0; a < 4; ++a) {
+    q[a] = rot[a];
+    n += q[a] * q[a];
+  }
+  n = std::sqrt(n);
+  if (!(n > 1e-12) || !std::isfinite(n)) return fail(PF_ERR_INVALID, "SDFCollider.setRotation: rotation must be a non-zero quaternion");
+  if (!(scale > 0) || !std::isfinite(scale))
+    return fail(PF_ERR_INVALID, "SDFCollider.setScale: scale must be positive, got " + std::to_string(scale));
+  for (int a = 0; a < 3; ++a) g->position[a] = pos[a];
+  for (int a = 0; a < 4; ++a) g->rot_q[a] = q[a] / n;
+  g->scale = scale;
+  return PF_OK;
+}
 
 pf_status not_built(const pf_scene* s, const char* what) {
   if (!s) return fail(PF_ERR_INVALID, std::string(what) + ": scene is NULL");
@@ -397,6 +427,54 @@ pf_status pf_set_primitive(pf_scene* s, uint32_t slot, const pf_primitive* p) {
   return PF_OK;
 }
 
+pf_status pf_add_sdf_collider(pf_scene* s, const pf_sdf_desc* d, uint32_t* slot) {
+  PF_TRY(not_built(s, "SDFCollider"));
+  if (!d || !d->data) return fail(PF_ERR_INVALID, "SDFCollider: no distance data");
+  for (int a = 0; a < 3; ++a)
+    if (d->res[a] < 4)
+      return fail(PF_ERR_INVALID, "SDFCollider: resolution must be integers >= 4, got [" + std::to_string(d->res[0]) +
+                                      ", " + std::to_string(d->res[1]) + ", " + std::to_string(d->res[2]) + "]");
+  const uint64_t n = (uint64_t)d->res[0] * d->res[1] * d->res[2];
+  if (n > (1ull << 31)) return fail(PF_ERR_INVALID, "SDFCollider: grid too large");
+  for (int a = 0; a < 3; ++a)
+    if (!(d->voxel_size[a] > 0) || !std::isfinite(d->voxel_size[a]))
+      return fail(PF_ERR_INVALID, "SDFCollider: voxel size must be positive");
+  if (!(d->thickness >= 0) || !std::isfinite(d->thickness))
+    return fail(PF_ERR_INVALID, "SDFCollider: thickness must be non-negative, got " + std::to_string(d->thickness));
+  if (!(d->mu_s >= 0) || !(d->mu_k >= 0))
+    return fail(PF_ERR_INVALID, "SDFCollider: friction coefficients must be non-negative");
+  SdfSpec g;
+  PF_TRY(sdf_transform(d->position, d->rotation, d->scale, &g));
+  for (int a = 0; a < 3; ++a) {
+    g.res[a] = d->res[a];
+    g.origin[a] = d->origin[a];
+    g.voxel[a] = d->voxel_size[a];
+  }
+  g.thickness = d->thickness;
+  g.mu_s = d->mu_s;
+  g.mu_k = d->mu_k;
+  g.half.resize(n);
+  for (uint64_t i = 0; i < n; ++i) g.half[i] = half_rn(d->data[i]);
+  s->spec.sdfs.push_back(std::move(g));
+  if (slot) *slot = (uint32_t)s->spec.sdfs.size() - 1;
+  return PF_OK;
+}
+
+pf_status pf_set_sdf_transform(pf_scene* s, uint32_t slot, const float position[3], const float rotation[4],
+                               float scale) {
+  if (!s || !position || !rotation) return fail(PF_ERR_INVALID, "SDFCollider: NULL argument");
+  if (slot >= s->spec.sdfs.size())
+    return fail(PF_ERR_INVALID, "SDFCollider: no collider in slot " + std::to_string(slot));
+  SdfSpec t;
+  PF_TRY(sdf_transform(position, rotation, scale, &t));
+  if (s->world) return s->world->set_sdf_transform(0, slot, t.position, t.rot_q, t.scale);
+  SdfSpec& g = s->spec.sdfs[slot];
+  for (int a = 0; a < 3; ++a) g.position[a] = t.position[a];
+  for (int a = 0; a < 4; ++a) g.rot_q[a] = t.rot_q[a];
+  g.scale = t.scale;
+  return PF_OK;
+}
+
 pf_status pf_loop_build(pf_scene* s, const pf_loop_desc* d) {
   PF_TRY(not_built(s, "SimLoop"));
   if (!d) return fail(PF_ERR_INVALID, "SimLoop: options are NULL");
@@ -422,7 +500,12 @@ pf_status pf_step(pf_scene* s, double dt) {
 pf_status pf_readback(pf_scene* s, uint32_t field, void* dst, size_t bytes) {
   if (!s || !dst) return fail(PF_ERR_INVALID, "readback: NULL argument");
   if (s->world) return s->world->readback(0, field, dst, bytes);
-  const SceneSpec& sp = s->spec;
+  return pf::spec_readback(s->spec, field, dst, bytes);
+}
+
+}  // extern "C"
+
+pf_status pf::spec_readback(const SceneSpec& sp, uint32_t field, void* dst, size_t bytes) {
   auto copy = [&](const void* src, size_t b) -> pf_status {
     if (bytes < b) return fail(PF_ERR_INVALID, "readback: destination too small");
     std::memcpy(dst, src, b);
@@ -440,6 +523,8 @@ pf_status pf_readback(pf_scene* s, uint32_t field, void* dst, size_t bytes) {
     default: return fail(PF_ERR_STATE, "readback: field is available once the SimLoop is built");
   }
 }
+
+extern "C" {
 
 pf_status pf_overflow_read(pf_scene* s, pf_overflow* out) {
   if (!s || !out) return fail(PF_ERR_INVALID, "readbackOverflow: NULL argument");
@@ -501,5 +586,21 @@ pf_status pf_batch_last_step_ms(pf_batch* b, float* ms) {
 }
 
 uint64_t pf_batch_particle_substeps(pf_batch* b) { return b ? b->world->particle_substeps_per_step() : 0; }
+
+uint64_t pf_batch_launches_per_step(pf_batch* b) { return b ? b->world->launches_per_step() : 0; }
+uint64_t pf_batch_step_upload_bytes(pf_batch* b) { return b ? b->world->step_upload_bytes() : 0; }
+
+void* pf_batch_stream(pf_batch* b) { return b ? (void*)b->world->stream() : nullptr; }
+void* pf_scene_stream(pf_scene* s) { return (s && s->world) ? (void*)s->world->stream() : nullptr; }
+
+pf_status pf_batch_read_positions(pf_batch* b, float* dst_host, size_t bytes) {
+  if (!b || !dst_host) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->read_positions(dst_host, bytes);
+}
+
+pf_status pf_batch_profile_stage(pf_batch* b, uint32_t stage, uint32_t reps, float* ms, uint64_t* items) {
+  if (!b || !ms) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->profile_stage(stage, reps, ms, items);
+}
 
 }  // extern "C"

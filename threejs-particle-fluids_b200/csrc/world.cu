@@ -18,6 +18,7 @@
 
 #include "world.cuh"
 #include "world_kernels.cuh"
+#include "world_tiles.cuh"
 
 namespace pf {
 
@@ -118,6 +119,9 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   V.nxt.tag[k] = V.cur.tag[o];
   V.ids[k] = id;
   V.inv[id] = k;
+  // lambda is read for every neighbour, fluid or not (positionDelta.ts:193),
+  // and is zero for particles no fluid solves; slots change owners here.
+  V.lambda[k] = 0.0f;
   for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
   if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_
   const DevBoundary B = V.bnds[b - 1];
   if (B.is_static != want_static) return;
   const DevScene& S = scene_at(V, k);
-  if (!want_static && sub >= S.substeps) return;
+  if (want_static ? !S.init_pending : sub >= S.substeps) return;
   const DevFluid& F = V.fluids[B.fluid];
   const float4* pos = want_static ? V.cur.x : V.cur.xs;
   const f3 xi = xyz(pos[k]);
@@ -158,112 +162,6 @@ __global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_
     return true;
   });
   V.cur.bv[k] = 1.0f / fmaxf(sum, 1e-12f);
-}
-
-// neighborList.ts:48-71: up to 64 neighbours within h at the predicted
-// positions of this substep, in walk order, self included; stored as slots,
-// column-major so a warp reads its m-th neighbours contiguously.
-__global__ void __launch_bounds__(kBlock) k_neighbors(WorldView V, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
-  const DevFluid& F = V.fluids[f - 1];
-  const f3 xi = xyz(V.cur.xs[k]);
-  uint32_t cnt = 0;
-  bool over = false;
-  const uint32_t n = V.n;
-  walk27(S, V.cstart, V.ccount, xi, [&](uint32_t j) {
-    const f3 off = xi - xyz(V.cur.xs[j]);
-    if (dot_rn(off) < F.hsq) {
-      if (cnt < kMaxNbr) {
-        V.nbr[(size_t)cnt * n + k] = j;
-        ++cnt;
-      } else {
-        over = true;
-        return false;
-      }
-    }
-    return true;
-  });
-  V.ncount[k] = cnt;
-  if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
-}
-
-// lambda.ts:41-71
-__global__ void __launch_bounds__(kBlock) k_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
-  const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps || it >= S.iterations) return;
-  const float4 xi4 = V.cur.xs[k];
-  const f3 xi = xyz(xi4);
-  float rho = 0.0f, gss = 0.0f;
-  f3 gs = mk(0.0f, 0.0f, 0.0f);
-  const uint32_t cnt = V.ncount[k];
-  const uint32_t n = V.n;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = V.nbr[(size_t)m * n + k];
-    const float4 xj = V.cur.xs[j];
-    const float mass = neighbor_mass(V.cur.bv[j], xj.w, F.rho0);
-    const f3 off = xi - xyz(xj);
-    rho += mass * poly6(dot(off, off), F);
-    const f3 g = spiky_grad(off, F) * mass;
-    gs = gs + g;
-    gss += dot(g, g) * xj.w;
-  }
-  V.density[k] = rho;
-  const float C = rho * F.inv_rho0 - 1.0f;
-  if (C <= 0.0f) {
-    V.lambda[k] = 0.0f;
-    return;
-  }
-  const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
-  const float at = F.compliance / (S.dt * S.dt);
-  V.lambda[k] = -C / fmaxf(gn + at, 1e-20f);
-}
-
-// positionDelta.ts:41-85 (with the reaction on dynamic boundary neighbours).
-__global__ void __launch_bounds__(kBlock) k_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
-  const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps || it >= S.iterations) return;
-  const float4 xi4 = V.cur.xs[k];
-  const f3 xi = xyz(xi4);
-  const float li = V.lambda[k];
-  const bool react = F.react_lo != F.react_hi && li != 0.0f;
-  f3 sum = mk(0.0f, 0.0f, 0.0f);
-  const uint32_t cnt = V.ncount[k];
-  const uint32_t n = V.n;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = V.nbr[(size_t)m * n + k];
-    const float4 xj = V.cur.xs[j];
-    const float bvj = V.cur.bv[j];
-    const float mass = neighbor_mass(bvj, xj.w, F.rho0);
-    const f3 g = spiky_grad(xi - xyz(xj), F);
-    sum = sum + g * ((li + V.lambda[j]) * mass);
-    if (react && bvj > 0.0f && xj.w > 0.0f) {
-      const uint32_t idj = V.ids[j];
-      bool in = false;
-      for (uint32_t b = 0; b < F.bnd_count; ++b) {
-        const DevBoundary B = V.bnds[F.bnd_first + b];
-        in = in || (idj >= B.start && idj < B.start + B.count);
-      }
-      if (in) acc_add(V.acc_react, j, g * (-(li / F.rho0) * (F.rho0 * bvj) * xj.w), F.react_scale);
-    }
-  }
-  V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
 }
 
 // positionDelta.ts:217-226, then the reaction accumulator's apply over the
@@ -304,32 +202,7 @@ __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t ra
   if (changed) V.cur.xs[k] = x;
 }
 
-// velocity.ts:43-70 (XSPH part) and 99-120 (apply).
-__global__ void __launch_bounds__(kBlock) k_xsph(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
-  const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank || !F.has_visc) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
-  const f3 xi = xyz(V.cur.x[k]);
-  const f3 vi = xyz(V.cur.v[k]);
-  f3 sm = mk(0.0f, 0.0f, 0.0f);
-  const uint32_t cnt = V.ncount[k];
-  const uint32_t n = V.n;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = V.nbr[(size_t)m * n + k];
-    const f3 off = xi - xyz(V.cur.x[j]);
-    const f3 vj = xyz(V.cur.v[j]);
-    const float bvj = V.cur.bv[j];
-    const float vol = bvj > 0.0f ? bvj : F.volume;
-    sm = sm + ((vj - vi) * poly6(dot(off, off), F)) * vol;
-  }
-  V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
-}
-
+// velocity.ts:99-120: add the XSPH change to the velocity.
 __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -356,7 +229,7 @@ __global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, u
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
-  if (S.prim_count == 0 || sub >= S.substeps || it >= S.iterations) return;
+  if (S.prim_count + S.sdf_count == 0 || sub >= S.substeps || it >= S.iterations) return;
   const float4 xs4 = V.cur.xs[k];
   const float w = xs4.w;
   if (!(w > 0.0f)) return;
@@ -390,6 +263,34 @@ __global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, u
     V.plam[(size_t)k * V.prim_stride + p] = lam;
     any = true;
   }
+  // SDFCollider.ts:256-281: static surface, reach = radius + thickness
+  for (uint32_t q = 0; q < S.sdf_count; ++q) {
+    const DevSdf& G = V.sdfs[S.sdf_base + q];
+    float phi;
+    f3 g;
+    sdf_sample(V.sdf_half, G, xstar, &phi, &g);
+    const float gl = len(g);
+    if (!(gl > 1e-6f)) continue;
+    const float reach = radius + G.thickness;
+    if (!(phi < reach)) continue;
+    const f3 nrm = g / gl;
+    const float depth = reach - phi;
+    const size_t li = (size_t)k * V.prim_stride + S.prim_count + q;
+    float2 lam = V.plam[li];
+    const float ln = lam.x + depth / w;
+    const f3 tang = disp - nrm * dot(disp, nrm);
+    const float tl = len(tang);
+    const bool sticks = tl > 1e-10f && (tl / w <= G.mu_s * ln - lam.y);
+    const f3 push = nrm * depth;
+    const f3 c = sticks ? push - tang : push;
+    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
+    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
+    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
+    lam.x = ln;
+    lam.y = lam.y + (sticks ? tl / w : 0.0f);
+    V.plam[li] = lam;
+    any = true;
+  }
   if (!any) return;
   bool sat = false;
   const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
@@ -404,7 +305,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
-  if (S.prim_count == 0 || sub >= S.substeps) return;
+  if (S.prim_count + S.sdf_count == 0 || sub >= S.substeps) return;
   const float4 xs4 = V.cur.xs[k];
   const float w = xs4.w;
   if (!(w > 0.0f)) return;
@@ -428,6 +329,28 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
     const float vtl = len(vt);
     if (vtl > 1e-6f) {
       const float change = fminf(P.velocity[3] * ln * w / S.dt, vtl);
+      const f3 c = neg((vt / vtl) * change);
+      tx += (uint32_t)to_ticks(c.x, S.vel_scale);
+      ty += (uint32_t)to_ticks(c.y, S.vel_scale);
+      tz += (uint32_t)to_ticks(c.z, S.vel_scale);
+      any = true;
+    }
+  }
+  // SDFCollider.ts:283-299 against a static surface
+  for (uint32_t q = 0; q < S.sdf_count; ++q) {
+    const float ln = V.plam[(size_t)k * V.prim_stride + S.prim_count + q].x;
+    if (!(ln > 0.0f)) continue;
+    const DevSdf& G = V.sdfs[S.sdf_base + q];
+    float phi;
+    f3 g;
+    sdf_sample(V.sdf_half, G, xstar, &phi, &g);
+    const float gl = len(g);
+    if (!(gl > 1e-6f)) continue;
+    const f3 nrm = g / gl;
+    const f3 vt = vel - nrm * dot(nrm, vel);
+    const float vtl = len(vt);
+    if (vtl > 1e-6f) {
+      const float change = fminf(G.mu_k * ln * w / S.dt, vtl);
       const f3 c = neg((vt / vtl) * change);
       tx += (uint32_t)to_ticks(c.x, S.vel_scale);
       ty += (uint32_t)to_ticks(c.y, S.vel_scale);
@@ -768,10 +691,52 @@ __global__ void __launch_bounds__(256) k_global_apply(WorldView V, uint32_t rank
   }
 }
 
+// Positions by particle index for read-back: one thread per id.
+__global__ void __launch_bounds__(kBlock) k_gather_positions(WorldView V, const uint64_t* __restrict__ prefix,
+                                                             float4* __restrict__ out) {
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= V.n) return;
+  const uint32_t s = V.chunk_scene[id >> 8];
+  const DevScene& S = V.scenes[s];
+  const uint32_t local = id - S.seg_start;
+  if (local >= S.cap) return;
+  const float4 x = V.cur.x[V.inv[id]];
+  out[prefix[s] + local] = make_float4(x.x, x.y, x.z, 0.0f);
+}
+
+// Dynamic state of one scene from another world, by particle index, written
+// the way build() writes a spec's state (x* = x, q* = q, zero w lanes).
+__global__ void __launch_bounds__(kBlock) k_import_scene(WorldView V, uint32_t seg, uint32_t cap,
+                                                         const float4* __restrict__ sx, const float4* __restrict__ sv,
+                                                         const float* __restrict__ sbv, const uint32_t* __restrict__ sinv,
+                                                         uint32_t sseg, const float4* __restrict__ sq,
+                                                         const float4* __restrict__ som) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cap) return;
+  const uint32_t from = sinv[sseg + i];
+  const float4 x = sx[from];
+  const float4 v = sv[from];
+  V.cur.x[seg + i] = x;
+  V.cur.xs[seg + i] = x;
+  V.cur.v[seg + i] = make_float4(v.x, v.y, v.z, 0.0f);
+  V.cur.bv[seg + i] = sbv[from];
+  if (V.q) {
+    const float4 q = sq ? sq[sseg + i] : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    const float4 w = som ? som[sseg + i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    V.q[seg + i] = q;
+    V.qp[seg + i] = q;
+    V.omega[seg + i] = make_float4(w.x, w.y, w.z, 0.0f);
+  }
+}
+
+// Kernel launches issued since the counter was last reset (per step).
+thread_local uint64_t t_launches = 0;
+
 template <typename K, typename... A>
 void launch_slots(K kernel, uint32_t n, cudaStream_t st, A... args) {
   if (n == 0) return;
   kernel<<<div_up(n, kBlock), kBlock, 0, st>>>(args...);
+  ++t_launches;
 }
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -789,6 +754,7 @@ World::~World() {
   if (arena_) cudaFree(arena_);
   if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
   if (h_pinned_prims_) cudaFreeHost(h_pinned_prims_);
+  if (h_pinned_sdfs_) cudaFreeHost(h_pinned_sdfs_);
 }
 
 WorldView World::view(uint32_t parity) const {
@@ -819,10 +785,40 @@ struct Carver {
 float f32(double v) { return static_cast<float>(v); }
 }  // namespace
 
-pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
+// Kernel-side view of an SDF collider: R from the unit quaternion (the
+// rotation part of three's Matrix4.makeRotationFromQuaternion, computed in
+// double and rounded to f32 as a mat3 uniform would be), its transpose, and
+// the reciprocals SDFCollider.ts:115-128 precomputes.
+DevSdf make_dev_sdf(const SdfSpec& g, uint32_t data_off) {
+  DevSdf d{};
+  for (int a = 0; a < 3; ++a) {
+    d.res[a] = g.res[a];
+    d.origin[a] = g.origin[a];
+    d.voxel[a] = g.voxel[a];
+    d.inv_voxel[a] = (float)(1.0 / (double)g.voxel[a]);
+    d.position[a] = g.position[a];
+  }
+  d.data_off = data_off;
+  const double x = g.rot_q[0], y = g.rot_q[1], z = g.rot_q[2], w = g.rot_q[3];
+  const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z),     2 * (x * z + w * y),
+                       2 * (x * y + w * z),     1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                       2 * (x * z - w * y),     2 * (y * z + w * x),     1 - 2 * (x * x + y * y)};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      d.rot[3 * r + c] = (float)R[3 * r + c];
+      d.inv_rot[3 * r + c] = (float)R[3 * c + r];
+    }
+  d.scale = g.scale;
+  d.inv_scale = (float)(1.0 / (double)g.scale);
+  d.thickness = g.thickness;
+  d.mu_s = g.mu_s;
+  d.mu_k = g.mu_k;
+  return d;
+}
+
+pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only) {
   specs_ = specs;
   use_graph_ = use_graph;
-  (void)sm_count();  // cache the SM count outside any stream capture
   const uint32_t K = (uint32_t)specs.size();
   if (K == 0) return fail(PF_ERR_INVALID, "SimLoop: no scenes to build");
   // ---- segments, grids, materials -----------------------------------
@@ -833,6 +829,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
   h_softs_.clear();
   h_bodies_.clear();
   h_prims_.clear();
+  h_sdfs_.clear();
+  uint64_t sdf_voxels = 0;
   max_rank_ = max_sub_ = max_iter_ = 0;
   prim_stride_ = 1;
   for (uint32_t s = 0; s < K; ++s) {
@@ -845,6 +843,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     S.substeps = sp.loop.substeps ? sp.loop.substeps : 4;
     S.iterations = sp.loop.iterations;
     S.substeps_f = (float)S.substeps;
+    S.init_pending = sp.initialized ? 0u : 1u;
     S.gx = sp.loop.gravity[0];
     S.gy = sp.loop.gravity[1];
     S.gz = sp.loop.gravity[2];
@@ -875,7 +874,12 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
         mx[a] = sp.loop.grid_max[a];
         auto_bounds = auto_bounds || !(mx[a] > mn[a]);
       }
-      if (auto_bounds) {
+      if (auto_bounds && sp.bounds_resolved) {
+        for (int a = 0; a < 3; ++a) {
+          mn[a] = sp.grid_lo[a];
+          mx[a] = sp.grid_hi[a];
+        }
+      } else if (auto_bounds) {
         for (int a = 0; a < 3; ++a) {
           mn[a] = 1e30;
           mx[a] = -1e30;
@@ -889,6 +893,14 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
           const double ext = std::max(mx[a] - mn[a], 4 * h);
           mn[a] -= 0.5 * ext;
           mx[a] += 0.5 * ext;
+        }
+        if (!plan_only) {
+          SceneSpec& w = *specs[s];
+          w.bounds_resolved = true;
+          for (int a = 0; a < 3; ++a) {
+            w.grid_lo[a] = mn[a];
+            w.grid_hi[a] = mx[a];
+          }
         }
       }
       const double org[3] = {S.ox, S.oy, S.oz};
@@ -913,7 +925,13 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     S.prim_base = (uint32_t)h_prims_.size();
     S.prim_count = (uint32_t)sp.prims.size();
     for (auto& p : sp.prims) h_prims_.push_back(p);
-    prim_stride_ = std::max(prim_stride_, S.prim_count);
+    S.sdf_base = (uint32_t)h_sdfs_.size();
+    S.sdf_count = (uint32_t)sp.sdfs.size();
+    for (auto& g : sp.sdfs) {
+      h_sdfs_.push_back(make_dev_sdf(g, (uint32_t)sdf_voxels));
+      sdf_voxels += g.half.size();
+    }
+    prim_stride_ = std::max(prim_stride_, S.prim_count + S.sdf_count);
     // fluids
     S.fluid_first = (uint32_t)h_fluids_.size();
     S.fluid_count = (uint32_t)sp.fluids.size();
@@ -988,7 +1006,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
       }
     }
     any_grid_ = any_grid_ || S.has_grid;
-    any_prims_ = any_prims_ || S.prim_count > 0;
+    any_prims_ = any_prims_ || S.prim_count > 0 || S.sdf_count > 0;
   }
   if (max_rank_ > 32) return fail(PF_ERR_INVALID, "SimLoop: at most 32 materials per scene");
   n_ = (uint32_t)slot;
@@ -1102,10 +1120,28 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     const DevBoundary& B = h_bnds_[b];
     for (uint32_t i = B.start; i < B.start + B.count; ++i) tag[i] = (tag[i] & 0xffffu) | ((b + 1) << 16);
   }
+  // ---- fluid grid rows and the tile budget ------------------------------
+  std::vector<uint32_t> row_base(1, 0), grid_scene;
+  uint64_t max_tiles = 1;
+  for (uint32_t s = 0; s < K; ++s) {
+    const DevScene& S = h_scenes_[s];
+    if (!S.has_grid || S.fluid_count == 0) continue;
+    grid_scene.push_back(s);
+    row_base.push_back(row_base.back() + S.dims[1] * S.dims[2]);
+    // every tile holds at least one particle and one cell
+    max_tiles += std::min<uint64_t>(S.cells, S.cap);
+  }
+  max_tiles = std::min<uint64_t>(max_tiles, 0xffffffffull);
   // ---- allocate one arena ----------------------------------------------
   const size_t N = n_;
   const size_t P = prim_stride_;
   const bool need_soft = !grp.empty() || !h_bodies_.empty();
+  uint64_t total_real = 0;
+  prefix_.assign(K, 0);
+  for (uint32_t s = 0; s < K; ++s) {
+    prefix_[s] = total_real;
+    total_real += h_scenes_[s].cap;
+  }
   auto layout = [&](Carver& cv) {
     base_.scenes_rw = cv.take<DevScene>(K);
     base_.chunk_scene = cv.take<uint32_t>(chunk.size());
@@ -1114,6 +1150,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     base_.fluids = cv.take<DevFluid>(h_fluids_.size());
     base_.bnds = cv.take<DevBoundary>(h_bnds_.size());
     base_.prims = cv.take<pf_primitive>(h_prims_.size());
+    base_.sdfs = cv.take<DevSdf>(h_sdfs_.size());
+    base_.sdf_half = cv.take<uint16_t>(sdf_voxels);
     for (int b = 0; b < 2; ++b) {
       buf_[b].x = cv.take<float4>(N);
       buf_[b].xs = cv.take<float4>(N);
@@ -1127,8 +1165,13 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     base_.perm = cv.take<uint32_t>(N);
     base_.cstart = cv.take<uint32_t>(cells_);
     base_.ccount = cv.take<uint32_t>(cells_);
-    base_.nbr = any_fluid_ ? cv.take<uint32_t>(N * kMaxNbr) : nullptr;
+    base_.nbr16 = any_fluid_ ? cv.take<uint16_t>(N * kMaxNbr) : nullptr;
     base_.ncount = cv.take<uint32_t>(N);
+    base_.slot_tile = cv.take<uint32_t>(N);
+    base_.tiles = cv.take<Tile>(max_tiles);
+    base_.tile_count = cv.take<uint32_t>(1);
+    base_.row_base = cv.take<uint32_t>(row_base.size());
+    base_.grid_scene = cv.take<uint32_t>(grid_scene.size());
     base_.lambda = cv.take<float>(N);
     base_.density = cv.take<float>(N);
     base_.dx = cv.take<float4>(N);
@@ -1160,11 +1203,15 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
     base_.c_comp = cv.take<float>(ccomp.size());
     base_.c_scene = cv.take<uint32_t>(csc.size());
     base_.c_lambda = cv.take<float>(ci.size());
+    stage_pos_ = cv.take<float4>(total_real);
+    prefix_dev_ = cv.take<uint64_t>(K);
   };
   Carver probe{nullptr};
   layout(probe);
   const size_t sort_bytes = sort_scratch_bytes(n_, cells_);
   bytes_ = probe.off + al256(sort_bytes);
+  if (plan_only) return PF_OK;
+  (void)sm_count();  // cache the SM count outside any stream capture
   if (cudaMalloc(&arena_, bytes_) != cudaSuccess) {
     cudaGetLastError();
     arena_ = nullptr;
@@ -1179,12 +1226,16 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
   base_.n_grp = (uint32_t)grp.size();
   base_.n_bodies = (uint32_t)h_bodies_.size();
   base_.n_cons = (uint32_t)ci.size();
+  base_.max_tiles = (uint32_t)max_tiles;
+  base_.n_grid_scenes = (uint32_t)grid_scene.size();
+  base_.n_rows = row_base.back();
   pair_entries_ = any_soft_local_ ? csr_idx.size() : 0;
   PF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   PF_CUDA(cudaEventCreate(&ev0_));
   PF_CUDA(cudaEventCreate(&ev1_));
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
+  PF_CUDA(cudaMallocHost(&h_pinned_sdfs_, sizeof(DevSdf) * std::max<size_t>(1, h_sdfs_.size())));
   // ---- upload ----------------------------------------------------------
   auto up = [&](const void* dst, const void* src, size_t bytes) -> pf_status {
     if (bytes == 0) return PF_OK;
@@ -1197,6 +1248,15 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
   PF_TRY(up(base_.fluids, h_fluids_.data(), sizeof(DevFluid) * h_fluids_.size()));
   PF_TRY(up(base_.bnds, h_bnds_.data(), sizeof(DevBoundary) * h_bnds_.size()));
   PF_TRY(up(base_.prims, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size()));
+  PF_TRY(up(base_.sdfs, h_sdfs_.data(), sizeof(DevSdf) * h_sdfs_.size()));
+  {
+    uint64_t off = 0;
+    for (uint32_t s = 0; s < K; ++s)
+      for (auto& g : specs[s]->sdfs) {
+        PF_TRY(up(base_.sdf_half + off, g.half.data(), 2 * g.half.size()));
+        off += g.half.size();
+      }
+  }
   PF_TRY(up(buf_[0].x, x.data(), 16 * N));
   PF_TRY(up(buf_[0].xs, x.data(), 16 * N));
   PF_TRY(up(buf_[0].v, v.data(), 16 * N));
@@ -1231,6 +1291,13 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph) {
   PF_TRY(up(base_.c_rest, crest.data(), 4 * crest.size()));
   PF_TRY(up(base_.c_comp, ccomp.data(), 4 * ccomp.size()));
   PF_TRY(up(base_.c_scene, csc.data(), 4 * csc.size()));
+  PF_TRY(up(prefix_dev_, prefix_.data(), 8 * prefix_.size()));
+  PF_TRY(up(base_.row_base, row_base.data(), 4 * row_base.size()));
+  PF_TRY(up(base_.grid_scene, grid_scene.data(), 4 * grid_scene.size()));
+  PF_CUDA(cudaFuncSetAttribute(k_t_neighbors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemNbr));
+  PF_CUDA(cudaFuncSetAttribute(k_t_lambda, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLambda));
+  PF_CUDA(cudaFuncSetAttribute(k_t_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemDelta));
+  PF_CUDA(cudaFuncSetAttribute(k_t_xsph, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemXsph));
   PF_CUDA(cudaStreamSynchronize(stream_));
   parity_ = 0;
   inited_ = true;
@@ -1250,11 +1317,30 @@ pf_status World::set_primitive(uint32_t scene, uint32_t slot, const pf_primitive
   return PF_OK;
 }
 
+pf_status World::set_sdf_transform(uint32_t scene, uint32_t slot, const float pos[3], const double q[4], float scale) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "SDFCollider: no such scene");
+  const DevScene& S = h_scenes_[scene];
+  if (slot >= S.sdf_count) return fail(PF_ERR_INVALID, "SDFCollider: no collider in slot " + std::to_string(slot));
+  SdfSpec& g = specs_[scene]->sdfs[slot];
+  for (int a = 0; a < 3; ++a) g.position[a] = pos[a];
+  for (int a = 0; a < 4; ++a) g.rot_q[a] = q[a];
+  g.scale = scale;
+  h_sdfs_[S.sdf_base + slot] = make_dev_sdf(g, h_sdfs_[S.sdf_base + slot].data_off);
+  sdfs_dirty_ = true;
+  return PF_OK;
+}
+
 pf_status World::upload_params(double dt) {
   const uint32_t K = (uint32_t)h_scenes_.size();
-  for (uint32_t s = 0; s < K; ++s) h_scenes_[s].dt = f32(dt / h_scenes_[s].substeps);
+  for (uint32_t s = 0; s < K; ++s) h_scenes_[s].dt = h_scenes_[s].substeps ? f32(dt / h_scenes_[s].substeps) : 0.0f;
   std::memcpy(h_pinned_scenes_, h_scenes_.data(), sizeof(DevScene) * K);
   PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, h_pinned_scenes_, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
+  if (sdfs_dirty_ && !h_sdfs_.empty()) {
+    std::memcpy(h_pinned_sdfs_, h_sdfs_.data(), sizeof(DevSdf) * h_sdfs_.size());
+    PF_CUDA(cudaMemcpyAsync(const_cast<DevSdf*>(base_.sdfs), h_pinned_sdfs_, sizeof(DevSdf) * h_sdfs_.size(),
+                            cudaMemcpyHostToDevice, stream_));
+    sdfs_dirty_ = false;
+  }
   if (prims_dirty_ && !h_prims_.empty()) {
     std::memcpy(h_pinned_prims_, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size());
     PF_CUDA(cudaMemcpyAsync(const_cast<pf_primitive*>(base_.prims), h_pinned_prims_,
@@ -1267,6 +1353,22 @@ pf_status World::upload_params(double dt) {
 void World::launch_frame_start_at(uint32_t parity) {
   const uint32_t K = (uint32_t)h_scenes_.size();
   k_frame_start<<<div_up(K, 128), 128, 0, stream_>>>(view(parity), K);
+  ++t_launches;
+}
+
+// Cut the fluid scenes' grid rows into tiles and build the neighbour lists.
+void World::launch_tiles_build(const WorldView& V, uint32_t s) {
+  cudaMemsetAsync(base_.tile_count, 0, 4, stream_);
+  launch_slots(k_build_tiles, base_.n_rows, stream_, V, s);
+  launch_tiled(k_t_neighbors, kSmemNbr, V, s);
+}
+
+template <typename K, typename... A>
+void World::launch_tiled(K kernel, size_t smem, const WorldView& V, A... args) {
+  const uint32_t grid = std::max<uint32_t>(
+      1, std::min<uint32_t>(div_up(base_.max_tiles, kTileWarps), (uint32_t)sm_count() * 16));
+  kernel<<<grid, kTileThreads, smem, stream_>>>(V, args...);
+  ++t_launches;
 }
 
 // Keys of the current predicted positions, stable sort, permute into the
@@ -1277,6 +1379,7 @@ void World::run_sort_and_permute(uint32_t parity, bool) {
   cudaMemsetAsync(sort_.counters, 0, 4ull * kNumCounters, stream_);
   launch_slots(k_keys, n_, stream_, V);
   launch_sort_from_hist(V.keys, n_, cells_, V.ccount, V.cstart, V.perm, sort_, stream_);
+  t_launches += 5;  // scan, scatter and the three fix-up tiers
   launch_slots(k_permute, n_, stream_, V);
 }
 
@@ -1301,7 +1404,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   }
   // preSolve
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
-  if (any_fluid_) launch_slots(k_neighbors, n_, stream_, V, s);
+  if (any_fluid_) launch_tiles_build(V, s);
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
   if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
@@ -1316,8 +1419,8 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         has_global = has_global || (D.rank == r && !D.local);
       }
       if (has_fluid) {
-        launch_slots(k_lambda, n_, stream_, V, r, s, it);
-        launch_slots(k_delta, n_, stream_, V, r, s, it);
+        launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
+        launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
         launch_slots(k_fluid_apply, n_, stream_, V, r, s, it);
       }
       if (has_local) {
@@ -1330,11 +1433,15 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (has_global && base_.n_bodies) {
         k_body_frame<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it, 1u);
         k_global_apply<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it);
+        t_launches += 2;
       }
       if (r < cloth_ranges_.size())
         for (auto& rg : cloth_ranges_[r])
           if (rg.second > rg.first)
+          {
             k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, stream_>>>(V, rg.first, rg.second, s, it);
+            ++t_launches;
+          }
     }
     if (any_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
   }
@@ -1344,18 +1451,22 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     for (auto& F : h_fluids_) has_visc = has_visc || (F.rank == r && F.has_visc);
     for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
     if (has_visc) {
-      launch_slots(k_xsph, n_, stream_, V, r, s);
+      launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
       launch_slots(k_xsph_apply, n_, stream_, V, r, s);
     }
     if (has_local) {
       launch_slots(k_rot_advect, base_.n_grp, stream_, V, s);
-      if (base_.n_bodies) k_body_frame<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, 0u, 0u);
+      if (base_.n_bodies) {
+        k_body_frame<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, 0u, 0u);
+        ++t_launches;
+      }
     }
   }
   if (any_prims_) {
     launch_slots(k_friction, n_, stream_, V, s);
     const uint32_t K = (uint32_t)h_scenes_.size();
     k_tick<<<div_up(K, 128), 128, 0, stream_>>>(V, K, s);
+    ++t_launches;
   }
 }
 
@@ -1368,9 +1479,11 @@ pf_status World::step(double dt) {
     run_init_pass();
     inited_ = true;
     for (auto* sp : specs_) sp->initialized = true;
+    for (auto& S : h_scenes_) S.init_pending = 0;
   }
   const uint32_t flips = any_grid_ ? (max_sub_ & 1u) : 0u;
   auto body = [&](uint32_t p0) {
+    t_launches = 0;
     launch_frame_start_at(p0);
     uint32_t p = p0;
     for (uint32_t s = 0; s < max_sub_; ++s) {
@@ -1384,6 +1497,7 @@ pf_status World::step(double dt) {
       cudaGraph_t graph;
       PF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       body(parity_);
+      launches_per_step_ = t_launches;
       PF_CUDA(cudaStreamEndCapture(stream_, &graph));
       const cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
       cudaGraphDestroy(graph);
@@ -1392,6 +1506,7 @@ pf_status World::step(double dt) {
     PF_CUDA(cudaGraphLaunch(g, stream_));
   } else {
     body(parity_);
+    launches_per_step_ = t_launches;
   }
   parity_ ^= flips;
   PF_CUDA(cudaEventRecord(ev1_, stream_));
@@ -1493,15 +1608,27 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
         return PF_OK;
       }
       std::fill(o, o + (size_t)cap * kMaxNbr, 0xffffffffu);
-      if (!base_.nbr) return PF_OK;
-      std::vector<uint32_t> col(seg), all_ids(n_);
+      if (!base_.nbr16) return PF_OK;
+      uint32_t nt = 0;
+      PF_CUDA(cudaMemcpy(&nt, base_.tile_count, 4, cudaMemcpyDeviceToHost));
+      nt = std::min(nt, base_.max_tiles);
+      std::vector<Tile> tiles(nt);
+      PF_CUDA(cudaMemcpy(tiles.data(), base_.tiles, sizeof(Tile) * nt, cudaMemcpyDeviceToHost));
+      std::vector<uint32_t> st(seg), all_ids(n_);
+      std::vector<uint16_t> col(seg);
+      PF_CUDA(cudaMemcpy(st.data(), base_.slot_tile + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
       PF_CUDA(cudaMemcpy(all_ids.data(), base_.ids, 4ull * n_, cudaMemcpyDeviceToHost));
       for (uint32_t m = 0; m < kMaxNbr; ++m) {
-        PF_CUDA(cudaMemcpy(col.data(), base_.nbr + (size_t)m * n_ + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+        PF_CUDA(cudaMemcpy(col.data(), base_.nbr16 + (size_t)m * n_ + S.seg_start, 2ull * seg, cudaMemcpyDeviceToHost));
         for (uint32_t k = 0; k < seg; ++k) {
           const uint32_t id = ids[k] - S.seg_start;
-          if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k]) continue;
-          o[(size_t)id * kMaxNbr + m] = all_ids[col[k]] - S.seg_start;
+          if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k] || st[k] >= nt) continue;
+          const Tile& T = tiles[st[k]];
+          const uint32_t h = col[k];
+          int r = 0;
+          while (r < 8 && h >= T.roff[r + 1]) ++r;
+          const uint32_t j = T.rs[r] + (h - T.roff[r]);
+          o[(size_t)id * kMaxNbr + m] = all_ids[j] - S.seg_start;
         }
       }
       return PF_OK;
@@ -1509,6 +1636,26 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
     default:
       return fail(PF_ERR_INVALID, "readback: unknown field " + std::to_string(field));
   }
+}
+
+pf_status World::import_scene(uint32_t s, const World& src, uint32_t src_s) {
+  if (s >= h_scenes_.size() || src_s >= src.h_scenes_.size()) return fail(PF_ERR_INVALID, "import: no such scene");
+  const DevScene& S = h_scenes_[s];
+  const DevScene& T = src.h_scenes_[src_s];
+  if (S.cap != T.cap) return fail(PF_ERR_INVALID, "import: scenes differ in capacity");
+  if (S.cap == 0) return PF_OK;
+  const StateBuf& B = src.buf_[src.parity_];
+  const WorldView V = view(parity_);
+  k_import_scene<<<div_up(S.cap, kBlock), kBlock, 0, stream_>>>(V, S.seg_start, S.cap, B.x, B.v, B.bv, src.base_.inv,
+                                                                 T.seg_start, src.base_.q, src.base_.omega);
+  PF_CUDA(cudaGetLastError());
+  return PF_OK;
+}
+
+void World::retire(uint32_t s) {
+  if (s >= h_scenes_.size()) return;
+  h_scenes_[s].substeps = 0;
+  h_scenes_[s].iterations = 0;
 }
 
 pf_status World::pull_state(uint32_t scene, SceneSpec* sp) {
@@ -1555,6 +1702,49 @@ pf_status World::elapsed_ms(float* ms) {
   PF_CUDA(cudaEventSynchronize(ev1_));
   PF_CUDA(cudaEventElapsedTime(ms, ev0_, ev1_));
   last_ms_ = *ms;
+  return PF_OK;
+}
+
+uint64_t World::total_particles() const {
+  uint64_t t = 0;
+  for (auto& S : h_scenes_) t += S.cap;
+  return t;
+}
+
+pf_status World::read_positions(float* dst, size_t bytes) {
+  const uint64_t total = total_particles();
+  if (bytes < 16ull * total) return fail(PF_ERR_INVALID, "readback: destination too small");
+  launch_slots(k_gather_positions, n_, stream_, view(parity_), (const uint64_t*)prefix_dev_, stage_pos_);
+  PF_CUDA(cudaMemcpyAsync(dst, stage_pos_, 16ull * total, cudaMemcpyDeviceToHost, stream_));
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  return PF_OK;
+}
+
+pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_t* items) {
+  const WorldView V = view(parity_);
+  uint64_t fluid = 0;
+  for (uint32_t s = 0; s < specs_.size(); ++s)
+    for (auto& f : specs_[s]->fluids) fluid += f.range.count;
+  auto run = [&]() {
+    switch (stage) {
+      case 0: launch_tiled(k_t_neighbors, kSmemNbr, V, 0u); break;
+      case 1: launch_tiled(k_t_lambda, kSmemLambda, V, 0u, 0u, 0u); break;
+      case 2: launch_tiled(k_t_delta, kSmemDelta, V, 0u, 0u, 0u); break;
+      case 3: launch_tiled(k_t_xsph, kSmemXsph, V, 0u, 0u); break;
+      case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
+      default: break;
+    }
+  };
+  if (stage > 4) return fail(PF_ERR_INVALID, "profile: unknown stage");
+  if (items) *items = stage == 4 ? total_particles() : fluid;
+  run();
+  PF_CUDA(cudaEventRecord(ev0_, stream_));
+  for (uint32_t r = 0; r < reps; ++r) run();
+  PF_CUDA(cudaEventRecord(ev1_, stream_));
+  PF_CUDA(cudaEventSynchronize(ev1_));
+  float t = 0;
+  PF_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
+  *ms = t / (float)std::max(reps, 1u);
   return PF_OK;
 }
 

@@ -73,6 +73,16 @@ struct ClothSpec {
   std::vector<std::vector<uint32_t>> colors;  // constraint indices per colour
 };
 
+// SDFCollider state (SDFCollider.ts:88-137): the grid as half floats plus
+// the transform and contact parameters.
+struct SdfSpec {
+  uint32_t res[3] = {0, 0, 0};
+  std::vector<uint16_t> half;  // res[0] * res[1] * res[2], x fastest
+  float origin[3], voxel[3], position[3];
+  double rot_q[4];             // unit quaternion (x, y, z, w)
+  float scale, thickness, mu_s, mu_k;
+};
+
 enum MatKind : uint32_t { MAT_FLUID = 0, MAT_SOFT = 1, MAT_CLOTH = 2 };
 
 struct SceneSpec {
@@ -86,9 +96,14 @@ struct SceneSpec {
   std::vector<SoftSpec> softs;
   std::vector<ClothSpec> cloths;
   std::vector<pf_primitive> prims;
+  std::vector<SdfSpec> sdfs;
   pf_loop_desc loop{};
   bool built = false;
   bool initialized = false;  // the one-time init pass (static boundaries) ran
+  // Grid bounds resolved from the initial positions at the first build; a
+  // scene rebuilt later (into a batch or a serving cohort) keeps its grid.
+  bool bounds_resolved = false;
+  double grid_lo[3] = {0, 0, 0}, grid_hi[3] = {0, 0, 0};
 };
 
 // ----------------------------------------------------------- device data ----
@@ -109,6 +124,18 @@ struct DevScene {
   float sb_scale, sb_inv;
   uint32_t fluid_first, fluid_count;  // this scene's fluids in the fluid table
   uint32_t soft_local_ranks;          // bit r: a local shape-matching system at material rank r
+  uint32_t init_pending;              // the one-time init pass has not run for this scene
+  uint32_t sdf_base, sdf_count;       // this scene's SDF colliders in the SDF table
+};
+
+// One SDF collider as the kernels read it (sdf.ts:17-80 fields).
+struct DevSdf {
+  uint32_t res[3];
+  uint32_t data_off;  // first voxel in the half-float pool
+  float origin[3], inv_voxel[3], voxel[3];
+  float position[3];
+  float rot[9], inv_rot[9];  // row-major R and R^T
+  float scale, inv_scale, thickness, mu_s, mu_k;
 };
 
 struct DevFluid {
@@ -154,6 +181,16 @@ enum FlagIdx : uint32_t {
 __host__ __device__ inline uint32_t tag_fluid(uint32_t t) { return t & 0xffffu; }
 __host__ __device__ inline uint32_t tag_bnd(uint32_t t) { return t >> 16; }
 
+// A tile of the fluid neighbour passes: own particles [p0, p1) of one grid
+// row segment, and its halo (the nine neighbouring row segments) as slot
+// ranges rs[r] .. rs[r] + (roff[r + 1] - roff[r]), concatenated in (dz, dy)
+// order starting at halo index roff[r].
+struct Tile {
+  uint32_t scene, p0, p1, halo;
+  uint32_t rs[9];
+  uint32_t roff[10];
+};
+
 struct StateBuf {
   float4* x = nullptr;   // committed positions, w = inverse mass
   float4* xs = nullptr;  // predicted positions, w = inverse mass
@@ -165,7 +202,7 @@ struct StateBuf {
 // Everything a stage kernel needs, passed by value.
 struct WorldView {
   uint32_t n;            // total slots
-  uint32_t prim_stride;  // primitives per slot in the collider lambda array
+  uint32_t prim_stride;  // colliders (primitives + SDFs) per slot in the collider lambda array
   const DevScene* scenes;
   const uint32_t* chunk_scene;  // scene of each 256-slot chunk
   DevScene* scenes_rw;
@@ -174,6 +211,8 @@ struct WorldView {
   const DevFluid* fluids;
   const DevBoundary* bnds;
   const pf_primitive* prims;
+  const DevSdf* sdfs;
+  const uint16_t* sdf_half;  // half-float voxels of every SDF collider
   StateBuf cur, nxt;
   uint32_t* ids;
   uint32_t* inv;
@@ -181,8 +220,16 @@ struct WorldView {
   uint32_t* perm;     // new slot -> id (sort output)
   uint32_t* cstart;
   uint32_t* ccount;
-  uint32_t* nbr;      // kMaxNbr * n, column-major
+  uint16_t* nbr16;    // kMaxNbr * n, column-major: halo index of each neighbour
   uint32_t* ncount;
+  uint32_t* slot_tile;  // tile of each slot (this substep)
+  Tile* tiles;
+  uint32_t* tile_count;
+  uint32_t max_tiles;
+  const uint32_t* row_base;    // first global grid row of each fluid scene (n_grid_scenes + 1)
+  const uint32_t* grid_scene;  // scene of each fluid scene index
+  uint32_t n_grid_scenes;
+  uint32_t n_rows;
   float* lambda;
   float* density;
   float4* dx;
@@ -228,10 +275,21 @@ class World {
   World(const World&) = delete;
   World& operator=(const World&) = delete;
 
-  // Pack `specs` (their current host state) into device arrays.
-  pf_status build(const std::vector<SceneSpec*>& specs, bool use_graph);
+  // Pack `specs` (their current host state) into device arrays. With
+  // `plan_only` nothing touches the GPU: the layout is computed and
+  // device_bytes() reports what the build would allocate.
+  pf_status build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only = false);
+  // Overwrite scene `s`'s dynamic state (positions with inverse mass,
+  // velocities, boundary volumes, orientations, angular velocities) with
+  // scene `src_s` of `src`, device to device. Both worlds hold the same
+  // scene spec; `src` must be idle.
+  pf_status import_scene(uint32_t s, const World& src, uint32_t src_s);
+  // Stop stepping scene `s` (its slots keep their last state).
+  void retire(uint32_t s);
+  bool retired(uint32_t s) const { return h_scenes_[s].substeps == 0; }
   pf_status step(double dt);
   pf_status set_primitive(uint32_t scene, uint32_t slot, const pf_primitive& p);
+  pf_status set_sdf_transform(uint32_t scene, uint32_t slot, const float pos[3], const double q[4], float scale);
   pf_status readback(uint32_t scene, uint32_t field, void* dst, size_t bytes);
   // Copies the scene's state (by particle index) back into its spec.
   pf_status pull_state(uint32_t scene, SceneSpec* spec);
@@ -241,6 +299,15 @@ class World {
   cudaStream_t stream() const { return stream_; }
   uint32_t scene_count() const { return (uint32_t)specs_.size(); }
   uint64_t particle_substeps_per_step() const;
+  // Positions of every scene, each in particle order, w = 0, concatenated in
+  // scene order, into host memory (one gather kernel + one copy).
+  pf_status read_positions(float* dst_host, size_t bytes);
+  uint64_t total_particles() const;
+  uint64_t launches_per_step() const { return launches_per_step_; }
+  size_t step_upload_bytes() const { return sizeof(DevScene) * h_scenes_.size(); }
+  // Average device milliseconds of one solver stage run `reps` times on the
+  // current state (substep 0, iteration 0, material rank 0).
+  pf_status profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_t* items);
   size_t device_bytes() const { return bytes_; }
 
  private:
@@ -248,6 +315,9 @@ class World {
   void run_substep(uint32_t s, uint32_t parity);
   void run_sort_and_permute(uint32_t parity, bool committed);
   void run_init_pass();
+  void launch_tiles_build(const WorldView& V, uint32_t s);
+  template <typename K, typename... A>
+  void launch_tiled(K kernel, size_t smem, const WorldView& V, A... args);
   void launch_frame_start_at(uint32_t parity);
   pf_status upload_params(double dt);
   WorldView view(uint32_t parity) const;
@@ -259,6 +329,8 @@ class World {
   std::vector<DevSoft> h_softs_;
   std::vector<DevBody> h_bodies_;
   std::vector<pf_primitive> h_prims_;
+  std::vector<DevSdf> h_sdfs_;
+  bool sdfs_dirty_ = false;
   // stage plan
   uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
@@ -284,8 +356,13 @@ class World {
   // pinned staging for per-step parameters
   DevScene* h_pinned_scenes_ = nullptr;
   pf_primitive* h_pinned_prims_ = nullptr;
+  DevSdf* h_pinned_sdfs_ = nullptr;
   bool prims_dirty_ = true;
   size_t pair_entries_ = 0;
+  float4* stage_pos_ = nullptr;  // gather buffer of read_positions
+  uint64_t* prefix_dev_ = nullptr;
+  uint64_t launches_per_step_ = 0;
+  std::vector<uint64_t> prefix_;   // particle offset of each scene in read_positions
 };
 
 }  // namespace pf

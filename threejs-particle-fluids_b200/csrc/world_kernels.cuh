@@ -3,6 +3,7 @@
 // decomposition and the 27-cell stencil walk over the sorted slots.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -61,6 +62,32 @@ __device__ __forceinline__ f3 spiky_grad(f3 r, const DevFluid& F) {
 __device__ __forceinline__ float neighbor_mass(float bv, float w, float rho0) {
   return bv > 0.0f ? rho0 * bv : (w > 0.0f ? 1.0f / w : 0.0f);
 }
+
+// The same quantities in the form the per-neighbour loops use: one
+// reciprocal square root instead of a square root and three divisions, and
+// an approximate reciprocal for the particle mass. Within the solver's
+// tolerance of the exactly rounded forms above.
+__device__ __forceinline__ float neighbor_mass_fast(float bv, float w, float rho0) {
+  return bv > 0.0f ? rho0 * bv : (w > 0.0f ? __fdividef(1.0f, w) : 0.0f);
+}
+// -45/(pi h^6) (h - r)^2 / r, the factor that turns r_vec into the Spiky
+// gradient; zero at r = 0 (rsqrt of the floored square stays finite).
+__device__ __forceinline__ float spiky_factor(float rsq, const DevFluid& F) {
+  const float inv_r = rsqrtf(fmaxf(rsq, 1e-40f));
+  const float t = fmaxf(F.h - rsq * inv_r, 0.0f);
+  return -(t * t * F.spiky) * inv_r;
+}
+
+// The forms the neighbour loops call. A build with PF_EXACT_ROUNDING (and
+// -fmad=false) uses the exactly rounded reference forms instead; it is a
+// diagnostic build that reproduces the oracle's FP32 arithmetic bit for bit.
+#ifdef PF_EXACT_ROUNDING
+__device__ __forceinline__ float nbr_mass(float bv, float w, float rho0) { return neighbor_mass(bv, w, rho0); }
+__device__ __forceinline__ f3 spiky_vec(f3 off, float, const DevFluid& F) { return spiky_grad(off, F); }
+#else
+__device__ __forceinline__ float nbr_mass(float bv, float w, float rho0) { return neighbor_mass_fast(bv, w, rho0); }
+__device__ __forceinline__ f3 spiky_vec(f3 off, float rsq, const DevFluid& F) { return off * spiky_factor(rsq, F); }
+#endif
 
 // ------------------------------------------------- fixed-point accumulation ----
 // accumulator.ts:108-115: round(v * scale) with ties to even, saturating.
@@ -151,11 +178,18 @@ __device__ __forceinline__ void prim_sdf(const pf_primitive& p, f3 xw, float rew
   const f3 spin = mk(p.spin[0], p.spin[1], p.spin[2]);
   const float rate = len(spin);
   const float half = rate * t * 0.5f;
-  const f3 axis = spin / fmaxf(rate, 1e-8f);
-  float sh, ch;
-  sincosf(half, &sh, &ch);
-  const float4 turn = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, ch);
-  const f3 x = pivot + qrot(turn, shifted - pivot);
+  float4 turn = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  f3 x;
+  if (half != 0.0f) {
+    const f3 axis = spin / fmaxf(rate, 1e-8f);
+    float sh, ch;
+    sincosf(half, &sh, &ch);
+    turn = make_float4(axis.x * sh, axis.y * sh, axis.z * sh, ch);
+    x = pivot + qrot(turn, shifted - pivot);
+  } else {
+    // rotating by the identity quaternion returns its argument exactly
+    x = pivot + (shifted - pivot);
+  }
   const float4 unturn = make_float4(-turn.x, -turn.y, -turn.z, turn.w);
   const f3 d0 = mk(p.data0[0], p.data0[1], p.data0[2]);
   const f3 d1 = mk(p.data1[0], p.data1[1], p.data1[2]);
@@ -201,7 +235,7 @@ __device__ __forceinline__ void prim_sdf(const pf_primitive& p, f3 xw, float rew
     g = neg(g);
   }
   *phi_out = phi;
-  *grad_out = qrot(unturn, g);
+  *grad_out = half != 0.0f ? qrot(unturn, g) : g;
 }
 
 // primitives.ts:342-360
@@ -223,6 +257,53 @@ __device__ __forceinline__ void jacobi_coeffs(float app, float aqq, float apq, f
   *t = sg / (ta + sqrtf(ta * ta + 1.0f));
   *c = 1.0f / sqrtf(*t * *t + 1.0f);
   *s = *t * *c;
+}
+
+// sample.ts:12-53 trilinear filter at continuous grid coordinate g (voxel
+// (i, j, k) centred at g = (i + 0.5, j + 0.5, k + 0.5)), clamp to edge.
+__device__ __forceinline__ float sdf_trilinear(const uint16_t* __restrict__ d, const DevSdf& G, float gx, float gy,
+                                               float gz) {
+  gx -= 0.5f;
+  gy -= 0.5f;
+  gz -= 0.5f;
+  const int nx = (int)G.res[0], ny = (int)G.res[1], nz = (int)G.res[2];
+  const int i0 = min(max((int)floorf(gx), 0), nx - 2);
+  const int j0 = min(max((int)floorf(gy), 0), ny - 2);
+  const int k0 = min(max((int)floorf(gz), 0), nz - 2);
+  const float tx = fminf(fmaxf(gx - (float)i0, 0.0f), 1.0f);
+  const float ty = fminf(fmaxf(gy - (float)j0, 0.0f), 1.0f);
+  const float tz = fminf(fmaxf(gz - (float)k0, 0.0f), 1.0f);
+  const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+  const uint16_t* b = d + G.data_off + (size_t)i0 + j0 * sy + k0 * sz;
+  auto h = [](uint16_t v) { return __half2float(__ushort_as_half(v)); };
+  auto lerp = [](float a, float c, float t) { return a + (c - a) * t; };
+  const float c00 = lerp(h(__ldg(b)), h(__ldg(b + 1)), tx);
+  const float c10 = lerp(h(__ldg(b + sy)), h(__ldg(b + sy + 1)), tx);
+  const float c01 = lerp(h(__ldg(b + sz)), h(__ldg(b + sz + 1)), tx);
+  const float c11 = lerp(h(__ldg(b + sz + sy)), h(__ldg(b + sz + sy + 1)), tx);
+  return lerp(lerp(c00, c10, ty), lerp(c01, c11, ty), tz);
+}
+
+// sdf.ts:107-147 (emitSampleSdf): world -> local frame, phi by the trilinear
+// filter, the gradient by central differences one voxel apart, back to world.
+__device__ __forceinline__ void sdf_sample(const uint16_t* __restrict__ d, const DevSdf& G, f3 x, float* phi,
+                                           f3* grad) {
+  const f3 off = mk(x.x - G.position[0], x.y - G.position[1], x.z - G.position[2]);
+  const float* I = G.inv_rot;
+  const f3 xl = mk(I[0] * off.x + I[1] * off.y + I[2] * off.z, I[3] * off.x + I[4] * off.y + I[5] * off.z,
+                   I[6] * off.x + I[7] * off.y + I[8] * off.z) *
+                G.inv_scale;
+  const float gx = (xl.x - G.origin[0]) * G.inv_voxel[0];
+  const float gy = (xl.y - G.origin[1]) * G.inv_voxel[1];
+  const float gz = (xl.z - G.origin[2]) * G.inv_voxel[2];
+  const float p0 = sdf_trilinear(d, G, gx, gy, gz);
+  const f3 gl = mk((sdf_trilinear(d, G, gx + 1.0f, gy, gz) - sdf_trilinear(d, G, gx - 1.0f, gy, gz)) / (2.0f * G.voxel[0]),
+                   (sdf_trilinear(d, G, gx, gy + 1.0f, gz) - sdf_trilinear(d, G, gx, gy - 1.0f, gz)) / (2.0f * G.voxel[1]),
+                   (sdf_trilinear(d, G, gx, gy, gz + 1.0f) - sdf_trilinear(d, G, gx, gy, gz - 1.0f)) / (2.0f * G.voxel[2]));
+  const float* R = G.rot;
+  *phi = p0 * G.scale;
+  *grad = mk(R[0] * gl.x + R[1] * gl.y + R[2] * gl.z, R[3] * gl.x + R[4] * gl.y + R[5] * gl.z,
+             R[6] * gl.x + R[7] * gl.y + R[8] * gl.z);
 }
 
 __device__ __forceinline__ void polar3(const float a[9], float r[9]) {

@@ -134,6 +134,21 @@ class Primitive(C.Structure):
     ]
 
 
+class SdfDesc(C.Structure):
+    _fields_ = [
+        ("res", C.c_uint32 * 3),
+        ("data", C.POINTER(C.c_float)),
+        ("origin", C.c_float * 3),
+        ("voxel_size", C.c_float * 3),
+        ("position", C.c_float * 3),
+        ("rotation", C.c_float * 4),
+        ("scale", C.c_float),
+        ("thickness", C.c_float),
+        ("mu_s", C.c_float),
+        ("mu_k", C.c_float),
+    ]
+
+
 class LoopDesc(C.Structure):
     _fields_ = [
         ("substeps", C.c_uint32),
@@ -161,17 +176,37 @@ class BatchOpts(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_scenes", C.c_uint32), ("use_graph", C.c_uint32)]
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64),
+        ("max_scenes", C.c_uint32),
+        ("use_graph", C.c_uint32),
+        ("max_cohorts", C.c_uint32),
+        ("mode", C.c_uint32),
+        ("async_build", C.c_uint32),
+    ]
+
+
+PF_SERVER_BATCHED, PF_SERVER_PLAIN = 0, 1
+PF_REQ_QUEUED, PF_REQ_BUILDING, PF_REQ_LIVE, PF_REQ_DONE = 0, 1, 2, 3
 
 
 class ServerStats(C.Structure):
     _fields_ = [
         ("live", C.c_uint32),
         ("queued", C.c_uint32),
+        ("building", C.c_uint32),
+        ("finished", C.c_uint32),
+        ("cohorts", C.c_uint32),
+        ("reserved0", C.c_uint32),
         ("ticks", C.c_uint64),
         ("particle_substeps", C.c_uint64),
         ("state_bytes", C.c_uint64),
+        ("rebuilds", C.c_uint64),
+        ("busy_ms", C.c_double),
         ("last_tick_ms", C.c_float),
+        ("p50_tick_ms", C.c_float),
+        ("p99_tick_ms", C.c_float),
+        ("max_tick_ms", C.c_float),
     ]
 
 
@@ -203,6 +238,17 @@ SIGNATURES = {
     "pf_overflow_read": (C.c_int, [_P, C.POINTER(Overflow)]),
     "pf_last_step_ms": (C.c_int, [_P, _f32p]),
     "pf_batch_create": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(BatchOpts), C.POINTER(_P)]),
+    "pf_add_sdf_collider": (C.c_int, [_P, C.POINTER(SdfDesc), _u32p]),
+    "pf_set_sdf_transform": (C.c_int, [_P, C.c_uint32, _f32p, _f32p, C.c_float]),
+    "pf_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(_P)]),
+    "pf_server_destroy": (None, [_P]),
+    "pf_server_submit": (C.c_int, [_P, _P, C.POINTER(LoopDesc), C.c_uint32, C.POINTER(C.c_uint64)]),
+    "pf_server_tick": (C.c_int, [_P, C.c_double]),
+    "pf_server_drain_build": (C.c_int, [_P]),
+    "pf_server_request_state": (C.c_int, [_P, C.c_uint64, _u32p, _u32p]),
+    "pf_server_readback": (C.c_int, [_P, C.c_uint64, C.c_uint32, _P, C.c_size_t]),
+    "pf_server_estimate_bytes": (C.c_int, [_P, C.POINTER(LoopDesc), C.POINTER(C.c_uint64)]),
+    "pf_server_stats_read": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "pf_batch_destroy": (None, [_P]),
     "pf_batch_step": (C.c_int, [_P, C.c_double]),
     "pf_batch_set_primitive": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(Primitive)]),
@@ -210,6 +256,12 @@ SIGNATURES = {
     "pf_batch_overflow_read": (C.c_int, [_P, C.c_uint32, C.POINTER(Overflow)]),
     "pf_batch_last_step_ms": (C.c_int, [_P, _f32p]),
     "pf_batch_particle_substeps": (C.c_uint64, [_P]),
+    "pf_batch_stream": (_P, [_P]),
+    "pf_batch_launches_per_step": (C.c_uint64, [_P]),
+    "pf_batch_step_upload_bytes": (C.c_uint64, [_P]),
+    "pf_scene_stream": (_P, [_P]),
+    "pf_batch_read_positions": (C.c_int, [_P, _f32p, C.c_size_t]),
+    "pf_batch_profile_stage": (C.c_int, [_P, C.c_uint32, C.c_uint32, _f32p, C.POINTER(C.c_uint64)]),
 }
 
 _lib: C.CDLL | None = None

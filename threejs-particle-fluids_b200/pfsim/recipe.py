@@ -94,6 +94,48 @@ class Prim:
         return p
 
 
+@dataclass
+class Sdf:
+    """SDFData + SDFColliderOptions (src/core/collision/SDFCollider.ts:32-58)."""
+
+    data: np.ndarray  # (nz, ny, nx) float32 distances, x fastest in memory
+    origin: tuple
+    voxel_size: tuple
+    position: tuple = (0.0, 0.0, 0.0)
+    rotation: tuple = (0.0, 0.0, 0.0, 1.0)
+    scale: float = 1.0
+    thickness: float = 0.0
+    mu_s: float = 0.5
+    mu_k: float = 0.4
+
+    def cstruct(self, keep) -> N.SdfDesc:
+        d = N.SdfDesc()
+        arr = np.ascontiguousarray(self.data, np.float32)
+        nz, ny, nx = arr.shape
+        d.res[:] = [nx, ny, nz]
+        d.data = keep.f32(arr.reshape(-1))
+        d.origin[:] = [float(v) for v in self.origin]
+        d.voxel_size[:] = [float(v) for v in self.voxel_size]
+        d.position[:] = [float(v) for v in self.position]
+        d.rotation[:] = [float(v) for v in self.rotation]
+        d.scale, d.thickness, d.mu_s, d.mu_k = float(self.scale), float(self.thickness), float(self.mu_s), float(self.mu_k)
+        return d
+
+
+def sphere_sdf(center, radius, res: int = 32, pad: float = 0.25, invert: bool = False, **kw) -> Sdf:
+    """A baked sphere: distances at voxel centres of a res^3 grid around it
+    (negated for a bowl that holds particles inside)."""
+    c = np.asarray(center, np.float64)
+    ext = radius * (1.0 + pad)
+    vs = 2.0 * ext / res
+    idx = (np.arange(res) + 0.5) * vs - ext
+    z, y, x = np.meshgrid(idx, idx, idx, indexing="ij")
+    d = np.sqrt(x * x + y * y + z * z) - radius
+    if invert:
+        d = -d
+    return Sdf(d.astype(np.float32), tuple(c - ext), (vs, vs, vs), **kw)
+
+
 def plane(normal, point, mu_s: float = 0.5, mu_k: float = 0.4) -> Prim:
     """PrimitiveSet.addPlane (PrimitiveSet.ts:166-170): the normal is normalised."""
     n = np.asarray(normal, np.float64)
@@ -148,6 +190,7 @@ class Recipe:
     uploads: list[Upload] = field(default_factory=list)
     materials: list[tuple[str, Any]] = field(default_factory=list)
     prims: list[Prim] = field(default_factory=list)
+    sdfs: list[Sdf] = field(default_factory=list)
     loop: LoopOpts = field(default_factory=LoopOpts)
     name: str = ""
     # optional per-step primitive motion: fn(step_index, dt) -> {slot: Prim}
@@ -327,7 +370,7 @@ class NativeBackend:
 
     name = "cuda"
 
-    def build(self, r: Recipe) -> Scene:
+    def build(self, r: Recipe, build_loop: bool = True) -> Scene:
         L = N.lib()
         desc = N.SceneDesc(r.capacity, r.radius)
         h = C.c_void_p()
@@ -351,8 +394,11 @@ class NativeBackend:
         for p in r.prims:
             cs = p.cstruct()
             N.check(L.pf_add_primitive(h, C.byref(cs), None))
-        ld = loop_desc(r.loop)
-        N.check(L.pf_loop_build(h, C.byref(ld)))
+        for g in r.sdfs:
+            N.check(L.pf_add_sdf_collider(h, C.byref(g.cstruct(keep)), None))
+        if build_loop:
+            ld = loop_desc(r.loop)
+            N.check(L.pf_loop_build(h, C.byref(ld)))
         return scene
 
 
@@ -402,6 +448,74 @@ class Batch:
     def close(self) -> None:
         if self.h:
             N.lib().pf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous batching (pf_server): scenes are admitted in FIFO order as
+    the HBM budget allows, every live scene is stepped once per tick, and a
+    scene retires after its lifetime. Primitive motion callbacks of recipes
+    are not applied to served scenes."""
+
+    def __init__(self, budget_bytes: int = 0, max_scenes: int = 0, use_graph: bool = True, max_cohorts: int = 0,
+                 plain: bool = False, async_build: bool = True):
+        opts = N.ServerOpts(int(budget_bytes), int(max_scenes), 1 if use_graph else 0, int(max_cohorts),
+                            N.PF_SERVER_PLAIN if plain else N.PF_SERVER_BATCHED, 1 if async_build else 0)
+        h = C.c_void_p()
+        N.check(N.lib().pf_server_create(C.byref(opts), C.byref(h)))
+        self.h = h
+        self.capacity: dict[int, int] = {}
+
+    @staticmethod
+    def estimate_bytes(r: Recipe) -> int:
+        scene = NativeBackend().build(r, build_loop=False)
+        out = C.c_uint64(0)
+        ld = loop_desc(r.loop)
+        N.check(N.lib().pf_server_estimate_bytes(scene.h, C.byref(ld), C.byref(out)))
+        scene.close()
+        return int(out.value)
+
+    def submit(self, r: Recipe, lifetime: int) -> int:
+        scene = NativeBackend().build(r, build_loop=False)
+        ld = loop_desc(r.loop)
+        t = C.c_uint64(0)
+        try:
+            N.check(N.lib().pf_server_submit(self.h, scene.h, C.byref(ld), int(lifetime), C.byref(t)))
+        finally:
+            scene.close()
+        self.capacity[t.value] = r.capacity
+        return int(t.value)
+
+    def tick(self, dt: float) -> None:
+        N.check(N.lib().pf_server_tick(self.h, float(dt)))
+
+    def drain(self) -> None:
+        N.check(N.lib().pf_server_drain_build(self.h))
+
+    def state(self, ticket: int) -> tuple[int, int]:
+        st, done = C.c_uint32(0), C.c_uint32(0)
+        N.check(N.lib().pf_server_request_state(self.h, ticket, C.byref(st), C.byref(done)))
+        return int(st.value), int(done.value)
+
+    def readback(self, ticket: int, field_id: int) -> np.ndarray:
+        out = alloc_field(field_id, self.capacity[ticket])
+        N.check(N.lib().pf_server_readback(self.h, ticket, field_id, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def stats(self) -> dict:
+        o = N.ServerStats()
+        N.check(N.lib().pf_server_stats_read(self.h, C.byref(o)))
+        return {k: getattr(o, k) for k, _ in N.ServerStats._fields_ if k != "reserved0"}
+
+    def close(self) -> None:
+        if self.h:
+            N.lib().pf_server_destroy(self.h)
             self.h = None
 
     def __del__(self):
