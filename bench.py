@@ -261,21 +261,33 @@ class BatchWorkload:
 
         L = N.lib()
         backend = R.NativeBackend()
-        recipes = self.recipes(1000 + rank)
+        recipes = self.recipes(replica_seed(rank))
         plain = [backend.build(r) for r in recipes]
         psub = sum(r.particle_substeps for r in recipes)
-        # ---- plain baseline: per-scene streams and launches, no graph
+        # ---- plain baseline: each scene its own launches, no graph.
+        # Sequential: step a scene and wait for it (the reference's
+        # `await simulation.step()` per scene); timed as the sum of each
+        # scene's device time between its step's start and end events.
+        # Overlapped: every scene launched on its own stream, one wait.
         for _ in range(warmup if plain_baseline else 0):
             for sc in plain:
                 sc.step(self.DT)
         torch.cuda.synchronize()
         p_steps = max(2, steps // 2) if plain_baseline else 0
+        seq_dev = 0.0
+        t0 = time.perf_counter()
+        for _ in range(p_steps):
+            for sc in plain:
+                sc.step(self.DT)
+                seq_dev += sc.last_step_ms()
+        seq_wall = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1)
+        plain_ms = seq_dev / max(p_steps, 1) if plain_baseline else float("nan")
         t0 = time.perf_counter()
         for _ in range(p_steps):
             for sc in plain:
                 sc.step(self.DT)
         torch.cuda.synchronize()
-        plain_ms = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1) if plain_baseline else float("nan")
+        overlap_ms = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1) if plain_baseline else float("nan")
         # ---- batched: one world, one launch per stage, one graph per tick
         batch = R.Batch(plain, use_graph=True)
         for sc in plain:
@@ -343,6 +355,9 @@ class BatchWorkload:
                 "plain_ms_per_step": plain_ms,
                 "plain_value": psub / (plain_ms * 1e-3),
                 "batched_over_plain": plain_ms / ms,
+                "plain_wall_ms_per_step": seq_wall if plain_baseline else float("nan"),
+                "plain_overlapped_ms_per_step": overlap_ms,
+                "batched_over_plain_overlapped": overlap_ms / ms,
                 "scenes": len(recipes),
                 "particles": total,
                 "fluid_particles": int(items.value),
@@ -427,7 +442,8 @@ class ServeWorkload:
             by_tick.setdefault(t, []).append((rec, life))
         for rec, life in by_tick.get(0, []):
             srv.submit(rec, life)
-        srv.drain()
+        srv.tick(self.DT)  # admits the initial population (its cohort build starts)
+        srv.drain()  # and waits for that build, so the run starts from a live population
         tick_ms, ps0 = [], 0
         clocks = ClockSampler(torch.cuda.current_device())
         for t in range(warmup + ticks):
@@ -435,7 +451,7 @@ class ServeWorkload:
                 torch.cuda.synchronize()
                 ps0 = srv.stats()["particle_substeps"]
                 clocks.start()
-            for rec, life in by_tick.get(t + 1, []) if t > 0 else []:
+            for rec, life in by_tick.get(t + 1, []):
                 srv.submit(rec, life)
             t0 = time.perf_counter()
             srv.tick(self.DT)
@@ -469,6 +485,24 @@ class ServeWorkload:
 
 
 WORKLOADS = {"sort": SortWorkload, "batch": BatchWorkload, "serve": ServeWorkload}
+
+
+# -------------------------------------------------------------- ranks ----
+def replica_seed(rank: int) -> int:
+    """Seed of rank `rank`'s scene stream: replicas step disjoint scene sets
+    (weak scaling, no data-path collective)."""
+    return 1000 + rank
+
+
+def max_over_ranks(values, device) -> list:
+    """Element-wise maximum of per-rank timings (the job's time is its
+    slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
 
 
 # -------------------------------------------------------------- main ----
@@ -549,9 +583,7 @@ def main() -> None:
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([ms, res["e2e_ms"]], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+        ms, e2e_ms = max_over_ranks([ms, res["e2e_ms"]], "cuda")
     else:
         e2e_ms = res["e2e_ms"]
     peak, peak_kind = hbm_peak()

@@ -31,3 +31,11 @@ def pfsim():
 
     P.lib()
     return P
+
+
+@pytest.fixture(params=["slots", "tiles"])
+def nbr_path(request, monkeypatch):
+    """Runs a test on each fluid neighbour path (one thread per slot, warp
+    tiles) instead of the one the autotuner would pick."""
+    monkeypatch.setenv("PFSIM_NBR_PATH", "0" if request.param == "slots" else "1")
+    return request.param

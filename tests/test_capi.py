@@ -5,6 +5,8 @@ CPU only: no compute call is made (there is no GPU here).
 
 import ctypes as C
 import re
+
+import numpy as np
 from pathlib import Path
 
 from pfsim import _native as N
@@ -63,3 +65,19 @@ def test_unbuilt_scene_is_refused_without_loop_options():
     rc = N.lib().pf_server_estimate_bytes(scene.h, None, C.byref(out))
     assert rc == N.PF_ERR_STATE
     assert b"SimLoop" in N.lib().pf_last_error()
+
+
+def test_api_validation_is_host_side():
+    """The reference's constructor checks run before any device work."""
+    import pytest
+
+    from pfsim import api as A
+
+    with pytest.raises(N.PfError, match="Simulation: give exactly one"):
+        A.Simulation(particles=100, particle_radius=0.01)
+    with pytest.raises(N.PfError, match="ParticleSystem: capacity"):
+        A.ParticleSystem(0, 0.01)
+    with pytest.raises(N.PfError, match="SoftbodySystem: shapeMatching"):
+        A.SoftbodySystem(A.ParticleSystem(4, 0.01), [], shape_matching="x")
+    with pytest.raises(N.PfError, match="SDFCollider: resolution"):
+        A.SDFCollider(A.ParticleSystem(4, 0.01), np.zeros((2, 4, 4)), (0, 0, 0), (1, 1, 1))

@@ -25,7 +25,7 @@ def cuda():
     return R.NativeBackend()
 
 
-def test_neighbor_lists_bit_exact(oracle, cuda):
+def test_neighbor_lists_bit_exact(oracle, cuda, nbr_path):
     """Lists built from identical positions hold the same particles in the
     same order (walk order dz, dy, dx; ascending index in a cell)."""
     r = W.dam_break(5000, seed=1, gravity=(0.0, 0.0, 0.0), substeps=1, iterations=1)
@@ -43,7 +43,7 @@ def test_neighbor_lists_bit_exact(oracle, cuda):
 
 
 @pytest.mark.parametrize("seed", [0, 7])
-def test_one_frame_positions_within_tolerance(oracle, cuda, seed):
+def test_one_frame_positions_within_tolerance(oracle, cuda, seed, nbr_path):
     r = W.dam_break(5000, seed=seed)
     a, b = cuda.build(r), oracle.OracleBackend().build(r)
     a.step(DT)

@@ -29,7 +29,8 @@ def test_free_fall(cuda, cpu):
     y = float(a.readback(N.PF_FIELD_POSITIONS)[0, 1])
     assert y < 0
     assert abs(y - K.free_fall_reference(60)) < 1e-4
-    assert abs(y - float(b.readback(N.PF_FIELD_POSITIONS)[0, 1])) < 1e-6
+    # 60 steps of |y| ~ 5 m: a few f32 ulps of contraction difference
+    assert abs(y - float(b.readback(N.PF_FIELD_POSITIONS)[0, 1])) < 1e-5
 
 
 def test_xpbd_rigid_limit(cuda, cpu):

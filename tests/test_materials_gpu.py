@@ -67,7 +67,7 @@ def test_softbodies_one_frame(oracle, cuda, mode):
         assert d.max() < 1e-4
 
 
-def test_mixed_scene_one_frame(oracle, cuda):
+def test_mixed_scene_one_frame(oracle, cuda, nbr_path):
     """Fluid with dynamic soft-body boundaries (Akinci volumes and reaction),
     local shape matching and a swept sphere on a circle."""
     r = W.mixed_scene(n_budget=12_000, n_fluid=8_000, n_bodies=4, seed=1)

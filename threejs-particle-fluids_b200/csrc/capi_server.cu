@@ -19,9 +19,10 @@
 // Scenes are independent and every stage is per-scene deterministic, so a
 // scene's result is the same alone and inside any cohort.
 //
-// PLAIN mode gives each request its own world (no graph, no folding): the
-// per-scene loop the batched mode is measured against, on the same stream
-// of requests and the same admission rule.
+// PLAIN mode gives each request its own world (no graph, no folding) and
+// steps the scenes one after another, waiting for each (the reference's
+// `await simulation.step()` per scene): the per-scene loop the batched mode
+// is measured against, on the same stream of requests and admission rule.
 
 #include <cuda_runtime.h>
 
@@ -360,13 +361,17 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   PF_TRY(admit(S));
   if (!S->opts.async_build && S->build) PF_TRY(swap_in(S));
   bool stepped = false;
+  const bool plain = S->opts.mode == PF_SERVER_PLAIN;
   for (auto& c : S->cohorts)
     if (c->live) {
       PF_TRY(c->world->step(dt));
+      // the per-scene loop steps one scene and waits for it
+      if (plain) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
       stepped = true;
     }
-  for (auto& c : S->cohorts)
-    if (c->live) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
+  if (!plain)
+    for (auto& c : S->cohorts)
+      if (c->live) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
   bool freed = false;
   for (auto& c : S->cohorts) {
     for (uint32_t j = 0; j < c->members.size(); ++j) {

@@ -14,10 +14,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "world.cuh"
 #include "world_kernels.cuh"
+#include "world_slots.cuh"
 #include "world_tiles.cuh"
 
 namespace pf {
@@ -1165,7 +1167,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.perm = cv.take<uint32_t>(N);
     base_.cstart = cv.take<uint32_t>(cells_);
     base_.ccount = cv.take<uint32_t>(cells_);
-    base_.nbr16 = any_fluid_ ? cv.take<uint16_t>(N * kMaxNbr) : nullptr;
+    base_.nbr = any_fluid_ ? cv.take<uint32_t>(N * kMaxNbr) : nullptr;
+    base_.nbr16 = reinterpret_cast<uint16_t*>(base_.nbr);
     base_.ncount = cv.take<uint32_t>(N);
     base_.slot_tile = cv.take<uint32_t>(N);
     base_.tiles = cv.take<Tile>(max_tiles);
@@ -1363,6 +1366,88 @@ void World::launch_tiles_build(const WorldView& V, uint32_t s) {
   launch_tiled(k_t_neighbors, kSmemNbr, V, s);
 }
 
+// One-thread-per-slot fluid kernels at the tuned block size.
+template <typename K, typename... A>
+void World::launch_fluid(K kernel, A... args) {
+  kernel<<<div_up(n_, slot_block_), slot_block_, 0, stream_>>>(args...);
+  ++t_launches;
+}
+
+void World::run_fluid_neighbors(const WorldView& V, uint32_t s) {
+  if (nbr_path_ == 1) {
+    launch_tiles_build(V, s);
+  } else {
+    launch_fluid(k_s_neighbors, V, s);
+  }
+}
+
+void World::run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it) {
+  if (nbr_path_ == 1) {
+    launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
+    launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
+  } else {
+    launch_fluid(k_s_lambda, V, r, s, it);
+    launch_fluid(k_s_delta, V, r, s, it);
+  }
+}
+
+void World::run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s) {
+  if (nbr_path_ == 1) {
+    launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
+  } else {
+    launch_fluid(k_s_xsph, V, r, s);
+  }
+}
+
+// Autotuner: on the world's own state (one grid rebuild, as the next
+// substep would do; the permutation is canonical, so no result changes), time
+// the neighbour build + density/lambda + position delta + XSPH of each
+// configuration and keep the fastest. The passes write only per-substep
+// scratch (lists, lambda, density, deltas), which every substep rebuilds.
+pf_status World::tune() {
+  tuned_ = true;
+  if (!any_fluid_ || n_ == 0) return PF_OK;
+  if (const char* e = std::getenv("PFSIM_NBR_PATH")) {  // fixed choice for measurements
+    nbr_path_ = (uint32_t)std::atoi(e) == 1 ? 1u : 0u;
+    if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) slot_block_ = (uint32_t)std::atoi(b);
+    if (slot_block_ != 128 && slot_block_ != 256 && slot_block_ != 512) slot_block_ = 256;
+    return PF_OK;
+  }
+  run_sort_and_permute(parity_, false);
+  parity_ ^= 1;
+  const WorldView V = view(parity_);
+  const uint32_t rank = h_fluids_[0].rank;
+  struct Cand { uint32_t path, block; };
+  const Cand cands[] = {{0, 128}, {0, 256}, {0, 512}, {1, 128}};
+  float best = 1e30f;
+  Cand pick = {0, 256};
+  for (const Cand& c : cands) {
+    nbr_path_ = c.path;
+    slot_block_ = c.block;
+    float t = 0;
+    for (int rep = 0; rep < 3; ++rep) {
+      PF_CUDA(cudaEventRecord(ev0_, stream_));
+      // one substep's worth: the list once, density/lambda + delta per iteration
+      run_fluid_neighbors(V, 0);
+      for (uint32_t it = 0; it < std::max(max_iter_, 1u); ++it) run_fluid_lambda_delta(V, rank, 0, 0);
+      if (any_visc_) run_fluid_xsph(V, rank, 0);
+      PF_CUDA(cudaEventRecord(ev1_, stream_));
+      PF_CUDA(cudaEventSynchronize(ev1_));
+      float ms = 0;
+      PF_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+      t = rep == 0 ? ms : std::min(t, ms);
+    }
+    PF_CUDA(cudaGetLastError());
+    if (t < best) {
+      best = t;
+      pick = c;
+    }
+  }
+  nbr_path_ = pick.path;
+  slot_block_ = pick.block;
+  return PF_OK;
+}
+
 template <typename K, typename... A>
 void World::launch_tiled(K kernel, size_t smem, const WorldView& V, A... args) {
   const uint32_t grid = std::max<uint32_t>(
@@ -1404,7 +1489,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   }
   // preSolve
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
-  if (any_fluid_) launch_tiles_build(V, s);
+  if (any_fluid_) run_fluid_neighbors(V, s);
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
   if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
@@ -1419,8 +1504,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         has_global = has_global || (D.rank == r && !D.local);
       }
       if (has_fluid) {
-        launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
-        launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
+        run_fluid_lambda_delta(V, r, s, it);
         launch_slots(k_fluid_apply, n_, stream_, V, r, s, it);
       }
       if (has_local) {
@@ -1451,7 +1535,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     for (auto& F : h_fluids_) has_visc = has_visc || (F.rank == r && F.has_visc);
     for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
     if (has_visc) {
-      launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
+      run_fluid_xsph(V, r, s);
       launch_slots(k_xsph_apply, n_, stream_, V, r, s);
     }
     if (has_local) {
@@ -1475,6 +1559,7 @@ pf_status World::step(double dt) {
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
   PF_TRY(upload_params(dt));
   PF_CUDA(cudaEventRecord(ev0_, stream_));
+  if (!tuned_) PF_TRY(tune());
   if (!inited_) {
     run_init_pass();
     inited_ = true;
@@ -1609,6 +1694,21 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
       }
       std::fill(o, o + (size_t)cap * kMaxNbr, 0xffffffffu);
       if (!base_.nbr16) return PF_OK;
+      if (nbr_path_ == 0) {
+        std::vector<uint32_t> colw(seg), seg_ids(seg);
+        PF_CUDA(cudaMemcpy(seg_ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+        for (uint32_t m = 0; m < kMaxNbr; ++m) {
+          PF_CUDA(cudaMemcpy(colw.data(), base_.nbr + (size_t)m * n_ + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+          for (uint32_t k = 0; k < seg; ++k) {
+            const uint32_t id = ids[k] - S.seg_start;
+            if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k]) continue;
+            const uint32_t j = colw[k];  // a neighbour is a slot of the same scene's segment
+            o[(size_t)id * kMaxNbr + m] = (j >= S.seg_start && j < S.seg_end) ? seg_ids[j - S.seg_start] - S.seg_start
+                                                                               : 0xfffffffeu;
+          }
+        }
+        return PF_OK;
+      }
       uint32_t nt = 0;
       PF_CUDA(cudaMemcpy(&nt, base_.tile_count, 4, cudaMemcpyDeviceToHost));
       nt = std::min(nt, base_.max_tiles);
@@ -1722,15 +1822,28 @@ pf_status World::read_positions(float* dst, size_t bytes) {
 
 pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_t* items) {
   const WorldView V = view(parity_);
+  const uint32_t rank = h_fluids_.empty() ? 0u : h_fluids_[0].rank;
   uint64_t fluid = 0;
   for (uint32_t s = 0; s < specs_.size(); ++s)
     for (auto& f : specs_[s]->fluids) fluid += f.range.count;
   auto run = [&]() {
     switch (stage) {
-      case 0: launch_tiled(k_t_neighbors, kSmemNbr, V, 0u); break;
-      case 1: launch_tiled(k_t_lambda, kSmemLambda, V, 0u, 0u, 0u); break;
-      case 2: launch_tiled(k_t_delta, kSmemDelta, V, 0u, 0u, 0u); break;
-      case 3: launch_tiled(k_t_xsph, kSmemXsph, V, 0u, 0u); break;
+      case 0:
+        if (nbr_path_ == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
+        else launch_fluid(k_s_neighbors, V, 0u);
+        break;
+      case 1:
+        if (nbr_path_ == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
+        else launch_fluid(k_s_lambda, V, rank, 0u, 0u);
+        break;
+      case 2:
+        if (nbr_path_ == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
+        else launch_fluid(k_s_delta, V, rank, 0u, 0u);
+        break;
+      case 3:
+        if (nbr_path_ == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
+        else launch_fluid(k_s_xsph, V, rank, 0u);
+        break;
       case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
       default: break;
     }

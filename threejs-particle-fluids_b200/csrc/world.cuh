@@ -220,7 +220,8 @@ struct WorldView {
   uint32_t* perm;     // new slot -> id (sort output)
   uint32_t* cstart;
   uint32_t* ccount;
-  uint16_t* nbr16;    // kMaxNbr * n, column-major: halo index of each neighbour
+  uint32_t* nbr;      // kMaxNbr * n, column-major: slot of each neighbour (slot path)
+  uint16_t* nbr16;    // the same storage, kMaxNbr * n halfwords: halo index of each neighbour (tile path)
   uint32_t* ncount;
   uint32_t* slot_tile;  // tile of each slot (this substep)
   Tile* tiles;
@@ -308,6 +309,12 @@ class World {
   // Average device milliseconds of one solver stage run `reps` times on the
   // current state (substep 0, iteration 0, material rank 0).
   pf_status profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_t* items);
+  // Neighbour-pass configuration the autotuner chose (path 0: one thread
+  // per slot with `block` threads per block; path 1: warp tiles).
+  void tuning(uint32_t* path, uint32_t* block) const {
+    *path = nbr_path_;
+    *block = slot_block_;
+  }
   size_t device_bytes() const { return bytes_; }
 
  private:
@@ -316,6 +323,12 @@ class World {
   void run_sort_and_permute(uint32_t parity, bool committed);
   void run_init_pass();
   void launch_tiles_build(const WorldView& V, uint32_t s);
+  template <typename K, typename... A>
+  void launch_fluid(K kernel, A... args);
+  void run_fluid_neighbors(const WorldView& V, uint32_t s);
+  void run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it);
+  void run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s);
+  pf_status tune();
   template <typename K, typename... A>
   void launch_tiled(K kernel, size_t smem, const WorldView& V, A... args);
   void launch_frame_start_at(uint32_t parity);
@@ -346,6 +359,9 @@ class World {
   SortScratch sort_{};
   uint32_t parity_ = 0;
   bool inited_ = false;
+  // neighbour passes: autotuned once per world, before the first graph capture
+  uint32_t nbr_path_ = 0, slot_block_ = 256;
+  bool tuned_ = false;
   // graph
   bool use_graph_ = false;
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};

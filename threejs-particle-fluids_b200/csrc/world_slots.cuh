@@ -1,0 +1,210 @@
+// world_slots.cuh — the fluid neighbour passes with one thread per slot.
+//
+// Each thread owns one particle (slot k, cell order) and gathers its
+// neighbours' state straight from the slot arrays; particles are in cell
+// order, so a warp's gathers fall on a few hundred consecutive slots that L1
+// holds. The neighbour list stores slots (32 bits), column-major, so a warp
+// reads its m-th entries as one coalesced line. The loops fetch the list and
+// the neighbours four at a time before using them: four independent loads in
+// flight per round instead of a dependent load per neighbour, with the sums
+// still formed in list order.
+//
+// The other neighbour path (world_tiles.cuh) stages tiles through shared
+// memory; the autotuner of World::tune picks one per world.
+#pragma once
+
+#include "world_kernels.cuh"
+
+namespace pf {
+
+constexpr uint32_t kNbrUnroll = 4;
+
+// neighborList.ts:48-71: up to 64 neighbours within h at the predicted
+// positions of this substep, in walk order, self included.
+__global__ void k_s_neighbors(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const DevFluid& F = V.fluids[f - 1];
+  const f3 xi = xyz(V.cur.xs[k]);
+  uint32_t cnt = 0;
+  bool over = false;
+  const size_t n = V.n;
+  walk27(S, V.cstart, V.ccount, xi, [&](uint32_t j) {
+    const f3 off = xi - xyz(__ldg(V.cur.xs + j));
+    if (dot_rn(off) < F.hsq) {
+      if (cnt < kMaxNbr) {
+        V.nbr[(size_t)cnt * n + k] = j;
+        ++cnt;
+      } else {
+        over = true;
+        return false;
+      }
+    }
+    return true;
+  });
+  V.ncount[k] = cnt;
+  if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
+}
+
+// lambda.ts:41-71
+__global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const float4 xi4 = V.cur.xs[k];
+  const f3 xi = xyz(xi4);
+  float rho = 0.0f, gss = 0.0f;
+  f3 gs = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  auto one = [&](float4 xj, float bvj) {
+    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+    const f3 off = xi - xyz(xj);
+    const float rsq = dot(off, off);
+    rho += mass * poly6(rsq, F);
+    const f3 g = spiky_vec(off, rsq, F) * mass;
+    gs = gs + g;
+    gss += dot(g, g) * xj.w;
+  };
+  uint32_t m = 0;
+  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+    uint32_t j[kNbrUnroll];
+    float4 xj[kNbrUnroll];
+    float bj[kNbrUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+      xj[q] = __ldg(V.cur.xs + j[q]);
+      bj[q] = __ldg(V.cur.bv + j[q]);
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], bj[q]);
+  }
+  for (; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    one(__ldg(V.cur.xs + j), __ldg(V.cur.bv + j));
+  }
+  V.density[k] = rho;
+  const float C = rho * F.inv_rho0 - 1.0f;
+  if (C <= 0.0f) {
+    V.lambda[k] = 0.0f;
+    return;
+  }
+  const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
+  const float at = F.compliance / (S.dt * S.dt);
+  V.lambda[k] = -C / fmaxf(gn + at, 1e-20f);
+}
+
+// positionDelta.ts:41-85 (the reaction on dynamic boundary neighbours goes
+// into the fixed-point reaction sums by slot).
+__global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const float4 xi4 = V.cur.xs[k];
+  const f3 xi = xyz(xi4);
+  const float li = V.lambda[k];
+  const bool react = F.react_lo != F.react_hi && li != 0.0f;
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  auto one = [&](uint32_t j, float4 xj, float bvj, float lj) {
+    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+    const f3 off = xi - xyz(xj);
+    const f3 g = spiky_vec(off, dot(off, off), F);
+    sum = sum + g * ((li + lj) * mass);
+    if (react && bvj > 0.0f && xj.w > 0.0f) {
+      const uint32_t idj = V.ids[j];
+      bool in = false;
+      for (uint32_t b = 0; b < F.bnd_count; ++b) {
+        const DevBoundary B = V.bnds[F.bnd_first + b];
+        in = in || (idj >= B.start && idj < B.start + B.count);
+      }
+      if (in) acc_add(V.acc_react, j, g * (-(li / F.rho0) * (F.rho0 * bvj) * xj.w), F.react_scale);
+    }
+  };
+  uint32_t m = 0;
+  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+    uint32_t j[kNbrUnroll];
+    float4 xj[kNbrUnroll];
+    float bj[kNbrUnroll], lj[kNbrUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+      xj[q] = __ldg(V.cur.xs + j[q]);
+      bj[q] = __ldg(V.cur.bv + j[q]);
+      lj[q] = __ldg(V.lambda + j[q]);
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], bj[q], lj[q]);
+  }
+  for (; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    one(j, __ldg(V.cur.xs + j), __ldg(V.cur.bv + j), __ldg(V.lambda + j));
+  }
+  V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
+}
+
+// velocity.ts:43-70 (XSPH): committed positions and velocities.
+__global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_visc) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const f3 xi = xyz(V.cur.x[k]);
+  const f3 vi = xyz(V.cur.v[k]);
+  f3 sm = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  auto one = [&](float4 xj, float4 vj, float bvj) {
+    const f3 off = xi - xyz(xj);
+    const float vol = bvj > 0.0f ? bvj : F.volume;
+    sm = sm + ((xyz(vj) - vi) * poly6(dot(off, off), F)) * vol;
+  };
+  uint32_t m = 0;
+  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+    uint32_t j[kNbrUnroll];
+    float4 xj[kNbrUnroll], vj[kNbrUnroll];
+    float bj[kNbrUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+      xj[q] = __ldg(V.cur.x + j[q]);
+      vj[q] = __ldg(V.cur.v + j[q]);
+      bj[q] = __ldg(V.cur.bv + j[q]);
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], vj[q], bj[q]);
+  }
+  for (; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), __ldg(V.cur.bv + j));
+  }
+  V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
+}
+
+}  // namespace pf

@@ -192,6 +192,21 @@ __device__ __forceinline__ void stage_rows(const WarpTile& W, const E* __restric
   }
 }
 
+// Visit a particle's list entries in order, fetching four halo indices per
+// round so their loads overlap.
+template <typename Fn>
+__device__ __forceinline__ void for_each_h(const uint16_t* __restrict__ nl, size_t n, uint32_t cnt, Fn&& one) {
+  uint32_t m = 0;
+  for (; m + 4 <= cnt; m += 4) {
+    uint32_t h[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) h[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) one(h[q]);
+  }
+  for (; m < cnt; ++m) one(__ldg(nl + m * n));
+}
+
 // neighborList.ts:48-71 over warp tiles: candidates are the 27 cells of the
 // particle's own cell; entries are halo indices of the tile.
 __global__ void __launch_bounds__(kTileThreads) k_t_neighbors(WorldView V, uint32_t sub) {
@@ -280,8 +295,7 @@ __global__ void __launch_bounds__(kTileThreads) k_t_lambda(WorldView V, uint32_t
       float rho = 0.0f, gss = 0.0f;
       f3 gs = mk(0.0f, 0.0f, 0.0f);
       const uint32_t cnt = V.ncount[i];
-      for (uint32_t m = 0; m < cnt; ++m) {
-        const uint32_t h = V.nbr16[(size_t)m * n + i];
+      auto one = [&](uint32_t h) {
         float4 xj;
         float bvj;
         if (staged) {
@@ -299,7 +313,8 @@ __global__ void __launch_bounds__(kTileThreads) k_t_lambda(WorldView V, uint32_t
         const f3 g = spiky_vec(off, rsq, F) * mass;
         gs = gs + g;
         gss += dot(g, g) * xj.w;
-      }
+      };
+      for_each_h(V.nbr16 + i, n, cnt, one);
       V.density[i] = rho;
       const float C = rho * F.inv_rho0 - 1.0f;
       if (C <= 0.0f) {
@@ -348,8 +363,7 @@ __global__ void __launch_bounds__(kTileThreads) k_t_delta(WorldView V, uint32_t 
       const bool react = F.react_lo != F.react_hi && li != 0.0f;
       f3 sum = mk(0.0f, 0.0f, 0.0f);
       const uint32_t cnt = V.ncount[i];
-      for (uint32_t m = 0; m < cnt; ++m) {
-        const uint32_t h = V.nbr16[(size_t)m * n + i];
+      auto one = [&](uint32_t h) {
         float4 xj;
         float bvj, lj;
         if (staged) {
@@ -376,7 +390,8 @@ __global__ void __launch_bounds__(kTileThreads) k_t_delta(WorldView V, uint32_t 
           }
           if (in) acc_add(V.acc_react, j, g * (-(li / F.rho0) * (F.rho0 * bvj) * xj.w), F.react_scale);
         }
-      }
+      };
+      for_each_h(V.nbr16 + i, n, cnt, one);
       V.dx[i] = with_w((sum / F.rho0) * xi4.w, 0.0f);
     }
     __syncwarp();
@@ -414,8 +429,7 @@ __global__ void __launch_bounds__(kTileThreads) k_t_xsph(WorldView V, uint32_t r
       const f3 vi = xyz(V.cur.v[i]);
       f3 sm = mk(0.0f, 0.0f, 0.0f);
       const uint32_t cnt = V.ncount[i];
-      for (uint32_t m = 0; m < cnt; ++m) {
-        const uint32_t h = V.nbr16[(size_t)m * n + i];
+      auto one = [&](uint32_t h) {
         float4 xj, vj;
         float bvj;
         if (staged) {
@@ -431,7 +445,8 @@ __global__ void __launch_bounds__(kTileThreads) k_t_xsph(WorldView V, uint32_t r
         const f3 off = xi - xyz(xj);
         const float vol = bvj > 0.0f ? bvj : F.volume;
         sm = sm + ((xyz(vj) - vi) * poly6(dot(off, off), F)) * vol;
-      }
+      };
+      for_each_h(V.nbr16 + i, n, cnt, one);
       V.dv[i] = with_w(sm * F.c_xsph, 0.0f);
     }
     __syncwarp();
