@@ -166,75 +166,13 @@ __global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_
   V.cur.bv[k] = 1.0f / fmaxf(sum, 1e-12f);
 }
 
-// positionDelta.ts:217-226, then the reaction accumulator's apply over the
-// covering range of the fluid's boundaries (FluidSystem.ts:280-287).
-__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t s = scene_index(V, k);
-  const DevScene& S = V.scenes[s];
-  if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  float4 x = V.cur.xs[k];
-  bool changed = false;
-  if (f && V.fluids[f - 1].rank == rank) {
-    const float4 d = V.dx[k];
-    x.x += d.x;
-    x.y += d.y;
-    x.z += d.z;
-    changed = true;
-  }
-  if (V.acc_react) {
-    const uint32_t id = V.ids[k];
-    for (uint32_t q = 0; q < S.fluid_count; ++q) {
-      const DevFluid& F = V.fluids[S.fluid_first + q];
-      if (F.rank != rank || F.react_lo == F.react_hi) continue;
-      if (id < F.react_lo || id >= F.react_hi) continue;
-      int4 t = V.acc_react[k];
-      bool sat = false;
-      const f3 c = ticks_change(t.x, t.y, t.z, F.react_inv, &sat);
-      V.acc_react[k] = make_int4(0, 0, 0, 0);
-      x.x += c.x;
-      x.y += c.y;
-      x.z += c.z;
-      changed = true;
-      if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_REACT, 1u);
-    }
-  }
-  if (changed) V.cur.xs[k] = x;
-}
-
-// velocity.ts:99-120: add the XSPH change to the velocity.
-__global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
-  const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank || !F.has_visc) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
-  const float4 d = V.dv[k];
-  float4 v = V.cur.v[k];
-  v.x += 0.0f + d.x;
-  v.y += 0.0f + d.y;
-  v.z += 0.0f + d.z;
-  V.cur.v[k] = v;
-}
-
-// ------------------------------------------------------------ colliders ----
-// PrimitiveSet.ts:339-365 with collider.ts:53-89, fused with the position
-// accumulator's apply (loop.ts:225): a primitive contact only adds to its own
-// particle, so the sum of rounded ticks is formed in registers.
-__global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t s = scene_index(V, k);
-  const DevScene& S = V.scenes[s];
-  if (S.prim_count + S.sdf_count == 0 || sub >= S.substeps || it >= S.iterations) return;
-  const float4 xs4 = V.cur.xs[k];
+// The colliders of particle k's scene against its predicted position xs4
+// (w = inverse mass), their multipliers updated; the fixed-point position
+// changes summed in registers and applied. Returns whether xs4 changed.
+__device__ __forceinline__ bool collide_particle(const WorldView& V, const DevScene& S, uint32_t s, uint32_t k,
+                                                 float4& xs4) {
   const float w = xs4.w;
-  if (!(w > 0.0f)) return;
+  if (!(w > 0.0f)) return false;
   const f3 xstar = xyz(xs4);
   const f3 disp = xstar - xyz(V.cur.x[k]);
   const float clock = V.clocks[s];
@@ -293,11 +231,86 @@ __global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, u
     V.plam[li] = lam;
     any = true;
   }
-  if (!any) return;
+  if (!any) return false;
   bool sat = false;
   const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
-  V.cur.xs[k] = with_w(xstar + c, w);
+  xs4 = with_w(xstar + c, w);
   if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_POS, 1u);
+  return true;
+}
+
+// positionDelta.ts:217-226, then the reaction accumulator's apply over the
+// covering range of the fluid's boundaries (FluidSystem.ts:280-287).
+__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  float4 x = V.cur.xs[k];
+  bool changed = false;
+  if (f && V.fluids[f - 1].rank == rank) {
+    const float4 d = V.dx[k];
+    x.x += d.x;
+    x.y += d.y;
+    x.z += d.z;
+    changed = true;
+  }
+  if (V.acc_react) {
+    const uint32_t id = V.ids[k];
+    for (uint32_t q = 0; q < S.fluid_count; ++q) {
+      const DevFluid& F = V.fluids[S.fluid_first + q];
+      if (F.rank != rank || F.react_lo == F.react_hi) continue;
+      if (id < F.react_lo || id >= F.react_hi) continue;
+      int4 t = V.acc_react[k];
+      bool sat = false;
+      const f3 c = ticks_change(t.x, t.y, t.z, F.react_inv, &sat);
+      V.acc_react[k] = make_int4(0, 0, 0, 0);
+      x.x += c.x;
+      x.y += c.y;
+      x.z += c.z;
+      changed = true;
+      if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_REACT, 1u);
+    }
+  }
+  // the scene's colliders follow its last material in the same pass
+  if (S.collide_rank1 == rank + 1 && collide_particle(V, S, s, k, x)) changed = true;
+  if (changed) V.cur.xs[k] = x;
+}
+
+// velocity.ts:99-120: add the XSPH change to the velocity.
+__global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_visc) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 d = V.dv[k];
+  float4 v = V.cur.v[k];
+  v.x += 0.0f + d.x;
+  v.y += 0.0f + d.y;
+  v.z += 0.0f + d.z;
+  V.cur.v[k] = v;
+}
+
+// ------------------------------------------------------------ colliders ----
+// PrimitiveSet.ts:339-365 + SDFCollider.ts:256-281 with collider.ts:53-89,
+// fused with the position accumulator's apply (loop.ts:225): a contact only
+// adds to its own particle, so the sum of rounded ticks is formed in
+// registers. Scenes whose last material is a fluid run this inside the
+// fluid's apply instead (collide_rank1).
+__global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (S.prim_count + S.sdf_count == 0 || S.collide_rank1 || sub >= S.substeps || it >= S.iterations) return;
+  float4 xs4 = V.cur.xs[k];
+  if (collide_particle(V, S, s, k, xs4)) V.cur.xs[k] = xs4;
 }
 
 // PrimitiveSet.ts:367-398 with collider.ts:96-118, fused with the velocity
@@ -752,6 +765,9 @@ World::~World() {
     if (g) cudaGraphExecDestroy(g);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  if (side_stream_) cudaStreamDestroy(side_stream_);
   if (stream_) cudaStreamDestroy(stream_);
   if (arena_) cudaFree(arena_);
   if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
@@ -1009,8 +1025,36 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
     any_grid_ = any_grid_ || S.has_grid;
     any_prims_ = any_prims_ || S.prim_count > 0 || S.sdf_count > 0;
+    // colliders fuse into the last material's pass when that is a fluid
+    S.collide_rank1 = 0;
+    if (S.prim_count + S.sdf_count > 0) {
+      if (!sp.materials.empty() && sp.materials.back().first == MAT_FLUID)
+        S.collide_rank1 = (uint32_t)sp.materials.size();
+      else
+        any_unfused_prims_ = true;
+    }
   }
   if (max_rank_ > 32) return fail(PF_ERR_INVALID, "SimLoop: at most 32 materials per scene");
+  // The side stream applies when every scene that holds cloth, or whose
+  // colliders run in their own pass, has cloth materials only.
+  {
+    bool any_side = false, ok = true;
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      bool cloth_only = true, has_cloth = false;
+      for (auto& m : sp.materials) {
+        cloth_only = cloth_only && m.first == MAT_CLOTH;
+        has_cloth = has_cloth || m.first == MAT_CLOTH;
+      }
+      const bool unfused = h_scenes_[s].prim_count + h_scenes_[s].sdf_count > 0 && h_scenes_[s].collide_rank1 == 0;
+      if (has_cloth || unfused) {
+        ok = ok && cloth_only;
+        any_side = true;
+      }
+    }
+    // only worth a second stream when other scenes run alongside
+    side_ok_ = ok && any_side && (any_fluid_ || !h_softs_.empty());
+  }
   n_ = (uint32_t)slot;
   cells_ = (uint32_t)cell;
   // ---- cloth constraints by (rank, colour) ----------------------------
@@ -1234,6 +1278,11 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   base_.n_rows = row_base.back();
   pair_entries_ = any_soft_local_ ? csr_idx.size() : 0;
   PF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  if (side_ok_) {
+    PF_CUDA(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking));
+    PF_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    PF_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+  }
   PF_CUDA(cudaEventCreate(&ev0_));
   PF_CUDA(cudaEventCreate(&ev1_));
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
@@ -1495,6 +1544,23 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
   if (base_.n_cons) cudaMemsetAsync(base_.c_lambda, 0, 4ull * base_.n_cons, stream_);
   // iterations
+  // Cloth-only scenes (and material-free scenes with colliders) share no
+  // slot with the others: their colour sweeps and collider passes run on a
+  // second stream, overlapping the fluid and soft-body iterations.
+  const bool fork = side_ok_ && side_stream_;
+  if (fork) {
+    cudaEventRecord(ev_fork_, stream_);
+    cudaStreamWaitEvent(side_stream_, ev_fork_, 0);
+    for (uint32_t it = 0; it < max_iter_; ++it) {
+      for (uint32_t r = 0; r < cloth_ranges_.size(); ++r)
+        for (auto& rg : cloth_ranges_[r])
+          if (rg.second > rg.first) {
+            k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, side_stream_>>>(V, rg.first, rg.second, s, it);
+            ++t_launches;
+          }
+      if (any_unfused_prims_) launch_slots(k_collide, n_, side_stream_, V, s, it);
+    }
+  }
   for (uint32_t it = 0; it < max_iter_; ++it) {
     for (uint32_t r = 0; r < max_rank_; ++r) {
       bool has_fluid = false, has_local = false, has_global = false;
@@ -1519,15 +1585,18 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         k_global_apply<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it);
         t_launches += 2;
       }
-      if (r < cloth_ranges_.size())
+      if (!fork && r < cloth_ranges_.size())
         for (auto& rg : cloth_ranges_[r])
-          if (rg.second > rg.first)
-          {
+          if (rg.second > rg.first) {
             k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, stream_>>>(V, rg.first, rg.second, s, it);
             ++t_launches;
           }
     }
-    if (any_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
+    if (!fork && any_unfused_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
+  }
+  if (fork) {
+    cudaEventRecord(ev_join_, side_stream_);
+    cudaStreamWaitEvent(stream_, ev_join_, 0);
   }
   launch_slots(k_advect, n_, stream_, V, s);
   for (uint32_t r = 0; r < max_rank_; ++r) {

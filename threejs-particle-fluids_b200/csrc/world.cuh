@@ -126,6 +126,7 @@ struct DevScene {
   uint32_t soft_local_ranks;          // bit r: a local shape-matching system at material rank r
   uint32_t init_pending;              // the one-time init pass has not run for this scene
   uint32_t sdf_base, sdf_count;       // this scene's SDF colliders in the SDF table
+  uint32_t collide_rank1;             // r + 1: colliders run inside the apply of fluid rank r (its last material)
 };
 
 // One SDF collider as the kernels read it (sdf.ts:17-80 fields).
@@ -350,6 +351,7 @@ class World {
   bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false;
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
   bool any_react_ = false;
+  bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass
   uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
   // device memory: one arena
   void* arena_ = nullptr;
@@ -367,6 +369,10 @@ class World {
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
   double graph_dt_ = -1;
   cudaStream_t stream_ = nullptr;
+  // second stream for cloth-only scenes (fork/join inside each substep)
+  bool side_ok_ = false;
+  cudaStream_t side_stream_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   float last_ms_ = 0;
   // pinned staging for per-step parameters

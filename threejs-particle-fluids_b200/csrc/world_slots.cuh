@@ -20,7 +20,10 @@ namespace pf {
 constexpr uint32_t kNbrUnroll = 4;
 
 // neighborList.ts:48-71: up to 64 neighbours within h at the predicted
-// positions of this substep, in walk order, self included.
+// positions of this substep, in walk order (query.ts:37-66: rows dz, dy;
+// inside a row ascending cell, inside a cell ascending index), self
+// included. The nine row ranges are fetched first, then each row's
+// candidates four at a time.
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -30,22 +33,50 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   if (sub >= S.substeps) return;
   const DevFluid& F = V.fluids[f - 1];
   const f3 xi = xyz(V.cur.xs[k]);
+  const float hsq = F.hsq;
+  int32_t cx, cy, cz;
+  local_cell(S, xi, &cx, &cy, &cz, nullptr);
+  const int32_t x0 = max(cx - 1, 0), x1 = min(cx + 1, (int32_t)S.dims[0] - 1);
+  uint32_t rs[9], re[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    const int32_t z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+    if (z < 0 || z >= (int32_t)S.dims[2] || y < 0 || y >= (int32_t)S.dims[1]) {
+      rs[r] = re[r] = 0;
+      continue;
+    }
+    const uint32_t row = S.cell_base + S.dims[0] * ((uint32_t)y + S.dims[1] * (uint32_t)z);
+    rs[r] = __ldg(V.cstart + row + x0);
+    re[r] = __ldg(V.cstart + row + x1) + __ldg(V.ccount + row + x1);
+  }
   uint32_t cnt = 0;
   bool over = false;
   const size_t n = V.n;
-  walk27(S, V.cstart, V.ccount, xi, [&](uint32_t j) {
-    const f3 off = xi - xyz(__ldg(V.cur.xs + j));
-    if (dot_rn(off) < F.hsq) {
+  uint32_t* __restrict__ out = V.nbr + k;
+  auto test = [&](uint32_t j, float4 xj) {
+    if (dot_rn(xi - xyz(xj)) < hsq) {
       if (cnt < kMaxNbr) {
-        V.nbr[(size_t)cnt * n + k] = j;
+        out[(size_t)cnt * n] = j;
         ++cnt;
       } else {
         over = true;
-        return false;
       }
     }
-    return true;
-  });
+  };
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    uint32_t j = rs[r];
+    const uint32_t e = re[r];
+    for (; j + kNbrUnroll <= e && !over; j += kNbrUnroll) {
+      float4 xj[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q)
+        if (!over) test(j + q, xj[q]);
+    }
+    for (; j < e && !over; ++j) test(j, __ldg(V.cur.xs + j));
+  }
   V.ncount[k] = cnt;
   if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
 }
