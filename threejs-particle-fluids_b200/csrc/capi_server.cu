@@ -94,6 +94,9 @@ struct pf_server {
   double busy_ms = 0;
   std::vector<float> tick_ms;
   bool blocked = false;  // the last build ran out of memory: wait for a cohort to free
+  std::string last_error;
+  bool have_tuning = false;  // the first cohort's autotuned neighbour path, reused by later cohorts
+  uint32_t tune_path = 0, tune_block = 256;
 
   ~pf_server() {
     if (build && build->result.valid()) build->result.wait();
@@ -132,14 +135,16 @@ pf_status swap_in(pf_server* S) {
     for (Cohort* f : B.folded) f->folding = false;
     S->used -= B.reserved;
     S->build.reset();
-    if (st == PF_ERR_OOM) {
-      S->blocked = true;
+    S->last_error = err;
+    if (st == PF_ERR_OOM && !S->cohorts.empty()) {
+      S->blocked = true;  // retried once a live cohort retires and frees its memory
       return PF_OK;
     }
     return fail(st, "server: cohort build failed: " + err);
   }
   Cohort& C = *B.cohort;
   World& W = *C.world;
+  if (S->have_tuning) W.set_tuning(S->tune_path, S->tune_block);
   for (uint32_t j = 0; j < B.members.size(); ++j) {
     Request* r = B.members[j];
     if (r->state == PF_REQ_LIVE) {
@@ -358,13 +363,19 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   if (!(dt > 0)) return fail(PF_ERR_INVALID, "server: dt must be positive");
   const auto t0 = Clock::now();
   if (build_ready(S)) PF_TRY(swap_in(S));
-  PF_TRY(admit(S));
-  if (!S->opts.async_build && S->build) PF_TRY(swap_in(S));
+  if (!S->opts.async_build || S->opts.mode == PF_SERVER_PLAIN) {
+    PF_TRY(admit(S));
+    if (S->build) PF_TRY(swap_in(S));
+  }
   bool stepped = false;
   const bool plain = S->opts.mode == PF_SERVER_PLAIN;
   for (auto& c : S->cohorts)
     if (c->live) {
       PF_TRY(c->world->step(dt));
+      if (!S->have_tuning && c->world->tuned() && c->world->has_fluid()) {
+        c->world->tuning(&S->tune_path, &S->tune_block);
+        S->have_tuning = true;
+      }
       // the per-scene loop steps one scene and waits for it
       if (plain) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
       stepped = true;
@@ -407,6 +418,9 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     }
   }
   if (freed) S->blocked = false;
+  // An asynchronous build starts after this tick's steps (and their first-step
+  // graph captures), and runs on the worker thread while the next ticks go on.
+  if (S->opts.async_build && S->opts.mode != PF_SERVER_PLAIN) PF_TRY(admit(S));
   S->ticks++;
   if (stepped) {  // latency statistics cover ticks that stepped at least one scene
     const double ms = ms_since(t0);

@@ -1259,10 +1259,12 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   bytes_ = probe.off + al256(sort_bytes);
   if (plan_only) return PF_OK;
   (void)sm_count();  // cache the SM count outside any stream capture
-  if (cudaMalloc(&arena_, bytes_) != cudaSuccess) {
+  if (const cudaError_t e = cudaMalloc(&arena_, bytes_); e != cudaSuccess) {
     cudaGetLastError();
     arena_ = nullptr;
-    return fail(PF_ERR_OOM, "SimLoop: out of device memory (" + std::to_string(bytes_) + " bytes)");
+    if (e == cudaErrorMemoryAllocation)
+      return fail(PF_ERR_OOM, "SimLoop: out of device memory (" + std::to_string(bytes_) + " bytes)");
+    return fail(PF_ERR_CUDA, std::string("SimLoop: device allocation failed: ") + cudaGetErrorString(e));
   }
   Carver cv{static_cast<char*>(arena_)};
   layout(cv);
@@ -1474,7 +1476,7 @@ pf_status World::tune() {
     nbr_path_ = c.path;
     slot_block_ = c.block;
     float t = 0;
-    for (int rep = 0; rep < 3; ++rep) {
+    for (int rep = 0; rep < 2; ++rep) {
       PF_CUDA(cudaEventRecord(ev0_, stream_));
       // one substep's worth: the list once, density/lambda + delta per iteration
       run_fluid_neighbors(V, 0);
@@ -1646,18 +1648,21 @@ pf_status World::step(double dt) {
     }
   };
   if (use_graph_) {
-    cudaGraphExec_t& g = graph_[parity_];
-    if (!g) {
+    // Both start parities are captured on the first step, so later steps
+    // only launch (no capture runs while a host thread builds another world).
+    for (uint32_t p : {parity_, parity_ ^ flips}) {
+      cudaGraphExec_t& g = graph_[p];
+      if (g) continue;
       cudaGraph_t graph;
       PF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      body(parity_);
+      body(p);
       launches_per_step_ = t_launches;
       PF_CUDA(cudaStreamEndCapture(stream_, &graph));
       const cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) return fail(PF_ERR_CUDA, std::string("SimLoop: graph instantiate: ") + cudaGetErrorString(e));
     }
-    PF_CUDA(cudaGraphLaunch(g, stream_));
+    PF_CUDA(cudaGraphLaunch(graph_[parity_], stream_));
   } else {
     body(parity_);
     launches_per_step_ = t_launches;

@@ -316,6 +316,15 @@ class World {
     *path = nbr_path_;
     *block = slot_block_;
   }
+  bool tuned() const { return tuned_; }
+  bool has_fluid() const { return any_fluid_; }
+  // Use a configuration tuned elsewhere (another world of the same kind of
+  // scenes) instead of timing candidates on the first step.
+  void set_tuning(uint32_t path, uint32_t block) {
+    nbr_path_ = path;
+    slot_block_ = block;
+    tuned_ = true;
+  }
   size_t device_bytes() const { return bytes_; }
 
  private:
