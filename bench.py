@@ -479,6 +479,8 @@ class ServeWorkload:
                 "plain_p99_tick_ms": p["p99"] if p else None,
                 "served_over_plain": (b["value"] / p["value"]) if p else None,
                 "requests": len(stream), "cohort_builds": b["stats"]["rebuilds"],
+                "max_swap_ms": b["stats"]["max_swap_ms"], "max_admit_ms": b["stats"]["max_admit_ms"],
+                "plain_max_admit_ms": p["stats"]["max_admit_ms"] if p else None,
                 "live_at_end": b["stats"]["live"], "queued_at_end": b["stats"]["queued"],
             },
         }

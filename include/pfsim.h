@@ -396,6 +396,8 @@ typedef struct pf_server_stats {
   float p50_tick_ms;
   float p99_tick_ms;
   float max_tick_ms;
+  float max_swap_ms;          /* longest swap-in of a built cohort (imports, frees) */
+  float max_admit_ms;         /* longest admission (synchronous builds included) */
 } pf_server_stats;
 
 /* Request states reported by pf_server_request_state. */

@@ -93,10 +93,11 @@ struct pf_server {
   uint32_t finished = 0;
   double busy_ms = 0;
   std::vector<float> tick_ms;
+  float max_swap_ms = 0, max_admit_ms = 0;
   bool blocked = false;  // the last build ran out of memory: wait for a cohort to free
   std::string last_error;
   bool have_tuning = false;  // the first cohort's autotuned neighbour path, reused by later cohorts
-  uint32_t tune_path = 0, tune_block = 256;
+  uint32_t tune_path = 0, tune_block = 256, tune_unroll = 4;
 
   ~pf_server() {
     if (build && build->result.valid()) build->result.wait();
@@ -144,7 +145,7 @@ pf_status swap_in(pf_server* S) {
   }
   Cohort& C = *B.cohort;
   World& W = *C.world;
-  if (S->have_tuning) W.set_tuning(S->tune_path, S->tune_block);
+  if (S->have_tuning) W.set_tuning(S->tune_path, S->tune_block, S->tune_unroll);
   for (uint32_t j = 0; j < B.members.size(); ++j) {
     Request* r = B.members[j];
     if (r->state == PF_REQ_LIVE) {
@@ -362,10 +363,15 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   if (!S) return fail(PF_ERR_INVALID, "server: NULL");
   if (!(dt > 0)) return fail(PF_ERR_INVALID, "server: dt must be positive");
   const auto t0 = Clock::now();
-  if (build_ready(S)) PF_TRY(swap_in(S));
+  if (build_ready(S)) {
+    PF_TRY(swap_in(S));
+    S->max_swap_ms = std::max(S->max_swap_ms, (float)ms_since(t0));
+  }
   if (!S->opts.async_build || S->opts.mode == PF_SERVER_PLAIN) {
+    const auto ta = Clock::now();
     PF_TRY(admit(S));
     if (S->build) PF_TRY(swap_in(S));
+    S->max_admit_ms = std::max(S->max_admit_ms, (float)ms_since(ta));
   }
   bool stepped = false;
   const bool plain = S->opts.mode == PF_SERVER_PLAIN;
@@ -373,7 +379,7 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     if (c->live) {
       PF_TRY(c->world->step(dt));
       if (!S->have_tuning && c->world->tuned() && c->world->has_fluid()) {
-        c->world->tuning(&S->tune_path, &S->tune_block);
+        c->world->tuning(&S->tune_path, &S->tune_block, &S->tune_unroll);
         S->have_tuning = true;
       }
       // the per-scene loop steps one scene and waits for it
@@ -420,7 +426,11 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   if (freed) S->blocked = false;
   // An asynchronous build starts after this tick's steps (and their first-step
   // graph captures), and runs on the worker thread while the next ticks go on.
-  if (S->opts.async_build && S->opts.mode != PF_SERVER_PLAIN) PF_TRY(admit(S));
+  if (S->opts.async_build && S->opts.mode != PF_SERVER_PLAIN) {
+    const auto ta = Clock::now();
+    PF_TRY(admit(S));
+    S->max_admit_ms = std::max(S->max_admit_ms, (float)ms_since(ta));
+  }
   S->ticks++;
   if (stepped) {  // latency statistics cover ticks that stepped at least one scene
     const double ms = ms_since(t0);
@@ -469,6 +479,8 @@ pf_status pf_server_stats_read(pf_server* S, pf_server_stats* o) {
     o->p99_tick_ms = pct(0.99);
     o->max_tick_ms = t.back();
   }
+  o->max_swap_ms = S->max_swap_ms;
+  o->max_admit_ms = S->max_admit_ms;
   return PF_OK;
 }
 

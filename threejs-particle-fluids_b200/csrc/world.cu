@@ -1424,11 +1424,19 @@ void World::launch_fluid(K kernel, A... args) {
   ++t_launches;
 }
 
+// The slot kernels at the tuned fetch depth.
+#define PF_BY_UNROLL(K, ...)                                  \
+  do {                                                        \
+    if (slot_unroll_ == 2) launch_fluid(K<2>, __VA_ARGS__);   \
+    else if (slot_unroll_ == 8) launch_fluid(K<8>, __VA_ARGS__); \
+    else launch_fluid(K<4>, __VA_ARGS__);                     \
+  } while (0)
+
 void World::run_fluid_neighbors(const WorldView& V, uint32_t s) {
   if (nbr_path_ == 1) {
     launch_tiles_build(V, s);
   } else {
-    launch_fluid(k_s_neighbors, V, s);
+    PF_BY_UNROLL(k_s_neighbors, V, s);
   }
 }
 
@@ -1437,8 +1445,8 @@ void World::run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, u
     launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
     launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
   } else {
-    launch_fluid(k_s_lambda, V, r, s, it);
-    launch_fluid(k_s_delta, V, r, s, it);
+    PF_BY_UNROLL(k_s_lambda, V, r, s, it);
+    PF_BY_UNROLL(k_s_delta, V, r, s, it);
   }
 }
 
@@ -1446,7 +1454,7 @@ void World::run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s) {
   if (nbr_path_ == 1) {
     launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
   } else {
-    launch_fluid(k_s_xsph, V, r, s);
+    PF_BY_UNROLL(k_s_xsph, V, r, s);
   }
 }
 
@@ -1462,19 +1470,23 @@ pf_status World::tune() {
     nbr_path_ = (uint32_t)std::atoi(e) == 1 ? 1u : 0u;
     if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) slot_block_ = (uint32_t)std::atoi(b);
     if (slot_block_ != 128 && slot_block_ != 256 && slot_block_ != 512) slot_block_ = 256;
+    if (const char* u = std::getenv("PFSIM_SLOT_UNROLL")) slot_unroll_ = (uint32_t)std::atoi(u);
+    if (slot_unroll_ != 2 && slot_unroll_ != 8) slot_unroll_ = 4;
     return PF_OK;
   }
   run_sort_and_permute(parity_, false);
   parity_ ^= 1;
   const WorldView V = view(parity_);
   const uint32_t rank = h_fluids_[0].rank;
-  struct Cand { uint32_t path, block; };
-  const Cand cands[] = {{0, 128}, {0, 256}, {0, 512}, {1, 128}};
+  struct Cand { uint32_t path, block, unroll; };
+  const Cand cands[] = {{0, 128, 4}, {0, 256, 4}, {0, 512, 4}, {0, 128, 2}, {0, 256, 2},
+                        {0, 128, 8}, {0, 256, 8}, {1, 128, 4}};
   float best = 1e30f;
-  Cand pick = {0, 256};
+  Cand pick = {0, 256, 4};
   for (const Cand& c : cands) {
     nbr_path_ = c.path;
     slot_block_ = c.block;
+    slot_unroll_ = c.unroll;
     float t = 0;
     for (int rep = 0; rep < 2; ++rep) {
       PF_CUDA(cudaEventRecord(ev0_, stream_));
@@ -1496,6 +1508,7 @@ pf_status World::tune() {
   }
   nbr_path_ = pick.path;
   slot_block_ = pick.block;
+  slot_unroll_ = pick.unroll;
   return PF_OK;
 }
 
@@ -1904,19 +1917,19 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
     switch (stage) {
       case 0:
         if (nbr_path_ == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
-        else launch_fluid(k_s_neighbors, V, 0u);
+        else PF_BY_UNROLL(k_s_neighbors, V, 0u);
         break;
       case 1:
         if (nbr_path_ == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
-        else launch_fluid(k_s_lambda, V, rank, 0u, 0u);
+        else PF_BY_UNROLL(k_s_lambda, V, rank, 0u, 0u);
         break;
       case 2:
         if (nbr_path_ == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
-        else launch_fluid(k_s_delta, V, rank, 0u, 0u);
+        else PF_BY_UNROLL(k_s_delta, V, rank, 0u, 0u);
         break;
       case 3:
         if (nbr_path_ == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
-        else launch_fluid(k_s_xsph, V, rank, 0u);
+        else PF_BY_UNROLL(k_s_xsph, V, rank, 0u);
         break;
       case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
       default: break;

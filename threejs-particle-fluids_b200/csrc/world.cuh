@@ -311,18 +311,21 @@ class World {
   // current state (substep 0, iteration 0, material rank 0).
   pf_status profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_t* items);
   // Neighbour-pass configuration the autotuner chose (path 0: one thread
-  // per slot with `block` threads per block; path 1: warp tiles).
-  void tuning(uint32_t* path, uint32_t* block) const {
+  // per slot, `block` threads per block, list entries fetched `unroll` at a
+  // time; path 1: warp tiles).
+  void tuning(uint32_t* path, uint32_t* block, uint32_t* unroll = nullptr) const {
     *path = nbr_path_;
     *block = slot_block_;
+    if (unroll) *unroll = slot_unroll_;
   }
   bool tuned() const { return tuned_; }
   bool has_fluid() const { return any_fluid_; }
   // Use a configuration tuned elsewhere (another world of the same kind of
   // scenes) instead of timing candidates on the first step.
-  void set_tuning(uint32_t path, uint32_t block) {
+  void set_tuning(uint32_t path, uint32_t block, uint32_t unroll) {
     nbr_path_ = path;
     slot_block_ = block;
+    slot_unroll_ = unroll;
     tuned_ = true;
   }
   size_t device_bytes() const { return bytes_; }
@@ -371,7 +374,7 @@ class World {
   uint32_t parity_ = 0;
   bool inited_ = false;
   // neighbour passes: autotuned once per world, before the first graph capture
-  uint32_t nbr_path_ = 0, slot_block_ = 256;
+  uint32_t nbr_path_ = 0, slot_block_ = 256, slot_unroll_ = 4;
   bool tuned_ = false;
   // graph
   bool use_graph_ = false;

@@ -5,25 +5,27 @@
 // order, so a warp's gathers fall on a few hundred consecutive slots that L1
 // holds. The neighbour list stores slots (32 bits), column-major, so a warp
 // reads its m-th entries as one coalesced line. The loops fetch the list and
-// the neighbours four at a time before using them: four independent loads in
+// the neighbours several at a time before using them: independent loads in
 // flight per round instead of a dependent load per neighbour, with the sums
 // still formed in list order.
 //
-// The other neighbour path (world_tiles.cuh) stages tiles through shared
-// memory; the autotuner of World::tune picks one per world.
+// The depth of that fetch (kNbrUnroll: 2, 4 or 8 entries per round) trades
+// loads in flight against registers and so occupancy; the autotuner of
+// World::tune picks it, the block size, and this path or the warp-tile path
+// (world_tiles.cuh) per world.
 #pragma once
 
 #include "world_kernels.cuh"
 
 namespace pf {
 
-constexpr uint32_t kNbrUnroll = 4;
 
 // neighborList.ts:48-71: up to 64 neighbours within h at the predicted
 // positions of this substep, in walk order (query.ts:37-66: rows dz, dy;
 // inside a row ascending cell, inside a cell ascending index), self
 // included. The nine row ranges are fetched first, then each row's
-// candidates four at a time.
+// candidates several at a time.
+template <uint32_t kNbrUnroll>
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -49,39 +51,42 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
     rs[r] = __ldg(V.cstart + row + x0);
     re[r] = __ldg(V.cstart + row + x1) + __ldg(V.ccount + row + x1);
   }
+  // Every candidate is tested; the first kMaxNbr hits in walk order are
+  // stored (as the reference's list keeps them) and any further hit only
+  // marks the overflow.
   uint32_t cnt = 0;
-  bool over = false;
   const size_t n = V.n;
   uint32_t* __restrict__ out = V.nbr + k;
   auto test = [&](uint32_t j, float4 xj) {
     if (dot_rn(xi - xyz(xj)) < hsq) {
       if (cnt < kMaxNbr) {
-        out[(size_t)cnt * n] = j;
-        ++cnt;
-      } else {
-        over = true;
+        *out = j;
+        out += n;
       }
+      ++cnt;
     }
   };
 #pragma unroll
   for (int r = 0; r < 9; ++r) {
     uint32_t j = rs[r];
     const uint32_t e = re[r];
-    for (; j + kNbrUnroll <= e && !over; j += kNbrUnroll) {
+    for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
       float4 xj[kNbrUnroll];
 #pragma unroll
       for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
 #pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q)
-        if (!over) test(j + q, xj[q]);
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
     }
-    for (; j < e && !over; ++j) test(j, __ldg(V.cur.xs + j));
+    for (; j < e; ++j) test(j, __ldg(V.cur.xs + j));
   }
+  const bool over = cnt > kMaxNbr;
+  cnt = min(cnt, kMaxNbr);
   V.ncount[k] = cnt;
   if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
 }
 
 // lambda.ts:41-71
+template <uint32_t kNbrUnroll>
 __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -139,6 +144,7 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
 
 // positionDelta.ts:41-85 (the reaction on dynamic boundary neighbours goes
 // into the fixed-point reaction sums by slot).
+template <uint32_t kNbrUnroll>
 __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -195,6 +201,7 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
 }
 
 // velocity.ts:43-70 (XSPH): committed positions and velocities.
+template <uint32_t kNbrUnroll>
 __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;

@@ -207,6 +207,8 @@ class ServerStats(C.Structure):
         ("p50_tick_ms", C.c_float),
         ("p99_tick_ms", C.c_float),
         ("max_tick_ms", C.c_float),
+        ("max_swap_ms", C.c_float),
+        ("max_admit_ms", C.c_float),
     ]
 
 
