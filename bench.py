@@ -242,6 +242,7 @@ class BatchWorkload:
     # algorithmic bytes per fluid particle of the density+lambda stage:
     # read x* (16 B) and the boundary volume (4 B), write lambda and density (4 B each)
     LAMBDA_BYTES = 28
+    LAMBDA_TRAFFIC_PER_PARTICLE = 156.2e6 / 960_919
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -315,6 +316,8 @@ class BatchWorkload:
         # ---- dominant stage, timed live on the batch stream
         st_ms, items = C.c_float(0), C.c_uint64(0)
         N.check(L.pf_batch_profile_stage(batch.h, 1, 20, C.byref(st_ms), C.byref(items)))
+        tp, tb, tu = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+        N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu)))
         # ---- end to end: per step the scene parameters go host->device (pinned)
         # and every scene's positions come back to pinned host memory
         total = sum(r.capacity for r in recipes)
@@ -342,8 +345,13 @@ class BatchWorkload:
             "ms": ms,
             "units_per_step": psub,
             "kernel_ms": st_ms.value,
-            "kernel_name": "k_lambda (density + lambda, one solver iteration)",
+            "kernel_name": ("k_t_lambda" if tp.value == 1 else f"k_s_lambda<{tu.value}>")
+            + " (density + lambda, one solver iteration)",
             "algorithmic_bytes": self.LAMBDA_BYTES * items.value,
+            # DRAM bytes of one launch: the per-fluid-particle figure of the ncu
+            # capture (profiles/k_s_lambda_batch32_full.md: 156.2 MB over 960,919
+            # fluid particles) scaled to this launch's fluid particles
+            "traffic": self.LAMBDA_TRAFFIC_PER_PARTICLE * items.value if tp.value == 0 else None,
             "gpu_launches_per_step": launches,
             "clocks": clk,
             "e2e_ms": e2e_ms,
@@ -358,6 +366,8 @@ class BatchWorkload:
                 "plain_wall_ms_per_step": seq_wall if plain_baseline else float("nan"),
                 "plain_overlapped_ms_per_step": overlap_ms,
                 "batched_over_plain_overlapped": overlap_ms / ms,
+                "tuning": {"nbr_path": "tiles" if tp.value == 1 else "slots", "block": tb.value,
+                           "fetch_depth": tu.value},
                 "scenes": len(recipes),
                 "particles": total,
                 "fluid_particles": int(items.value),
@@ -597,7 +607,8 @@ def main() -> None:
         "dtype": "u32", "data": "synthetic (seeded)",
         "config": {"workload": wl.name, "inputs_larger_than_l2": True, "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": res["kernel_name"], "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None},
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": res.get("traffic")},
         "e2e": {"value": res["units_per_step"] * world / (e2e_ms * 1e-3), "unit": wl.unit,
                 "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": res["gpu_launches_per_step"] * args.steps,

@@ -358,6 +358,10 @@ PF_API pf_status pf_batch_read_positions(pf_batch* batch, float* dst_host, size_
  * that the next pf_batch_step reads. */
 PF_API pf_status pf_batch_profile_stage(pf_batch* batch, uint32_t stage, uint32_t reps, float* ms,
                                         uint64_t* items);
+/* The fluid neighbour-pass configuration the autotuner chose on the batch's
+ * first step: path 0 = one thread per slot (block threads per block, list
+ * entries fetched `unroll` at a time), 1 = warp tiles. */
+PF_API pf_status pf_batch_tuning(pf_batch* batch, uint32_t* path, uint32_t* block, uint32_t* unroll);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching under an HBM budget                           */

@@ -598,6 +598,12 @@ pf_status pf_batch_read_positions(pf_batch* b, float* dst_host, size_t bytes) {
   return b->world->read_positions(dst_host, bytes);
 }
 
+pf_status pf_batch_tuning(pf_batch* b, uint32_t* path, uint32_t* block, uint32_t* unroll) {
+  if (!b || !path || !block || !unroll) return fail(PF_ERR_INVALID, "batch: NULL");
+  b->world->tuning(path, block, unroll);
+  return PF_OK;
+}
+
 pf_status pf_batch_profile_stage(pf_batch* b, uint32_t stage, uint32_t reps, float* ms, uint64_t* items) {
   if (!b || !ms) return fail(PF_ERR_INVALID, "batch: NULL");
   return b->world->profile_stage(stage, reps, ms, items);

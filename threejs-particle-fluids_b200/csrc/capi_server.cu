@@ -208,14 +208,18 @@ pf_status start_build(pf_server* S, std::vector<Request*> fresh, std::vector<Coh
   B->cohort->world = std::make_unique<World>();
   S->used += reserve;
   std::vector<SceneSpec*> specs;
-  for (Request* r : B->members) specs.push_back(r->spec.get());
+  std::vector<uint8_t> imported;  // folded scenes get their state by import at the swap
+  for (Request* r : B->members) {
+    specs.push_back(r->spec.get());
+    imported.push_back(r->state == PF_REQ_LIVE ? 1 : 0);
+  }
   World* W = B->cohort->world.get();
   Cohort* C = B->cohort.get();
   const bool graph = S->opts.mode == PF_SERVER_BATCHED && S->opts.use_graph;
   const int dev = S->device;
-  auto job = [W, C, specs, graph, dev]() -> std::pair<pf_status, std::string> {
+  auto job = [W, C, specs, imported, graph, dev]() -> std::pair<pf_status, std::string> {
     cudaSetDevice(dev);
-    const pf_status st = W->build(specs, graph);
+    const pf_status st = W->build(specs, graph, false, &imported);
     if (st != PF_OK) return {st, get_error()};
     C->bytes = W->device_bytes();
     return {PF_OK, std::string()};

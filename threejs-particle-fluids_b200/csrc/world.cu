@@ -719,6 +719,19 @@ __global__ void __launch_bounds__(kBlock) k_gather_positions(WorldView V, const 
   out[prefix[s] + local] = make_float4(x.x, x.y, x.z, 0.0f);
 }
 
+// Fresh slot maps (ids = inv = identity) and identity orientations.
+__global__ void __launch_bounds__(kBlock) k_init_slots(uint32_t* __restrict__ ids, uint32_t* __restrict__ inv,
+                                                       float4* __restrict__ q, float4* __restrict__ qp, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ids[i] = i;
+  inv[i] = i;
+  if (q) {
+    q[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    qp[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  }
+}
+
 // Dynamic state of one scene from another world, by particle index, written
 // the way build() writes a spec's state (x* = x, q* = q, zero w lanes).
 __global__ void __launch_bounds__(kBlock) k_import_scene(WorldView V, uint32_t seg, uint32_t cap,
@@ -834,7 +847,8 @@ DevSdf make_dev_sdf(const SdfSpec& g, uint32_t data_off) {
   return d;
 }
 
-pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only) {
+pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only,
+                       const std::vector<uint8_t>* skip_state) {
   specs_ = specs;
   use_graph_ = use_graph;
   const uint32_t K = (uint32_t)specs.size();
@@ -1133,27 +1147,11 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   std::vector<uint32_t> chunk(n_ / kSegAlign, 0);
   for (uint32_t s = 0; s < K; ++s)
     for (uint32_t c = h_scenes_[s].seg_start / kSegAlign; c < h_scenes_[s].seg_end / kSegAlign; ++c) chunk[c] = s;
-  std::vector<float4> x(n_), v(n_), q(n_), om(n_);
-  std::vector<float> bv(n_, 0.0f), dens(n_, 0.0f);
-  std::vector<uint32_t> tag(n_, 0), ids(n_);
-  for (uint32_t i = 0; i < n_; ++i) {
-    x[i] = make_float4(0, 0, 0, 0);
-    v[i] = make_float4(0, 0, 0, 0);
-    q[i] = make_float4(0, 0, 0, 1);
-    om[i] = make_float4(0, 0, 0, 0);
-    ids[i] = i;
-  }
+  std::vector<float> dens(n_, 0.0f);
+  std::vector<uint32_t> tag(n_, 0);
   for (uint32_t s = 0; s < K; ++s) {
     const SceneSpec& sp = *specs[s];
     const uint32_t base = h_scenes_[s].seg_start;
-    for (uint32_t i = 0; i < sp.cap; ++i) {
-      x[base + i] = make_float4(sp.pos4[4 * i], sp.pos4[4 * i + 1], sp.pos4[4 * i + 2], sp.inv_mass[i]);
-      v[base + i] = make_float4(sp.vel4[4 * i], sp.vel4[4 * i + 1], sp.vel4[4 * i + 2], 0.0f);
-      bv[base + i] = sp.bvol[i];
-      if (!sp.rot4.empty())
-        q[base + i] = make_float4(sp.rot4[4 * i], sp.rot4[4 * i + 1], sp.rot4[4 * i + 2], sp.rot4[4 * i + 3]);
-      if (!sp.angv4.empty()) om[base + i] = make_float4(sp.angv4[4 * i], sp.angv4[4 * i + 1], sp.angv4[4 * i + 2], 0.0f);
-    }
     for (uint32_t f = 0; f < h_scenes_[s].fluid_count; ++f) {
       const FluidSpec& fs = sp.fluids[f];
       for (uint32_t i = fs.range.start; i < fs.range.start + fs.range.count; ++i) {
@@ -1311,13 +1309,41 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         off += g.half.size();
       }
   }
-  PF_TRY(up(buf_[0].x, x.data(), 16 * N));
-  PF_TRY(up(buf_[0].xs, x.data(), 16 * N));
-  PF_TRY(up(buf_[0].v, v.data(), 16 * N));
-  PF_TRY(up(buf_[0].bv, bv.data(), 4 * N));
+  // identity slot maps and orientations on the device; the scenes' own state
+  // goes to their segments (scenes whose state is imported afterwards skip it)
+  k_init_slots<<<div_up(n_, kBlock), kBlock, 0, stream_>>>(base_.ids, base_.inv, base_.q, base_.qp, n_);
+  PF_CUDA(cudaGetLastError());
+  {
+    // pageable copies: the call returns once the source has been consumed,
+    // so the staging vectors can be refilled for the next scene
+    std::vector<float4> sx, sv, so;
+    for (uint32_t s = 0; s < K; ++s) {
+      if (skip_state && (*skip_state)[s]) continue;
+      const SceneSpec& sp = *specs[s];
+      const uint32_t base = h_scenes_[s].seg_start, cap = sp.cap;
+      sx.resize(cap);
+      sv.resize(cap);
+      for (uint32_t i = 0; i < cap; ++i) {
+        sx[i] = make_float4(sp.pos4[4 * i], sp.pos4[4 * i + 1], sp.pos4[4 * i + 2], sp.inv_mass[i]);
+        sv[i] = make_float4(sp.vel4[4 * i], sp.vel4[4 * i + 1], sp.vel4[4 * i + 2], 0.0f);
+      }
+      PF_TRY(up(buf_[0].x + base, sx.data(), 16ull * cap));
+      PF_TRY(up(buf_[0].xs + base, sx.data(), 16ull * cap));
+      PF_TRY(up(buf_[0].v + base, sv.data(), 16ull * cap));
+      PF_TRY(up(buf_[0].bv + base, sp.bvol.data(), 4ull * cap));
+      if (base_.q && !sp.rot4.empty()) {
+        PF_TRY(up(base_.q + base, sp.rot4.data(), 16ull * cap));
+        PF_TRY(up(base_.qp + base, sp.rot4.data(), 16ull * cap));
+      }
+      if (base_.omega && !sp.angv4.empty()) {
+        so.resize(cap);
+        for (uint32_t i = 0; i < cap; ++i)
+          so[i] = make_float4(sp.angv4[4 * i], sp.angv4[4 * i + 1], sp.angv4[4 * i + 2], 0.0f);
+        PF_TRY(up(base_.omega + base, so.data(), 16ull * cap));
+      }
+    }
+  }
   PF_TRY(up(buf_[0].tag, tag.data(), 4 * N));
-  PF_TRY(up(base_.ids, ids.data(), 4 * N));
-  PF_TRY(up(base_.inv, ids.data(), 4 * N));
   PF_TRY(up(base_.density, dens.data(), 4 * N));
   PF_TRY(up(base_.softs, h_softs_.data(), sizeof(DevSoft) * h_softs_.size()));
   PF_TRY(up(base_.bodies, h_bodies_.data(), sizeof(DevBody) * h_bodies_.size()));
@@ -1329,9 +1355,6 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     PF_TRY(up(base_.rest, rest4.data(), 16 * N));
     PF_TRY(up(base_.rest_c, restc4.data(), 16 * N));
     PF_TRY(up(base_.weights, weights.data(), 4 * N));
-    PF_TRY(up(base_.q, q.data(), 16 * N));
-    PF_TRY(up(base_.qp, q.data(), 16 * N));
-    PF_TRY(up(base_.omega, om.data(), 16 * N));
     std::vector<float4> ident(3 * h_bodies_.size());
     for (size_t b = 0; b < h_bodies_.size(); ++b) {
       ident[3 * b] = make_float4(1, 0, 0, 0);

@@ -280,7 +280,10 @@ class World {
   // Pack `specs` (their current host state) into device arrays. With
   // `plan_only` nothing touches the GPU: the layout is computed and
   // device_bytes() reports what the build would allocate.
-  pf_status build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only = false);
+  // `skip_state[s]` set: scene s's dynamic state is not uploaded (it is
+  // imported with import_scene before the first step).
+  pf_status build(const std::vector<SceneSpec*>& specs, bool use_graph, bool plan_only = false,
+                  const std::vector<uint8_t>* skip_state = nullptr);
   // Overwrite scene `s`'s dynamic state (positions with inverse mass,
   // velocities, boundary volumes, orientations, angular velocities) with
   // scene `src_s` of `src`, device to device. Both worlds hold the same
