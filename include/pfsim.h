@@ -164,6 +164,11 @@ PF_API pf_status pf_set_inv_mass(pf_scene* scene, pf_range range, float inv_mass
  * XSPH viscosity runs only when PF_FLUID_VISCOSITY is set, as optional effects
  * only compile in when given (FluidSystem.ts:111-115). */
 #define PF_FLUID_VISCOSITY 1u
+/* Vorticity confinement with strength `vorticity` (FluidSystemOptions.vorticity,
+ * FluidSystem.ts:48; velocity.ts:13-120): the curl is gathered in the XSPH
+ * walk, then eta = grad|omega| over fluid neighbours and
+ * v += vorticity * dt * (eta/|eta| x omega). */
+#define PF_FLUID_VORTICITY 2u
 typedef struct pf_fluid_desc {
   pf_range range;               /* count 0 = every particle */
   float rest_density;
@@ -175,6 +180,7 @@ typedef struct pf_fluid_desc {
   uint32_t n_boundaries;
   const pf_range* boundaries;   /* host, n_boundaries entries */
   const uint8_t* boundary_static; /* host or NULL: 1 = static boundary (addBoundary dynamic:false) */
+  float vorticity;              /* used when PF_FLUID_VORTICITY is set */
 } pf_fluid_desc;
 PF_API pf_status pf_add_fluid(pf_scene* scene, const pf_fluid_desc* desc, uint32_t* material_index);
 

@@ -283,15 +283,17 @@ struct Range {
 template <typename T>
 struct Fluid {
   Range range;
-  double restDensity, spacing, h, compliance, viscosity;
-  bool hasViscosity;
+  double restDensity, spacing, h, compliance, viscosity, vorticity = 0;
+  bool hasViscosity, hasVorticity = false;
   std::vector<Range> boundaries;
   std::vector<uint8_t> boundaryStatic;
   // uniforms at engine precision
-  T uRho0, uVolume, uMass, uH, uHSq, uPoly6, uSpiky, uCompliance, uC;
+  T uRho0, uVolume, uMass, uH, uHSq, uPoly6, uSpiky, uCompliance, uC, uEps = 0;
   // buffers (capacity sized like the reference)
   std::vector<T> density, lambda;
   std::vector<V3<T>> deltaX, deltaV;
+  std::vector<V3<T>> omega, eta;  // vorticity confinement (velocity.ts:13-21)
+  std::vector<T> omegaLength;
   std::vector<uint32_t> nbrIdx, nbrCount;  // column-major k*count + local
   uint32_t nbrOverflow = 0;
   bool hasReaction = false;
@@ -624,25 +626,56 @@ struct Engine {
   }
 
   // velocity.ts:36-120 (XSPH only; vorticity is not part of this path)
-  void fluid_xsph(Fluid<T>& f) {
+  // velocity.ts:36-120: one walk for the curl (vorticity) and the XSPH
+  // change, the gradient of |omega| over fluid neighbours, then the apply.
+  void fluid_velocity(Fluid<T>& f) {
     const uint32_t rc = f.range.count;
+    const bool vort = f.hasVorticity, visc = f.hasViscosity;
     parallel_for(0, static_cast<int64_t>(rc), [&](int64_t li) {
       const uint32_t local = static_cast<uint32_t>(li), i = f.range.start + local;
       const V3<T> xi = p3(pos, i), vi = p3(vel, i);
-      V3<T> smoothing = v3<T>(0, 0, 0);
+      V3<T> curl = v3<T>(0, 0, 0), smoothing = v3<T>(0, 0, 0);
       const uint32_t nc = f.nbrCount[local];
       for (uint32_t k = 0; k < nc; ++k) {
         const uint32_t j = f.nbrIdx[static_cast<size_t>(k) * rc + local];
         const V3<T> off = xi - p3(pos, j);
         const V3<T> vj = p3(vel, j);
         const T volume = bvol[j] > 0 ? bvol[j] : f.uVolume;
-        smoothing = smoothing + ((vj - vi) * poly6(dot(off, off), f)) * volume;
+        if (vort) curl = curl + cross(vi - vj, spiky_grad(off, f)) * volume;
+        if (visc) smoothing = smoothing + ((vj - vi) * poly6(dot(off, off), f)) * volume;
       }
-      f.deltaV[i] = smoothing * f.uC;
+      if (vort) {
+        f.omega[i] = curl;
+        f.omegaLength[i] = length(curl);
+      }
+      if (visc) f.deltaV[i] = smoothing * f.uC;
     });
+    if (vort) {
+      // velocity.ts:75-92: eta = sum over fluid neighbours of grad W (|w_j| - |w_i|) V
+      parallel_for(0, static_cast<int64_t>(rc), [&](int64_t li) {
+        const uint32_t local = static_cast<uint32_t>(li), i = f.range.start + local;
+        const V3<T> xi = p3(pos, i);
+        const T wi = f.omegaLength[i];
+        V3<T> e = v3<T>(0, 0, 0);
+        const uint32_t nc = f.nbrCount[local];
+        for (uint32_t k = 0; k < nc; ++k) {
+          const uint32_t j = f.nbrIdx[static_cast<size_t>(k) * rc + local];
+          if (bvol[j] > 0) continue;
+          e = e + spiky_grad(xi - p3(pos, j), f) * ((f.omegaLength[j] - wi) * f.uVolume);
+        }
+        f.eta[i] = e;
+      });
+    }
+    // velocity.ts:99-120
     for (uint32_t li = 0; li < rc; ++li) {
       const uint32_t i = f.range.start + li;
-      const V3<T> change = v3<T>(0, 0, 0) + f.deltaV[i];
+      V3<T> change = v3<T>(0, 0, 0);
+      if (vort) {
+        const V3<T> e = f.eta[i];
+        const T el = length(e);
+        if (el >= static_cast<T>(1e-12)) change = change + cross(e / el, f.omega[i]) * f.uEps * dt;
+      }
+      if (visc) change = change + f.deltaV[i];
       set3(vel, i, p3(vel, i) + change, vel[4 * i + 3]);
     }
   }
@@ -1348,7 +1381,7 @@ struct Engine {
     for (auto& m : materials) {
       if (m.first == MAT_FLUID) {
         Fluid<T>& f = fluids[m.second];
-        if (f.hasViscosity) fluid_xsph(f);
+        if (f.hasViscosity || f.hasVorticity) fluid_velocity(f);
       } else if (m.first == MAT_SOFT) {
         Softbodies<T>& sb = softs[m.second];
         if (sb.local) {
@@ -1605,6 +1638,8 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.compliance = d->compliance >= 0 ? d->compliance : 1e-4;
     f.hasViscosity = (d->flags & PF_FLUID_VISCOSITY) != 0;
     f.viscosity = d->viscosity;
+    f.hasVorticity = (d->flags & PF_FLUID_VORTICITY) != 0;
+    f.vorticity = d->vorticity;
     const double mass = f.restDensity * f.spacing * f.spacing * f.spacing;
     for (uint32_t b = 0; b < d->n_boundaries; ++b) {
       f.boundaries.push_back({d->boundaries[b].start, d->boundaries[b].count});
@@ -1623,6 +1658,7 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.uSpiky = U(45.0 / (M_PI * std::pow(f.h, 6)));
     f.uCompliance = U(f.compliance);
     f.uC = U(f.viscosity);
+    f.uEps = U(f.vorticity);
     // particles.setInvMass(range, 1 / mass) into a Float32Array.
     const float w = static_cast<float>(1.0 / mass);
     for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) e.invMass[i] = w;
@@ -1632,6 +1668,9 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.lambda.assign(e.cap, 0);
     f.deltaX.assign(e.cap, v3<T>(0, 0, 0));
     f.deltaV.assign(e.cap, v3<T>(0, 0, 0));
+    f.omega.assign(e.cap, v3<T>(0, 0, 0));
+    f.eta.assign(e.cap, v3<T>(0, 0, 0));
+    f.omegaLength.assign(e.cap, 0);
     f.nbrIdx.assign(static_cast<size_t>(f.range.count) * kMaxNeighbors, 0);
     f.nbrCount.assign(f.range.count, 0);
     f.hasReaction = !f.boundaries.empty();

@@ -115,3 +115,19 @@ def test_batched_equals_plain(cuda, use_graph):
     for i, s in enumerate(plain):
         assert np.array_equal(s.readback(N.PF_FIELD_POSITIONS), batch.readback(i, N.PF_FIELD_POSITIONS))
         assert np.array_equal(s.readback(N.PF_FIELD_VELOCITIES), batch.readback(i, N.PF_FIELD_VELOCITIES))
+
+
+@pytest.mark.parametrize("seed", [4, 9])
+def test_vorticity_confinement_one_frame(oracle, cuda, seed):
+    """FluidSystem with vorticity (velocity.ts:36-120): curl in the XSPH walk,
+    eta over fluid neighbours, eps (N x omega) dt added with the XSPH change."""
+    r = W.dam_break(5000, seed=seed)
+    r.materials[0][1].vorticity = 0.02
+    a, b = cuda.build(r), oracle.OracleBackend().build(r)
+    for _ in range(2):
+        a.step(DT)
+        b.step(DT)
+    xa, xb = a.readback(N.PF_FIELD_POSITIONS), b.readback(N.PF_FIELD_POSITIONS)
+    assert np.abs(xa - xb).max() <= POS_TOL
+    va, vb = a.readback(N.PF_FIELD_VELOCITIES), b.readback(N.PF_FIELD_VELOCITIES)
+    assert np.abs(va - vb).max() <= POS_TOL / (DT / r.loop.substeps)

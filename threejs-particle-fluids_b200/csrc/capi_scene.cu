@@ -220,6 +220,10 @@ pf_status pf_add_fluid(pf_scene* s, const pf_fluid_desc* d, uint32_t* mat) {
   f.viscosity = d->viscosity;
   if (f.has_visc && !std::isfinite(f.viscosity))
     return fail(PF_ERR_INVALID, "FluidSystem: viscosity must be finite");
+  f.has_vort = (d->flags & PF_FLUID_VORTICITY) != 0;
+  f.vorticity = f.has_vort ? d->vorticity : 0.0;
+  if (f.has_vort && !std::isfinite(f.vorticity))
+    return fail(PF_ERR_INVALID, "FluidSystem: vorticity must be finite");
   for (uint32_t b = 0; b < d->n_boundaries; ++b) {
     RangeU r{d->boundaries[b].start, d->boundaries[b].count};
     if (!range_ok(sp, r)) return fail(PF_ERR_INVALID, "FluidSystem.addBoundary: invalid particle range");

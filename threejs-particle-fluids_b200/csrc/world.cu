@@ -279,21 +279,28 @@ __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t ra
   if (changed) V.cur.xs[k] = x;
 }
 
-// velocity.ts:99-120: add the XSPH change to the velocity.
+// velocity.ts:99-120: the vorticity confinement force eps (N x omega) dt with
+// N = eta / |eta| (eta from k_s_vort_grad, in dx), then the XSPH change.
 __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank || !F.has_visc) return;
+  if (F.rank != rank || !(F.has_visc || F.has_vort)) return;
   const DevScene& S = scene_at(V, k);
   if (sub >= S.substeps) return;
-  const float4 d = V.dv[k];
+  f3 change = mk(0.0f, 0.0f, 0.0f);
+  if (F.has_vort) {
+    const f3 eta = xyz(V.dx[k]);
+    const float el = len(eta);
+    if (el >= 1e-12f) change = change + cross(eta / el, xyz(V.vort[k])) * F.vort_eps * S.dt;
+  }
+  if (F.has_visc) change = change + xyz(V.dv[k]);
   float4 v = V.cur.v[k];
-  v.x += 0.0f + d.x;
-  v.y += 0.0f + d.y;
-  v.z += 0.0f + d.z;
+  v.x += change.x;
+  v.y += change.y;
+  v.z += change.z;
   V.cur.v[k] = v;
 }
 
@@ -986,6 +993,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         F.compliance = f32(fs.compliance);
         F.c_xsph = f32(fs.viscosity);
         F.has_visc = fs.has_visc ? 1u : 0u;
+        F.has_vort = fs.has_vort ? 1u : 0u;
+        F.vort_eps = f32(fs.vorticity);
         F.bnd_first = (uint32_t)h_bnds_.size();
         F.bnd_count = (uint32_t)fs.bnd.size();
         uint32_t lo = UINT32_MAX, hi = 0;
@@ -1008,6 +1017,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         F.react_inv = S.pos_inv;
         any_fluid_ = true;
         any_visc_ = any_visc_ || fs.has_visc;
+        any_vort_ = any_vort_ || fs.has_vort;
         h_fluids_.push_back(F);
       } else if (kind == MAT_SOFT) {
         const SoftSpec& ss = sp.softs[idx];
@@ -1221,6 +1231,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.density = cv.take<float>(N);
     base_.dx = cv.take<float4>(N);
     base_.dv = cv.take<float4>(N);
+    base_.vort = any_vort_ ? cv.take<float4>(N) : nullptr;
     base_.plam = cv.take<float2>(N * P);
     base_.acc_react = any_react_ ? cv.take<int4>(N) : nullptr;
     base_.acc_soft = any_soft_local_ ? cv.take<int4>(N) : nullptr;
@@ -1490,7 +1501,7 @@ pf_status World::tune() {
   tuned_ = true;
   if (!any_fluid_ || n_ == 0) return PF_OK;
   if (const char* e = std::getenv("PFSIM_NBR_PATH")) {  // fixed choice for measurements
-    nbr_path_ = (uint32_t)std::atoi(e) == 1 ? 1u : 0u;
+    nbr_path_ = ((uint32_t)std::atoi(e) == 1 && !any_vort_) ? 1u : 0u;
     if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) slot_block_ = (uint32_t)std::atoi(b);
     if (slot_block_ != 128 && slot_block_ != 256 && slot_block_ != 512) slot_block_ = 256;
     if (const char* u = std::getenv("PFSIM_SLOT_UNROLL")) slot_unroll_ = (uint32_t)std::atoi(u);
@@ -1501,12 +1512,15 @@ pf_status World::tune() {
   parity_ ^= 1;
   const WorldView V = view(parity_);
   const uint32_t rank = h_fluids_[0].rank;
+  // the warp-tile path has no vorticity pass: worlds with it stay on slots
+  const uint32_t n_cands_max = any_vort_ ? 7u : 8u;
   struct Cand { uint32_t path, block, unroll; };
   const Cand cands[] = {{0, 128, 4}, {0, 256, 4}, {0, 512, 4}, {0, 128, 2}, {0, 256, 2},
                         {0, 128, 8}, {0, 256, 8}, {1, 128, 4}};
   float best = 1e30f;
   Cand pick = {0, 256, 4};
-  for (const Cand& c : cands) {
+  for (uint32_t ci = 0; ci < n_cands_max; ++ci) {
+    const Cand& c = cands[ci];
     nbr_path_ = c.path;
     slot_block_ = c.block;
     slot_unroll_ = c.unroll;
@@ -1516,7 +1530,7 @@ pf_status World::tune() {
       // one substep's worth: the list once, density/lambda + delta per iteration
       run_fluid_neighbors(V, 0);
       for (uint32_t it = 0; it < std::max(max_iter_, 1u); ++it) run_fluid_lambda_delta(V, rank, 0, 0);
-      if (any_visc_) run_fluid_xsph(V, rank, 0);
+      if (any_visc_ || any_vort_) run_fluid_xsph(V, rank, 0);
       PF_CUDA(cudaEventRecord(ev1_, stream_));
       PF_CUDA(cudaEventSynchronize(ev1_));
       float ms = 0;
@@ -1638,11 +1652,15 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   }
   launch_slots(k_advect, n_, stream_, V, s);
   for (uint32_t r = 0; r < max_rank_; ++r) {
-    bool has_visc = false, has_local = false;
-    for (auto& F : h_fluids_) has_visc = has_visc || (F.rank == r && F.has_visc);
+    bool has_velocity = false, has_vort = false, has_local = false;
+    for (auto& F : h_fluids_) {
+      has_velocity = has_velocity || (F.rank == r && (F.has_visc || F.has_vort));
+      has_vort = has_vort || (F.rank == r && F.has_vort);
+    }
     for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
-    if (has_visc) {
+    if (has_velocity) {
       run_fluid_xsph(V, r, s);
+      if (has_vort) PF_BY_UNROLL(k_s_vort_grad, V, r, s);
       launch_slots(k_xsph_apply, n_, stream_, V, r, s);
     }
     if (has_local) {

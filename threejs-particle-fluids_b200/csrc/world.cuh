@@ -42,8 +42,8 @@ struct RangeU {
 
 struct FluidSpec {
   RangeU range;
-  double rho0, spacing, h, compliance, viscosity;
-  bool has_visc;
+  double rho0, spacing, h, compliance, viscosity, vorticity = 0;
+  bool has_visc, has_vort = false;
   std::vector<RangeU> bnd;
   std::vector<uint8_t> bnd_static;
 };
@@ -143,6 +143,8 @@ struct DevFluid {
   uint32_t scene, rank;
   float rho0, inv_rho0, volume, h, hsq, poly6, spiky, compliance, c_xsph;
   uint32_t has_visc;
+  uint32_t has_vort;
+  float vort_eps;  // vorticity confinement strength
   uint32_t bnd_first, bnd_count;
   uint32_t react_lo, react_hi;  // covering id range of the boundaries (lo == hi: no reaction)
   float react_scale, react_inv;
@@ -236,6 +238,7 @@ struct WorldView {
   float* density;
   float4* dx;
   float4* dv;
+  float4* vort;       // curl of the velocity per slot, w = its length (vorticity confinement)
   float2* plam;       // (lambda_n, lambda_t) per slot x primitive
   int4* acc_react;    // fixed-point reaction sums per slot
   int4* acc_soft;     // fixed-point shape-matching sums per slot
@@ -363,7 +366,7 @@ class World {
   // stage plan
   uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
-  bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false;
+  bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false, any_vort_ = false;
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
   bool any_react_ = false;
   bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass

@@ -200,7 +200,9 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
   V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
 }
 
-// velocity.ts:43-70 (XSPH): committed positions and velocities.
+// velocity.ts:43-70: one walk over the list at the committed positions for
+// the XSPH change (Delta v = c sum V_j (v_j - v_i) W) and, with vorticity
+// confinement, the curl omega = sum V_j (v_i - v_j) x grad W.
 template <uint32_t kNbrUnroll>
 __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,19 +210,22 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
-  if (F.rank != rank || !F.has_visc) return;
+  const bool visc = F.has_visc, vort = F.has_vort;
+  if (F.rank != rank || !(visc || vort)) return;
   const DevScene& S = scene_at(V, k);
   if (sub >= S.substeps) return;
   const f3 xi = xyz(V.cur.x[k]);
   const f3 vi = xyz(V.cur.v[k]);
-  f3 sm = mk(0.0f, 0.0f, 0.0f);
+  f3 sm = mk(0.0f, 0.0f, 0.0f), curl = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
   auto one = [&](float4 xj, float4 vj, float bvj) {
     const f3 off = xi - xyz(xj);
     const float vol = bvj > 0.0f ? bvj : F.volume;
-    sm = sm + ((xyz(vj) - vi) * poly6(dot(off, off), F)) * vol;
+    const float rsq = dot(off, off);
+    if (vort) curl = curl + cross(vi - xyz(vj), spiky_vec(off, rsq, F)) * vol;
+    if (visc) sm = sm + ((xyz(vj) - vi) * poly6(rsq, F)) * vol;
   };
   uint32_t m = 0;
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
@@ -242,7 +247,35 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
     const uint32_t j = __ldg(nl + m * n);
     one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), __ldg(V.cur.bv + j));
   }
-  V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
+  if (visc) V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
+  if (vort) V.vort[k] = with_w(curl, len(curl));
+}
+
+// velocity.ts:75-92: eta = sum over fluid neighbours (no boundary volume) of
+// grad W (|omega_j| - |omega_i|) V, into dx (free after the iterations).
+template <uint32_t kNbrUnroll>
+__global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_vort) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const f3 xi = xyz(V.cur.x[k]);
+  const float wi = V.vort[k].w;
+  f3 eta = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    if (__ldg(V.cur.bv + j) > 0.0f) continue;
+    const f3 off = xi - xyz(__ldg(V.cur.x + j));
+    eta = eta + spiky_vec(off, dot(off, off), F) * ((V.vort[j].w - wi) * F.volume);
+  }
+  V.dx[k] = with_w(eta, 0.0f);
 }
 
 }  // namespace pf

@@ -25,6 +25,7 @@ PF_KEY_LINEAR = 0
 PF_KEY_MORTON = 1
 
 PF_FLUID_VISCOSITY = 1
+PF_FLUID_VORTICITY = 2
 PF_SHAPE_MATCH_GLOBAL = 0
 PF_SHAPE_MATCH_LOCAL = 1
 PF_PRIM_PLANE, PF_PRIM_SPHERE, PF_PRIM_BOX, PF_PRIM_CAPSULE = 0, 1, 2, 3
@@ -87,6 +88,7 @@ class FluidDesc(C.Structure):
         ("n_boundaries", C.c_uint32),
         ("boundaries", C.POINTER(Range)),
         ("boundary_static", C.POINTER(C.c_uint8)),
+        ("vorticity", C.c_float),
     ]
 
 

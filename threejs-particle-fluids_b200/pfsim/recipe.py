@@ -40,6 +40,7 @@ class FluidOpts:
     smoothing_radius: float = 0.0
     compliance: float = -1.0
     viscosity: float | None = None
+    vorticity: float | None = None
     boundaries: list[tuple[int, int]] = field(default_factory=list)
     boundary_static: list[bool] = field(default_factory=list)
 
@@ -238,6 +239,9 @@ def fluid_desc(o: FluidOpts, keep: _Keep) -> N.FluidDesc:
     if o.viscosity is not None:
         d.viscosity = o.viscosity
         d.flags |= N.PF_FLUID_VISCOSITY
+    if o.vorticity is not None:
+        d.vorticity = o.vorticity
+        d.flags |= N.PF_FLUID_VORTICITY
     if o.boundaries:
         arr = (N.Range * len(o.boundaries))(*[N.Range(s, c) for s, c in o.boundaries])
         keep.refs.append(arr)
