@@ -476,6 +476,29 @@ class ServeWorkload:
                 "p99": float(np.percentile(tick_ms, 99)), "clocks": clk, "stats": st,
                 "ps_per_tick": ps / ticks}
 
+    def run_cpu(self, threads: int, budget_particles: int = 150_000, steps: int = 2) -> dict:
+        """The oracle on the first requests of the same stream, up to
+        `budget_particles`, stepped `steps` ticks."""
+        from oracle import oracle as O
+
+        sample, n = [], 0
+        for _, rec, _ in self.stream(1):
+            if n >= budget_particles:
+                break
+            sample.append(rec)
+            n += rec.capacity
+        be = O.OracleBackend(threads=threads)
+        scenes = [be.build(r) for r in sample]
+        for sc in scenes:
+            sc.step(self.DT)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for sc in scenes:
+                sc.step(self.DT)
+        sec = (time.perf_counter() - t0) / steps
+        return {"seconds_per_step": sec, "units_per_step": sum(r.particle_substeps for r in sample), "cores": threads,
+                "sample": f"{len(sample)} requests ({n} particles) of the same stream, {steps} ticks"}
+
     def run_gpu(self, steps: int, warmup: int, rank: int, world: int, dist_barrier, plain_baseline=True) -> dict:
         stream = self.stream(warmup + steps + 1)
         b = self.serve(stream, steps, warmup, plain=False)
@@ -496,7 +519,64 @@ class ServeWorkload:
         }
 
 
-WORKLOADS = {"sort": SortWorkload, "batch": BatchWorkload, "serve": ServeWorkload}
+class SceneWorkload:
+    """One plain scene stepped through pf_step: `dam` is the 5,000-particle
+    dam break (2 substeps x 4 iterations, XSPH 0.01), `mixed` the 50,000-particle
+    fluid + 20 soft bodies + moving sphere scene (3 substeps x 4 iterations)."""
+
+    metric = "particle-substeps/s (one plain scene)"
+    unit = "particle-substeps/s"
+    DT = 1.0 / 60.0
+
+    def __init__(self, which: str):
+        self.which = which
+        self.name = {"dam": "dam_break_5k_S2_I4", "mixed": "mixed_50k_fluid30k_soft20x1k_sphere_S3_I4"}[which]
+
+    def recipe(self):
+        from pfsim import workloads as W
+
+        return W.dam_break(5000, seed=0) if self.which == "dam" else W.mixed_scene(50_000, seed=0)
+
+    def run_gpu(self, steps: int, warmup: int) -> dict:
+        import torch
+
+        from pfsim import _native as N
+        from pfsim import recipe as R
+
+        r = self.recipe()
+        sc = R.NativeBackend().build(r)
+        for _ in range(warmup):
+            sc.step(self.DT)
+        torch.cuda.synchronize()
+        stream = torch.cuda.ExternalStream(N.lib().pf_scene_stream(sc.h))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        e0.record(stream)
+        for _ in range(steps):
+            sc.step(self.DT)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / steps
+        return {"ms": ms, "value": r.particle_substeps / (ms * 1e-3), "clocks": clk, "particles": r.capacity}
+
+    def run_cpu(self, threads: int, steps: int = 3) -> dict:
+        from oracle import oracle as O
+
+        r = self.recipe()
+        sc = O.OracleBackend(threads=threads).build(r)
+        sc.step(self.DT)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sc.step(self.DT)
+        sec = (time.perf_counter() - t0) / steps
+        return {"seconds_per_step": sec, "units_per_step": r.particle_substeps, "cores": threads,
+                "sample": f"the same scene, {steps} frames after one warm-up frame"}
+
+
+WORKLOADS = {"sort": SortWorkload, "batch": BatchWorkload, "serve": ServeWorkload, "dam": SceneWorkload,
+             "mixed": SceneWorkload}
 
 
 # -------------------------------------------------------------- ranks ----
@@ -539,6 +619,8 @@ def main() -> None:
         wl = WORKLOADS["batch"](args.scenes)
     elif args.workload == "serve":
         wl = WORKLOADS["serve"](args.live)
+    elif args.workload in ("dam", "mixed"):
+        wl = SceneWorkload(args.workload)
     else:
         wl = WORKLOADS[args.workload]()
 
@@ -552,7 +634,7 @@ def main() -> None:
             "impl": "reference", "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": warmup, "ms_per_step": cpu["seconds_per_step"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.workload == "batch" else "u32", "data": "synthetic",
+            "dtype": "u32" if args.workload == "sort" else "f32", "data": "synthetic",
             "config": {"workload": wl.name},
             "cpu_baseline": {"value": value, "unit": wl.unit, "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]},
             "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -576,6 +658,19 @@ def main() -> None:
         def barrier():
             pass
 
+    if args.workload in ("dam", "mixed"):
+        res = wl.run_gpu(args.steps, warmup)
+        line = {"metric": wl.metric, "value": res["value"], "unit": wl.unit, "n_gpus": world, "steps": args.steps,
+                "warmup": warmup, "ms_per_step": res["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": {"workload": wl.name, "particles": res["particles"]}, "clocks": res["clocks"]}
+        if rank == 0 and not args.no_cpu_baseline:
+            cpu = wl.run_cpu(os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": cpu["units_per_step"] / cpu["seconds_per_step"], "unit": wl.unit,
+                                    "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     if args.workload == "serve":
         res = wl.run_gpu(args.steps, warmup, rank, world, barrier, plain_baseline=not args.no_plain)
         line = {"metric": wl.metric, "value": res["units_per_step"] / (res["ms"] * 1e-3), "unit": wl.unit,
@@ -614,7 +709,7 @@ def main() -> None:
         "gpu_launches": res["gpu_launches_per_step"] * args.steps,
         "clocks": res["clocks"],
     }
-    line["dtype"] = "f32" if args.workload == "batch" else "u32"
+    line["dtype"] = "u32" if args.workload == "sort" else "f32"
     line.update(res.get("extra", {}))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = wl.run_cpu(os.cpu_count() or 1)
