@@ -78,6 +78,14 @@ __device__ __forceinline__ float spiky_factor(float rsq, const DevFluid& F) {
   return -(t * t * F.spiky) * inv_r;
 }
 
+// (h - r)^2 / r from r^2, without the -45/(pi h^6) constant (the slot
+// kernels apply it once to their sums): zero at r = 0.
+__device__ __forceinline__ float spiky_shape(float rsq, const DevFluid& F) {
+  const float inv_r = rsqrtf(fmaxf(rsq, 1e-40f));
+  const float t = fmaxf(F.h - rsq * inv_r, 0.0f);
+  return t * t * inv_r;
+}
+
 // The forms the neighbour loops call. A build with PF_EXACT_ROUNDING (and
 // -fmad=false) uses the exactly rounded reference forms instead; it is a
 // diagnostic build that reproduces the oracle's FP32 arithmetic bit for bit.

@@ -103,6 +103,7 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
+#ifdef PF_EXACT_ROUNDING
   auto one = [&](float4 xj, float bvj) {
     const float mass = nbr_mass(bvj, xj.w, F.rho0);
     const f3 off = xi - xyz(xj);
@@ -112,6 +113,21 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
     gs = gs + g;
     gss += dot(g, g) * xj.w;
   };
+#else
+  // The kernel constants leave the sums: rho = poly6 * sum m d^3,
+  // sum grad = -spiky * sum f r, sum |grad|^2 w = spiky^2 * sum f^2 r^2 w
+  // with f = m (h - r)^2 / r.
+  auto one = [&](float4 xj, float bvj) {
+    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+    const f3 off = xi - xyz(xj);
+    const float rsq = dot(off, off);
+    const float d = fmaxf(F.hsq - rsq, 0.0f);
+    rho += mass * (d * d * d);
+    const float f = spiky_shape(rsq, F) * mass;
+    gs = gs + off * f;
+    gss += (f * f) * (rsq * xj.w);
+  };
+#endif
   uint32_t m = 0;
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
     uint32_t j[kNbrUnroll];
@@ -131,6 +147,11 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
     const uint32_t j = __ldg(nl + m * n);
     one(__ldg(V.cur.xs + j), __ldg(V.cur.bv + j));
   }
+#ifndef PF_EXACT_ROUNDING
+  rho *= F.poly6;
+  gs = gs * -F.spiky;
+  gss *= F.spiky * F.spiky;
+#endif
   V.density[k] = rho;
   const float C = rho * F.inv_rho0 - 1.0f;
   if (C <= 0.0f) {
@@ -165,8 +186,17 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
   auto one = [&](uint32_t j, float4 xj, float bvj, float lj) {
     const float mass = nbr_mass(bvj, xj.w, F.rho0);
     const f3 off = xi - xyz(xj);
+#ifdef PF_EXACT_ROUNDING
     const f3 g = spiky_vec(off, dot(off, off), F);
     sum = sum + g * ((li + lj) * mass);
+#else
+    // sum stays without the -spiky constant until the end; the gradient is
+    // formed only for a reaction
+    const float rsq = dot(off, off);
+    const float shape = spiky_shape(rsq, F);
+    sum = sum + off * (shape * ((li + lj) * mass));
+    const f3 g = off * (shape * -F.spiky);
+#endif
     if (react && bvj > 0.0f && xj.w > 0.0f) {
       const uint32_t idj = V.ids[j];
       bool in = false;
@@ -197,6 +227,9 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
     const uint32_t j = __ldg(nl + m * n);
     one(j, __ldg(V.cur.xs + j), __ldg(V.cur.bv + j), __ldg(V.lambda + j));
   }
+#ifndef PF_EXACT_ROUNDING
+  sum = sum * -F.spiky;
+#endif
   V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
 }
 
