@@ -247,29 +247,36 @@ k_scatter(const uint32_t* __restrict__ keys, uint32_t n, const uint32_t* __restr
   const uint32_t peers = __match_any_sync(active, key);
   const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
   uint32_t base = 0;
+  // 0: nothing to record; 1/2/3: this lane's cell goes on the small / mid /
+  // giant fix-up list (its run was started by another warp)
+  uint32_t need = 0;
   if (lane_id() == leader) {
     const uint32_t old = atomicAdd(fill + key, (uint32_t)__popc(peers));
     base = start[key] + old;
     if (old != 0) {
-      // A second warp reached this cell: its run may be out of order.
       const uint32_t bit = 1u << (key & 31u);
       const uint32_t prev = atomicOr(dirty_bits + (key >> 5), bit);
       if (!(prev & bit)) {
         const uint32_t c = counts[key];
-        if (c <= kSmallMax) {
-          const uint32_t at = atomicAdd(counters + kCounterSmall, 1u);
-          if (at < lists.small_cap) lists.small[at] = key;
-          else atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
-        } else if (c <= kMidMax) {
-          const uint32_t at = atomicAdd(counters + kCounterMid, 1u);
-          if (at < lists.mid_cap) lists.mid[at] = key;
-          else atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
-        } else {
-          const uint32_t at = atomicAdd(counters + kCounterGiant, 1u);
-          if (at < lists.giant_cap) lists.giant[at] = key;
-          else atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
-        }
+        need = c <= kSmallMax ? 1u : (c <= kMidMax ? 2u : 3u);
       }
+    }
+  }
+  // one counter atomic per warp and list for the cells this warp records
+#pragma unroll
+  for (uint32_t l = 1; l <= 3; ++l) {
+    const uint32_t mask = __ballot_sync(active, need == l);
+    if (!mask) continue;
+    const uint32_t first = (uint32_t)(__ffs(mask) - 1);
+    const uint32_t ctr = l == 1 ? kCounterSmall : (l == 2 ? kCounterMid : kCounterGiant);
+    uint32_t at = 0;
+    if (lane_id() == first) at = atomicAdd(counters + ctr, (uint32_t)__popc(mask));
+    at = __shfl_sync(active, at, first) + __popc(mask & lanemask_lt());
+    if (need == l) {
+      uint32_t* list = l == 1 ? lists.small : (l == 2 ? lists.mid : lists.giant);
+      const uint32_t cap = l == 1 ? lists.small_cap : (l == 2 ? lists.mid_cap : lists.giant_cap);
+      if (at < cap) list[at] = key;
+      else atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
     }
   }
   base = __shfl_sync(active, base, leader);

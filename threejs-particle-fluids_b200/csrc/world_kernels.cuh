@@ -180,6 +180,19 @@ __device__ __forceinline__ f3 prim_pivot(const pf_primitive& p) {
 
 // primitives.ts:203-335 with the PrimitiveSet fields (velocity and spin).
 __device__ __forceinline__ void prim_sdf(const pf_primitive& p, f3 xw, float rewind, float* phi_out, f3* grad_out) {
+  if (p.kind == PF_PRIM_PLANE && !(p.flags & PF_PRIM_SWEEP) && p.spin[0] == 0.0f && p.spin[1] == 0.0f &&
+      p.spin[2] == 0.0f) {
+    // an unswept, unspun plane: the general path below with t = 0 and the
+    // identity turn, term for term (x = pivot + (x_w - pivot))
+    const f3 d0 = mk(p.data0[0], p.data0[1], p.data0[2]);
+    const f3 d1 = mk(p.data1[0], p.data1[1], p.data1[2]);
+    const f3 x = d1 + ((xw + mk(p.velocity[0], p.velocity[1], p.velocity[2]) * 0.0f) - d1);
+    const float phi = dot(d0, x - d1);
+    const bool inv = (p.flags & PF_PRIM_INVERT) != 0;
+    *phi_out = inv ? -phi : phi;
+    *grad_out = inv ? neg(d0) : d0;
+    return;
+  }
   const float t = (p.flags & PF_PRIM_SWEEP) ? rewind : 0.0f;
   const f3 shifted = xw + mk(p.velocity[0], p.velocity[1], p.velocity[2]) * t;
   const f3 pivot = prim_pivot(p);
