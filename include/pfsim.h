@@ -169,6 +169,14 @@ PF_API pf_status pf_set_inv_mass(pf_scene* scene, pf_range range, float inv_mass
  * walk, then eta = grad|omega| over fluid neighbours and
  * v += vorticity * dt * (eta/|eta| x omega). */
 #define PF_FLUID_VORTICITY 2u
+/* Surface tension (FluidSystemOptions.surfaceTension; Akinci et al. 2013
+ * cohesion + curvature, cohesion.ts:33-120) and adhesion to boundary
+ * particles (FluidSystemOptions.adhesion, adhesion.ts:33-76): velocity
+ * changes gathered in a fixed-point accumulator (maxMag 50) once per
+ * substep after the neighbour list, applied to v and to x* (times dt)
+ * before the pressure solve (FluidSystem.ts:233-255). */
+#define PF_FLUID_SURFACE_TENSION 4u
+#define PF_FLUID_ADHESION 8u
 typedef struct pf_fluid_desc {
   pf_range range;               /* count 0 = every particle */
   float rest_density;
@@ -181,6 +189,8 @@ typedef struct pf_fluid_desc {
   const pf_range* boundaries;   /* host, n_boundaries entries */
   const uint8_t* boundary_static; /* host or NULL: 1 = static boundary (addBoundary dynamic:false) */
   float vorticity;              /* used when PF_FLUID_VORTICITY is set */
+  float surface_tension;        /* gamma, used when PF_FLUID_SURFACE_TENSION is set */
+  float adhesion;               /* beta, used when PF_FLUID_ADHESION is set */
 } pf_fluid_desc;
 PF_API pf_status pf_add_fluid(pf_scene* scene, const pf_fluid_desc* desc, uint32_t* material_index);
 

@@ -283,8 +283,8 @@ struct Range {
 template <typename T>
 struct Fluid {
   Range range;
-  double restDensity, spacing, h, compliance, viscosity, vorticity = 0;
-  bool hasViscosity, hasVorticity = false;
+  double restDensity, spacing, h, compliance, viscosity, vorticity = 0, surfaceTension = 0, adhesion = 0;
+  bool hasViscosity, hasVorticity = false, hasSurfaceTension = false, hasAdhesion = false;
   std::vector<Range> boundaries;
   std::vector<uint8_t> boundaryStatic;
   // uniforms at engine precision
@@ -294,6 +294,10 @@ struct Fluid {
   std::vector<V3<T>> deltaX, deltaV;
   std::vector<V3<T>> omega, eta;  // vorticity confinement (velocity.ts:13-21)
   std::vector<T> omegaLength;
+  // surface tension and adhesion (cohesion.ts, adhesion.ts)
+  T uGamma = 0, uBeta = 0;
+  std::vector<V3<T>> normal;
+  Accum<T> impulses;  // velocity changes, maxMag 50 (FluidSystem.ts:237)
   std::vector<uint32_t> nbrIdx, nbrCount;  // column-major k*count + local
   uint32_t nbrOverflow = 0;
   bool hasReaction = false;
@@ -626,6 +630,86 @@ struct Engine {
   }
 
   // velocity.ts:36-120 (XSPH only; vorticity is not part of this path)
+  // cohesion.ts:33-48: n_i = h sum_j V_j grad W(x*_i - x*_j)
+  void color_normal(Fluid<T>& f) {
+    const uint32_t rc = f.range.count;
+    parallel_for(0, static_cast<int64_t>(rc), [&](int64_t li) {
+      const uint32_t local = static_cast<uint32_t>(li), i = f.range.start + local;
+      const V3<T> xi = p3(pred, i);
+      V3<T> sum = v3<T>(0, 0, 0);
+      const uint32_t nc = f.nbrCount[local];
+      for (uint32_t k = 0; k < nc; ++k) {
+        const uint32_t j = f.nbrIdx[static_cast<size_t>(k) * rc + local];
+        const T volume = bvol[j] > 0 ? bvol[j] : f.uVolume;
+        sum = sum + spiky_grad(xi - p3(pred, j), f) * volume;
+      }
+      f.normal[i] = sum * f.uH;
+    });
+  }
+  // cohesion.ts:54-66: the cohesion spline C(r), constants as f32 literals
+  T cohesion_spline(T r, const Fluid<T>& f) const {
+    const bool dbl = sizeof(T) == 8;
+    auto U = [&](double v) { return dbl ? static_cast<T>(v) : static_cast<T>(static_cast<float>(v)); };
+    const T h = U(f.h);
+    const T gap = tmax(h - r, static_cast<T>(0));
+    const T shared = gap * gap * gap * (r * r * r);
+    const T value = r * static_cast<T>(2) > h ? shared : shared * static_cast<T>(2) - U(std::pow(f.h, 6) / 64.0);
+    return (r > 0 && r <= h) ? value * U(32.0 / (M_PI * std::pow(f.h, 9))) : static_cast<T>(0);
+  }
+  // adhesion.ts:33-47: the adhesion spline A(r)
+  T adhesion_spline(T r, const Fluid<T>& f) const {
+    const bool dbl = sizeof(T) == 8;
+    auto U = [&](double v) { return dbl ? static_cast<T>(v) : static_cast<T>(static_cast<float>(v)); };
+    const T h = U(f.h);
+    const T inner = tmax(r * r * U(-4.0 / f.h) + r * static_cast<T>(6) - U(2.0 * f.h), static_cast<T>(0));
+    const T root = std::sqrt(std::sqrt(inner));
+    return (r * static_cast<T>(2) > h && r <= h) ? root * U(0.007 / std::pow(f.h, 3.25)) : static_cast<T>(0);
+  }
+  // cohesion.ts:75-120: each fluid pair once (j > i inside the range)
+  void surface_tension(Fluid<T>& f) {
+    const uint32_t rc = f.range.count, end = f.range.start + rc;
+    parallel_for(0, static_cast<int64_t>(rc), [&](int64_t li) {
+      const uint32_t local = static_cast<uint32_t>(li), i = f.range.start + local;
+      const V3<T> xi = p3(pred, i);
+      const V3<T> ni = f.normal[i];
+      const T rhoI = f.density[i];
+      const uint32_t nc = f.nbrCount[local];
+      for (uint32_t k = 0; k < nc; ++k) {
+        const uint32_t j = f.nbrIdx[static_cast<size_t>(k) * rc + local];
+        if (j <= i || j >= end) continue;
+        const V3<T> off = xi - p3(pred, j);
+        const T r = length(off);
+        if (r < static_cast<T>(1e-20)) continue;
+        const T corr = (f.uRho0 * static_cast<T>(2)) / tmax(rhoI + f.density[j], static_cast<T>(1));
+        const V3<T> coh = (off / r) * neg1(f.uGamma * f.uMass * f.uMass * cohesion_spline(r, f));
+        const V3<T> curv = (ni - f.normal[j]) * neg1(f.uGamma * f.uMass);
+        const V3<T> dv = (coh + curv) * corr / f.uMass * dt;
+        f.impulses.add(i, dv);
+        f.impulses.add(j, v3<T>(-dv.x, -dv.y, -dv.z));
+      }
+    });
+  }
+  // adhesion.ts:55-76: toward boundary neighbours, fluid side only
+  void adhesion(Fluid<T>& f) {
+    const uint32_t rc = f.range.count;
+    parallel_for(0, static_cast<int64_t>(rc), [&](int64_t li) {
+      const uint32_t local = static_cast<uint32_t>(li), i = f.range.start + local;
+      const V3<T> xi = p3(pred, i);
+      const uint32_t nc = f.nbrCount[local];
+      for (uint32_t k = 0; k < nc; ++k) {
+        const uint32_t j = f.nbrIdx[static_cast<size_t>(k) * rc + local];
+        const T volume = bvol[j];
+        if (volume <= 0) continue;
+        const V3<T> off = xi - p3(pred, j);
+        const T r = length(off);
+        if (r < static_cast<T>(1e-20)) continue;
+        const V3<T> force = (off / r) * neg1(f.uBeta * f.uMass * (f.uRho0 * volume) * adhesion_spline(r, f));
+        f.impulses.add(i, force / f.uMass * dt);
+      }
+    });
+  }
+  static T neg1(T v) { return -v; }
+
   // velocity.ts:36-120: one walk for the curl (vorticity) and the XSPH
   // change, the gradient of |omega| over fluid neighbours, then the apply.
   void fluid_velocity(Fluid<T>& f) {
@@ -1329,6 +1413,20 @@ struct Engine {
         for (size_t b = 0; b < f.boundaries.size(); ++b)
           if (!f.boundaryStatic[b]) boundary_volume(f, f.boundaries[b], pred);
         build_neighbors(f);
+        // FluidSystem.ts:233-255: impulses once per substep, before the solve
+        if (f.hasSurfaceTension || f.hasAdhesion) {
+          f.impulses.reset();
+          if (f.hasSurfaceTension) {
+            color_normal(f);
+            surface_tension(f);
+          }
+          if (f.hasAdhesion) adhesion(f);
+          for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) {
+            const V3<T> c = f.impulses.take(i, &f.impulses.flag);
+            set3(vel, i, p3(vel, i) + c, vel[4 * i + 3]);
+            set3(pred, i, p3(pred, i) + c * dt, pred[4 * i + 3]);
+          }
+        }
         if (f.hasReaction) {
           f.reaction.reset();
           f.reaction.flag = 0;
@@ -1640,6 +1738,10 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.viscosity = d->viscosity;
     f.hasVorticity = (d->flags & PF_FLUID_VORTICITY) != 0;
     f.vorticity = d->vorticity;
+    f.hasSurfaceTension = (d->flags & PF_FLUID_SURFACE_TENSION) != 0;
+    f.surfaceTension = d->surface_tension;
+    f.hasAdhesion = (d->flags & PF_FLUID_ADHESION) != 0;
+    f.adhesion = d->adhesion;
     const double mass = f.restDensity * f.spacing * f.spacing * f.spacing;
     for (uint32_t b = 0; b < d->n_boundaries; ++b) {
       f.boundaries.push_back({d->boundaries[b].start, d->boundaries[b].count});
@@ -1659,6 +1761,8 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.uCompliance = U(f.compliance);
     f.uC = U(f.viscosity);
     f.uEps = U(f.vorticity);
+    f.uGamma = U(f.surfaceTension);
+    f.uBeta = U(f.adhesion);
     // particles.setInvMass(range, 1 / mass) into a Float32Array.
     const float w = static_cast<float>(1.0 / mass);
     for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) e.invMass[i] = w;
@@ -1671,6 +1775,8 @@ int or_add_fluid(void* h, const pf_fluid_desc* d, uint32_t* mat) {
     f.omega.assign(e.cap, v3<T>(0, 0, 0));
     f.eta.assign(e.cap, v3<T>(0, 0, 0));
     f.omegaLength.assign(e.cap, 0);
+    f.normal.assign(e.cap, v3<T>(0, 0, 0));
+    f.impulses.init(e.cap, 50.0);
     f.nbrIdx.assign(static_cast<size_t>(f.range.count) * kMaxNeighbors, 0);
     f.nbrCount.assign(f.range.count, 0);
     f.hasReaction = !f.boundaries.empty();

@@ -162,3 +162,17 @@ def test_cloth_side_stream_batch_matches_plain(cuda):
     for i, s in enumerate(plain):
         assert np.array_equal(s.readback(N.PF_FIELD_POSITIONS), batch.readback(i, N.PF_FIELD_POSITIONS)), i
         assert np.array_equal(s.readback(N.PF_FIELD_VELOCITIES), batch.readback(i, N.PF_FIELD_VELOCITIES)), i
+
+
+def test_surface_tension_and_adhesion_one_frame(oracle, cuda):
+    """FluidSystem surfaceTension + adhesion (cohesion.ts, adhesion.ts) on the
+    mixed scene, whose soft bodies are the fluid's dynamic boundaries:
+    pairwise cohesion/curvature impulses and adhesion toward boundary
+    particles through the velocity accumulator, before the pressure solve."""
+    r = W.mixed_scene(n_budget=12_000, n_fluid=8_000, n_bodies=4, seed=21)
+    r.motion = None
+    fo = r.materials[1][1]
+    fo.surface_tension, fo.adhesion, fo.vorticity = 0.1, 0.1, 0.02
+    a, b = one_frame(oracle, cuda, r, frames=2)
+    assert max_dev(a, b) <= TOL
+    assert max_dev(a, b, N.PF_FIELD_DENSITY) <= 0.5  # kg/m^3, rho ~ 1000

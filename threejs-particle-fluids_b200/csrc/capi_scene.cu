@@ -224,6 +224,14 @@ pf_status pf_add_fluid(pf_scene* s, const pf_fluid_desc* d, uint32_t* mat) {
   f.vorticity = f.has_vort ? d->vorticity : 0.0;
   if (f.has_vort && !std::isfinite(f.vorticity))
     return fail(PF_ERR_INVALID, "FluidSystem: vorticity must be finite");
+  f.has_st = (d->flags & PF_FLUID_SURFACE_TENSION) != 0;
+  f.surface_tension = f.has_st ? d->surface_tension : 0.0;
+  if (f.has_st && !std::isfinite(f.surface_tension))
+    return fail(PF_ERR_INVALID, "FluidSystem: surfaceTension must be finite");
+  f.has_ad = (d->flags & PF_FLUID_ADHESION) != 0;
+  f.adhesion = f.has_ad ? d->adhesion : 0.0;
+  if (f.has_ad && !std::isfinite(f.adhesion))
+    return fail(PF_ERR_INVALID, "FluidSystem: adhesion must be finite");
   for (uint32_t b = 0; b < d->n_boundaries; ++b) {
     RangeU r{d->boundaries[b].start, d->boundaries[b].count};
     if (!range_ok(sp, r)) return fail(PF_ERR_INVALID, "FluidSystem.addBoundary: invalid particle range");

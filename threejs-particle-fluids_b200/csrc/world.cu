@@ -119,6 +119,7 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   V.nxt.v[k] = V.cur.v[o];
   V.nxt.bv[k] = V.cur.bv[o];
   V.nxt.tag[k] = V.cur.tag[o];
+  V.nxt.dens[k] = V.cur.dens[o];
   V.ids[k] = id;
   V.inv[id] = k;
   // lambda is read for every neighbour, fluid or not (positionDelta.ts:193),
@@ -127,6 +128,7 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
   if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
+  if (V.acc_imp) V.acc_imp[k] = make_int4(0, 0, 0, 0);
 }
 
 // Without a grid the slots never move; only the per-substep sums reset.
@@ -726,6 +728,30 @@ __global__ void __launch_bounds__(kBlock) k_gather_positions(WorldView V, const 
   out[prefix[s] + local] = make_float4(x.x, x.y, x.z, 0.0f);
 }
 
+// FluidSystem.ts:248-253: the impulse accumulator's apply over the fluid's
+// range, into the velocity and (times dt) the predicted position.
+__global__ void __launch_bounds__(kBlock) k_imp_apply(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !(F.has_st || F.has_ad)) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (sub >= S.substeps) return;
+  const int4 t = V.acc_imp[k];
+  V.acc_imp[k] = make_int4(0, 0, 0, 0);
+  bool sat = false;
+  const f3 c = ticks_change(t.x, t.y, t.z, F.imp_inv, &sat);
+  const float4 v = V.cur.v[k];
+  V.cur.v[k] = make_float4(v.x + c.x, v.y + c.y, v.z + c.z, v.w);
+  const float4 x = V.cur.xs[k];
+  const f3 d = c * S.dt;
+  V.cur.xs[k] = make_float4(x.x + d.x, x.y + d.y, x.z + d.z, x.w);
+  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_VEL, 1u);
+}
+
 // Fresh slot maps (ids = inv = identity) and identity orientations.
 __global__ void __launch_bounds__(kBlock) k_init_slots(uint32_t* __restrict__ ids, uint32_t* __restrict__ inv,
                                                        float4* __restrict__ q, float4* __restrict__ qp, uint32_t n) {
@@ -995,6 +1021,19 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         F.has_visc = fs.has_visc ? 1u : 0u;
         F.has_vort = fs.has_vort ? 1u : 0u;
         F.vort_eps = f32(fs.vorticity);
+        F.has_st = fs.has_st ? 1u : 0u;
+        F.has_ad = fs.has_ad ? 1u : 0u;
+        F.gamma = f32(fs.surface_tension);
+        F.beta = f32(fs.adhesion);
+        F.mass = f32(fs.rho0 * fs.spacing * fs.spacing * fs.spacing);
+        F.coh_coef = f32(32.0 / (M_PI * std::pow(fs.h, 9)));
+        F.coh_h6_64 = f32(std::pow(fs.h, 6) / 64.0);
+        F.adh_coef = f32(0.007 / std::pow(fs.h, 3.25));
+        F.adh_m4h = f32(-4.0 / fs.h);
+        F.adh_2h = f32(2.0 * fs.h);
+        F.range_end = S.seg_start + fs.range.start + fs.range.count;
+        F.imp_scale = S.vel_scale;
+        F.imp_inv = S.vel_inv;
         F.bnd_first = (uint32_t)h_bnds_.size();
         F.bnd_count = (uint32_t)fs.bnd.size();
         uint32_t lo = UINT32_MAX, hi = 0;
@@ -1018,6 +1057,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         any_fluid_ = true;
         any_visc_ = any_visc_ || fs.has_visc;
         any_vort_ = any_vort_ || fs.has_vort;
+        any_imp_ = any_imp_ || fs.has_st || fs.has_ad;
         h_fluids_.push_back(F);
       } else if (kind == MAT_SOFT) {
         const SoftSpec& ss = sp.softs[idx];
@@ -1212,6 +1252,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
       buf_[b].v = cv.take<float4>(N);
       buf_[b].bv = cv.take<float>(N);
       buf_[b].tag = cv.take<uint32_t>(N);
+      buf_[b].dens = cv.take<float>(N);
     }
     base_.ids = cv.take<uint32_t>(N);
     base_.inv = cv.take<uint32_t>(N);
@@ -1228,10 +1269,11 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.row_base = cv.take<uint32_t>(row_base.size());
     base_.grid_scene = cv.take<uint32_t>(grid_scene.size());
     base_.lambda = cv.take<float>(N);
-    base_.density = cv.take<float>(N);
     base_.dx = cv.take<float4>(N);
     base_.dv = cv.take<float4>(N);
     base_.vort = any_vort_ ? cv.take<float4>(N) : nullptr;
+    base_.normal = any_imp_ ? cv.take<float4>(N) : nullptr;
+    base_.acc_imp = any_imp_ ? cv.take<int4>(N) : nullptr;
     base_.plam = cv.take<float2>(N * P);
     base_.acc_react = any_react_ ? cv.take<int4>(N) : nullptr;
     base_.acc_soft = any_soft_local_ ? cv.take<int4>(N) : nullptr;
@@ -1355,7 +1397,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
   }
   PF_TRY(up(buf_[0].tag, tag.data(), 4 * N));
-  PF_TRY(up(base_.density, dens.data(), 4 * N));
+  PF_TRY(up(buf_[0].dens, dens.data(), 4 * N));
   PF_TRY(up(base_.softs, h_softs_.data(), sizeof(DevSoft) * h_softs_.size()));
   PF_TRY(up(base_.bodies, h_bodies_.data(), sizeof(DevBody) * h_bodies_.size()));
   PF_TRY(up(base_.grp, grp.data(), 4 * grp.size()));
@@ -1501,7 +1543,7 @@ pf_status World::tune() {
   tuned_ = true;
   if (!any_fluid_ || n_ == 0) return PF_OK;
   if (const char* e = std::getenv("PFSIM_NBR_PATH")) {  // fixed choice for measurements
-    nbr_path_ = ((uint32_t)std::atoi(e) == 1 && !any_vort_) ? 1u : 0u;
+    nbr_path_ = ((uint32_t)std::atoi(e) == 1 && !any_vort_ && !any_imp_) ? 1u : 0u;
     if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) slot_block_ = (uint32_t)std::atoi(b);
     if (slot_block_ != 128 && slot_block_ != 256 && slot_block_ != 512) slot_block_ = 256;
     if (const char* u = std::getenv("PFSIM_SLOT_UNROLL")) slot_unroll_ = (uint32_t)std::atoi(u);
@@ -1512,8 +1554,13 @@ pf_status World::tune() {
   parity_ ^= 1;
   const WorldView V = view(parity_);
   const uint32_t rank = h_fluids_[0].rank;
+  // the density passes below overwrite the densities the first substep's
+  // surface tension reads: keep them in the sort-key buffer (free until the
+  // next sort)
+  float* keep = reinterpret_cast<float*>(base_.keys);
+  PF_CUDA(cudaMemcpyAsync(keep, V.cur.dens, 4ull * n_, cudaMemcpyDeviceToDevice, stream_));
   // the warp-tile path has no vorticity pass: worlds with it stay on slots
-  const uint32_t n_cands_max = any_vort_ ? 7u : 8u;
+  const uint32_t n_cands_max = (any_vort_ || any_imp_) ? 7u : 8u;
   struct Cand { uint32_t path, block, unroll; };
   const Cand cands[] = {{0, 128, 4}, {0, 256, 4}, {0, 512, 4}, {0, 128, 2}, {0, 256, 2},
                         {0, 128, 8}, {0, 256, 8}, {1, 128, 4}};
@@ -1546,6 +1593,7 @@ pf_status World::tune() {
   nbr_path_ = pick.path;
   slot_block_ = pick.block;
   slot_unroll_ = pick.unroll;
+  PF_CUDA(cudaMemcpyAsync(V.cur.dens, keep, 4ull * n_, cudaMemcpyDeviceToDevice, stream_));
   return PF_OK;
 }
 
@@ -1591,6 +1639,19 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   // preSolve
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
   if (any_fluid_) run_fluid_neighbors(V, s);
+  // FluidSystem.ts:233-255: surface tension and adhesion, once per substep
+  if (any_imp_)
+    for (uint32_t r = 0; r < max_rank_; ++r) {
+      bool st = false, imp = false;
+      for (auto& F : h_fluids_) {
+        st = st || (F.rank == r && F.has_st);
+        imp = imp || (F.rank == r && (F.has_st || F.has_ad));
+      }
+      if (!imp) continue;
+      if (st) PF_BY_UNROLL(k_s_color_normal, V, r, s);
+      PF_BY_UNROLL(k_s_impulses, V, r, s);
+      launch_slots(k_imp_apply, n_, stream_, V, r, s);
+    }
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
   if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
@@ -1790,7 +1851,7 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
     case PF_FIELD_VELOCITIES: return by_slot4(B.v, true, false);
     case PF_FIELD_INV_MASS: return by_slot4(B.x, false, true);
     case PF_FIELD_BOUNDARY_VOLUME: return by_slot1(B.bv, false);
-    case PF_FIELD_DENSITY: return by_slot1(base_.density, true);
+    case PF_FIELD_DENSITY: return by_slot1(B.dens, true);
     case PF_FIELD_LAMBDA: return by_slot1(base_.lambda, true);
     case PF_FIELD_ROTATION: return by_id4(base_.q);
     case PF_FIELD_PREDICTED_ROTATION: return by_id4(base_.qp);

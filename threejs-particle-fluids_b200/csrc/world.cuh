@@ -42,8 +42,8 @@ struct RangeU {
 
 struct FluidSpec {
   RangeU range;
-  double rho0, spacing, h, compliance, viscosity, vorticity = 0;
-  bool has_visc, has_vort = false;
+  double rho0, spacing, h, compliance, viscosity, vorticity = 0, surface_tension = 0, adhesion = 0;
+  bool has_visc, has_vort = false, has_st = false, has_ad = false;
   std::vector<RangeU> bnd;
   std::vector<uint8_t> bnd_static;
 };
@@ -145,6 +145,12 @@ struct DevFluid {
   uint32_t has_visc;
   uint32_t has_vort;
   float vort_eps;  // vorticity confinement strength
+  uint32_t has_st, has_ad;  // surface tension, adhesion
+  float gamma, beta, mass;
+  float coh_coef, coh_h6_64;   // cohesion spline: 32/(pi h^9), h^6/64
+  float adh_coef, adh_m4h, adh_2h;  // adhesion spline: 0.007/h^3.25, -4/h, 2h
+  uint32_t range_end;          // first id past the fluid's range
+  float imp_scale, imp_inv;    // impulse accumulator (maxMag 50)
   uint32_t bnd_first, bnd_count;
   uint32_t react_lo, react_hi;  // covering id range of the boundaries (lo == hi: no reaction)
   float react_scale, react_inv;
@@ -200,6 +206,7 @@ struct StateBuf {
   float4* v = nullptr;   // velocities
   float* bv = nullptr;   // boundary volume
   uint32_t* tag = nullptr;
+  float* dens = nullptr;  // fluid density of the last density pass (read by surface tension)
 };
 
 // Everything a stage kernel needs, passed by value.
@@ -235,10 +242,11 @@ struct WorldView {
   uint32_t n_grid_scenes;
   uint32_t n_rows;
   float* lambda;
-  float* density;
   float4* dx;
   float4* dv;
   float4* vort;       // curl of the velocity per slot, w = its length (vorticity confinement)
+  float4* normal;     // scaled colour-field normal per slot (surface tension)
+  int4* acc_imp;      // fixed-point velocity changes of surface tension and adhesion
   float2* plam;       // (lambda_n, lambda_t) per slot x primitive
   int4* acc_react;    // fixed-point reaction sums per slot
   int4* acc_soft;     // fixed-point shape-matching sums per slot
@@ -367,6 +375,7 @@ class World {
   uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
   bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false, any_vort_ = false;
+  bool any_imp_ = false;  // surface tension or adhesion somewhere
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
   bool any_react_ = false;
   bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass

@@ -152,7 +152,7 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   gs = gs * -F.spiky;
   gss *= F.spiky * F.spiky;
 #endif
-  V.density[k] = rho;
+  V.cur.dens[k] = rho;
   const float C = rho * F.inv_rho0 - 1.0f;
   if (C <= 0.0f) {
     V.lambda[k] = 0.0f;
@@ -309,6 +309,98 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
     eta = eta + spiky_vec(off, dot(off, off), F) * ((V.vort[j].w - wi) * F.volume);
   }
   V.dx[k] = with_w(eta, 0.0f);
+}
+
+// cohesion.ts:33-48: n_i = h sum_j V_j grad W(x*_i - x*_j), at this
+// substep's predicted positions.
+template <uint32_t kNbrUnroll>
+__global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !F.has_st) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const f3 xi = xyz(V.cur.xs[k]);
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    const float bvj = __ldg(V.cur.bv + j);
+    const f3 off = xi - xyz(__ldg(V.cur.xs + j));
+    sum = sum + spiky_vec(off, dot(off, off), F) * (bvj > 0.0f ? bvj : F.volume);
+  }
+  V.normal[k] = with_w(sum * F.h, 0.0f);
+}
+
+// cohesion.ts:54-66: the cohesion spline C(r).
+__device__ __forceinline__ float cohesion_spline(float r, const DevFluid& F) {
+  const float gap = fmaxf(F.h - r, 0.0f);
+  const float shared = gap * gap * gap * (r * r * r);
+  const float value = r * 2.0f > F.h ? shared : shared * 2.0f - F.coh_h6_64;
+  return (r > 0.0f && r <= F.h) ? value * F.coh_coef : 0.0f;
+}
+// adhesion.ts:33-47: the adhesion spline A(r), non-zero on (h/2, h].
+__device__ __forceinline__ float adhesion_spline(float r, const DevFluid& F) {
+  const float inner = fmaxf(r * r * F.adh_m4h + r * 6.0f - F.adh_2h, 0.0f);
+  const float root = sqrtf(sqrtf(inner));
+  return (r * 2.0f > F.h && r <= F.h) ? root * F.adh_coef : 0.0f;
+}
+
+// cohesion.ts:75-120 and adhesion.ts:55-76 in one walk: surface tension on
+// each fluid pair once (partner id above this one, inside the fluid's range;
+// the negated change goes to the partner), adhesion toward boundary
+// neighbours on the fluid side only; both as fixed-point velocity changes.
+template <uint32_t kNbrUnroll>
+__global__ void k_s_impulses(WorldView V, uint32_t rank, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  if (!f) return;
+  const DevFluid& F = V.fluids[f - 1];
+  if (F.rank != rank || !(F.has_st || F.has_ad)) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const f3 xi = xyz(V.cur.xs[k]);
+  const uint32_t idi = V.ids[k];
+  const f3 ni = F.has_st ? xyz(V.normal[k]) : mk(0.0f, 0.0f, 0.0f);
+  const float rhoi = V.cur.dens[k];
+  const float dt = S.dt;
+  const uint32_t cnt = V.ncount[k];
+  const size_t n = V.n;
+  const uint32_t* __restrict__ nl = V.nbr + k;
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const uint32_t j = __ldg(nl + m * n);
+    const f3 off = xi - xyz(__ldg(V.cur.xs + j));
+    if (F.has_st) {
+      const uint32_t idj = V.ids[j];
+      if (idj > idi && idj < F.range_end) {
+        const float r = len(off);
+        if (!(r < 1e-20f)) {
+          const float corr = (F.rho0 * 2.0f) / fmaxf(rhoi + V.cur.dens[j], 1.0f);
+          const f3 coh = (off / r) * -(F.gamma * F.mass * F.mass * cohesion_spline(r, F));
+          const f3 curv = (ni - xyz(V.normal[j])) * -(F.gamma * F.mass);
+          const f3 dv = (coh + curv) * corr / F.mass * dt;
+          acc_add(V.acc_imp, k, dv, F.imp_scale);
+          acc_add(V.acc_imp, j, neg(dv), F.imp_scale);
+        }
+      }
+    }
+    if (F.has_ad) {
+      const float vol = __ldg(V.cur.bv + j);
+      if (vol > 0.0f) {
+        const float r = len(off);
+        if (!(r < 1e-20f)) {
+          const f3 force = (off / r) * -(F.beta * F.mass * (F.rho0 * vol) * adhesion_spline(r, F));
+          acc_add(V.acc_imp, k, force / F.mass * dt, F.imp_scale);
+        }
+      }
+    }
+  }
 }
 
 }  // namespace pf

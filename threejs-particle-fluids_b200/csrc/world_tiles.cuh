@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kTileThreads) k_t_lambda(WorldView V, uint32_t
         gss += dot(g, g) * xj.w;
       };
       for_each_h(V.nbr16 + i, n, cnt, one);
-      V.density[i] = rho;
+      V.cur.dens[i] = rho;
       const float C = rho * F.inv_rho0 - 1.0f;
       if (C <= 0.0f) {
         V.lambda[i] = 0.0f;

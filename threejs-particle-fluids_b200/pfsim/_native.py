@@ -26,6 +26,8 @@ PF_KEY_MORTON = 1
 
 PF_FLUID_VISCOSITY = 1
 PF_FLUID_VORTICITY = 2
+PF_FLUID_SURFACE_TENSION = 4
+PF_FLUID_ADHESION = 8
 PF_SHAPE_MATCH_GLOBAL = 0
 PF_SHAPE_MATCH_LOCAL = 1
 PF_PRIM_PLANE, PF_PRIM_SPHERE, PF_PRIM_BOX, PF_PRIM_CAPSULE = 0, 1, 2, 3
@@ -89,6 +91,8 @@ class FluidDesc(C.Structure):
         ("boundaries", C.POINTER(Range)),
         ("boundary_static", C.POINTER(C.c_uint8)),
         ("vorticity", C.c_float),
+        ("surface_tension", C.c_float),
+        ("adhesion", C.c_float),
     ]
 
 

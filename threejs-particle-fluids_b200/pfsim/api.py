@@ -15,7 +15,7 @@ the reference compiles its kernels). Errors are PfError with the reference's
 "<Class>: <reason>" text. `Simulation` is the façade
 (src/simulation/Simulation.ts:301-634) for containers, fluid boxes, soft
 spheres and boxes, cloth sheets and primitive colliders, with the reference's
-viscosity and vorticity defaults; it has no surface tension or adhesion.
+fluid defaults (viscosity, surface tension, vorticity, adhesion).
 """
 
 from __future__ import annotations
@@ -92,13 +92,15 @@ class FluidSystem:
     def __init__(self, particles: ParticleSystem, range: tuple[int, int] | None = None, rest_density: float = 1000.0,
                  particle_spacing: float | None = None, smoothing_radius: float | None = None,
                  compliance: float = 1e-4, viscosity: float | None = None, vorticity: float | None = None,
+                 surface_tension: float | None = None, adhesion: float | None = None,
                  boundaries: Sequence[tuple[int, int]] = (), boundary_static: Sequence[bool] = ()):
         spacing = particle_spacing if particle_spacing is not None else 2.0 * particles.particle_radius
         h = smoothing_radius if smoothing_radius is not None else 2.0 * spacing
         self.particles = particles
         self.opts = R.FluidOpts(range=tuple(range) if range else (0, particles.capacity), rest_density=rest_density,
                                 particle_spacing=spacing, smoothing_radius=h, compliance=compliance,
-                                viscosity=viscosity, vorticity=vorticity, boundaries=list(boundaries),
+                                viscosity=viscosity, vorticity=vorticity, surface_tension=surface_tension,
+                                adhesion=adhesion, boundaries=list(boundaries),
                                 boundary_static=list(boundary_static))
     kind = "fluid"
 
@@ -250,6 +252,8 @@ class _FluidReq:
     box: tuple
     viscosity: float
     vorticity: float
+    surface_tension: float
+    adhesion: float
 
 
 @dataclass
@@ -302,11 +306,13 @@ class Simulation:
         if self.loop is not None:
             raise N.PfError(N.PF_ERR_STATE, f"{what}: the simulation has started")
 
-    def add_fluid(self, box, viscosity: float = 0.01, vorticity: float = 0.02) -> None:
-        """Simulation.addFluid (Simulation.ts:342-368) with its viscosity and
-        vorticity defaults; surface tension and adhesion are not built."""
+    def add_fluid(self, box, viscosity: float = 0.01, vorticity: float = 0.02, surface_tension: float = 0.1,
+                  adhesion: float = 0.1) -> None:
+        """Simulation.addFluid (Simulation.ts:342-368) with its defaults:
+        viscosity 0.01, surface tension 0.1, vorticity 0.02, adhesion 0.1."""
         self._not_started("addFluid")
-        self.fluids.append(_FluidReq((tuple(box[0]), tuple(box[1])), viscosity, vorticity))
+        self.fluids.append(_FluidReq((tuple(box[0]), tuple(box[1])), viscosity, vorticity, surface_tension,
+                                     adhesion))
 
     def add_softbody(self, shape: str, center, size: float, softness: float = 0.5, density: float = 1000.0) -> None:
         self._not_started("addSoftbody")
@@ -367,7 +373,9 @@ class Simulation:
             mats.append(("fluid", R.FluidOpts(range=(n, len(pts)), rest_density=rho0,
                                               particle_spacing=(mass / rho0) ** (1 / 3), smoothing_radius=h,
                                               compliance=1e-4, viscosity=f.viscosity,
-                                              vorticity=f.vorticity or None)))
+                                              vorticity=f.vorticity or None,
+                                              surface_tension=f.surface_tension or None,
+                                              adhesion=f.adhesion or None)))
             n += len(pts)
         bodies = []
         for b in self.softs:

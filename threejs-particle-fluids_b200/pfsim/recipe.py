@@ -41,6 +41,8 @@ class FluidOpts:
     compliance: float = -1.0
     viscosity: float | None = None
     vorticity: float | None = None
+    surface_tension: float | None = None
+    adhesion: float | None = None
     boundaries: list[tuple[int, int]] = field(default_factory=list)
     boundary_static: list[bool] = field(default_factory=list)
 
@@ -242,6 +244,12 @@ def fluid_desc(o: FluidOpts, keep: _Keep) -> N.FluidDesc:
     if o.vorticity is not None:
         d.vorticity = o.vorticity
         d.flags |= N.PF_FLUID_VORTICITY
+    if o.surface_tension is not None:
+        d.surface_tension = o.surface_tension
+        d.flags |= N.PF_FLUID_SURFACE_TENSION
+    if o.adhesion is not None:
+        d.adhesion = o.adhesion
+        d.flags |= N.PF_FLUID_ADHESION
     if o.boundaries:
         arr = (N.Range * len(o.boundaries))(*[N.Range(s, c) for s, c in o.boundaries])
         keep.refs.append(arr)
