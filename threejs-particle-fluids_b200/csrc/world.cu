@@ -168,11 +168,32 @@ __global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_
   V.cur.bv[k] = 1.0f / fmaxf(sum, 1e-12f);
 }
 
+// A 256-thread block covers one 256-slot chunk, hence one scene: its
+// primitives are staged in shared memory once per block (all threads,
+// before any returns), and read from there by every particle.
+constexpr uint32_t kSmemPrims = 16;
+struct PrimStage {
+  pf_primitive p[kSmemPrims];
+};
+__device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, PrimStage& st) {
+  const uint32_t first = blockIdx.x * blockDim.x;
+  const uint32_t sb = first < V.n ? scene_index(V, first) : 0u;
+  const DevScene& S = V.scenes[sb];
+  const pf_primitive* src = V.prims + S.prim_base;
+  if (S.prim_count > kSmemPrims) return src;  // uniform over the block
+  constexpr uint32_t kWords = sizeof(pf_primitive) / 4;
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(st.p);
+  for (uint32_t t = threadIdx.x; t < S.prim_count * kWords; t += blockDim.x) d[t] = __ldg(w + t);
+  __syncthreads();
+  return st.p;
+}
+
 // The colliders of particle k's scene against its predicted position xs4
 // (w = inverse mass), their multipliers updated; the fixed-point position
 // changes summed in registers and applied. Returns whether xs4 changed.
 __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevScene& S, uint32_t s, uint32_t k,
-                                                 float4& xs4) {
+                                                 float4& xs4, const pf_primitive* __restrict__ prims) {
   const float w = xs4.w;
   if (!(w > 0.0f)) return false;
   const f3 xstar = xyz(xs4);
@@ -182,7 +203,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
   uint32_t tx = 0, ty = 0, tz = 0;
   bool any = false;
   for (uint32_t p = 0; p < S.prim_count; ++p) {
-    const pf_primitive& P = V.prims[S.prim_base + p];
+    const pf_primitive& P = prims[p];
     float phi;
     f3 nrm;
     prim_sdf(P, xstar, clock, &phi, &nrm);
@@ -244,6 +265,8 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
 // positionDelta.ts:217-226, then the reaction accumulator's apply over the
 // covering range of the fluid's boundaries (FluidSystem.ts:280-287).
 __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  __shared__ PrimStage st;
+  const pf_primitive* prims = stage_prims(V, st);
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
@@ -277,7 +300,7 @@ __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t ra
     }
   }
   // the scene's colliders follow its last material in the same pass
-  if (S.collide_rank1 == rank + 1 && collide_particle(V, S, s, k, x)) changed = true;
+  if (S.collide_rank1 == rank + 1 && collide_particle(V, S, s, k, x, prims)) changed = true;
   if (changed) V.cur.xs[k] = x;
 }
 
@@ -307,24 +330,29 @@ __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t ran
 }
 
 // ------------------------------------------------------------ colliders ----
+
 // PrimitiveSet.ts:339-365 + SDFCollider.ts:256-281 with collider.ts:53-89,
 // fused with the position accumulator's apply (loop.ts:225): a contact only
 // adds to its own particle, so the sum of rounded ticks is formed in
 // registers. Scenes whose last material is a fluid run this inside the
 // fluid's apply instead (collide_rank1).
 __global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, uint32_t it) {
+  __shared__ PrimStage st;
+  const pf_primitive* prims = stage_prims(V, st);
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
   if (S.prim_count + S.sdf_count == 0 || S.collide_rank1 || sub >= S.substeps || it >= S.iterations) return;
   float4 xs4 = V.cur.xs[k];
-  if (collide_particle(V, S, s, k, xs4)) V.cur.xs[k] = xs4;
+  if (collide_particle(V, S, s, k, xs4, prims)) V.cur.xs[k] = xs4;
 }
 
 // PrimitiveSet.ts:367-398 with collider.ts:96-118, fused with the velocity
 // accumulator's apply (loop.ts:226-230).
 __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) {
+  __shared__ PrimStage st;
+  const pf_primitive* prims = stage_prims(V, st);
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
@@ -341,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   for (uint32_t p = 0; p < S.prim_count; ++p) {
     const float ln = V.plam[(size_t)k * V.prim_stride + p].x;
     if (!(ln > 0.0f)) continue;
-    const pf_primitive& P = V.prims[S.prim_base + p];
+    const pf_primitive& P = prims[p];
     float phi;
     f3 g;
     prim_sdf(P, xstar, clock, &phi, &g);
