@@ -213,10 +213,12 @@ typedef struct pf_softbody_desc {
 PF_API pf_status pf_add_softbodies(pf_scene* scene, const pf_softbody_desc* desc,
                                    uint32_t* material_index);
 
-/* new ClothSystem(particles, {graph, offset, stretchCompliance})
- * (src/cloth/ClothSystem.ts:37-70, 102-141, 190-202) with the graph produced
- * by createClothGraph (src/cloth/graph.ts:130-342). Distance (stretch)
- * constraints only; the cloth's particles are uploaded from the graph. */
+/* new ClothSystem(particles, {graph, offset, stretchCompliance, bendCompliance})
+ * (src/cloth/ClothSystem.ts:37-70, 102-141, 190-212) with the graph produced
+ * by createClothGraph (src/cloth/graph.ts:130-342): distance (stretch)
+ * constraints, and dihedral bending constraints when the graph has bending
+ * tuples (src/cloth/bending.ts, solved after the stretch colours each
+ * iteration). The cloth's particles are uploaded from the graph. */
 typedef struct pf_cloth_desc {
   uint32_t offset;
   uint32_t n_particles;
@@ -226,6 +228,10 @@ typedef struct pf_cloth_desc {
   const uint32_t* pairs;        /* host cloth-local pairs (graph.distancePairs) */
   const float* rest_lengths;    /* host n_pairs (graph.distanceRestLengths) */
   float stretch_compliance;     /* < 0 selects the default 1e-7 */
+  uint32_t n_bending;           /* 0: no bending constraints */
+  const uint32_t* bending;      /* host cloth-local (p1, p2, p3, p4) x n_bending (graph.bendingTuples) */
+  const float* bending_rest;    /* host n_bending signed rest angles (graph.bendingRestAngles) */
+  float bend_compliance;        /* < 0 selects the default 1e-5 */
 } pf_cloth_desc;
 PF_API pf_status pf_add_cloth(pf_scene* scene, const pf_cloth_desc* desc, uint32_t* material_index);
 

@@ -342,6 +342,11 @@ struct Cloth {
   std::vector<T> rest, compliance;
   std::vector<T> lambda;
   std::vector<std::vector<uint32_t>> groups;
+  // bending.ts: (p1, p2, p3, p4) absolute indices, rest angles, one compliance
+  std::vector<uint32_t> bend;
+  std::vector<T> bendRest, bendLambda;
+  T bendCompliance = 0;
+  std::vector<std::vector<uint32_t>> bendGroups;
 };
 
 struct Prim {
@@ -1385,6 +1390,39 @@ struct Engine {
         cl.lambda[c] = lc + dl;
       }
     }
+    // bending.ts:130-235, after the stretch colours (ClothSystem.ts:193-212)
+    for (const auto& grp : cl.bendGroups) {
+      for (uint32_t c : grp) {
+        const uint32_t* t = cl.bend.data() + 4 * static_cast<size_t>(c);
+        const V3<T> x1 = p3(pred, t[0]), x2 = p3(pred, t[1]), x3 = p3(pred, t[2]), x4 = p3(pred, t[3]);
+        const T w1 = invMass[t[0]], w2 = invMass[t[1]], w3 = invMass[t[2]], w4 = invMass[t[3]];
+        const V3<T> E = x2 - x1;
+        const T e2 = dot(E, E);
+        if (e2 < static_cast<T>(1e-24)) continue;
+        const T el = std::sqrt(e2);
+        const V3<T> a3 = x3 - x1, b3 = x3 - x2, n1 = cross(a3, b3);
+        const V3<T> a4 = x4 - x2, b4 = x4 - x1, n2 = cross(a4, b4);
+        const T n1s = dot(n1, n1), n2s = dot(n2, n2);
+        if (n1s < static_cast<T>(1e-24) || n2s < static_cast<T>(1e-24)) continue;
+        const T theta = std::atan2(dot(cross(n1, n2), E), dot(n1, n2) * el);
+        const T C = theta - cl.bendRest[c];
+        const V3<T> N1 = n1 / n1s, N2 = n2 / n2s;
+        const V3<T> g3 = neg(N1 * el), g4 = neg(N2 * el);
+        const T c31 = dot(b3, E) / el, c32 = dot(a4, E) / el, c41 = dot(a3, E) / el, c42 = dot(b4, E) / el;
+        const V3<T> g1 = neg(N1 * c31 + N2 * c32);
+        const V3<T> g2 = N1 * c41 + N2 * c42;
+        const T sg = dot(g1, g1) * w1 + dot(g2, g2) * w2 + dot(g3, g3) * w3 + dot(g4, g4) * w4;
+        if (sg <= static_cast<T>(1e-30)) continue;
+        const T lc = cl.bendLambda[c];
+        const T at = cl.bendCompliance / (dt * dt);
+        const T dl = (-C - at * lc) / (sg + at);
+        set3(pred, t[0], x1 + g1 * (w1 * dl), 0);
+        set3(pred, t[1], x2 + g2 * (w2 * dl), 0);
+        set3(pred, t[2], x3 + g3 * (w3 * dl), 0);
+        set3(pred, t[3], x4 + g4 * (w4 * dl), 0);
+        cl.bendLambda[c] = lc + dl;
+      }
+    }
   }
 
   // --------------------------------------------------------- the loop ----
@@ -1443,6 +1481,7 @@ struct Engine {
       } else {
         Cloth<T>& cl = cloths[m.second];
         std::fill(cl.lambda.begin(), cl.lambda.end(), static_cast<T>(0));
+        std::fill(cl.bendLambda.begin(), cl.bendLambda.end(), static_cast<T>(0));
       }
     }
     for (uint32_t it = 0; it < iterations; ++it) {
@@ -1564,7 +1603,8 @@ uint32_t next_pow2(uint64_t n) {
 }
 
 // Greedy colouring in constraint order (types.ts:95-150).
-std::vector<std::vector<uint32_t>> color_constraints(const std::vector<uint32_t>& pairs, uint32_t n) {
+std::vector<std::vector<uint32_t>> color_constraints(const std::vector<uint32_t>& pairs, uint32_t n,
+                                                     int arity = 2) {
   std::vector<uint32_t> groupOf(n);
   std::vector<std::vector<uint32_t>> particleGroups;
   uint32_t maxP = 0;
@@ -1575,8 +1615,8 @@ std::vector<std::vector<uint32_t>> color_constraints(const std::vector<uint32_t>
     uint32_t g = 0;
     for (;;) {
       bool conflict = false;
-      for (int k = 0; k < 2 && !conflict; ++k) {
-        const auto& owned = particleGroups[pairs[2 * c + k]];
+      for (int k = 0; k < arity && !conflict; ++k) {
+        const auto& owned = particleGroups[pairs[static_cast<size_t>(arity) * c + k]];
         conflict = std::find(owned.begin(), owned.end(), g) != owned.end();
       }
       if (!conflict) break;
@@ -1584,8 +1624,8 @@ std::vector<std::vector<uint32_t>> color_constraints(const std::vector<uint32_t>
     }
     groupOf[c] = g;
     numGroups = std::max(numGroups, g + 1);
-    for (int k = 0; k < 2; ++k) {
-      auto& owned = particleGroups[pairs[2 * c + k]];
+    for (int k = 0; k < arity; ++k) {
+      auto& owned = particleGroups[pairs[static_cast<size_t>(arity) * c + k]];
       if (std::find(owned.begin(), owned.end(), g) == owned.end()) owned.push_back(g);
     }
   }
@@ -1951,6 +1991,16 @@ int or_add_cloth(void* h, const pf_cloth_desc* d, uint32_t* mat) {
     for (uint32_t c = 0; c < d->n_pairs; ++c) cl.rest[c] = d->rest_lengths[c];
     cl.lambda.assign(d->n_pairs, 0);
     cl.groups = color_constraints(cl.pairs, d->n_pairs);
+    if (d->n_bending) {
+      const double bc = d->bend_compliance >= 0 ? d->bend_compliance : 1e-5;
+      cl.bend.resize(4 * static_cast<size_t>(d->n_bending));
+      for (size_t q = 0; q < cl.bend.size(); ++q) cl.bend[q] = d->offset + d->bending[q];
+      cl.bendRest.resize(d->n_bending);
+      for (uint32_t c = 0; c < d->n_bending; ++c) cl.bendRest[c] = d->bending_rest[c];
+      cl.bendLambda.assign(d->n_bending, 0);
+      cl.bendCompliance = static_cast<T>(static_cast<float>(bc));
+      cl.bendGroups = color_constraints(cl.bend, d->n_bending, 4);
+    }
     e.cloths.push_back(std::move(cl));
     e.materials.push_back({MAT_CLOTH, static_cast<int>(e.cloths.size() - 1)});
     if (mat) *mat = static_cast<uint32_t>(e.materials.size() - 1);

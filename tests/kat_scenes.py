@@ -236,3 +236,28 @@ def sdf_rotated_scaled():
                    sdfs=[g], loop=R.LoopOpts(substeps=1, iterations=4, gravity=(0.0, 0.0, 0.0)),
                    name="sdf-rotated-scaled")
     return rec, center, scale * 0.5
+
+
+# ---- cloth bending (tests/analytical/cloth/bending-rest.gpu.test.ts) ----
+def folded_quad(dihedral: float):
+    """bending-rest.gpu.test.ts:33-54: two triangles sharing the edge
+    (0,0,0)-(1,0,0), the second rotated about it so that the dihedral is
+    `dihedral`; edge endpoints pinned; stretch 1e-7, bend 1e-5, radius 0.05,
+    8 substeps x 1 iteration, no gravity."""
+    from pfsim import shapes
+
+    c, s = np.cos(np.pi - dihedral), np.sin(np.pi - dihedral)
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1, 0], [0.5, c, s]], np.float64)
+    g = shapes.create_cloth_graph(pos, np.array([0, 1, 2, 0, 3, 1]), 0.2, pinned=[0, 1])
+    cloth = R.ClothOpts(offset=0, positions=g.positions.astype(np.float32), inv_mass=g.inv_mass, pairs=g.pairs,
+                        rest_lengths=g.rest_lengths, stretch_compliance=1e-7, bending=g.bending,
+                        bending_rest=g.bending_rest.astype(np.float32), bend_compliance=1e-5)
+    rec = R.Recipe(capacity=4, radius=0.05, materials=[("cloth", cloth)],
+                   loop=R.LoopOpts(substeps=8, iterations=1, gravity=(0.0, 0.0, 0.0)), name="folded-quad")
+    return rec, g
+
+
+def signed_dihedral(pos: np.ndarray) -> float:
+    from pfsim import shapes
+
+    return float(shapes.dihedral_angles(np.asarray(pos, np.float64)[:, :3], np.array([[0, 1, 2, 3]]))[0])

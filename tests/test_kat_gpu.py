@@ -84,3 +84,15 @@ def test_sdf_rotated_scaled_projection(cuda, cpu):
     assert (d < radius - 5e-3).sum() == 0
     # 1e-5 of the extent: the scaled sphere spans 2 m
     assert float(np.abs(pa - b.readback(N.PF_FIELD_POSITIONS)).max()) < 2e-5
+
+
+def test_bending_holds_rest_angle(cuda, cpu):
+    rec, g = K.folded_quad(np.pi / 2)
+    a, b = cuda.build(rec), cpu.build(rec)
+    a0 = K.signed_dihedral(g.positions)
+    for _ in range(60):
+        a.step(K.DT)
+        b.step(K.DT)
+    pa = a.readback(N.PF_FIELD_POSITIONS)
+    assert abs(np.degrees(K.signed_dihedral(pa) - a0)) < 2.0
+    assert float(np.abs(pa - b.readback(N.PF_FIELD_POSITIONS)).max()) < 1e-5

@@ -176,3 +176,25 @@ def test_surface_tension_and_adhesion_one_frame(oracle, cuda):
     a, b = one_frame(oracle, cuda, r, frames=2)
     assert max_dev(a, b) <= TOL
     assert max_dev(a, b, N.PF_FIELD_DENSITY) <= 0.5  # kg/m^3, rho ~ 1000
+
+
+@pytest.mark.parametrize("side", [32, 64])
+def test_cloth_bending_one_frame(oracle, cuda, side):
+    """Stretch and dihedral bending colours (bending.ts) against the oracle."""
+    r = W.cloth_sheet(side, seed=side + 1, bend_compliance=1e-5)
+    a, b = one_frame(oracle, cuda, r, frames=3)
+    assert max_dev(a, b) <= TOL
+
+
+def test_cloth_bending_batch_matches_plain(cuda):
+    """Bending cloths batched with fluids (second stream) equal their plain steps."""
+    recipes = [W.cloth_sheet(48, seed=2, bend_compliance=1e-5), W.dam_break(4000, seed=3),
+               W.cloth_sheet(32, seed=4, bend_compliance=1e-4)]
+    plain = [cuda.build(r) for r in recipes]
+    batch = R.Batch([cuda.build(r) for r in recipes], use_graph=True)
+    for _ in range(3):
+        for s in plain:
+            s.step(DT)
+        batch.step(DT)
+    for i, s in enumerate(plain):
+        assert np.array_equal(s.readback(N.PF_FIELD_POSITIONS), batch.readback(i, N.PF_FIELD_POSITIONS)), i

@@ -108,24 +108,32 @@ double smallest_eigenvalue(double a00, double a01, double a02, double a11, doubl
 
 // Greedy colouring in constraint order: each constraint takes the lowest
 // colour none of its particles has yet (types.ts:95-150).
-std::vector<std::vector<uint32_t>> color_pairs(const std::vector<uint32_t>& pairs, uint32_t n, uint32_t cap) {
+// types.ts:59-114: greedy colouring in constraint order; each constraint of
+// `arity` particles takes the lowest group none of its particles owns yet.
+std::vector<std::vector<uint32_t>> color_groups(const std::vector<uint32_t>& parts, uint32_t arity, uint32_t n,
+                                                uint32_t cap) {
   std::vector<std::vector<uint32_t>> owned(cap);
   std::vector<std::vector<uint32_t>> colors;
   for (uint32_t c = 0; c < n; ++c) {
-    const uint32_t a = pairs[2 * c], b = pairs[2 * c + 1];
     uint32_t g = 0;
     for (;;) {
-      const bool ca = std::find(owned[a].begin(), owned[a].end(), g) != owned[a].end();
-      const bool cb = std::find(owned[b].begin(), owned[b].end(), g) != owned[b].end();
-      if (!ca && !cb) break;
+      bool clash = false;
+      for (uint32_t k = 0; k < arity && !clash; ++k) {
+        const auto& o = owned[parts[(size_t)arity * c + k]];
+        clash = std::find(o.begin(), o.end(), g) != o.end();
+      }
+      if (!clash) break;
       ++g;
     }
     if (g >= colors.size()) colors.resize(g + 1);
     colors[g].push_back(c);
-    owned[a].push_back(g);
-    owned[b].push_back(g);
+    for (uint32_t k = 0; k < arity; ++k) owned[parts[(size_t)arity * c + k]].push_back(g);
   }
   return colors;
+}
+
+std::vector<std::vector<uint32_t>> color_pairs(const std::vector<uint32_t>& pairs, uint32_t n, uint32_t cap) {
+  return color_groups(pairs, 2, n, cap);
 }
 
 }  // namespace
@@ -415,6 +423,28 @@ pf_status pf_add_cloth(pf_scene* s, const pf_cloth_desc* d, uint32_t* mat) {
   cl.rest.assign(d->rest_lengths, d->rest_lengths + d->n_pairs);
   cl.compliance = (float)comp;
   cl.colors = color_pairs(cl.pairs, d->n_pairs, sp.cap);
+  // bending.ts:46-129: tuples of four distinct cloth particles, rest angles,
+  // one compliance (ClothSystem default 1e-5), coloured with arity 4
+  if (d->n_bending) {
+    if (!d->bending || !d->bending_rest)
+      return fail(PF_ERR_INVALID, "createClothBendingConstraints: tuples or restAngles missing");
+    const double bc = d->bend_compliance >= 0 ? d->bend_compliance : 1e-5;
+    if (!std::isfinite(bc)) return fail(PF_ERR_INVALID, "ClothSystem: bendCompliance must be >= 0");
+    cl.bend.resize(4ull * d->n_bending);
+    for (uint32_t q = 0; q < d->n_bending; ++q) {
+      const uint32_t* t = d->bending + 4ull * q;
+      for (int k = 0; k < 4; ++k) {
+        if (t[k] >= d->n_particles)
+          return fail(PF_ERR_INVALID, "createClothBendingConstraints: tuple index exceeds the cloth's particles");
+        for (int m = 0; m < k; ++m)
+          if (t[m] == t[k]) return fail(PF_ERR_INVALID, "createClothBendingConstraints: tuple has duplicate indices");
+        cl.bend[4ull * q + k] = d->offset + t[k];
+      }
+    }
+    cl.bend_rest.assign(d->bending_rest, d->bending_rest + d->n_bending);
+    cl.bend_compliance = (float)bc;
+    cl.bend_colors = color_groups(cl.bend, 4, d->n_bending, sp.cap);
+  }
   sp.cloths.push_back(std::move(cl));
   sp.materials.push_back({MAT_CLOTH, (uint32_t)sp.cloths.size() - 1});
   if (mat) *mat = (uint32_t)sp.materials.size() - 1;

@@ -441,6 +441,52 @@ __global__ void __launch_bounds__(kBlock) k_cloth(WorldView V, uint32_t begin, u
   V.c_lambda[q] = lc + dl;
 }
 
+// bending.ts:130-235: one colour of dihedral bending constraints (no two
+// share a particle); the closed-form gradients of the signed angle
+// theta = atan2((N1 x N2).E, (N1.N2)|E|) with E = p2 - p1,
+// N1 = (p3 - p1) x (p3 - p2), N2 = (p4 - p2) x (p4 - p1), and the XPBD
+// multiplier update (xpbd.ts:26-36).
+__global__ void __launch_bounds__(kBlock) k_bend(WorldView V, uint32_t begin, uint32_t end, uint32_t sub, uint32_t it) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const DevScene& S = V.scenes[V.b_scene[q]];
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const uint4 id = V.b_idx[q];
+  const uint32_t i1 = V.inv[id.x], i2 = V.inv[id.y], i3 = V.inv[id.z], i4 = V.inv[id.w];
+  const float4 p1 = V.cur.xs[i1], p2 = V.cur.xs[i2], p3 = V.cur.xs[i3], p4 = V.cur.xs[i4];
+  const f3 x1 = xyz(p1), x2 = xyz(p2), x3 = xyz(p3), x4 = xyz(p4);
+  const f3 E = x2 - x1;
+  const float e2 = dot(E, E);
+  if (e2 < 1e-24f) return;
+  const float el = sqrtf(e2);
+  const f3 a3 = x3 - x1, b3 = x3 - x2;
+  const f3 n1 = cross(a3, b3);
+  const f3 a4 = x4 - x2, b4 = x4 - x1;
+  const f3 n2 = cross(a4, b4);
+  const float n1s = dot(n1, n1), n2s = dot(n2, n2);
+  if (n1s < 1e-24f || n2s < 1e-24f) return;
+  const float st = dot(cross(n1, n2), E);
+  const float ct = dot(n1, n2) * el;
+  const float C = atan2f(st, ct) - V.b_rest[q];
+  const f3 N1 = n1 / n1s, N2 = n2 / n2s;
+  const f3 g3 = neg(N1 * el), g4 = neg(N2 * el);
+  const float c31 = dot(b3, E) / el, c32 = dot(a4, E) / el;
+  const float c41 = dot(a3, E) / el, c42 = dot(b4, E) / el;
+  const f3 g1 = neg(N1 * c31 + N2 * c32);
+  const f3 g2 = N1 * c41 + N2 * c42;
+  const float w1 = p1.w, w2 = p2.w, w3 = p3.w, w4 = p4.w;
+  const float sg = dot(g1, g1) * w1 + dot(g2, g2) * w2 + dot(g3, g3) * w3 + dot(g4, g4) * w4;
+  if (sg <= 1e-30f) return;
+  const float lc = V.b_lambda[q];
+  const float at = V.b_comp[q] / (S.dt * S.dt);
+  const float dl = (-C - at * lc) / (sg + at);
+  V.cur.xs[i1] = with_w(x1 + g1 * (w1 * dl), w1);
+  V.cur.xs[i2] = with_w(x2 + g2 * (w2 * dl), w2);
+  V.cur.xs[i3] = with_w(x3 + g3 * (w3 * dl), w3);
+  V.cur.xs[i4] = with_w(x4 + g4 * (w4 * dl), w4);
+  V.b_lambda[q] = lc + dl;
+}
+
 // ---------------------------------------------------------- soft bodies ----
 __device__ __forceinline__ bool group_active(const WorldView& V, uint32_t g, uint32_t rank, uint32_t sub,
                                              uint32_t it, const DevSoft** D, const DevScene** S) {
@@ -1179,6 +1225,37 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
       cloth_ranges_[r].push_back({begin, (uint32_t)ci.size()});
     }
   }
+  // ---- cloth bending constraints by (rank, colour) ---------------------
+  std::vector<uint4> bidx;
+  std::vector<float> brest, bcomp;
+  std::vector<uint32_t> bsc;
+  bend_ranges_.assign(max_rank_, {});
+  for (uint32_t r = 0; r < max_rank_; ++r) {
+    uint32_t ncol = 0;
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      if (r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)
+        ncol = std::max(ncol, (uint32_t)sp.cloths[sp.materials[r].second].bend_colors.size());
+    }
+    for (uint32_t c = 0; c < ncol; ++c) {
+      const uint32_t begin = (uint32_t)bidx.size();
+      for (uint32_t s = 0; s < K; ++s) {
+        const SceneSpec& sp = *specs[s];
+        if (!(r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)) continue;
+        const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+        if (c >= cl.bend_colors.size()) continue;
+        const uint32_t base = h_scenes_[s].seg_start;
+        for (uint32_t q : cl.bend_colors[c]) {
+          const uint32_t* t = cl.bend.data() + 4ull * q;
+          bidx.push_back(make_uint4(base + t[0], base + t[1], base + t[2], base + t[3]));
+          brest.push_back(cl.bend_rest[q]);
+          bcomp.push_back(cl.bend_compliance);
+          bsc.push_back(s);
+        }
+      }
+      bend_ranges_[r].push_back({begin, (uint32_t)bidx.size()});
+    }
+  }
   // ---- soft-body tables (global by id) ----------------------------------
   std::vector<uint32_t> grp, grp_soft, csr_off(n_ + 1, 0), csr_idx;
   std::vector<float> rest4(4ull * n_, 0.0f), restc4(4ull * n_, 0.0f), weights(n_, 0.0f);
@@ -1329,6 +1406,11 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.c_comp = cv.take<float>(ccomp.size());
     base_.c_scene = cv.take<uint32_t>(csc.size());
     base_.c_lambda = cv.take<float>(ci.size());
+    base_.b_idx = cv.take<uint4>(bidx.size());
+    base_.b_rest = cv.take<float>(brest.size());
+    base_.b_comp = cv.take<float>(bcomp.size());
+    base_.b_scene = cv.take<uint32_t>(bsc.size());
+    base_.b_lambda = cv.take<float>(bidx.size());
     stage_pos_ = cv.take<float4>(total_real);
     prefix_dev_ = cv.take<uint64_t>(K);
   };
@@ -1354,6 +1436,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   base_.n_grp = (uint32_t)grp.size();
   base_.n_bodies = (uint32_t)h_bodies_.size();
   base_.n_cons = (uint32_t)ci.size();
+  base_.n_bend = (uint32_t)bidx.size();
   base_.max_tiles = (uint32_t)max_tiles;
   base_.n_grid_scenes = (uint32_t)grid_scene.size();
   base_.n_rows = row_base.back();
@@ -1449,6 +1532,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_TRY(up(base_.c_rest, crest.data(), 4 * crest.size()));
   PF_TRY(up(base_.c_comp, ccomp.data(), 4 * ccomp.size()));
   PF_TRY(up(base_.c_scene, csc.data(), 4 * csc.size()));
+  PF_TRY(up(base_.b_idx, bidx.data(), sizeof(uint4) * bidx.size()));
+  PF_TRY(up(base_.b_rest, brest.data(), 4 * brest.size()));
+  PF_TRY(up(base_.b_comp, bcomp.data(), 4 * bcomp.size()));
+  PF_TRY(up(base_.b_scene, bsc.data(), 4 * bsc.size()));
   PF_TRY(up(prefix_dev_, prefix_.data(), 8 * prefix_.size()));
   PF_TRY(up(base_.row_base, row_base.data(), 4 * row_base.size()));
   PF_TRY(up(base_.grid_scene, grid_scene.data(), 4 * grid_scene.size()));
@@ -1654,6 +1741,21 @@ void World::run_init_pass() {
   launch_slots(k_boundary_volume, n_, stream_, view(parity_), 1u, 0u);
 }
 
+// ClothSystem.ts:193-212: the stretch colours, then the bending colours.
+void World::launch_cloth_rank(const WorldView& V, uint32_t r, uint32_t s, uint32_t it, cudaStream_t st) {
+  for (auto& rg : cloth_ranges_[r])
+    if (rg.second > rg.first) {
+      k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, st>>>(V, rg.first, rg.second, s, it);
+      ++t_launches;
+    }
+  if (r < bend_ranges_.size())
+    for (auto& rg : bend_ranges_[r])
+      if (rg.second > rg.first) {
+        k_bend<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, st>>>(V, rg.first, rg.second, s, it);
+        ++t_launches;
+      }
+}
+
 void World::run_substep(uint32_t s, uint32_t parity) {
   WorldView V = view(parity);
   launch_slots(k_predict, n_, stream_, V, s);
@@ -1684,6 +1786,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
   if (base_.n_cons) cudaMemsetAsync(base_.c_lambda, 0, 4ull * base_.n_cons, stream_);
+  if (base_.n_bend) cudaMemsetAsync(base_.b_lambda, 0, 4ull * base_.n_bend, stream_);
   // iterations
   // Cloth-only scenes (and material-free scenes with colliders) share no
   // slot with the others: their colour sweeps and collider passes run on a
@@ -1693,12 +1796,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     cudaEventRecord(ev_fork_, stream_);
     cudaStreamWaitEvent(side_stream_, ev_fork_, 0);
     for (uint32_t it = 0; it < max_iter_; ++it) {
-      for (uint32_t r = 0; r < cloth_ranges_.size(); ++r)
-        for (auto& rg : cloth_ranges_[r])
-          if (rg.second > rg.first) {
-            k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, side_stream_>>>(V, rg.first, rg.second, s, it);
-            ++t_launches;
-          }
+      for (uint32_t r = 0; r < cloth_ranges_.size(); ++r) launch_cloth_rank(V, r, s, it, side_stream_);
       if (any_unfused_prims_) launch_slots(k_collide, n_, side_stream_, V, s, it);
     }
   }
@@ -1726,12 +1824,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         k_global_apply<<<base_.n_bodies, 256, 0, stream_>>>(V, r, s, it);
         t_launches += 2;
       }
-      if (!fork && r < cloth_ranges_.size())
-        for (auto& rg : cloth_ranges_[r])
-          if (rg.second > rg.first) {
-            k_cloth<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, stream_>>>(V, rg.first, rg.second, s, it);
-            ++t_launches;
-          }
+      if (!fork && r < cloth_ranges_.size()) launch_cloth_rank(V, r, s, it, stream_);
     }
     if (!fork && any_unfused_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
   }

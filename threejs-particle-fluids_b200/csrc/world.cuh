@@ -71,6 +71,11 @@ struct ClothSpec {
   std::vector<float> rest;
   float compliance = 1e-7f;
   std::vector<std::vector<uint32_t>> colors;  // constraint indices per colour
+  // bending (bending.ts): (p1, p2, p3, p4) absolute indices per constraint
+  std::vector<uint32_t> bend;
+  std::vector<float> bend_rest;
+  float bend_compliance = 1e-5f;
+  std::vector<std::vector<uint32_t>> bend_colors;
 };
 
 // SDFCollider state (SDFCollider.ts:88-137): the grid as half floats plus
@@ -279,6 +284,13 @@ struct WorldView {
   const uint32_t* c_scene;
   float* c_lambda;
   uint32_t n_cons;
+  // cloth bending (bending.ts), by (rank, colour)
+  const uint4* b_idx;  // particle ids (p1, p2, p3, p4)
+  const float* b_rest;
+  const float* b_comp;
+  const uint32_t* b_scene;
+  float* b_lambda;
+  uint32_t n_bend;
 };
 
 class World {
@@ -374,6 +386,8 @@ class World {
   // stage plan
   uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> bend_ranges_;   // [rank] -> per colour [begin,end)
+  void launch_cloth_rank(const WorldView& V, uint32_t r, uint32_t s, uint32_t it, cudaStream_t st);
   bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false, any_vort_ = false;
   bool any_imp_ = false;  // surface tension or adhesion somewhere
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;

@@ -125,6 +125,10 @@ class ClothDesc(C.Structure):
         ("pairs", C.POINTER(C.c_uint32)),
         ("rest_lengths", C.POINTER(C.c_float)),
         ("stretch_compliance", C.c_float),
+        ("n_bending", C.c_uint32),
+        ("bending", C.POINTER(C.c_uint32)),
+        ("bending_rest", C.POINTER(C.c_float)),
+        ("bend_compliance", C.c_float),
     ]
 
 

@@ -121,14 +121,19 @@ class SoftbodySystem:
 
 
 class ClothSystem:
-    """src/cloth/ClothSystem.ts:37-141 with a ClothGraph (pfsim.shapes)."""
+    """src/cloth/ClothSystem.ts:37-141, 190-212 with a ClothGraph (pfsim.shapes):
+    stretch and dihedral bending constraints (aerodynamics and tethers are
+    not built)."""
 
-    def __init__(self, particles: ParticleSystem, graph, offset: int = 0, stretch_compliance: float = 1e-7):
+    def __init__(self, particles: ParticleSystem, graph, offset: int = 0, stretch_compliance: float = 1e-7,
+                 bend_compliance: float = 1e-5):
         self.particles = particles
         self.opts = R.ClothOpts(offset=offset, positions=np.asarray(graph.positions, np.float32),
                                 inv_mass=np.asarray(graph.inv_mass, np.float32), pairs=graph.pairs,
                                 rest_lengths=np.asarray(graph.rest_lengths, np.float32),
-                                stretch_compliance=stretch_compliance)
+                                stretch_compliance=stretch_compliance,
+                                bending=graph.bending, bending_rest=np.asarray(graph.bending_rest, np.float32),
+                                bend_compliance=bend_compliance)
     kind = "cloth"
 
 
@@ -400,7 +405,9 @@ class Simulation:
             g = shapes.create_cloth_graph(pos, idx, 0.2, pinned=pinned)
             mats.append(("cloth", R.ClothOpts(offset=n, positions=g.positions.astype(np.float32), inv_mass=g.inv_mass,
                                               pairs=g.pairs, rest_lengths=g.rest_lengths,
-                                              stretch_compliance=1e-7 * (1.0 + 1e4 * c.softness))))
+                                              stretch_compliance=1e-7 * (1.0 + 1e4 * c.softness),
+                                              bending=g.bending, bending_rest=g.bending_rest.astype(np.float32),
+                                              bend_compliance=1e-5)))
             n += len(pos)
         if n == 0:
             raise N.PfError(N.PF_ERR_STATE, "Simulation: nothing to simulate; add a fluid, soft body or cloth")

@@ -74,6 +74,9 @@ class ClothOpts:
     pairs: np.ndarray  # (m, 2) cloth-local
     rest_lengths: np.ndarray  # (m,)
     stretch_compliance: float = -1.0
+    bending: np.ndarray | None = None  # (b, 4) cloth-local (p1, p2, p3, p4)
+    bending_rest: np.ndarray | None = None  # (b,) signed rest angles
+    bend_compliance: float = -1.0
 
 
 @dataclass
@@ -292,6 +295,12 @@ def cloth_desc(o: ClothOpts, keep: _Keep) -> N.ClothDesc:
     d.pairs = keep.u32(pr)
     d.rest_lengths = keep.f32(o.rest_lengths)
     d.stretch_compliance = o.stretch_compliance
+    if o.bending is not None and len(o.bending):
+        b = np.asarray(o.bending, np.uint32).reshape(-1)
+        d.n_bending = b.size // 4
+        d.bending = keep.u32(b)
+        d.bending_rest = keep.f32(np.asarray(o.bending_rest, np.float32))
+    d.bend_compliance = o.bend_compliance
     return d
 
 

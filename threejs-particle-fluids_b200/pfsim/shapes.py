@@ -12,7 +12,8 @@ all 26 neighbours, which makes each particle's shape-matching group a
 index layout and the reference's createClothGraph (src/cloth/graph.ts:130-342):
 unique triangle edges in first-seen order as distance constraints (structural
 edges plus one shear diagonal per quad), lumped vertex masses from a third of
-each incident triangle's area, pinned vertices at zero inverse mass.
+each incident triangle's area, pinned vertices at zero inverse mass, and a
+bending tuple with its signed rest angle for every edge two triangles share.
 """
 
 from __future__ import annotations
@@ -111,6 +112,25 @@ class ClothGraph:
     inv_mass: np.ndarray  # (n,)
     pairs: np.ndarray  # (m, 2)
     rest_lengths: np.ndarray  # (m,)
+    bending: np.ndarray  # (b, 4): (p1, p2, p3, p4) per edge shared by two triangles
+    bending_rest: np.ndarray  # (b,) signed rest dihedral angles
+
+
+def dihedral_angles(pos: np.ndarray, tuples: np.ndarray) -> np.ndarray:
+    """graph.ts:346-402: the signed dihedral angle of each (p1, p2, p3, p4)
+    tuple, atan2((N1 x N2).E, (N1.N2)|E|) with E = p2 - p1,
+    N1 = (p3 - p1) x (p3 - p2), N2 = (p4 - p2) x (p4 - p1); 0 for a degenerate
+    edge or triangle."""
+    p1, p2, p3, p4 = (pos[tuples[:, k]] for k in range(4))
+    e = p2 - p1
+    el = np.sqrt((e * e).sum(1))
+    n1 = np.cross(p3 - p1, p3 - p2)
+    n2 = np.cross(p4 - p2, p4 - p1)
+    s = (np.cross(n1, n2) * e).sum(1)
+    c = (n1 * n2).sum(1) * el
+    ang = np.arctan2(s, c)
+    bad = (el < 1e-12) | ((n1 * n1).sum(1) < 1e-24) | ((n2 * n2).sum(1) < 1e-24)
+    return np.where(bad, 0.0, ang)
 
 
 def create_cloth_graph(positions, index, surface_density: float = 0.2, pinned=()) -> ClothGraph:
@@ -136,4 +156,26 @@ def create_cloth_graph(positions, index, surface_density: float = 0.2, pinned=()
     inv = np.where(area > 0, 1.0 / np.where(area > 0, area * surface_density, 1.0), 0.0)
     inv[list(pinned)] = 0.0
     rest = np.linalg.norm(pos[pairs[:, 0]] - pos[pairs[:, 1]], axis=1)
-    return ClothGraph(pos, inv, pairs, rest)
+    # graph.ts:300-330: every edge with exactly two incident triangles gives a
+    # bending tuple (edge endpoints ascending, then the two far vertices in
+    # triangle order), in the edges' first-seen order
+    far = np.stack([c, a, b], 1).reshape(-1)
+    order_e = np.argsort(key, kind="stable")
+    sk = key[order_e]
+    starts = np.flatnonzero(np.r_[True, sk[1:] != sk[:-1]])
+    counts = np.diff(np.r_[starts, sk.size])
+    two = counts == 2
+    k2 = sk[starts[two]]
+    f1 = far[order_e[starts[two]]]
+    f2 = far[order_e[starts[two] + 1]]
+    ordr = np.argsort(_edge_rank(keys, k2), kind="stable")
+    tuples = np.stack([k2 // n, k2 % n, f1, f2], -1)[ordr].astype(np.uint32)
+    bending_rest = dihedral_angles(pos, tuples.astype(np.int64))
+    return ClothGraph(pos, inv, pairs, rest, tuples, bending_rest)
+
+
+def _edge_rank(edge_keys_in_order: np.ndarray, query: np.ndarray) -> np.ndarray:
+    """Index of each query key in the first-seen edge order."""
+    idx = np.argsort(edge_keys_in_order, kind="stable")
+    pos = np.searchsorted(edge_keys_in_order[idx], query)
+    return idx[pos]

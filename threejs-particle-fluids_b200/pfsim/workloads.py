@@ -114,7 +114,7 @@ def dam_break(n_budget: int = 5000, seed: int = 0, scale: float = 1.0, jitter: f
 
 
 def cloth_sheet(side: int = 64, seed: int = 0, scale: float = 1.0, compliance: float = 1e-6,
-                substeps: int = 2, iterations: int = 4, offset=(0.0, 0.0, 0.0)):
+                substeps: int = 2, iterations: int = 4, offset=(0.0, 0.0, 0.0), bend_compliance: float | None = None):
     """A hanging cloth sheet of side x side particles (PlaneGeometry with
     side-1 segments per axis, structural + shear distance constraints, the
     top row pinned) inside the dam-break container scaled by `scale`; the
@@ -143,6 +143,9 @@ def cloth_sheet(side: int = 64, seed: int = 0, scale: float = 1.0, compliance: f
     edge = width / (side - 1)
     cloth = R.ClothOpts(offset=0, positions=graph.positions.astype(np.float32), inv_mass=graph.inv_mass,
                         pairs=graph.pairs, rest_lengths=graph.rest_lengths, stretch_compliance=compliance)
+    if bend_compliance is not None:  # dihedral bending as well (the batch configuration has stretch only)
+        cloth.bending, cloth.bending_rest = graph.bending, graph.bending_rest.astype(np.float32)
+        cloth.bend_compliance = bend_compliance
     loop = R.LoopOpts(substeps=substeps, iterations=iterations)
     return R.Recipe(capacity=n, radius=0.5 * edge, materials=[("cloth", cloth)],
                     prims=R.container_walls(tuple(c_lo), tuple(c_hi)), loop=loop, name=f"cloth_{side}x{side}")
