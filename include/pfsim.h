@@ -213,12 +213,19 @@ typedef struct pf_softbody_desc {
 PF_API pf_status pf_add_softbodies(pf_scene* scene, const pf_softbody_desc* desc,
                                    uint32_t* material_index);
 
-/* new ClothSystem(particles, {graph, offset, stretchCompliance, bendCompliance})
- * (src/cloth/ClothSystem.ts:37-70, 102-141, 190-212) with the graph produced
- * by createClothGraph (src/cloth/graph.ts:130-342): distance (stretch)
- * constraints, and dihedral bending constraints when the graph has bending
- * tuples (src/cloth/bending.ts, solved after the stretch colours each
- * iteration). The cloth's particles are uploaded from the graph. */
+/* new ClothSystem(particles, {graph, offset, stretchCompliance, bendCompliance,
+ * tetherCompliance, wind, drag, lift, damping})
+ * (src/cloth/ClothSystem.ts:37-141, 190-245) with the graph produced by
+ * createClothGraph (src/cloth/graph.ts:130-342). Each iteration solves the
+ * distance (stretch) colours, then the dihedral bending colours when the graph
+ * has bending tuples (src/cloth/bending.ts), then the long-range tether
+ * colours when tethers are given (src/cloth/tether.ts; build them from the
+ * pins with pf_cloth_build_tethers). With triangles, aerodynamic drag and
+ * lift move the predicted positions once per substep before the solve
+ * (src/cloth/aero.ts); with has_damping, each particle's velocity is blended
+ * toward the mean of its edge neighbours' after the substep
+ * (ClothSystem.buildDamping, ClothSystem.ts:249-287). The cloth's particles
+ * are uploaded from the graph. */
 typedef struct pf_cloth_desc {
   uint32_t offset;
   uint32_t n_particles;
@@ -232,8 +239,59 @@ typedef struct pf_cloth_desc {
   const uint32_t* bending;      /* host cloth-local (p1, p2, p3, p4) x n_bending (graph.bendingTuples) */
   const float* bending_rest;    /* host n_bending signed rest angles (graph.bendingRestAngles) */
   float bend_compliance;        /* < 0 selects the default 1e-5 */
+  uint32_t n_tethers;           /* 0: no tethers */
+  const uint32_t* tether_particle; /* host cloth-local free particle per tether */
+  const uint32_t* tether_anchor;   /* host cloth-local pinned anchor per tether */
+  const float* tether_rest;        /* host rest radius per tether (metres) */
+  float tether_compliance;      /* < 0 selects the default 0 */
+  uint32_t n_triangles;         /* 0: no drag or lift */
+  const uint32_t* triangles;    /* host cloth-local (i1, i2, i3) x n_triangles (graph.triangles) */
+  float wind[3];                /* m/s */
+  float drag;                   /* 1/2 C_D rho_air; < 0 selects the default 0.6125 */
+  float lift;                   /* 1/2 C_L rho_air; < 0 selects the default 0.3 */
+  uint32_t has_damping;         /* 0: no velocity smoothing pass (damping undefined) */
+  float damping;                /* in [0, 1] */
 } pf_cloth_desc;
 PF_API pf_status pf_add_cloth(pf_scene* scene, const pf_cloth_desc* desc, uint32_t* material_index);
+
+/* ClothSystem.wind / drag / lift / damping / bendCompliance setters
+ * (ClothSystem.ts:143-188) for the cloth added as `material_index`: they
+ * take effect from the next step. drag, lift and bend_compliance must be
+ * >= 0 and finite, damping in [0, 1] (it needs has_damping at creation).
+ * On a scene inside a batch, use the pf_batch_ form with the scene's index. */
+typedef struct pf_cloth_params {
+  float wind[3];
+  float drag;
+  float lift;
+  float damping;
+  float bend_compliance;
+} pf_cloth_params;
+PF_API pf_status pf_cloth_get_params(pf_scene* scene, uint32_t material_index, pf_cloth_params* out);
+PF_API pf_status pf_cloth_set_params(pf_scene* scene, uint32_t material_index, const pf_cloth_params* params);
+
+/* buildTethers (src/cloth/tetherBuild.ts:84-219): long-range attachments of
+ * every free particle (inv_mass > 0) to the nearest pinned particle of each
+ * of its `max_attachments` geodesically closest pinned islands, with rest
+ * radius = geodesic distance x (1 + stretch_tolerance). Islands are the
+ * connected components of the pinned particles over pinned-only edges; the
+ * geodesic distances come from a multi-source Dijkstra per island over the
+ * edge graph weighted by rest length, whose binary-heap order settles ties
+ * as the reference's does. Outputs are cloth-local, particle-major, each
+ * particle's islands nearest first; `capacity` entries are available in
+ * each output array (n_particles x max_attachments always suffices) and
+ * `count` receives the number written. max_attachments 0 selects 4. */
+typedef struct pf_tether_build_desc {
+  uint32_t n_particles;
+  const float* inv_mass;        /* host n_particles (graph.invMass) */
+  uint32_t n_pairs;
+  const uint32_t* pairs;        /* host cloth-local pairs (graph.distancePairs) */
+  const double* rest_lengths;   /* host n_pairs (graph.distanceRestLengths, doubles) */
+  uint32_t max_attachments;
+  double stretch_tolerance;     /* >= 0 */
+} pf_tether_build_desc;
+PF_API pf_status pf_cloth_build_tethers(const pf_tether_build_desc* desc, uint32_t* particle,
+                                        uint32_t* anchor, float* rest, uint32_t capacity,
+                                        uint32_t* count);
 
 /* PrimitiveSet.addPlane/addSphere/addBox/addCapsule and setSphere
  * (src/core/collision/PrimitiveSet.ts:166-257), using the packed GPU record
@@ -318,6 +376,13 @@ typedef enum pf_field {
   PF_FIELD_CELL_PERM = 12          /* uint32 x capacity: particle index per sorted slot */
 } pf_field;
 PF_API pf_status pf_readback(pf_scene* scene, uint32_t field, void* dst_host, size_t bytes);
+/* Whole-field write of POSITIONS, PREDICTED, VELOCITIES (float4 x capacity,
+ * w ignored) or INV_MASS (float x capacity) in particle order, as the
+ * reference's callers set a buffer's array and flag needsUpdate (for
+ * example a test damping velocities between frames, or moving pinned
+ * particles; particles.ts:81-113). Synchronous; takes effect from the next
+ * step. PREDICTED needs a built scene. */
+PF_API pf_status pf_write(pf_scene* scene, uint32_t field, const void* src_host, size_t bytes);
 
 /* SimLoop.readbackOverflow() (loop.ts:59-69, 286-295) plus the neighbour-list
  * flag of FluidSystem.readbackOverflow(). */
@@ -355,8 +420,13 @@ PF_API pf_status pf_batch_step(pf_batch* batch, double dt);
 /* Move scene `index`'s primitive `slot` (PrimitiveSet.setSphere etc.). */
 PF_API pf_status pf_batch_set_primitive(pf_batch* batch, uint32_t index, uint32_t slot,
                                         const pf_primitive* prim);
+/* Scene `index`'s cloth parameters (pf_cloth_set_params). */
+PF_API pf_status pf_batch_cloth_set_params(pf_batch* batch, uint32_t index, uint32_t material_index,
+                                           const pf_cloth_params* params);
 PF_API pf_status pf_batch_readback(pf_batch* batch, uint32_t index, uint32_t field, void* dst_host,
                                    size_t bytes);
+PF_API pf_status pf_batch_write(pf_batch* batch, uint32_t index, uint32_t field, const void* src_host,
+                                size_t bytes);
 PF_API pf_status pf_batch_overflow_read(pf_batch* batch, uint32_t index, pf_overflow* out);
 PF_API pf_status pf_batch_last_step_ms(pf_batch* batch, float* ms);
 /* Particle-substeps one pf_batch_step advances (sum over scenes of N * substeps). */

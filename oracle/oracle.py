@@ -72,6 +72,8 @@ def _bind(L: C.CDLL) -> None:
         "or_sdf_sample": (C.c_int, [C.POINTER(N.SdfDesc), C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float)]),
         "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
+        "or_cloth_set_params": (C.c_int, [P, C.c_uint32, C.POINTER(N.ClothParams)]),
+        "or_write": (C.c_int, [P, C.c_uint32, f32p, C.c_size_t]),
         "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
         "or_step": (C.c_int, [P, C.c_double]),
         "or_readback": (C.c_int, [P, C.c_uint32, P, C.c_size_t, C.c_int]),
@@ -170,6 +172,115 @@ def color_constraints(pairs: np.ndarray) -> tuple[np.ndarray, int]:
     return g, int(k)
 
 
+class _RefHeap:
+    """tetherBuild.ts:226-275: binary min-heap ordered on the distance alone,
+    strict comparisons in both sifts (equal distances keep heap order)."""
+
+    def __init__(self):
+        self.d = []
+
+    def push(self, item):
+        d = self.d
+        d.append(item)
+        i = len(d) - 1
+        while i > 0:
+            p = (i - 1) >> 1
+            if d[i][0] < d[p][0]:
+                d[i], d[p] = d[p], d[i]
+                i = p
+            else:
+                break
+
+    def pop(self):
+        d = self.d
+        top = d[0]
+        last = d.pop()
+        if d:
+            d[0] = last
+            i, n = 0, len(d)
+            while True:
+                l, r, m = 2 * i + 1, 2 * i + 2, i
+                if l < n and d[l][0] < d[m][0]:
+                    m = l
+                if r < n and d[r][0] < d[m][0]:
+                    m = r
+                if m == i:
+                    break
+                d[i], d[m] = d[m], d[i]
+                i = m
+        return top
+
+
+def build_tethers(inv_mass, pairs, rest_lengths, max_attachments: int = 4, stretch_tolerance: float = 0.0):
+    """buildTethers (tetherBuild.ts:84-219) in pure Python for small graphs:
+    pinned islands over pinned-only edges, one multi-source Dijkstra per
+    island over the rest-length-weighted edges, the nearest max_attachments
+    islands of each free particle. Returns (particle, anchor, rest radius
+    as float32) arrays, particle-major."""
+    inv = np.asarray(inv_mass, np.float32)
+    n = inv.size
+    pr = np.asarray(pairs, np.int64).reshape(-1, 2)
+    rl = [float(x) for x in np.asarray(rest_lengths, np.float64)]
+    pinned = [bool(inv[i] == 0) for i in range(n)]
+    empty = (np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.float32))
+    if not any(pinned):
+        return empty
+    adj = [[] for _ in range(n)]
+    for e, (a, b) in enumerate(pr.tolist()):
+        adj[a].append((b, rl[e]))
+        adj[b].append((a, rl[e]))
+    island = [-1] * n
+    n_isl = 0
+    for s0 in range(n):
+        if not pinned[s0] or island[s0] != -1:
+            continue
+        ident = n_isl
+        n_isl += 1
+        stack = [s0]
+        island[s0] = ident
+        while stack:
+            u = stack.pop()
+            for t, _ in adj[u]:
+                if pinned[t] and island[t] == -1:
+                    island[t] = ident
+                    stack.append(t)
+    per = [[] for _ in range(n)]
+    inf = float("inf")
+    for ident in range(n_isl):
+        dist = [inf] * n
+        near = [-1] * n
+        heap = _RefHeap()
+        for i in range(n):
+            if pinned[i] and island[i] == ident:
+                dist[i] = 0.0
+                near[i] = i
+                heap.push((0.0, i))
+        while heap.d:
+            du, u = heap.pop()
+            if du > dist[u]:
+                continue
+            for t, w in adj[u]:
+                nd = du + w
+                if nd < dist[t]:
+                    dist[t] = nd
+                    near[t] = near[u]
+                    heap.push((nd, t))
+        for v in range(n):
+            if not pinned[v] and dist[v] != inf:
+                per[v].append((dist[v], ident, near[v]))
+    scale = 1.0 + float(stretch_tolerance)
+    part, anch, rad = [], [], []
+    for v in range(n):
+        if pinned[v] or not per[v]:
+            continue
+        lst = sorted(per[v], key=lambda a: (a[0], a[1]))
+        for dv, _, an in lst[:max_attachments]:
+            part.append(v)
+            anch.append(an)
+            rad.append(dv * scale)
+    return np.asarray(part, np.uint32), np.asarray(anch, np.uint32), np.asarray(rad, np.float32)
+
+
 # ----------------------------------------------------------- scene backend ----
 class OracleScene:
     """A recipe replayed on the CPU oracle; same methods as pfsim's Scene."""
@@ -193,6 +304,14 @@ class OracleScene:
     def set_primitive(self, slot, prim) -> None:
         p = prim.cstruct()
         check(lib().or_set_primitive(self.h, slot, C.byref(p)))
+
+    def set_cloth_params(self, material: int, params) -> None:
+        """params: a pfsim._native.ClothParams (ClothSystem setters)."""
+        check(lib().or_cloth_set_params(self.h, material, C.byref(params)))
+
+    def write(self, field_id: int, data: np.ndarray) -> None:
+        a = np.ascontiguousarray(data, np.float32)
+        check(lib().or_write(self.h, field_id, _p(a), a.nbytes))
 
     def readback(self, field_id: int, as_f64: bool = False) -> "np.ndarray":
         from pfsim import recipe as R

@@ -347,6 +347,19 @@ struct Cloth {
   std::vector<T> bendRest, bendLambda;
   T bendCompliance = 0;
   std::vector<std::vector<uint32_t>> bendGroups;
+  // tether.ts: (free particle, anchor) absolute indices, rest radii
+  std::vector<uint32_t> tether;
+  std::vector<T> tetherRest, tetherLambda;
+  T tetherCompliance = 0;
+  std::vector<std::vector<uint32_t>> tetherGroups;
+  // aero.ts: absolute triangles and the per-vertex incidence CSR
+  std::vector<uint32_t> tris, incOff, incTri;
+  float wind[3] = {0, 0, 0};
+  float drag = 0.6125f, lift = 0.3f;
+  // ClothSystem.buildDamping: edge-neighbour CSR (cloth-local)
+  bool hasDamping = false;
+  float damping = 0;
+  std::vector<uint32_t> dampOff, dampNbr;
 };
 
 struct Prim {
@@ -1423,6 +1436,81 @@ struct Engine {
         cl.bendLambda[c] = lc + dl;
       }
     }
+    // tether.ts:117-154, after the bending colours (ClothSystem.ts:213-224)
+    for (const auto& grp : cl.tetherGroups) {
+      for (uint32_t c : grp) {
+        const uint32_t i = cl.tether[2 * c], a = cl.tether[2 * c + 1];
+        const V3<T> x = p3(pred, i);
+        const T w = invMass[i];
+        if (w <= 0) continue;
+        const V3<T> d = x - p3(pred, a);
+        const T len = length(d);
+        if (len <= cl.tetherRest[c]) {
+          cl.tetherLambda[c] = 0;
+          continue;
+        }
+        if (len < static_cast<T>(1e-12)) continue;
+        const T lc = cl.tetherLambda[c];
+        const T at = cl.tetherCompliance / (dt * dt);
+        const T dl = (-(len - cl.tetherRest[c]) - at * lc) / (w + at);
+        set3(pred, i, x + (d / len) * (w * dl), 0);
+        cl.tetherLambda[c] = lc + dl;
+      }
+    }
+  }
+
+  // aero.ts:203-283: per cloth vertex, a third of the drag and lift of each
+  // incident triangle from committed positions and velocities; the sum moves
+  // the predicted position by dt^2 w F. Each vertex writes only its own slot.
+  void cloth_aero(Cloth<T>& cl) {
+    if (cl.tris.empty()) return;
+    const V3<T> wind = v3<T>(cl.wind[0], cl.wind[1], cl.wind[2]);
+    const T drag = cl.drag, lift = cl.lift, three = 3;
+    for (uint32_t v = 0; v < cl.n; ++v) {
+      const uint32_t i = cl.offset + v;
+      const T w = invMass[i];
+      if (w <= 0) continue;
+      V3<T> f = v3<T>(0, 0, 0);
+      for (uint32_t m = cl.incOff[v]; m < cl.incOff[v + 1]; ++m) {
+        const uint32_t* t = cl.tris.data() + 3 * static_cast<size_t>(cl.incTri[m]);
+        const V3<T> vrel = (p3(vel, t[0]) + p3(vel, t[1]) + p3(vel, t[2])) / three - wind;
+        const T vrs = dot(vrel, vrel);
+        if (!(vrs > static_cast<T>(1e-12))) continue;
+        const V3<T> x1 = p3(pos, t[0]);
+        const V3<T> nraw = cross(p3(pos, t[1]) - x1, p3(pos, t[2]) - x1);
+        const T nms = dot(nraw, nraw);
+        if (!(nms > static_cast<T>(1e-12))) continue;
+        const T nm = std::sqrt(nms);
+        const T area = nm * static_cast<T>(0.5);
+        const V3<T> nunit = nraw / nm;
+        const V3<T> nbar = nunit * (dot(nunit, vrel) < 0 ? static_cast<T>(-1) : static_cast<T>(1));
+        const V3<T> vhat = vrel / std::sqrt(vrs);
+        const V3<T> fdrag = neg(vhat * (drag * vrs * area * dot(nbar, vhat)));
+        const V3<T> flift = cross(cross(nbar, vhat), vhat) * (lift * vrs * area);
+        f = f + (fdrag + flift) / three;
+      }
+      set3(pred, i, p3(pred, i) + f * (dt * dt * w), 0);
+    }
+  }
+
+  // ClothSystem.ts:249-287: blend each velocity toward the mean of the
+  // particle's edge neighbours (mix(v, mean, damping)); pinned particles keep
+  // theirs.
+  void cloth_damping(Cloth<T>& cl) {
+    if (!cl.hasDamping) return;
+    const T t = cl.damping, one = 1;
+    std::vector<V3<T>> sm(cl.n);
+    for (uint32_t v = 0; v < cl.n; ++v) {
+      V3<T> sum = v3<T>(0, 0, 0);
+      const uint32_t m0 = cl.dampOff[v], m1 = cl.dampOff[v + 1];
+      for (uint32_t m = m0; m < m1; ++m) sum = sum + p3(vel, cl.offset + cl.dampNbr[m]);
+      const V3<T> mean = sum / static_cast<T>(std::max(m1 - m0, 1u));
+      sm[v] = p3(vel, cl.offset + v) * (one - t) + mean * t;
+    }
+    for (uint32_t v = 0; v < cl.n; ++v) {
+      const uint32_t i = cl.offset + v;
+      if (invMass[i] > 0) set3(vel, i, sm[v], vel[4 * i + 3]);
+    }
   }
 
   // --------------------------------------------------------- the loop ----
@@ -1482,6 +1570,9 @@ struct Engine {
         Cloth<T>& cl = cloths[m.second];
         std::fill(cl.lambda.begin(), cl.lambda.end(), static_cast<T>(0));
         std::fill(cl.bendLambda.begin(), cl.bendLambda.end(), static_cast<T>(0));
+        std::fill(cl.tetherLambda.begin(), cl.tetherLambda.end(), static_cast<T>(0));
+        // ClothSystem.ts:226-238: drag and lift after the multiplier resets
+        cloth_aero(cl);
       }
     }
     for (uint32_t it = 0; it < iterations; ++it) {
@@ -1525,6 +1616,8 @@ struct Engine {
           rotation_advect(sb);
           body_frame(sb);
         }
+      } else {
+        cloth_damping(cloths[m.second]);
       }
     }
     if (hasColliders) {
@@ -2001,9 +2094,77 @@ int or_add_cloth(void* h, const pf_cloth_desc* d, uint32_t* mat) {
       cl.bendCompliance = static_cast<T>(static_cast<float>(bc));
       cl.bendGroups = color_constraints(cl.bend, d->n_bending, 4);
     }
+    if (d->n_tethers) {
+      // tether.ts:100-110: one compliance, colours of arity 1 on the particle
+      cl.tether.resize(2 * static_cast<size_t>(d->n_tethers));
+      std::vector<uint32_t> who(d->n_tethers);
+      for (uint32_t c = 0; c < d->n_tethers; ++c) {
+        cl.tether[2 * c] = who[c] = d->offset + d->tether_particle[c];
+        cl.tether[2 * c + 1] = d->offset + d->tether_anchor[c];
+      }
+      cl.tetherRest.resize(d->n_tethers);
+      for (uint32_t c = 0; c < d->n_tethers; ++c) cl.tetherRest[c] = d->tether_rest[c];
+      cl.tetherLambda.assign(d->n_tethers, 0);
+      const double tc = d->tether_compliance >= 0 ? d->tether_compliance : 0.0;
+      cl.tetherCompliance = static_cast<T>(static_cast<float>(tc));
+      cl.tetherGroups = color_constraints(who, d->n_tethers, 1);
+    }
+    if (d->n_triangles) {
+      // aero.ts:160-183: incidence CSR in triangle order
+      cl.tris.resize(3 * static_cast<size_t>(d->n_triangles));
+      cl.incOff.assign(d->n_particles + 1, 0);
+      for (size_t q = 0; q < cl.tris.size(); ++q) {
+        cl.tris[q] = d->offset + d->triangles[q];
+        ++cl.incOff[d->triangles[q] + 1];
+      }
+      for (uint32_t v = 0; v < d->n_particles; ++v) cl.incOff[v + 1] += cl.incOff[v];
+      cl.incTri.resize(cl.incOff.back());
+      std::vector<uint32_t> cur(cl.incOff.begin(), cl.incOff.end() - 1);
+      for (uint32_t t = 0; t < d->n_triangles; ++t)
+        for (int k = 0; k < 3; ++k) cl.incTri[cur[d->triangles[3 * t + k]]++] = t;
+    }
+    for (int a = 0; a < 3; ++a) cl.wind[a] = d->wind[a];
+    cl.drag = d->drag >= 0 ? d->drag : 0.6125f;
+    cl.lift = d->lift >= 0 ? d->lift : 0.3f;
+    if (d->has_damping) {
+      // ClothSystem.ts:252-263: neighbours in pair order, both directions
+      cl.hasDamping = true;
+      cl.damping = d->damping;
+      cl.dampOff.assign(d->n_particles + 1, 0);
+      for (uint32_t q = 0; q < 2 * d->n_pairs; ++q) ++cl.dampOff[d->pairs[q] + 1];
+      for (uint32_t v = 0; v < d->n_particles; ++v) cl.dampOff[v + 1] += cl.dampOff[v];
+      cl.dampNbr.resize(cl.dampOff.back());
+      std::vector<uint32_t> cur(cl.dampOff.begin(), cl.dampOff.end() - 1);
+      for (uint32_t q = 0; q < d->n_pairs; ++q) {
+        const uint32_t i = d->pairs[2 * q], j = d->pairs[2 * q + 1];
+        cl.dampNbr[cur[i]++] = j;
+        cl.dampNbr[cur[j]++] = i;
+      }
+    }
     e.cloths.push_back(std::move(cl));
     e.materials.push_back({MAT_CLOTH, static_cast<int>(e.cloths.size() - 1)});
     if (mat) *mat = static_cast<uint32_t>(e.materials.size() - 1);
+  });
+  return rc;
+}
+
+// ClothSystem.wind / drag / lift / damping / bendCompliance setters
+// (ClothSystem.ts:143-188).
+int or_cloth_set_params(void* h, uint32_t mat, const pf_cloth_params* p) {
+  Scene* s = static_cast<Scene*>(h);
+  int rc = PF_OK;
+  s->visit([&](auto& e) {
+    using T = typename std::remove_reference<decltype(e.pos[0])>::type;
+    if (mat >= e.materials.size() || e.materials[mat].first != MAT_CLOTH) {
+      rc = fail(PF_ERR_INVALID, "ClothSystem: material is not a cloth");
+      return;
+    }
+    auto& cl = e.cloths[e.materials[mat].second];
+    for (int a = 0; a < 3; ++a) cl.wind[a] = p->wind[a];
+    cl.drag = p->drag;
+    cl.lift = p->lift;
+    cl.damping = p->damping;
+    cl.bendCompliance = static_cast<T>(p->bend_compliance);
   });
   return rc;
 }
@@ -2146,6 +2307,35 @@ int or_step(void* h, double dt) {
 
 // Field readback (pf_field numbering); float fields are converted to float32,
 // or written as float64 when as_f64 is set.
+// Whole-field write in particle order (positions, predicted, velocities with
+// w set to 0 as the reference's buffers hold it; inverse mass).
+int or_write(void* h, uint32_t field, const float* src, size_t bytes) {
+  Scene* s = static_cast<Scene*>(h);
+  int rc = PF_OK;
+  s->visit([&](auto& e) {
+    using T = typename std::remove_reference<decltype(e.pos[0])>::type;
+    const size_t cap = e.cap;
+    auto put4 = [&](auto& dst) {
+      if (bytes < 16 * cap) { rc = fail(PF_ERR_INVALID, "write: source too small"); return; }
+      for (size_t i = 0; i < cap; ++i) {
+        for (int c = 0; c < 3; ++c) dst[4 * i + c] = static_cast<T>(src[4 * i + c]);
+        dst[4 * i + 3] = 0;
+      }
+    };
+    switch (field) {
+      case PF_FIELD_POSITIONS: put4(e.pos); break;
+      case PF_FIELD_PREDICTED: put4(e.pred); break;
+      case PF_FIELD_VELOCITIES: put4(e.vel); break;
+      case PF_FIELD_INV_MASS:
+        if (bytes < 4 * cap) { rc = fail(PF_ERR_INVALID, "write: source too small"); return; }
+        for (size_t i = 0; i < cap; ++i) e.invMass[i] = static_cast<T>(src[i]);
+        break;
+      default: rc = fail(PF_ERR_INVALID, "write: field cannot be written");
+    }
+  });
+  return rc;
+}
+
 int or_readback(void* h, uint32_t field, void* dst, size_t bytes, int as_f64) {
   Scene* s = static_cast<Scene*>(h);
   int rc = PF_OK;

@@ -261,3 +261,89 @@ def signed_dihedral(pos: np.ndarray) -> float:
     from pfsim import shapes
 
     return float(shapes.dihedral_angles(np.asarray(pos, np.float64)[:, :3], np.array([[0, 1, 2, 3]]))[0])
+
+
+def grid_sheet(m: int, x0: float = 0.0):
+    """The m x m sheets of tests/analytical/cloth/tether-stretch.gpu.test.ts:
+    39-70, tether-unilateral.gpu.test.ts:40-66 (x0 = 0) and
+    wind-deflection.gpu.test.ts:55-83 (x0 = -0.5): vertex (i, j) at
+    (x0 + i/(m-1), -j/(m-1), 0) as float32, triangles (a, c, d), (a, d, b)
+    per quad, the top row pinned. Returns (positions, index, pinned)."""
+    j, i = np.meshgrid(np.arange(m), np.arange(m), indexing="ij")
+    pos = np.stack([x0 + i / (m - 1), -(j / (m - 1)), np.zeros((m, m))], -1).reshape(-1, 3)
+    pos = pos.astype(np.float32).astype(np.float64)
+    idx = []
+    for jj in range(m - 1):
+        for ii in range(m - 1):
+            a, b = jj * m + ii, jj * m + ii + 1
+            c, d = (jj + 1) * m + ii, (jj + 1) * m + ii + 1
+            idx += [a, c, d, a, d, b]
+    return pos, np.array(idx, np.int64), list(range(m))
+
+
+def cloth_system(graph, substeps: int, iterations: int, gravity=(0.0, -G, 0.0), stretch: float = 1e-7,
+                 bend: float = 1e-5, tether_compliance: float = 0.0, wind=(0.0, 0.0, 0.0), drag: float = 0.6125,
+                 lift: float = 0.3, radius: float = 0.05, positions=None, name: str = "cloth"):
+    """new ClothSystem(particles, {graph, stretchCompliance, bendCompliance,
+    tetherCompliance, wind, drag, lift}) in a SimLoop of its own
+    (ClothSystem.ts:102-141, 190-245): stretch, bending and tether colours,
+    drag and lift on the graph's triangles. `positions` replaces the
+    uploaded positions after the cloth wrote its own (as the tests'
+    uploadParticles calls do). Returns (recipe, tethers)."""
+    from pfsim import shapes
+
+    tp, ta, tr = shapes.build_tethers(graph.inv_mass, graph.pairs, graph.rest_lengths)
+    n = graph.positions.shape[0]
+    cloth = R.ClothOpts(offset=0, positions=graph.positions.astype(np.float32),
+                        inv_mass=np.asarray(graph.inv_mass, np.float32), pairs=graph.pairs,
+                        rest_lengths=np.asarray(graph.rest_lengths, np.float32), stretch_compliance=stretch,
+                        bending=graph.bending, bending_rest=graph.bending_rest.astype(np.float32),
+                        bend_compliance=bend, tether_particle=tp, tether_anchor=ta, tether_rest=tr,
+                        tether_compliance=tether_compliance, triangles=graph.triangles, wind=tuple(wind),
+                        drag=drag, lift=lift)
+    r = R.Recipe(capacity=n, radius=radius, materials=[("cloth", cloth)],
+                 loop=R.LoopOpts(substeps=substeps, iterations=iterations, gravity=tuple(gravity)), name=name)
+    if positions is not None:
+        cloth.positions = np.asarray(positions, np.float32)
+    return r, (tp, ta, tr)
+
+
+def run_damped(scene, frames: int, damp: float) -> None:
+    """The tests' frame loop: step, then scale every velocity by `damp`
+    (read the buffer, multiply, write it back)."""
+    from pfsim import _native as N
+
+    for _ in range(frames):
+        scene.step(DT)
+        scene.write(N.PF_FIELD_VELOCITIES, scene.readback(N.PF_FIELD_VELOCITIES) * np.float32(damp))
+
+
+def wind_deflection_analytic(surface_density: float, g: float, v: float, drag: float, lift: float) -> float:
+    """wind-deflection.gpu.test.ts:85-121: Newton iteration on
+    rho_s g sin(t) = v^2 (drag cos^2(t) - lift sin^2(t))."""
+    rsg, vsq = surface_density * g, v * v
+    f = lambda t: rsg * math.sin(t) - vsq * (drag * math.cos(t) ** 2 - lift * math.sin(t) ** 2)
+    df = lambda t: rsg * math.cos(t) + vsq * (2 * drag * math.cos(t) * math.sin(t)
+                                              + 2 * lift * math.sin(t) * math.cos(t))
+    t = math.atan(vsq * drag / max(rsg, 1e-9))
+    for _ in range(12):
+        d = df(t)
+        if abs(d) < 1e-12:
+            break
+        nt = t - f(t) / d
+        if abs(nt - t) < 1e-9:
+            t = nt
+            break
+        t = nt
+    return t
+
+
+def wind_deflection_angle(pos4: np.ndarray, inv_mass: np.ndarray, top: list) -> tuple:
+    """wind-deflection.gpu.test.ts:177-212: the pivot (mean of the top row)
+    to the free particles' centre of mass, as (angle from vertical, dy, dz)."""
+    py = float(np.mean(pos4[top, 1]))
+    pz = float(np.mean(pos4[top, 2]))
+    free = inv_mass != 0
+    dy = float(np.mean(pos4[free, 1])) - py
+    dz = float(np.mean(pos4[free, 2])) - pz
+    return math.atan2(dz, abs(dy)), dy, dz

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -445,9 +446,258 @@ pf_status pf_add_cloth(pf_scene* s, const pf_cloth_desc* d, uint32_t* mat) {
     cl.bend_compliance = (float)bc;
     cl.bend_colors = color_groups(cl.bend, 4, d->n_bending, sp.cap);
   }
+  // tether.ts:64-110: (free particle, anchor, rest radius) per tether, one
+  // compliance (ClothSystem default 0), coloured with arity 1 on the particle
+  if (d->n_tethers) {
+    if (!d->tether_particle || !d->tether_anchor || !d->tether_rest)
+      return fail(PF_ERR_INVALID, "createClothTetherConstraints: tether arrays missing");
+    const double tc = d->tether_compliance >= 0 ? d->tether_compliance : 0.0;
+    if (!std::isfinite(tc))
+      return fail(PF_ERR_INVALID, "createClothTetherConstraints: compliance must be a non-negative finite number");
+    cl.tether.resize(2ull * d->n_tethers);
+    std::vector<uint32_t> who(d->n_tethers);
+    for (uint32_t q = 0; q < d->n_tethers; ++q) {
+      const uint32_t p = d->tether_particle[q], a = d->tether_anchor[q];
+      if (p >= d->n_particles)
+        return fail(PF_ERR_INVALID, "createClothTetherConstraints: tether particle " + std::to_string(p) + " out of range");
+      if (a >= d->n_particles)
+        return fail(PF_ERR_INVALID, "createClothTetherConstraints: tether anchor " + std::to_string(a) + " out of range");
+      if (!(d->tether_rest[q] >= 0) || !std::isfinite(d->tether_rest[q]))
+        return fail(PF_ERR_INVALID, "createClothTetherConstraints: tether for particle " + std::to_string(p) +
+                                        " has invalid restRadius");
+      cl.tether[2 * q] = d->offset + p;
+      cl.tether[2 * q + 1] = d->offset + a;
+      who[q] = d->offset + p;
+    }
+    cl.tether_rest.assign(d->tether_rest, d->tether_rest + d->n_tethers);
+    cl.tether_compliance = (float)tc;
+    cl.tether_colors = color_groups(who, 1, d->n_tethers, sp.cap);
+  }
+  // aero.ts:118-158: cloth-local triangles; drag 0.6125, lift 0.3 by default
+  if (d->n_triangles) {
+    if (!d->triangles) return fail(PF_ERR_INVALID, "createClothAeroKernel: triangles missing");
+    cl.tris.resize(3ull * d->n_triangles);
+    for (size_t q = 0; q < cl.tris.size(); ++q) {
+      if (d->triangles[q] >= d->n_particles)
+        return fail(PF_ERR_INVALID, "createClothAeroKernel: triangle " + std::to_string(q / 3) +
+                                        " has out-of-range vertex " + std::to_string(d->triangles[q]));
+      cl.tris[q] = d->offset + d->triangles[q];
+    }
+  }
+  cl.drag = d->drag >= 0 ? d->drag : 0.6125f;
+  cl.lift = d->lift >= 0 ? d->lift : 0.3f;
+  if (!std::isfinite(cl.drag)) return fail(PF_ERR_INVALID, "ClothSystem: drag must be >= 0");
+  if (!std::isfinite(cl.lift)) return fail(PF_ERR_INVALID, "ClothSystem: lift must be >= 0");
+  for (int a = 0; a < 3; ++a) {
+    if (!std::isfinite(d->wind[a])) return fail(PF_ERR_INVALID, "ClothSystem: wind must be finite");
+    cl.wind[a] = d->wind[a];
+  }
+  cl.has_damping = d->has_damping != 0;
+  if (cl.has_damping) {
+    if (!(d->damping >= 0 && d->damping <= 1))
+      return fail(PF_ERR_INVALID, "ClothSystem: damping must be between 0 and 1, got " + std::to_string(d->damping));
+    cl.damping = d->damping;
+  }
   sp.cloths.push_back(std::move(cl));
   sp.materials.push_back({MAT_CLOTH, (uint32_t)sp.cloths.size() - 1});
   if (mat) *mat = (uint32_t)sp.materials.size() - 1;
+  return PF_OK;
+}
+
+static const ClothSpec* cloth_of(const SceneSpec& sp, uint32_t mat) {
+  if (mat >= sp.materials.size() || sp.materials[mat].first != MAT_CLOTH) return nullptr;
+  return &sp.cloths[sp.materials[mat].second];
+}
+
+// ClothSystem.ts:152-188: the setters' checks.
+static pf_status check_cloth_params(const ClothSpec& cl, const pf_cloth_params& p) {
+  auto nonneg = [](float v, const char* name) -> pf_status {
+    if (!(v >= 0) || !std::isfinite(v))
+      return fail(PF_ERR_INVALID, std::string("ClothSystem: ") + name + " must be >= 0, got " + std::to_string(v));
+    return PF_OK;
+  };
+  PF_TRY(nonneg(p.drag, "drag"));
+  PF_TRY(nonneg(p.lift, "lift"));
+  PF_TRY(nonneg(p.bend_compliance, "bendCompliance"));
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(p.wind[a])) return fail(PF_ERR_INVALID, "ClothSystem: wind must be finite");
+  if (!(p.damping >= 0 && p.damping <= 1))
+    return fail(PF_ERR_INVALID, "ClothSystem: damping must be between 0 and 1, got " + std::to_string(p.damping));
+  if (p.damping != cl.damping && !cl.has_damping)
+    return fail(PF_ERR_INVALID, "ClothSystem: damping was not given at creation, so there is no smoothing pass to change");
+  return PF_OK;
+}
+
+pf_status pf_cloth_get_params(pf_scene* s, uint32_t mat, pf_cloth_params* out) {
+  if (!s || !out) return fail(PF_ERR_INVALID, "ClothSystem: NULL argument");
+  const ClothSpec* cl = cloth_of(s->spec, mat);
+  if (!cl) return fail(PF_ERR_INVALID, "ClothSystem: material " + std::to_string(mat) + " is not a cloth");
+  for (int a = 0; a < 3; ++a) out->wind[a] = cl->wind[a];
+  out->drag = cl->drag;
+  out->lift = cl->lift;
+  out->damping = cl->damping;
+  out->bend_compliance = cl->bend_compliance;
+  return PF_OK;
+}
+
+pf_status pf_cloth_set_params(pf_scene* s, uint32_t mat, const pf_cloth_params* p) {
+  if (!s || !p) return fail(PF_ERR_INVALID, "ClothSystem: NULL argument");
+  const ClothSpec* cl = cloth_of(s->spec, mat);
+  if (!cl) return fail(PF_ERR_INVALID, "ClothSystem: material " + std::to_string(mat) + " is not a cloth");
+  PF_TRY(check_cloth_params(*cl, *p));
+  if (s->world) return s->world->set_cloth_params(0, mat, *p);
+  ClothSpec& w = s->spec.cloths[s->spec.materials[mat].second];
+  for (int a = 0; a < 3; ++a) w.wind[a] = p->wind[a];
+  w.drag = p->drag;
+  w.lift = p->lift;
+  w.damping = p->damping;
+  w.bend_compliance = p->bend_compliance;
+  return PF_OK;
+}
+
+// tetherBuild.ts:226-275: a binary min-heap on the distance alone, with the
+// reference's sift rules (strict comparisons), so that equal distances leave
+// the heap in the same order and Dijkstra keeps the same nearest anchor.
+namespace {
+struct DistHeap {
+  std::vector<std::pair<double, uint32_t>> d;
+  void push(double dist, uint32_t u) {
+    d.push_back({dist, u});
+    size_t i = d.size() - 1;
+    while (i > 0) {
+      const size_t p = (i - 1) >> 1;
+      if (d[i].first < d[p].first) {
+        std::swap(d[i], d[p]);
+        i = p;
+      } else {
+        break;
+      }
+    }
+  }
+  std::pair<double, uint32_t> pop() {
+    const auto top = d[0];
+    const auto last = d.back();
+    d.pop_back();
+    if (!d.empty()) {
+      d[0] = last;
+      size_t i = 0;
+      const size_t n = d.size();
+      for (;;) {
+        const size_t l = 2 * i + 1, r = 2 * i + 2;
+        size_t m = i;
+        if (l < n && d[l].first < d[m].first) m = l;
+        if (r < n && d[r].first < d[m].first) m = r;
+        if (m == i) break;
+        std::swap(d[i], d[m]);
+        i = m;
+      }
+    }
+    return top;
+  }
+};
+}  // namespace
+
+pf_status pf_cloth_build_tethers(const pf_tether_build_desc* desc, uint32_t* particle, uint32_t* anchor,
+                                 float* rest, uint32_t capacity, uint32_t* count) {
+  if (!desc || !count) return fail(PF_ERR_INVALID, "buildTethers: NULL argument");
+  *count = 0;
+  const uint32_t n = desc->n_particles;
+  const uint32_t max_att = desc->max_attachments ? desc->max_attachments : 4u;
+  if (!(desc->stretch_tolerance >= 0) || !std::isfinite(desc->stretch_tolerance))
+    return fail(PF_ERR_INVALID, "buildTethers: stretchTolerance must be a non-negative finite number, got " +
+                                    std::to_string(desc->stretch_tolerance));
+  if (n && !desc->inv_mass) return fail(PF_ERR_INVALID, "buildTethers: invMass missing");
+  if (desc->n_pairs && (!desc->pairs || !desc->rest_lengths)) return fail(PF_ERR_INVALID, "buildTethers: pairs missing");
+  for (uint64_t q = 0; q < 2ull * desc->n_pairs; ++q)
+    if (desc->pairs[q] >= n) return fail(PF_ERR_INVALID, "buildTethers: pair has out-of-range index");
+  std::vector<uint8_t> pinned(n);
+  uint32_t n_pinned = 0;
+  for (uint32_t i = 0; i < n; ++i) n_pinned += (pinned[i] = desc->inv_mass[i] == 0.0f);
+  if (n_pinned == 0) return PF_OK;
+  // adjacency in pair order, both directions (tetherBuild.ts:129-136)
+  std::vector<uint32_t> off(n + 1, 0);
+  for (uint64_t q = 0; q < 2ull * desc->n_pairs; ++q) ++off[desc->pairs[q] + 1];
+  for (uint32_t v = 0; v < n; ++v) off[v + 1] += off[v];
+  std::vector<uint32_t> to(off.back()), cur(off.begin(), off.end() - 1);
+  std::vector<double> wt(off.back());
+  for (uint32_t e = 0; e < desc->n_pairs; ++e) {
+    const uint32_t a = desc->pairs[2 * e], b = desc->pairs[2 * e + 1];
+    to[cur[a]] = b;
+    wt[cur[a]++] = desc->rest_lengths[e];
+    to[cur[b]] = a;
+    wt[cur[b]++] = desc->rest_lengths[e];
+  }
+  // islands: connected pinned particles over pinned-only edges (:141-157)
+  std::vector<int32_t> island(n, -1);
+  int32_t n_islands = 0;
+  for (uint32_t s0 = 0; s0 < n; ++s0) {
+    if (!pinned[s0] || island[s0] != -1) continue;
+    const int32_t id = n_islands++;
+    std::vector<uint32_t> stack{s0};
+    island[s0] = id;
+    while (!stack.empty()) {
+      const uint32_t u = stack.back();
+      stack.pop_back();
+      for (uint32_t m = off[u]; m < off[u + 1]; ++m)
+        if (pinned[to[m]] && island[to[m]] == -1) {
+          island[to[m]] = id;
+          stack.push_back(to[m]);
+        }
+    }
+  }
+  // one multi-source Dijkstra per island (:172-207)
+  struct Att {
+    int32_t island;
+    double dist;
+    uint32_t anchor;
+  };
+  std::vector<std::vector<Att>> atts(n);
+  std::vector<double> dist(n);
+  std::vector<int64_t> nearest(n);
+  for (int32_t id = 0; id < n_islands; ++id) {
+    std::fill(dist.begin(), dist.end(), std::numeric_limits<double>::infinity());
+    std::fill(nearest.begin(), nearest.end(), -1);
+    DistHeap heap;
+    for (uint32_t i = 0; i < n; ++i)
+      if (pinned[i] && island[i] == id) {
+        dist[i] = 0;
+        nearest[i] = i;
+        heap.push(0.0, i);
+      }
+    while (!heap.d.empty()) {
+      const auto [du, u] = heap.pop();
+      if (du > dist[u]) continue;
+      for (uint32_t m = off[u]; m < off[u + 1]; ++m) {
+        const double nd = du + wt[m];
+        if (nd < dist[to[m]]) {
+          dist[to[m]] = nd;
+          nearest[to[m]] = nearest[u];
+          heap.push(nd, to[m]);
+        }
+      }
+    }
+    for (uint32_t v = 0; v < n; ++v)
+      if (!pinned[v] && std::isfinite(dist[v])) atts[v].push_back({id, dist[v], (uint32_t)nearest[v]});
+  }
+  // the closest max_attachments islands of each free particle (:211-219)
+  const double scale = 1.0 + desc->stretch_tolerance;
+  uint32_t k = 0;
+  for (uint32_t v = 0; v < n; ++v) {
+    if (pinned[v]) continue;
+    auto& list = atts[v];
+    std::stable_sort(list.begin(), list.end(), [](const Att& a, const Att& b) {
+      return a.dist < b.dist || (a.dist == b.dist && a.island < b.island);
+    });
+    const size_t take = std::min<size_t>(max_att, list.size());
+    for (size_t q = 0; q < take; ++q) {
+      if (k >= capacity) return fail(PF_ERR_INVALID, "buildTethers: output capacity " + std::to_string(capacity) + " too small");
+      if (particle) particle[k] = v;
+      if (anchor) anchor[k] = list[q].anchor;
+      if (rest) rest[k] = (float)(list[q].dist * scale);
+      ++k;
+    }
+  }
+  *count = k;
   return PF_OK;
 }
 
@@ -539,6 +789,36 @@ pf_status pf_step(pf_scene* s, double dt) {
   return s->world->step(dt);
 }
 
+pf_status pf_write(pf_scene* s, uint32_t field, const void* src, size_t bytes) {
+  if (!s || !src) return fail(PF_ERR_INVALID, "write: NULL argument");
+  if (s->world) return s->world->write(0, field, src, bytes);
+  SceneSpec& sp = s->spec;
+  const float* f = static_cast<const float*>(src);
+  const size_t n4 = 16ull * sp.cap, n1 = 4ull * sp.cap;
+  switch (field) {
+    case PF_FIELD_POSITIONS:
+    case PF_FIELD_VELOCITIES: {
+      if (bytes < n4) return fail(PF_ERR_INVALID, "write: source too small");
+      std::vector<float>& dst = field == PF_FIELD_POSITIONS ? sp.pos4 : sp.vel4;
+      for (size_t i = 0; i < 4ull * sp.cap; ++i)
+        if (!std::isfinite(f[i])) return fail(PF_ERR_INVALID, "write: values must be finite");
+      for (size_t i = 0; i < sp.cap; ++i)
+        for (int c = 0; c < 3; ++c) dst[4 * i + c] = f[4 * i + c];
+      return PF_OK;
+    }
+    case PF_FIELD_INV_MASS:
+      if (bytes < n1) return fail(PF_ERR_INVALID, "write: source too small");
+      for (size_t i = 0; i < sp.cap; ++i)
+        if (!(f[i] >= 0) || !std::isfinite(f[i])) return fail(PF_ERR_INVALID, "write: invMass must be a finite number >= 0");
+      std::copy(f, f + sp.cap, sp.inv_mass.begin());
+      return PF_OK;
+    case PF_FIELD_PREDICTED:
+      return fail(PF_ERR_STATE, "write: predicted positions exist once the SimLoop is built");
+    default:
+      return fail(PF_ERR_INVALID, "write: field " + std::to_string(field) + " cannot be written");
+  }
+}
+
 pf_status pf_readback(pf_scene* s, uint32_t field, void* dst, size_t bytes) {
   if (!s || !dst) return fail(PF_ERR_INVALID, "readback: NULL argument");
   if (s->world) return s->world->readback(0, field, dst, bytes);
@@ -610,6 +890,20 @@ pf_status pf_batch_step(pf_batch* b, double dt) {
 pf_status pf_batch_set_primitive(pf_batch* b, uint32_t index, uint32_t slot, const pf_primitive* p) {
   if (!b || !p) return fail(PF_ERR_INVALID, "batch: NULL");
   return b->world->set_primitive(index, slot, *p);
+}
+
+pf_status pf_batch_cloth_set_params(pf_batch* b, uint32_t index, uint32_t mat, const pf_cloth_params* p) {
+  if (!b || !p) return fail(PF_ERR_INVALID, "batch: NULL");
+  if (index >= b->specs.size()) return fail(PF_ERR_INVALID, "batch: no scene " + std::to_string(index));
+  const ClothSpec* cl = cloth_of(*b->specs[index], mat);
+  if (!cl) return fail(PF_ERR_INVALID, "ClothSystem: material " + std::to_string(mat) + " is not a cloth");
+  PF_TRY(check_cloth_params(*cl, *p));
+  return b->world->set_cloth_params(index, mat, *p);
+}
+
+pf_status pf_batch_write(pf_batch* b, uint32_t index, uint32_t field, const void* src, size_t bytes) {
+  if (!b || !src) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->write(index, field, src, bytes);
 }
 
 pf_status pf_batch_readback(pf_batch* b, uint32_t index, uint32_t field, void* dst, size_t bytes) {

@@ -478,13 +478,112 @@ __global__ void __launch_bounds__(kBlock) k_bend(WorldView V, uint32_t begin, ui
   const float sg = dot(g1, g1) * w1 + dot(g2, g2) * w2 + dot(g3, g3) * w3 + dot(g4, g4) * w4;
   if (sg <= 1e-30f) return;
   const float lc = V.b_lambda[q];
-  const float at = V.b_comp[q] / (S.dt * S.dt);
+  const float at = V.cloth_par[V.b_cloth[q]].bend_compliance / (S.dt * S.dt);
   const float dl = (-C - at * lc) / (sg + at);
   V.cur.xs[i1] = with_w(x1 + g1 * (w1 * dl), w1);
   V.cur.xs[i2] = with_w(x2 + g2 * (w2 * dl), w2);
   V.cur.xs[i3] = with_w(x3 + g3 * (w3 * dl), w3);
   V.cur.xs[i4] = with_w(x4 + g4 * (w4 * dl), w4);
   V.b_lambda[q] = lc + dl;
+}
+
+// tether.ts:117-154: one colour of long-range attachments (no two share a
+// free particle). Unilateral: slack inside the rest radius (lambda reset),
+// otherwise the XPBD projection of the free particle onto the sphere about
+// its pinned anchor, read at its predicted position.
+__global__ void __launch_bounds__(kBlock) k_tether(WorldView V, uint32_t begin, uint32_t end, uint32_t sub,
+                                                   uint32_t it) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const DevScene& S = V.scenes[V.t_scene[q]];
+  if (sub >= S.substeps || it >= S.iterations) return;
+  const uint4 r = V.t_rec[q];
+  const uint32_t i = V.inv[r.x];
+  const float4 xi = V.cur.xs[i];
+  const float w = xi.w;
+  if (w <= 0.0f) return;
+  const f3 d = xyz(xi) - xyz(V.cur.xs[V.inv[r.y]]);
+  const float l = len(d);
+  const float rest = __uint_as_float(r.z);
+  if (l <= rest) {
+    V.t_lambda[q] = 0.0f;
+    return;
+  }
+  if (l < 1e-12f) return;
+  const float lc = V.t_lambda[q];
+  const float at = __uint_as_float(r.w) / (S.dt * S.dt);
+  const float dl = (-(l - rest) - at * lc) / (w + at);
+  V.cur.xs[i] = with_w(xyz(xi) + (d / l) * (w * dl), w);
+  V.t_lambda[q] = lc + dl;
+}
+
+// aero.ts:203-283: drag and lift of each incident triangle (Keckeisen et al.
+// 2004), a third of each triangle's force per vertex, gathered per cloth
+// particle (no scatter) from the committed positions and the velocities after
+// the prediction; the sum moves the predicted position by dt^2 w F.
+__global__ void __launch_bounds__(kBlock) k_aero(WorldView V, uint32_t begin, uint32_t end, uint32_t sub) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const uint2 rec = V.a_vtx[q];
+  const uint32_t k = V.inv[rec.x];
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 xs = V.cur.xs[k];
+  const float w = xs.w;
+  if (w <= 0.0f) return;
+  const DevCloth& P = V.cloth_par[rec.y];
+  const f3 wind = mk(P.wind[0], P.wind[1], P.wind[2]);
+  const float drag = P.drag, lift = P.lift;
+  f3 fsum = mk(0.0f, 0.0f, 0.0f);
+  const uint32_t m1 = V.a_off[q + 1];
+  for (uint32_t m = V.a_off[q]; m < m1; ++m) {
+    const uint4 t = V.a_tri[m];
+    const uint32_t s1 = V.inv[t.x], s2 = V.inv[t.y], s3 = V.inv[t.z];
+    const f3 vrel = (xyz(V.cur.v[s1]) + xyz(V.cur.v[s2]) + xyz(V.cur.v[s3])) / 3.0f - wind;
+    const float vrs = dot(vrel, vrel);
+    if (!(vrs > 1e-12f)) continue;
+    const f3 x1 = xyz(V.cur.x[s1]);
+    const f3 nraw = cross(xyz(V.cur.x[s2]) - x1, xyz(V.cur.x[s3]) - x1);
+    const float nms = dot(nraw, nraw);
+    if (!(nms > 1e-12f)) continue;
+    const float nm = sqrtf(nms);
+    const float area = nm * 0.5f;
+    const f3 nunit = nraw / nm;
+    const f3 nbar = nunit * (dot(nunit, vrel) < 0.0f ? -1.0f : 1.0f);
+    const f3 vhat = vrel / sqrtf(vrs);
+    const f3 fdrag = neg(vhat * (drag * vrs * area * dot(nbar, vhat)));
+    const f3 flift = cross(cross(nbar, vhat), vhat) * (lift * vrs * area);
+    fsum = fsum + (fdrag + flift) / 3.0f;
+  }
+  V.cur.xs[k] = with_w(xyz(xs) + fsum * (S.dt * S.dt * w), w);
+}
+
+// ClothSystem.ts:264-277: the mean velocity of each cloth particle's edge
+// neighbours, blended with its own (mix(v, mean, damping)).
+__global__ void __launch_bounds__(kBlock) k_damp_mean(WorldView V, uint32_t begin, uint32_t end, uint32_t sub) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const uint2 rec = V.d_vtx[q];
+  const uint32_t k = V.inv[rec.x];
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  const float4 v = V.cur.v[k];
+  const uint32_t m0 = V.d_off[q], m1 = V.d_off[q + 1];
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  for (uint32_t m = m0; m < m1; ++m) sum = sum + xyz(V.cur.v[V.inv[V.d_nbr[m]]]);
+  const f3 mean = sum / (float)max(m1 - m0, 1u);
+  const float t = V.cloth_par[rec.y].damping;
+  V.d_smooth[q] = with_w(xyz(v) * (1.0f - t) + mean * t, v.w);
+}
+
+// ClothSystem.ts:278-284: particles with inverse mass > 0 take the blend.
+__global__ void __launch_bounds__(kBlock) k_damp_apply(WorldView V, uint32_t begin, uint32_t end, uint32_t sub) {
+  const uint32_t q = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= end) return;
+  const uint32_t k = V.inv[V.d_vtx[q].x];
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || !(V.cur.x[k].w > 0.0f)) return;
+  V.cur.v[k] = V.d_smooth[q];
 }
 
 // ---------------------------------------------------------- soft bodies ----
@@ -893,6 +992,7 @@ World::~World() {
   if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
   if (h_pinned_prims_) cudaFreeHost(h_pinned_prims_);
   if (h_pinned_sdfs_) cudaFreeHost(h_pinned_sdfs_);
+  if (h_pinned_cloth_) cudaFreeHost(h_pinned_cloth_);
 }
 
 WorldView World::view(uint32_t parity) const {
@@ -921,6 +1021,12 @@ struct Carver {
 };
 
 float f32(double v) { return static_cast<float>(v); }
+
+uint32_t bits_of(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
 }  // namespace
 
 // Kernel-side view of an SDF collider: R from the unit quaternion (the
@@ -1195,6 +1301,26 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   n_ = (uint32_t)slot;
   cells_ = (uint32_t)cell;
+  // ---- cloth parameters, one record per cloth material -------------------
+  h_cloth_par_.clear();
+  cloth_par_of_.assign(K, {});
+  for (uint32_t s = 0; s < K; ++s) {
+    const SceneSpec& sp = *specs[s];
+    cloth_par_of_[s].assign(sp.materials.size(), -1);
+    for (uint32_t r = 0; r < sp.materials.size(); ++r) {
+      if (sp.materials[r].first != MAT_CLOTH) continue;
+      const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+      DevCloth P{};
+      for (int a = 0; a < 3; ++a) P.wind[a] = cl.wind[a];
+      P.drag = cl.drag;
+      P.lift = cl.lift;
+      P.damping = cl.damping;
+      P.bend_compliance = cl.bend_compliance;
+      cloth_par_of_[s][r] = (int32_t)h_cloth_par_.size();
+      h_cloth_par_.push_back(P);
+    }
+  }
+  cloth_par_dirty_ = false;
   // ---- cloth constraints by (rank, colour) ----------------------------
   std::vector<uint32_t> ci, cj, csc;
   std::vector<float> crest, ccomp;
@@ -1227,8 +1353,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   // ---- cloth bending constraints by (rank, colour) ---------------------
   std::vector<uint4> bidx;
-  std::vector<float> brest, bcomp;
-  std::vector<uint32_t> bsc;
+  std::vector<float> brest;
+  std::vector<uint32_t> bsc, bcl;
   bend_ranges_.assign(max_rank_, {});
   for (uint32_t r = 0; r < max_rank_; ++r) {
     uint32_t ncol = 0;
@@ -1249,12 +1375,112 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
           const uint32_t* t = cl.bend.data() + 4ull * q;
           bidx.push_back(make_uint4(base + t[0], base + t[1], base + t[2], base + t[3]));
           brest.push_back(cl.bend_rest[q]);
-          bcomp.push_back(cl.bend_compliance);
+          bcl.push_back((uint32_t)cloth_par_of_[s][r]);
           bsc.push_back(s);
         }
       }
       bend_ranges_[r].push_back({begin, (uint32_t)bidx.size()});
     }
+  }
+  // ---- cloth tethers by (rank, colour) -----------------------------------
+  std::vector<uint4> trec;
+  std::vector<uint32_t> tsc;
+  teth_ranges_.assign(max_rank_, {});
+  for (uint32_t r = 0; r < max_rank_; ++r) {
+    uint32_t ncol = 0;
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      if (r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)
+        ncol = std::max(ncol, (uint32_t)sp.cloths[sp.materials[r].second].tether_colors.size());
+    }
+    for (uint32_t c = 0; c < ncol; ++c) {
+      const uint32_t begin = (uint32_t)trec.size();
+      for (uint32_t s = 0; s < K; ++s) {
+        const SceneSpec& sp = *specs[s];
+        if (!(r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)) continue;
+        const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+        if (c >= cl.tether_colors.size()) continue;
+        const uint32_t base = h_scenes_[s].seg_start;
+        for (uint32_t q : cl.tether_colors[c]) {
+          trec.push_back(make_uint4(base + cl.tether[2 * q], base + cl.tether[2 * q + 1], bits_of(cl.tether_rest[q]),
+                                    bits_of(cl.tether_compliance)));
+          tsc.push_back(s);
+        }
+      }
+      teth_ranges_[r].push_back({begin, (uint32_t)trec.size()});
+    }
+  }
+  // ---- cloth aerodynamics: per particle, its incident triangles ----------
+  // A cloth's drag and lift run before the fluids' preSolve (stage 0) when no
+  // fluid precedes it in its scene's materials, else after it (stage 1): the
+  // fluid neighbour lists see the cloth's predicted positions as the
+  // reference's material order leaves them.
+  std::vector<uint2> avtx;
+  std::vector<uint32_t> aoff(1, 0);
+  std::vector<uint4> atri;
+  for (uint32_t stage = 0; stage < 2; ++stage) {
+    const uint32_t begin = (uint32_t)avtx.size();
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      const uint32_t base = h_scenes_[s].seg_start;
+      bool fluid_before = false;
+      for (uint32_t r = 0; r < sp.materials.size(); ++r) {
+        if (sp.materials[r].first == MAT_FLUID) fluid_before = true;
+        if (sp.materials[r].first != MAT_CLOTH) continue;
+        const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+        if (cl.tris.empty() || (fluid_before ? 1u : 0u) != stage) continue;
+        // aero.ts:160-183: CSR of incident triangles in triangle order
+        const size_t nt = cl.tris.size() / 3;
+        std::vector<uint32_t> off(cl.n + 1, 0);
+        for (uint32_t v : cl.tris) ++off[v - cl.offset + 1];
+        for (uint32_t v = 0; v < cl.n; ++v) off[v + 1] += off[v];
+        std::vector<uint32_t> inc(off.back()), cur(off.begin(), off.end() - 1);
+        for (size_t t = 0; t < nt; ++t)
+          for (int c = 0; c < 3; ++c) inc[cur[cl.tris[3 * t + c] - cl.offset]++] = (uint32_t)t;
+        const uint32_t par = (uint32_t)cloth_par_of_[s][r];
+        for (uint32_t v = 0; v < cl.n; ++v) {
+          avtx.push_back(make_uint2(base + cl.offset + v, par));
+          for (uint32_t m = off[v]; m < off[v + 1]; ++m) {
+            const uint32_t* t = cl.tris.data() + 3ull * inc[m];
+            atri.push_back(make_uint4(base + t[0], base + t[1], base + t[2], 0u));
+          }
+          aoff.push_back((uint32_t)atri.size());
+        }
+      }
+    }
+    aero_ranges_[stage] = {begin, (uint32_t)avtx.size()};
+  }
+  // ---- cloth velocity smoothing by rank: per particle, its edge neighbours -
+  std::vector<uint2> dvtx;
+  std::vector<uint32_t> doff(1, 0), dnbr;
+  damp_ranges_.assign(max_rank_, {0, 0});
+  for (uint32_t r = 0; r < max_rank_; ++r) {
+    const uint32_t begin = (uint32_t)dvtx.size();
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      if (!(r < sp.materials.size() && sp.materials[r].first == MAT_CLOTH)) continue;
+      const ClothSpec& cl = sp.cloths[sp.materials[r].second];
+      if (!cl.has_damping) continue;
+      const uint32_t base = h_scenes_[s].seg_start;
+      // ClothSystem.ts:252-263: neighbours in pair order, both directions
+      const size_t np = cl.pairs.size() / 2;
+      std::vector<uint32_t> off(cl.n + 1, 0);
+      for (uint32_t v : cl.pairs) ++off[v - cl.offset + 1];
+      for (uint32_t v = 0; v < cl.n; ++v) off[v + 1] += off[v];
+      std::vector<uint32_t> nb(off.back()), cur(off.begin(), off.end() - 1);
+      for (size_t q = 0; q < np; ++q) {
+        const uint32_t i = cl.pairs[2 * q], j = cl.pairs[2 * q + 1];
+        nb[cur[i - cl.offset]++] = j;
+        nb[cur[j - cl.offset]++] = i;
+      }
+      const uint32_t par = (uint32_t)cloth_par_of_[s][r];
+      for (uint32_t v = 0; v < cl.n; ++v) {
+        dvtx.push_back(make_uint2(base + cl.offset + v, par));
+        for (uint32_t m = off[v]; m < off[v + 1]; ++m) dnbr.push_back(base + nb[m]);
+        doff.push_back((uint32_t)dnbr.size());
+      }
+    }
+    damp_ranges_[r] = {begin, (uint32_t)dvtx.size()};
   }
   // ---- soft-body tables (global by id) ----------------------------------
   std::vector<uint32_t> grp, grp_soft, csr_off(n_ + 1, 0), csr_idx;
@@ -1408,9 +1634,21 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.c_lambda = cv.take<float>(ci.size());
     base_.b_idx = cv.take<uint4>(bidx.size());
     base_.b_rest = cv.take<float>(brest.size());
-    base_.b_comp = cv.take<float>(bcomp.size());
+    base_.b_cloth = cv.take<uint32_t>(bcl.size());
     base_.b_scene = cv.take<uint32_t>(bsc.size());
     base_.b_lambda = cv.take<float>(bidx.size());
+    base_.t_rec = cv.take<uint4>(trec.size());
+    base_.t_scene = cv.take<uint32_t>(tsc.size());
+    base_.t_lambda = cv.take<float>(trec.size());
+    base_.a_vtx = cv.take<uint2>(avtx.size());
+    base_.a_off = cv.take<uint32_t>(aoff.size());
+    base_.a_tri = cv.take<uint4>(atri.size());
+    base_.d_vtx = cv.take<uint2>(dvtx.size());
+    base_.d_off = cv.take<uint32_t>(doff.size());
+    base_.d_nbr = cv.take<uint32_t>(dnbr.size());
+    base_.d_smooth = cv.take<float4>(dvtx.size());
+    cloth_par_dev_ = cv.take<DevCloth>(h_cloth_par_.size());
+    base_.cloth_par = cloth_par_dev_;
     stage_pos_ = cv.take<float4>(total_real);
     prefix_dev_ = cv.take<uint64_t>(K);
   };
@@ -1437,6 +1675,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   base_.n_bodies = (uint32_t)h_bodies_.size();
   base_.n_cons = (uint32_t)ci.size();
   base_.n_bend = (uint32_t)bidx.size();
+  base_.n_teth = (uint32_t)trec.size();
   base_.max_tiles = (uint32_t)max_tiles;
   base_.n_grid_scenes = (uint32_t)grid_scene.size();
   base_.n_rows = row_base.back();
@@ -1452,6 +1691,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_sdfs_, sizeof(DevSdf) * std::max<size_t>(1, h_sdfs_.size())));
+  PF_CUDA(cudaMallocHost(&h_pinned_cloth_, sizeof(DevCloth) * std::max<size_t>(1, h_cloth_par_.size())));
   // ---- upload ----------------------------------------------------------
   auto up = [&](const void* dst, const void* src, size_t bytes) -> pf_status {
     if (bytes == 0) return PF_OK;
@@ -1534,7 +1774,16 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_TRY(up(base_.c_scene, csc.data(), 4 * csc.size()));
   PF_TRY(up(base_.b_idx, bidx.data(), sizeof(uint4) * bidx.size()));
   PF_TRY(up(base_.b_rest, brest.data(), 4 * brest.size()));
-  PF_TRY(up(base_.b_comp, bcomp.data(), 4 * bcomp.size()));
+  PF_TRY(up(base_.b_cloth, bcl.data(), 4 * bcl.size()));
+  PF_TRY(up(base_.t_rec, trec.data(), sizeof(uint4) * trec.size()));
+  PF_TRY(up(base_.t_scene, tsc.data(), 4 * tsc.size()));
+  PF_TRY(up(base_.a_vtx, avtx.data(), sizeof(uint2) * avtx.size()));
+  PF_TRY(up(base_.a_off, aoff.data(), 4 * aoff.size()));
+  PF_TRY(up(base_.a_tri, atri.data(), sizeof(uint4) * atri.size()));
+  PF_TRY(up(base_.d_vtx, dvtx.data(), sizeof(uint2) * dvtx.size()));
+  PF_TRY(up(base_.d_off, doff.data(), 4 * doff.size()));
+  PF_TRY(up(base_.d_nbr, dnbr.data(), 4 * dnbr.size()));
+  PF_TRY(up(cloth_par_dev_, h_cloth_par_.data(), sizeof(DevCloth) * h_cloth_par_.size()));
   PF_TRY(up(base_.b_scene, bsc.data(), 4 * bsc.size()));
   PF_TRY(up(prefix_dev_, prefix_.data(), 8 * prefix_.size()));
   PF_TRY(up(base_.row_base, row_base.data(), 4 * row_base.size()));
@@ -1575,6 +1824,21 @@ pf_status World::set_sdf_transform(uint32_t scene, uint32_t slot, const float po
   return PF_OK;
 }
 
+pf_status World::set_cloth_params(uint32_t scene, uint32_t material, const pf_cloth_params& p) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "ClothSystem: no such scene");
+  if (material >= cloth_par_of_[scene].size() || cloth_par_of_[scene][material] < 0)
+    return fail(PF_ERR_INVALID, "ClothSystem: material " + std::to_string(material) + " is not a cloth");
+  ClothSpec& cl = specs_[scene]->cloths[specs_[scene]->materials[material].second];
+  DevCloth& P = h_cloth_par_[(size_t)cloth_par_of_[scene][material]];
+  for (int a = 0; a < 3; ++a) P.wind[a] = cl.wind[a] = p.wind[a];
+  P.drag = cl.drag = p.drag;
+  P.lift = cl.lift = p.lift;
+  P.damping = cl.damping = p.damping;
+  P.bend_compliance = cl.bend_compliance = p.bend_compliance;
+  cloth_par_dirty_ = true;
+  return PF_OK;
+}
+
 pf_status World::upload_params(double dt) {
   const uint32_t K = (uint32_t)h_scenes_.size();
   for (uint32_t s = 0; s < K; ++s) h_scenes_[s].dt = h_scenes_[s].substeps ? f32(dt / h_scenes_[s].substeps) : 0.0f;
@@ -1585,6 +1849,12 @@ pf_status World::upload_params(double dt) {
     PF_CUDA(cudaMemcpyAsync(const_cast<DevSdf*>(base_.sdfs), h_pinned_sdfs_, sizeof(DevSdf) * h_sdfs_.size(),
                             cudaMemcpyHostToDevice, stream_));
     sdfs_dirty_ = false;
+  }
+  if (cloth_par_dirty_ && !h_cloth_par_.empty()) {
+    std::memcpy(h_pinned_cloth_, h_cloth_par_.data(), sizeof(DevCloth) * h_cloth_par_.size());
+    PF_CUDA(cudaMemcpyAsync(cloth_par_dev_, h_pinned_cloth_, sizeof(DevCloth) * h_cloth_par_.size(),
+                            cudaMemcpyHostToDevice, stream_));
+    cloth_par_dirty_ = false;
   }
   if (prims_dirty_ && !h_prims_.empty()) {
     std::memcpy(h_pinned_prims_, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size());
@@ -1754,6 +2024,19 @@ void World::launch_cloth_rank(const WorldView& V, uint32_t r, uint32_t s, uint32
         k_bend<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, st>>>(V, rg.first, rg.second, s, it);
         ++t_launches;
       }
+  if (r < teth_ranges_.size())
+    for (auto& rg : teth_ranges_[r])
+      if (rg.second > rg.first) {
+        k_tether<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, st>>>(V, rg.first, rg.second, s, it);
+        ++t_launches;
+      }
+}
+
+void World::launch_aero(const WorldView& V, uint32_t stage, uint32_t s) {
+  const auto& rg = aero_ranges_[stage];
+  if (rg.second <= rg.first) return;
+  k_aero<<<div_up(rg.second - rg.first, kBlock), kBlock, 0, stream_>>>(V, rg.first, rg.second, s);
+  ++t_launches;
 }
 
 void World::run_substep(uint32_t s, uint32_t parity) {
@@ -1767,6 +2050,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     launch_slots(k_reset_sums, n_, stream_, V);
   }
   // preSolve
+  launch_aero(V, 0, s);
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
   if (any_fluid_) run_fluid_neighbors(V, s);
   // FluidSystem.ts:233-255: surface tension and adhesion, once per substep
@@ -1782,11 +2066,13 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       PF_BY_UNROLL(k_s_impulses, V, r, s);
       launch_slots(k_imp_apply, n_, stream_, V, r, s);
     }
+  launch_aero(V, 1, s);
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
   if (any_soft_local_ && pair_entries_) cudaMemsetAsync(base_.pair_lambda, 0, 16ull * pair_entries_, stream_);
   if (any_soft_global_) cudaMemsetAsync(base_.lambda_g, 0, 16ull * n_, stream_);
   if (base_.n_cons) cudaMemsetAsync(base_.c_lambda, 0, 4ull * base_.n_cons, stream_);
   if (base_.n_bend) cudaMemsetAsync(base_.b_lambda, 0, 4ull * base_.n_bend, stream_);
+  if (base_.n_teth) cudaMemsetAsync(base_.t_lambda, 0, 4ull * base_.n_teth, stream_);
   // iterations
   // Cloth-only scenes (and material-free scenes with colliders) share no
   // slot with the others: their colour sweeps and collider passes run on a
@@ -1852,6 +2138,13 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         ++t_launches;
       }
     }
+    if (r < damp_ranges_.size() && damp_ranges_[r].second > damp_ranges_[r].first) {
+      const auto& rg = damp_ranges_[r];
+      const uint32_t g = div_up(rg.second - rg.first, kBlock);
+      k_damp_mean<<<g, kBlock, 0, stream_>>>(V, rg.first, rg.second, s);
+      k_damp_apply<<<g, kBlock, 0, stream_>>>(V, rg.first, rg.second, s);
+      t_launches += 2;
+    }
   }
   if (any_prims_) {
     launch_slots(k_friction, n_, stream_, V, s);
@@ -1909,6 +2202,56 @@ pf_status World::step(double dt) {
   return PF_OK;
 }
 
+
+// Whole-field host write in particle order, the inverse of readback for the
+// writable fields: the slot array of the current parity is read, its
+// particles' entries patched through the id map, and written back (the w
+// lane of positions holds the inverse mass and is kept).
+pf_status World::write(uint32_t scene, uint32_t field, const void* src, size_t bytes) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "write: no such scene");
+  if (field > PF_FIELD_INV_MASS)
+    return fail(PF_ERR_INVALID, "write: field " + std::to_string(field) + " cannot be written");
+  const DevScene& S = h_scenes_[scene];
+  const uint32_t cap = S.cap, seg = S.seg_end - S.seg_start;
+  const bool w_only = field == PF_FIELD_INV_MASS;
+  const size_t need = (w_only ? 4ull : 16ull) * cap;
+  if (!src || bytes < need)
+    return fail(PF_ERR_INVALID, "write: source holds " + std::to_string(bytes) + " bytes, need " + std::to_string(need));
+  const float* f = static_cast<const float*>(src);
+  for (size_t i = 0; i < need / 4; ++i) {
+    if (!std::isfinite(f[i])) return fail(PF_ERR_INVALID, "write: values must be finite");
+    if (w_only && !(f[i] >= 0)) return fail(PF_ERR_INVALID, "write: invMass must be a finite number >= 0");
+  }
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<uint32_t> ids(seg);
+  PF_CUDA(cudaMemcpy(ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+  const StateBuf& B = buf_[parity_];
+  auto patch = [&](float4* dev) -> pf_status {
+    std::vector<float4> tmp(seg);
+    PF_CUDA(cudaMemcpy(tmp.data(), dev + S.seg_start, 16ull * seg, cudaMemcpyDeviceToHost));
+    for (uint32_t k = 0; k < seg; ++k) {
+      const uint32_t id = ids[k] - S.seg_start;
+      if (id >= cap) continue;
+      if (w_only) {
+        tmp[k].w = f[id];
+      } else {
+        tmp[k].x = f[4ull * id];
+        tmp[k].y = f[4ull * id + 1];
+        tmp[k].z = f[4ull * id + 2];
+      }
+    }
+    PF_CUDA(cudaMemcpy(dev + S.seg_start, tmp.data(), 16ull * seg, cudaMemcpyHostToDevice));
+    return PF_OK;
+  };
+  switch (field) {
+    case PF_FIELD_POSITIONS: return patch(B.x);
+    case PF_FIELD_PREDICTED: return patch(B.xs);
+    case PF_FIELD_VELOCITIES: return patch(B.v);
+    default:
+      PF_TRY(patch(B.x));
+      return patch(B.xs);
+  }
+}
 
 pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t bytes) {
   if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "readback: no such scene");

@@ -76,6 +76,18 @@ struct ClothSpec {
   std::vector<float> bend_rest;
   float bend_compliance = 1e-5f;
   std::vector<std::vector<uint32_t>> bend_colors;
+  // tethers (tether.ts): (free particle, pinned anchor) absolute indices
+  std::vector<uint32_t> tether;
+  std::vector<float> tether_rest;
+  float tether_compliance = 0.0f;
+  std::vector<std::vector<uint32_t>> tether_colors;
+  // aerodynamics (aero.ts): absolute triangle indices
+  std::vector<uint32_t> tris;
+  float wind[3] = {0.0f, 0.0f, 0.0f};
+  float drag = 0.6125f, lift = 0.3f;
+  // velocity smoothing (ClothSystem.buildDamping)
+  bool has_damping = false;
+  float damping = 0.0f;
 };
 
 // SDFCollider state (SDFCollider.ts:88-137): the grid as half floats plus
@@ -159,6 +171,12 @@ struct DevFluid {
   uint32_t bnd_first, bnd_count;
   uint32_t react_lo, react_hi;  // covering id range of the boundaries (lo == hi: no reaction)
   float react_scale, react_inv;
+};
+
+// Mutable parameters of one cloth (ClothSystem.ts:143-188 setters).
+struct DevCloth {
+  float wind[3];
+  float drag, lift, damping, bend_compliance, pad;
 };
 
 struct DevBoundary {
@@ -287,10 +305,27 @@ struct WorldView {
   // cloth bending (bending.ts), by (rank, colour)
   const uint4* b_idx;  // particle ids (p1, p2, p3, p4)
   const float* b_rest;
-  const float* b_comp;
+  const uint32_t* b_cloth;  // cloth parameter index (bending compliance)
   const uint32_t* b_scene;
   float* b_lambda;
   uint32_t n_bend;
+  // cloth tethers (tether.ts), by (rank, colour)
+  const uint4* t_rec;  // (particle id, anchor id, rest bits, compliance bits)
+  const uint32_t* t_scene;
+  float* t_lambda;
+  uint32_t n_teth;
+  // cloth aerodynamics (aero.ts): one record per cloth particle, its
+  // incident triangles as a CSR over a_tri
+  const uint2* a_vtx;   // (particle id, cloth parameter index)
+  const uint32_t* a_off;
+  const uint4* a_tri;   // (i1, i2, i3) particle ids
+  // cloth velocity smoothing (ClothSystem.buildDamping): one record per
+  // cloth particle, its edge neighbours as a CSR over d_nbr
+  const uint2* d_vtx;   // (particle id, cloth parameter index)
+  const uint32_t* d_off;
+  const uint32_t* d_nbr;  // particle ids
+  float4* d_smooth;     // blended velocity per record
+  const DevCloth* cloth_par;
 };
 
 class World {
@@ -318,6 +353,8 @@ class World {
   pf_status step(double dt);
   pf_status set_primitive(uint32_t scene, uint32_t slot, const pf_primitive& p);
   pf_status set_sdf_transform(uint32_t scene, uint32_t slot, const float pos[3], const double q[4], float scale);
+  pf_status set_cloth_params(uint32_t scene, uint32_t material, const pf_cloth_params& p);
+  pf_status write(uint32_t scene, uint32_t field, const void* src, size_t bytes);
   pf_status readback(uint32_t scene, uint32_t field, void* dst, size_t bytes);
   // Copies the scene's state (by particle index) back into its spec.
   pf_status pull_state(uint32_t scene, SceneSpec* spec);
@@ -387,7 +424,15 @@ class World {
   uint32_t max_rank_ = 0, max_sub_ = 0, max_iter_ = 0;
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> cloth_ranges_;  // [rank] -> per colour [begin,end)
   std::vector<std::vector<std::pair<uint32_t, uint32_t>>> bend_ranges_;   // [rank] -> per colour [begin,end)
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> teth_ranges_;   // [rank] -> per colour [begin,end)
+  std::pair<uint32_t, uint32_t> aero_ranges_[2] = {{0, 0}, {0, 0}};      // before / after the fluid preSolve
+  std::vector<std::pair<uint32_t, uint32_t>> damp_ranges_;               // [rank] -> [begin,end)
+  std::vector<DevCloth> h_cloth_par_;
+  std::vector<std::vector<int32_t>> cloth_par_of_;  // [scene][material] -> parameter index (-1: not a cloth)
+  bool cloth_par_dirty_ = false;
+  DevCloth* cloth_par_dev_ = nullptr;
   void launch_cloth_rank(const WorldView& V, uint32_t r, uint32_t s, uint32_t it, cudaStream_t st);
+  void launch_aero(const WorldView& V, uint32_t stage, uint32_t s);
   bool any_grid_ = false, any_prims_ = false, any_fluid_ = false, any_visc_ = false, any_vort_ = false;
   bool any_imp_ = false;  // surface tension or adhesion somewhere
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
@@ -420,6 +465,7 @@ class World {
   DevScene* h_pinned_scenes_ = nullptr;
   pf_primitive* h_pinned_prims_ = nullptr;
   DevSdf* h_pinned_sdfs_ = nullptr;
+  DevCloth* h_pinned_cloth_ = nullptr;
   bool prims_dirty_ = true;
   size_t pair_entries_ = 0;
   float4* stage_pos_ = nullptr;  // gather buffer of read_positions

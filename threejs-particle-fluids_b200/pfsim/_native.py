@@ -129,6 +129,40 @@ class ClothDesc(C.Structure):
         ("bending", C.POINTER(C.c_uint32)),
         ("bending_rest", C.POINTER(C.c_float)),
         ("bend_compliance", C.c_float),
+        ("n_tethers", C.c_uint32),
+        ("tether_particle", C.POINTER(C.c_uint32)),
+        ("tether_anchor", C.POINTER(C.c_uint32)),
+        ("tether_rest", C.POINTER(C.c_float)),
+        ("tether_compliance", C.c_float),
+        ("n_triangles", C.c_uint32),
+        ("triangles", C.POINTER(C.c_uint32)),
+        ("wind", C.c_float * 3),
+        ("drag", C.c_float),
+        ("lift", C.c_float),
+        ("has_damping", C.c_uint32),
+        ("damping", C.c_float),
+    ]
+
+
+class ClothParams(C.Structure):
+    _fields_ = [
+        ("wind", C.c_float * 3),
+        ("drag", C.c_float),
+        ("lift", C.c_float),
+        ("damping", C.c_float),
+        ("bend_compliance", C.c_float),
+    ]
+
+
+class TetherBuildDesc(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_uint32),
+        ("inv_mass", C.POINTER(C.c_float)),
+        ("n_pairs", C.c_uint32),
+        ("pairs", C.POINTER(C.c_uint32)),
+        ("rest_lengths", C.POINTER(C.c_double)),
+        ("max_attachments", C.c_uint32),
+        ("stretch_tolerance", C.c_double),
     ]
 
 
@@ -242,6 +276,9 @@ SIGNATURES = {
     "pf_add_fluid": (C.c_int, [_P, C.POINTER(FluidDesc), _u32p]),
     "pf_add_softbodies": (C.c_int, [_P, C.POINTER(SoftbodyDesc), _u32p]),
     "pf_add_cloth": (C.c_int, [_P, C.POINTER(ClothDesc), _u32p]),
+    "pf_cloth_get_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
+    "pf_cloth_set_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
+    "pf_cloth_build_tethers": (C.c_int, [C.POINTER(TetherBuildDesc), _u32p, _u32p, _f32p, C.c_uint32, _u32p]),
     "pf_add_primitive": (C.c_int, [_P, C.POINTER(Primitive), _u32p]),
     "pf_set_primitive": (C.c_int, [_P, C.c_uint32, C.POINTER(Primitive)]),
     "pf_loop_build": (C.c_int, [_P, C.POINTER(LoopDesc)]),
@@ -265,6 +302,9 @@ SIGNATURES = {
     "pf_batch_destroy": (None, [_P]),
     "pf_batch_step": (C.c_int, [_P, C.c_double]),
     "pf_batch_set_primitive": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(Primitive)]),
+    "pf_batch_cloth_set_params": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(ClothParams)]),
+    "pf_batch_write": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t]),
+    "pf_write": (C.c_int, [_P, C.c_uint32, C.c_void_p, C.c_size_t]),
     "pf_batch_readback": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_size_t]),
     "pf_batch_overflow_read": (C.c_int, [_P, C.c_uint32, C.POINTER(Overflow)]),
     "pf_batch_last_step_ms": (C.c_int, [_P, _f32p]),

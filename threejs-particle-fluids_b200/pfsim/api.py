@@ -28,6 +28,7 @@ import numpy as np
 
 from . import _native as N
 from . import recipe as R
+from . import shapes
 
 
 def _err(cls: str, msg: str) -> N.PfError:
@@ -121,20 +122,117 @@ class SoftbodySystem:
 
 
 class ClothSystem:
-    """src/cloth/ClothSystem.ts:37-141, 190-212 with a ClothGraph (pfsim.shapes):
-    stretch and dihedral bending constraints (aerodynamics and tethers are
-    not built)."""
+    """src/cloth/ClothSystem.ts:37-304 with a ClothGraph (pfsim.shapes):
+    stretch, dihedral bending and long-range tether constraints (tethers
+    built from the graph's pins by buildTethers), aerodynamic drag and lift
+    on the graph's triangles, and the optional velocity smoothing pass. The
+    wind, drag, lift, damping and bend_compliance setters take effect from
+    the next step."""
+
+    kind = "cloth"
 
     def __init__(self, particles: ParticleSystem, graph, offset: int = 0, stretch_compliance: float = 1e-7,
-                 bend_compliance: float = 1e-5):
+                 bend_compliance: float = 1e-5, tether_compliance: float = 0.0, stretch_tolerance: float = 0.0,
+                 wind=(0.0, 0.0, 0.0), drag: float = 0.6125, lift: float = 0.3, damping: float | None = None):
+        for name, v in (("stretchCompliance", stretch_compliance), ("bendCompliance", bend_compliance),
+                        ("tetherCompliance", tether_compliance), ("stretchTolerance", stretch_tolerance),
+                        ("drag", drag), ("lift", lift)):
+            _non_negative(name, v)
+        if damping is not None:
+            _unit_interval("damping", damping)
         self.particles = particles
+        self.graph = graph
+        self.offset = offset
+        self._wind = tuple(float(w) for w in wind)
+        self._drag, self._lift = float(drag), float(lift)
+        self._damping = damping
+        self._bend = float(bend_compliance)
+        self.tethers = shapes.build_tethers(graph.inv_mass, graph.pairs, graph.rest_lengths,
+                                            stretch_tolerance=stretch_tolerance)
+        tp, ta, tr = self.tethers
         self.opts = R.ClothOpts(offset=offset, positions=np.asarray(graph.positions, np.float32),
                                 inv_mass=np.asarray(graph.inv_mass, np.float32), pairs=graph.pairs,
                                 rest_lengths=np.asarray(graph.rest_lengths, np.float32),
                                 stretch_compliance=stretch_compliance,
                                 bending=graph.bending, bending_rest=np.asarray(graph.bending_rest, np.float32),
-                                bend_compliance=bend_compliance)
-    kind = "cloth"
+                                bend_compliance=bend_compliance,
+                                tether_particle=tp, tether_anchor=ta, tether_rest=tr,
+                                tether_compliance=tether_compliance, triangles=graph.triangles,
+                                wind=self._wind, drag=drag, lift=lift, damping=damping)
+
+    def _push(self) -> None:
+        loop = self.particles.loop
+        if loop is None or loop.scene is None or self not in loop.materials:
+            return
+        loop.scene.set_cloth_params(loop.materials.index(self), self.params())
+
+    def params(self):
+        return R.cloth_params(self._wind, self._drag, self._lift, self._damping or 0.0, self._bend)
+
+    @property
+    def wind(self) -> tuple:
+        return self._wind
+
+    @wind.setter
+    def wind(self, value) -> None:
+        w = tuple(float(x) for x in value)
+        if len(w) != 3 or not all(math.isfinite(x) for x in w):
+            raise _err("ClothSystem", f"wind must be three finite numbers, got {value}")
+        self._wind = w
+        self._push()
+
+    @property
+    def drag(self) -> float:
+        return self._drag
+
+    @drag.setter
+    def drag(self, value: float) -> None:
+        self._drag = _non_negative("drag", value)
+        self._push()
+
+    @property
+    def lift(self) -> float:
+        return self._lift
+
+    @lift.setter
+    def lift(self, value: float) -> None:
+        self._lift = _non_negative("lift", value)
+        self._push()
+
+    @property
+    def damping(self) -> float:
+        return self._damping or 0.0
+
+    @damping.setter
+    def damping(self, value: float) -> None:
+        _unit_interval("damping", value)
+        if self._damping is None:
+            raise _err("ClothSystem", "damping was not given at creation, so there is no smoothing pass to change")
+        self._damping = float(value)
+        self._push()
+
+    @property
+    def bend_compliance(self) -> float:
+        return self._bend
+
+    @bend_compliance.setter
+    def bend_compliance(self, value: float) -> None:
+        self._bend = _non_negative("bendCompliance", value)
+        self._push()
+
+
+def _non_negative(name: str, value: float) -> float:
+    """ClothSystem.ts:290-295."""
+    if not (value >= 0) or not math.isfinite(value):
+        raise _err("ClothSystem", f"{name} must be ≥ 0, got {value}")
+    return float(value)
+
+
+def _unit_interval(name: str, value: float) -> float:
+    """ClothSystem.ts:297-302."""
+    if not (0 <= value <= 1):
+        raise _err("ClothSystem", f"{name} must be between 0 and 1, got {value}")
+    return float(value)
 
 
 class PrimitiveSet:
@@ -277,6 +375,8 @@ class _ClothReq:
     position: tuple
     softness: float
     pin: str
+    weight: float
+    wind: tuple
 
 
 class Simulation:
@@ -325,10 +425,25 @@ class Simulation:
             raise _err("addSoftbody", f"shape must be 'sphere' or 'box', got {shape}")
         self.softs.append(_SoftReq(shape, tuple(center), float(size), float(softness), float(density)))
 
-    def add_cloth(self, width: float, height: float, position=(0.0, 0.5, 0.0), softness: float = 0.0,
-                  pin: str = "top") -> None:
+    def add_cloth(self, width: float, height: float, position=(0.0, 0.5, 0.0), softness: float = 0.75,
+                  pin: str = "top", weight: float = 0.1, wind=(0.0, 0.0, 0.0)) -> int:
+        """Simulation.addCloth (Simulation.ts:416-426) with its defaults:
+        softness 0.75, weight 0.1 kg/m^2, no wind. Returns the cloth's index
+        for set_cloth_wind."""
         self._not_started("addCloth")
-        self.cloths.append(_ClothReq(width, height, tuple(position), softness, pin))
+        if pin not in ("top", "none"):
+            raise _err("addCloth", f"pin must be 'top' or 'none', got {pin}")
+        self.cloths.append(_ClothReq(width, height, tuple(position), softness, pin, float(weight),
+                                     tuple(float(w) for w in wind)))
+        return len(self.cloths) - 1
+
+    def set_cloth_wind(self, index: int, wind) -> None:
+        """Cloth.wind (the façade copies it into its ClothSystem before each
+        step, Simulation.ts:632)."""
+        c = self.cloths[index]
+        c.wind = tuple(float(w) for w in wind)
+        if self.loop is not None:
+            self._cloth_systems[index].wind = c.wind
 
     def add_floor(self, y: float = 0.0) -> None:
         self.prims.append(R.plane((0, 1, 0), (0.0, y, 0.0)))
@@ -402,12 +517,11 @@ class Simulation:
             pos, idx = shapes.plane_geometry(c.width, c.height, seg_w, seg_h)
             pos = pos + np.asarray(c.position)
             pinned = range(seg_w + 1) if c.pin == "top" else ()
-            g = shapes.create_cloth_graph(pos, idx, 0.2, pinned=pinned)
-            mats.append(("cloth", R.ClothOpts(offset=n, positions=g.positions.astype(np.float32), inv_mass=g.inv_mass,
-                                              pairs=g.pairs, rest_lengths=g.rest_lengths,
-                                              stretch_compliance=1e-7 * (1.0 + 1e4 * c.softness),
-                                              bending=g.bending, bending_rest=g.bending_rest.astype(np.float32),
-                                              bend_compliance=1e-5)))
+            g = shapes.create_cloth_graph(pos, idx, c.weight, pinned=pinned)
+            # Simulation.ts:703-718, handles.ts:298-300
+            bend = 10 ** (-1 + c.softness * 5) * (seg_w / 30) ** 4 * (0.35 / c.weight)
+            mats.append(("cloth", (g, n, dict(bend_compliance=bend, stretch_tolerance=0.06, wind=c.wind,
+                                              drag=0.18, lift=0.02, damping=0.1))))
             n += len(pos)
         if n == 0:
             raise N.PfError(N.PF_ERR_STATE, "Simulation: nothing to simulate; add a fluid, soft body or cloth")
@@ -423,9 +537,15 @@ class Simulation:
         rec_loop = dict(substeps=int(substeps), iterations=2, gravity=self.gravity)
         self.particles = ps
         matobjs = []
+        self._cloth_systems = []
         for kind, opts in mats:
-            o = object.__new__({"fluid": FluidSystem, "soft": SoftbodySystem, "cloth": ClothSystem}[kind])
-            o.particles, o.opts = ps, opts
+            if kind == "cloth":
+                g, off, kw = opts
+                o = ClothSystem(ps, g, offset=off, **kw)
+                self._cloth_systems.append(o)
+            else:
+                o = object.__new__({"fluid": FluidSystem, "soft": SoftbodySystem}[kind])
+                o.particles, o.opts = ps, opts
             matobjs.append(o)
         pset = PrimitiveSet(ps)
         pset.prims = prims

@@ -77,6 +77,24 @@ class ClothOpts:
     bending: np.ndarray | None = None  # (b, 4) cloth-local (p1, p2, p3, p4)
     bending_rest: np.ndarray | None = None  # (b,) signed rest angles
     bend_compliance: float = -1.0
+    tether_particle: np.ndarray | None = None  # (t,) cloth-local free particles
+    tether_anchor: np.ndarray | None = None  # (t,) cloth-local pinned anchors
+    tether_rest: np.ndarray | None = None  # (t,) rest radii
+    tether_compliance: float = -1.0
+    triangles: np.ndarray | None = None  # (k, 3) cloth-local: drag and lift (aero.ts)
+    wind: tuple = (0.0, 0.0, 0.0)
+    drag: float = -1.0
+    lift: float = -1.0
+    damping: float | None = None  # None: no velocity smoothing pass
+
+
+def cloth_params(wind=(0.0, 0.0, 0.0), drag: float = 0.6125, lift: float = 0.3, damping: float = 0.0,
+                 bend_compliance: float = 1e-5) -> N.ClothParams:
+    """The ClothSystem setters' values as the C-ABI's pf_cloth_params."""
+    p = N.ClothParams()
+    p.wind[:] = [float(w) for w in wind]
+    p.drag, p.lift, p.damping, p.bend_compliance = drag, lift, damping, bend_compliance
+    return p
 
 
 @dataclass
@@ -301,6 +319,20 @@ def cloth_desc(o: ClothOpts, keep: _Keep) -> N.ClothDesc:
         d.bending = keep.u32(b)
         d.bending_rest = keep.f32(np.asarray(o.bending_rest, np.float32))
     d.bend_compliance = o.bend_compliance
+    if o.tether_particle is not None and len(o.tether_particle):
+        d.n_tethers = len(o.tether_particle)
+        d.tether_particle = keep.u32(np.asarray(o.tether_particle, np.uint32))
+        d.tether_anchor = keep.u32(np.asarray(o.tether_anchor, np.uint32))
+        d.tether_rest = keep.f32(np.asarray(o.tether_rest, np.float32))
+    d.tether_compliance = o.tether_compliance
+    if o.triangles is not None and len(o.triangles):
+        t = np.asarray(o.triangles, np.uint32).reshape(-1)
+        d.n_triangles = t.size // 3
+        d.triangles = keep.u32(t)
+    d.wind[:] = [float(w) for w in o.wind]
+    d.drag, d.lift = o.drag, o.lift
+    if o.damping is not None:
+        d.has_damping, d.damping = 1, o.damping
     return d
 
 
@@ -358,6 +390,16 @@ class Scene:
     def set_primitive(self, slot: int, prim: Prim) -> None:
         p = prim.cstruct()
         N.check(N.lib().pf_set_primitive(self.h, slot, C.byref(p)))
+
+    def write(self, field_id: int, data: np.ndarray) -> None:
+        """pf_write: a whole field (positions, predicted, velocities: float4 x
+        capacity; inverse mass: float x capacity) in particle order."""
+        a = np.ascontiguousarray(data, np.float32)
+        N.check(N.lib().pf_write(self.h, field_id, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def set_cloth_params(self, material: int, params: N.ClothParams) -> None:
+        """pf_cloth_set_params: the ClothSystem setters of material `material`."""
+        N.check(N.lib().pf_cloth_set_params(self.h, material, C.byref(params)))
 
     def readback(self, field_id: int) -> np.ndarray:
         out = alloc_field(field_id, self.capacity)
@@ -452,6 +494,13 @@ class Batch:
         out = alloc_field(field_id, self.capacities[index])
         N.check(N.lib().pf_batch_readback(self.h, index, field_id, out.ctypes.data_as(C.c_void_p), out.nbytes))
         return out
+
+    def write(self, index: int, field_id: int, data: np.ndarray) -> None:
+        a = np.ascontiguousarray(data, np.float32)
+        N.check(N.lib().pf_batch_write(self.h, index, field_id, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def set_cloth_params(self, index: int, material: int, params: N.ClothParams) -> None:
+        N.check(N.lib().pf_batch_cloth_set_params(self.h, index, material, C.byref(params)))
 
     def overflow(self, index: int) -> dict:
         o = N.Overflow()

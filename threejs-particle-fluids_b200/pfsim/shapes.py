@@ -114,6 +114,7 @@ class ClothGraph:
     rest_lengths: np.ndarray  # (m,)
     bending: np.ndarray  # (b, 4): (p1, p2, p3, p4) per edge shared by two triangles
     bending_rest: np.ndarray  # (b,) signed rest dihedral angles
+    triangles: np.ndarray  # (t, 3) non-degenerate triangles in index order
 
 
 def dihedral_angles(pos: np.ndarray, tuples: np.ndarray) -> np.ndarray:
@@ -171,7 +172,8 @@ def create_cloth_graph(positions, index, surface_density: float = 0.2, pinned=()
     ordr = np.argsort(_edge_rank(keys, k2), kind="stable")
     tuples = np.stack([k2 // n, k2 % n, f1, f2], -1)[ordr].astype(np.uint32)
     bending_rest = dihedral_angles(pos, tuples.astype(np.int64))
-    return ClothGraph(pos, inv, pairs, rest, tuples, bending_rest)
+    triangles = np.stack([a, b, c], -1).astype(np.uint32)
+    return ClothGraph(pos, inv, pairs, rest, tuples, bending_rest, triangles)
 
 
 def _edge_rank(edge_keys_in_order: np.ndarray, query: np.ndarray) -> np.ndarray:
@@ -179,3 +181,40 @@ def _edge_rank(edge_keys_in_order: np.ndarray, query: np.ndarray) -> np.ndarray:
     idx = np.argsort(edge_keys_in_order, kind="stable")
     pos = np.searchsorted(edge_keys_in_order[idx], query)
     return idx[pos]
+
+
+def build_tethers(inv_mass, pairs, rest_lengths, max_attachments: int = 4, stretch_tolerance: float = 0.0):
+    """buildTethers (src/cloth/tetherBuild.ts:84-219) in the native library
+    (pf_cloth_build_tethers): for every free particle, one long-range
+    attachment to the nearest pinned particle of each of its
+    `max_attachments` geodesically closest pinned islands. Returns cloth-local
+    (particle, anchor) uint32 arrays and float32 rest radii, particle-major."""
+    import ctypes as C
+
+    from . import _native as N
+
+    if not (isinstance(max_attachments, int) and max_attachments > 0):
+        raise N.PfError(N.PF_ERR_INVALID,
+                        f"buildTethers: maxAttachmentsPerParticle must be a positive integer, got {max_attachments}")
+    inv = np.ascontiguousarray(inv_mass, np.float32)
+    pr = np.ascontiguousarray(pairs, np.uint32).reshape(-1)
+    rl = np.ascontiguousarray(rest_lengths, np.float64)
+    n = inv.size
+    d = N.TetherBuildDesc()
+    d.n_particles = n
+    d.inv_mass = inv.ctypes.data_as(C.POINTER(C.c_float))
+    d.n_pairs = pr.size // 2
+    d.pairs = pr.ctypes.data_as(C.POINTER(C.c_uint32))
+    d.rest_lengths = rl.ctypes.data_as(C.POINTER(C.c_double))
+    d.max_attachments = max_attachments
+    d.stretch_tolerance = float(stretch_tolerance)
+    cap = max(1, n * max_attachments)
+    part = np.empty(cap, np.uint32)
+    anch = np.empty(cap, np.uint32)
+    rest = np.empty(cap, np.float32)
+    cnt = C.c_uint32(0)
+    N.check(N.lib().pf_cloth_build_tethers(C.byref(d), part.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           anch.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           rest.ctypes.data_as(C.POINTER(C.c_float)), cap, C.byref(cnt)))
+    k = cnt.value
+    return part[:k].copy(), anch[:k].copy(), rest[:k].copy()

@@ -114,7 +114,9 @@ def dam_break(n_budget: int = 5000, seed: int = 0, scale: float = 1.0, jitter: f
 
 
 def cloth_sheet(side: int = 64, seed: int = 0, scale: float = 1.0, compliance: float = 1e-6,
-                substeps: int = 2, iterations: int = 4, offset=(0.0, 0.0, 0.0), bend_compliance: float | None = None):
+                substeps: int = 2, iterations: int = 4, offset=(0.0, 0.0, 0.0), bend_compliance: float | None = None,
+                tethers: bool = False, tether_compliance: float = 0.0, stretch_tolerance: float = 0.0,
+                wind=None, drag: float = 0.6125, lift: float = 0.3, damping: float | None = None):
     """A hanging cloth sheet of side x side particles (PlaneGeometry with
     side-1 segments per axis, structural + shear distance constraints, the
     top row pinned) inside the dam-break container scaled by `scale`; the
@@ -146,6 +148,13 @@ def cloth_sheet(side: int = 64, seed: int = 0, scale: float = 1.0, compliance: f
     if bend_compliance is not None:  # dihedral bending as well (the batch configuration has stretch only)
         cloth.bending, cloth.bending_rest = graph.bending, graph.bending_rest.astype(np.float32)
         cloth.bend_compliance = bend_compliance
+    if tethers:  # long-range attachments to the pinned top row
+        cloth.tether_particle, cloth.tether_anchor, cloth.tether_rest = shapes.build_tethers(
+            graph.inv_mass, graph.pairs, graph.rest_lengths, stretch_tolerance=stretch_tolerance)
+        cloth.tether_compliance = tether_compliance
+    if wind is not None:  # drag and lift on the sheet's triangles
+        cloth.triangles, cloth.wind, cloth.drag, cloth.lift = graph.triangles, tuple(wind), drag, lift
+    cloth.damping = damping
     loop = R.LoopOpts(substeps=substeps, iterations=iterations)
     return R.Recipe(capacity=n, radius=0.5 * edge, materials=[("cloth", cloth)],
                     prims=R.container_walls(tuple(c_lo), tuple(c_hi)), loop=loop, name=f"cloth_{side}x{side}")
