@@ -209,6 +209,11 @@ typedef struct pf_softbody_desc {
   uint32_t n_bodies;
   const pf_softbody_def* bodies;
   uint32_t shape_matching;      /* PF_SHAPE_MATCH_* */
+  /* SoftbodySystemOptions.selfCollision (SoftbodySystem.ts:72, 218-234):
+   * 0 = at pf_loop_build every body whose particles share no non-zero
+   * collision group gets a fresh one (above every uploaded group), so its
+   * particles never contact each other. */
+  uint32_t self_collision;
 } pf_softbody_desc;
 PF_API pf_status pf_add_softbodies(pf_scene* scene, const pf_softbody_desc* desc,
                                    uint32_t* material_index);
@@ -351,8 +356,31 @@ typedef struct pf_loop_desc {
    * uploaded particles and primitives plus a margin. */
   float grid_min[3];
   float grid_max[3];
+  /* SimLoopOptions.contact (loop.ts:20-30, 347-417; src/core/contact/):
+   * particle-particle contacts between every pair of particles within 2r
+   * (candidates within 2r x 1.1) outside a common non-zero collision group,
+   * found from the particles outside the noSelfContacts ranges (the fluids'
+   * and pf_add_no_self_contacts'), with static friction in the solve and
+   * kinetic friction after it. */
+  uint32_t contact;             /* 0 = off */
+  float contact_mu_s;           /* < 0 selects the default 0.5 */
+  float contact_mu_k;           /* < 0 selects the default 0.4 */
+  uint32_t max_contacts;        /* pairs kept per substep; 0 selects 8 x capacity */
 } pf_loop_desc;
 PF_API pf_status pf_loop_build(pf_scene* scene, const pf_loop_desc* desc);
+
+/* A material that only declares MaterialKernels.noSelfContacts
+ * (materials.ts:45): particles of `range` search for no contacts, so pairs
+ * of two of them are never generated (pairs with another particle are found
+ * from the other side). Fluids declare their own range this way. */
+PF_API pf_status pf_add_no_self_contacts(pf_scene* scene, pf_range range);
+
+/* ContactBuffer.readbackCount / readbackPairs (ContactBuffer.ts:75-97): the
+ * pairs the last substep generated, dropped ones included in `count`;
+ * `pairs` receives up to `capacity` (i, j) particle-index pairs, each pair
+ * ordered i < j and the list sorted. Synchronous. */
+PF_API pf_status pf_contacts_read(pf_scene* scene, uint32_t* pairs, uint32_t capacity, uint32_t* count,
+                                  uint32_t* stored);
 
 /* SimLoop.step(dt) (loop.ts:267-279): one frame of `substeps` substeps, dt in
  * seconds (a double, as the reference's JavaScript number). Asynchronous. */

@@ -74,6 +74,8 @@ def _bind(L: C.CDLL) -> None:
         "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
         "or_cloth_set_params": (C.c_int, [P, C.c_uint32, C.POINTER(N.ClothParams)]),
         "or_write": (C.c_int, [P, C.c_uint32, f32p, C.c_size_t]),
+        "or_add_no_self_contacts": (C.c_int, [P, N.Range]),
+        "or_contacts_read": (C.c_int, [P, u32p, C.c_uint32, u32p, u32p]),
         "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
         "or_step": (C.c_int, [P, C.c_double]),
         "or_readback": (C.c_int, [P, C.c_uint32, P, C.c_size_t, C.c_int]),
@@ -309,6 +311,16 @@ class OracleScene:
         """params: a pfsim._native.ClothParams (ClothSystem setters)."""
         check(lib().or_cloth_set_params(self.h, material, C.byref(params)))
 
+    def contacts(self) -> tuple:
+        """(pairs found in the last substep, the stored pairs (m, 2), each
+        ascending, sorted)."""
+        cap = max(1, 32 * self.capacity)
+        out = np.empty(2 * cap, np.uint32)
+        count, stored = C.c_uint32(0), C.c_uint32(0)
+        check(lib().or_contacts_read(self.h, _p(out, C.c_uint32), cap, C.byref(count), C.byref(stored)))
+        m = min(stored.value, cap)
+        return int(count.value), out[: 2 * m].reshape(-1, 2).copy()
+
     def write(self, field_id: int, data: np.ndarray) -> None:
         a = np.ascontiguousarray(data, np.float32)
         check(lib().or_write(self.h, field_id, _p(a), a.nbytes))
@@ -366,7 +378,8 @@ class OracleBackend:
             p = R.pos4(u.pos)
             v = None if u.vel is None else keep.f32(R.pos4(u.vel))
             w = None if u.inv_mass is None else keep.f32(u.inv_mass)
-            check(L.or_upload_particles(h, keep.f32(p), v, w, None, u.start, p.shape[0]))
+            g = None if u.group is None else keep.u32(np.asarray(u.group, np.uint32))
+            check(L.or_upload_particles(h, keep.f32(p), v, w, g, u.start, p.shape[0]))
         for kind, opts in r.materials:
             if kind == "fluid":
                 check(L.or_add_fluid(h, C.byref(R.fluid_desc(opts, keep)), None))
@@ -374,6 +387,8 @@ class OracleBackend:
                 check(L.or_add_softbodies(h, C.byref(R.softbody_desc(opts, keep)), None))
             elif kind == "cloth":
                 check(L.or_add_cloth(h, C.byref(R.cloth_desc(opts, keep)), None))
+        for q in r.quiet:
+            check(L.or_add_no_self_contacts(h, N.Range(*q)))
         for p in r.prims:
             cs = p.cstruct()
             check(L.or_add_primitive(h, C.byref(cs), None))

@@ -317,6 +317,7 @@ template <typename T>
 struct Softbodies {
   std::vector<Body<T>> bodies;
   bool local = true;
+  bool selfCollision = false;
   Range span;
   std::vector<float> restOffsets;  // float4 per particle (reference Float32Array)
   std::vector<float> weights;
@@ -447,6 +448,19 @@ struct Engine {
   // colliders
   bool hasColliders = false;
   Accum<T> accPos, accVel;
+  // particle contacts (loop.ts:347-417, src/core/contact/)
+  bool hasContact = false;
+  T cMuS = 0, cMuK = 0, cDist = 0, cCand2 = 0;
+  uint32_t maxContacts = 0, contactCount = 0;
+  std::vector<Range> quietRanges;  // Material.noSelfContacts besides the fluids'
+  std::vector<uint8_t> quiet;
+  struct Contact {
+    uint32_t i, j;
+    int32_t ln, lt;  // ticks of 2^-20 kg m (ContactBuffer.ts:16)
+    V3<T> n;
+  };
+  std::vector<Contact> contacts;
+  bool hasAcc() const { return hasColliders || hasContact; }
   std::vector<T> primLambda;  // 2 * cap * primCap
   uint32_t primCap = 0;
   T clock = 0;
@@ -1513,13 +1527,109 @@ struct Engine {
     }
   }
 
+  // ---------------------------------------------------------- contacts ----
+  // f32 -> i32 toward zero, saturating (the shader's toInt()).
+  static int32_t lam_ticks(T v) { return sat_i32(std::trunc(static_cast<double>(v * static_cast<T>(1048576)))); }
+  static int32_t wrap_add(int32_t a, int32_t b) {
+    return static_cast<int32_t>(static_cast<uint32_t>(a) + static_cast<uint32_t>(b));
+  }
+
+  // generate.ts:53-88: every particle outside the noSelfContacts ranges, in
+  // index order, walks its 27 buckets; a pair of two emitters is kept by the
+  // lower index. Pairs past maxContacts are counted, not stored.
+  void contact_generate() {
+    contacts.clear();
+    contactCount = 0;
+    for (uint32_t i = 0; i < cap; ++i) {
+      if (quiet[i]) continue;
+      const V3<T> xi = p3(pred, i);
+      const uint32_t gi = group[i];
+      const T wi = invMass[i];
+      for_each_neighbor(xi, [&](uint32_t j, uint32_t) {
+        if (j == i) return;
+        if (!quiet[j] && j < i) return;
+        if (gi != 0 && gi == group[j]) return;
+        if (wi <= 0 && invMass[j] <= 0) return;
+        const V3<T> d = xi - p3(pred, j);
+        if (dot(d, d) >= cCand2) return;
+        if (contactCount < maxContacts) contacts.push_back({i, j, 0, 0, v3<T>(0, 0, 0)});
+        ++contactCount;
+      });
+    }
+  }
+
+  // solve.ts:115-150, then the accumulator applied to the committed and the
+  // predicted positions (loop.ts:388-394).
+  void contact_stabilize() {
+    for (const Contact& c : contacts) {
+      const V3<T> off = p3(pos, c.i) - p3(pos, c.j);
+      const T d = length(off);
+      const T wi = invMass[c.i], wj = invMass[c.j], ws = wi + wj;
+      if (d <= static_cast<T>(1e-8) || d >= cDist || ws <= 0) continue;
+      const V3<T> n = off / d;
+      const T dl = (cDist - d) / ws;
+      accPos.add(c.i, n * (wi * dl));
+      accPos.add(c.j, neg(n * (wj * dl)));
+    }
+    for (uint32_t i = 0; i < cap; ++i) {
+      const V3<T> ch = accPos.take(i, &accPos.flag);
+      set3(pos, i, p3(pos, i) + ch, pos[4 * i + 3]);
+      set3(pred, i, p3(pred, i) + ch, pred[4 * i + 3]);
+    }
+  }
+
+  // solve.ts:34-104: non-penetration and static friction, scattered.
+  void contact_solve() {
+    const T inv = static_cast<T>(1) / static_cast<T>(1048576);
+    for (Contact& c : contacts) {
+      const V3<T> xi = p3(pred, c.i), xj = p3(pred, c.j);
+      const V3<T> off = xi - xj;
+      const T d = length(off);
+      const T wi = invMass[c.i], wj = invMass[c.j], ws = wi + wj;
+      if (d <= static_cast<T>(1e-8) || d >= cDist || ws <= 0) continue;
+      const V3<T> n = off / d;
+      const T dln = (cDist - d) / ws;
+      c.ln = wrap_add(c.ln, lam_ticks(dln));
+      c.n = n;
+      const V3<T> slip = (xi - p3(pos, c.i)) - (xj - p3(pos, c.j));
+      const V3<T> tang = slip - n * dot(slip, n);
+      const T tl = length(tang);
+      const T ln = static_cast<T>(c.ln) * inv, lt = static_cast<T>(c.lt) * inv;
+      const T dlt = tl / ws;
+      const bool sticks = tl > static_cast<T>(1e-10) && dlt <= cMuS * ln - lt;
+      const V3<T> ni = n * (wi * dln), nj = neg(n * (wj * dln));
+      accPos.add(c.i, sticks ? ni + neg(tang * (wi / ws)) : ni);
+      accPos.add(c.j, sticks ? nj + tang * (wj / ws) : nj);
+      c.lt = wrap_add(c.lt, lam_ticks(sticks ? dlt : static_cast<T>(0)));
+    }
+  }
+
+  // solve.ts:158-189: kinetic friction on the velocities, scattered.
+  void contact_friction() {
+    const T inv = static_cast<T>(1) / static_cast<T>(1048576);
+    for (const Contact& c : contacts) {
+      const T wi = invMass[c.i], wj = invMass[c.j], ws = wi + wj;
+      const T ln = static_cast<T>(c.ln) * inv;
+      if (ws <= 0 || ln <= 0) continue;
+      const V3<T> n = c.n;
+      const V3<T> v = p3(vel, c.i) - p3(vel, c.j);
+      const V3<T> vt = v - n * dot(n, v);
+      const T vtl = length(vt);
+      if (vtl < static_cast<T>(1e-6)) continue;
+      const T change = tmin(cMuK * ln * ws / dt, vtl);
+      const V3<T> imp = neg((vt / vtl) * change) / ws;
+      accVel.add(c.i, imp * wi);
+      accVel.add(c.j, neg(imp * wj));
+    }
+  }
+
   // --------------------------------------------------------- the loop ----
   void frame_start() {
-    if (hasColliders) {
+    if (hasAcc()) {
       accPos.flag = 0;
       accVel.flag = 0;
-      clock = dt * (uSubsteps - static_cast<T>(1));
     }
+    if (hasColliders) clock = dt * (uSubsteps - static_cast<T>(1));
   }
 
   void substep() {
@@ -1527,8 +1637,12 @@ struct Engine {
     for (auto& sb : softs)
       if (sb.local) rotation_predict(sb);
     // preSolve
-    if (hasColliders) accPos.reset();
+    if (hasAcc()) accPos.reset();
     if (hasGrid) rebuild_grid(pred);
+    if (hasContact) {
+      contact_generate();
+      contact_stabilize();
+    }
     if (hasColliders) {
       std::fill(primLambda.begin(), primLambda.end(), static_cast<T>(0));
       std::fill(sdfLambda.begin(), sdfLambda.end(), static_cast<T>(0));
@@ -1599,9 +1713,12 @@ struct Engine {
           cloth_solve(cloths[m.second]);
         }
       }
-      if (hasColliders) {
-        collider_solve();
-        sdf_solve();
+      if (hasAcc()) {
+        if (hasContact) contact_solve();
+        if (hasColliders) {
+          collider_solve();
+          sdf_solve();
+        }
         apply_acc(accPos, pred, 0, cap);
       }
     }
@@ -1620,13 +1737,16 @@ struct Engine {
         cloth_damping(cloths[m.second]);
       }
     }
-    if (hasColliders) {
+    if (hasAcc()) {
       accVel.reset();
-      collider_friction();
-      sdf_friction();
+      if (hasContact) contact_friction();
+      if (hasColliders) {
+        collider_friction();
+        sdf_friction();
+      }
       apply_acc(accVel, vel, 0, cap);
-      clock = tmax(clock - dt, static_cast<T>(0));
     }
+    if (hasColliders) clock = tmax(clock - dt, static_cast<T>(0));
   }
 
   void init_pass() {
@@ -1934,6 +2054,7 @@ int or_add_softbodies(void* h, const pf_softbody_desc* d, uint32_t* mat) {
     }
     Softbodies<T> sb;
     sb.local = d->shape_matching == PF_SHAPE_MATCH_LOCAL;
+    sb.selfCollision = d->self_collision != 0;
     sb.restOffsets.assign(4 * static_cast<size_t>(e.cap), 0.0f);
     sb.weights.assign(e.cap, 0.0f);
     sb.bodyCompliance.assign(d->n_bodies, 0.0f);
@@ -2267,9 +2388,45 @@ int or_loop_build(void* h, const pf_loop_desc* d, uint32_t table_size) {
     e.gy = static_cast<T>(d->gravity[1]);
     e.gz = static_cast<T>(d->gravity[2]);
     e.uSubsteps = static_cast<T>(e.substeps);
-    double nr = 0;
+    // loop.ts:148-160: one grid, cells sized for the widest query
+    e.hasContact = d->contact != 0;
+    double nr = e.hasContact ? 2.0 * e.radius * 1.1 : 0.0;
     for (auto& f : e.fluids) nr = std::max(nr, f.h);
     e.hasGrid = nr > 0;
+    if (e.hasContact) {
+      const double cr = 2.0 * e.radius * 1.1;
+      e.cMuS = static_cast<T>(d->contact_mu_s >= 0 ? d->contact_mu_s : 0.5f);
+      e.cMuK = static_cast<T>(d->contact_mu_k >= 0 ? d->contact_mu_k : 0.4f);
+      e.cDist = static_cast<T>(static_cast<float>(2.0 * e.radius));
+      e.cCand2 = static_cast<T>(static_cast<float>(cr * cr));
+      e.maxContacts = d->max_contacts ? d->max_contacts : static_cast<uint32_t>(8ull * e.cap);
+      e.quiet.assign(e.cap, 0);
+      for (auto& f : e.fluids)
+        for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) e.quiet[i] = 1;
+      for (auto& q : e.quietRanges)
+        for (uint32_t i = q.start; i < q.start + q.count; ++i) e.quiet[i] = 1;
+    }
+    // loop.ts:163-166, SoftbodySystem.ts:218-234: collision groups for the
+    // soft bodies that have none, above every uploaded group
+    {
+      uint32_t next = 1;
+      for (uint32_t g : e.group) next = std::max(next, g + 1);
+      for (auto& m : e.materials) {
+        if (m.first != MAT_SOFT || e.softs[m.second].selfCollision) continue;
+        for (auto& b : e.softs[m.second].bodies) {
+          const uint32_t g0 = e.group[b.range.start];
+          bool shared = true;
+          for (uint32_t i = b.range.start; i < b.range.start + b.range.count; ++i) shared = shared && e.group[i] == g0;
+          if (shared && g0 != 0) continue;
+          if (!shared) {
+            rc = fail(PF_ERR_INVALID, "SoftbodySystem: a body has mixed collision groups");
+            return;
+          }
+          for (uint32_t i = b.range.start; i < b.range.start + b.range.count; ++i) e.group[i] = next;
+          ++next;
+        }
+      }
+    }
     if (e.hasGrid) {
       e.grid.key_kind = PF_KEY_MORTON;
       for (int c = 0; c < 3; ++c) e.grid.origin[c] = d->hash_origin[c];
@@ -2278,9 +2435,11 @@ int or_loop_build(void* h, const pf_loop_desc* d, uint32_t table_size) {
                                      : std::min<uint32_t>(next_pow2(2ull * e.cap), 1u << 20);
     }
     e.hasColliders = !e.prims.empty() || !e.sdfs.empty();
-    if (e.hasColliders) {
+    if (e.hasAcc()) {
       e.accPos.init(e.cap, 10.0);
       e.accVel.init(e.cap, 50.0);
+    }
+    if (e.hasColliders) {
       e.primCap = static_cast<uint32_t>(e.prims.size());
       e.primLambda.assign(2 * static_cast<size_t>(e.cap) * e.primCap, 0);
       e.sdfLambda.assign(2 * static_cast<size_t>(e.cap) * e.sdfs.size(), 0);
@@ -2396,6 +2555,42 @@ int or_readback(void* h, uint32_t field, void* dst, size_t bytes, int as_f64) {
   return rc;
 }
 
+int or_add_no_self_contacts(void* h, pf_range r) {
+  Scene* s = static_cast<Scene*>(h);
+  int rc = PF_OK;
+  s->visit([&](auto& e) {
+    if (!range_ok(e.cap, r)) {
+      rc = fail(PF_ERR_INVALID, "Material: invalid noSelfContacts range");
+      return;
+    }
+    e.quietRanges.push_back({r.start, r.count});
+  });
+  return rc;
+}
+
+// The last substep's pairs (particle indices, each pair ascending, sorted)
+// and its pair count including dropped ones.
+int or_contacts_read(void* h, uint32_t* pairs, uint32_t capacity, uint32_t* count, uint32_t* stored) {
+  Scene* s = static_cast<Scene*>(h);
+  int rc = PF_OK;
+  s->visit([&](auto& e) {
+    if (!e.hasContact) {
+      rc = fail(PF_ERR_STATE, "contacts: the SimLoop was built without contact");
+      return;
+    }
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    for (auto& c : e.contacts) out.push_back({std::min(c.i, c.j), std::max(c.i, c.j)});
+    std::sort(out.begin(), out.end());
+    if (count) *count = e.contactCount;
+    if (stored) *stored = static_cast<uint32_t>(out.size());
+    for (size_t q = 0; pairs && q < out.size() && q < capacity; ++q) {
+      pairs[2 * q] = out[q].first;
+      pairs[2 * q + 1] = out[q].second;
+    }
+  });
+  return rc;
+}
+
 int or_overflow_read(void* h, pf_overflow* o) {
   Scene* s = static_cast<Scene*>(h);
   s->visit([&](auto& e) {
@@ -2403,6 +2598,7 @@ int or_overflow_read(void* h, pf_overflow* o) {
     o->positions = e.accPos.flag;
     o->velocities = e.accVel.flag;
     o->grid = e.gridOverflow;
+    o->contacts = e.hasContact && e.contactCount > e.maxContacts;
     for (auto& f : e.fluids) o->neighbors |= f.nbrOverflow;
   });
   return PF_OK;

@@ -347,3 +347,60 @@ def wind_deflection_angle(pos4: np.ndarray, inv_mass: np.ndarray, top: list) -> 
     dy = float(np.mean(pos4[free, 1])) - py
     dz = float(np.mean(pos4[free, 2])) - pz
     return math.atan2(dz, abs(dy)), dy, dz
+
+
+def particles(pos, radius: float, substeps: int, iterations: int, gravity=(0.0, -G, 0.0), vel=None,
+              inv_mass=None, group=None, contact=None, prims=(), quiet=(), name: str = "particles") -> R.Recipe:
+    """new ParticleSystem(capacity, r) + uploadParticles + SimLoop({substeps,
+    iterations, gravity, contact: {maxContacts, muS, muK}, colliders}) of the
+    contact tests (tests/analytical/contact/*.gpu.test.ts). `contact` is
+    (max_contacts, mu_s, mu_k) or None; `quiet` lists noSelfContacts ranges
+    of materials with no other kernels."""
+    p = np.asarray(pos, np.float32).reshape(-1, 3)
+    n = len(p)
+    up = R.Upload(0, p, None if vel is None else np.asarray(vel, np.float32).reshape(-1, 3),
+                  None if inv_mass is None else np.asarray(inv_mass, np.float32),
+                  None if group is None else np.asarray(group, np.uint32))
+    loop = R.LoopOpts(substeps=substeps, iterations=iterations, gravity=tuple(gravity))
+    if contact is not None:
+        loop.contact = True
+        loop.max_contacts, loop.contact_mu_s, loop.contact_mu_k = contact
+    return R.Recipe(capacity=n, radius=radius, uploads=[up], prims=list(prims), loop=loop, quiet=list(quiet),
+                    name=name)
+
+
+def lattice(side: int, spacing: float, origin=(0.0, 0.0, 0.0), centred_xz: bool = True) -> np.ndarray:
+    """side^3 points, x outermost then y then z (the tests' ix, iy, iz loops)."""
+    c = (side - 1) / 2 if centred_xz else 0.0
+    pts = [((ix - c) * spacing + origin[0], iy * spacing + origin[1], (iz - c) * spacing + origin[2])
+           for ix in range(side) for iy in range(side) for iz in range(side)]
+    return np.array(pts, np.float64)
+
+
+def column_on_slab(r: float = 0.025, columns: int = 200, slab: int = 60):
+    """contact-generate-emitters.gpu.test.ts:35-76: a column of particles in
+    collision group 1 resting on a pinned slab in group 2. Returns
+    (positions, inverse masses, groups)."""
+    sp = 2 * r
+    side = math.ceil(columns ** (1 / 3))
+    pos, w, g = [], [], []
+    for i in range(columns):
+        x, y, z = i % side, (i // side) % side, i // (side * side)
+        pos.append((-side * sp * 0.5 + (x + 0.5) * sp, (y + 0.5) * sp, -side * sp * 0.5 + (z + 0.5) * sp))
+        w.append(1.0)
+        g.append(1)
+    ss = math.ceil(math.sqrt(slab))
+    for i in range(slab):
+        x, z = i % ss, i // ss
+        pos.append((-ss * sp * 0.5 + (x + 0.5) * sp, -sp * 0.5, -ss * sp * 0.5 + (z + 0.5) * sp))
+        w.append(0.0)
+        g.append(2)
+    return np.array(pos), np.array(w, np.float32), np.array(g, np.uint32)
+
+
+def pair_overlap(pos4: np.ndarray, two_r: float) -> float:
+    """Largest 2r - |x_a - x_b| over all pairs (contact-non-interpenetration)."""
+    p = pos4[:, :3].astype(np.float64)
+    d = np.linalg.norm(p[:, None, :] - p[None, :, :], axis=-1)
+    iu = np.triu_indices(len(p), 1)
+    return float((two_r - d[iu]).max())

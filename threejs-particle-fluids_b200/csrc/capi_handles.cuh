@@ -23,4 +23,7 @@ namespace pf {
 // Host copy of a scene's state fields (positions, velocities, inverse mass,
 // boundary volume, rotation, angular velocity) in the layout of pf_readback.
 pf_status spec_readback(const SceneSpec& spec, uint32_t field, void* dst, size_t bytes);
+// Collision groups handed out when a scene's SimLoop is built (loop.ts:163-166,
+// SoftbodySystem.ts:218-234).
+pf_status allocate_collision_groups(SceneSpec& spec);
 }  // namespace pf

@@ -266,6 +266,7 @@ pf_status pf_add_softbodies(pf_scene* s, const pf_softbody_desc* d, uint32_t* ma
   SceneSpec& sp = s->spec;
   SoftSpec ss;
   ss.local = d->shape_matching == PF_SHAPE_MATCH_LOCAL;
+  ss.self_collision = d->self_collision != 0;
   ss.rest4.assign(4ull * sp.cap, 0.0f);
   ss.weights.assign(sp.cap, 0.0f);
   std::vector<uint8_t> used(sp.cap, 0);
@@ -767,10 +768,31 @@ pf_status pf_set_sdf_transform(pf_scene* s, uint32_t slot, const float position[
   return PF_OK;
 }
 
+pf_status pf_add_no_self_contacts(pf_scene* s, pf_range r) {
+  PF_TRY(not_built(s, "Material"));
+  if (!range_ok(s->spec, {r.start, r.count}))
+    return fail(PF_ERR_INVALID, "Material: invalid noSelfContacts range start=" + std::to_string(r.start) +
+                                    " count=" + std::to_string(r.count));
+  s->spec.quiet.push_back({r.start, r.count});
+  return PF_OK;
+}
+
+pf_status pf_contacts_read(pf_scene* s, uint32_t* pairs, uint32_t capacity, uint32_t* count, uint32_t* stored) {
+  if (!s) return fail(PF_ERR_INVALID, "contacts: scene is NULL");
+  if (!s->world) return fail(PF_ERR_STATE, "contacts: build the SimLoop first");
+  return s->world->contacts(0, pairs, capacity, count, stored);
+}
+
 pf_status pf_loop_build(pf_scene* s, const pf_loop_desc* d) {
   PF_TRY(not_built(s, "SimLoop"));
   if (!d) return fail(PF_ERR_INVALID, "SimLoop: options are NULL");
   if (d->substeps < 1) return fail(PF_ERR_INVALID, "SimLoop: substeps must be an integer >= 1, got 0");
+  if (d->contact) {
+    const float ms = d->contact_mu_s >= 0 ? d->contact_mu_s : 0.5f, mk = d->contact_mu_k >= 0 ? d->contact_mu_k : 0.4f;
+    if (!std::isfinite(ms) || !std::isfinite(mk))
+      return fail(PF_ERR_INVALID, "SimLoop: friction coefficients must be non-negative");
+  }
+  PF_TRY(allocate_collision_groups(s->spec));
   s->spec.loop = *d;
   s->spec.built = true;
   auto w = std::make_unique<World>();
@@ -826,6 +848,33 @@ pf_status pf_readback(pf_scene* s, uint32_t field, void* dst, size_t bytes) {
 }
 
 }  // extern "C"
+
+// loop.ts:163-166 with SoftbodySystem.ts:218-234: collision groups above
+// every uploaded one, one per soft body that has none of its own, in
+// material then body order (unless the system collides with itself).
+pf_status pf::allocate_collision_groups(SceneSpec& sp) {
+  uint32_t next = 1;
+  for (uint32_t g : sp.group) next = std::max(next, g + 1);
+  for (auto& m : sp.materials) {
+    if (m.first != MAT_SOFT) continue;
+    const SoftSpec& ss = sp.softs[m.second];
+    if (ss.self_collision) continue;
+    for (size_t b = 0; b < ss.bodies.size(); ++b) {
+      const RangeU r = ss.bodies[b].range;
+      if (!r.count) continue;
+      const uint32_t g0 = sp.group[r.start];
+      bool shared = true;
+      for (uint32_t i = r.start; i < r.start + r.count; ++i) shared = shared && sp.group[i] == g0;
+      if (shared && g0 != 0) continue;
+      if (!shared)
+        return fail(PF_ERR_INVALID, "SoftbodySystem: body " + std::to_string(b) +
+                                        " has mixed collision groups; give all its particles one group, or none");
+      for (uint32_t i = r.start; i < r.start + r.count; ++i) sp.group[i] = next;
+      ++next;
+    }
+  }
+  return PF_OK;
+}
 
 pf_status pf::spec_readback(const SceneSpec& sp, uint32_t field, void* dst, size_t bytes) {
   auto copy = [&](const void* src, size_t b) -> pf_status {

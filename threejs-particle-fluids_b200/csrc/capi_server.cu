@@ -340,6 +340,7 @@ pf_status pf_server_submit(pf_server* S, pf_scene* scene, const pf_loop_desc* lo
     if (loop->substeps < 1) return fail(PF_ERR_INVALID, "SimLoop: substeps must be an integer >= 1, got 0");
     r->spec->loop = *loop;
   }
+  if (!scene->world) PF_TRY(allocate_collision_groups(*r->spec));
   r->spec->built = true;
   PF_TRY(plan_bytes(r->spec.get(), &r->est_bytes));
   if (r->est_bytes > S->opts.hbm_budget_bytes)

@@ -21,6 +21,7 @@
 #include "world_kernels.cuh"
 #include "world_slots.cuh"
 #include "world_tiles.cuh"
+#include "world_contacts.cuh"
 
 namespace pf {
 
@@ -191,18 +192,21 @@ __device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, P
 
 // The colliders of particle k's scene against its predicted position xs4
 // (w = inverse mass), their multipliers updated; the fixed-point position
-// changes summed in registers and applied. Returns whether xs4 changed.
+// changes summed in registers, on top of the ticks `start` that particle
+// contacts scattered for k, and applied. Returns whether xs4 changed.
 __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevScene& S, uint32_t s, uint32_t k,
-                                                 float4& xs4, const pf_primitive* __restrict__ prims) {
+                                                 float4& xs4, const pf_primitive* __restrict__ prims,
+                                                 int4 start = make_int4(0, 0, 0, 0)) {
   const float w = xs4.w;
-  if (!(w > 0.0f)) return false;
+  const bool moves = w > 0.0f;
+  const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
   const f3 xstar = xyz(xs4);
   const f3 disp = xstar - xyz(V.cur.x[k]);
   const float clock = V.clocks[s];
   const float radius = S.radius;
-  uint32_t tx = 0, ty = 0, tz = 0;
-  bool any = false;
-  for (uint32_t p = 0; p < S.prim_count; ++p) {
+  uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
+  bool any = (start.x | start.y | start.z) != 0;
+  for (uint32_t p = 0; p < n_prim; ++p) {
     const pf_primitive& P = prims[p];
     float phi;
     f3 nrm;
@@ -227,7 +231,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     any = true;
   }
   // SDFCollider.ts:256-281: static surface, reach = radius + thickness
-  for (uint32_t q = 0; q < S.sdf_count; ++q) {
+  for (uint32_t q = 0; q < n_sdf; ++q) {
     const DevSdf& G = V.sdfs[S.sdf_base + q];
     float phi;
     f3 g;
@@ -343,9 +347,15 @@ __global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, u
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
-  if (S.prim_count + S.sdf_count == 0 || S.collide_rank1 || sub >= S.substeps || it >= S.iterations) return;
+  if ((S.prim_count + S.sdf_count == 0 && !S.contact) || S.collide_rank1 || sub >= S.substeps || it >= S.iterations)
+    return;
   float4 xs4 = V.cur.xs[k];
-  if (collide_particle(V, S, s, k, xs4, prims)) V.cur.xs[k] = xs4;
+  int4 start = make_int4(0, 0, 0, 0);
+  if (S.contact) {
+    start = V.acc_con[k];
+    if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
+  }
+  if (collide_particle(V, S, s, k, xs4, prims, start)) V.cur.xs[k] = xs4;
 }
 
 // PrimitiveSet.ts:367-398 with collider.ts:96-118, fused with the velocity
@@ -357,16 +367,23 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   if (k >= V.n) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
-  if (S.prim_count + S.sdf_count == 0 || sub >= S.substeps) return;
+  if ((S.prim_count + S.sdf_count == 0 && !S.contact) || sub >= S.substeps) return;
   const float4 xs4 = V.cur.xs[k];
   const float w = xs4.w;
-  if (!(w > 0.0f)) return;
+  // contact friction (k_con_friction) scattered its velocity ticks first
+  int4 start = make_int4(0, 0, 0, 0);
+  if (S.contact) {
+    start = V.acc_con[k];
+    if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
+  }
+  const bool moves = w > 0.0f;
+  const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
   const f3 xstar = xyz(xs4);
   const f3 vel = xyz(V.cur.v[k]);
   const float clock = V.clocks[s];
-  uint32_t tx = 0, ty = 0, tz = 0;
-  bool any = false;
-  for (uint32_t p = 0; p < S.prim_count; ++p) {
+  uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
+  bool any = (start.x | start.y | start.z) != 0;
+  for (uint32_t p = 0; p < n_prim; ++p) {
     const float ln = V.plam[(size_t)k * V.prim_stride + p].x;
     if (!(ln > 0.0f)) continue;
     const pf_primitive& P = prims[p];
@@ -389,7 +406,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
     }
   }
   // SDFCollider.ts:283-299 against a static surface
-  for (uint32_t q = 0; q < S.sdf_count; ++q) {
+  for (uint32_t q = 0; q < n_sdf; ++q) {
     const float ln = V.plam[(size_t)k * V.prim_stride + S.prim_count + q].x;
     if (!(ln > 0.0f)) continue;
     const DevSdf& G = V.sdfs[S.sdf_base + q];
@@ -1102,8 +1119,19 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     max_sub_ = std::max(max_sub_, S.substeps);
     max_iter_ = std::max(max_iter_, S.iterations);
     max_rank_ = std::max(max_rank_, (uint32_t)sp.materials.size());
-    // grid
-    double h = 0;
+    // particle contacts (loop.ts:148-160, 388-417)
+    S.contact = sp.loop.contact ? 1u : 0u;
+    S.max_contacts = sp.loop.max_contacts ? sp.loop.max_contacts : (uint32_t)std::min<uint64_t>(8ull * sp.cap, 0xffffffffull);
+    S.c_mus = sp.loop.contact_mu_s >= 0 ? sp.loop.contact_mu_s : 0.5f;
+    S.c_muk = sp.loop.contact_mu_k >= 0 ? sp.loop.contact_mu_k : 0.4f;
+    S.c_dist = f32(2.0 * sp.radius);
+    {
+      const double cr = 2.0 * sp.radius * kContactRadiusExpansion;
+      S.c_cand2 = f32(cr * cr);
+    }
+    any_contact_ = any_contact_ || S.contact;
+    // grid: one grid for every neighbour query, sized for the widest
+    double h = S.contact ? 2.0 * sp.radius * kContactRadiusExpansion : 0.0;
     for (auto& f : sp.fluids) h = std::max(h, f.h);
     S.has_grid = h > 0;
     if (S.has_grid) {
@@ -1271,8 +1299,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     any_prims_ = any_prims_ || S.prim_count > 0 || S.sdf_count > 0;
     // colliders fuse into the last material's pass when that is a fluid
     S.collide_rank1 = 0;
-    if (S.prim_count + S.sdf_count > 0) {
-      if (!sp.materials.empty() && sp.materials.back().first == MAT_FLUID)
+    if (S.prim_count + S.sdf_count > 0 || S.contact) {
+      // contact pairs are solved after every material and before the
+      // colliders, so a scene with contacts keeps its collider pass apart
+      if (!S.contact && !sp.materials.empty() && sp.materials.back().first == MAT_FLUID)
         S.collide_rank1 = (uint32_t)sp.materials.size();
       else
         any_unfused_prims_ = true;
@@ -1290,7 +1320,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         cloth_only = cloth_only && m.first == MAT_CLOTH;
         has_cloth = has_cloth || m.first == MAT_CLOTH;
       }
-      const bool unfused = h_scenes_[s].prim_count + h_scenes_[s].sdf_count > 0 && h_scenes_[s].collide_rank1 == 0;
+      const bool unfused = (h_scenes_[s].prim_count + h_scenes_[s].sdf_count > 0 || h_scenes_[s].contact) &&
+                           h_scenes_[s].collide_rank1 == 0;
       if (has_cloth || unfused) {
         ok = ok && cloth_only;
         any_side = true;
@@ -1649,6 +1680,20 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.d_smooth = cv.take<float4>(dvtx.size());
     cloth_par_dev_ = cv.take<DevCloth>(h_cloth_par_.size());
     base_.cloth_par = cloth_par_dev_;
+    // particle contacts
+    const size_t CH = N / kSegAlign;
+    base_.cgroup = any_contact_ ? cv.take<uint32_t>(N) : nullptr;
+    base_.cquiet = any_contact_ ? cv.take<uint8_t>(N) : nullptr;
+    base_.con_nbr = any_contact_ ? cv.take<uint32_t>(kMaxContacts * N) : nullptr;
+    base_.con_cnt = any_contact_ ? cv.take<uint32_t>(N) : nullptr;
+    base_.con_pre = any_contact_ ? cv.take<uint32_t>(N) : nullptr;
+    base_.chunk_sum = any_contact_ ? cv.take<uint32_t>(CH) : nullptr;
+    base_.chunk_drop = any_contact_ ? cv.take<uint32_t>(CH) : nullptr;
+    base_.chunk_off = any_contact_ ? cv.take<uint32_t>(CH) : nullptr;
+    base_.con_lam = any_contact_ ? cv.take<int2>(kMaxContacts * N) : nullptr;
+    base_.con_nrm = any_contact_ ? cv.take<float4>(kMaxContacts * N) : nullptr;
+    base_.acc_con = any_contact_ ? cv.take<int4>(N) : nullptr;
+    base_.con_stat = any_contact_ ? cv.take<uint2>(K) : nullptr;
     stage_pos_ = cv.take<float4>(total_real);
     prefix_dev_ = cv.take<uint64_t>(K);
   };
@@ -1784,6 +1829,28 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_TRY(up(base_.d_off, doff.data(), 4 * doff.size()));
   PF_TRY(up(base_.d_nbr, dnbr.data(), 4 * dnbr.size()));
   PF_TRY(up(cloth_par_dev_, h_cloth_par_.data(), sizeof(DevCloth) * h_cloth_par_.size()));
+  if (any_contact_) {
+    // collision groups and noSelfContacts membership by id
+    std::vector<uint32_t> cg(n_, 0);
+    std::vector<uint8_t> cq(n_, 1);
+    for (uint32_t s = 0; s < K; ++s) {
+      const SceneSpec& sp = *specs[s];
+      const uint32_t base = h_scenes_[s].seg_start;
+      for (uint32_t i = 0; i < sp.cap; ++i) {
+        cg[base + i] = sp.group[i];
+        cq[base + i] = 0;
+      }
+      for (auto& f : sp.fluids)
+        for (uint32_t i = f.range.start; i < f.range.start + f.range.count; ++i) cq[base + i] = 1;
+      for (auto& q : sp.quiet)
+        for (uint32_t i = q.start; i < q.start + q.count; ++i) cq[base + i] = 1;
+    }
+    PF_TRY(up(base_.cgroup, cg.data(), 4ull * n_));
+    PF_TRY(up(base_.cquiet, cq.data(), n_));
+    PF_CUDA(cudaMemsetAsync(base_.acc_con, 0, 16ull * n_, stream_));
+    PF_CUDA(cudaMemsetAsync(base_.con_cnt, 0, 4ull * n_, stream_));
+    PF_CUDA(cudaMemsetAsync(base_.con_stat, 0, 8ull * K, stream_));
+  }
   PF_TRY(up(base_.b_scene, bsc.data(), 4 * bsc.size()));
   PF_TRY(up(prefix_dev_, prefix_.data(), 8 * prefix_.size()));
   PF_TRY(up(base_.row_base, row_base.data(), 4 * row_base.size()));
@@ -2049,7 +2116,15 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   } else {
     launch_slots(k_reset_sums, n_, stream_, V);
   }
-  // preSolve
+  // preSolve: contacts first (loop.ts:196-223), then the materials'
+  if (any_contact_) {
+    const uint32_t K = (uint32_t)h_scenes_.size();
+    k_con_gen<<<n_ / kBlock, kBlock, 0, stream_>>>(V, s);
+    k_con_scan<<<K, 1024, 0, stream_>>>(V, s);
+    launch_slots(k_con_stab, n_, stream_, V, s);
+    launch_slots(k_con_apply2, n_, stream_, V, s);
+    t_launches += 2;
+  }
   launch_aero(V, 0, s);
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
   if (any_fluid_) run_fluid_neighbors(V, s);
@@ -2083,6 +2158,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     cudaStreamWaitEvent(side_stream_, ev_fork_, 0);
     for (uint32_t it = 0; it < max_iter_; ++it) {
       for (uint32_t r = 0; r < cloth_ranges_.size(); ++r) launch_cloth_rank(V, r, s, it, side_stream_);
+      if (any_contact_) launch_slots(k_con_solve, n_, side_stream_, V, s, it);
       if (any_unfused_prims_) launch_slots(k_collide, n_, side_stream_, V, s, it);
     }
   }
@@ -2112,6 +2188,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       }
       if (!fork && r < cloth_ranges_.size()) launch_cloth_rank(V, r, s, it, stream_);
     }
+    if (!fork && any_contact_) launch_slots(k_con_solve, n_, stream_, V, s, it);
     if (!fork && any_unfused_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
   }
   if (fork) {
@@ -2146,8 +2223,11 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       t_launches += 2;
     }
   }
+  // friction: the velocity sums reset, contact friction, collider friction,
+  // applied (loop.ts:226-230)
+  if (any_contact_) launch_slots(k_con_friction, n_, stream_, V, s);
+  if (any_prims_ || any_contact_) launch_slots(k_friction, n_, stream_, V, s);
   if (any_prims_) {
-    launch_slots(k_friction, n_, stream_, V, s);
     const uint32_t K = (uint32_t)h_scenes_.size();
     k_tick<<<div_up(K, 128), 128, 0, stream_>>>(V, K, s);
     ++t_launches;
@@ -2446,8 +2526,51 @@ pf_status World::overflow(uint32_t scene, pf_overflow* out) {
   out->velocities = f[FLAG_VEL];
   out->grid = f[FLAG_GRID];
   out->contacts = f[FLAG_CONTACTS];
+  if (h_scenes_[scene].contact) {
+    // loop.ts:290-301: the last substep's pair count against maxContacts
+    uint2 st;
+    PF_CUDA(cudaMemcpy(&st, base_.con_stat + scene, sizeof(uint2), cudaMemcpyDeviceToHost));
+    out->contacts |= (st.x > h_scenes_[scene].max_contacts || st.y > 0) ? 1u : 0u;
+  }
   out->neighbors = f[FLAG_NBR];
   out->device_error = err | f[FLAG_DEVICE];
+  return PF_OK;
+}
+
+// ContactBuffer.readbackCount / readbackPairs for one scene: the pairs of
+// the last substep as particle indices, each pair ascending, sorted.
+pf_status World::contacts(uint32_t scene, uint32_t* pairs, uint32_t capacity, uint32_t* count, uint32_t* stored) {
+  if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "contacts: no such scene");
+  const DevScene& S = h_scenes_[scene];
+  if (!S.contact) return fail(PF_ERR_STATE, "contacts: the SimLoop was built without contact");
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  const uint32_t seg = S.seg_end - S.seg_start;
+  uint2 st;
+  PF_CUDA(cudaMemcpy(&st, base_.con_stat + scene, sizeof(uint2), cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> ids(seg), cnt(seg), pre(seg), off(seg / kSegAlign), nb((size_t)kMaxContacts * seg);
+  PF_CUDA(cudaMemcpy(ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+  PF_CUDA(cudaMemcpy(cnt.data(), base_.con_cnt + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+  PF_CUDA(cudaMemcpy(pre.data(), base_.con_pre + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+  PF_CUDA(cudaMemcpy(off.data(), base_.chunk_off + S.seg_start / kSegAlign, 4ull * off.size(), cudaMemcpyDeviceToHost));
+  for (uint32_t m = 0; m < kMaxContacts; ++m)
+    PF_CUDA(cudaMemcpy(nb.data() + (size_t)m * seg, base_.con_nbr + (size_t)m * n_ + S.seg_start, 4ull * seg,
+                       cudaMemcpyDeviceToHost));
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  for (uint32_t k = 0; k < seg; ++k) {
+    const uint32_t c = std::min(cnt[k], kMaxContacts);
+    const uint32_t first = off[k / kSegAlign] + pre[k];
+    for (uint32_t m = 0; m < c && first + m < S.max_contacts; ++m) {
+      const uint32_t a = ids[k] - S.seg_start, b = ids[nb[(size_t)m * seg + k] - S.seg_start] - S.seg_start;
+      out.push_back({std::min(a, b), std::max(a, b)});
+    }
+  }
+  std::sort(out.begin(), out.end());
+  if (count) *count = st.x;
+  if (stored) *stored = (uint32_t)out.size();
+  for (size_t q = 0; pairs && q < out.size() && q < capacity; ++q) {
+    pairs[2 * q] = out[q].first;
+    pairs[2 * q + 1] = out[q].second;
+  }
   return PF_OK;
 }
 

@@ -33,6 +33,7 @@ namespace pf {
 constexpr uint32_t kSegAlign = 256;
 constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts:14)
 constexpr uint32_t kBlock = 256;
+constexpr uint32_t kMaxContacts = 32;  // contact pairs kept per emitting particle per substep
 
 // ------------------------------------------------------------- host spec ----
 struct RangeU {
@@ -56,6 +57,7 @@ struct BodySpec {
 
 struct SoftSpec {
   bool local = true;
+  bool self_collision = false;
   std::vector<BodySpec> bodies;
   RangeU span;
   std::vector<float> rest4;        // float4 per particle of the scene (cap)
@@ -114,6 +116,7 @@ struct SceneSpec {
   std::vector<ClothSpec> cloths;
   std::vector<pf_primitive> prims;
   std::vector<SdfSpec> sdfs;
+  std::vector<RangeU> quiet;  // pf_add_no_self_contacts ranges (fluids' ranges are implied)
   pf_loop_desc loop{};
   bool built = false;
   bool initialized = false;  // the one-time init pass (static boundaries) ran
@@ -144,6 +147,10 @@ struct DevScene {
   uint32_t init_pending;              // the one-time init pass has not run for this scene
   uint32_t sdf_base, sdf_count;       // this scene's SDF colliders in the SDF table
   uint32_t collide_rank1;             // r + 1: colliders run inside the apply of fluid rank r (its last material)
+  uint32_t contact;                   // particle-particle contacts on
+  uint32_t max_contacts;              // pairs solved per substep (the first in slot order)
+  float c_mus, c_muk;                 // contact friction
+  float c_dist, c_cand2;              // 2r and (2r * 1.1)^2 as f32 literals
 };
 
 // One SDF collider as the kernels read it (sdf.ts:17-80 fields).
@@ -326,6 +333,21 @@ struct WorldView {
   const uint32_t* d_nbr;  // particle ids
   float4* d_smooth;     // blended velocity per record
   const DevCloth* cloth_par;
+  // particle contacts (src/core/contact/): per emitting slot, up to
+  // kMaxContacts partner slots in column-major lists (entry m of slot k at
+  // m * n + k) with their multipliers and last normal
+  const uint32_t* cgroup;   // collision group by id
+  const uint8_t* cquiet;    // 1: inside a noSelfContacts range, by id
+  uint32_t* con_nbr;
+  uint32_t* con_cnt;        // pairs found per slot (uncapped)
+  uint32_t* con_pre;        // exclusive prefix of con_cnt inside the slot's 256-slot chunk
+  uint32_t* chunk_sum;      // per chunk: pairs found, and pairs past the per-slot cap
+  uint32_t* chunk_drop;
+  uint32_t* chunk_off;      // per chunk: first pair index inside its scene
+  int2* con_lam;            // (lambda_n, lambda_t) ticks of 2^-20 kg m
+  float4* con_nrm;
+  int4* acc_con;            // fixed-point position (then velocity) sums per slot
+  uint2* con_stat;          // per scene: pairs found in the last substep, pairs past the per-slot cap
 };
 
 class World {
@@ -359,6 +381,7 @@ class World {
   // Copies the scene's state (by particle index) back into its spec.
   pf_status pull_state(uint32_t scene, SceneSpec* spec);
   pf_status overflow(uint32_t scene, pf_overflow* out);
+  pf_status contacts(uint32_t scene, uint32_t* pairs, uint32_t capacity, uint32_t* count, uint32_t* stored);
   // Device milliseconds between the start and end events of the last step.
   pf_status elapsed_ms(float* ms);
   cudaStream_t stream() const { return stream_; }
@@ -438,6 +461,7 @@ class World {
   bool any_soft_local_ = false, any_soft_global_ = false, any_static_bnd_ = false, any_dyn_bnd_ = false;
   bool any_react_ = false;
   bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass
+  bool any_contact_ = false;        // a scene with particle contacts
   uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
   // device memory: one arena
   void* arena_ = nullptr;

@@ -112,6 +112,7 @@ class SoftbodyDesc(C.Structure):
         ("n_bodies", C.c_uint32),
         ("bodies", C.POINTER(SoftbodyDef)),
         ("shape_matching", C.c_uint32),
+        ("self_collision", C.c_uint32),
     ]
 
 
@@ -201,6 +202,10 @@ class LoopDesc(C.Structure):
         ("hash_origin", C.c_float * 3),
         ("grid_min", C.c_float * 3),
         ("grid_max", C.c_float * 3),
+        ("contact", C.c_uint32),
+        ("contact_mu_s", C.c_float),
+        ("contact_mu_k", C.c_float),
+        ("max_contacts", C.c_uint32),
     ]
 
 
@@ -276,6 +281,8 @@ SIGNATURES = {
     "pf_add_fluid": (C.c_int, [_P, C.POINTER(FluidDesc), _u32p]),
     "pf_add_softbodies": (C.c_int, [_P, C.POINTER(SoftbodyDesc), _u32p]),
     "pf_add_cloth": (C.c_int, [_P, C.POINTER(ClothDesc), _u32p]),
+    "pf_add_no_self_contacts": (C.c_int, [_P, Range]),
+    "pf_contacts_read": (C.c_int, [_P, _u32p, C.c_uint32, _u32p, _u32p]),
     "pf_cloth_get_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
     "pf_cloth_set_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
     "pf_cloth_build_tethers": (C.c_int, [C.POINTER(TetherBuildDesc), _u32p, _u32p, _f32p, C.c_uint32, _u32p]),

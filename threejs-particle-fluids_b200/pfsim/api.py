@@ -110,14 +110,15 @@ class SoftbodySystem:
     """src/softbody/SoftbodySystem.ts:29-199: bodies of {range, surface_count,
     compliance, rest_positions?, edges?}; shape_matching 'local' or 'global'."""
 
-    def __init__(self, particles: ParticleSystem, bodies: list[dict], shape_matching: str = "local"):
+    def __init__(self, particles: ParticleSystem, bodies: list[dict], shape_matching: str = "local",
+                 self_collision: bool = False):
         if shape_matching not in ("local", "global"):
             raise _err("SoftbodySystem", f"shapeMatching must be 'local' or 'global', got {shape_matching}")
         self.particles = particles
         self.opts = R.SoftbodyOpts([R.BodyDef(range=tuple(b["range"]), surface_count=b.get("surface_count"),
                                               compliance=b.get("compliance", 0.0),
                                               rest_positions=b.get("rest_positions"), edges=b.get("edges"))
-                                    for b in bodies], shape_matching)
+                                    for b in bodies], shape_matching, bool(self_collision))
     kind = "soft"
 
 
@@ -296,7 +297,8 @@ class SimLoop:
 
     def __init__(self, particles: ParticleSystem, substeps: int = 4, iterations: int = 2,
                  gravity=(0.0, -9.81, 0.0), materials: Sequence = (), colliders: Sequence = (),
-                 hash_origin=(0.0, 0.0, 0.0), grid_min=(0.0, 0.0, 0.0), grid_max=(0.0, 0.0, 0.0)):
+                 hash_origin=(0.0, 0.0, 0.0), grid_min=(0.0, 0.0, 0.0), grid_max=(0.0, 0.0, 0.0),
+                 contact: bool | dict = False):
         if not (isinstance(substeps, int) and substeps >= 1):
             raise _err("SimLoop", f"substeps must be an integer >= 1, got {substeps}")
         if not (isinstance(iterations, int) and iterations >= 0):
@@ -311,6 +313,16 @@ class SimLoop:
                        loop=R.LoopOpts(substeps=substeps, iterations=iterations, gravity=tuple(gravity),
                                        hash_origin=tuple(hash_origin), grid_min=tuple(grid_min),
                                        grid_max=tuple(grid_max)))
+        if contact:
+            # SimLoopOptions.contact: true or {muS, muK, maxContacts} (loop.ts:20-30)
+            c = contact if isinstance(contact, dict) else {}
+            mus, muk = c.get("mu_s", 0.5), c.get("mu_k", 0.4)
+            if not (mus >= 0) or not (muk >= 0):
+                raise _err("SimLoop", f"friction coefficients must be non-negative (got muS={mus}, muK={muk})")
+            mc = c.get("max_contacts", 8 * particles.capacity)
+            if not (isinstance(mc, int) and mc > 0):
+                raise N.PfError(N.PF_ERR_INVALID, f"ContactBuffer: maxContacts must be a positive integer, got {mc}")
+            rec.loop.contact, rec.loop.contact_mu_s, rec.loop.contact_mu_k, rec.loop.max_contacts = True, mus, muk, mc
         for m in self.materials:
             rec.materials.append((m.kind, m.opts))
         for c in self.colliders:
@@ -342,6 +354,10 @@ class SimLoop:
 
     def readback_overflow(self) -> dict:
         return self.scene.overflow()
+
+    def contacts(self) -> tuple[int, np.ndarray]:
+        """loop.contacts.readbackCount() and readbackPairs() (ContactBuffer.ts:75-97)."""
+        return self.scene.contacts()
 
     def dispose(self) -> None:
         if not self.disposed:
@@ -525,6 +541,14 @@ class Simulation:
             n += len(pos)
         if n == 0:
             raise N.PfError(N.PF_ERR_STATE, "Simulation: nothing to simulate; add a fluid, soft body or cloth")
+        # Simulation.ts:722-737: every fluid treats the soft bodies' surfaces
+        # and the cloths as dynamic boundaries
+        solids = [(b.range[0], b.surface_count) for b in bodies]
+        solids += [(opts[1], len(opts[0].positions)) for kind, opts in mats if kind == "cloth"]
+        for kind, opts in mats:
+            if kind == "fluid":
+                opts.boundaries = list(solids)
+                opts.boundary_static = [False] * len(solids)
         ps = ParticleSystem(n, r)
         for ch in chunks:
             start, pts = ch[0], ch[1]
@@ -533,8 +557,13 @@ class Simulation:
         prims = list(self.prims)
         if self.container is not None:
             prims += R.container_walls(self.container[0], self.container[1], self.closed)
-        substeps = self.substeps or min(24, math.ceil(2 * max(1.0, 0.018 / r)))
+        # Simulation.ts:820-836: substeps from the stiffest material at this
+        # particle size; contacts when soft bodies or cloth are present
+        base = max(4 if self.fluids else 0, 6 if bodies else 0, 8 if self.cloths else 0)
+        substeps = self.substeps or min(24, math.ceil(base * max(1.0, 0.018 / r)))
         rec_loop = dict(substeps=int(substeps), iterations=2, gravity=self.gravity)
+        if bodies or self.cloths:
+            rec_loop["contact"] = {"mu_s": 0.3, "mu_k": 0.2}
         self.particles = ps
         matobjs = []
         self._cloth_systems = []

@@ -28,6 +28,7 @@ class Upload:
     pos: np.ndarray  # (n, 3) or (n, 4) float32
     vel: np.ndarray | None = None
     inv_mass: np.ndarray | None = None
+    group: np.ndarray | None = None  # collision groups (uint32)
 
 
 @dataclass
@@ -62,6 +63,7 @@ class BodyDef:
 class SoftbodyOpts:
     bodies: list[BodyDef]
     shape_matching: str = "global"
+    self_collision: bool = False
 
 
 @dataclass
@@ -205,6 +207,10 @@ class LoopOpts:
     hash_origin: tuple = (0.0, 0.0, 0.0)
     grid_min: tuple = (0.0, 0.0, 0.0)
     grid_max: tuple = (0.0, 0.0, 0.0)
+    contact: bool = False  # SimLoopOptions.contact
+    contact_mu_s: float = -1.0
+    contact_mu_k: float = -1.0
+    max_contacts: int = 0
 
 
 @dataclass
@@ -216,6 +222,7 @@ class Recipe:
     prims: list[Prim] = field(default_factory=list)
     sdfs: list[Sdf] = field(default_factory=list)
     loop: LoopOpts = field(default_factory=LoopOpts)
+    quiet: list = field(default_factory=list)  # noSelfContacts ranges (start, count) of no material
     name: str = ""
     # optional per-step primitive motion: fn(step_index, dt) -> {slot: Prim}
     motion: Any = None
@@ -299,6 +306,7 @@ def softbody_desc(o: SoftbodyOpts, keep: _Keep) -> N.SoftbodyDesc:
     d.n_bodies = len(o.bodies)
     d.bodies = C.cast(defs, C.POINTER(N.SoftbodyDef))
     d.shape_matching = N.PF_SHAPE_MATCH_LOCAL if o.shape_matching == "local" else N.PF_SHAPE_MATCH_GLOBAL
+    d.self_collision = 1 if o.self_collision else 0
     return d
 
 
@@ -343,7 +351,18 @@ def loop_desc(o: LoopOpts) -> N.LoopDesc:
     d.hash_origin[:] = list(o.hash_origin)
     d.grid_min[:] = list(o.grid_min)
     d.grid_max[:] = list(o.grid_max)
+    d.contact = 1 if o.contact else 0
+    d.contact_mu_s, d.contact_mu_k, d.max_contacts = o.contact_mu_s, o.contact_mu_k, o.max_contacts
     return d
+
+
+def read_contacts(fn, handle, capacity: int) -> tuple[int, np.ndarray]:
+    cap = max(1, 32 * capacity)
+    out = np.empty(2 * cap, np.uint32)
+    count, stored = C.c_uint32(0), C.c_uint32(0)
+    N.check(fn(handle, out.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(count), C.byref(stored)))
+    m = min(stored.value, cap)
+    return int(count.value), out[: 2 * m].reshape(-1, 2).copy()
 
 
 # --------------------------------------------------------- native backend ----
@@ -390,6 +409,12 @@ class Scene:
     def set_primitive(self, slot: int, prim: Prim) -> None:
         p = prim.cstruct()
         N.check(N.lib().pf_set_primitive(self.h, slot, C.byref(p)))
+
+    def contacts(self) -> tuple[int, np.ndarray]:
+        """pf_contacts_read: (pairs found in the last substep, dropped ones
+        included; the stored pairs as an (m, 2) array, each pair ascending,
+        sorted)."""
+        return read_contacts(N.lib().pf_contacts_read, self.h, self.capacity)
 
     def write(self, field_id: int, data: np.ndarray) -> None:
         """pf_write: a whole field (positions, predicted, velocities: float4 x
@@ -444,7 +469,8 @@ class NativeBackend:
             p = pos4(u.pos)
             v = None if u.vel is None else keep.f32(pos4(u.vel))
             w = None if u.inv_mass is None else keep.f32(u.inv_mass)
-            N.check(L.pf_upload_particles(h, keep.f32(p), v, w, None, u.start, p.shape[0]))
+            g = None if u.group is None else keep.u32(np.asarray(u.group, np.uint32))
+            N.check(L.pf_upload_particles(h, keep.f32(p), v, w, g, u.start, p.shape[0]))
         for kind, opts in r.materials:
             if kind == "fluid":
                 N.check(L.pf_add_fluid(h, C.byref(fluid_desc(opts, keep)), None))
@@ -454,6 +480,8 @@ class NativeBackend:
                 N.check(L.pf_add_cloth(h, C.byref(cloth_desc(opts, keep)), None))
             else:
                 raise ValueError(kind)
+        for q in r.quiet:
+            N.check(L.pf_add_no_self_contacts(h, N.Range(*q)))
         for p in r.prims:
             cs = p.cstruct()
             N.check(L.pf_add_primitive(h, C.byref(cs), None))
