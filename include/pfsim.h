@@ -484,6 +484,56 @@ PF_API pf_status pf_batch_profile_stage(pf_batch* batch, uint32_t stage, uint32_
 PF_API pf_status pf_batch_tuning(pf_batch* batch, uint32_t* path, uint32_t* block, uint32_t* unroll);
 
 /* ------------------------------------------------------------------------ */
+/* Mesh -> particle setup on the GPU                                          */
+/* ------------------------------------------------------------------------ */
+
+/* A triangle mesh as toTriangleMesh reads a BufferGeometry (src/core/mesh.ts:
+ * 16-56): xyz float vertices and three indices per triangle. */
+typedef struct pf_mesh {
+  const float* vertices;        /* host xyz x n_vertices */
+  uint32_t n_vertices;
+  const uint32_t* indices;      /* host, n_indices entries (a multiple of 3) */
+  uint32_t n_indices;
+} pf_mesh;
+
+/* Output of the voxeliser (VoxelizeResult, voxelize.ts:23-36). `count`,
+ * `surface_count` and `edge_count` are always set; `positions` (xyz x count,
+ * surface particles first) is written when `capacity` >= count, `edges`
+ * (pairs i < j) up to `edge_capacity` pairs, so a first call with NULL
+ * buffers sizes the second. */
+typedef struct pf_voxels {
+  float* positions;
+  uint32_t capacity;
+  uint32_t* edges;
+  uint32_t edge_capacity;
+  uint32_t count, surface_count, edge_count;
+} pf_voxels;
+
+/* voxelize(mesh, {particleRadius, largestPiece}) (src/softbody/voxelize.ts:
+ * 50-161): grid points at spacing 2r over the mesh's box, inside by
+ * ray-cast parity (every point against every triangle on the GPU, in
+ * doubles as the reference computes), then the largest face-connected
+ * piece when asked, surface particles first, face-adjacent pairs. */
+PF_API pf_status pf_voxelize_mesh(const pf_mesh* mesh, double particle_radius, uint32_t largest_piece,
+                                  pf_voxels* out);
+/* voxelize(SDFData, {particleRadius, dilation, largestPiece}): inside where
+ * the trilinear field (sample.ts:12-47) is below `dilation`. `data` is the
+ * float field, x fastest. */
+PF_API pf_status pf_voxelize_sdf(const float* data, const uint32_t res[3], const double origin[3],
+                                 const double voxel_size[3], double particle_radius, double dilation,
+                                 uint32_t largest_piece, pf_voxels* out);
+/* bakeMeshToSdf(mesh, {resolution, padding}) (src/sdf/bake.ts:84-139): a
+ * resolution^3 cubic grid around the mesh (padding < 0 selects two voxels,
+ * one below resolution 8), per voxel centre the distance to the closest
+ * triangle and the sign of the three jittered axis-ray parities' majority,
+ * on the GPU in doubles. `data` receives resolution^3 floats (x fastest),
+ * `origin` and `voxel_size` the grid, `inconsistent` the voxels whose
+ * votes split; more than 1% of them fails as the reference throws (the
+ * field is written first). */
+PF_API pf_status pf_bake_sdf(const pf_mesh* mesh, uint32_t resolution, double padding, float* data,
+                             double origin[3], double* voxel_size, uint64_t* inconsistent);
+
+/* ------------------------------------------------------------------------ */
 /* Serving: continuous batching under an HBM budget                           */
 /* ------------------------------------------------------------------------ */
 

@@ -74,6 +74,11 @@ def _bind(L: C.CDLL) -> None:
         "or_set_primitive": (C.c_int, [P, C.c_uint32, C.POINTER(N.Primitive)]),
         "or_cloth_set_params": (C.c_int, [P, C.c_uint32, C.POINTER(N.ClothParams)]),
         "or_write": (C.c_int, [P, C.c_uint32, f32p, C.c_size_t]),
+        "or_voxelize_mesh": (C.c_int, [C.POINTER(N.Mesh), C.c_double, C.c_uint32, C.POINTER(N.Voxels)]),
+        "or_voxelize_sdf": (C.c_int, [f32p, u32p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                      C.c_double, C.c_uint32, C.POINTER(N.Voxels)]),
+        "or_bake_sdf": (C.c_int, [C.POINTER(N.Mesh), C.c_uint32, C.c_double, f32p, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
         "or_add_no_self_contacts": (C.c_int, [P, N.Range]),
         "or_contacts_read": (C.c_int, [P, u32p, C.c_uint32, u32p, u32p]),
         "or_loop_build": (C.c_int, [P, C.POINTER(N.LoopDesc), C.c_uint32]),
@@ -172,6 +177,45 @@ def color_constraints(pairs: np.ndarray) -> tuple[np.ndarray, int]:
     g = np.empty(n, np.uint32)
     k = lib().or_color_constraints(_p(p, C.c_uint32), n, _p(g, C.c_uint32))
     return g, int(k)
+
+
+def voxelize_mesh(vertices, indices, particle_radius: float, largest_piece: bool = False):
+    """voxelize(mesh) on the CPU: (positions (n, 3) float32, surface count,
+    edges (m, 2) uint32)."""
+    from pfsim import mesh as M
+
+    return M.run_voxelize(lambda m, v: lib().or_voxelize_mesh(C.byref(m), float(particle_radius),
+                                                              1 if largest_piece else 0, C.byref(v)),
+                          vertices, indices)
+
+
+def voxelize_sdf(data, res, origin, voxel_size, particle_radius: float, dilation: float = 0.0,
+                 largest_piece: bool = False):
+    from pfsim import mesh as M
+
+    d = np.ascontiguousarray(data, np.float32)
+    r = np.ascontiguousarray(res, np.uint32)
+    o = np.ascontiguousarray(origin, np.float64)
+    vs = np.ascontiguousarray(voxel_size, np.float64)
+    return M.run_voxelize(lambda m, v: lib().or_voxelize_sdf(_p(d), _p(r, C.c_uint32), _p(o, C.c_double),
+                                                             _p(vs, C.c_double), float(particle_radius),
+                                                             float(dilation), 1 if largest_piece else 0,
+                                                             C.byref(v)), None, None)
+
+
+def bake_sdf(vertices, indices, resolution: int, padding: float | None = None):
+    """bakeMeshToSdf on the CPU: (data (res, res, res) float32 z-major,
+    origin, voxel size, inconsistent voxels)."""
+    from pfsim import mesh as M
+
+    m, keep = M.mesh_struct(vertices, indices)
+    out = np.empty(resolution ** 3, np.float32)
+    org = np.zeros(3, np.float64)
+    vs = C.c_double(0)
+    bad = C.c_uint64(0)
+    check(lib().or_bake_sdf(C.byref(m), resolution, -1.0 if padding is None else float(padding), _p(out),
+                            _p(org, C.c_double), C.byref(vs), C.byref(bad)))
+    return out.reshape(resolution, resolution, resolution), org, vs.value, bad.value
 
 
 class _RefHeap:

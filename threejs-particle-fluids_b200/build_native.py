@@ -49,11 +49,16 @@ def _headers() -> list[Path]:
     return sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "pfsim.h"]
 
 
+# Per-file flags: the mesh setup kernels keep every double multiply and add
+# separately rounded, as the reference's JavaScript arithmetic is.
+EXTRA_FLAGS = {"mesh_setup.cu": ["-fmad=false"]}
+
+
 def _compile(src: Path, newest_header: float, verbose: bool) -> Path:
     obj = BUILD / (src.stem + ".o")
     if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest_header):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

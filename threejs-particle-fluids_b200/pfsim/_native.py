@@ -145,6 +145,27 @@ class ClothDesc(C.Structure):
     ]
 
 
+class Mesh(C.Structure):
+    _fields_ = [
+        ("vertices", C.POINTER(C.c_float)),
+        ("n_vertices", C.c_uint32),
+        ("indices", C.POINTER(C.c_uint32)),
+        ("n_indices", C.c_uint32),
+    ]
+
+
+class Voxels(C.Structure):
+    _fields_ = [
+        ("positions", C.POINTER(C.c_float)),
+        ("capacity", C.c_uint32),
+        ("edges", C.POINTER(C.c_uint32)),
+        ("edge_capacity", C.c_uint32),
+        ("count", C.c_uint32),
+        ("surface_count", C.c_uint32),
+        ("edge_count", C.c_uint32),
+    ]
+
+
 class ClothParams(C.Structure):
     _fields_ = [
         ("wind", C.c_float * 3),
@@ -282,6 +303,11 @@ SIGNATURES = {
     "pf_add_softbodies": (C.c_int, [_P, C.POINTER(SoftbodyDesc), _u32p]),
     "pf_add_cloth": (C.c_int, [_P, C.POINTER(ClothDesc), _u32p]),
     "pf_add_no_self_contacts": (C.c_int, [_P, Range]),
+    "pf_voxelize_mesh": (C.c_int, [C.POINTER(Mesh), C.c_double, C.c_uint32, C.POINTER(Voxels)]),
+    "pf_voxelize_sdf": (C.c_int, [_f32p, _u32p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_double,
+                                  C.c_uint32, C.POINTER(Voxels)]),
+    "pf_bake_sdf": (C.c_int, [C.POINTER(Mesh), C.c_uint32, C.c_double, _f32p, C.POINTER(C.c_double),
+                              C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "pf_contacts_read": (C.c_int, [_P, _u32p, C.c_uint32, _u32p, _u32p]),
     "pf_cloth_get_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
     "pf_cloth_set_params": (C.c_int, [_P, C.c_uint32, C.POINTER(ClothParams)]),
