@@ -131,3 +131,31 @@ def test_vorticity_confinement_one_frame(oracle, cuda, seed):
     assert np.abs(xa - xb).max() <= POS_TOL
     va, vb = a.readback(N.PF_FIELD_VELOCITIES), b.readback(N.PF_FIELD_VELOCITIES)
     assert np.abs(va - vb).max() <= POS_TOL / (DT / r.loop.substeps)
+
+
+def test_two_fluids_in_one_scene(oracle):
+    """Two fluids on one particle system (halves of a dam break, rest
+    densities 1 and 1.3 of the lattice's): each fluid's position correction
+    reads its own multipliers only (the reference keeps one lambda buffer
+    per FluidSystem), against the oracle after one frame."""
+    import copy
+
+    from pfsim import _native as N
+    from pfsim import recipe as R
+    from pfsim import workloads as W
+
+    r = copy.deepcopy(W.dam_break(6000, seed=12))
+    f = r.materials[0][1]
+    n = r.capacity
+    h = n // 2
+    a = R.FluidOpts(**{**f.__dict__, "range": (0, h)})
+    b = R.FluidOpts(**{**f.__dict__, "range": (h, n - h), "rest_density": f.rest_density * 1.3})
+    r.materials = [("fluid", a), ("fluid", b)]
+    g = R.NativeBackend().build(r)
+    o = oracle.OracleBackend(precision=32).build(r)
+    for _ in range(2):
+        g.step(1.0 / 60.0)
+        o.step(1.0 / 60.0)
+    dev = float(np.abs(g.readback(N.PF_FIELD_POSITIONS).astype(np.float64)
+                       - o.readback(N.PF_FIELD_POSITIONS).astype(np.float64)).max())
+    assert dev <= 1e-5, dev

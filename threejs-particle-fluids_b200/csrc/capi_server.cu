@@ -97,7 +97,7 @@ struct pf_server {
   bool blocked = false;  // the last build ran out of memory: wait for a cohort to free
   std::string last_error;
   bool have_tuning = false;  // the first cohort's autotuned neighbour path, reused by later cohorts
-  uint32_t tune_path = 0, tune_block = 256, tune_unroll = 4;
+  World::Tuning tuning{};
 
   ~pf_server() {
     if (build && build->result.valid()) build->result.wait();
@@ -145,7 +145,7 @@ pf_status swap_in(pf_server* S) {
   }
   Cohort& C = *B.cohort;
   World& W = *C.world;
-  if (S->have_tuning) W.set_tuning(S->tune_path, S->tune_block, S->tune_unroll);
+  if (S->have_tuning) W.set_tuning(S->tuning);
   for (uint32_t j = 0; j < B.members.size(); ++j) {
     Request* r = B.members[j];
     if (r->state == PF_REQ_LIVE) {
@@ -384,7 +384,7 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     if (c->live) {
       PF_TRY(c->world->step(dt));
       if (!S->have_tuning && c->world->tuned() && c->world->has_fluid()) {
-        c->world->tuning(&S->tune_path, &S->tune_block, &S->tune_unroll);
+        S->tuning = c->world->tuning_all();
         S->have_tuning = true;
       }
       // the per-scene loop steps one scene and waits for it

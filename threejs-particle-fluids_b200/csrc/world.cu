@@ -115,10 +115,13 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   if (k >= V.n) return;
   const uint32_t id = V.perm[k];
   const uint32_t o = V.inv[id];
-  V.nxt.x[k] = V.cur.x[o];
+  const float4 xo = V.cur.x[o];
+  const float bvo = V.cur.bv[o];
+  V.nxt.x[k] = xo;
   V.nxt.xs[k] = V.cur.xs[o];
   V.nxt.v[k] = V.cur.v[o];
-  V.nxt.bv[k] = V.cur.bv[o];
+  V.nxt.bv[k] = bvo;
+  if (V.lm) V.lm[k] = make_float2(0.0f, mass_code(bvo, xo.w));
   V.nxt.tag[k] = V.cur.tag[o];
   V.nxt.dens[k] = V.cur.dens[o];
   V.ids[k] = id;
@@ -166,7 +169,9 @@ __global__ void __launch_bounds__(kBlock) k_boundary_volume(WorldView V, uint32_
     sum += poly6(rsq, F);
     return true;
   });
-  V.cur.bv[k] = 1.0f / fmaxf(sum, 1e-12f);
+  const float bv = 1.0f / fmaxf(sum, 1e-12f);
+  V.cur.bv[k] = bv;
+  if (V.lm) V.lm[k].y = bv;
 }
 
 // A 256-thread block covers one 256-slot chunk, hence one scene: its
@@ -1130,6 +1135,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
       S.c_cand2 = f32(cr * cr);
     }
     any_contact_ = any_contact_ || S.contact;
+    any_multi_fluid_ = any_multi_fluid_ || sp.fluids.size() > 1;
     // grid: one grid for every neighbour query, sized for the widest
     double h = S.contact ? 2.0 * sp.radius * kContactRadiusExpansion : 0.0;
     for (auto& f : sp.fluids) h = std::max(h, f.h);
@@ -1189,6 +1195,14 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         return fail(PF_ERR_INVALID, "SimLoop: neighbour grid over " + std::to_string(cells) +
                                         " cells; give tighter grid bounds");
       S.cells = (uint32_t)cells;
+      // the neighbour walk prunes a cell only when its box, widened by this
+      // slack (far above the f32 rounding of cell_of and of the box edges),
+      // is out of reach
+      double big = 0;
+      for (int a = 0; a < 3; ++a)
+        big = std::max(big, std::fabs(org[a]) + std::max(std::fabs((double)S.lo[a]),
+                                                         std::fabs((double)S.lo[a] + S.dims[a])) * cs);
+      S.prune_slack = f32(big * (1.0 / 65536.0) + 1e-9);
     } else {
       S.cells = sp.cap;
     }
@@ -1631,6 +1645,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.row_base = cv.take<uint32_t>(row_base.size());
     base_.grid_scene = cv.take<uint32_t>(grid_scene.size());
     base_.lambda = cv.take<float>(N);
+    base_.lm = any_fluid_ ? cv.take<float2>(N) : nullptr;
     base_.dx = cv.take<float4>(N);
     base_.dv = cv.take<float4>(N);
     base_.vort = any_vort_ ? cv.take<float4>(N) : nullptr;
@@ -1945,61 +1960,84 @@ void World::launch_tiles_build(const WorldView& V, uint32_t s) {
   launch_tiled(k_t_neighbors, kSmemNbr, V, s);
 }
 
-// One-thread-per-slot fluid kernels at the tuned block size.
+// One-thread-per-slot fluid kernels at a tuned block size.
 template <typename K, typename... A>
-void World::launch_fluid(K kernel, A... args) {
-  kernel<<<div_up(n_, slot_block_), slot_block_, 0, stream_>>>(args...);
+void World::launch_fluid(uint32_t block, K kernel, A... args) {
+  kernel<<<div_up(n_, block), block, 0, stream_>>>(args...);
   ++t_launches;
 }
 
-// The slot kernels at the tuned fetch depth.
-#define PF_BY_UNROLL(K, ...)                                  \
-  do {                                                        \
-    if (slot_unroll_ == 2) launch_fluid(K<2>, __VA_ARGS__);   \
-    else if (slot_unroll_ == 8) launch_fluid(K<8>, __VA_ARGS__); \
-    else launch_fluid(K<4>, __VA_ARGS__);                     \
+// A slot kernel of kind KIND at that kind's tuned block size and fetch depth.
+#define PF_BY_UNROLL(KIND, K, ...)                                                      \
+  do {                                                                                  \
+    const uint32_t b_ = tune_.block[KIND], u_ = tune_.unroll[KIND];                     \
+    if (u_ == 2) launch_fluid(b_, K<2>, __VA_ARGS__);                                   \
+    else if (u_ == 8) launch_fluid(b_, K<8>, __VA_ARGS__);                              \
+    else launch_fluid(b_, K<4>, __VA_ARGS__);                                           \
+  } while (0)
+// The position pass, without the boundary-reaction code when no fluid has
+// boundaries.
+#define PF_DELTA(...)                                                                   \
+  do {                                                                                  \
+    const uint32_t b_ = tune_.block[kSlotDelta], u_ = tune_.unroll[kSlotDelta];         \
+    if (any_react_) {                                                                   \
+      if (u_ == 2) launch_fluid(b_, k_s_delta<2, true>, __VA_ARGS__);                   \
+      else if (u_ == 8) launch_fluid(b_, k_s_delta<8, true>, __VA_ARGS__);              \
+      else launch_fluid(b_, k_s_delta<4, true>, __VA_ARGS__);                           \
+    } else {                                                                            \
+      if (u_ == 2) launch_fluid(b_, k_s_delta<2, false>, __VA_ARGS__);                  \
+      else if (u_ == 8) launch_fluid(b_, k_s_delta<8, false>, __VA_ARGS__);             \
+      else launch_fluid(b_, k_s_delta<4, false>, __VA_ARGS__);                          \
+    }                                                                                   \
   } while (0)
 
 void World::run_fluid_neighbors(const WorldView& V, uint32_t s) {
-  if (nbr_path_ == 1) {
+  if (tune_.path == 1) {
     launch_tiles_build(V, s);
   } else {
-    PF_BY_UNROLL(k_s_neighbors, V, s);
+    PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, s);
   }
 }
 
 void World::run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it) {
-  if (nbr_path_ == 1) {
+  if (tune_.path == 1) {
     launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
     launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
   } else {
-    PF_BY_UNROLL(k_s_lambda, V, r, s, it);
-    PF_BY_UNROLL(k_s_delta, V, r, s, it);
+    PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, r, s, it);
+    PF_DELTA(V, r, s, it);
   }
 }
 
 void World::run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s) {
-  if (nbr_path_ == 1) {
+  if (tune_.path == 1) {
     launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
   } else {
-    PF_BY_UNROLL(k_s_xsph, V, r, s);
+    PF_BY_UNROLL(kSlotVel, k_s_xsph, V, r, s);
   }
 }
 
 // Autotuner: on the world's own state (one grid rebuild, as the next
-// substep would do; the permutation is canonical, so no result changes), time
-// the neighbour build + density/lambda + position delta + XSPH of each
-// configuration and keep the fastest. The passes write only per-substep
-// scratch (lists, lambda, density, deltas), which every substep rebuilds.
+// substep would do; the permutation is canonical, so no result changes),
+// time each slot kernel (list build, density + lambda, position correction,
+// XSPH) at every block size and fetch depth and keep each kernel's fastest;
+// then time one substep's worth of the warp-tile path against the tuned slot
+// path and keep the faster. The passes write only per-substep scratch (lists,
+// lambda, density, deltas), which every substep rebuilds.
 pf_status World::tune() {
   tuned_ = true;
   if (!any_fluid_ || n_ == 0) return PF_OK;
   if (const char* e = std::getenv("PFSIM_NBR_PATH")) {  // fixed choice for measurements
-    nbr_path_ = ((uint32_t)std::atoi(e) == 1 && !any_vort_ && !any_imp_) ? 1u : 0u;
-    if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) slot_block_ = (uint32_t)std::atoi(b);
-    if (slot_block_ != 128 && slot_block_ != 256 && slot_block_ != 512) slot_block_ = 256;
-    if (const char* u = std::getenv("PFSIM_SLOT_UNROLL")) slot_unroll_ = (uint32_t)std::atoi(u);
-    if (slot_unroll_ != 2 && slot_unroll_ != 8) slot_unroll_ = 4;
+    tune_.path = ((uint32_t)std::atoi(e) == 1 && !any_vort_ && !any_imp_ && !any_multi_fluid_) ? 1u : 0u;
+    uint32_t blk = 256, unr = 4;
+    if (const char* b = std::getenv("PFSIM_SLOT_BLOCK")) blk = (uint32_t)std::atoi(b);
+    if (blk != 128 && blk != 256 && blk != 512) blk = 256;
+    if (const char* u = std::getenv("PFSIM_SLOT_UNROLL")) unr = (uint32_t)std::atoi(u);
+    if (unr != 2 && unr != 8) unr = 4;
+    for (int q = 0; q < 4; ++q) {
+      tune_.block[q] = blk;
+      tune_.unroll[q] = unr;
+    }
     return PF_OK;
   }
   run_sort_and_permute(parity_, false);
@@ -2011,25 +2049,11 @@ pf_status World::tune() {
   // next sort)
   float* keep = reinterpret_cast<float*>(base_.keys);
   PF_CUDA(cudaMemcpyAsync(keep, V.cur.dens, 4ull * n_, cudaMemcpyDeviceToDevice, stream_));
-  // the warp-tile path has no vorticity pass: worlds with it stay on slots
-  const uint32_t n_cands_max = (any_vort_ || any_imp_) ? 7u : 8u;
-  struct Cand { uint32_t path, block, unroll; };
-  const Cand cands[] = {{0, 128, 4}, {0, 256, 4}, {0, 512, 4}, {0, 128, 2}, {0, 256, 2},
-                        {0, 128, 8}, {0, 256, 8}, {1, 128, 4}};
-  float best = 1e30f;
-  Cand pick = {0, 256, 4};
-  for (uint32_t ci = 0; ci < n_cands_max; ++ci) {
-    const Cand& c = cands[ci];
-    nbr_path_ = c.path;
-    slot_block_ = c.block;
-    slot_unroll_ = c.unroll;
+  auto timed = [&](auto&& body, float* out) -> pf_status {
     float t = 0;
     for (int rep = 0; rep < 2; ++rep) {
       PF_CUDA(cudaEventRecord(ev0_, stream_));
-      // one substep's worth: the list once, density/lambda + delta per iteration
-      run_fluid_neighbors(V, 0);
-      for (uint32_t it = 0; it < std::max(max_iter_, 1u); ++it) run_fluid_lambda_delta(V, rank, 0, 0);
-      if (any_visc_ || any_vort_) run_fluid_xsph(V, rank, 0);
+      body();
       PF_CUDA(cudaEventRecord(ev1_, stream_));
       PF_CUDA(cudaEventSynchronize(ev1_));
       float ms = 0;
@@ -2037,14 +2061,58 @@ pf_status World::tune() {
       t = rep == 0 ? ms : std::min(t, ms);
     }
     PF_CUDA(cudaGetLastError());
-    if (t < best) {
-      best = t;
-      pick = c;
-    }
+    *out = t;
+    return PF_OK;
+  };
+  const uint32_t iters = std::max(max_iter_, 1u);
+  const bool vel = any_visc_ || any_vort_;
+  // the slot path, kernel by kernel (the list first: the others read it)
+  tune_.path = 0;
+  const uint32_t blocks[3] = {128, 256, 512}, unrolls[3] = {2, 4, 8};
+  float slot_total = 0;
+  for (int kind = 0; kind < 4; ++kind) {
+    if (kind == kSlotVel && !vel) continue;
+    float best = 1e30f;
+    uint32_t bb = 256, bu = 4;
+    for (uint32_t b : blocks)
+      for (uint32_t u : unrolls) {
+        if (u == 8 && b == 512) continue;
+        tune_.block[kind] = b;
+        tune_.unroll[kind] = u;
+        float t = 0;
+        PF_TRY(timed(
+            [&] {
+              if (kind == kSlotNbr) PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, 0u);
+              else if (kind == kSlotLambda) PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
+              else if (kind == kSlotDelta) PF_DELTA(V, rank, 0u, 0u);
+              else PF_BY_UNROLL(kSlotVel, k_s_xsph, V, rank, 0u);
+            },
+            &t));
+        if (t < best) {
+          best = t;
+          bb = b;
+          bu = u;
+        }
+      }
+    tune_.block[kind] = bb;
+    tune_.unroll[kind] = bu;
+    slot_total += (kind == kSlotLambda || kind == kSlotDelta) ? best * iters : best;
   }
-  nbr_path_ = pick.path;
-  slot_block_ = pick.block;
-  slot_unroll_ = pick.unroll;
+  // the warp-tile path has no vorticity or surface pass and reads one shared
+  // lambda buffer: worlds with those, or with a scene of several fluids,
+  // stay on slots
+  if (!(any_vort_ || any_imp_ || any_multi_fluid_)) {
+    tune_.path = 1;
+    float t = 0;
+    PF_TRY(timed(
+        [&] {
+          run_fluid_neighbors(V, 0);
+          for (uint32_t it = 0; it < iters; ++it) run_fluid_lambda_delta(V, rank, 0, 0);
+          if (vel) run_fluid_xsph(V, rank, 0);
+        },
+        &t));
+    tune_.path = t < slot_total ? 1u : 0u;
+  }
   PF_CUDA(cudaMemcpyAsync(V.cur.dens, keep, 4ull * n_, cudaMemcpyDeviceToDevice, stream_));
   return PF_OK;
 }
@@ -2137,8 +2205,8 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         imp = imp || (F.rank == r && (F.has_st || F.has_ad));
       }
       if (!imp) continue;
-      if (st) PF_BY_UNROLL(k_s_color_normal, V, r, s);
-      PF_BY_UNROLL(k_s_impulses, V, r, s);
+      if (st) PF_BY_UNROLL(kSlotVel, k_s_color_normal, V, r, s);
+      PF_BY_UNROLL(kSlotVel, k_s_impulses, V, r, s);
       launch_slots(k_imp_apply, n_, stream_, V, r, s);
     }
   launch_aero(V, 1, s);
@@ -2205,7 +2273,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
     if (has_velocity) {
       run_fluid_xsph(V, r, s);
-      if (has_vort) PF_BY_UNROLL(k_s_vort_grad, V, r, s);
+      if (has_vort) PF_BY_UNROLL(kSlotVel, k_s_vort_grad, V, r, s);
       launch_slots(k_xsph_apply, n_, stream_, V, r, s);
     }
     if (has_local) {
@@ -2427,7 +2495,7 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
       }
       std::fill(o, o + (size_t)cap * kMaxNbr, 0xffffffffu);
       if (!base_.nbr16) return PF_OK;
-      if (nbr_path_ == 0) {
+      if (tune_.path == 0) {
         std::vector<uint32_t> colw(seg), seg_ids(seg);
         PF_CUDA(cudaMemcpy(seg_ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
         for (uint32_t m = 0; m < kMaxNbr; ++m) {
@@ -2605,20 +2673,20 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
   auto run = [&]() {
     switch (stage) {
       case 0:
-        if (nbr_path_ == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
-        else PF_BY_UNROLL(k_s_neighbors, V, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
+        else PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, 0u);
         break;
       case 1:
-        if (nbr_path_ == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
-        else PF_BY_UNROLL(k_s_lambda, V, rank, 0u, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
+        else PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
         break;
       case 2:
-        if (nbr_path_ == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
-        else PF_BY_UNROLL(k_s_delta, V, rank, 0u, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
+        else PF_DELTA(V, rank, 0u, 0u);
         break;
       case 3:
-        if (nbr_path_ == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
-        else PF_BY_UNROLL(k_s_xsph, V, rank, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
+        else PF_BY_UNROLL(kSlotVel, k_s_xsph, V, rank, 0u);
         break;
       case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
       default: break;

@@ -151,6 +151,7 @@ struct DevScene {
   uint32_t max_contacts;              // pairs solved per substep (the first in slot order)
   float c_mus, c_muk;                 // contact friction
   float c_dist, c_cand2;              // 2r and (2r * 1.1)^2 as f32 literals
+  float prune_slack;                  // metres the neighbour walk's cell boxes are widened by when pruning
 };
 
 // One SDF collider as the kernels read it (sdf.ts:17-80 fields).
@@ -272,6 +273,10 @@ struct WorldView {
   uint32_t n_grid_scenes;
   uint32_t n_rows;
   float* lambda;
+  // per slot (lambda, q): the slot path's lambda, and the neighbour mass code
+  // q = bv > 0 ? bv : -(own mass), so a neighbour pass reads both the
+  // multiplier and the SPH mass (shared.ts:52-62) in one 8-byte gather
+  float2* lm;
   float4* dx;
   float4* dv;
   float4* vort;       // curl of the velocity per slot, w = its length (vorticity confinement)
@@ -399,19 +404,26 @@ class World {
   // Neighbour-pass configuration the autotuner chose (path 0: one thread
   // per slot, `block` threads per block, list entries fetched `unroll` at a
   // time; path 1: warp tiles).
+  // The slot path tunes each of its kernels on its own: kSlotNbr (list
+  // build), kSlotLambda (density + lambda), kSlotDelta (position
+  // correction), kSlotVel (XSPH and the other velocity-stage passes).
+  struct Tuning {
+    uint32_t path = 0;
+    uint32_t block[4] = {256, 256, 256, 256};
+    uint32_t unroll[4] = {4, 4, 4, 4};
+  };
   void tuning(uint32_t* path, uint32_t* block, uint32_t* unroll = nullptr) const {
-    *path = nbr_path_;
-    *block = slot_block_;
-    if (unroll) *unroll = slot_unroll_;
+    *path = tune_.path;
+    *block = tune_.block[kSlotLambda];
+    if (unroll) *unroll = tune_.unroll[kSlotLambda];
   }
+  const Tuning& tuning_all() const { return tune_; }
   bool tuned() const { return tuned_; }
   bool has_fluid() const { return any_fluid_; }
   // Use a configuration tuned elsewhere (another world of the same kind of
   // scenes) instead of timing candidates on the first step.
-  void set_tuning(uint32_t path, uint32_t block, uint32_t unroll) {
-    nbr_path_ = path;
-    slot_block_ = block;
-    slot_unroll_ = unroll;
+  void set_tuning(const Tuning& t) {
+    tune_ = t;
     tuned_ = true;
   }
   size_t device_bytes() const { return bytes_; }
@@ -423,7 +435,7 @@ class World {
   void run_init_pass();
   void launch_tiles_build(const WorldView& V, uint32_t s);
   template <typename K, typename... A>
-  void launch_fluid(K kernel, A... args);
+  void launch_fluid(uint32_t block, K kernel, A... args);
   void run_fluid_neighbors(const WorldView& V, uint32_t s);
   void run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it);
   void run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s);
@@ -462,6 +474,7 @@ class World {
   bool any_react_ = false;
   bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass
   bool any_contact_ = false;        // a scene with particle contacts
+  bool any_multi_fluid_ = false;    // a scene with two or more fluids (slot path only)
   uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
   // device memory: one arena
   void* arena_ = nullptr;
@@ -472,7 +485,8 @@ class World {
   uint32_t parity_ = 0;
   bool inited_ = false;
   // neighbour passes: autotuned once per world, before the first graph capture
-  uint32_t nbr_path_ = 0, slot_block_ = 256, slot_unroll_ = 4;
+  static constexpr int kSlotNbr = 0, kSlotLambda = 1, kSlotDelta = 2, kSlotVel = 3;
+  Tuning tune_{};
   bool tuned_ = false;
   // graph
   bool use_graph_ = false;

@@ -63,6 +63,14 @@ __device__ __forceinline__ float neighbor_mass(float bv, float w, float rho0) {
   return bv > 0.0f ? rho0 * bv : (w > 0.0f ? 1.0f / w : 0.0f);
 }
 
+// The mass code of a slot (its lm.y): the boundary volume of a boundary
+// particle, minus its own mass otherwise; and the mass a fluid with rest
+// density rho0 sees from it.
+__device__ __forceinline__ float mass_code(float bv, float w) {
+  return bv > 0.0f ? bv : -(w > 0.0f ? 1.0f / w : 0.0f);
+}
+__device__ __forceinline__ float code_mass(float q, float rho0) { return q > 0.0f ? rho0 * q : -q; }
+
 // The same quantities in the form the per-neighbour loops use: one
 // reciprocal square root instead of a square root and three divisions, and
 // an approximate reciprocal for the particle mass. Within the solver's

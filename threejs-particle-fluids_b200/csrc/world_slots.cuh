@@ -39,17 +39,41 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   int32_t cx, cy, cz;
   local_cell(S, xi, &cx, &cy, &cz, nullptr);
   const int32_t x0 = max(cx - 1, 0), x1 = min(cx + 1, (int32_t)S.dims[0] - 1);
+  // Cells whose box lies at least h away cannot hold a neighbour, so they
+  // are left out of the walk; the hits, and their order, stay those of the
+  // full 27-cell walk. Border cells (which hold the clamped particles) are
+  // never left out.
+  auto gap = [&](float p, int32_t c, int a, float o) {
+    const float lo = o + (float)(S.lo[a] + c) * S.cell, hi = lo + S.cell;
+    const float d = fmaxf(fmaxf(lo - p, p - hi), 0.0f);
+    return fmaxf(d - S.prune_slack, 0.0f);
+  };
+  const int32_t nx = (int32_t)S.dims[0], ny = (int32_t)S.dims[1], nz = (int32_t)S.dims[2];
+  const float gl = (x0 < cx && x0 > 0) ? gap(xi.x, x0, 0, S.ox) : 0.0f;
+  const float gr = (x1 > cx && x1 < nx - 1) ? gap(xi.x, x1, 0, S.ox) : 0.0f;
+  const bool can_l = x0 < cx && x0 > 0, can_r = x1 > cx && x1 < nx - 1;
   uint32_t rs[9], re[9];
 #pragma unroll
   for (int r = 0; r < 9; ++r) {
     const int32_t z = cz + r / 3 - 1, y = cy + r % 3 - 1;
-    if (z < 0 || z >= (int32_t)S.dims[2] || y < 0 || y >= (int32_t)S.dims[1]) {
+    if (z < 0 || z >= nz || y < 0 || y >= ny) {
       rs[r] = re[r] = 0;
       continue;
     }
+    int32_t a0 = x0, a1 = x1;
+    if (y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
+      const float gy = y != cy ? gap(xi.y, y, 1, S.oy) : 0.0f, gz = z != cz ? gap(xi.z, z, 2, S.oz) : 0.0f;
+      const float perp = gy * gy + gz * gz;
+      if (perp >= hsq) {
+        rs[r] = re[r] = 0;
+        continue;
+      }
+      if (can_l && perp + gl * gl >= hsq) a0 = cx;
+      if (can_r && perp + gr * gr >= hsq) a1 = cx;
+    }
     const uint32_t row = S.cell_base + S.dims[0] * ((uint32_t)y + S.dims[1] * (uint32_t)z);
-    rs[r] = __ldg(V.cstart + row + x0);
-    re[r] = __ldg(V.cstart + row + x1) + __ldg(V.ccount + row + x1);
+    rs[r] = __ldg(V.cstart + row + a0);
+    re[r] = __ldg(V.cstart + row + a1) + __ldg(V.ccount + row + a1);
   }
   // Every candidate is tested; the first kMaxNbr hits in walk order are
   // stored (as the reference's list keeps them) and any further hit only
@@ -104,8 +128,8 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
 #ifdef PF_EXACT_ROUNDING
-  auto one = [&](float4 xj, float bvj) {
-    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+  auto one = [&](float4 xj, float qj) {
+    const float mass = code_mass(qj, F.rho0);
     const f3 off = xi - xyz(xj);
     const float rsq = dot(off, off);
     rho += mass * poly6(rsq, F);
@@ -117,8 +141,8 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   // The kernel constants leave the sums: rho = poly6 * sum m d^3,
   // sum grad = -spiky * sum f r, sum |grad|^2 w = spiky^2 * sum f^2 r^2 w
   // with f = m (h - r)^2 / r.
-  auto one = [&](float4 xj, float bvj) {
-    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+  auto one = [&](float4 xj, float qj) {
+    const float mass = code_mass(qj, F.rho0);
     const f3 off = xi - xyz(xj);
     const float rsq = dot(off, off);
     const float d = fmaxf(F.hsq - rsq, 0.0f);
@@ -128,6 +152,7 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
     gss += (f * f) * (rsq * xj.w);
   };
 #endif
+  const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
   uint32_t m = 0;
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
     uint32_t j[kNbrUnroll];
@@ -138,14 +163,14 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) {
       xj[q] = __ldg(V.cur.xs + j[q]);
-      bj[q] = __ldg(V.cur.bv + j[q]);
+      bj[q] = __ldg(q_of + 2 * (size_t)j[q]);
     }
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], bj[q]);
   }
   for (; m < cnt; ++m) {
     const uint32_t j = __ldg(nl + m * n);
-    one(__ldg(V.cur.xs + j), __ldg(V.cur.bv + j));
+    one(__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j));
   }
 #ifndef PF_EXACT_ROUNDING
   rho *= F.poly6;
@@ -154,18 +179,19 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
 #endif
   V.cur.dens[k] = rho;
   const float C = rho * F.inv_rho0 - 1.0f;
-  if (C <= 0.0f) {
-    V.lambda[k] = 0.0f;
-    return;
+  float lam = 0.0f;
+  if (C > 0.0f) {
+    const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
+    const float at = F.compliance / (S.dt * S.dt);
+    lam = -C / fmaxf(gn + at, 1e-20f);
   }
-  const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
-  const float at = F.compliance / (S.dt * S.dt);
-  V.lambda[k] = -C / fmaxf(gn + at, 1e-20f);
+  V.lambda[k] = lam;
+  V.lm[k].x = lam;
 }
 
 // positionDelta.ts:41-85 (the reaction on dynamic boundary neighbours goes
 // into the fixed-point reaction sums by slot).
-template <uint32_t kNbrUnroll>
+template <uint32_t kNbrUnroll, bool kReact>
 __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -177,14 +203,19 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
   if (sub >= S.substeps || it >= S.iterations) return;
   const float4 xi4 = V.cur.xs[k];
   const f3 xi = xyz(xi4);
-  const float li = V.lambda[k];
-  const bool react = F.react_lo != F.react_hi && li != 0.0f;
+  const float li = V.lm[k].x;
+  const bool react = kReact && F.react_lo != F.react_hi && li != 0.0f;
+  // each fluid reads its own multipliers, zero for other particles (the
+  // reference keeps one lambda buffer per fluid)
+  const bool multi = S.fluid_count > 1;
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
-  auto one = [&](uint32_t j, float4 xj, float bvj, float lj) {
-    const float mass = nbr_mass(bvj, xj.w, F.rho0);
+  auto one = [&](uint32_t j, float4 xj, float2 lq) {
+    const float bvj = lq.y;
+    const float lj = (multi && tag_fluid(__ldg(V.cur.tag + j)) != f) ? 0.0f : lq.x;
+    const float mass = code_mass(bvj, F.rho0);
     const f3 off = xi - xyz(xj);
 #ifdef PF_EXACT_ROUNDING
     const f3 g = spiky_vec(off, dot(off, off), F);
@@ -211,21 +242,20 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
     uint32_t j[kNbrUnroll];
     float4 xj[kNbrUnroll];
-    float bj[kNbrUnroll], lj[kNbrUnroll];
+    float2 lq[kNbrUnroll];
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) {
       xj[q] = __ldg(V.cur.xs + j[q]);
-      bj[q] = __ldg(V.cur.bv + j[q]);
-      lj[q] = __ldg(V.lambda + j[q]);
+      lq[q] = __ldg(V.lm + j[q]);
     }
 #pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], bj[q], lj[q]);
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], lq[q]);
   }
   for (; m < cnt; ++m) {
     const uint32_t j = __ldg(nl + m * n);
-    one(j, __ldg(V.cur.xs + j), __ldg(V.cur.bv + j), __ldg(V.lambda + j));
+    one(j, __ldg(V.cur.xs + j), __ldg(V.lm + j));
   }
 #ifndef PF_EXACT_ROUNDING
   sum = sum * -F.spiky;
@@ -253,6 +283,7 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
+  const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y: volume if > 0
   auto one = [&](float4 xj, float4 vj, float bvj) {
     const f3 off = xi - xyz(xj);
     const float vol = bvj > 0.0f ? bvj : F.volume;
@@ -271,14 +302,14 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
     for (uint32_t q = 0; q < kNbrUnroll; ++q) {
       xj[q] = __ldg(V.cur.x + j[q]);
       vj[q] = __ldg(V.cur.v + j[q]);
-      bj[q] = __ldg(V.cur.bv + j[q]);
+      bj[q] = __ldg(q_of + 2 * (size_t)j[q]);
     }
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], vj[q], bj[q]);
   }
   for (; m < cnt; ++m) {
     const uint32_t j = __ldg(nl + m * n);
-    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), __ldg(V.cur.bv + j));
+    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), __ldg(q_of + 2 * (size_t)j));
   }
   if (visc) V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
   if (vort) V.vort[k] = with_w(curl, len(curl));
