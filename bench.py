@@ -265,30 +265,10 @@ class BatchWorkload:
         recipes = self.recipes(replica_seed(rank))
         plain = [backend.build(r) for r in recipes]
         psub = sum(r.particle_substeps for r in recipes)
-        # ---- plain baseline: each scene its own launches, no graph.
-        # Sequential: step a scene and wait for it (the reference's
-        # `await simulation.step()` per scene); timed as the sum of each
-        # scene's device time between its step's start and end events.
-        # Overlapped: every scene launched on its own stream, one wait.
-        for _ in range(warmup if plain_baseline else 0):
-            for sc in plain:
-                sc.step(self.DT)
-        torch.cuda.synchronize()
-        p_steps = max(2, steps // 2) if plain_baseline else 0
-        seq_dev = 0.0
-        t0 = time.perf_counter()
-        for _ in range(p_steps):
-            for sc in plain:
-                sc.step(self.DT)
-                seq_dev += sc.last_step_ms()
-        seq_wall = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1)
-        plain_ms = seq_dev / max(p_steps, 1) if plain_baseline else float("nan")
-        t0 = time.perf_counter()
-        for _ in range(p_steps):
-            for sc in plain:
-                sc.step(self.DT)
-        torch.cuda.synchronize()
-        overlap_ms = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1) if plain_baseline else float("nan")
+        # Both arms start from the scenes' initial state and are timed over
+        # the same frames (after `warmup` frames): the batch copies the built
+        # scenes' initial state, and the plain scenes are built afresh from
+        # the same recipes once the batch is gone (each arm alone on the GPU).
         # ---- batched: one world, one launch per stage, one graph per tick
         batch = R.Batch(plain, use_graph=True)
         for sc in plain:
@@ -341,6 +321,35 @@ class BatchWorkload:
         batch.close()
         if not ok:
             raise RuntimeError("non-finite positions after the timed steps")
+        # ---- plain baseline: each scene its own launches and waits.
+        # Sequential: step a scene and wait for it (the reference's
+        # `await simulation.step()` per scene); timed as the sum of each
+        # scene's device time between its step's start and end events.
+        # Overlapped: every scene launched on its own stream, one wait.
+        plain = [backend.build(r) for r in recipes] if plain_baseline else []
+        for _ in range(warmup if plain_baseline else 0):
+            for sc in plain:
+                sc.step(self.DT)
+        torch.cuda.synchronize()
+        p_steps = max(2, steps) if plain_baseline else 0
+        seq_dev = 0.0
+        t0 = time.perf_counter()
+        for _ in range(p_steps):
+            for sc in plain:
+                sc.step(self.DT)
+                seq_dev += sc.last_step_ms()
+        seq_wall = (time.perf_counter() - t0) * 1e3 / max(p_steps, 1)
+        plain_ms = seq_dev / max(p_steps, 1) if plain_baseline else float("nan")
+        o_steps = max(2, steps // 2) if plain_baseline else 0
+        t0 = time.perf_counter()
+        for _ in range(o_steps):
+            for sc in plain:
+                sc.step(self.DT)
+        torch.cuda.synchronize()
+        overlap_ms = (time.perf_counter() - t0) * 1e3 / max(o_steps, 1) if plain_baseline else float("nan")
+        for sc in plain:
+            sc.close()
+        plain = None
         return {
             "ms": ms,
             "units_per_step": psub,

@@ -274,18 +274,26 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
 // positionDelta.ts:217-226, then the reaction accumulator's apply over the
 // covering range of the fluid's boundaries (FluidSystem.ts:280-287).
 __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  // the slot's own loads go out first, so their latency overlaps the
+  // primitive staging and the scene lookup
+  const bool live = k < V.n;
+  uint32_t tg = 0;
+  float4 x = make_float4(0, 0, 0, 0), d = make_float4(0, 0, 0, 0);
+  if (live) {
+    tg = __ldg(V.cur.tag + k);
+    x = V.cur.xs[k];
+    d = V.dx[k];
+  }
   __shared__ PrimStage st;
   const pf_primitive* prims = stage_prims(V, st);
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  if (!live) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
   if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0) return;
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  float4 x = V.cur.xs[k];
+  const uint32_t f = tag_fluid(tg);
   bool changed = false;
   if (f && V.fluids[f - 1].rank == rank) {
-    const float4 d = V.dx[k];
     x.x += d.x;
     x.y += d.y;
     x.z += d.z;
@@ -1136,6 +1144,18 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
     any_contact_ = any_contact_ || S.contact;
     any_multi_fluid_ = any_multi_fluid_ || sp.fluids.size() > 1;
+    S.homog = 0;
+    S.homog_mass = 0.0f;
+    if (sp.fluids.size() == 1 && sp.fluids[0].range.start == 0 && sp.fluids[0].range.count == sp.cap &&
+        sp.fluids[0].bnd.empty() && sp.cap > 0) {
+      const float w0 = sp.inv_mass[0];
+      bool same = w0 > 0.0f;
+      for (uint32_t i = 1; i < sp.cap && same; ++i) same = sp.inv_mass[i] == w0;
+      if (same) {
+        S.homog = 1;
+        S.homog_mass = 1.0f / w0;  // the mass code_mass gives every neighbour
+      }
+    }
     // grid: one grid for every neighbour query, sized for the widest
     double h = S.contact ? 2.0 * sp.radius * kContactRadiusExpansion : 0.0;
     for (auto& f : sp.fluids) h = std::max(h, f.h);
@@ -1495,6 +1515,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
     aero_ranges_[stage] = {begin, (uint32_t)avtx.size()};
   }
+  // the list build forms the first iteration's density when nothing moves
+  // particles between the two passes
+  fuse_dens_ = !any_imp_ && aero_ranges_[1].second == aero_ranges_[1].first;
   // ---- cloth velocity smoothing by rank: per particle, its edge neighbours -
   std::vector<uint2> dvtx;
   std::vector<uint32_t> doff(1, 0), dnbr;
@@ -1646,6 +1669,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.grid_scene = cv.take<uint32_t>(grid_scene.size());
     base_.lambda = cv.take<float>(N);
     base_.lm = any_fluid_ ? cv.take<float2>(N) : nullptr;
+    base_.xl = any_fluid_ ? cv.take<float4>(N) : nullptr;
     base_.dx = cv.take<float4>(N);
     base_.dv = cv.take<float4>(N);
     base_.vort = any_vort_ ? cv.take<float4>(N) : nullptr;
@@ -1975,6 +1999,35 @@ void World::launch_fluid(uint32_t block, K kernel, A... args) {
     else if (u_ == 8) launch_fluid(b_, K<8>, __VA_ARGS__);                              \
     else launch_fluid(b_, K<4>, __VA_ARGS__);                                           \
   } while (0)
+// The list build, forming the first iteration's density and lambda of
+// first-material fluids when nothing moves between the two (fuse_dens_).
+#define PF_NBR(...)                                                                     \
+  do {                                                                                  \
+    const uint32_t b_ = tune_.block[kSlotNbr], u_ = tune_.unroll[kSlotNbr];             \
+    if (fuse_dens_) {                                                                   \
+      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, true>, __VA_ARGS__);               \
+      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, true>, __VA_ARGS__);          \
+      else launch_fluid(b_, k_s_neighbors<4, true>, __VA_ARGS__);                       \
+    } else {                                                                            \
+      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, false>, __VA_ARGS__);              \
+      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, false>, __VA_ARGS__);         \
+      else launch_fluid(b_, k_s_neighbors<4, false>, __VA_ARGS__);                      \
+    }                                                                                   \
+  } while (0)
+// XSPH, without the boundary-volume gather when the world has no boundaries.
+#define PF_XSPH(...)                                                                    \
+  do {                                                                                  \
+    const uint32_t b_ = tune_.block[kSlotVel], u_ = tune_.unroll[kSlotVel];             \
+    if (any_static_bnd_ || any_dyn_bnd_) {                                              \
+      if (u_ == 2) launch_fluid(b_, k_s_xsph<2, true>, __VA_ARGS__);                    \
+      else if (u_ == 8) launch_fluid(b_, k_s_xsph<8, true>, __VA_ARGS__);               \
+      else launch_fluid(b_, k_s_xsph<4, true>, __VA_ARGS__);                            \
+    } else {                                                                            \
+      if (u_ == 2) launch_fluid(b_, k_s_xsph<2, false>, __VA_ARGS__);                   \
+      else if (u_ == 8) launch_fluid(b_, k_s_xsph<8, false>, __VA_ARGS__);              \
+      else launch_fluid(b_, k_s_xsph<4, false>, __VA_ARGS__);                           \
+    }                                                                                   \
+  } while (0)
 // The position pass, without the boundary-reaction code when no fluid has
 // boundaries.
 #define PF_DELTA(...)                                                                   \
@@ -1995,7 +2048,7 @@ void World::run_fluid_neighbors(const WorldView& V, uint32_t s) {
   if (tune_.path == 1) {
     launch_tiles_build(V, s);
   } else {
-    PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, s);
+    PF_NBR(V, s);
   }
 }
 
@@ -2004,7 +2057,8 @@ void World::run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, u
     launch_tiled(k_t_lambda, kSmemLambda, V, r, s, it);
     launch_tiled(k_t_delta, kSmemDelta, V, r, s, it);
   } else {
-    PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, r, s, it);
+    // the list build formed rank 0's first density and lambda
+    if (!(fuse_dens_ && r == 0 && it == 0)) PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, r, s, it);
     PF_DELTA(V, r, s, it);
   }
 }
@@ -2013,7 +2067,7 @@ void World::run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s) {
   if (tune_.path == 1) {
     launch_tiled(k_t_xsph, kSmemXsph, V, r, s);
   } else {
-    PF_BY_UNROLL(kSlotVel, k_s_xsph, V, r, s);
+    PF_XSPH(V, r, s);
   }
 }
 
@@ -2082,10 +2136,10 @@ pf_status World::tune() {
         float t = 0;
         PF_TRY(timed(
             [&] {
-              if (kind == kSlotNbr) PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, 0u);
+              if (kind == kSlotNbr) PF_NBR(V, 0u);
               else if (kind == kSlotLambda) PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
               else if (kind == kSlotDelta) PF_DELTA(V, rank, 0u, 0u);
-              else PF_BY_UNROLL(kSlotVel, k_s_xsph, V, rank, 0u);
+              else PF_XSPH(V, rank, 0u);
             },
             &t));
         if (t < best) {
@@ -2096,7 +2150,8 @@ pf_status World::tune() {
       }
     tune_.block[kind] = bb;
     tune_.unroll[kind] = bu;
-    slot_total += (kind == kSlotLambda || kind == kSlotDelta) ? best * iters : best;
+    const uint32_t reps = kind == kSlotDelta ? iters : (kind == kSlotLambda ? iters - (fuse_dens_ ? 1u : 0u) : 1u);
+    slot_total += best * reps;
   }
   // the warp-tile path has no vorticity or surface pass and reads one shared
   // lambda buffer: worlds with those, or with a scene of several fluids,
@@ -2374,6 +2429,7 @@ pf_status World::write(uint32_t scene, uint32_t field, const void* src, size_t b
   std::vector<uint32_t> ids(seg);
   PF_CUDA(cudaMemcpy(ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
   const StateBuf& B = buf_[parity_];
+  if (w_only) h_scenes_[scene].homog = 0;  // masses may differ from now on
   auto patch = [&](float4* dev) -> pf_status {
     std::vector<float4> tmp(seg);
     PF_CUDA(cudaMemcpy(tmp.data(), dev + S.seg_start, 16ull * seg, cudaMemcpyDeviceToHost));
@@ -2674,7 +2730,7 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
     switch (stage) {
       case 0:
         if (tune_.path == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
-        else PF_BY_UNROLL(kSlotNbr, k_s_neighbors, V, 0u);
+        else PF_NBR(V, 0u);
         break;
       case 1:
         if (tune_.path == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
@@ -2686,7 +2742,7 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
         break;
       case 3:
         if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
-        else PF_BY_UNROLL(kSlotVel, k_s_xsph, V, rank, 0u);
+        else PF_XSPH(V, rank, 0u);
         break;
       case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
       default: break;

@@ -152,6 +152,11 @@ struct DevScene {
   float c_mus, c_muk;                 // contact friction
   float c_dist, c_cand2;              // 2r and (2r * 1.1)^2 as f32 literals
   float prune_slack;                  // metres the neighbour walk's cell boxes are widened by when pruning
+  // one fluid over every particle, no boundaries, one inverse mass: every
+  // neighbour has mass homog_mass, and the position pass gathers (x*, lambda)
+  // from xl in one load
+  uint32_t homog;
+  float homog_mass;
 };
 
 // One SDF collider as the kernels read it (sdf.ts:17-80 fields).
@@ -277,6 +282,7 @@ struct WorldView {
   // q = bv > 0 ? bv : -(own mass), so a neighbour pass reads both the
   // multiplier and the SPH mass (shared.ts:52-62) in one 8-byte gather
   float2* lm;
+  float4* xl;  // (x*, lambda) per fluid slot of homogeneous scenes, written by the density pass
   float4* dx;
   float4* dv;
   float4* vort;       // curl of the velocity per slot, w = its length (vorticity confinement)
@@ -475,6 +481,7 @@ class World {
   bool any_unfused_prims_ = false;  // a scene whose colliders run in their own pass
   bool any_contact_ = false;        // a scene with particle contacts
   bool any_multi_fluid_ = false;    // a scene with two or more fluids (slot path only)
+  bool fuse_dens_ = false;          // the slot list build forms the first density and lambda
   uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
   // device memory: one arena
   void* arena_ = nullptr;

@@ -20,12 +20,64 @@
 namespace pf {
 
 
+// lambda.ts:60-71: density and the multiplier from the neighbour sums (in
+// the fast path the kernel constants are applied here).
+__device__ __forceinline__ void finish_lambda(const WorldView& V, const DevScene& S, const DevFluid& F, uint32_t k,
+                                              float4 xi4, float rho, f3 gs, float gss) {
+  const float wi = xi4.w;
+#ifndef PF_EXACT_ROUNDING
+  rho *= F.poly6;
+  gs = gs * -F.spiky;
+  gss *= F.spiky * F.spiky;
+#endif
+  V.cur.dens[k] = rho;
+  const float C = rho * F.inv_rho0 - 1.0f;
+  float lam = 0.0f;
+  if (C > 0.0f) {
+    const float gn = (dot(gs, gs) * wi + gss) * (F.inv_rho0 * F.inv_rho0);
+    const float at = F.compliance / (S.dt * S.dt);
+    lam = -C / fmaxf(gn + at, 1e-20f);
+  }
+  V.lambda[k] = lam;
+  V.lm[k].x = lam;
+  if (S.homog) V.xl[k] = make_float4(xi4.x, xi4.y, xi4.z, lam);
+}
+
+// lambda.ts:41-59: one neighbour's terms of the density and constraint-
+// gradient sums.
+__device__ __forceinline__ void lambda_terms(const DevFluid& F, f3 xi, float4 xj, float qj, float& rho, f3& gs,
+                                             float& gss) {
+  const float mass = code_mass(qj, F.rho0);
+  const f3 off = xi - xyz(xj);
+  const float rsq = dot(off, off);
+#ifdef PF_EXACT_ROUNDING
+  rho += mass * poly6(rsq, F);
+  const f3 g = spiky_vec(off, rsq, F) * mass;
+  gs = gs + g;
+  gss += dot(g, g) * xj.w;
+#else
+  // The kernel constants leave the sums: rho = poly6 * sum m d^3,
+  // sum grad = -spiky * sum f r, sum |grad|^2 w = spiky^2 * sum f^2 r^2 w
+  // with f = m (h - r)^2 / r.
+  const float d = fmaxf(F.hsq - rsq, 0.0f);
+  rho += mass * (d * d * d);
+  const float f = spiky_shape(rsq, F) * mass;
+  gs = gs + off * f;
+  gss += (f * f) * (rsq * xj.w);
+#endif
+}
+
 // neighborList.ts:48-71: up to 64 neighbours within h at the predicted
 // positions of this substep, in walk order (query.ts:37-66: rows dz, dy;
 // inside a row ascending cell, inside a cell ascending index), self
 // included. The nine row ranges are fetched first, then each row's
 // candidates several at a time.
-template <uint32_t kNbrUnroll>
+//
+// With kDens, a fluid that is its scene's first material also forms the
+// density and lambda of its first solver iteration from the same hits, in
+// the same order (nothing moves between the list and that pass when the
+// world has no surface impulses and no late drag and lift).
+template <uint32_t kNbrUnroll, bool kDens>
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -34,7 +86,12 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const DevScene& S = scene_at(V, k);
   if (sub >= S.substeps) return;
   const DevFluid& F = V.fluids[f - 1];
-  const f3 xi = xyz(V.cur.xs[k]);
+  const float4 xi4 = V.cur.xs[k];
+  const f3 xi = xyz(xi4);
+  const bool dens = kDens && F.rank == 0 && S.iterations > 0;
+  float rho = 0.0f, gss = 0.0f;
+  f3 gs = mk(0.0f, 0.0f, 0.0f);
+  const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;
   const float hsq = F.hsq;
   int32_t cx, cy, cz;
   local_cell(S, xi, &cx, &cy, &cz, nullptr);
@@ -86,6 +143,8 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
       if (cnt < kMaxNbr) {
         *out = j;
         out += n;
+        if (kDens && dens)
+          lambda_terms(F, xi, xj, S.homog ? -S.homog_mass : __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
       }
       ++cnt;
     }
@@ -107,6 +166,7 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   cnt = min(cnt, kMaxNbr);
   V.ncount[k] = cnt;
   if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
+  if (kDens && dens) finish_lambda(V, S, F, k, xi4, rho, gs, gss);
 }
 
 // lambda.ts:41-71
@@ -127,33 +187,23 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
-#ifdef PF_EXACT_ROUNDING
-  auto one = [&](float4 xj, float qj) {
-    const float mass = code_mass(qj, F.rho0);
-    const f3 off = xi - xyz(xj);
-    const float rsq = dot(off, off);
-    rho += mass * poly6(rsq, F);
-    const f3 g = spiky_vec(off, rsq, F) * mass;
-    gs = gs + g;
-    gss += dot(g, g) * xj.w;
-  };
-#else
-  // The kernel constants leave the sums: rho = poly6 * sum m d^3,
-  // sum grad = -spiky * sum f r, sum |grad|^2 w = spiky^2 * sum f^2 r^2 w
-  // with f = m (h - r)^2 / r.
-  auto one = [&](float4 xj, float qj) {
-    const float mass = code_mass(qj, F.rho0);
-    const f3 off = xi - xyz(xj);
-    const float rsq = dot(off, off);
-    const float d = fmaxf(F.hsq - rsq, 0.0f);
-    rho += mass * (d * d * d);
-    const float f = spiky_shape(rsq, F) * mass;
-    gs = gs + off * f;
-    gss += (f * f) * (rsq * xj.w);
-  };
-#endif
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
   uint32_t m = 0;
+  if (S.homog) {
+    // one fluid, one mass: no mass gather
+    const float qh = -S.homog_mass;
+    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+      uint32_t j[kNbrUnroll];
+      float4 xj[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j[q]);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], qh, rho, gs, gss);
+    }
+    for (; m < cnt; ++m) lambda_terms(F, xi, __ldg(V.cur.xs + __ldg(nl + m * n)), qh, rho, gs, gss);
+  }
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
     uint32_t j[kNbrUnroll];
     float4 xj[kNbrUnroll];
@@ -166,27 +216,13 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
       bj[q] = __ldg(q_of + 2 * (size_t)j[q]);
     }
 #pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], bj[q]);
+    for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], bj[q], rho, gs, gss);
   }
   for (; m < cnt; ++m) {
     const uint32_t j = __ldg(nl + m * n);
-    one(__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j));
+    lambda_terms(F, xi, __ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
   }
-#ifndef PF_EXACT_ROUNDING
-  rho *= F.poly6;
-  gs = gs * -F.spiky;
-  gss *= F.spiky * F.spiky;
-#endif
-  V.cur.dens[k] = rho;
-  const float C = rho * F.inv_rho0 - 1.0f;
-  float lam = 0.0f;
-  if (C > 0.0f) {
-    const float gn = (dot(gs, gs) * xi4.w + gss) * (F.inv_rho0 * F.inv_rho0);
-    const float at = F.compliance / (S.dt * S.dt);
-    lam = -C / fmaxf(gn + at, 1e-20f);
-  }
-  V.lambda[k] = lam;
-  V.lm[k].x = lam;
+  finish_lambda(V, S, F, k, xi4, rho, gs, gss);
 }
 
 // positionDelta.ts:41-85 (the reaction on dynamic boundary neighbours goes
@@ -239,6 +275,25 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
     }
   };
   uint32_t m = 0;
+  if (S.homog) {
+    // one fluid, one mass: (x*, lambda) of a neighbour in one gather
+    const float qh = -S.homog_mass;
+    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+      uint32_t j[kNbrUnroll];
+      float4 xj[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.xl + j[q]);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], make_float2(xj[q].w, qh));
+    }
+    for (; m < cnt; ++m) {
+      const uint32_t j = __ldg(nl + m * n);
+      const float4 xj = __ldg(V.xl + j);
+      one(j, xj, make_float2(xj.w, qh));
+    }
+  }
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
     uint32_t j[kNbrUnroll];
     float4 xj[kNbrUnroll];
@@ -266,7 +321,7 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
 // velocity.ts:43-70: one walk over the list at the committed positions for
 // the XSPH change (Delta v = c sum V_j (v_j - v_i) W) and, with vorticity
 // confinement, the curl omega = sum V_j (v_i - v_j) x grad W.
-template <uint32_t kNbrUnroll>
+template <uint32_t kNbrUnroll, bool kBnd>
 __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
@@ -284,12 +339,20 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y: volume if > 0
+  // without boundaries in the world every neighbour has the fluid volume
   auto one = [&](float4 xj, float4 vj, float bvj) {
     const f3 off = xi - xyz(xj);
-    const float vol = bvj > 0.0f ? bvj : F.volume;
+    const float vol = (kBnd && bvj > 0.0f) ? bvj : F.volume;
     const float rsq = dot(off, off);
     if (vort) curl = curl + cross(vi - xyz(vj), spiky_vec(off, rsq, F)) * vol;
+#ifdef PF_EXACT_ROUNDING
     if (visc) sm = sm + ((xyz(vj) - vi) * poly6(rsq, F)) * vol;
+#else
+    if (visc) {
+      const float d = fmaxf(F.hsq - rsq, 0.0f);
+      sm = sm + (xyz(vj) - vi) * ((d * d * d) * vol);
+    }
+#endif
   };
   uint32_t m = 0;
   for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
@@ -302,15 +365,18 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
     for (uint32_t q = 0; q < kNbrUnroll; ++q) {
       xj[q] = __ldg(V.cur.x + j[q]);
       vj[q] = __ldg(V.cur.v + j[q]);
-      bj[q] = __ldg(q_of + 2 * (size_t)j[q]);
+      bj[q] = kBnd ? __ldg(q_of + 2 * (size_t)j[q]) : 0.0f;
     }
 #pragma unroll
     for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], vj[q], bj[q]);
   }
   for (; m < cnt; ++m) {
     const uint32_t j = __ldg(nl + m * n);
-    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), __ldg(q_of + 2 * (size_t)j));
+    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), kBnd ? __ldg(q_of + 2 * (size_t)j) : 0.0f);
   }
+#ifndef PF_EXACT_ROUNDING
+  sm = sm * F.poly6;
+#endif
   if (visc) V.dv[k] = with_w(sm * F.c_xsph, 0.0f);
   if (vort) V.vort[k] = with_w(curl, len(curl));
 }
