@@ -143,8 +143,6 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
       if (cnt < kMaxNbr) {
         *out = j;
         out += n;
-        if (kDens && dens)
-          lambda_terms(F, xi, xj, S.homog ? -S.homog_mass : __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
       }
       ++cnt;
     }
@@ -166,7 +164,32 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   cnt = min(cnt, kMaxNbr);
   V.ncount[k] = cnt;
   if (over) atomicOr(V.flags + scene_index(V, k) * kNumFlags + FLAG_NBR, 1u);
-  if (kDens && dens) finish_lambda(V, S, F, k, xi4, rho, gs, gss);
+  if (kDens && dens) {
+    // the density pass over the list just written (still in cache), in list
+    // order, outside the divergent walk
+    const uint32_t* __restrict__ nl = V.nbr + k;
+    const float qh = -S.homog_mass;
+    uint32_t m = 0;
+    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
+      uint32_t jj[kNbrUnroll];
+      float4 xj[kNbrUnroll];
+      float bj[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) jj[q] = nl[(m + q) * n];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+        xj[q] = __ldg(V.cur.xs + jj[q]);
+        bj[q] = S.homog ? qh : __ldg(q_of + 2 * (size_t)jj[q]);
+      }
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], bj[q], rho, gs, gss);
+    }
+    for (; m < cnt; ++m) {
+      const uint32_t j = nl[m * n];
+      lambda_terms(F, xi, __ldg(V.cur.xs + j), S.homog ? qh : __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
+    }
+    finish_lambda(V, S, F, k, xi4, rho, gs, gss);
+  }
 }
 
 // lambda.ts:41-71
