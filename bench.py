@@ -242,7 +242,7 @@ class BatchWorkload:
     # algorithmic bytes per fluid particle of the density+lambda stage:
     # read x* (16 B) and the boundary volume (4 B), write lambda and density (4 B each)
     LAMBDA_BYTES = 28
-    LAMBDA_TRAFFIC_PER_PARTICLE = 156.2e6 / 960_919
+    LAMBDA_TRAFFIC_PER_PARTICLE = 169.1e6 / 960_919
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -357,9 +357,9 @@ class BatchWorkload:
             "kernel_name": ("k_t_lambda" if tp.value == 1 else f"k_s_lambda<{tu.value}>")
             + " (density + lambda, one solver iteration)",
             "algorithmic_bytes": self.LAMBDA_BYTES * items.value,
-            # DRAM bytes of one launch: the per-fluid-particle figure of the ncu
-            # capture (profiles/k_s_lambda_batch32_full.md: 156.2 MB over 960,919
-            # fluid particles) scaled to this launch's fluid particles
+            # DRAM bytes of one launch: the per-fluid-particle figure of a full
+            # ncu capture of this pass on the 32-scene cut of the workload
+            # (169.1 MB over 960,919 fluid particles) scaled to this launch
             "traffic": self.LAMBDA_TRAFFIC_PER_PARTICLE * items.value if tp.value == 0 else None,
             "gpu_launches_per_step": launches,
             "clocks": clk,
@@ -531,20 +531,36 @@ class ServeWorkload:
 class SceneWorkload:
     """One plain scene stepped through pf_step: `dam` is the 5,000-particle
     dam break (2 substeps x 4 iterations, XSPH 0.01), `mixed` the 50,000-particle
-    fluid + 20 soft bodies + moving sphere scene (3 substeps x 4 iterations)."""
+    fluid + 20 soft bodies + moving sphere scene (3 substeps x 4 iterations),
+    `contacts` 50,000 particles of soft bodies (100 of ~500) piling up with
+    particle contacts on (3 x 4), `cloth` a 256 x 256 sheet with stretch,
+    bending and tether colours, drag and lift in a wind, and velocity
+    smoothing (2 x 4)."""
 
     metric = "particle-substeps/s (one plain scene)"
     unit = "particle-substeps/s"
     DT = 1.0 / 60.0
+    NAMES = {"dam": "dam_break_5k_S2_I4", "mixed": "mixed_50k_fluid30k_soft20x1k_sphere_S3_I4",
+             "contacts": "softbody_pile_50k_contacts_S3_I4",
+             "cloth": "cloth_256x256_bend_tether_aero_damping_S2_I4"}
 
     def __init__(self, which: str):
         self.which = which
-        self.name = {"dam": "dam_break_5k_S2_I4", "mixed": "mixed_50k_fluid30k_soft20x1k_sphere_S3_I4"}[which]
+        self.name = self.NAMES[which]
 
     def recipe(self):
         from pfsim import workloads as W
 
-        return W.dam_break(5000, seed=0) if self.which == "dam" else W.mixed_scene(50_000, seed=0)
+        if self.which == "dam":
+            return W.dam_break(5000, seed=0)
+        if self.which == "mixed":
+            return W.mixed_scene(50_000, seed=0)
+        if self.which == "contacts":
+            r = W.softbody_pile(50_000, seed=0, per_body=500)
+            r.loop.contact = True
+            return r
+        return W.cloth_sheet(256, seed=0, bend_compliance=1e-5, tethers=True, stretch_tolerance=0.06,
+                             wind=(0.8, 0.0, 1.5), drag=0.18, lift=0.02, damping=0.1)
 
     def run_gpu(self, steps: int, warmup: int) -> dict:
         import torch
@@ -584,8 +600,77 @@ class SceneWorkload:
                 "sample": f"the same scene, {steps} frames after one warm-up frame"}
 
 
+class MeshWorkload:
+    """Mesh -> particle setup on the GPU: `bake` bakes a 64 x 64 UV sphere
+    (3,968 triangles) into a 128^3 signed-distance grid (pf_bake_sdf);
+    `voxelize` fills a 48 x 24 torus (2,304 triangles) with particles of
+    radius 2.5 mm (pf_voxelize_mesh, about 1.9 M grid points). The unit is
+    grid-point x triangle tests per second (the brute force both the
+    reference and this build run)."""
+
+    unit = "point-triangle tests/s"
+
+    def __init__(self, which: str):
+        self.which = which
+        self.metric = {"bake": "SDF bake throughput", "voxelize": "voxeliser throughput"}[which]
+        self.name = {"bake": "bake_uv_sphere_64x64_res128", "voxelize": "voxelize_torus_48x24_r2.5mm"}[which]
+
+    def mesh(self):
+        from pfsim import mesh as M
+
+        return M.uv_sphere(0.5, 64, 64) if self.which == "bake" else M.torus(0.4, 0.12, 48, 24)
+
+    def run_gpu(self, steps: int, warmup: int) -> dict:
+        import torch
+
+        from pfsim import mesh as M
+
+        v, i = self.mesh()
+        n_tri = len(i) // 3
+        clocks = ClockSampler(torch.cuda.current_device())
+        if self.which == "bake":
+            run = lambda: M.bake_sdf(v, i, 128, None)
+            points = 128 ** 3
+        else:
+            run = lambda: M.voxelize_mesh(v, i, 0.0025)
+            ext = v.max(0).astype(np.float64) - v.min(0)
+            points = int(np.prod(np.maximum(1, np.ceil(ext / 0.005))))
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        clocks.start()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            run()
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / steps
+        return {"ms": sec * 1e3, "value": points * n_tri / sec, "points": points, "triangles": n_tri,
+                "clocks": clocks.stop()}
+
+    def run_cpu(self, threads: int, steps: int = 1) -> dict:
+        """The oracle (one thread) on a bounded sample: the same mesh at a
+        coarser grid (32^3 for the bake, 4x the particle radius for the
+        voxeliser)."""
+        from oracle import oracle as O
+
+        v, i = self.mesh()
+        n_tri = len(i) // 3
+        t0 = time.perf_counter()
+        if self.which == "bake":
+            O.bake_sdf(v, i, 32, None)
+            points = 32 ** 3
+        else:
+            O.voxelize_mesh(v, i, 0.01)
+            ext = v.max(0).astype(np.float64) - v.min(0)
+            points = int(np.prod(np.maximum(1, np.ceil(ext / 0.02))))
+        sec = time.perf_counter() - t0
+        return {"seconds_per_step": sec, "units_per_step": points * n_tri, "cores": 1,
+                "sample": f"the same mesh on a coarser grid ({points} points), one pass, one thread"}
+
+
 WORKLOADS = {"sort": SortWorkload, "batch": BatchWorkload, "serve": ServeWorkload, "dam": SceneWorkload,
-             "mixed": SceneWorkload}
+             "mixed": SceneWorkload, "contacts": SceneWorkload, "cloth": SceneWorkload, "bake": MeshWorkload,
+             "voxelize": MeshWorkload}
 
 
 # -------------------------------------------------------------- ranks ----
@@ -628,8 +713,10 @@ def main() -> None:
         wl = WORKLOADS["batch"](args.scenes)
     elif args.workload == "serve":
         wl = WORKLOADS["serve"](args.live)
-    elif args.workload in ("dam", "mixed"):
+    elif args.workload in SceneWorkload.NAMES:
         wl = SceneWorkload(args.workload)
+    elif args.workload in ("bake", "voxelize"):
+        wl = MeshWorkload(args.workload)
     else:
         wl = WORKLOADS[args.workload]()
 
@@ -667,7 +754,21 @@ def main() -> None:
         def barrier():
             pass
 
-    if args.workload in ("dam", "mixed"):
+    if args.workload in ("bake", "voxelize"):
+        res = wl.run_gpu(args.steps, warmup)
+        line = {"metric": wl.metric, "value": res["value"], "unit": wl.unit, "n_gpus": world, "steps": args.steps,
+                "warmup": warmup, "ms_per_step": res["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (procedural mesh)",
+                "config": {"workload": wl.name, "points": res["points"], "triangles": res["triangles"]},
+                "clocks": res["clocks"]}
+        if rank == 0 and not args.no_cpu_baseline:
+            cpu = wl.run_cpu(1)
+            line["cpu_baseline"] = {"value": cpu["units_per_step"] / cpu["seconds_per_step"], "unit": wl.unit,
+                                    "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    if args.workload in SceneWorkload.NAMES:
         res = wl.run_gpu(args.steps, warmup)
         line = {"metric": wl.metric, "value": res["value"], "unit": wl.unit, "n_gpus": world, "steps": args.steps,
                 "warmup": warmup, "ms_per_step": res["ms"], "higher_is_better": True, "scaling": "weak",

@@ -407,62 +407,24 @@ def pair_overlap(pos4: np.ndarray, two_r: float) -> float:
 
 
 def unit_cube_mesh(half=(0.5, 0.5, 0.5)):
-    """softbody-voxelize.test.ts:20-62: a box of 8 corners and 12 outward
-    triangles (half extents `half`; the unit cube by default)."""
-    hx, hy, hz = half
-    v = np.array([[-hx, -hy, -hz], [hx, -hy, -hz], [-hx, hy, -hz], [hx, hy, -hz],
-                  [-hx, -hy, hz], [hx, -hy, hz], [-hx, hy, hz], [hx, hy, hz]], np.float32)
-    i = np.array([0, 2, 1, 1, 2, 3, 4, 5, 6, 5, 7, 6, 0, 1, 4, 1, 5, 4, 2, 6, 3, 3, 6, 7, 0, 4, 2, 2, 4, 6,
-                  1, 3, 5, 3, 7, 5], np.uint32)
-    return v, i
+    """softbody-voxelize.test.ts:20-62: the box mesh of pfsim.mesh.box_mesh."""
+    from pfsim import mesh as M
+
+    return M.box_mesh(half)
 
 
 def uv_sphere(radius: float, stacks: int, slices: int):
-    """The tests' UV sphere (tests/_helpers/sdf-test-meshes.ts:23-87): poles
-    at +-radius, stacks - 1 rings of `slices` vertices, fans at the poles and
-    two triangles per quad; float32 vertices."""
-    n = 2 + (stacks - 1) * slices
-    pos = np.zeros((n, 3), np.float64)
-    pos[0] = (0, radius, 0)
-    pos[n - 1] = (0, -radius, 0)
-    for s in range(1, stacks):
-        phi = math.pi * s / stacks
-        y, rr = math.cos(phi) * radius, math.sin(phi) * radius
-        for k in range(slices):
-            th = 2 * math.pi * k / slices
-            pos[1 + (s - 1) * slices + k] = (math.cos(th) * rr, y, math.sin(th) * rr)
-    ring = lambda s: 1 + (s - 1) * slices
-    idx = []
-    for k in range(slices):
-        idx += [0, ring(1) + k, ring(1) + (k + 1) % slices]
-    for s in range(1, stacks - 1):
-        for k in range(slices):
-            kn = (k + 1) % slices
-            a, b, c, d = ring(s) + k, ring(s) + kn, ring(s + 1) + k, ring(s + 1) + kn
-            idx += [a, c, d, a, d, b]
-    last = ring(stacks - 1)
-    for k in range(slices):
-        idx += [last + k, n - 1, last + (k + 1) % slices]
-    return pos.astype(np.float32), np.array(idx, np.uint32)
+    """The tests' UV sphere (tests/_helpers/sdf-test-meshes.ts:23-87)."""
+    from pfsim import mesh as M
+
+    return M.uv_sphere(radius, stacks, slices)
 
 
 def torus(ring_radius: float, tube_radius: float, ring_segs: int, tube_segs: int):
-    """The tests' torus (sdf-test-meshes.ts:102-141) as float32 vertices."""
-    pos = np.zeros((ring_segs * tube_segs, 3), np.float64)
-    for i in range(ring_segs):
-        u = 2 * math.pi * i / ring_segs
-        for j in range(tube_segs):
-            v = 2 * math.pi * j / tube_segs
-            r = ring_radius + tube_radius * math.cos(v)
-            pos[i * tube_segs + j] = (r * math.cos(u), tube_radius * math.sin(v), r * math.sin(u))
-    idx = []
-    for i in range(ring_segs):
-        inx = (i + 1) % ring_segs
-        for j in range(tube_segs):
-            jn = (j + 1) % tube_segs
-            a, b, c, d = i * tube_segs + j, i * tube_segs + jn, inx * tube_segs + j, inx * tube_segs + jn
-            idx += [a, c, d, a, d, b]
-    return pos.astype(np.float32), np.array(idx, np.uint32)
+    """The tests' torus (sdf-test-meshes.ts:102-141)."""
+    from pfsim import mesh as M
+
+    return M.torus(ring_radius, tube_radius, ring_segs, tube_segs)
 
 
 def sample_field(data: np.ndarray, origin, voxel, p) -> float:
