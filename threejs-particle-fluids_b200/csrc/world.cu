@@ -195,85 +195,12 @@ __device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, P
   return st.p;
 }
 
-// The colliders of particle k's scene against its predicted position xs4
-// (w = inverse mass), their multipliers updated; the fixed-point position
-// changes summed in registers, on top of the ticks `start` that particle
-// contacts scattered for k, and applied. Returns whether xs4 changed.
-__device__ __forceinline__ bool collide_particle(const WorldView& V, const DevScene& S, uint32_t s, uint32_t k,
-                                                 float4& xs4, const pf_primitive* __restrict__ prims,
-                                                 int4 start = make_int4(0, 0, 0, 0)) {
-  const float w = xs4.w;
-  const bool moves = w > 0.0f;
-  const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
-  const f3 xstar = xyz(xs4);
-  const f3 disp = xstar - xyz(V.cur.x[k]);
-  const float clock = V.clocks[s];
-  const float radius = S.radius;
-  uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
-  bool any = (start.x | start.y | start.z) != 0;
-  for (uint32_t p = 0; p < n_prim; ++p) {
-    const pf_primitive& P = prims[p];
-    float phi;
-    f3 nrm;
-    prim_sdf(P, xstar, clock, &phi, &nrm);
-    if (!(phi < radius)) continue;
-    const f3 coldisp = prim_surface_velocity(P, xstar, clock) * S.dt;
-    const float depth = radius - phi;
-    float2 lam = V.plam[(size_t)k * V.prim_stride + p];
-    const float ln = lam.x + depth / w;
-    const f3 slip = disp - coldisp;
-    const f3 tang = slip - nrm * dot(slip, nrm);
-    const float tl = len(tang);
-    const bool sticks = tl > 1e-10f && (tl / w <= P.data1[3] * ln - lam.y);
-    const f3 push = nrm * depth;
-    const f3 c = sticks ? push - tang : push;
-    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
-    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
-    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
-    lam.x = ln;
-    lam.y = lam.y + (sticks ? tl / w : 0.0f);
-    V.plam[(size_t)k * V.prim_stride + p] = lam;
-    any = true;
-  }
-  // SDFCollider.ts:256-281: static surface, reach = radius + thickness
-  for (uint32_t q = 0; q < n_sdf; ++q) {
-    const DevSdf& G = V.sdfs[S.sdf_base + q];
-    float phi;
-    f3 g;
-    sdf_sample(V.sdf_half, G, xstar, &phi, &g);
-    const float gl = len(g);
-    if (!(gl > 1e-6f)) continue;
-    const float reach = radius + G.thickness;
-    if (!(phi < reach)) continue;
-    const f3 nrm = g / gl;
-    const float depth = reach - phi;
-    const size_t li = (size_t)k * V.prim_stride + S.prim_count + q;
-    float2 lam = V.plam[li];
-    const float ln = lam.x + depth / w;
-    const f3 tang = disp - nrm * dot(disp, nrm);
-    const float tl = len(tang);
-    const bool sticks = tl > 1e-10f && (tl / w <= G.mu_s * ln - lam.y);
-    const f3 push = nrm * depth;
-    const f3 c = sticks ? push - tang : push;
-    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
-    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
-    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
-    lam.x = ln;
-    lam.y = lam.y + (sticks ? tl / w : 0.0f);
-    V.plam[li] = lam;
-    any = true;
-  }
-  if (!any) return false;
-  bool sat = false;
-  const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
-  xs4 = with_w(xstar + c, w);
-  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_POS, 1u);
-  return true;
-}
-
 // positionDelta.ts:217-226, then the reaction accumulator's apply over the
 // covering range of the fluid's boundaries (FluidSystem.ts:280-287).
-__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+// With skip_homog the slots of single-fluid scenes of one mass are left to
+// the position pass, which applies them itself (k_s_delta).
+__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it,
+                                                        uint32_t skip_homog) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   // the slot's own loads go out first, so their latency overlaps the
   // primitive staging and the scene lookup
@@ -290,7 +217,7 @@ __global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t ra
   if (!live) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
-  if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0) return;
+  if (sub >= S.substeps || it >= S.iterations || S.fluid_count == 0 || (skip_homog && S.homog)) return;
   const uint32_t f = tag_fluid(tg);
   bool changed = false;
   if (f && V.fluids[f - 1].rank == rank) {
@@ -1009,9 +936,16 @@ size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // ================================================================ World ====
 
-World::~World() {
+void World::drop_graphs() {
   for (auto& g : graph_)
-    if (g) cudaGraphExecDestroy(g);
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+World::~World() {
+  drop_graphs();
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
@@ -2059,7 +1993,7 @@ void World::run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, u
   } else {
     // the list build formed rank 0's first density and lambda
     if (!(fuse_dens_ && r == 0 && it == 0)) PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, r, s, it);
-    PF_DELTA(V, r, s, it);
+    PF_DELTA(V, r, s, it, 1u);
   }
 }
 
@@ -2138,7 +2072,7 @@ pf_status World::tune() {
             [&] {
               if (kind == kSlotNbr) PF_NBR(V, 0u);
               else if (kind == kSlotLambda) PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
-              else if (kind == kSlotDelta) PF_DELTA(V, rank, 0u, 0u);
+              else if (kind == kSlotDelta) PF_DELTA(V, rank, 0u, 0u, 0u);
               else PF_XSPH(V, rank, 0u);
             },
             &t));
@@ -2295,7 +2229,11 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       }
       if (has_fluid) {
         run_fluid_lambda_delta(V, r, s, it);
-        launch_slots(k_fluid_apply, n_, stream_, V, r, s, it);
+        // on the slot path the position pass applies homogeneous scenes itself
+        const bool slot = tune_.path == 0;
+        bool rest = !slot;
+        for (auto& S : h_scenes_) rest = rest || (S.fluid_count && !S.homog);
+        if (rest) launch_slots(k_fluid_apply, n_, stream_, V, r, s, it, slot ? 1u : 0u);
       }
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
@@ -2429,7 +2367,12 @@ pf_status World::write(uint32_t scene, uint32_t field, const void* src, size_t b
   std::vector<uint32_t> ids(seg);
   PF_CUDA(cudaMemcpy(ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
   const StateBuf& B = buf_[parity_];
-  if (w_only) h_scenes_[scene].homog = 0;  // masses may differ from now on
+  if (w_only && h_scenes_[scene].homog) {
+    // masses may differ from now on; the captured steps launch the separate
+    // apply only for inhomogeneous scenes, so they are captured again
+    h_scenes_[scene].homog = 0;
+    drop_graphs();
+  }
   auto patch = [&](float4* dev) -> pf_status {
     std::vector<float4> tmp(seg);
     PF_CUDA(cudaMemcpy(tmp.data(), dev + S.seg_start, 16ull * seg, cudaMemcpyDeviceToHost));
@@ -2738,7 +2681,7 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
         break;
       case 2:
         if (tune_.path == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
-        else PF_DELTA(V, rank, 0u, 0u);
+        else PF_DELTA(V, rank, 0u, 0u, 0u);
         break;
       case 3:
         if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);

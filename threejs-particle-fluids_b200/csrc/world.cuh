@@ -431,6 +431,7 @@ class World {
   void set_tuning(const Tuning& t) {
     tune_ = t;
     tuned_ = true;
+    drop_graphs();  // captured launches depend on the path
   }
   size_t device_bytes() const { return bytes_; }
 
@@ -498,6 +499,7 @@ class World {
   // graph
   bool use_graph_ = false;
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  void drop_graphs();
   double graph_dt_ = -1;
   cudaStream_t stream_ = nullptr;
   // second stream for cloth-only scenes (fork/join inside each substep)

@@ -418,4 +418,80 @@ __device__ __forceinline__ void polar3(const float a[9], float r[9]) {
   r[8] = a[6] * s02 + a[7] * s12 + a[8] * s22;
 }
 
+// The colliders of particle k's scene against its predicted position xs4
+// (w = inverse mass), their multipliers updated; the fixed-point position
+// changes summed in registers, on top of the ticks `start` that particle
+// contacts scattered for k, and applied. Returns whether xs4 changed.
+__device__ __forceinline__ bool collide_particle(const WorldView& V, const DevScene& S, uint32_t s, uint32_t k,
+                                                 float4& xs4, const pf_primitive* __restrict__ prims,
+                                                 int4 start = make_int4(0, 0, 0, 0)) {
+  const float w = xs4.w;
+  const bool moves = w > 0.0f;
+  const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
+  const f3 xstar = xyz(xs4);
+  const f3 disp = xstar - xyz(V.cur.x[k]);
+  const float clock = V.clocks[s];
+  const float radius = S.radius;
+  uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
+  bool any = (start.x | start.y | start.z) != 0;
+  for (uint32_t p = 0; p < n_prim; ++p) {
+    const pf_primitive& P = prims[p];
+    float phi;
+    f3 nrm;
+    prim_sdf(P, xstar, clock, &phi, &nrm);
+    if (!(phi < radius)) continue;
+    const f3 coldisp = prim_surface_velocity(P, xstar, clock) * S.dt;
+    const float depth = radius - phi;
+    float2 lam = V.plam[(size_t)k * V.prim_stride + p];
+    const float ln = lam.x + depth / w;
+    const f3 slip = disp - coldisp;
+    const f3 tang = slip - nrm * dot(slip, nrm);
+    const float tl = len(tang);
+    const bool sticks = tl > 1e-10f && (tl / w <= P.data1[3] * ln - lam.y);
+    const f3 push = nrm * depth;
+    const f3 c = sticks ? push - tang : push;
+    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
+    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
+    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
+    lam.x = ln;
+    lam.y = lam.y + (sticks ? tl / w : 0.0f);
+    V.plam[(size_t)k * V.prim_stride + p] = lam;
+    any = true;
+  }
+  // SDFCollider.ts:256-281: static surface, reach = radius + thickness
+  for (uint32_t q = 0; q < n_sdf; ++q) {
+    const DevSdf& G = V.sdfs[S.sdf_base + q];
+    float phi;
+    f3 g;
+    sdf_sample(V.sdf_half, G, xstar, &phi, &g);
+    const float gl = len(g);
+    if (!(gl > 1e-6f)) continue;
+    const float reach = radius + G.thickness;
+    if (!(phi < reach)) continue;
+    const f3 nrm = g / gl;
+    const float depth = reach - phi;
+    const size_t li = (size_t)k * V.prim_stride + S.prim_count + q;
+    float2 lam = V.plam[li];
+    const float ln = lam.x + depth / w;
+    const f3 tang = disp - nrm * dot(disp, nrm);
+    const float tl = len(tang);
+    const bool sticks = tl > 1e-10f && (tl / w <= G.mu_s * ln - lam.y);
+    const f3 push = nrm * depth;
+    const f3 c = sticks ? push - tang : push;
+    tx += (uint32_t)to_ticks(c.x, S.pos_scale);
+    ty += (uint32_t)to_ticks(c.y, S.pos_scale);
+    tz += (uint32_t)to_ticks(c.z, S.pos_scale);
+    lam.x = ln;
+    lam.y = lam.y + (sticks ? tl / w : 0.0f);
+    V.plam[li] = lam;
+    any = true;
+  }
+  if (!any) return false;
+  bool sat = false;
+  const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
+  xs4 = with_w(xstar + c, w);
+  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_POS, 1u);
+  return true;
+}
+
 }  // namespace pf

@@ -19,6 +19,61 @@
 
 namespace pf {
 
+// Walks list entries [0, cnt) of one slot (its column starts at nl, entries
+// n apart), kU per round, in list order: a round gathers its neighbours'
+// records (fetch), then fetches the next round's list entries, then uses the
+// records (use). The list entries come from DRAM and the records mostly from
+// L1, so the next round's entries are in flight while this round's records
+// arrive and are used. The last partial round is one batch as well.
+// kFresh: the list was written by this same thread in this kernel, so its
+// entries are read with plain (coherent) loads.
+template <uint32_t kU, bool kFresh = false, typename Fetch, typename Use>
+__device__ __forceinline__ void walk_list(const uint32_t* __restrict__ nl, size_t n, uint32_t cnt, Fetch fetch,
+                                          Use use) {
+  using Rec = decltype(fetch(0u));
+  auto entry = [&](uint32_t m) { return kFresh ? nl[m * n] : __ldg(nl + m * n); };
+  uint32_t jn[kU];
+#pragma unroll
+  for (uint32_t q = 0; q < kU; ++q) jn[q] = q < cnt ? entry(q) : 0u;
+  uint32_t m = 0;
+  for (; m + kU <= cnt; m += kU) {
+    uint32_t j[kU];
+    Rec r[kU];
+#pragma unroll
+    for (uint32_t q = 0; q < kU; ++q) {
+      j[q] = jn[q];
+      r[q] = fetch(j[q]);
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kU; ++q)
+      if (m + kU + q < cnt) jn[q] = entry(m + kU + q);
+#pragma unroll
+    for (uint32_t q = 0; q < kU; ++q) use(j[q], r[q]);
+  }
+  if (m < cnt) {
+    Rec r[kU];
+#pragma unroll
+    for (uint32_t q = 0; q < kU; ++q)
+      if (m + q < cnt) r[q] = fetch(jn[q]);
+#pragma unroll
+    for (uint32_t q = 0; q < kU; ++q)
+      if (m + q < cnt) use(jn[q], r[q]);
+  }
+}
+
+// neighbour records gathered by the list walks
+struct NbrXQ {  // predicted position (w = inverse mass) and mass code
+  float4 x;
+  float q;
+};
+struct NbrXL {  // predicted position and (lambda, mass code)
+  float4 x;
+  float2 lq;
+};
+struct NbrXV {  // committed position, velocity (or curl) and mass code (or volume)
+  float4 x, v;
+  float q;
+};
 
 // lambda.ts:60-71: density and the multiplier from the neighbour sums (in
 // the fast path the kernel constants are applied here).
@@ -169,25 +224,11 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
     // order, outside the divergent walk
     const uint32_t* __restrict__ nl = V.nbr + k;
     const float qh = -S.homog_mass;
-    uint32_t m = 0;
-    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-      uint32_t jj[kNbrUnroll];
-      float4 xj[kNbrUnroll];
-      float bj[kNbrUnroll];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) jj[q] = nl[(m + q) * n];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) {
-        xj[q] = __ldg(V.cur.xs + jj[q]);
-        bj[q] = S.homog ? qh : __ldg(q_of + 2 * (size_t)jj[q]);
-      }
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], bj[q], rho, gs, gss);
-    }
-    for (; m < cnt; ++m) {
-      const uint32_t j = nl[m * n];
-      lambda_terms(F, xi, __ldg(V.cur.xs + j), S.homog ? qh : __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
-    }
+    const bool homog = S.homog;
+    walk_list<kNbrUnroll, true>(
+        nl, n, cnt,
+        [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), homog ? qh : __ldg(q_of + 2 * (size_t)j)}; },
+        [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
     finish_lambda(V, S, F, k, xi4, rho, gs, gss);
   }
 }
@@ -211,47 +252,30 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
-  uint32_t m = 0;
   if (S.homog) {
     // one fluid, one mass: no mass gather
     const float qh = -S.homog_mass;
-    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-      uint32_t j[kNbrUnroll];
-      float4 xj[kNbrUnroll];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j[q]);
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], qh, rho, gs, gss);
-    }
-    for (; m < cnt; ++m) lambda_terms(F, xi, __ldg(V.cur.xs + __ldg(nl + m * n)), qh, rho, gs, gss);
-  }
-  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-    uint32_t j[kNbrUnroll];
-    float4 xj[kNbrUnroll];
-    float bj[kNbrUnroll];
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
-      xj[q] = __ldg(V.cur.xs + j[q]);
-      bj[q] = __ldg(q_of + 2 * (size_t)j[q]);
-    }
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) lambda_terms(F, xi, xj[q], bj[q], rho, gs, gss);
-  }
-  for (; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
-    lambda_terms(F, xi, __ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j), rho, gs, gss);
+    walk_list<kNbrUnroll>(
+        nl, n, cnt, [&](uint32_t j) { return __ldg(V.cur.xs + j); },
+        [&](uint32_t, const float4& xj) { lambda_terms(F, xi, xj, qh, rho, gs, gss); });
+  } else {
+    walk_list<kNbrUnroll>(
+        nl, n, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j)}; },
+        [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
   }
   finish_lambda(V, S, F, k, xi4, rho, gs, gss);
 }
 
 // positionDelta.ts:41-85 (the reaction on dynamic boundary neighbours goes
 // into the fixed-point reaction sums by slot).
+//
+// With `apply`, the slots of single-fluid scenes of one mass (S.homog) also
+// take the apply of k_fluid_apply in the same thread: x* += delta, then the
+// scene's colliders when they follow the fluid. Their neighbours' positions
+// come from xl (written by the density pass), not from x*, so x* of the slot
+// is rewritten in place; the arithmetic is that of the separate apply.
 template <uint32_t kNbrUnroll, bool kReact>
-__global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+__global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it, uint32_t apply) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
   const uint32_t f = tag_fluid(V.cur.tag[k]);
@@ -297,48 +321,31 @@ __global__ void k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it)
       if (in) acc_add(V.acc_react, j, g * (-(li / F.rho0) * (F.rho0 * bvj) * xj.w), F.react_scale);
     }
   };
-  uint32_t m = 0;
   if (S.homog) {
     // one fluid, one mass: (x*, lambda) of a neighbour in one gather
     const float qh = -S.homog_mass;
-    for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-      uint32_t j[kNbrUnroll];
-      float4 xj[kNbrUnroll];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.xl + j[q]);
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], make_float2(xj[q].w, qh));
-    }
-    for (; m < cnt; ++m) {
-      const uint32_t j = __ldg(nl + m * n);
-      const float4 xj = __ldg(V.xl + j);
-      one(j, xj, make_float2(xj.w, qh));
-    }
-  }
-  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-    uint32_t j[kNbrUnroll];
-    float4 xj[kNbrUnroll];
-    float2 lq[kNbrUnroll];
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
-      xj[q] = __ldg(V.cur.xs + j[q]);
-      lq[q] = __ldg(V.lm + j[q]);
-    }
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(j[q], xj[q], lq[q]);
-  }
-  for (; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
-    one(j, __ldg(V.cur.xs + j), __ldg(V.lm + j));
+    walk_list<kNbrUnroll>(
+        nl, n, cnt, [&](uint32_t j) { return __ldg(V.xl + j); },
+        [&](uint32_t j, const float4& xj) { one(j, xj, make_float2(xj.w, qh)); });
+  } else {
+    walk_list<kNbrUnroll>(
+        nl, n, cnt, [&](uint32_t j) { return NbrXL{__ldg(V.cur.xs + j), __ldg(V.lm + j)}; },
+        [&](uint32_t j, const NbrXL& r) { one(j, r.x, r.lq); });
   }
 #ifndef PF_EXACT_ROUNDING
   sum = sum * -F.spiky;
 #endif
-  V.dx[k] = with_w((sum / F.rho0) * xi4.w, 0.0f);
+  const float4 d = with_w((sum / F.rho0) * xi4.w, 0.0f);
+  if (apply && S.homog) {
+    float4 x = xi4;
+    x.x += d.x;
+    x.y += d.y;
+    x.z += d.z;
+    if (S.collide_rank1 == rank + 1) collide_particle(V, S, scene_index(V, k), k, x, V.prims + S.prim_base);
+    V.cur.xs[k] = x;
+    return;
+  }
+  V.dx[k] = d;
 }
 
 // velocity.ts:43-70: one walk over the list at the committed positions for
@@ -377,26 +384,10 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
     }
 #endif
   };
-  uint32_t m = 0;
-  for (; m + kNbrUnroll <= cnt; m += kNbrUnroll) {
-    uint32_t j[kNbrUnroll];
-    float4 xj[kNbrUnroll], vj[kNbrUnroll];
-    float bj[kNbrUnroll];
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) j[q] = __ldg(nl + (m + q) * n);
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) {
-      xj[q] = __ldg(V.cur.x + j[q]);
-      vj[q] = __ldg(V.cur.v + j[q]);
-      bj[q] = kBnd ? __ldg(q_of + 2 * (size_t)j[q]) : 0.0f;
-    }
-#pragma unroll
-    for (uint32_t q = 0; q < kNbrUnroll; ++q) one(xj[q], vj[q], bj[q]);
-  }
-  for (; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
-    one(__ldg(V.cur.x + j), __ldg(V.cur.v + j), kBnd ? __ldg(q_of + 2 * (size_t)j) : 0.0f);
-  }
+  walk_list<kNbrUnroll>(
+      nl, n, cnt,
+      [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), __ldg(V.cur.v + j), kBnd ? __ldg(q_of + 2 * (size_t)j) : 0.0f}; },
+      [&](uint32_t, const NbrXV& r) { one(r.x, r.v, r.q); });
 #ifndef PF_EXACT_ROUNDING
   sm = sm * F.poly6;
 #endif
@@ -422,12 +413,13 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
-    if (__ldg(V.cur.bv + j) > 0.0f) continue;
-    const f3 off = xi - xyz(__ldg(V.cur.x + j));
-    eta = eta + spiky_vec(off, dot(off, off), F) * ((V.vort[j].w - wi) * F.volume);
-  }
+  walk_list<kNbrUnroll>(
+      nl, n, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
+      [&](uint32_t, const NbrXV& r) {
+        if (r.q > 0.0f) return;
+        const f3 off = xi - xyz(r.x);
+        eta = eta + spiky_vec(off, dot(off, off), F) * ((r.v.w - wi) * F.volume);
+      });
   V.dx[k] = with_w(eta, 0.0f);
 }
 
@@ -448,12 +440,12 @@ __global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t cnt = V.ncount[k];
   const size_t n = V.n;
   const uint32_t* __restrict__ nl = V.nbr + k;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
-    const float bvj = __ldg(V.cur.bv + j);
-    const f3 off = xi - xyz(__ldg(V.cur.xs + j));
-    sum = sum + spiky_vec(off, dot(off, off), F) * (bvj > 0.0f ? bvj : F.volume);
-  }
+  walk_list<kNbrUnroll>(
+      nl, n, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
+      [&](uint32_t, const NbrXQ& r) {
+        const f3 off = xi - xyz(r.x);
+        sum = sum + spiky_vec(off, dot(off, off), F) * (r.q > 0.0f ? r.q : F.volume);
+      });
   V.normal[k] = with_w(sum * F.h, 0.0f);
 }
 
