@@ -2495,14 +2495,15 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
       std::fill(o, o + (size_t)cap * kMaxNbr, 0xffffffffu);
       if (!base_.nbr16) return PF_OK;
       if (tune_.path == 0) {
-        std::vector<uint32_t> colw(seg), seg_ids(seg);
+        // segments start on a warp boundary, so their list blocks are one range
+        std::vector<uint32_t> all((size_t)seg * kMaxNbr), seg_ids(seg);
         PF_CUDA(cudaMemcpy(seg_ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+        PF_CUDA(cudaMemcpy(all.data(), base_.nbr + nbr_col(S.seg_start), 4ull * seg * kMaxNbr, cudaMemcpyDeviceToHost));
         for (uint32_t m = 0; m < kMaxNbr; ++m) {
-          PF_CUDA(cudaMemcpy(colw.data(), base_.nbr + (size_t)m * n_ + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
           for (uint32_t k = 0; k < seg; ++k) {
             const uint32_t id = ids[k] - S.seg_start;
             if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k]) continue;
-            const uint32_t j = colw[k];  // a neighbour is a slot of the same scene's segment
+            const uint32_t j = all[nbr_col(k) + (size_t)m * kNbrStride];  // a slot of the same scene's segment
             o[(size_t)id * kMaxNbr + m] = (j >= S.seg_start && j < S.seg_end) ? seg_ids[j - S.seg_start] - S.seg_start
                                                                                : 0xfffffffeu;
           }

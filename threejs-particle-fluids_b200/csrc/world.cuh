@@ -32,6 +32,14 @@ namespace pf {
 
 constexpr uint32_t kSegAlign = 256;
 constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts:14)
+// The slot path's neighbour list is blocked by warp: slot k's m-th entry is
+// word nbr_col(k) + m * kNbrStride, so a warp's m-th entries are one 128-byte
+// line and its successive entries successive lines of one 8 KB block.
+constexpr uint32_t kNbrStride = 32;
+static_assert(kSegAlign % kNbrStride == 0, "a scene's segment starts on a list block");
+__host__ __device__ __forceinline__ size_t nbr_col(size_t k) {
+  return (k >> 5) * (size_t)kMaxNbr * kNbrStride + (k & 31);
+}
 constexpr uint32_t kBlock = 256;
 constexpr uint32_t kMaxContacts = 32;  // contact pairs kept per emitting particle per substep
 
@@ -266,7 +274,7 @@ struct WorldView {
   uint32_t* perm;     // new slot -> id (sort output)
   uint32_t* cstart;
   uint32_t* ccount;
-  uint32_t* nbr;      // kMaxNbr * n, column-major: slot of each neighbour (slot path)
+  uint32_t* nbr;      // kMaxNbr * n, blocked by warp (nbr_col): slot of each neighbour (slot path)
   uint16_t* nbr16;    // the same storage, kMaxNbr * n halfwords: halo index of each neighbour (tile path)
   uint32_t* ncount;
   uint32_t* slot_tile;  // tile of each slot (this substep)

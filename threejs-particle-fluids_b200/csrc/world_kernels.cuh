@@ -429,7 +429,17 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
   const bool moves = w > 0.0f;
   const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
   const f3 xstar = xyz(xs4);
-  const f3 disp = xstar - xyz(V.cur.x[k]);
+  // the displacement this substep, read on the first contact only (most
+  // particles touch no collider)
+  f3 disp_v = mk(0.0f, 0.0f, 0.0f);
+  bool have_disp = false;
+  auto disp = [&]() {
+    if (!have_disp) {
+      disp_v = xstar - xyz(V.cur.x[k]);
+      have_disp = true;
+    }
+    return disp_v;
+  };
   const float clock = V.clocks[s];
   const float radius = S.radius;
   uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
@@ -444,7 +454,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     const float depth = radius - phi;
     float2 lam = V.plam[(size_t)k * V.prim_stride + p];
     const float ln = lam.x + depth / w;
-    const f3 slip = disp - coldisp;
+    const f3 slip = disp() - coldisp;
     const f3 tang = slip - nrm * dot(slip, nrm);
     const float tl = len(tang);
     const bool sticks = tl > 1e-10f && (tl / w <= P.data1[3] * ln - lam.y);
@@ -473,7 +483,8 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     const size_t li = (size_t)k * V.prim_stride + S.prim_count + q;
     float2 lam = V.plam[li];
     const float ln = lam.x + depth / w;
-    const f3 tang = disp - nrm * dot(disp, nrm);
+    const f3 dp = disp();
+    const f3 tang = dp - nrm * dot(dp, nrm);
     const float tl = len(tang);
     const bool sticks = tl > 1e-10f && (tl / w <= G.mu_s * ln - lam.y);
     const f3 push = nrm * depth;

@@ -3,8 +3,9 @@
 // Each thread owns one particle (slot k, cell order) and gathers its
 // neighbours' state straight from the slot arrays; particles are in cell
 // order, so a warp's gathers fall on a few hundred consecutive slots that L1
-// holds. The neighbour list stores slots (32 bits), column-major, so a warp
-// reads its m-th entries as one coalesced line. The loops fetch the list and
+// holds. The neighbour list stores slots (32 bits) blocked by warp (nbr_col),
+// so a warp reads its m-th entries as one coalesced line and its next
+// entries from the next line. The loops fetch the list and
 // the neighbours several at a time before using them: independent loads in
 // flight per round instead of a dependent load per neighbour, with the sums
 // still formed in list order.
@@ -19,8 +20,16 @@
 
 namespace pf {
 
+// A list entry (read-only for the kernel). A miss fetches 256 bytes into L2:
+// with the warp-blocked layout that is the warp's next line of entries too.
+__device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
+  uint32_t v;
+  asm("ld.global.nc.L2::256B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 // Walks list entries [0, cnt) of one slot (its column starts at nl, entries
-// n apart), kU per round, in list order: a round gathers its neighbours'
+// `stride` words apart), kU per round, in list order: a round gathers its neighbours'
 // records (fetch), then fetches the next round's list entries, then uses the
 // records (use). The list entries come from DRAM and the records mostly from
 // L1, so the next round's entries are in flight while this round's records
@@ -28,10 +37,10 @@ namespace pf {
 // kFresh: the list was written by this same thread in this kernel, so its
 // entries are read with plain (coherent) loads.
 template <uint32_t kU, bool kFresh = false, typename Fetch, typename Use>
-__device__ __forceinline__ void walk_list(const uint32_t* __restrict__ nl, size_t n, uint32_t cnt, Fetch fetch,
+__device__ __forceinline__ void walk_list(const uint32_t* __restrict__ nl, uint32_t stride, uint32_t cnt, Fetch fetch,
                                           Use use) {
   using Rec = decltype(fetch(0u));
-  auto entry = [&](uint32_t m) { return kFresh ? nl[m * n] : __ldg(nl + m * n); };
+  auto entry = [&](uint32_t m) { return kFresh ? nl[m * stride] : ld_entry(nl + m * stride); };
   uint32_t jn[kU];
 #pragma unroll
   for (uint32_t q = 0; q < kU; ++q) jn[q] = q < cnt ? entry(q) : 0u;
@@ -191,13 +200,12 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   // stored (as the reference's list keeps them) and any further hit only
   // marks the overflow.
   uint32_t cnt = 0;
-  const size_t n = V.n;
-  uint32_t* __restrict__ out = V.nbr + k;
+  uint32_t* __restrict__ out = V.nbr + nbr_col(k);
   auto test = [&](uint32_t j, float4 xj) {
     if (dot_rn(xi - xyz(xj)) < hsq) {
       if (cnt < kMaxNbr) {
         *out = j;
-        out += n;
+        out += kNbrStride;
       }
       ++cnt;
     }
@@ -206,6 +214,8 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   for (int r = 0; r < 9; ++r) {
     uint32_t j = rs[r];
     const uint32_t e = re[r];
+    // whole rounds, then the row's last 1 to kNbrUnroll - 1 candidates as
+    // one guarded round (their loads in flight together)
     for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
       float4 xj[kNbrUnroll];
 #pragma unroll
@@ -213,7 +223,15 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
 #pragma unroll
       for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
     }
-    for (; j < e; ++j) test(j, __ldg(V.cur.xs + j));
+    if (j < e) {
+      float4 xj[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q)
+        if (j + q < e) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q)
+        if (j + q < e) test(j + q, xj[q]);
+    }
   }
   const bool over = cnt > kMaxNbr;
   cnt = min(cnt, kMaxNbr);
@@ -222,11 +240,11 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   if (kDens && dens) {
     // the density pass over the list just written (still in cache), in list
     // order, outside the divergent walk
-    const uint32_t* __restrict__ nl = V.nbr + k;
+    const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
     const float qh = -S.homog_mass;
     const bool homog = S.homog;
     walk_list<kNbrUnroll, true>(
-        nl, n, cnt,
+        nl, kNbrStride, cnt,
         [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), homog ? qh : __ldg(q_of + 2 * (size_t)j)}; },
         [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
     finish_lambda(V, S, F, k, xi4, rho, gs, gss);
@@ -249,18 +267,17 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   float rho = 0.0f, gss = 0.0f;
   f3 gs = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
   if (S.homog) {
     // one fluid, one mass: no mass gather
     const float qh = -S.homog_mass;
     walk_list<kNbrUnroll>(
-        nl, n, cnt, [&](uint32_t j) { return __ldg(V.cur.xs + j); },
+        nl, kNbrStride, cnt, [&](uint32_t j) { return __ldg(V.cur.xs + j); },
         [&](uint32_t, const float4& xj) { lambda_terms(F, xi, xj, qh, rho, gs, gss); });
   } else {
     walk_list<kNbrUnroll>(
-        nl, n, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j)}; },
+        nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j)}; },
         [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
   }
   finish_lambda(V, S, F, k, xi4, rho, gs, gss);
@@ -293,8 +310,7 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
   const bool multi = S.fluid_count > 1;
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   auto one = [&](uint32_t j, float4 xj, float2 lq) {
     const float bvj = lq.y;
     const float lj = (multi && tag_fluid(__ldg(V.cur.tag + j)) != f) ? 0.0f : lq.x;
@@ -325,11 +341,11 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
     // one fluid, one mass: (x*, lambda) of a neighbour in one gather
     const float qh = -S.homog_mass;
     walk_list<kNbrUnroll>(
-        nl, n, cnt, [&](uint32_t j) { return __ldg(V.xl + j); },
+        nl, kNbrStride, cnt, [&](uint32_t j) { return __ldg(V.xl + j); },
         [&](uint32_t j, const float4& xj) { one(j, xj, make_float2(xj.w, qh)); });
   } else {
     walk_list<kNbrUnroll>(
-        nl, n, cnt, [&](uint32_t j) { return NbrXL{__ldg(V.cur.xs + j), __ldg(V.lm + j)}; },
+        nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXL{__ldg(V.cur.xs + j), __ldg(V.lm + j)}; },
         [&](uint32_t j, const NbrXL& r) { one(j, r.x, r.lq); });
   }
 #ifndef PF_EXACT_ROUNDING
@@ -366,8 +382,7 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const f3 vi = xyz(V.cur.v[k]);
   f3 sm = mk(0.0f, 0.0f, 0.0f), curl = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y: volume if > 0
   // without boundaries in the world every neighbour has the fluid volume
   auto one = [&](float4 xj, float4 vj, float bvj) {
@@ -385,7 +400,7 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
 #endif
   };
   walk_list<kNbrUnroll>(
-      nl, n, cnt,
+      nl, kNbrStride, cnt,
       [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), __ldg(V.cur.v + j), kBnd ? __ldg(q_of + 2 * (size_t)j) : 0.0f}; },
       [&](uint32_t, const NbrXV& r) { one(r.x, r.v, r.q); });
 #ifndef PF_EXACT_ROUNDING
@@ -411,10 +426,9 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
   const float wi = V.vort[k].w;
   f3 eta = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   walk_list<kNbrUnroll>(
-      nl, n, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
+      nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXV& r) {
         if (r.q > 0.0f) return;
         const f3 off = xi - xyz(r.x);
@@ -438,10 +452,9 @@ __global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
   const f3 xi = xyz(V.cur.xs[k]);
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   walk_list<kNbrUnroll>(
-      nl, n, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
+      nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXQ& r) {
         const f3 off = xi - xyz(r.x);
         sum = sum + spiky_vec(off, dot(off, off), F) * (r.q > 0.0f ? r.q : F.volume);
@@ -483,10 +496,9 @@ __global__ void k_s_impulses(WorldView V, uint32_t rank, uint32_t sub) {
   const float rhoi = V.cur.dens[k];
   const float dt = S.dt;
   const uint32_t cnt = V.ncount[k];
-  const size_t n = V.n;
-  const uint32_t* __restrict__ nl = V.nbr + k;
+  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
   for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * n);
+    const uint32_t j = __ldg(nl + m * kNbrStride);
     const f3 off = xi - xyz(__ldg(V.cur.xs + j));
     if (F.has_st) {
       const uint32_t idj = V.ids[j];
