@@ -129,7 +129,9 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   // lambda is read for every neighbour, fluid or not (positionDelta.ts:193),
   // and is zero for particles no fluid solves; slots change owners here.
   V.lambda[k] = 0.0f;
-  for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
+  // the first 32 collider multipliers start at zero through the mask
+  V.cmask[k] = 0u;
+  for (uint32_t p = 32; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
   if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
   if (V.acc_imp) V.acc_imp[k] = make_int4(0, 0, 0, 0);
@@ -139,7 +141,8 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
 __global__ void __launch_bounds__(kBlock) k_reset_sums(WorldView V) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= V.n) return;
-  for (uint32_t p = 0; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
+  V.cmask[k] = 0u;
+  for (uint32_t p = 32; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
   if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
 }
@@ -199,7 +202,7 @@ __device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, P
 // covering range of the fluid's boundaries (FluidSystem.ts:280-287).
 // With skip_homog the slots of single-fluid scenes of one mass are left to
 // the position pass, which applies them itself (k_s_delta).
-__global__ void __launch_bounds__(kBlock) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it,
+__global__ void __launch_bounds__(kBlock, 4) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it,
                                                         uint32_t skip_homog) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   // the slot's own loads go out first, so their latency overlaps the
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t ran
 // adds to its own particle, so the sum of rounded ticks is formed in
 // registers. Scenes whose last material is a fluid run this inside the
 // fluid's apply instead (collide_rank1).
-__global__ void __launch_bounds__(kBlock) k_collide(WorldView V, uint32_t sub, uint32_t it) {
+__global__ void __launch_bounds__(kBlock, 4) k_collide(WorldView V, uint32_t sub, uint32_t it) {
   __shared__ PrimStage st;
   const pf_primitive* prims = stage_prims(V, st);
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -308,14 +311,21 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
   if ((S.prim_count + S.sdf_count == 0 && !S.contact) || sub >= S.substeps) return;
-  const float4 xs4 = V.cur.xs[k];
-  const float w = xs4.w;
   // contact friction (k_con_friction) scattered its velocity ticks first
   int4 start = make_int4(0, 0, 0, 0);
   if (S.contact) {
     start = V.acc_con[k];
     if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
   }
+  // colliders that never touched the particle this substep have zero
+  // multipliers and add nothing
+  const uint32_t mask = V.cmask[k];
+  if (!mask && S.prim_count + S.sdf_count <= 32 && !(start.x | start.y | start.z)) return;
+  auto ln_at = [&](uint32_t i) {
+    return (i < 32 && !((mask >> i) & 1u)) ? 0.0f : V.plam[(size_t)k * V.prim_stride + i].x;
+  };
+  const float4 xs4 = V.cur.xs[k];
+  const float w = xs4.w;
   const bool moves = w > 0.0f;
   const uint32_t n_prim = moves ? S.prim_count : 0u, n_sdf = moves ? S.sdf_count : 0u;
   const f3 xstar = xyz(xs4);
@@ -324,7 +334,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
   bool any = (start.x | start.y | start.z) != 0;
   for (uint32_t p = 0; p < n_prim; ++p) {
-    const float ln = V.plam[(size_t)k * V.prim_stride + p].x;
+    const float ln = ln_at(p);
     if (!(ln > 0.0f)) continue;
     const pf_primitive& P = prims[p];
     float phi;
@@ -347,7 +357,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   }
   // SDFCollider.ts:283-299 against a static surface
   for (uint32_t q = 0; q < n_sdf; ++q) {
-    const float ln = V.plam[(size_t)k * V.prim_stride + S.prim_count + q].x;
+    const float ln = ln_at(S.prim_count + q);
     if (!(ln > 0.0f)) continue;
     const DevSdf& G = V.sdfs[S.sdf_base + q];
     float phi;
@@ -1610,6 +1620,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.normal = any_imp_ ? cv.take<float4>(N) : nullptr;
     base_.acc_imp = any_imp_ ? cv.take<int4>(N) : nullptr;
     base_.plam = cv.take<float2>(N * P);
+    base_.cmask = cv.take<uint32_t>(N);
     base_.acc_react = any_react_ ? cv.take<int4>(N) : nullptr;
     base_.acc_soft = any_soft_local_ ? cv.take<int4>(N) : nullptr;
     base_.softs = cv.take<DevSoft>(h_softs_.size());

@@ -297,6 +297,7 @@ struct WorldView {
   float4* normal;     // scaled colour-field normal per slot (surface tension)
   int4* acc_imp;      // fixed-point velocity changes of surface tension and adhesion
   float2* plam;       // (lambda_n, lambda_t) per slot x primitive
+  uint32_t* cmask;    // per slot: bit p set once collider p < 32 touched it this substep (plam entry valid)
   int4* acc_react;    // fixed-point reaction sums per slot
   int4* acc_soft;     // fixed-point shape-matching sums per slot
   // soft bodies (by id unless noted)

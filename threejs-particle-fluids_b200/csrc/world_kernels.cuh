@@ -440,6 +440,17 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     }
     return disp_v;
   };
+  // collider multipliers: entry i < 32 is valid once bit i of the slot's
+  // mask is set this substep (zero before)
+  uint32_t mask = n_prim + n_sdf ? V.cmask[k] : 0u;
+  const uint32_t mask0 = mask;
+  auto lam_at = [&](uint32_t i) {
+    return (i >= 32 || ((mask >> i) & 1u)) ? V.plam[(size_t)k * V.prim_stride + i] : make_float2(0.0f, 0.0f);
+  };
+  auto lam_put = [&](uint32_t i, float2 lam) {
+    V.plam[(size_t)k * V.prim_stride + i] = lam;
+    if (i < 32) mask |= 1u << i;
+  };
   const float clock = V.clocks[s];
   const float radius = S.radius;
   uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
@@ -452,7 +463,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     if (!(phi < radius)) continue;
     const f3 coldisp = prim_surface_velocity(P, xstar, clock) * S.dt;
     const float depth = radius - phi;
-    float2 lam = V.plam[(size_t)k * V.prim_stride + p];
+    float2 lam = lam_at(p);
     const float ln = lam.x + depth / w;
     const f3 slip = disp() - coldisp;
     const f3 tang = slip - nrm * dot(slip, nrm);
@@ -465,7 +476,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     tz += (uint32_t)to_ticks(c.z, S.pos_scale);
     lam.x = ln;
     lam.y = lam.y + (sticks ? tl / w : 0.0f);
-    V.plam[(size_t)k * V.prim_stride + p] = lam;
+    lam_put(p, lam);
     any = true;
   }
   // SDFCollider.ts:256-281: static surface, reach = radius + thickness
@@ -480,8 +491,8 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     if (!(phi < reach)) continue;
     const f3 nrm = g / gl;
     const float depth = reach - phi;
-    const size_t li = (size_t)k * V.prim_stride + S.prim_count + q;
-    float2 lam = V.plam[li];
+    const uint32_t li = S.prim_count + q;
+    float2 lam = lam_at(li);
     const float ln = lam.x + depth / w;
     const f3 dp = disp();
     const f3 tang = dp - nrm * dot(dp, nrm);
@@ -494,9 +505,10 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     tz += (uint32_t)to_ticks(c.z, S.pos_scale);
     lam.x = ln;
     lam.y = lam.y + (sticks ? tl / w : 0.0f);
-    V.plam[li] = lam;
+    lam_put(li, lam);
     any = true;
   }
+  if (mask != mask0) V.cmask[k] = mask;
   if (!any) return false;
   bool sat = false;
   const f3 c = ticks_change((int)tx, (int)ty, (int)tz, S.pos_inv, &sat);
