@@ -28,6 +28,18 @@ __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
   return v;
 }
 
+// Before a walk: one lane of the warp has its list block's first max(cnt)
+// lines (128 bytes each, contiguous) fetched into L2 in one bulk prefetch,
+// so the later rounds' entries come from L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_list(const WorldView& V, uint32_t k, uint32_t cnt) {
+  const uint32_t act = __activemask();
+  const uint32_t most = __reduce_max_sync(act, cnt);
+  if (most && (threadIdx.x & 31u) == (uint32_t)(__ffs(act) - 1)) {
+    const uint32_t* base = V.nbr + nbr_col(k & ~31u);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base), "r"(most * kNbrStride * 4u) : "memory");
+  }
+}
+
 // Walks list entries [0, cnt) of one slot (its column starts at nl, entries
 // `stride` words apart), kU per round, in list order: a round gathers its neighbours'
 // records (fetch), then fetches the next round's list entries, then uses the
@@ -268,6 +280,7 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   f3 gs = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  prefetch_list(V, k, cnt);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
   if (S.homog) {
     // one fluid, one mass: no mass gather
@@ -311,6 +324,7 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  prefetch_list(V, k, cnt);
   auto one = [&](uint32_t j, float4 xj, float2 lq) {
     const float bvj = lq.y;
     const float lj = (multi && tag_fluid(__ldg(V.cur.tag + j)) != f) ? 0.0f : lq.x;
@@ -383,6 +397,7 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   f3 sm = mk(0.0f, 0.0f, 0.0f), curl = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  prefetch_list(V, k, cnt);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y: volume if > 0
   // without boundaries in the world every neighbour has the fluid volume
   auto one = [&](float4 xj, float4 vj, float bvj) {
@@ -427,6 +442,7 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
   f3 eta = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  prefetch_list(V, k, cnt);
   walk_list<kNbrUnroll>(
       nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXV& r) {
@@ -453,6 +469,7 @@ __global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
   const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  prefetch_list(V, k, cnt);
   walk_list<kNbrUnroll>(
       nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXQ& r) {
