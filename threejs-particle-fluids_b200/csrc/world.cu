@@ -304,23 +304,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_collide(WorldView V, uint32_t sub
 // PrimitiveSet.ts:367-398 with collider.ts:96-118, fused with the velocity
 // accumulator's apply (loop.ts:226-230).
 __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  // A slot has work when a collider touched it this substep (the others'
+  // multipliers are zero and add nothing) or contact friction
+  // (k_con_friction) scattered velocity ticks for it first. A block without
+  // any leaves before staging its scene's primitives.
+  bool work = false;
+  uint32_t s = 0, mask = 0;
+  int4 start = make_int4(0, 0, 0, 0);
+  if (k < V.n) {
+    s = scene_index(V, k);
+    const DevScene& S0 = V.scenes[s];
+    if ((S0.prim_count + S0.sdf_count > 0 || S0.contact) && sub < S0.substeps) {
+      if (S0.contact) {
+        start = V.acc_con[k];
+        if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
+      }
+      mask = V.cmask[k];
+      work = mask || S0.prim_count + S0.sdf_count > 32 || (start.x | start.y | start.z);
+    }
+  }
+  if (!__syncthreads_or(work)) return;
   __shared__ PrimStage st;
   const pf_primitive* prims = stage_prims(V, st);
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t s = scene_index(V, k);
+  if (!work) return;
   const DevScene& S = V.scenes[s];
-  if ((S.prim_count + S.sdf_count == 0 && !S.contact) || sub >= S.substeps) return;
-  // contact friction (k_con_friction) scattered its velocity ticks first
-  int4 start = make_int4(0, 0, 0, 0);
-  if (S.contact) {
-    start = V.acc_con[k];
-    if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
-  }
-  // colliders that never touched the particle this substep have zero
-  // multipliers and add nothing
-  const uint32_t mask = V.cmask[k];
-  if (!mask && S.prim_count + S.sdf_count <= 32 && !(start.x | start.y | start.z)) return;
   auto ln_at = [&](uint32_t i) {
     return (i < 32 && !((mask >> i) & 1u)) ? 0.0f : V.plam[(size_t)k * V.prim_stride + i].x;
   };
@@ -965,6 +973,7 @@ World::~World() {
   if (arena_) cudaFree(arena_);
   if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
   if (h_pinned_prims_) cudaFreeHost(h_pinned_prims_);
+  if (h_pinned_plane4_) cudaFreeHost(h_pinned_plane4_);
   if (h_pinned_sdfs_) cudaFreeHost(h_pinned_sdfs_);
   if (h_pinned_cloth_) cudaFreeHost(h_pinned_cloth_);
 }
@@ -1287,6 +1296,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
   }
   if (max_rank_ > 32) return fail(PF_ERR_INVALID, "SimLoop: at most 32 materials per scene");
+  refresh_planes(-1);
   // The side stream applies when every scene that holds cloth, or whose
   // colliders run in their own pass, has cloth materials only.
   {
@@ -1587,6 +1597,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.fluids = cv.take<DevFluid>(h_fluids_.size());
     base_.bnds = cv.take<DevBoundary>(h_bnds_.size());
     base_.prims = cv.take<pf_primitive>(h_prims_.size());
+    base_.plane4 = cv.take<float4>(2 * h_prims_.size());
     base_.sdfs = cv.take<DevSdf>(h_sdfs_.size());
     base_.sdf_half = cv.take<uint16_t>(sdf_voxels);
     for (int b = 0; b < 2; ++b) {
@@ -1719,6 +1730,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_CUDA(cudaEventCreate(&ev1_));
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
+  PF_CUDA(cudaMallocHost(&h_pinned_plane4_, sizeof(float4) * 2 * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_sdfs_, sizeof(DevSdf) * std::max<size_t>(1, h_sdfs_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_cloth_, sizeof(DevCloth) * std::max<size_t>(1, h_cloth_par_.size())));
   // ---- upload ----------------------------------------------------------
@@ -1733,6 +1745,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_TRY(up(base_.fluids, h_fluids_.data(), sizeof(DevFluid) * h_fluids_.size()));
   PF_TRY(up(base_.bnds, h_bnds_.data(), sizeof(DevBoundary) * h_bnds_.size()));
   PF_TRY(up(base_.prims, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size()));
+  PF_TRY(up(const_cast<float4*>(base_.plane4), h_plane4_.data(), sizeof(float4) * 2 * h_prims_.size()));
   PF_TRY(up(base_.sdfs, h_sdfs_.data(), sizeof(DevSdf) * h_sdfs_.size()));
   {
     uint64_t off = 0;
@@ -1852,12 +1865,37 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   return PF_OK;
 }
 
+// The compact form of each primitive for the collider passes' plane test,
+// and per scene whether every primitive takes it: a plane that neither
+// sweeps nor spins, with a finite velocity (prim_sdf's unswept plane; its
+// x_w + v * 0 is x_w but for the sign of a zero, which d1 + (x - d1) does
+// not keep).
+void World::refresh_planes(int only_scene) {
+  if (only_scene < 0) h_plane4_.assign(2 * std::max<size_t>(1, h_prims_.size()), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+  for (size_t s = 0; s < h_scenes_.size(); ++s) {
+    if (only_scene >= 0 && s != (size_t)only_scene) continue;
+    DevScene& S = h_scenes_[s];
+    bool fast = true;
+    for (uint32_t q = 0; q < S.prim_count; ++q) {
+      const pf_primitive& p = h_prims_[S.prim_base + q];
+      h_plane4_[2 * (S.prim_base + q)] =
+          make_float4(p.data0[0], p.data0[1], p.data0[2], (p.flags & PF_PRIM_INVERT) ? 1.0f : 0.0f);
+      h_plane4_[2 * (S.prim_base + q) + 1] = make_float4(p.data1[0], p.data1[1], p.data1[2], 0.0f);
+      fast = fast && p.kind == PF_PRIM_PLANE && !(p.flags & PF_PRIM_SWEEP) && p.spin[0] == 0.0f &&
+             p.spin[1] == 0.0f && p.spin[2] == 0.0f && std::isfinite(p.velocity[0]) &&
+             std::isfinite(p.velocity[1]) && std::isfinite(p.velocity[2]);
+    }
+    S.planes_fast = fast ? 1u : 0u;
+  }
+}
+
 pf_status World::set_primitive(uint32_t scene, uint32_t slot, const pf_primitive& p) {
   if (scene >= specs_.size()) return fail(PF_ERR_INVALID, "PrimitiveSet: no such scene");
   const DevScene& S = h_scenes_[scene];
   if (slot >= S.prim_count) return fail(PF_ERR_INVALID, "PrimitiveSet: no primitive in slot " + std::to_string(slot));
   h_prims_[S.prim_base + slot] = p;
   specs_[scene]->prims[slot] = p;
+  refresh_planes((int)scene);
   prims_dirty_ = true;
   return PF_OK;
 }
@@ -1893,6 +1931,9 @@ pf_status World::set_cloth_params(uint32_t scene, uint32_t material, const pf_cl
 pf_status World::upload_params(double dt) {
   const uint32_t K = (uint32_t)h_scenes_.size();
   for (uint32_t s = 0; s < K; ++s) h_scenes_[s].dt = h_scenes_[s].substeps ? f32(dt / h_scenes_[s].substeps) : 0.0f;
+  // where this step's density passes leave lambda (read back by PF_FIELD_LAMBDA)
+  lam_in_xl_.resize(K);
+  for (uint32_t s = 0; s < K; ++s) lam_in_xl_[s] = h_scenes_[s].homog != 0;
   std::memcpy(h_pinned_scenes_, h_scenes_.data(), sizeof(DevScene) * K);
   PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, h_pinned_scenes_, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
   if (sdfs_dirty_ && !h_sdfs_.empty()) {
@@ -1909,6 +1950,9 @@ pf_status World::upload_params(double dt) {
   }
   if (prims_dirty_ && !h_prims_.empty()) {
     std::memcpy(h_pinned_prims_, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size());
+    std::memcpy(h_pinned_plane4_, h_plane4_.data(), sizeof(float4) * 2 * h_prims_.size());
+    PF_CUDA(cudaMemcpyAsync(const_cast<float4*>(base_.plane4), h_pinned_plane4_, sizeof(float4) * 2 * h_prims_.size(),
+                            cudaMemcpyHostToDevice, stream_));
     PF_CUDA(cudaMemcpyAsync(const_cast<pf_primitive*>(base_.prims), h_pinned_prims_,
                             sizeof(pf_primitive) * h_prims_.size(), cudaMemcpyHostToDevice, stream_));
     prims_dirty_ = false;
@@ -2444,11 +2488,10 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
     }
     return PF_OK;
   };
-  auto by_slot1 = [&](const float* src, bool fluid_only) -> pf_status {
+  // one float per slot of the segment (host copy), out by particle id
+  auto by_host1 = [&](const float* tmp, bool fluid_only) -> pf_status {
     PF_TRY(need(4ull * cap));
-    std::vector<float> tmp(seg);
     std::vector<uint32_t> tag(seg);
-    PF_CUDA(cudaMemcpy(tmp.data(), src + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
     PF_CUDA(cudaMemcpy(tag.data(), B.tag + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
     float* o = static_cast<float*>(dst);
     for (uint32_t k = 0; k < seg; ++k) {
@@ -2456,6 +2499,11 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
       if (id < cap) o[id] = (fluid_only && !tag_fluid(tag[k])) ? 0.0f : tmp[k];
     }
     return PF_OK;
+  };
+  auto by_slot1 = [&](const float* src, bool fluid_only) -> pf_status {
+    std::vector<float> tmp(seg);
+    PF_CUDA(cudaMemcpy(tmp.data(), src + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
+    return by_host1(tmp.data(), fluid_only);
   };
   auto by_id4 = [&](const float4* src) -> pf_status {
     PF_TRY(need(16ull * cap));
@@ -2474,7 +2522,19 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
     case PF_FIELD_INV_MASS: return by_slot4(B.x, false, true);
     case PF_FIELD_BOUNDARY_VOLUME: return by_slot1(B.bv, false);
     case PF_FIELD_DENSITY: return by_slot1(B.dens, true);
-    case PF_FIELD_LAMBDA: return by_slot1(base_.lambda, true);
+    case PF_FIELD_LAMBDA: {
+      // the slot path keeps lambda beside x* (xl) in single-fluid scenes of
+      // one mass and in lm otherwise; the warp-tile path in lambda
+      if (tune_.path == 1 || !base_.lm) return by_slot1(base_.lambda, true);
+      const bool in_xl = scene < lam_in_xl_.size() && lam_in_xl_[scene];
+      const size_t words = in_xl ? 4 : 2;
+      std::vector<float> raw(words * seg);
+      PF_CUDA(cudaMemcpy(raw.data(), in_xl ? (const float*)(base_.xl + S.seg_start) : (const float*)(base_.lm + S.seg_start),
+                         4ull * words * seg, cudaMemcpyDeviceToHost));
+      std::vector<float> lam(seg);
+      for (uint32_t k = 0; k < seg; ++k) lam[k] = raw[words * k + (in_xl ? 3 : 0)];
+      return by_host1(lam.data(), true);
+    }
     case PF_FIELD_ROTATION: return by_id4(base_.q);
     case PF_FIELD_PREDICTED_ROTATION: return by_id4(base_.qp);
     case PF_FIELD_ANGULAR_VELOCITY: return by_id4(base_.omega);

@@ -148,6 +148,7 @@ struct DevScene {
   int32_t lo[3];
   uint32_t dims[3];
   uint32_t prim_base, prim_count;
+  uint32_t planes_fast;  // every primitive is a plane that neither sweeps nor spins (plane4 holds it)
   float pos_scale, pos_inv, vel_scale, vel_inv;
   float sb_scale, sb_inv;
   uint32_t fluid_first, fluid_count;  // this scene's fluids in the fluid table
@@ -265,6 +266,7 @@ struct WorldView {
   const DevFluid* fluids;
   const DevBoundary* bnds;
   const pf_primitive* prims;
+  const float4* plane4;  // 2 per primitive: (normal, inverted), (point, 0); read in scenes with planes_fast
   const DevSdf* sdfs;
   const uint16_t* sdf_half;  // half-float voxels of every SDF collider
   StateBuf cur, nxt;
@@ -520,6 +522,10 @@ class World {
   // pinned staging for per-step parameters
   DevScene* h_pinned_scenes_ = nullptr;
   pf_primitive* h_pinned_prims_ = nullptr;
+  std::vector<float4> h_plane4_;
+  float4* h_pinned_plane4_ = nullptr;
+  void refresh_planes(int only_scene);
+  std::vector<bool> lam_in_xl_;  // per scene: the last step kept lambda in xl (homogeneous scene)
   DevSdf* h_pinned_sdfs_ = nullptr;
   DevCloth* h_pinned_cloth_ = nullptr;
   bool prims_dirty_ = true;

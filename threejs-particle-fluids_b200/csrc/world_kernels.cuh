@@ -456,11 +456,23 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
   uint32_t tx = (uint32_t)start.x, ty = (uint32_t)start.y, tz = (uint32_t)start.z;
   bool any = (start.x | start.y | start.z) != 0;
   for (uint32_t p = 0; p < n_prim; ++p) {
-    const pf_primitive& P = prims[p];
     float phi;
     f3 nrm;
-    prim_sdf(P, xstar, clock, &phi, &nrm);
+    if (S.planes_fast) {
+      // prim_sdf's unswept plane, term for term, from the compact table
+      const float4 a = __ldg(V.plane4 + 2 * ((size_t)S.prim_base + p));
+      const float4 b = __ldg(V.plane4 + 2 * ((size_t)S.prim_base + p) + 1);
+      const f3 d0 = xyz(a), d1 = xyz(b);
+      const f3 x = d1 + (xstar - d1);
+      const float ph = dot(d0, x - d1);
+      const bool inv = a.w != 0.0f;
+      phi = inv ? -ph : ph;
+      nrm = inv ? neg(d0) : d0;
+    } else {
+      prim_sdf(prims[p], xstar, clock, &phi, &nrm);
+    }
     if (!(phi < radius)) continue;
+    const pf_primitive& P = prims[p];
     const f3 coldisp = prim_surface_velocity(P, xstar, clock) * S.dt;
     const float depth = radius - phi;
     float2 lam = lam_at(p);

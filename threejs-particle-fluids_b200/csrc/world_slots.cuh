@@ -114,9 +114,12 @@ __device__ __forceinline__ void finish_lambda(const WorldView& V, const DevScene
     const float at = F.compliance / (S.dt * S.dt);
     lam = -C / fmaxf(gn + at, 1e-20f);
   }
-  V.lambda[k] = lam;
-  V.lm[k].x = lam;
-  if (S.homog) V.xl[k] = make_float4(xi4.x, xi4.y, xi4.z, lam);
+  // the position pass of a single-fluid scene of one mass reads (x*, lambda)
+  // from xl, the others lambda from lm (the warp-tile path keeps its own)
+  if (S.homog)
+    V.xl[k] = make_float4(xi4.x, xi4.y, xi4.z, lam);
+  else
+    V.lm[k].x = lam;
 }
 
 // lambda.ts:41-59: one neighbour's terms of the density and constraint-
@@ -316,7 +319,7 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
   if (sub >= S.substeps || it >= S.iterations) return;
   const float4 xi4 = V.cur.xs[k];
   const f3 xi = xyz(xi4);
-  const float li = V.lm[k].x;
+  const float li = S.homog ? V.xl[k].w : V.lm[k].x;
   const bool react = kReact && F.react_lo != F.react_hi && li != 0.0f;
   // each fluid reads its own multipliers, zero for other particles (the
   // reference keeps one lambda buffer per fluid)
