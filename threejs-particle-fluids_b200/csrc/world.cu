@@ -184,8 +184,8 @@ constexpr uint32_t kSmemPrims = 16;
 struct PrimStage {
   pf_primitive p[kSmemPrims];
 };
-__device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, PrimStage& st) {
-  const uint32_t first = blockIdx.x * blockDim.x;
+__device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, PrimStage& st,
+                                                           uint32_t first = blockIdx.x * blockDim.x) {
   const uint32_t sb = first < V.n ? scene_index(V, first) : 0u;
   const DevScene& S = V.scenes[sb];
   const pf_primitive* src = V.prims + S.prim_base;
@@ -284,10 +284,14 @@ __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t ran
 // registers. Scenes whose last material is a fluid run this inside the
 // fluid's apply instead (collide_rank1).
 __global__ void __launch_bounds__(kBlock, 4) k_collide(WorldView V, uint32_t sub, uint32_t it) {
+  // launched over the chunks of the scenes that need this pass (a block is
+  // one chunk)
+  static_assert(kBlock == kSegAlign, "one block per chunk");
   __shared__ PrimStage st;
-  const pf_primitive* prims = stage_prims(V, st);
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const pf_primitive* prims = stage_prims(V, st, chunk_slot(V.cchunk, blockIdx.x * blockDim.x));
+  if (g >= V.n_cchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.cchunk, g);
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
   if ((S.prim_count + S.sdf_count == 0 && !S.contact) || S.collide_rank1 || sub >= S.substeps || it >= S.iterations)
@@ -1550,6 +1554,12 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   std::vector<uint32_t> chunk(n_ / kSegAlign, 0);
   for (uint32_t s = 0; s < K; ++s)
     for (uint32_t c = h_scenes_[s].seg_start / kSegAlign; c < h_scenes_[s].seg_end / kSegAlign; ++c) chunk[c] = s;
+  std::vector<uint32_t> fchunk, cchunk;
+  for (uint32_t c = 0; c < chunk.size(); ++c) {
+    const DevScene& S = h_scenes_[chunk[c]];
+    if (S.fluid_count) fchunk.push_back(c);
+    if ((S.prim_count + S.sdf_count > 0 || S.contact) && S.collide_rank1 == 0) cchunk.push_back(c);
+  }
   std::vector<float> dens(n_, 0.0f);
   std::vector<uint32_t> tag(n_, 0);
   for (uint32_t s = 0; s < K; ++s) {
@@ -1592,6 +1602,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   auto layout = [&](Carver& cv) {
     base_.scenes_rw = cv.take<DevScene>(K);
     base_.chunk_scene = cv.take<uint32_t>(chunk.size());
+    base_.fchunk = cv.take<uint32_t>(fchunk.size());
+    base_.cchunk = cv.take<uint32_t>(cchunk.size());
+    base_.n_fchunk = (uint32_t)fchunk.size();
+    base_.n_cchunk = (uint32_t)cchunk.size();
     base_.flags = cv.take<uint32_t>(K * kNumFlags);
     base_.clocks = cv.take<float>(K);
     base_.fluids = cv.take<DevFluid>(h_fluids_.size());
@@ -1742,6 +1756,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_CUDA(cudaMemsetAsync(arena_, 0, probe.off, stream_));
   PF_TRY(up(base_.scenes_rw, h_scenes_.data(), sizeof(DevScene) * K));
   PF_TRY(up(base_.chunk_scene, chunk.data(), 4 * chunk.size()));
+  PF_TRY(up(const_cast<uint32_t*>(base_.fchunk), fchunk.data(), 4 * fchunk.size()));
+  PF_TRY(up(const_cast<uint32_t*>(base_.cchunk), cchunk.data(), 4 * cchunk.size()));
   PF_TRY(up(base_.fluids, h_fluids_.data(), sizeof(DevFluid) * h_fluids_.size()));
   PF_TRY(up(base_.bnds, h_bnds_.data(), sizeof(DevBoundary) * h_bnds_.size()));
   PF_TRY(up(base_.prims, h_prims_.data(), sizeof(pf_primitive) * h_prims_.size()));
@@ -1976,7 +1992,9 @@ void World::launch_tiles_build(const WorldView& V, uint32_t s) {
 // One-thread-per-slot fluid kernels at a tuned block size.
 template <typename K, typename... A>
 void World::launch_fluid(uint32_t block, K kernel, A... args) {
-  kernel<<<div_up(n_, block), block, 0, stream_>>>(args...);
+  const uint32_t slots = base_.n_fchunk * kSegAlign;  // the chunks of the scenes with a fluid
+  if (!slots) return;
+  kernel<<<div_up(slots, block), block, 0, stream_>>>(args...);
   ++t_launches;
 }
 
@@ -2271,7 +2289,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     for (uint32_t it = 0; it < max_iter_; ++it) {
       for (uint32_t r = 0; r < cloth_ranges_.size(); ++r) launch_cloth_rank(V, r, s, it, side_stream_);
       if (any_contact_) launch_slots(k_con_solve, n_, side_stream_, V, s, it);
-      if (any_unfused_prims_) launch_slots(k_collide, n_, side_stream_, V, s, it);
+      if (any_unfused_prims_) launch_slots(k_collide, base_.n_cchunk * kSegAlign, side_stream_, V, s, it);
     }
   }
   for (uint32_t it = 0; it < max_iter_; ++it) {
@@ -2305,7 +2323,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (!fork && r < cloth_ranges_.size()) launch_cloth_rank(V, r, s, it, stream_);
     }
     if (!fork && any_contact_) launch_slots(k_con_solve, n_, stream_, V, s, it);
-    if (!fork && any_unfused_prims_) launch_slots(k_collide, n_, stream_, V, s, it);
+    if (!fork && any_unfused_prims_) launch_slots(k_collide, base_.n_cchunk * kSegAlign, stream_, V, s, it);
   }
   if (fork) {
     cudaEventRecord(ev_join_, side_stream_);

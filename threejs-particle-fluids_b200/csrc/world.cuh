@@ -260,6 +260,12 @@ struct WorldView {
   uint32_t prim_stride;  // colliders (primitives + SDFs) per slot in the collider lambda array
   const DevScene* scenes;
   const uint32_t* chunk_scene;  // scene of each 256-slot chunk
+  // the 256-slot chunks (ascending) of the scenes with a fluid, and of the
+  // scenes whose colliders run in their own pass: those passes' slot kernels
+  // are launched over their chunks only
+  const uint32_t* fchunk;
+  const uint32_t* cchunk;
+  uint32_t n_fchunk, n_cchunk;
   DevScene* scenes_rw;
   uint32_t* flags;              // kNumFlags per scene
   float* clocks;                // collider sweep clock per scene (PrimitiveSet.motionClock)

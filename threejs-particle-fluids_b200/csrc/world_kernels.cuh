@@ -19,6 +19,10 @@ __device__ __forceinline__ const DevScene& scene_at(const WorldView& V, uint32_t
 __device__ __forceinline__ uint32_t scene_index(const WorldView& V, uint32_t slot) {
   return V.chunk_scene[slot >> 8];
 }
+// Slot of the g-th slot of a chunk list (launch index g over its chunks).
+__device__ __forceinline__ uint32_t chunk_slot(const uint32_t* __restrict__ list, uint32_t g) {
+  return __ldg(list + g / kSegAlign) * kSegAlign + g % kSegAlign;
+}
 
 // ----------------------------------------------------------- vector math ----
 struct f3 {

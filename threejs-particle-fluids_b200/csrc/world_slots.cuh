@@ -158,8 +158,9 @@ __device__ __forceinline__ void lambda_terms(const DevFluid& F, f3 xi, float4 xj
 // world has no surface impulses and no late drag and lift).
 template <uint32_t kNbrUnroll, bool kDens>
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevScene& S = scene_at(V, k);
@@ -269,8 +270,9 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
 // lambda.ts:41-71
 template <uint32_t kNbrUnroll>
 __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -309,8 +311,9 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
 // is rewritten in place; the arithmetic is that of the separate apply.
 template <uint32_t kNbrUnroll, bool kReact>
 __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, uint32_t rank, uint32_t sub, uint32_t it, uint32_t apply) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -386,8 +389,9 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
 // confinement, the curl omega = sum V_j (v_i - v_j) x grad W.
 template <uint32_t kNbrUnroll, bool kBnd>
 __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -432,8 +436,9 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
 // grad W (|omega_j| - |omega_i|) V, into dx (free after the iterations).
 template <uint32_t kNbrUnroll>
 __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -460,8 +465,9 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
 // substep's predicted positions.
 template <uint32_t kNbrUnroll>
 __global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -502,8 +508,9 @@ __device__ __forceinline__ float adhesion_spline(float r, const DevFluid& F) {
 // neighbours on the fluid side only; both as fixed-point velocity changes.
 template <uint32_t kNbrUnroll>
 __global__ void k_s_impulses(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
