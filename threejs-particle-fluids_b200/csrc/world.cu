@@ -204,10 +204,12 @@ __device__ __forceinline__ const pf_primitive* stage_prims(const WorldView& V, P
 // the position pass, which applies them itself (k_s_delta).
 __global__ void __launch_bounds__(kBlock, 4) k_fluid_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it,
                                                         uint32_t skip_homog) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  // launched over the chunks of the scenes with a fluid (a block is one chunk)
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = g < V.n_fchunk * kSegAlign;
+  const uint32_t k = live ? chunk_slot(V.fchunk, g) : 0u;
   // the slot's own loads go out first, so their latency overlaps the
   // primitive staging and the scene lookup
-  const bool live = k < V.n;
   uint32_t tg = 0;
   float4 x = make_float4(0, 0, 0, 0), d = make_float4(0, 0, 0, 0);
   if (live) {
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_fluid_apply(WorldView V, uint32_t
     d = V.dx[k];
   }
   __shared__ PrimStage st;
-  const pf_primitive* prims = stage_prims(V, st);
+  const pf_primitive* prims = stage_prims(V, st, chunk_slot(V.fchunk, blockIdx.x * blockDim.x));
   if (!live) return;
   const uint32_t s = scene_index(V, k);
   const DevScene& S = V.scenes[s];
@@ -254,8 +256,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_fluid_apply(WorldView V, uint32_t
 // velocity.ts:99-120: the vorticity confinement force eps (N x omega) dt with
 // N = eta / |eta| (eta from k_s_vort_grad, in dx), then the XSPH change.
 __global__ void __launch_bounds__(kBlock) k_xsph_apply(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -883,8 +886,9 @@ __global__ void __launch_bounds__(kBlock) k_gather_positions(WorldView V, const 
 // FluidSystem.ts:248-253: the impulse accumulator's apply over the fluid's
 // range, into the velocity and (times dt) the predicted position.
 __global__ void __launch_bounds__(kBlock) k_imp_apply(WorldView V, uint32_t rank, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
   const uint32_t f = tag_fluid(V.cur.tag[k]);
   if (!f) return;
   const DevFluid& F = V.fluids[f - 1];
@@ -2269,7 +2273,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (!imp) continue;
       if (st) PF_BY_UNROLL(kSlotVel, k_s_color_normal, V, r, s);
       PF_BY_UNROLL(kSlotVel, k_s_impulses, V, r, s);
-      launch_slots(k_imp_apply, n_, stream_, V, r, s);
+      launch_slots(k_imp_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s);
     }
   launch_aero(V, 1, s);
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
@@ -2306,7 +2310,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         const bool slot = tune_.path == 0;
         bool rest = !slot;
         for (auto& S : h_scenes_) rest = rest || (S.fluid_count && !S.homog);
-        if (rest) launch_slots(k_fluid_apply, n_, stream_, V, r, s, it, slot ? 1u : 0u);
+        if (rest) launch_slots(k_fluid_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s, it, slot ? 1u : 0u);
       }
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
@@ -2340,7 +2344,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
     if (has_velocity) {
       run_fluid_xsph(V, r, s);
       if (has_vort) PF_BY_UNROLL(kSlotVel, k_s_vort_grad, V, r, s);
-      launch_slots(k_xsph_apply, n_, stream_, V, r, s);
+      launch_slots(k_xsph_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s);
     }
     if (has_local) {
       launch_slots(k_rot_advect, base_.n_grp, stream_, V, s);
