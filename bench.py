@@ -239,10 +239,13 @@ class BatchWorkload:
     metric = "particle-substeps/s & p99 step latency: batched/served vs plain, 1\u00d7B200"
     unit = "particle-substeps/s"
     DT = 1.0 / 60.0
-    # algorithmic bytes per fluid particle of the density+lambda stage:
-    # read x* (16 B) and the boundary volume (4 B), write lambda and density (4 B each)
-    LAMBDA_BYTES = 28
-    LAMBDA_TRAFFIC_PER_PARTICLE = 169.1e6 / 960_919
+    # algorithmic bytes per fluid particle of the density+lambda stage in
+    # these single-fluid scenes of one mass: read x* (16 B); write the density
+    # (4 B) and the (x*, lambda) record the position pass gathers (16 B)
+    LAMBDA_BYTES = 36
+    # DRAM bytes per fluid particle of one launch, from a full ncu capture of
+    # the pass on the 32-scene cut (158.6 MB over 960,919 fluid particles)
+    LAMBDA_TRAFFIC_PER_PARTICLE = 158.6e6 / 960_919
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -359,7 +362,7 @@ class BatchWorkload:
             "algorithmic_bytes": self.LAMBDA_BYTES * items.value,
             # DRAM bytes of one launch: the per-fluid-particle figure of a full
             # ncu capture of this pass on the 32-scene cut of the workload
-            # (169.1 MB over 960,919 fluid particles) scaled to this launch
+            # scaled to this launch
             "traffic": self.LAMBDA_TRAFFIC_PER_PARTICLE * items.value if tp.value == 0 else None,
             "gpu_launches_per_step": launches,
             "clocks": clk,
