@@ -133,7 +133,6 @@ __global__ void __launch_bounds__(kBlock) k_permute(WorldView V) {
   V.cmask[k] = 0u;
   for (uint32_t p = 32; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
-  if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
   if (V.acc_imp) V.acc_imp[k] = make_int4(0, 0, 0, 0);
 }
 
@@ -144,7 +143,6 @@ __global__ void __launch_bounds__(kBlock) k_reset_sums(WorldView V) {
   V.cmask[k] = 0u;
   for (uint32_t p = 32; p < V.prim_stride; ++p) V.plam[(size_t)k * V.prim_stride + p] = make_float2(0.0f, 0.0f);
   if (V.acc_react) V.acc_react[k] = make_int4(0, 0, 0, 0);
-  if (V.acc_soft) V.acc_soft[k] = make_int4(0, 0, 0, 0);
 }
 
 // ---------------------------------------------------------------- fluid ----
@@ -697,53 +695,56 @@ __global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank
   V.rot3[3 * (size_t)i + 2] = make_float4(r[6], r[7], r[8], 0.0f);
 }
 
-// shapeMatchImplicit.ts:248-308
-__global__ void __launch_bounds__(kBlock) k_sm_scatter(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= V.n_grp) return;
-  const DevSoft* D;
-  const DevScene* S;
-  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
-  const uint32_t i = V.grp[g];
-  const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
-  const f3 R0 = xyz(V.rot3[3 * (size_t)i]), R1 = xyz(V.rot3[3 * (size_t)i + 1]), R2 = xyz(V.rot3[3 * (size_t)i + 2]);
-  const f3 c = xyz(V.centers[i]);
-  const f3 cb = xyz(V.rest_c[i]);
-  const float at = V.rest[i].w / (S->dt * S->dt);
-  for (uint32_t m = s; m < e; ++m) {
-    const uint32_t j = V.csr_idx[m];
-    const uint32_t sj = V.inv[j];
-    const f3 rr = xyz(V.rest[j]) - cb;
-    const f3 goal = mk(dot(R0, rr), dot(R1, rr), dot(R2, rr)) + c;
-    const float4 xj = V.cur.xs[sj];
-    const f3 C = xyz(xj) - goal;
-    const float wj = xj.w;
-    const float denom = wj + at;
+// shapeMatchImplicit.ts:248-308 taken by member, with the accumulator's
+// apply (accumulator.ts:148-178) for the particle. The reference scatters
+// each cluster's corrections to its members as fixed-point ticks (integer
+// sums, so their order does not matter); here each particle (by id) forms
+// the corrections of every cluster that holds it, term for term as the
+// cluster would, updates those pairs' multipliers (each pair belongs to one
+// member), sums the ticks in registers and applies them to its own
+// predicted position. No other thread reads that position in this pass: the
+// clusters' centres and rotations come from the passes before.
+__global__ void __launch_bounds__(kBlock) k_sm_gather(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= V.n) return;
+  const uint32_t b = V.mem_off[j], e = V.mem_off[j + 1];
+  if (b == e) return;
+  const DevSoft& D = V.softs[V.mem_soft[j]];
+  const DevScene& S = V.scenes[D.scene];
+  if (D.rank != rank || sub >= S.substeps || it >= S.iterations) return;
+  const uint32_t sj = V.inv[j];
+  const float4 xj = V.cur.xs[sj];
+  const f3 rj = xyz(V.rest[j]);
+  const float wj = xj.w;
+  const float mj = fmaxf((float)(V.csr_off[j + 1] - V.csr_off[j]), 1.0f);
+  const float dt2 = S.dt * S.dt;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  for (uint32_t q = b; q < e; ++q) {
+    const uint2 im = __ldg(V.mem + q);
+    const uint32_t i = im.x, m = im.y;
+    const f3 R0 = xyz(V.rot3[3 * (size_t)i]), R1 = xyz(V.rot3[3 * (size_t)i + 1]), R2 = xyz(V.rot3[3 * (size_t)i + 2]);
+    const f3 c = xyz(V.centers[i]);
+    const f3 cb = xyz(V.rest_c[i]);
+    const float at = V.rest[i].w / dt2;
     const f3 lo = xyz(V.pair_lambda[m]);
+    const f3 rr = rj - cb;
+    const f3 goal = mk(dot(R0, rr), dot(R1, rr), dot(R2, rr)) + c;
+    const f3 C = xyz(xj) - goal;
+    const float denom = wj + at;
     const f3 dl = (neg(C) - lo * at) / denom;
     V.pair_lambda[m] = with_w(lo + dl, 0.0f);
-    const float mj = fmaxf((float)(V.csr_off[j + 1] - V.csr_off[j]), 1.0f);
     const f3 dx = (dl * wj) / mj;
-    const float sc = sqrtf(D->maxc2 / fmaxf(dot(dx, dx), D->maxc2));
-    acc_add(V.acc_soft, sj, dx * sc, S->sb_scale);
+    const float sc = sqrtf(D.maxc2 / fmaxf(dot(dx, dx), D.maxc2));
+    const f3 v = dx * sc;
+    tx += (uint32_t)to_ticks(v.x, S.sb_scale);
+    ty += (uint32_t)to_ticks(v.y, S.sb_scale);
+    tz += (uint32_t)to_ticks(v.z, S.sb_scale);
   }
-}
-
-// accumulator.ts:148-178 over every particle of scenes with a local system at this rank.
-__global__ void __launch_bounds__(kBlock) k_soft_apply(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const uint32_t s = scene_index(V, k);
-  const DevScene& S = V.scenes[s];
-  if (!((S.soft_local_ranks >> rank) & 1u) || sub >= S.substeps || it >= S.iterations) return;
-  const int4 t = V.acc_soft[k];
-  if (!(t.x | t.y | t.z)) return;
+  if (!(tx | ty | tz)) return;
   bool sat = false;
-  const f3 c = ticks_change(t.x, t.y, t.z, S.sb_inv, &sat);
-  V.acc_soft[k] = make_int4(0, 0, 0, 0);
-  const float4 x = V.cur.xs[k];
-  V.cur.xs[k] = with_w(xyz(x) + c, x.w);
-  if (sat) atomicOr(V.flags + s * kNumFlags + FLAG_SOFT, 1u);
+  const f3 ch = ticks_change((int)tx, (int)ty, (int)tz, S.sb_inv, &sat);
+  V.cur.xs[sj] = with_w(xyz(xj) + ch, wj);
+  if (sat) atomicOr(V.flags + D.scene * kNumFlags + FLAG_SOFT, 1u);
 }
 
 // shapeMatchImplicit.ts:325-401
@@ -1554,6 +1555,21 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
       }
     }
   }
+  // the clusters that hold each particle: (centre id, CSR position) by member
+  std::vector<uint32_t> mem_off(n_ + 1, 0), mem_soft(n_, 0);
+  std::vector<uint2> mem;
+  {
+    for (uint32_t g = 0; g < grp.size(); ++g)
+      for (uint32_t m = csr_off[grp[g]]; m < csr_off[grp[g] + 1]; ++m) {
+        ++mem_off[csr_idx[m] + 1];
+        mem_soft[csr_idx[m]] = grp_soft[g];
+      }
+    for (uint32_t i = 0; i < n_; ++i) mem_off[i + 1] += mem_off[i];
+    mem.assign(std::max<uint32_t>(1, mem_off[n_]), make_uint2(0, 0));
+    std::vector<uint32_t> at(mem_off.begin(), mem_off.end() - 1);
+    for (uint32_t g = 0; g < grp.size(); ++g)
+      for (uint32_t m = csr_off[grp[g]]; m < csr_off[grp[g] + 1]; ++m) mem[at[csr_idx[m]]++] = make_uint2(grp[g], m);
+  }
   // ---- chunk table and per-slot state ----------------------------------
   std::vector<uint32_t> chunk(n_ / kSegAlign, 0);
   for (uint32_t s = 0; s < K; ++s)
@@ -1651,7 +1667,6 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.plam = cv.take<float2>(N * P);
     base_.cmask = cv.take<uint32_t>(N);
     base_.acc_react = any_react_ ? cv.take<int4>(N) : nullptr;
-    base_.acc_soft = any_soft_local_ ? cv.take<int4>(N) : nullptr;
     base_.softs = cv.take<DevSoft>(h_softs_.size());
     base_.bodies = cv.take<DevBody>(h_bodies_.size());
     base_.grp = cv.take<uint32_t>(grp.size());
@@ -1667,6 +1682,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.qp = need_soft ? cv.take<float4>(N) : nullptr;
     base_.omega = need_soft ? cv.take<float4>(N) : nullptr;
     base_.pair_lambda = cv.take<float4>(csr_idx.size());
+    base_.mem_off = any_soft_local_ ? cv.take<uint32_t>(N + 1) : nullptr;
+    base_.mem = any_soft_local_ ? cv.take<uint2>(mem.size()) : nullptr;
+    base_.mem_soft = any_soft_local_ ? cv.take<uint32_t>(N) : nullptr;
     base_.lambda_g = need_soft ? cv.take<float4>(N) : nullptr;
     base_.body_c = cv.take<float4>(h_bodies_.size());
     base_.body_r = cv.take<float4>(3 * h_bodies_.size());
@@ -1818,6 +1836,11 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   if (need_soft) {
     PF_TRY(up(base_.csr_off, csr_off.data(), 4 * csr_off.size()));
     PF_TRY(up(base_.csr_idx, csr_idx.data(), 4 * csr_idx.size()));
+    if (any_soft_local_) {
+      PF_TRY(up(const_cast<uint32_t*>(base_.mem_off), mem_off.data(), 4 * mem_off.size()));
+      PF_TRY(up(const_cast<uint2*>(base_.mem), mem.data(), sizeof(uint2) * mem.size()));
+      PF_TRY(up(const_cast<uint32_t*>(base_.mem_soft), mem_soft.data(), 4 * mem_soft.size()));
+    }
     PF_TRY(up(base_.rest, rest4.data(), 16 * N));
     PF_TRY(up(base_.rest_c, restc4.data(), 16 * N));
     PF_TRY(up(base_.weights, weights.data(), 4 * N));
@@ -2315,8 +2338,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
         launch_slots(k_sm_moment, base_.n_grp, stream_, V, r, s, it);
-        launch_slots(k_sm_scatter, base_.n_grp, stream_, V, r, s, it);
-        launch_slots(k_soft_apply, n_, stream_, V, r, s, it);
+        launch_slots(k_sm_gather, n_, stream_, V, r, s, it);
         launch_slots(k_sm_qp, base_.n_grp, stream_, V, r, s, it);
       }
       if (has_global && base_.n_bodies) {

@@ -307,7 +307,6 @@ struct WorldView {
   float2* plam;       // (lambda_n, lambda_t) per slot x primitive
   uint32_t* cmask;    // per slot: bit p set once collider p < 32 touched it this substep (plam entry valid)
   int4* acc_react;    // fixed-point reaction sums per slot
-  int4* acc_soft;     // fixed-point shape-matching sums per slot
   // soft bodies (by id unless noted)
   const DevSoft* softs;
   const DevBody* bodies;
@@ -325,6 +324,12 @@ struct WorldView {
   float4* qp;                // predicted orientation
   float4* omega;             // angular velocity
   float4* pair_lambda;       // per CSR entry
+  // the clusters that hold each particle (by id): entries [mem_off[j],
+  // mem_off[j + 1]) of mem are (cluster centre id, CSR position), mem_soft[j]
+  // the particle's soft system
+  const uint32_t* mem_off;
+  const uint2* mem;
+  const uint32_t* mem_soft;
   float4* lambda_g;          // global matching multipliers per id
   float4* body_c;            // per body
   float4* body_r;            // 3 rows per body
