@@ -697,21 +697,22 @@ __global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank
 
 // shapeMatchImplicit.ts:248-308 taken by member, with the accumulator's
 // apply (accumulator.ts:148-178) for the particle. The reference scatters
-// each cluster's corrections to its members as fixed-point ticks (integer
-// sums, so their order does not matter); here each particle (by id) forms
-// the corrections of every cluster that holds it, term for term as the
-// cluster would, updates those pairs' multipliers (each pair belongs to one
-// member), sums the ticks in registers and applies them to its own
-// predicted position. No other thread reads that position in this pass: the
-// clusters' centres and rotations come from the passes before.
+// each cluster's corrections to its members as fixed-point ticks, integer
+// sums whose order does not matter. Here one warp takes one particle (by id,
+// from the list of cluster members): each lane forms the corrections of
+// clusters that hold it, term for term as the cluster would, and updates
+// those pairs' multipliers (each pair belongs to one member); the lanes' tick
+// sums are added across the warp, and one lane applies them to the
+// particle's predicted position. No other warp reads that position in this
+// pass: the clusters' centres and rotations come from the passes before.
 __global__ void __launch_bounds__(kBlock) k_sm_gather(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= V.n) return;
-  const uint32_t b = V.mem_off[j], e = V.mem_off[j + 1];
-  if (b == e) return;
+  const uint32_t w = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31u;
+  if (w >= V.n_mem_ids) return;  // whole warps
+  const uint32_t j = __ldg(V.mem_ids + w);
   const DevSoft& D = V.softs[V.mem_soft[j]];
   const DevScene& S = V.scenes[D.scene];
   if (D.rank != rank || sub >= S.substeps || it >= S.iterations) return;
+  const uint32_t b = V.mem_off[j], e = V.mem_off[j + 1];
   const uint32_t sj = V.inv[j];
   const float4 xj = V.cur.xs[sj];
   const f3 rj = xyz(V.rest[j]);
@@ -719,7 +720,7 @@ __global__ void __launch_bounds__(kBlock) k_sm_gather(WorldView V, uint32_t rank
   const float mj = fmaxf((float)(V.csr_off[j + 1] - V.csr_off[j]), 1.0f);
   const float dt2 = S.dt * S.dt;
   uint32_t tx = 0, ty = 0, tz = 0;
-  for (uint32_t q = b; q < e; ++q) {
+  for (uint32_t q = b + lane; q < e; q += 32) {
     const uint2 im = __ldg(V.mem + q);
     const uint32_t i = im.x, m = im.y;
     const f3 R0 = xyz(V.rot3[3 * (size_t)i]), R1 = xyz(V.rot3[3 * (size_t)i + 1]), R2 = xyz(V.rot3[3 * (size_t)i + 2]);
@@ -740,7 +741,10 @@ __global__ void __launch_bounds__(kBlock) k_sm_gather(WorldView V, uint32_t rank
     ty += (uint32_t)to_ticks(v.y, S.sb_scale);
     tz += (uint32_t)to_ticks(v.z, S.sb_scale);
   }
-  if (!(tx | ty | tz)) return;
+  tx = __reduce_add_sync(0xffffffffu, tx);
+  ty = __reduce_add_sync(0xffffffffu, ty);
+  tz = __reduce_add_sync(0xffffffffu, tz);
+  if (lane != 0 || !(tx | ty | tz)) return;
   bool sat = false;
   const f3 ch = ticks_change((int)tx, (int)ty, (int)tz, S.sb_inv, &sat);
   V.cur.xs[sj] = with_w(xyz(xj) + ch, wj);
@@ -1556,7 +1560,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     }
   }
   // the clusters that hold each particle: (centre id, CSR position) by member
-  std::vector<uint32_t> mem_off(n_ + 1, 0), mem_soft(n_, 0);
+  std::vector<uint32_t> mem_off(n_ + 1, 0), mem_soft(n_, 0), mem_ids;
   std::vector<uint2> mem;
   {
     for (uint32_t g = 0; g < grp.size(); ++g)
@@ -1564,7 +1568,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         ++mem_off[csr_idx[m] + 1];
         mem_soft[csr_idx[m]] = grp_soft[g];
       }
-    for (uint32_t i = 0; i < n_; ++i) mem_off[i + 1] += mem_off[i];
+    for (uint32_t i = 0; i < n_; ++i) {
+      if (mem_off[i + 1]) mem_ids.push_back(i);
+      mem_off[i + 1] += mem_off[i];
+    }
     mem.assign(std::max<uint32_t>(1, mem_off[n_]), make_uint2(0, 0));
     std::vector<uint32_t> at(mem_off.begin(), mem_off.end() - 1);
     for (uint32_t g = 0; g < grp.size(); ++g)
@@ -1685,6 +1692,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.mem_off = any_soft_local_ ? cv.take<uint32_t>(N + 1) : nullptr;
     base_.mem = any_soft_local_ ? cv.take<uint2>(mem.size()) : nullptr;
     base_.mem_soft = any_soft_local_ ? cv.take<uint32_t>(N) : nullptr;
+    base_.mem_ids = any_soft_local_ ? cv.take<uint32_t>(mem_ids.size()) : nullptr;
+    base_.n_mem_ids = any_soft_local_ ? (uint32_t)mem_ids.size() : 0u;
     base_.lambda_g = need_soft ? cv.take<float4>(N) : nullptr;
     base_.body_c = cv.take<float4>(h_bodies_.size());
     base_.body_r = cv.take<float4>(3 * h_bodies_.size());
@@ -1840,6 +1849,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
       PF_TRY(up(const_cast<uint32_t*>(base_.mem_off), mem_off.data(), 4 * mem_off.size()));
       PF_TRY(up(const_cast<uint2*>(base_.mem), mem.data(), sizeof(uint2) * mem.size()));
       PF_TRY(up(const_cast<uint32_t*>(base_.mem_soft), mem_soft.data(), 4 * mem_soft.size()));
+      PF_TRY(up(const_cast<uint32_t*>(base_.mem_ids), mem_ids.data(), 4 * mem_ids.size()));
     }
     PF_TRY(up(base_.rest, rest4.data(), 16 * N));
     PF_TRY(up(base_.rest_c, restc4.data(), 16 * N));
@@ -2338,7 +2348,10 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
         launch_slots(k_sm_moment, base_.n_grp, stream_, V, r, s, it);
-        launch_slots(k_sm_gather, n_, stream_, V, r, s, it);
+        if (base_.n_mem_ids) {  // one warp per cluster member
+          k_sm_gather<<<(uint32_t)((32ull * base_.n_mem_ids + kBlock - 1) / kBlock), kBlock, 0, stream_>>>(V, r, s, it);
+          ++t_launches;
+        }
         launch_slots(k_sm_qp, base_.n_grp, stream_, V, r, s, it);
       }
       if (has_global && base_.n_bodies) {

@@ -330,6 +330,8 @@ struct WorldView {
   const uint32_t* mem_off;
   const uint2* mem;
   const uint32_t* mem_soft;
+  const uint32_t* mem_ids;   // the ids held by at least one cluster, ascending
+  uint32_t n_mem_ids;
   float4* lambda_g;          // global matching multipliers per id
   float4* body_c;            // per body
   float4* body_r;            // 3 rows per body
