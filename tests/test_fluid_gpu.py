@@ -159,3 +159,36 @@ def test_two_fluids_in_one_scene(oracle):
     dev = float(np.abs(g.readback(N.PF_FIELD_POSITIONS).astype(np.float64)
                        - o.readback(N.PF_FIELD_POSITIONS).astype(np.float64)).max())
     assert dev <= 1e-5, dev
+
+
+def test_mass_write_leaves_the_one_mass_path(oracle, cuda):
+    """A single-fluid scene of one mass takes the one-mass path (the position
+    pass gathers (x*, lambda) and applies the slot itself). Writing unequal
+    inverse masses moves it to the general path from the next step on, in a
+    plain scene and inside a batch stepped by a captured graph: the two agree
+    bit for bit, and positions stay within the tolerance of the oracle given
+    the same write. The masses change by 10 %: with every other particle's
+    mass doubled the step is ill-conditioned (the oracle's own FP32 and FP64
+    runs then differ by centimetres after one frame), so such a write is no
+    parity case at 1e-5."""
+    r = W.dam_break(4000, seed=21)
+    a = cuda.build(r)
+    o = oracle.OracleBackend(precision=32).build(r)
+    batch = R.Batch([cuda.build(r), cuda.build(W.dam_break(2000, seed=22))], use_graph=True)
+    a.step(DT)
+    o.step(DT)
+    batch.step(DT)
+    w = a.readback(N.PF_FIELD_INV_MASS)
+    w[::2] *= np.float32(0.9)
+    a.write(N.PF_FIELD_INV_MASS, w)
+    o.write(N.PF_FIELD_INV_MASS, w)
+    batch.write(0, N.PF_FIELD_INV_MASS, w)
+    a.step(DT)
+    o.step(DT)
+    batch.step(DT)
+    xa = a.readback(N.PF_FIELD_POSITIONS)
+    assert np.array_equal(xa, batch.readback(0, N.PF_FIELD_POSITIONS))
+    assert np.array_equal(a.readback(N.PF_FIELD_LAMBDA), batch.readback(0, N.PF_FIELD_LAMBDA))
+    assert np.array_equal(a.readback(N.PF_FIELD_INV_MASS), w)
+    assert np.abs(xa - o.readback(N.PF_FIELD_POSITIONS)).max() <= POS_TOL
+    assert np.array_equal(a.readback(N.PF_FIELD_DENSITY), batch.readback(0, N.PF_FIELD_DENSITY))
