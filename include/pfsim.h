@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define PFSIM_ABI_VERSION 1
+#define PFSIM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PF_API __attribute__((visibility("default")))
@@ -351,9 +351,13 @@ typedef struct pf_loop_desc {
   uint32_t iterations;
   float gravity[3];
   float hash_origin[3];
-  /* Bounds of the linear neighbour grid in metres; particles outside are
-   * clamped into the border cells. min >= max selects the bounds of the
-   * uploaded particles and primitives plus a margin. */
+  /* Size and first placement of the neighbour grid window in metres. The
+   * grid is a window over the reference's cell lattice (cell = the widest
+   * query radius, aligned to hash_origin) that moves with the particles
+   * each substep; only particles spread wider than the window are clamped
+   * into its border cells (pf_overflow.grid_clamped). min >= max on any
+   * axis selects a window four times the extent of the uploaded particles
+   * (at least 16 cells more), centred on them. */
   float grid_min[3];
   float grid_max[3];
   /* SimLoopOptions.contact (loop.ts:20-30, 347-417; src/core/contact/):
@@ -413,7 +417,16 @@ PF_API pf_status pf_readback(pf_scene* scene, uint32_t field, void* dst_host, si
 PF_API pf_status pf_write(pf_scene* scene, uint32_t field, const void* src_host, size_t bytes);
 
 /* SimLoop.readbackOverflow() (loop.ts:59-69, 286-295) plus the neighbour-list
- * flag of FluidSystem.readbackOverflow(). */
+ * flag of FluidSystem.readbackOverflow().
+ *   grid          a cell coordinate left the reference's Morton range
+ *                 (|cell| >= 512 cells from hashOrigin; cellIndex.ts:145-169),
+ *                 exactly where the reference raises its flag
+ *   grid_clamped  (no reference counterpart) the scene's particles spread
+ *                 wider than its grid window, so some were clamped into the
+ *                 window's border cells: neighbour sets stay complete, but
+ *                 their order can depart from the reference's walk. The window
+ *                 follows the particles each substep; it is sized by
+ *                 pf_loop_desc.grid_min/max, or four times the initial extent. */
 typedef struct pf_overflow {
   uint32_t positions;
   uint32_t velocities;
@@ -421,6 +434,7 @@ typedef struct pf_overflow {
   uint32_t contacts;
   uint32_t neighbors;
   uint32_t device_error;
+  uint32_t grid_clamped;
 } pf_overflow;
 PF_API pf_status pf_overflow_read(pf_scene* scene, pf_overflow* out);
 

@@ -33,15 +33,19 @@ def assert_same(gpu: H.HashGridSnapshot, ref: dict):
 
 
 @pytest.mark.parametrize("dist", ["uniform", "blobs"])
-@pytest.mark.parametrize("n", [1_000, 100_000, 1_000_000])
+@pytest.mark.parametrize("n", [1_000, 100_000, 1_000_000, 4_000_000, 16_000_000])
 def test_linear_sort_bit_exact(oracle, pfsim, dist, n):
+    """The standalone sort workload at each of its sizes (1M, 4M, 16M) and in
+    both distributions: keys, counts, cell starts and the permutation equal
+    the oracle's stable counting sort bit for bit."""
     pos = W.sort_uniform(n, 100 + n) if dist == "uniform" else W.sort_blobs(n, 200 + n)
     g = linear_grid()
     assert_same(H.sort(pos, g), oracle_sort(oracle, pos, g))
 
 
-@pytest.mark.parametrize("n", [64, 10_000, 300_000])
+@pytest.mark.parametrize("n", [64, 10_000, 300_000, 3_000_000])
 def test_morton_sort_bit_exact(oracle, pfsim, n):
+    """The reference's Morton buckets (one radix pass of 11 bits or fewer, or two)."""
     r = np.random.default_rng(n)
     pos = np.zeros((n, 4), np.float32)
     pos[:, :3] = r.uniform(-3.0, 3.0, (n, 3))
@@ -113,3 +117,24 @@ def test_16m_properties(pfsim, dist):
     same = sk[1:] == sk[:-1]
     assert np.all(perm[1:][same] > perm[:-1][same])
     assert np.array_equal(np.sort(perm), np.arange(n))
+
+
+@pytest.mark.parametrize("cells", [(1, 1, 1), (2, 1, 1), (40, 40, 1), (64, 64, 64), (2048, 2048, 64)])
+def test_radix_plans(oracle, pfsim, cells):
+    """Grids whose keys need no, one, two and three radix passes (1 cell,
+    1 bit, 11 bits, 18 bits, 28 bits), with ragged last tiles."""
+    r = np.random.default_rng(sum(cells))
+    n = 123_457
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = r.random((n, 3)) * np.array(cells, np.float32) * 0.01
+    g = H.GridOptions(cell_size=0.01, kind="linear", dims=cells)
+    assert_same(H.sort(pos, g), oracle_sort(oracle, pos, g))
+
+
+def test_sizes_shrink_and_grow(oracle, pfsim):
+    """Successive sorts of different sizes on one workspace: each pass leaves
+    the look-back words of the next call clear."""
+    g = linear_grid()
+    for n in (300_000, 5_000, 2_000_000, 4_097, 1_000_000):
+        pos = W.sort_blobs(n, 400 + n)
+        assert_same(H.sort(pos, g), oracle_sort(oracle, pos, g))

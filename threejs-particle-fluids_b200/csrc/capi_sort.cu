@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -40,19 +41,22 @@ namespace {
 // stream run in order and reuse it; calls on different streams get their own.
 struct Workspace {
   void* scratch = nullptr;
-  size_t scratch_bytes = 0;
+  uint32_t n_cap = 0;
+  uint64_t c_cap = 0;
+  SortScratch s{};
   // staging for pf_sort_host
   void* io = nullptr;
   size_t io_bytes = 0;
-  // counters of the most recent call (its error word is read by
-  // pf_sort_device_errors)
+  // counters of the most recent sort on this stream: pf_sort's own, or the
+  // fixed block's after a pf_sort_noalloc; pf_sort_device_errors reads its
+  // error word
   uint32_t* counters = nullptr;
 };
 
 std::mutex g_ws_mutex;
 std::map<std::pair<int, cudaStream_t>, Workspace> g_ws;
 
-pf_status ensure(void** ptr, size_t* have, size_t need) {
+pf_status ensure_io(void** ptr, size_t* have, size_t need) {
   if (*have >= need && *ptr) return PF_OK;
   if (*ptr) cudaFree(*ptr);
   *ptr = nullptr;
@@ -60,9 +64,36 @@ pf_status ensure(void** ptr, size_t* have, size_t need) {
   const size_t grow = need + need / 4;
   if (cudaMalloc(ptr, grow) != cudaSuccess) {
     cudaGetLastError();
-    return fail(PF_ERR_OOM, "HashGrid: out of device memory for sort scratch");
+    return fail(PF_ERR_OOM, "HashGrid: out of device memory for sort staging");
   }
   *have = grow;
+  return PF_OK;
+}
+
+// Grows the workspace's sort scratch to hold n elements and C cells. The
+// layout follows the capacity, not the call, and a new block starts zeroed.
+pf_status ensure_scratch(Workspace& ws, uint32_t n, uint64_t C, cudaStream_t st) {
+  if (ws.scratch && ws.n_cap >= n && ws.c_cap >= C) return PF_OK;
+  if (ws.scratch) {
+    PF_CUDA(cudaStreamSynchronize(st));
+    cudaFree(ws.scratch);
+  }
+  ws.scratch = nullptr;
+  ws.counters = nullptr;
+  const uint32_t n_cap =
+      (uint32_t)std::min<uint64_t>(std::max<uint64_t>(ws.n_cap, (uint64_t)n + n / 4), (1u << 30) - 1);
+  const uint64_t c_cap = std::max<uint64_t>(ws.c_cap, C + C / 4);
+  if (cudaMalloc(&ws.scratch, sort_scratch_bytes(n_cap, c_cap)) != cudaSuccess) {
+    cudaGetLastError();
+    ws.scratch = nullptr;
+    ws.n_cap = 0;
+    ws.c_cap = 0;
+    return fail(PF_ERR_OOM, "HashGrid: out of device memory for sort scratch");
+  }
+  ws.n_cap = n_cap;
+  ws.c_cap = c_cap;
+  sort_scratch_carve(ws.scratch, n_cap, c_cap, &ws.s);
+  PF_CUDA(sort_scratch_zero(ws.s, st));
   return PF_OK;
 }
 
@@ -72,33 +103,13 @@ Workspace& workspace_for(cudaStream_t st) {
   return g_ws[{dev, st}];
 }
 
-pf_status validate(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_t* C) {
-  if (!grid) return fail(PF_ERR_INVALID, "HashGrid: grid descriptor is NULL");
-  if (!make_key_fn(*grid, kf, C)) {
-    if (!(grid->cell_size > 0))
-      return fail(PF_ERR_INVALID, "HashGrid: cellSize must be a positive finite number, got " +
-                                      std::to_string(grid->cell_size));
-    if (grid->key_kind == PF_KEY_MORTON)
-      return fail(PF_ERR_INVALID, "HashGrid: hashTableSize must be a positive power of two, got " +
-                                      std::to_string(grid->table_size));
-    return fail(PF_ERR_INVALID, "HashGrid: invalid grid descriptor");
-  }
-  if (n > 0x7fffffffu) return fail(PF_ERR_INVALID, "HashGrid: too many particles");
-  return PF_OK;
-}
-
-// Runs the sort on prepared device buffers with scratch `s`.
-void run_sort(const float4* pos, uint32_t n, const KeyFn& kf, uint64_t C, uint32_t* perm, uint32_t* start,
-              uint32_t* count, uint32_t* keys, uint32_t* overflow, const SortScratch& s, cudaStream_t st) {
-  cudaMemsetAsync(count, 0, 4ull * C, st);
-  cudaMemsetAsync(s.counters, 0, 4ull * kNumCounters, st);
-  uint32_t* ovf = overflow ? overflow : s.counters + kCounterOverflow;
-  if (overflow) cudaMemsetAsync(overflow, 0, 4, st);
-  launch_keys_hist(pos, n, kf, keys, count, ovf, st);
-  launch_sort_from_hist(keys, n, C, count, start, perm, s, st);
-}
-
 }  // namespace
+
+void sort_note_counters(cudaStream_t st, uint32_t* counters) {
+  std::lock_guard<std::mutex> g(g_ws_mutex);
+  workspace_for(st).counters = counters;
+}
+
 }  // namespace pf
 
 using namespace pf;
@@ -120,24 +131,22 @@ pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* grid, uin
                   void* stream) {
   KeyFn kf;
   uint64_t C = 0;
-  PF_TRY(validate(n, grid, &kf, &C));
+  PF_TRY(validate_sort(n, grid, &kf, &C));
   if (n > 0 && (!d_pos4 || !d_perm)) return fail(PF_ERR_INVALID, "HashGrid: NULL positions or perm");
   if (!d_start || !d_count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> g(g_ws_mutex);
   Workspace& ws = workspace_for(st);
-  PF_TRY(ensure(&ws.scratch, &ws.scratch_bytes, sort_scratch_bytes(n, C)));
-  SortScratch s;
-  sort_scratch_carve(ws.scratch, n, C, &s);
-  ws.counters = s.counters;
-  run_sort(reinterpret_cast<const float4*>(d_pos4), n, kf, C, d_perm, d_start, d_count,
-           d_keys ? d_keys : s.keys, d_overflow, s, st);
-  PF_CUDA(cudaGetLastError());
+  PF_TRY(ensure_scratch(ws, n, C, st));
+  ws.counters = ws.s.counters;
+  PF_CUDA(sort_run(reinterpret_cast<const float4*>(d_pos4), n, kf, C, d_perm, d_start, d_count,
+                   d_keys ? d_keys : ws.s.keys, d_overflow, ws.s, st));
   return PF_OK;
 }
 
 // Synchronises `stream` and returns (and clears) the device error word of the
-// standalone sort's workspace on that stream.
+// most recent standalone sort on that stream: pf_sort's workspace, or the
+// fixed block of pf_sort_noalloc when that ran last.
 pf_status pf_sort_device_errors(void* stream, uint32_t* bits) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> g(g_ws_mutex);
@@ -156,15 +165,16 @@ pf_status pf_sort_host(const float* h_pos4, uint32_t n, const pf_grid_desc* grid
                        uint32_t* h_start, uint32_t* h_count, uint32_t* h_keys, uint32_t* h_overflow) {
   KeyFn kf;
   uint64_t C = 0;
-  PF_TRY(validate(n, grid, &kf, &C));
+  PF_TRY(validate_sort(n, grid, &kf, &C));
   if (n > 0 && !h_pos4) return fail(PF_ERR_INVALID, "HashGrid: NULL positions");
   cudaStream_t st = nullptr;
   std::lock_guard<std::mutex> g(g_ws_mutex);
   Workspace& ws = workspace_for(st);
   auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
   const size_t io = al(16ull * n) + al(4ull * n) + al(4ull * C) + al(4ull * C) + al(4ull * n) + al(4);
-  PF_TRY(ensure(&ws.io, &ws.io_bytes, io));
-  PF_TRY(ensure(&ws.scratch, &ws.scratch_bytes, sort_scratch_bytes(n, C)));
+  PF_TRY(ensure_io(&ws.io, &ws.io_bytes, io));
+  PF_TRY(ensure_scratch(ws, n, C, st));
+  ws.counters = ws.s.counters;
   char* p = static_cast<char*>(ws.io);
   float4* d_pos = reinterpret_cast<float4*>(p);
   p += al(16ull * n);
@@ -177,11 +187,9 @@ pf_status pf_sort_host(const float* h_pos4, uint32_t n, const pf_grid_desc* grid
   uint32_t* d_keys = reinterpret_cast<uint32_t*>(p);
   p += al(4ull * n);
   uint32_t* d_ovf = reinterpret_cast<uint32_t*>(p);
-  SortScratch s;
-  sort_scratch_carve(ws.scratch, n, C, &s);
+  const SortScratch& s = ws.s;
   if (n) PF_CUDA(cudaMemcpyAsync(d_pos, h_pos4, 16ull * n, cudaMemcpyHostToDevice, st));
-  run_sort(d_pos, n, kf, C, d_perm, d_start, d_count, d_keys, d_ovf, s, st);
-  PF_CUDA(cudaGetLastError());
+  PF_CUDA(sort_run(d_pos, n, kf, C, d_perm, d_start, d_count, d_keys, d_ovf, s, st));
   uint32_t err = 0;
   PF_CUDA(cudaMemcpyAsync(&err, s.counters + kCounterError, 4, cudaMemcpyDeviceToHost, st));
   if (h_perm && n) PF_CUDA(cudaMemcpyAsync(h_perm, d_perm, 4ull * n, cudaMemcpyDeviceToHost, st));

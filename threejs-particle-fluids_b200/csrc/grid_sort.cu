@@ -1,16 +1,22 @@
 // grid_sort.cu — stable counting sort of particles by hash-grid cell key.
 //
 // Replaces the reference's 8-kernel HashGrid rebuild (src/core/hashGrid/
-// cellIndex.ts:113-170, sort.ts:72-192): the same histogram -> exclusive scan
-// -> scatter structure, re-planned for B200:
-//   * the histogram aggregates equal keys inside a warp with __match_any_sync,
-//     so a warp issues one L2 atomic per distinct key;
-//   * the scan is a single-pass decoupled look-back over 4096-entry tiles, so
-//     the bucket count is not capped at 1024^2 as in the two-level
-//     workgroup scan (sort.ts:22-28);
-//   * the scatter is stable: equal keys inside a warp are ranked by lane, and
-//     the (rare at low occupancy) cells filled by several warps are re-sorted
-//     by a fix-up that runs only over those cells.
+// cellIndex.ts:113-170, sort.ts:72-192): the reference's histogram ->
+// exclusive scan -> scatter becomes, for B200,
+//   * keys with every radix pass's digit counts, from shared-memory
+//     histograms (one global atomic per digit per block);
+//   * one least-significant-digit radix pass per 11 key bits (two for a
+//     128^3 grid), each a single kernel: tiles rank their elements by digit
+//     in element order with warp-aggregated ranks (__match_any_sync), find
+//     each digit's output position by a decoupled look-back over the tiles
+//     before them, and write their elements run by run through shared memory
+//     (Adinets and Merrill's "Onesweep" structure). The passes are stable,
+//     unlike the reference's atomic write cursor (sort.ts:187-192), so the
+//     permutation lists each cell's particles in ascending index;
+//   * cell counts from the sorted keys (one atomic per run of equal keys in a
+//     warp) and a single-pass decoupled look-back scan to the cell starts,
+//     so the bucket count is not capped at 1024^2 as in the two-level
+//     workgroup scan (sort.ts:22-28).
 // Every spin-wait is bounded and reports DEV_ERR_LOOKBACK_TIMEOUT.
 
 #include <cuda_runtime.h>
@@ -18,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 
 #include "grid_sort.cuh"
 
@@ -29,9 +36,25 @@ constexpr uint32_t kHistThreads = 256;
 constexpr uint32_t kScanThreads = 256;
 constexpr uint32_t kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096
-constexpr uint32_t kSmallMax = 16;     // thread-per-cell fix-up
-constexpr uint32_t kMidMax = 4096;     // CTA bitonic fix-up in shared memory
-constexpr uint32_t kFixThreads = 256;
+// radix passes: 256 threads x 16 elements per tile, elements warp-striped
+// (warp w ranks elements [512 w, 512 w + 512) of its tile, 32 per round)
+constexpr uint32_t kOsThreads = 256;
+constexpr uint32_t kOsItems = 16;
+constexpr uint32_t kOsWarps = kOsThreads / 32;
+constexpr uint32_t kOsStripe = kOsItems * 32;
+static_assert(kOsThreads * kOsItems == kRadixTile, "tile size");
+constexpr uint32_t kOsPer = kRadixMaxDigits / kOsThreads;  // digits per thread in the look-back
+// shared memory of a pass, in words: warp histograms (u16) or the staged
+// tile (keys then element indices), then each digit's first tile position
+// and first output position
+constexpr uint32_t kOsStageWords = 2 * kRadixTile;
+static_assert(kOsWarps * kRadixMaxDigits / 2 <= kOsStageWords, "histograms fit the staging area");
+constexpr size_t kOsSmemBytes = 4ull * (kOsStageWords + 2 * kRadixMaxDigits);
+// look-back status word: bits 31..30 flag (1 tile count, 2 inclusive
+// prefix), bits 29..0 the value (so n < 2^30)
+constexpr uint32_t kStAgg = 1u << 30;
+constexpr uint32_t kStInc = 2u << 30;
+constexpr uint32_t kStVal = (1u << 30) - 1u;
 constexpr uint32_t kMortonBias = 512;
 constexpr int32_t kCellCoordMax = 1 << 30;
 
@@ -80,26 +103,6 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
-}
-
-// ---------------------------------------------------------------- keys ----
-__global__ void __launch_bounds__(kHistThreads)
-k_keys_hist(const float4* __restrict__ pos, uint32_t n, KeyFn kf, uint32_t* __restrict__ keys,
-            uint32_t* __restrict__ counts, uint32_t* __restrict__ overflow) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < n;
-  uint32_t key = 0, over = 0;
-  if (valid) {
-    const float4 p = __ldg(pos + i);
-    key = cell_key(kf, p.x, p.y, p.z, &over);
-    keys[i] = key;
-  }
-  const uint32_t active = __ballot_sync(0xffffffffu, valid);
-  if (valid) {
-    const uint32_t peers = __match_any_sync(active, key);
-    if (lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + key, (uint32_t)__popc(peers));
-  }
-  if (__any_sync(0xffffffffu, over) && lane_id() == 0) atomicOr(overflow, 1u);
 }
 
 // ---------------------------------------------------------------- scan ----
@@ -227,211 +230,257 @@ k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t* __
   }
 }
 
-// ------------------------------------------------------------- scatter ----
-struct Lists {
-  uint32_t* small;
-  uint32_t* mid;
-  uint32_t* giant;
-  uint32_t small_cap, mid_cap, giant_cap;
-};
 
+// -------------------------------------------------------- keys + digits ----
+// Keys of every element with the radix digit counts of every pass, in a
+// grid-stride loop: each block keeps its digit histograms in shared memory
+// and adds them to the global counts once.
 __global__ void __launch_bounds__(kHistThreads)
-k_scatter(const uint32_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ start,
-          const uint32_t* __restrict__ counts, uint32_t* __restrict__ fill, uint32_t* __restrict__ perm,
-          uint32_t* __restrict__ dirty_bits, Lists lists, uint32_t* __restrict__ counters) {
+k_keys_digits(const float4* __restrict__ pos, uint32_t n, KeyFn kf, DigitHist h, uint32_t* __restrict__ keys,
+              uint32_t* __restrict__ overflow) {
+  extern __shared__ uint32_t sh[];
+  digit_hist_zero(sh, h);
+  __syncthreads();
+  uint32_t over_any = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 p = __ldg(pos + i);
+    uint32_t over = 0;
+    const uint32_t key = cell_key(kf, p.x, p.y, p.z, &over);
+    keys[i] = key;
+    over_any |= over;
+    digit_hist_add(sh, h, key);
+  }
+  if (__any_sync(0xffffffffu, over_any) && lane_id() == 0) atomicOr(overflow, 1u);
+  __syncthreads();
+  digit_hist_flush(sh, h);
+}
+
+// Each pass's digit counts -> each digit's first output position (one block
+// of 1024 threads per pass, two digits per thread).
+__global__ void __launch_bounds__(1024) k_digit_first(uint32_t* __restrict__ dc, uint32_t digits) {
+  __shared__ uint32_t s_warp[32];
+  uint32_t* c = dc + blockIdx.x * kRadixMaxDigits;
+  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
+  const uint32_t a = 2 * t < digits ? c[2 * t] : 0u, b = 2 * t + 1 < digits ? c[2 * t + 1] : 0u;
+  const uint32_t own = a + b;
+  uint32_t x = own;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= (uint32_t)off) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (uint32_t w = 0; w < warp; ++w) before += s_warp[w];
+  const uint32_t excl = before + x - own;
+  if (2 * t < digits) c[2 * t] = excl;
+  if (2 * t + 1 < digits) c[2 * t + 1] = excl + a;
+}
+
+// ------------------------------------------------------------ radix pass ----
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// One stable LSD pass over digit (key >> shift) & (digits - 1). Tiles are
+// numbered in launch order by a ticket, so every tile's predecessors have
+// started and its look-back ends. kFirst: the values are the element indices.
+// `status` holds this pass's look-back words (clear on entry); `clear`, when
+// given, is the next pass's region, whose row of this tile is cleared here.
+template <bool kFirst>
+__global__ void __launch_bounds__(kOsThreads, 2)
+k_radix_pass(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
+             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
+             const uint32_t* __restrict__ first, uint32_t* __restrict__ status, uint32_t* __restrict__ clear,
+             uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
+  extern __shared__ uint32_t sm[];
+  uint16_t* whist = reinterpret_cast<uint16_t*>(sm);  // [warp][digit], then the staged tile
+  uint32_t* stage_k = sm;
+  uint32_t* stage_v = sm + kRadixTile;
+  uint32_t* lstart = sm + kOsStageWords;     // first tile position of each digit
+  uint32_t* gstart = lstart + kRadixMaxDigits;  // first output position of each digit
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_wsum[kOsWarps];
+  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  for (uint32_t w = tid; w < kOsWarps * digits / 2; w += kOsThreads) sm[w] = 0u;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (clear)
+    for (uint32_t d = tid; d < kRadixMaxDigits; d += kOsThreads) clear[(size_t)tile * kRadixMaxDigits + d] = 0u;
+  const uint32_t mask = digits - 1u;
+  const uint32_t base = tile * kRadixTile + warp * kOsStripe;
+  uint32_t key[kOsItems], val[kOsItems], pos[kOsItems];
+#pragma unroll
+  for (uint32_t i = 0; i < kOsItems; ++i) {
+    const uint32_t e = base + i * 32u + lane;
+    const bool valid = e < n;
+    key[i] = valid ? __ldg(kin + e) : 0u;
+    val[i] = kFirst ? e : (valid ? __ldg(vin + e) : 0u);
+  }
+  // rank in element order inside the warp's stripe: a round's equal digits
+  // by lane, after the counts of the warp's earlier rounds
+  uint16_t* wh = whist + warp * digits;
+#pragma unroll
+  for (uint32_t i = 0; i < kOsItems; ++i) {
+    const uint32_t e = base + i * 32u + lane;
+    const uint32_t vm = __ballot_sync(0xffffffffu, e < n);
+    pos[i] = 0;
+    if (!vm) continue;  // warp-uniform
+    const uint32_t d = (key[i] >> shift) & mask;
+    uint32_t peers = 0, old = 0;
+    if (e < n) {
+      peers = __match_any_sync(vm, d);
+      old = wh[d];
+      pos[i] = old + __popc(peers & lanemask_lt());
+    }
+    __syncwarp();
+    if (e < n && lane == (uint32_t)(__ffs(peers) - 1)) wh[d] = (uint16_t)(old + __popc(peers));
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: the warps' counts -> exclusive offsets over warps; the tile's count
+  for (uint32_t d = tid; d < digits; d += kOsThreads) {
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kOsWarps; ++w) {
+      const uint32_t c = whist[w * digits + d];
+      whist[w * digits + d] = (uint16_t)sum;
+      sum += c;
+    }
+    lstart[d] = sum;
+  }
+  __syncthreads();
+  // exclusive scan of the tile's digit counts (a run of digits per thread)
+  {
+    const uint32_t per = (digits + kOsThreads - 1) / kOsThreads, d0 = tid * per;
+    uint32_t run = 0;
+    for (uint32_t q = 0; q < per; ++q)
+      if (d0 + q < digits) run += lstart[d0 + q];
+    uint32_t x = run;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= (uint32_t)off) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t acc = x - run;
+    for (uint32_t w = 0; w < warp; ++w) acc += s_wsum[w];
+    for (uint32_t q = 0; q < per; ++q)
+      if (d0 + q < digits) {
+        const uint32_t c = lstart[d0 + q];
+        lstart[d0 + q] = acc;
+        acc += c;
+      }
+  }
+  __syncthreads();
+  // publish this tile's digit counts, then look back over the preceding
+  // tiles for each digit's output position (all of a thread's digits at once)
+  const uint32_t tile_valid = min(kRadixTile, n - tile * kRadixTile);
+  uint32_t* row = status + (size_t)tile * kRadixMaxDigits;
+  uint32_t cnt[kOsPer], excl[kOsPer];
+  int32_t pred[kOsPer];
+  uint32_t pending = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < kOsPer; ++j) {
+    const uint32_t d = tid + j * kOsThreads;
+    cnt[j] = 0;
+    excl[j] = 0;
+    pred[j] = (int32_t)tile - 1;
+    if (d < digits) {
+      cnt[j] = (d + 1 < digits ? lstart[d + 1] : tile_valid) - lstart[d];
+      if (tile == 0) {
+        excl[j] = first[d];
+        st_relaxed(row + d, kStInc | (excl[j] + cnt[j]));
+      } else {
+        st_relaxed(row + d, kStAgg | cnt[j]);
+        pending |= 1u << j;
+      }
+    }
+  }
+  uint32_t spins = 0;
+  while (pending) {
+    bool waiting = false;
+#pragma unroll
+    for (uint32_t j = 0; j < kOsPer; ++j) {
+      if (!((pending >> j) & 1u)) continue;
+      const uint32_t d = tid + j * kOsThreads;
+      const uint32_t s = ld_relaxed(status + (size_t)pred[j] * kRadixMaxDigits + d);
+      const uint32_t f = s >> 30;
+      if (f == 0) {
+        waiting = true;
+        continue;
+      }
+      excl[j] += s & kStVal;
+      if (f == 2) {
+        pending &= ~(1u << j);
+        st_relaxed(row + d, kStInc | (excl[j] + cnt[j]));
+      } else {
+        --pred[j];
+      }
+    }
+    if (waiting && ++spins >= kLookbackSpinLimit) {
+      // give up: report, and publish what we have so that no later tile waits
+      atomicOr(err, DEV_ERR_LOOKBACK_TIMEOUT);
+#pragma unroll
+      for (uint32_t j = 0; j < kOsPer; ++j)
+        if ((pending >> j) & 1u) st_relaxed(row + tid + j * kOsThreads, kStInc | ((excl[j] + cnt[j]) & kStVal));
+      break;
+    }
+    if (waiting) __nanosleep(32);
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < kOsPer; ++j) {
+    const uint32_t d = tid + j * kOsThreads;
+    if (d < digits) gstart[d] = excl[j];
+  }
+  // tile positions, then the tile staged in digit order
+#pragma unroll
+  for (uint32_t i = 0; i < kOsItems; ++i) {
+    const uint32_t d = (key[i] >> shift) & mask;
+    if (base + i * 32u + lane < n) pos[i] += lstart[d] + whist[warp * digits + d];
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t i = 0; i < kOsItems; ++i)
+    if (base + i * 32u + lane < n) {
+      stage_k[pos[i]] = key[i];
+      stage_v[pos[i]] = val[i];
+    }
+  __syncthreads();
+  // out run by run: consecutive threads write consecutive positions of a digit
+  for (uint32_t k = tid; k < tile_valid; k += kOsThreads) {
+    const uint32_t kk = stage_k[k];
+    const uint32_t d = (kk >> shift) & mask;
+    const uint32_t dst = gstart[d] + (k - lstart[d]);
+    kout[dst] = kk;
+    vout[dst] = stage_v[k];
+  }
+}
+
+// A plan of no passes (one cell): the identity permutation.
+__global__ void __launch_bounds__(256) k_identity(uint32_t* __restrict__ perm, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = i;
+}
+
+// Cell counts from the sorted keys: one atomic per run of equal keys in a warp.
+__global__ void __launch_bounds__(256) k_run_counts(const uint32_t* __restrict__ sk, uint32_t n,
+                                                    uint32_t* __restrict__ count) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
-  const uint32_t key = valid ? keys[i] : 0u;
+  const uint32_t key = valid ? __ldg(sk + i) : 0u;
   const uint32_t active = __ballot_sync(0xffffffffu, valid);
   if (!valid) return;
   const uint32_t peers = __match_any_sync(active, key);
-  const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-  uint32_t base = 0;
-  // 0: nothing to record; 1/2/3: this lane's cell goes on the small / mid /
-  // giant fix-up list (its run was started by another warp)
-  uint32_t need = 0;
-  if (lane_id() == leader) {
-    const uint32_t old = atomicAdd(fill + key, (uint32_t)__popc(peers));
-    base = start[key] + old;
-    if (old != 0) {
-      const uint32_t bit = 1u << (key & 31u);
-      const uint32_t prev = atomicOr(dirty_bits + (key >> 5), bit);
-      if (!(prev & bit)) {
-        const uint32_t c = counts[key];
-        need = c <= kSmallMax ? 1u : (c <= kMidMax ? 2u : 3u);
-      }
-    }
-  }
-  // one counter atomic per warp and list for the cells this warp records
-#pragma unroll
-  for (uint32_t l = 1; l <= 3; ++l) {
-    const uint32_t mask = __ballot_sync(active, need == l);
-    if (!mask) continue;
-    const uint32_t first = (uint32_t)(__ffs(mask) - 1);
-    const uint32_t ctr = l == 1 ? kCounterSmall : (l == 2 ? kCounterMid : kCounterGiant);
-    uint32_t at = 0;
-    if (lane_id() == first) at = atomicAdd(counters + ctr, (uint32_t)__popc(mask));
-    at = __shfl_sync(active, at, first) + __popc(mask & lanemask_lt());
-    if (need == l) {
-      uint32_t* list = l == 1 ? lists.small : (l == 2 ? lists.mid : lists.giant);
-      const uint32_t cap = l == 1 ? lists.small_cap : (l == 2 ? lists.mid_cap : lists.giant_cap);
-      if (at < cap) list[at] = key;
-      else atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
-    }
-  }
-  base = __shfl_sync(active, base, leader);
-  const uint32_t slot = base + __popc(peers & lanemask_lt());
-  if (slot < n)
-    perm[slot] = i;
-  else
-    atomicOr(counters + kCounterError, DEV_ERR_SORT_CAPACITY);
-}
-
-// -------------------------------------------------------------- fix-up ----
-__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
-  const uint32_t lo = min(a, b), hi = max(a, b);
-  a = lo;
-  b = hi;
-}
-
-__global__ void __launch_bounds__(kFixThreads)
-k_fix_small(const uint32_t* __restrict__ list, const uint32_t* __restrict__ counters_len,
-            const uint32_t* __restrict__ start, const uint32_t* __restrict__ counts,
-            uint32_t* __restrict__ perm, uint32_t cap) {
-  const uint32_t total = min(*counters_len, cap);
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    const uint32_t c = list[t];
-    const uint32_t s = start[c], m = counts[c];
-    uint32_t v[kSmallMax];
-#pragma unroll
-    for (int k = 0; k < (int)kSmallMax; ++k) v[k] = (uint32_t)k < m ? perm[s + k] : 0xffffffffu;
-    // Odd-even transposition network: kSmallMax rounds sort kSmallMax keys.
-#pragma unroll
-    for (int r = 0; r < (int)kSmallMax; ++r) {
-#pragma unroll
-      for (int k = r & 1; k + 1 < (int)kSmallMax; k += 2) cswap(v[k], v[k + 1]);
-    }
-#pragma unroll
-    for (int k = 0; k < (int)kSmallMax; ++k)
-      if ((uint32_t)k < m) perm[s + k] = v[k];
-  }
-}
-
-__global__ void __launch_bounds__(kFixThreads)
-k_fix_mid(const uint32_t* __restrict__ list, const uint32_t* __restrict__ counters_len,
-          const uint32_t* __restrict__ start, const uint32_t* __restrict__ counts,
-          uint32_t* __restrict__ perm, uint32_t cap) {
-  __shared__ uint32_t sh[kMidMax];
-  const uint32_t total = min(*counters_len, cap);
-  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
-    const uint32_t c = list[t];
-    const uint32_t s = start[c], m = counts[c];
-    uint32_t P = 32;
-    while (P < m) P <<= 1;
-    for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) sh[k] = k < m ? perm[s + k] : 0xffffffffu;
-    __syncthreads();
-    for (uint32_t size = 2; size <= P; size <<= 1) {
-      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-        for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) {
-          const uint32_t j = k ^ stride;
-          if (j > k) {
-            const uint32_t a = sh[k], b = sh[j];
-            const bool up = (k & size) == 0;
-            if ((a > b) == up) {
-              sh[k] = b;
-              sh[j] = a;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) perm[s + k] = sh[k];
-    __syncthreads();
-  }
-}
-
-// Giant cells (> kMidMax elements): one CTA runs a stable LSD radix sort
-// (8-bit digits) over the cell's run, ping-ponging with the same range of a
-// scratch buffer, 256 elements per round.
-__global__ void __launch_bounds__(kFixThreads)
-k_fix_giant(const uint32_t* __restrict__ list, const uint32_t* __restrict__ counters_len,
-            const uint32_t* __restrict__ start, const uint32_t* __restrict__ counts,
-            uint32_t* __restrict__ perm, uint32_t* __restrict__ tmp, uint32_t cap, uint32_t value_bits) {
-  __shared__ uint32_t hist[256];
-  __shared__ uint32_t offs[256];
-  __shared__ uint32_t wcount[kFixThreads / 32][256];
-  const uint32_t total = min(*counters_len, cap);
-  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  const uint32_t passes = (value_bits + 7) / 8;
-  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
-    const uint32_t c = list[t];
-    const uint32_t s = start[c], m = counts[c];
-    uint32_t* src = perm + s;
-    uint32_t* dst = tmp + s;
-    for (uint32_t pass = 0; pass < passes; ++pass) {
-      const uint32_t shift = 8 * pass;
-      hist[threadIdx.x] = 0;
-      for (uint32_t w = 0; w < kFixThreads / 32; ++w) wcount[w][threadIdx.x] = 0;
-      __syncthreads();
-      for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&hist[(src[k] >> shift) & 255u], 1u);
-      __syncthreads();
-      if (warp == 0) {
-        uint32_t run = 0;
-        for (uint32_t q = 0; q < 8; ++q) {
-          const uint32_t d = q * 32 + lane;
-          const uint32_t h = hist[d];
-          uint32_t x = h;
-#pragma unroll
-          for (int off = 1; off < 32; off <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
-            if (lane >= (uint32_t)off) x += y;
-          }
-          offs[d] = run + x - h;
-          run += __shfl_sync(0xffffffffu, x, 31);
-        }
-      }
-      __syncthreads();
-      for (uint32_t r = 0; r < m; r += blockDim.x) {
-        const uint32_t k = r + threadIdx.x;
-        const bool valid = k < m;
-        const uint32_t val = valid ? src[k] : 0u;
-        const uint32_t d = (val >> shift) & 255u;
-        const uint32_t active = __ballot_sync(0xffffffffu, valid);
-        uint32_t peers = 0, rank = 0;
-        if (valid) {
-          peers = __match_any_sync(active, d);
-          rank = __popc(peers & lanemask_lt());
-          if (lane == (uint32_t)(__ffs(peers) - 1)) wcount[warp][d] = __popc(peers);
-        }
-        __syncthreads();
-        if (valid) {
-          uint32_t before = 0;
-          for (uint32_t w = 0; w < warp; ++w) before += wcount[w][d];
-          dst[offs[d] + before + rank] = val;
-        }
-        __syncthreads();
-        {
-          const uint32_t dd = threadIdx.x;
-          uint32_t add = 0;
-          for (uint32_t w = 0; w < kFixThreads / 32; ++w) {
-            add += wcount[w][dd];
-            wcount[w][dd] = 0;
-          }
-          offs[dd] += add;
-        }
-        __syncthreads();
-      }
-      uint32_t* sw = src;
-      src = dst;
-      dst = sw;
-      __syncthreads();
-    }
-    if (src != perm + s) {
-      for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) perm[s + k] = src[k];
-    }
-    __syncthreads();
-  }
+  if (lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(count + key, (uint32_t)__popc(peers));
 }
 
 }  // namespace
@@ -465,100 +514,161 @@ bool make_key_fn(const pf_grid_desc& g, KeyFn* out, uint64_t* cells) {
   return true;
 }
 
+pf_status validate_sort(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_t* C) {
+  if (!grid) return fail(PF_ERR_INVALID, "HashGrid: grid descriptor is NULL");
+  if (!make_key_fn(*grid, kf, C)) {
+    if (!(grid->cell_size > 0) || !std::isfinite(grid->cell_size))
+      return fail(PF_ERR_INVALID, "HashGrid: cellSize must be a positive finite number, got " +
+                                      std::to_string(grid->cell_size));
+    if (grid->key_kind == PF_KEY_MORTON)
+      return fail(PF_ERR_INVALID, "HashGrid: hashTableSize must be a positive power of two, got " +
+                                      std::to_string(grid->table_size));
+    return fail(PF_ERR_INVALID, "HashGrid: invalid grid descriptor");
+  }
+  if (n >= (1u << 30)) return fail(PF_ERR_INVALID, "HashGrid: too many particles (at most 2^30 - 1)");
+  return PF_OK;
+}
+
+RadixPlan radix_plan(uint64_t cells) {
+  uint32_t bits = 0;
+  while (bits < 40 && (1ull << bits) < cells) ++bits;
+  RadixPlan p;
+  p.passes = (bits + kRadixMaxBits - 1) / kRadixMaxBits;
+  p.width = p.passes ? (bits + p.passes - 1) / p.passes : 0;
+  p.digits = 1u << p.width;
+  return p;
+}
+
 uint32_t scan_tiles(uint64_t n) { return (uint32_t)((n + kScanTile - 1) / kScanTile); }
 
-namespace {
-struct ListCaps {
-  uint32_t small, mid, giant;
-};
-ListCaps list_caps(uint32_t n, uint64_t C) {
-  const uint64_t cmax = std::min<uint64_t>(C, n / 2 + 1);
-  ListCaps c;
-  c.small = (uint32_t)cmax;
-  c.mid = (uint32_t)std::min<uint64_t>(C, n / (kSmallMax + 1) + 1);
-  c.giant = (uint32_t)std::min<uint64_t>(C, n / (kMidMax + 1) + 1);
-  return c;
+uint32_t keys_grid(uint32_t n, uint32_t threads) {
+  return std::max<uint32_t>(1, std::min<uint32_t>(div_up(std::max<uint32_t>(n, 1), threads), (uint32_t)sm_count() * 8));
 }
+
+namespace {
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+uint32_t radix_tiles(uint32_t n) { return std::max<uint32_t>(1, div_up(n, kRadixTile)); }
 }  // namespace
 
 size_t sort_scratch_bytes(uint32_t n, uint64_t C) {
-  const ListCaps lc = list_caps(n, C);
   size_t b = 0;
-  b += align256(4ull * n);                    // keys
-  b += align256(4ull * C);                    // fill
-  b += align256(4ull * ((C + 31) / 32));      // dirty bits
-  b += align256(4ull * ((uint64_t)lc.small + lc.mid + lc.giant));  // lists
-  b += align256(8ull * scan_tiles(C));        // tile status
-  b += align256(4ull * kNumCounters);         // counters
-  b += align256(4ull * n);                    // radix tmp
+  b += 5 * align256(4ull * n);                                          // keys, ka, va, kb, vb
+  b += align256(4ull * kRadixMaxPasses * kRadixMaxDigits);             // digit counts
+  b += align256(4ull * kRadixMaxPasses * radix_tiles(n) * kRadixMaxDigits);  // look-back words
+  b += align256(8ull * scan_tiles(std::max<uint64_t>(C, 1)));           // scan tile status
+  b += align256(4ull * kNumCounters);                                   // counters
   return b;
 }
 
 void sort_scratch_carve(void* base, uint32_t n, uint64_t C, SortScratch* s) {
-  const ListCaps lc = list_caps(n, C);
   char* p = static_cast<char*>(base);
-  s->keys = reinterpret_cast<uint32_t*>(p);
-  p += align256(4ull * n);
-  s->fill = reinterpret_cast<uint32_t*>(p);
-  p += align256(4ull * C);
-  s->dirty_bits = reinterpret_cast<uint32_t*>(p);
-  p += align256(4ull * ((C + 31) / 32));
-  s->lists = reinterpret_cast<uint32_t*>(p);
-  p += align256(4ull * ((uint64_t)lc.small + lc.mid + lc.giant));
-  s->tile_status = reinterpret_cast<uint64_t*>(p);
-  p += align256(8ull * scan_tiles(C));
-  s->counters = reinterpret_cast<uint32_t*>(p);
-  p += align256(4ull * kNumCounters);
-  s->radix_tmp = reinterpret_cast<uint32_t*>(p);
+  auto take = [&](size_t bytes) {
+    char* q = p;
+    p += align256(bytes);
+    return q;
+  };
+  s->keys = reinterpret_cast<uint32_t*>(take(4ull * n));
+  s->ka = reinterpret_cast<uint32_t*>(take(4ull * n));
+  s->va = reinterpret_cast<uint32_t*>(take(4ull * n));
+  s->kb = reinterpret_cast<uint32_t*>(take(4ull * n));
+  s->vb = reinterpret_cast<uint32_t*>(take(4ull * n));
+  s->digit_count = reinterpret_cast<uint32_t*>(take(4ull * kRadixMaxPasses * kRadixMaxDigits));
+  s->tiles_cap = radix_tiles(n);
+  s->status = reinterpret_cast<uint32_t*>(take(4ull * kRadixMaxPasses * s->tiles_cap * kRadixMaxDigits));
+  s->scan_tiles_cap = scan_tiles(std::max<uint64_t>(C, 1));
+  s->scan_status = reinterpret_cast<uint64_t*>(take(8ull * s->scan_tiles_cap));
+  s->counters = reinterpret_cast<uint32_t*>(take(4ull * kNumCounters));
   s->n_cap = n;
   s->c_cap = (uint32_t)C;
-  s->list_cap = lc.small;
-  s->tiles_cap = scan_tiles(C);
 }
 
-void launch_keys_hist(const float4* pos, uint32_t n, const KeyFn& kf, uint32_t* keys, uint32_t* counts,
-                      uint32_t* overflow, cudaStream_t st) {
-  if (n == 0) return;
-  k_keys_hist<<<div_up(n, kHistThreads), kHistThreads, 0, st>>>(pos, n, kf, keys, counts, overflow);
+cudaError_t sort_scratch_zero(const SortScratch& s, cudaStream_t st) {
+  // the look-back words, digit counts, scan status and counters
+  const char* a = reinterpret_cast<const char*>(s.digit_count);
+  const char* b = reinterpret_cast<const char*>(s.counters) + 4ull * kNumCounters;
+  return cudaMemsetAsync(const_cast<char*>(a), 0, (size_t)(b - a), st);
 }
 
-void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* zero_out, uint64_t n,
-                           uint64_t* tile_status, uint32_t* counters, cudaStream_t st) {
+void launch_keys_digits(const float4* pos, uint32_t n, const KeyFn& kf, const RadixPlan& plan, uint32_t* keys,
+                        uint32_t* overflow, const SortScratch& s, cudaStream_t st) {
   if (n == 0) return;
+  const DigitHist h = digit_hist(plan, s);
+  k_keys_digits<<<keys_grid(n, kHistThreads), kHistThreads, 4ull * plan.passes * plan.digits, st>>>(pos, n, kf, h, keys,
+                                                                                                   overflow);
+}
+
+cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* zero_out, uint64_t n,
+                                  uint64_t* tile_status, uint32_t* counters, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
   const uint32_t tiles = scan_tiles(n);
-  cudaMemsetAsync(tile_status, 0, 8ull * tiles, st);
-  cudaMemsetAsync(counters + kCounterTicket, 0, 4, st);
+  if (cudaError_t e = cudaMemsetAsync(tile_status, 0, 8ull * tiles, st); e != cudaSuccess) return e;
+  if (cudaError_t e = cudaMemsetAsync(counters + kCounterTicket, 0, 4, st); e != cudaSuccess) return e;
   k_scan<<<tiles, kScanThreads, 0, st>>>(in, out, zero_out, n, tile_status, counters);
+  return cudaGetLastError();
 }
 
-void launch_sort_from_hist(const uint32_t* keys, uint32_t n, uint64_t C, const uint32_t* counts,
-                           uint32_t* start, uint32_t* perm, const SortScratch& s, cudaStream_t st) {
-  if (C == 0) return;
-  const ListCaps lc = list_caps(n, C);
-  // Reset the fix-up lists and dirty bits (the error word is left to the caller).
-  cudaMemsetAsync(s.counters + kCounterSmall, 0, 3 * 4, st);
-  cudaMemsetAsync(s.dirty_bits, 0, 4ull * ((C + 31) / 32), st);
-  launch_exclusive_scan(counts, start, s.fill, C, s.tile_status, s.counters, st);
-  if (n == 0) return;
-  Lists L;
-  L.small = s.lists;
-  L.mid = s.lists + lc.small;
-  L.giant = s.lists + lc.small + lc.mid;
-  L.small_cap = lc.small;
-  L.mid_cap = lc.mid;
-  L.giant_cap = lc.giant;
-  k_scatter<<<div_up(n, kHistThreads), kHistThreads, 0, st>>>(keys, n, start, counts, s.fill, perm,
-                                                             s.dirty_bits, L, s.counters);
-  const int sms = sm_count();
-  k_fix_small<<<sms * 8, kFixThreads, 0, st>>>(L.small, s.counters + kCounterSmall, start, counts, perm,
-                                               L.small_cap);
-  k_fix_mid<<<sms * 4, kFixThreads, 0, st>>>(L.mid, s.counters + kCounterMid, start, counts, perm,
-                                             L.mid_cap);
-  uint32_t bits = 1;
-  while (bits < 32 && (1ull << bits) < n) ++bits;
-  k_fix_giant<<<sms, kFixThreads, 0, st>>>(L.giant, s.counters + kCounterGiant, start, counts, perm,
-                                           s.radix_tmp, L.giant_cap, bits);
+cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const RadixPlan& plan, uint32_t* count,
+                             uint32_t* start, uint32_t* perm, const SortScratch& s, cudaStream_t st) {
+  if (C == 0) return cudaSuccess;
+  if (cudaError_t e = cudaMemsetAsync(count, 0, 4ull * C, st); e != cudaSuccess) return e;
+  if (n > 0) {
+    const uint32_t tiles = radix_tiles(n);
+    const uint32_t* sorted = keys;
+    if (plan.passes == 0) {
+      k_identity<<<div_up(n, 256), 256, 0, st>>>(perm, n);
+    } else {
+      static bool attr_set = false;  // per process; the attribute is per function and device
+      if (!attr_set) {
+        cudaFuncSetAttribute(k_radix_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOsSmemBytes);
+        cudaFuncSetAttribute(k_radix_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOsSmemBytes);
+        attr_set = true;
+      }
+      if (cudaError_t e = cudaMemsetAsync(s.counters + kCounterPass0, 0, 4 * kRadixMaxPasses, st); e != cudaSuccess)
+        return e;
+      k_digit_first<<<plan.passes, 1024, 0, st>>>(s.digit_count, plan.digits);
+      const size_t region = (size_t)s.tiles_cap * kRadixMaxDigits;
+      const uint32_t* kin = keys;
+      const uint32_t* vin = nullptr;
+      for (uint32_t p = 0; p < plan.passes; ++p) {
+        const bool last = p + 1 == plan.passes;
+        // pass outputs: 0 -> (ka, va), 1 -> (kb, vb), the last -> (sorted keys, perm)
+        uint32_t* kout = last ? (p == 2 ? s.ka : s.kb) : (p == 0 ? s.ka : s.kb);
+        uint32_t* vout = last ? perm : (p == 0 ? s.va : s.vb);
+        uint32_t* clear = plan.passes >= 2 ? s.status + ((p + 1) % plan.passes) * region : nullptr;
+        if (p == 0)
+          k_radix_pass<true><<<tiles, kOsThreads, kOsSmemBytes, st>>>(
+              kin, vin, n, kout, vout, p * plan.width, plan.digits, s.digit_count + p * kRadixMaxDigits,
+              s.status + p * region, clear, s.counters + kCounterPass0 + p, s.counters + kCounterError);
+        else
+          k_radix_pass<false><<<tiles, kOsThreads, kOsSmemBytes, st>>>(
+              kin, vin, n, kout, vout, p * plan.width, plan.digits, s.digit_count + p * kRadixMaxDigits,
+              s.status + p * region, clear, s.counters + kCounterPass0 + p, s.counters + kCounterError);
+        kin = kout;
+        vin = vout;
+      }
+      sorted = kin;
+      // one pass: nothing clears its look-back words for the next call
+      if (plan.passes == 1)
+        if (cudaError_t e = cudaMemsetAsync(s.status, 0, 4ull * tiles * kRadixMaxDigits, st); e != cudaSuccess) return e;
+    }
+    k_run_counts<<<div_up(n, 256), 256, 0, st>>>(sorted, n, count);
+  }
+  if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
+  return launch_exclusive_scan(count, start, nullptr, C, s.scan_status, s.counters, st);
+}
+
+cudaError_t sort_run(const float4* pos, uint32_t n, const KeyFn& kf, uint64_t C, uint32_t* perm, uint32_t* start,
+                     uint32_t* count, uint32_t* keys, uint32_t* overflow, const SortScratch& s, cudaStream_t st) {
+  const RadixPlan plan = radix_plan(C);
+  if (cudaError_t e = cudaMemsetAsync(s.counters, 0, 4ull * kNumCounters, st); e != cudaSuccess) return e;
+  if (cudaError_t e = cudaMemsetAsync(s.digit_count, 0, 4ull * kRadixMaxPasses * kRadixMaxDigits, st);
+      e != cudaSuccess)
+    return e;
+  uint32_t* ovf = overflow ? overflow : s.counters + kCounterOverflow;
+  if (overflow)
+    if (cudaError_t e = cudaMemsetAsync(overflow, 0, 4, st); e != cudaSuccess) return e;
+  launch_keys_digits(pos, n, kf, plan, keys, ovf, s, st);
+  return launch_grid_sort(keys, n, C, plan, count, start, perm, s, st);
 }
 
 }  // namespace pf

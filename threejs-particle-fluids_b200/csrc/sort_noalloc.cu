@@ -9,22 +9,33 @@
 // a workspace that it grows with cudaMalloc; this entry point instead uses one
 // fixed block of device memory that is part of the library image.
 //
-// The scratch block below is a file-scope __device__ array, so every GPU that
-// loads libpfsim.so holds it (kNoAllocScratchBytes, about 21 MB) until the
-// process exits. Its size caps the problem: at most kNoAllocMaxParticles
-// particles and kNoAllocMaxCells cells per call.
+// The scratch block below is a file-scope __device__ array of
+// kNoAllocScratchBytes (27 MiB). Its size caps the problem: at most
+// kNoAllocMaxParticles particles and kNoAllocMaxCells cells per call. The
+// CUDA runtime loads this file's device code lazily (CUDA 12 defaults to
+// lazy module loading), so the block is reserved on a device by the first
+// call there, when the address lookup below loads the module, and it stays
+// reserved until the process exits. A caller whose own pool takes the
+// device's memory should therefore make one call per device before the pool
+// claims it; a call with n = 0 and no start/count buffers does only this
+// set-up. The lookup is also why that first call must come before any stream
+// capture begins.
 //
 // In host code the name g_noalloc_scratch is only a stand-in for the device
 // symbol, not a device address: passing it to a kernel would fault, or on a
 // system where the GPU can reach host memory, silently use the wrong memory.
 // The real address comes from cudaGetSymbolAddress, once per device, with
-// that device current; the first pf_sort_noalloc call on a device does this
-// set-up, so make that first call before any stream capture begins.
+// that device current.
 //
 // All calls share the one block and it keeps the last call's contents: each
-// call clears what must start at zero itself, and two calls whose GPU work
+// call clears what must start at zero itself (the radix passes leave their
+// look-back words clear for the next call), and two calls whose GPU work
 // overlaps (for example on two streams) race on the block and corrupt each
 // other's results. Serialise them.
+//
+// Errors found on the device (a bounded look-back wait that expired) go to
+// the block's error word; pf_sort_device_errors on the call's stream reads
+// and clears it, as it does for pf_sort.
 
 #include <cuda_runtime.h>
 
@@ -39,7 +50,7 @@ namespace {
 
 constexpr uint32_t kNoAllocMaxParticles = 1u << 20;  // 1,048,576
 constexpr uint64_t kNoAllocMaxCells = 1ull << 21;    // 2,097,152 (a 128^3 grid)
-constexpr size_t kNoAllocScratchBytes = 21ull << 20; // >= sort_scratch_bytes(max particles, max cells)
+constexpr size_t kNoAllocScratchBytes = 27ull << 20; // >= sort_scratch_bytes(max particles, max cells)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -74,33 +85,31 @@ using namespace pf;
 extern "C" pf_status pf_sort_noalloc(const float* d_pos4, uint32_t n, const pf_grid_desc* grid,
                                      uint32_t* d_perm, uint32_t* d_start, uint32_t* d_count,
                                      uint32_t* d_keys, uint32_t* d_overflow, void* stream) {
-  if (!grid) return fail(PF_ERR_INVALID, "HashGrid: grid descriptor is NULL");
   KeyFn kf;
   uint64_t C = 0;
-  if (!make_key_fn(*grid, &kf, &C)) return fail(PF_ERR_INVALID, "HashGrid: invalid grid descriptor");
+  PF_TRY(validate_sort(n, grid, &kf, &C));
   if (n > kNoAllocMaxParticles)
     return fail(PF_ERR_INVALID, "HashGrid: pf_sort_noalloc takes at most " + std::to_string(kNoAllocMaxParticles) +
                                     " particles, got " + std::to_string(n) + " (use pf_sort)");
   if (C > kNoAllocMaxCells)
     return fail(PF_ERR_INVALID, "HashGrid: pf_sort_noalloc takes at most " + std::to_string(kNoAllocMaxCells) +
                                     " cells, got " + std::to_string(C) + " (use pf_sort)");
-  if (sort_scratch_bytes(n, C) > kNoAllocScratchBytes)
-    return fail(PF_ERR_INVALID, "HashGrid: pf_sort_noalloc scratch too small for this size (use pf_sort)");
+  if (sort_scratch_bytes(kNoAllocMaxParticles, kNoAllocMaxCells) > kNoAllocScratchBytes)
+    return fail(PF_ERR_INVALID, "HashGrid: pf_sort_noalloc scratch block is smaller than its limits need");
+  void* base = nullptr;
+  // set-up only: the block's address on this device (see the file comment)
+  if (n == 0 && !d_start && !d_count) return noalloc_scratch(&base);
   if (n > 0 && (!d_pos4 || !d_perm)) return fail(PF_ERR_INVALID, "HashGrid: NULL positions or perm");
   if (!d_start || !d_count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
 
-  void* base = nullptr;
   PF_TRY(noalloc_scratch(&base));
+  // carved for the block's limits, whatever this call's size: the look-back
+  // words stay where the previous call cleared them
   SortScratch s;
-  sort_scratch_carve(base, n, C, &s);
+  sort_scratch_carve(base, kNoAllocMaxParticles, kNoAllocMaxCells, &s);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // What must start at zero: the histogram, the counters and the flag.
-  PF_CUDA(cudaMemsetAsync(d_count, 0, 4ull * C, st));
-  PF_CUDA(cudaMemsetAsync(s.counters, 0, 4ull * kNumCounters, st));
-  uint32_t* ovf = d_overflow ? d_overflow : s.counters + kCounterOverflow;
-  if (d_overflow) PF_CUDA(cudaMemsetAsync(d_overflow, 0, 4, st));
-  launch_keys_hist(reinterpret_cast<const float4*>(d_pos4), n, kf, d_keys ? d_keys : s.keys, d_count, ovf, st);
-  launch_sort_from_hist(d_keys ? d_keys : s.keys, n, C, d_count, d_start, d_perm, s, st);
-  PF_CUDA(cudaGetLastError());
+  PF_CUDA(sort_run(reinterpret_cast<const float4*>(d_pos4), n, kf, C, d_perm, d_start, d_count,
+                   d_keys ? d_keys : s.keys, d_overflow, s, st));
+  sort_note_counters(st, s.counters);
   return PF_OK;
 }

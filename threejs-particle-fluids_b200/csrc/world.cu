@@ -47,19 +47,66 @@ __global__ void k_tick(WorldView V, uint32_t nscenes, uint32_t sub) {
 }
 
 // ------------------------------------------------------------ integrate ----
-// integrate.ts:25-34
+// integrate.ts:25-34, and the cell bounds of every scene's predicted
+// positions (the grid window follows them; scenes past their substeps give
+// their unchanged ones). A 256-slot block belongs to one scene.
 __global__ void __launch_bounds__(kBlock) k_predict(WorldView V, uint32_t sub) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
   const float4 x = V.cur.x[k];
-  if (!(x.w > 0.0f)) return;
-  const float4 v = V.cur.v[k];
-  const float dt = S.dt;
-  const f3 vel = xyz(v) + mk(S.gx, S.gy, S.gz) * dt;
-  V.cur.v[k] = with_w(vel, 0.0f);
-  V.cur.xs[k] = with_w(xyz(x) + vel * dt, x.w);
+  f3 p = mk(0.0f, 0.0f, 0.0f);
+  if (sub < S.substeps && x.w > 0.0f) {
+    const float4 v = V.cur.v[k];
+    const float dt = S.dt;
+    const f3 vel = xyz(v) + mk(S.gx, S.gy, S.gz) * dt;
+    V.cur.v[k] = with_w(vel, 0.0f);
+    p = xyz(x) + vel * dt;
+    V.cur.xs[k] = with_w(p, x.w);
+  } else if (S.has_grid) {
+    p = xyz(V.cur.xs[k]);
+  }
+  if (S.has_grid) bbox_block_add(V, S, s, k < S.seg_start + S.cap, p);
+}
+
+// The cell bounds of every scene's predicted positions, where no predict
+// pass gathered them (the one-time init pass and the autotuner's sort).
+__global__ void __launch_bounds__(kBlock) k_bbox(WorldView V) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = scene_index(V, k);
+  const DevScene& S = V.scenes[s];
+  if (S.has_grid) bbox_block_add(V, S, s, k < S.seg_start + S.cap, xyz(V.cur.xs[k]));
+}
+
+// Places each grid scene's window for this substep: the least move of the
+// build-time window (lo0) that covers the scene's cell bounds, or lo0 where
+// the bounds are wider than the window (the keys then clamp and flag). The
+// bounds are reset for the next substep.
+__global__ void k_grid_fit(WorldView V, uint32_t nscenes) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nscenes) return;
+  DevScene& S = V.scenes_rw[s];
+  if (!S.has_grid) return;
+  int32_t* b = V.bbox + 6 * s;
+  float big = 0.0f;
+  const float org[3] = {S.ox, S.oy, S.oz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int64_t mn = b[a], mx = b[a + 3], d = S.dims[a];
+    int64_t lo = S.lo0[a];
+    if (mn <= mx && mx - mn + 1 <= d) {
+      if (lo > mn) lo = mn;
+      if (lo + d - 1 < mx) lo = mx - d + 1;
+    }
+    S.lo[a] = (int32_t)lo;
+    b[a] = INT32_MAX;
+    b[a + 3] = INT32_MIN;
+    big = fmaxf(big, fabsf(org[a]) + fmaxf(fabsf((float)lo), fabsf((float)(lo + d))) * S.cell);
+  }
+  // the neighbour walk prunes a cell only when its box, widened by this
+  // slack (far above the f32 rounding of cell_of and of the box edges), is
+  // out of reach
+  S.prune_slack = big * (1.0f / 65536.0f) + 1e-9f;
 }
 
 // integrate.ts:36-44
@@ -76,36 +123,36 @@ __global__ void __launch_bounds__(kBlock) k_advect(WorldView V, uint32_t sub) {
 }
 
 // ---------------------------------------------------------------- grid ----
-// Keys by particle id (cell of the predicted position in the scene's linear
-// grid, offset by the scene's key base; dead padding goes to the scene's
-// last key) with a warp-aggregated histogram.
-__global__ void __launch_bounds__(kBlock) k_keys(WorldView V) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = k < V.n;
-  uint32_t key = 0;
-  bool clamped = false;
-  uint32_t s = 0;
-  if (valid) {
-    s = scene_index(V, k);
+// Keys by particle id (cell of the predicted position in the scene's grid
+// window, offset by the scene's key base; dead padding goes to the scene's
+// last key), with the radix digit counts of the sort in a block histogram
+// (grid-stride loop, one flush per block).
+__global__ void __launch_bounds__(kBlock) k_keys(WorldView V, DigitHist h) {
+  extern __shared__ uint32_t sh[];
+  digit_hist_zero(sh, h);
+  __syncthreads();
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < V.n; k += gridDim.x * blockDim.x) {
+    const uint32_t s = scene_index(V, k);
     const DevScene& S = V.scenes[s];
     const uint32_t id = V.ids[k];
+    uint32_t key;
+    bool clamped = false, ref_over = false;
     if (id >= S.seg_start + S.cap) {
       key = S.cell_base + S.cells;
     } else if (S.has_grid) {
       int32_t cx, cy, cz;
-      local_cell(S, xyz(V.cur.xs[k]), &cx, &cy, &cz, &clamped);
+      local_cell(S, xyz(V.cur.xs[k]), &cx, &cy, &cz, &clamped, &ref_over);
       key = S.cell_base + (uint32_t)cx + S.dims[0] * ((uint32_t)cy + S.dims[1] * (uint32_t)cz);
     } else {
       key = S.cell_base + (id - S.seg_start);
     }
     V.keys[id] = key;
+    digit_hist_add(sh, h, key);
+    if (clamped) atomicOr(V.flags + s * kNumFlags + FLAG_CLAMP, 1u);
+    if (ref_over) atomicOr(V.flags + s * kNumFlags + FLAG_GRID, 1u);
   }
-  const uint32_t active = __ballot_sync(0xffffffffu, valid);
-  if (valid) {
-    const uint32_t peers = __match_any_sync(active, key);
-    if (lane_of() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(V.ccount + key, (uint32_t)__popc(peers));
-    if (clamped) atomicOr(V.flags + s * kNumFlags + FLAG_GRID, 1u);
-  }
+  __syncthreads();
+  digit_hist_flush(sh, h);
 }
 
 // Gather the per-slot state into cell order: new slot k takes particle
@@ -1154,10 +1201,20 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
             mn[a] = std::min(mn[a], (double)sp.pos4[4 * i + a]);
             mx[a] = std::max(mx[a], (double)sp.pos4[4 * i + a]);
           }
+        // a window four times the initial extent per axis (at least 16
+        // cells more), centred on the particles: it moves with them each
+        // substep, so it clamps only once the particles spread wider than it
+        double ext[3], cells_w = 1.0;
         for (int a = 0; a < 3; ++a) {
-          const double ext = std::max(mx[a] - mn[a], 4 * h);
-          mn[a] -= 0.5 * ext;
-          mx[a] += 0.5 * ext;
+          ext[a] = std::max(4.0 * (mx[a] - mn[a]), (mx[a] - mn[a]) + 16.0 * h);
+          cells_w *= ext[a] / h + 5.0;
+        }
+        // at most 2^24 cells of window: shrink it evenly past that
+        const double shrink = cells_w > double(1u << 24) ? std::cbrt(double(1u << 24) / cells_w) : 1.0;
+        for (int a = 0; a < 3; ++a) {
+          const double c = 0.5 * (mn[a] + mx[a]), half = 0.5 * std::max(ext[a] * shrink, mx[a] - mn[a]);
+          mn[a] = c - half;
+          mx[a] = c + half;
         }
         if (!plan_only) {
           SceneSpec& w = *specs[s];
@@ -1174,6 +1231,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         const int64_t lo = (int64_t)std::floor((mn[a] - org[a]) / cs) - 2;
         const int64_t hi = (int64_t)std::floor((mx[a] - org[a]) / cs) + 2;
         S.lo[a] = (int32_t)lo;
+        S.lo0[a] = (int32_t)lo;
         S.dims[a] = (uint32_t)(hi - lo + 1);
         cells *= S.dims[a];
       }
@@ -1634,6 +1692,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.n_fchunk = (uint32_t)fchunk.size();
     base_.n_cchunk = (uint32_t)cchunk.size();
     base_.flags = cv.take<uint32_t>(K * kNumFlags);
+    base_.bbox = cv.take<int32_t>(6 * K);
     base_.clocks = cv.take<float>(K);
     base_.fluids = cv.take<DevFluid>(h_fluids_.size());
     base_.bnds = cv.take<DevBoundary>(h_bnds_.size());
@@ -1753,6 +1812,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   Carver cv{static_cast<char*>(arena_)};
   layout(cv);
   sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, cells_, &sort_);
+  radix_ = radix_plan(cells_);
   base_.scenes = base_.scenes_rw;
   base_.n = n_;
   base_.prim_stride = prim_stride_;
@@ -1785,7 +1845,19 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     return PF_OK;
   };
   PF_CUDA(cudaMemsetAsync(arena_, 0, probe.off, stream_));
+  PF_CUDA(sort_scratch_zero(sort_, stream_));
   PF_TRY(up(base_.scenes_rw, h_scenes_.data(), sizeof(DevScene) * K));
+  {
+    // empty cell bounds: the predict pass narrows them (a pageable source:
+    // the copy has read it when the call returns)
+    std::vector<int32_t> empty(6 * K, 0);
+    for (uint32_t s = 0; s < K; ++s)
+      for (int a = 0; a < 3; ++a) {
+        empty[6 * s + a] = INT32_MAX;
+        empty[6 * s + a + 3] = INT32_MIN;
+      }
+    PF_TRY(up(base_.bbox, empty.data(), 4ull * empty.size()));
+  }
   PF_TRY(up(base_.chunk_scene, chunk.data(), 4 * chunk.size()));
   PF_TRY(up(const_cast<uint32_t*>(base_.fchunk), fchunk.data(), 4 * fchunk.size()));
   PF_TRY(up(const_cast<uint32_t*>(base_.cchunk), cchunk.data(), 4 * cchunk.size()));
@@ -2226,13 +2298,18 @@ void World::launch_tiled(K kernel, size_t smem, const WorldView& V, A... args) {
 
 // Keys of the current predicted positions, stable sort, permute into the
 // other buffer; `parity` names the current buffer.
-void World::run_sort_and_permute(uint32_t parity, bool) {
+void World::run_sort_and_permute(uint32_t parity, bool bbox_ready) {
   const WorldView V = view(parity);
-  cudaMemsetAsync(V.ccount, 0, 4ull * cells_, stream_);
+  const uint32_t K = (uint32_t)h_scenes_.size();
+  if (!bbox_ready) launch_slots(k_bbox, n_, stream_, V);
+  k_grid_fit<<<div_up(K, 128), 128, 0, stream_>>>(V, K);
+  ++t_launches;
   cudaMemsetAsync(sort_.counters, 0, 4ull * kNumCounters, stream_);
-  launch_slots(k_keys, n_, stream_, V);
-  launch_sort_from_hist(V.keys, n_, cells_, V.ccount, V.cstart, V.perm, sort_, stream_);
-  t_launches += 5;  // scan, scatter and the three fix-up tiers
+  cudaMemsetAsync(sort_.digit_count, 0, 4ull * kRadixMaxPasses * kRadixMaxDigits, stream_);
+  k_keys<<<keys_grid(n_, kBlock), kBlock, 4ull * radix_.passes * radix_.digits, stream_>>>(V, digit_hist(radix_, sort_));
+  launch_grid_sort(V.keys, n_, cells_, radix_, V.ccount, V.cstart, V.perm, sort_, stream_);
+  // keys, then the digit scan, the radix passes, the run counts and the scan
+  t_launches += 1 + (radix_.passes ? radix_.passes + 3 : 3);
   launch_slots(k_permute, n_, stream_, V);
 }
 
@@ -2240,7 +2317,7 @@ void World::run_init_pass() {
   // FluidSystem.ts:228-231 + loop.ts:237: static boundaries get their volume
   // once, from committed positions, after a grid rebuild.
   if (!any_static_bnd_) return;
-  run_sort_and_permute(parity_, true);
+  run_sort_and_permute(parity_, false);
   parity_ ^= 1;
   launch_slots(k_boundary_volume, n_, stream_, view(parity_), 1u, 0u);
 }
@@ -2278,7 +2355,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   launch_slots(k_predict, n_, stream_, V, s);
   if (any_soft_local_) launch_slots(k_rot_predict, base_.n_grp, stream_, V, s);
   if (any_grid_) {
-    run_sort_and_permute(parity, false);
+    run_sort_and_permute(parity, true);
     V = view(parity ^ 1);
   } else {
     launch_slots(k_reset_sums, n_, stream_, V);
@@ -2721,6 +2798,7 @@ pf_status World::overflow(uint32_t scene, pf_overflow* out) {
   out->positions = f[FLAG_POS] | f[FLAG_SOFT] | f[FLAG_REACT];
   out->velocities = f[FLAG_VEL];
   out->grid = f[FLAG_GRID];
+  out->grid_clamped = f[FLAG_CLAMP];
   out->contacts = f[FLAG_CONTACTS];
   if (h_scenes_[scene].contact) {
     // loop.ts:290-301: the last substep's pair count against maxContacts

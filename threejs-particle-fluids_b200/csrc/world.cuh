@@ -145,7 +145,14 @@ struct DevScene {
   uint32_t has_grid;
   uint32_t cell_base, cells;  // dead cell = cell_base + cells
   float ox, oy, oz, cell;
+  // The grid is a window of dims cells over the reference's unbounded cell
+  // lattice: cell (i, j, k) = floor((x - origin) / cell) lies at local cell
+  // (i, j, k) - lo. lo0 is the window placed at build; each substep the
+  // window moves the least that covers every particle of the scene
+  // (k_grid_fit writes lo), so a window at least as large as the scene's
+  // extent never clamps.
   int32_t lo[3];
+  int32_t lo0[3];
   uint32_t dims[3];
   uint32_t prim_base, prim_count;
   uint32_t planes_fast;  // every primitive is a plane that neither sweeps nor spins (plane4 holds it)
@@ -228,7 +235,8 @@ enum FlagIdx : uint32_t {
   FLAG_SOFT = 5,
   FLAG_REACT = 6,
   FLAG_DEVICE = 7,
-  kNumFlags = 8
+  FLAG_CLAMP = 8,  // a particle lay outside its scene's grid window and was clamped into it
+  kNumFlags = 9
 };
 
 // Per-slot tag: low 16 bits fluid index + 1, high 16 bits boundary index + 1.
@@ -268,6 +276,7 @@ struct WorldView {
   uint32_t n_fchunk, n_cchunk;
   DevScene* scenes_rw;
   uint32_t* flags;              // kNumFlags per scene
+  int32_t* bbox;                // per scene: lowest and highest cell of the predicted positions (6 words)
   float* clocks;                // collider sweep clock per scene (PrimitiveSet.motionClock)
   const DevFluid* fluids;
   const DevBoundary* bnds;
@@ -462,7 +471,9 @@ class World {
  private:
   pf_status alloc_all();
   void run_substep(uint32_t s, uint32_t parity);
-  void run_sort_and_permute(uint32_t parity, bool committed);
+  // bbox_ready: the predict pass of this substep gathered the cell bounds
+  // the grid window follows (otherwise a separate pass gathers them)
+  void run_sort_and_permute(uint32_t parity, bool bbox_ready);
   void run_init_pass();
   void launch_tiles_build(const WorldView& V, uint32_t s);
   template <typename K, typename... A>
@@ -514,6 +525,7 @@ class World {
   WorldView base_{};
   StateBuf buf_[2];
   SortScratch sort_{};
+  RadixPlan radix_{};
   uint32_t parity_ = 0;
   bool inited_ = false;
   // neighbour passes: autotuned once per world, before the first graph capture

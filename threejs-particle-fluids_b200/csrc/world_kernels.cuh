@@ -135,16 +135,59 @@ __device__ __forceinline__ int32_t clampi(int64_t v, int32_t lo, int32_t hi) {
   return (int32_t)(v < lo ? lo : (v > hi ? hi : v));
 }
 
-// Local (grid) cell of a position, clamped into the grid.
+// Cell coordinates outside the reference's Morton range raise its grid
+// overflow flag (cellIndex.ts:145-169, mortonHash.ts:71-79: bias 512).
+constexpr int32_t kMortonBias = 512;
+__device__ __forceinline__ bool morton_over(int32_t c) { return c < -kMortonBias || c >= kMortonBias; }
+
+// Local (grid) cell of a position, clamped into the grid window; `clamped`
+// reports a clamp, `ref_over` a cell the reference's hash flags.
 __device__ __forceinline__ void local_cell(const DevScene& S, f3 p, int32_t* cx, int32_t* cy, int32_t* cz,
-                                           bool* clamped) {
-  const int64_t ax = (int64_t)cell_of(p.x, S.ox, S.cell) - S.lo[0];
-  const int64_t ay = (int64_t)cell_of(p.y, S.oy, S.cell) - S.lo[1];
-  const int64_t az = (int64_t)cell_of(p.z, S.oz, S.cell) - S.lo[2];
+                                           bool* clamped, bool* ref_over = nullptr) {
+  const int32_t rx = cell_of(p.x, S.ox, S.cell), ry = cell_of(p.y, S.oy, S.cell), rz = cell_of(p.z, S.oz, S.cell);
+  const int64_t ax = (int64_t)rx - S.lo[0];
+  const int64_t ay = (int64_t)ry - S.lo[1];
+  const int64_t az = (int64_t)rz - S.lo[2];
   *cx = clampi(ax, 0, (int32_t)S.dims[0] - 1);
   *cy = clampi(ay, 0, (int32_t)S.dims[1] - 1);
   *cz = clampi(az, 0, (int32_t)S.dims[2] - 1);
   if (clamped) *clamped = (*cx != ax) || (*cy != ay) || (*cz != az);
+  if (ref_over) *ref_over = morton_over(rx) || morton_over(ry) || morton_over(rz);
+}
+
+// Adds the cells of this block's positions (`in` lanes) to the scene's
+// bounds (V.bbox[6 s ...]): a block reduction, then six atomics. Every
+// thread of the block must call it; the block belongs to scene s.
+__device__ __forceinline__ void bbox_block_add(const WorldView& V, const DevScene& S, uint32_t s, bool in, f3 p) {
+  __shared__ int32_t sb[kBlock / 32][6];
+  int32_t c[6];
+  if (in) {
+    c[0] = c[3] = cell_of(p.x, S.ox, S.cell);
+    c[1] = c[4] = cell_of(p.y, S.oy, S.cell);
+    c[2] = c[5] = cell_of(p.z, S.oz, S.cell);
+  } else {
+    c[0] = c[1] = c[2] = INT32_MAX;
+    c[3] = c[4] = c[5] = INT32_MIN;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    c[a] = __reduce_min_sync(0xffffffffu, c[a]);
+    c[a + 3] = __reduce_max_sync(0xffffffffu, c[a + 3]);
+  }
+  const uint32_t w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31u) == 0)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) sb[w][a] = c[a];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int a = (int)threadIdx.x;
+    int32_t v = sb[0][a];
+    for (uint32_t q = 1; q < blockDim.x / 32; ++q) v = a < 3 ? min(v, sb[q][a]) : max(v, sb[q][a]);
+    if (a < 3 ? v != INT32_MAX : v != INT32_MIN) {
+      if (a < 3) atomicMin(V.bbox + 6 * s + a, v);
+      else atomicMax(V.bbox + 6 * s + a, v);
+    }
+  }
 }
 
 // Visit the sorted slots of the 27 cells around p in the reference's order

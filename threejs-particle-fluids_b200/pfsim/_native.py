@@ -238,6 +238,7 @@ class Overflow(C.Structure):
         ("contacts", C.c_uint32),
         ("neighbors", C.c_uint32),
         ("device_error", C.c_uint32),
+        ("grid_clamped", C.c_uint32),
     ]
 
 

@@ -21,6 +21,8 @@ fluid defaults (viscosity, surface tension, vorticity, adhesion).
 from __future__ import annotations
 
 import math
+import threading
+import time
 from dataclasses import dataclass, field
 from typing import Sequence
 
@@ -365,6 +367,52 @@ class SimLoop:
             self.disposed = True
 
 
+# -------------------------------------------------------- frame pacing ----
+STEP_TOLERANCE = 1e-6  # a millionth of a step still counts as a whole step (frameStepper.ts:2)
+
+
+class FrameStepper:
+    """src/core/frameStepper.ts:35-88: a fixed-timestep accumulator. Each
+    pump adds the wall-clock time since the previous pump and takes whole
+    steps of `fixed_dt` from it, at most `max_steps_per_frame`; time past
+    that cap is dropped (the simulation runs slower than real time instead
+    of falling behind). The first pump only starts the clock."""
+
+    def __init__(self, fixed_dt: float, max_steps_per_frame: int = 4):
+        if not (isinstance(fixed_dt, (int, float)) and math.isfinite(fixed_dt) and fixed_dt > 0):
+            raise _err("FrameStepper", f"fixedDt must be positive, got {fixed_dt}")
+        if not (isinstance(max_steps_per_frame, int) and max_steps_per_frame > 0):
+            raise _err("FrameStepper", f"maxStepsPerFrame must be a positive integer, got {max_steps_per_frame}")
+        self.fixed_dt = float(fixed_dt)
+        self.max_steps_per_frame = max_steps_per_frame
+        self.accumulator = 0.0
+        self.last_ms: float | None = None
+
+    def pump(self, now_ms: float, step) -> dict:
+        """Runs step(fixed_dt) as many times as the elapsed time allows;
+        returns {steps, truncated, remainder_seconds}."""
+        if self.last_ms is None:
+            self.last_ms = now_ms
+            return {"steps": 0, "truncated": False, "remainder_seconds": 0.0}
+        self.accumulator += max(0.0, (now_ms - self.last_ms) / 1000.0)
+        self.last_ms = now_ms
+        # whole steps counted, not subtracted one by one, so rounding cannot
+        # leave a step's worth of time behind
+        available = self.accumulator / self.fixed_dt
+        truncated = available > self.max_steps_per_frame + STEP_TOLERANCE
+        steps = self.max_steps_per_frame if truncated else min(math.floor(available + STEP_TOLERANCE),
+                                                               self.max_steps_per_frame)
+        self.accumulator = 0.0 if truncated else max(0.0, self.accumulator - steps * self.fixed_dt)
+        for _ in range(steps):
+            step(self.fixed_dt)
+        return {"steps": steps, "truncated": truncated, "remainder_seconds": self.accumulator}
+
+    def reset(self) -> None:
+        """Forget elapsed time (after a pause), so the next pump does not catch up."""
+        self.accumulator = 0.0
+        self.last_ms = None
+
+
 # ------------------------------------------------------------- façade ----
 @dataclass
 class _FluidReq:
@@ -422,6 +470,15 @@ class Simulation:
         self.prims: list[R.Prim] = []
         self.loop: SimLoop | None = None
         self.particles: ParticleSystem | None = None
+        # Simulation.ts:313-318: 60 steps per second of wall clock when
+        # step() gets no dt; a pause of over 250 ms restarts the clock
+        self.stepper = FrameStepper(1.0 / 60.0)
+        self._last_step_ms = -math.inf
+        self._clock = lambda: time.perf_counter() * 1000.0
+        # Simulation.ts:542-546: a step() while another runs (another thread
+        # here) waits for that one and does not step again
+        self._step_lock = threading.Lock()
+        self._stepping: threading.Event | None = None
 
     def _not_started(self, what: str):
         if self.loop is not None:
@@ -564,6 +621,16 @@ class Simulation:
         rec_loop = dict(substeps=int(substeps), iterations=2, gravity=self.gravity)
         if bodies or self.cloths:
             rec_loop["contact"] = {"mu_s": 0.3, "mu_k": 0.2}
+        # the neighbour grid window: the container (open top: twice as
+        # high) plus two smoothing radii, so the fluid never outgrows it
+        grid = {}
+        if self.container is not None:
+            lo, hi = np.asarray(self.container[0], float), np.asarray(self.container[1], float)
+            pad = 2.0 * 2.0 * s
+            top = hi.copy()
+            if not self.closed:
+                top[1] += hi[1] - lo[1]
+            grid = dict(grid_min=tuple(lo - pad), grid_max=tuple(top + pad))
         self.particles = ps
         matobjs = []
         self._cloth_systems = []
@@ -578,11 +645,48 @@ class Simulation:
             matobjs.append(o)
         pset = PrimitiveSet(ps)
         pset.prims = prims
-        self.loop = SimLoop(ps, materials=matobjs, colliders=[pset] if prims else [], **rec_loop)
+        self.loop = SimLoop(ps, materials=matobjs, colliders=[pset] if prims else [], **rec_loop, **grid)
 
-    def step(self, dt: float = 1.0 / 60.0) -> None:
+    def start(self) -> None:
+        """Simulation.start (Simulation.ts:549-560): build now instead of at
+        the first step."""
         if self.loop is None:
             self._build()
+
+    def step(self, dt: float | None = None) -> None:
+        """Simulation.step (Simulation.ts:542-584). With dt, advance by dt;
+        without it, keep pace with the wall clock at 60 fixed steps per
+        second (at most 4 per call; a pause of over 250 ms starts the clock
+        again instead of catching up). A call made while another thread's
+        step runs waits for that step and returns: it covers this frame."""
+        with self._step_lock:
+            running = self._stepping
+            if running is None:
+                self._stepping = threading.Event()
+        if running is not None:
+            running.wait()
+            return
+        try:
+            self.start()
+            if dt is None:
+                now = self._clock()
+                if now - self._last_step_ms > 250.0:
+                    self.stepper.reset()
+                self._last_step_ms = now
+                self.stepper.pump(now, self._advance)
+            else:
+                self._advance(dt)
+        finally:
+            with self._step_lock:
+                self._stepping.set()
+                self._stepping = None
+
+    def _advance(self, dt: float) -> None:
+        """Simulation.advance (Simulation.ts:611-634): the cloths take their
+        current wind, then the loop steps."""
+        for c, system in zip(self.cloths, self._cloth_systems):
+            if system.wind != c.wind:
+                system.wind = c.wind
         self.loop.step(dt)
 
     def readback(self) -> Snapshot:
