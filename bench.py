@@ -239,13 +239,23 @@ class BatchWorkload:
     metric = "particle-substeps/s & p99 step latency: batched/served vs plain, 1\u00d7B200"
     unit = "particle-substeps/s"
     DT = 1.0 / 60.0
-    # algorithmic bytes per fluid particle of the density+lambda stage in
-    # these single-fluid scenes of one mass: read x* (16 B); write the density
-    # (4 B) and the (x*, lambda) record the position pass gathers (16 B)
-    LAMBDA_BYTES = 36
-    # DRAM bytes per fluid particle of one launch, from a full ncu capture of
-    # the pass on the 32-scene cut (158.6 MB over 960,919 fluid particles)
-    LAMBDA_TRAFFIC_PER_PARTICLE = 158.6e6 / 960_919
+    # The fluid neighbour stages, as pf_batch_profile_stage numbers them, with
+    # their compulsory bytes per fluid particle in these single-fluid scenes of
+    # one mass (neighbour gathers served on chip, the list itself excluded):
+    #   0 list build (+ the first iteration's density and lambda): x* in;
+    #     density and the (x*, lambda) record out = 16 + 4 + 16
+    #   1 density + lambda: x* in; density and (x*, lambda) out = 36
+    #   2 position correction with the apply fused: (x*, lambda) in, x* out
+    #     and the collider test's committed position read on contact = 36
+    #   3 XSPH: x and v in, the velocity change out = 48
+    STAGES = {0: ("list build + first density", 36), 1: ("density + lambda", 36),
+              2: ("position correction + apply", 36), 3: ("XSPH", 48)}
+    # DRAM bytes per fluid particle of one launch of a stage, from a one-pass
+    # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of that
+    # stage's pf_batch_profile_stage launch on this workload at the frame the
+    # bench profiles it (after 3 warm-up and 20 timed frames); the command
+    # and the figures are in profiles/batch256_stage_traffic.md
+    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {}
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -296,9 +306,19 @@ class BatchWorkload:
         per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
         ms = evs[0].elapsed_time(evs[-1]) / steps
         launches = int(L.pf_batch_launches_per_step(batch.h))
-        # ---- dominant stage, timed live on the batch stream
-        st_ms, items = C.c_float(0), C.c_uint64(0)
-        N.check(L.pf_batch_profile_stage(batch.h, 1, 20, C.byref(st_ms), C.byref(items)))
+        # ---- the neighbour stages, event-timed on the batch stream on the
+        # state the timed frames left (each launched 10 times after one
+        # untimed launch); launches per step from the substeps and iterations
+        sub = max(r.loop.substeps for r in recipes)
+        its = max(r.loop.iterations for r in recipes)
+        per_step = {0: sub, 1: sub * (its - 1), 2: sub * its, 3: sub}
+        stages, items = {}, C.c_uint64(0)
+        torch.cuda.nvtx.range_push("stage_profile")
+        for sid in self.STAGES:
+            st_ms = C.c_float(0)
+            N.check(L.pf_batch_profile_stage(batch.h, sid, 10, C.byref(st_ms), C.byref(items)))
+            stages[sid] = st_ms.value
+        torch.cuda.nvtx.range_pop()
         tp, tb, tu = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
         N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu)))
         # ---- end to end: per step the scene parameters go host->device (pinned)
@@ -353,17 +373,24 @@ class BatchWorkload:
         for sc in plain:
             sc.close()
         plain = None
+        peak, _ = hbm_peak()
+        table = {}
+        for sid, (label, bpp) in self.STAGES.items():
+            gbs = bpp * items.value / (stages[sid] * 1e-3) / 1e9
+            table[label] = {"ms_per_launch": stages[sid], "launches_per_step": per_step[sid],
+                            "ms_per_step": stages[sid] * per_step[sid],
+                            "share_of_step": stages[sid] * per_step[sid] / ms,
+                            "bytes_per_fluid_particle": bpp, "achieved_gbs": gbs, "frac": gbs / peak}
+        dom = max(self.STAGES, key=lambda sid: stages[sid] * per_step[sid])
+        tpp = self.STAGE_TRAFFIC_PER_PARTICLE.get(dom)
         return {
             "ms": ms,
             "units_per_step": psub,
-            "kernel_ms": st_ms.value,
-            "kernel_name": ("k_t_lambda" if tp.value == 1 else f"k_s_lambda<{tu.value}>")
-            + " (density + lambda, one solver iteration)",
-            "algorithmic_bytes": self.LAMBDA_BYTES * items.value,
-            # DRAM bytes of one launch: the per-fluid-particle figure of a full
-            # ncu capture of this pass on the 32-scene cut of the workload
-            # scaled to this launch
-            "traffic": self.LAMBDA_TRAFFIC_PER_PARTICLE * items.value if tp.value == 0 else None,
+            "kernel_ms": stages[dom],
+            "kernel_name": self.STAGES[dom][0] + (" (warp-tile path)" if tp.value == 1 else " (slot path)"),
+            "algorithmic_bytes": self.STAGES[dom][1] * items.value,
+            "traffic": tpp * items.value if (tpp is not None and tp.value == 0) else None,
+            "stages": table,
             "gpu_launches_per_step": launches,
             "clocks": clk,
             "e2e_ms": e2e_ms,
@@ -466,7 +493,7 @@ class ServeWorkload:
             srv.submit(rec, life)
         srv.tick(self.DT)  # admits the initial population (its cohort build starts)
         srv.drain()  # and waits for that build, so the run starts from a live population
-        tick_ms, ps0 = [], 0
+        tick_ms, step_ms, ps0 = [], [], 0
         clocks = ClockSampler(torch.cuda.current_device())
         for t in range(warmup + ticks):
             if t == warmup:
@@ -478,15 +505,21 @@ class ServeWorkload:
             t0 = time.perf_counter()
             srv.tick(self.DT)
             if t >= warmup:
-                tick_ms.append((time.perf_counter() - t0) * 1e3)
+                ms = (time.perf_counter() - t0) * 1e3
+                tick_ms.append(ms)
+                # the tick without its admission: the plain server builds each
+                # admitted request's world inside the tick, the batched one
+                # only starts a cohort build there (it runs on a worker thread)
+                step_ms.append(max(ms - srv.stats()["last_admit_ms"], 0.0))
         clk = clocks.stop()
         st = srv.stats()
         srv.close()
         ps = st["particle_substeps"] - ps0
-        wall = sum(tick_ms)
+        wall, stepping = sum(tick_ms), sum(step_ms)
         return {"value": ps / (wall * 1e-3), "ms": wall / ticks, "p50": float(np.percentile(tick_ms, 50)),
                 "p99": float(np.percentile(tick_ms, 99)), "clocks": clk, "stats": st,
-                "ps_per_tick": ps / ticks}
+                "ps_per_tick": ps / ticks, "step_value": ps / (stepping * 1e-3),
+                "step_p50": float(np.percentile(step_ms, 50)), "step_p99": float(np.percentile(step_ms, 99))}
 
     def run_cpu(self, threads: int, budget_particles: int = 150_000, steps: int = 2) -> dict:
         """The oracle on the first requests of the same stream, up to
@@ -519,10 +552,14 @@ class ServeWorkload:
             "ms": b["ms"], "units_per_step": b["ps_per_tick"], "clocks": b["clocks"],
             "extra": {
                 "p50_tick_ms": b["p50"], "p99_tick_ms": b["p99"],
-                "plain_value": p["value"] if p else None,
-                "plain_p50_tick_ms": p["p50"] if p else None,
-                "plain_p99_tick_ms": p["p99"] if p else None,
-                "served_over_plain": (b["value"] / p["value"]) if p else None,
+                # the plain arm without its world builds (a fair per-tick
+                # stepping cost), and with them
+                "plain_value": p["step_value"] if p else None,
+                "plain_p50_tick_ms": p["step_p50"] if p else None,
+                "plain_p99_tick_ms": p["step_p99"] if p else None,
+                "served_over_plain": (b["value"] / p["step_value"]) if p else None,
+                "plain_with_builds_value": p["value"] if p else None,
+                "plain_with_builds_p99_tick_ms": p["p99"] if p else None,
                 "requests": len(stream), "cohort_builds": b["stats"]["rebuilds"],
                 "max_swap_ms": b["stats"]["max_swap_ms"], "max_admit_ms": b["stats"]["max_admit_ms"],
                 "plain_max_admit_ms": p["stats"]["max_admit_ms"] if p else None,
@@ -706,6 +743,8 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-scene baseline (profiling runs)")
     ap.add_argument("--scenes", type=int, default=256, help="scenes of the batch workload (smaller for profiling)")
     ap.add_argument("--live", type=int, default=96, help="steady-state live scenes of the serve workload")
+    ap.add_argument("--no-serve", action="store_true", help="batch workload without its served arm")
+    ap.add_argument("--serve-ticks", type=int, default=40, help="timed ticks of the batch workload's served arm")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -823,7 +862,25 @@ def main() -> None:
         "clocks": res["clocks"],
     }
     line["dtype"] = "u32" if args.workload == "sort" else "f32"
+    if "stages" in res:
+        line["roofline"]["stages"] = res["stages"]
     line.update(res.get("extra", {}))
+    if args.workload == "batch" and not args.no_serve and world == 1:
+        # the served half of the metric: the Poisson request stream, batched
+        # (cohorts, graphs) against the plain per-scene loop, on this GPU
+        sv = WORKLOADS["serve"](args.live)
+        sres = sv.run_gpu(args.serve_ticks, 5, rank, world, barrier, plain_baseline=not args.no_plain)
+        ex = sres["extra"]
+        line["served"] = {
+            "workload": sv.name, "ticks": args.serve_ticks, "value": sres["units_per_step"] / (sres["ms"] * 1e-3),
+            "unit": wl.unit, "p50_tick_ms": ex["p50_tick_ms"], "p99_tick_ms": ex["p99_tick_ms"],
+            "plain_value": ex["plain_value"], "plain_p50_tick_ms": ex["plain_p50_tick_ms"],
+            "plain_p99_tick_ms": ex["plain_p99_tick_ms"], "served_over_plain": ex["served_over_plain"],
+            "plain_with_builds_value": ex["plain_with_builds_value"],
+            "plain_with_builds_p99_tick_ms": ex["plain_with_builds_p99_tick_ms"],
+            "timing": "host wall clock per tick; the plain arm's ticks without its world builds",
+            "clocks": sres["clocks"],
+        }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = wl.run_cpu(os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": cpu["units_per_step"] / cpu["seconds_per_step"], "unit": wl.unit,

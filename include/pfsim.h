@@ -104,19 +104,24 @@ PF_API pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* gr
 /* pf_sort that allocates no device memory (no counterpart in the reference;
  * added for callers that cannot allocate, such as hosts whose own pool owns
  * the device memory or loops where an allocation would stall the frame).
- * Same arguments and results as pf_sort. Its scratch is one fixed block
- * compiled into the library (about 21 MB held on every GPU that loads it), so
- * n <= 1,048,576 particles and at most 2,097,152 cells per call; larger sizes
- * return PF_ERR_INVALID. The first call on a device looks up that block's
- * device address, so make it before any stream capture. Calls share the
- * block: calls whose GPU work overlaps race, so serialise them. */
+ * Same arguments and results as pf_sort. Its scratch is one fixed 27 MiB
+ * block compiled into the library, so n <= 1,048,576 particles and at most
+ * 2,097,152 cells per call; larger sizes return PF_ERR_INVALID. The runtime
+ * loads that block lazily: the first call on a device reserves it there
+ * (until the process exits) and looks up its address, so make that call
+ * before the host's pool claims the device's memory and before any stream
+ * capture. A call with n = 0 and NULL start and count does only this
+ * set-up. Calls share the block: calls whose GPU work overlaps race, so
+ * serialise them. pf_sort_device_errors on the same stream reads the
+ * block's device error word. */
 PF_API pf_status pf_sort_noalloc(const float* d_pos4, uint32_t n, const pf_grid_desc* grid,
                                  uint32_t* d_perm, uint32_t* d_start, uint32_t* d_count,
                                  uint32_t* d_keys, uint32_t* d_overflow, void* stream);
 
 /* Synchronises `stream` and returns, then clears, the device error word of
- * the most recent pf_sort on that stream (0 = no error; bit 0 = a bounded
- * look-back wait expired, bit 1 = a fix-up list overflowed). */
+ * the most recent pf_sort or pf_sort_noalloc on that stream (0 = no error;
+ * bit 0 = a bounded look-back wait expired and the outputs are not to be
+ * trusted). */
 PF_API pf_status pf_sort_device_errors(void* stream, uint32_t* bits);
 
 /* pf_sort with host buffers: copies the positions in, sorts, copies the
@@ -586,6 +591,8 @@ typedef struct pf_server_stats {
   float max_tick_ms;
   float max_swap_ms;          /* longest swap-in of a built cohort (imports, frees) */
   float max_admit_ms;         /* longest admission (synchronous builds included) */
+  float last_admit_ms;        /* admission inside the last tick (PLAIN: its world builds);
+                                 last_tick_ms minus this is that tick's stepping */
 } pf_server_stats;
 
 /* Request states reported by pf_server_request_state. */

@@ -94,6 +94,7 @@ struct pf_server {
   double busy_ms = 0;
   std::vector<float> tick_ms;
   float max_swap_ms = 0, max_admit_ms = 0;
+  float last_admit_ms = 0;  // admission (and synchronous builds) inside the last tick
   bool blocked = false;  // the last build ran out of memory: wait for a cohort to free
   std::string last_error;
   bool have_tuning = false;  // the first cohort's autotuned neighbour path, reused by later cohorts
@@ -372,11 +373,13 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     PF_TRY(swap_in(S));
     S->max_swap_ms = std::max(S->max_swap_ms, (float)ms_since(t0));
   }
+  S->last_admit_ms = 0;
   if (!S->opts.async_build || S->opts.mode == PF_SERVER_PLAIN) {
     const auto ta = Clock::now();
     PF_TRY(admit(S));
     if (S->build) PF_TRY(swap_in(S));
-    S->max_admit_ms = std::max(S->max_admit_ms, (float)ms_since(ta));
+    S->last_admit_ms = (float)ms_since(ta);
+    S->max_admit_ms = std::max(S->max_admit_ms, S->last_admit_ms);
   }
   bool stepped = false;
   const bool plain = S->opts.mode == PF_SERVER_PLAIN;
@@ -434,7 +437,9 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   if (S->opts.async_build && S->opts.mode != PF_SERVER_PLAIN) {
     const auto ta = Clock::now();
     PF_TRY(admit(S));
-    S->max_admit_ms = std::max(S->max_admit_ms, (float)ms_since(ta));
+    const float ms = (float)ms_since(ta);
+    S->last_admit_ms += ms;
+    S->max_admit_ms = std::max(S->max_admit_ms, ms);
   }
   S->ticks++;
   if (stepped) {  // latency statistics cover ticks that stepped at least one scene
@@ -486,6 +491,7 @@ pf_status pf_server_stats_read(pf_server* S, pf_server_stats* o) {
   }
   o->max_swap_ms = S->max_swap_ms;
   o->max_admit_ms = S->max_admit_ms;
+  o->last_admit_ms = S->last_admit_ms;
   return PF_OK;
 }
 

@@ -43,12 +43,11 @@ int sm_count();
 // wait or find an inconsistent input; read back by the host after a call.
 enum DeviceError : uint32_t {
   DEV_ERR_LOOKBACK_TIMEOUT = 1u << 0,
-  DEV_ERR_SORT_CAPACITY = 1u << 1,
 };
 
 // Upper bound on spins of a decoupled look-back before it reports
 // DEV_ERR_LOOKBACK_TIMEOUT and returns (forward progress is guaranteed by
-// dynamic tile ids, so this only triggers on a bug).
+// tile ids taken in launch order, so this only triggers on a bug).
 constexpr uint32_t kLookbackSpinLimit = 1u << 24;
 
 __host__ __device__ inline uint32_t div_up(uint32_t a, uint32_t b) { return (a + b - 1) / b; }

@@ -1715,6 +1715,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.cstart = cv.take<uint32_t>(cells_);
     base_.ccount = cv.take<uint32_t>(cells_);
     base_.nbr = any_fluid_ ? cv.take<uint32_t>(N * kMaxNbr) : nullptr;
+    base_.nbr_base = any_fluid_ ? cv.take<uint32_t>(N / 32) : nullptr;
     base_.nbr16 = reinterpret_cast<uint16_t*>(base_.nbr);
     base_.ncount = cv.take<uint32_t>(N);
     base_.slot_tile = cv.take<uint32_t>(N);
@@ -2701,14 +2702,19 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
       if (!base_.nbr16) return PF_OK;
       if (tune_.path == 0) {
         // segments start on a warp boundary, so their list blocks are one range
-        std::vector<uint32_t> all((size_t)seg * kMaxNbr), seg_ids(seg);
+        std::vector<uint32_t> all((size_t)seg * kMaxNbr), seg_ids(seg), wbase(seg / 32);
         PF_CUDA(cudaMemcpy(seg_ids.data(), base_.ids + S.seg_start, 4ull * seg, cudaMemcpyDeviceToHost));
         PF_CUDA(cudaMemcpy(all.data(), base_.nbr + nbr_col(S.seg_start), 4ull * seg * kMaxNbr, cudaMemcpyDeviceToHost));
+        PF_CUDA(cudaMemcpy(wbase.data(), base_.nbr_base + S.seg_start / 32, 4ull * (seg / 32), cudaMemcpyDeviceToHost));
+        const uint16_t* all16 = reinterpret_cast<const uint16_t*>(all.data());
         for (uint32_t m = 0; m < kMaxNbr; ++m) {
           for (uint32_t k = 0; k < seg; ++k) {
             const uint32_t id = ids[k] - S.seg_start;
             if (id >= cap || !tag_fluid(tag[k]) || m >= cnt[k]) continue;
-            const uint32_t j = all[nbr_col(k) + (size_t)m * kNbrStride];  // a slot of the same scene's segment
+            const uint32_t wb = wbase[k / 32];
+            // a slot of the same scene's segment
+            const uint32_t j = (wb & kNbrWide) ? all[nbr_col(k) + (size_t)m * kNbrStride]
+                                               : wb + all16[nbr16_col(k) + (size_t)m * kNbrStride];
             o[(size_t)id * kMaxNbr + m] = (j >= S.seg_start && j < S.seg_end) ? seg_ids[j - S.seg_start] - S.seg_start
                                                                                : 0xfffffffeu;
           }
@@ -2886,9 +2892,9 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
         if (tune_.path == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
         else PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
         break;
-      case 2:
+      case 2:  // with the apply the step fuses in (it rewrites x*, which the next predict replaces)
         if (tune_.path == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
-        else PF_DELTA(V, rank, 0u, 0u, 0u);
+        else PF_DELTA(V, rank, 0u, 0u, 1u);
         break;
       case 3:
         if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);

@@ -32,13 +32,21 @@ namespace pf {
 
 constexpr uint32_t kSegAlign = 256;
 constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts:14)
-// The slot path's neighbour list is blocked by warp: slot k's m-th entry is
-// word nbr_col(k) + m * kNbrStride, so a warp's m-th entries are one 128-byte
-// line and its successive entries successive lines of one 8 KB block.
+// The slot path's neighbour list is blocked by warp: each warp of slots owns
+// an 8 KB block. Entries are 16-bit offsets from a per-warp base slot
+// (nbr_base[k / 32]) when every slot the warp's 27-cell rows reach lies
+// within 65,536 slots of the lowest, which is the common case; then slot k's
+// m-th entry is halfword nbr16_col(k) + m * kNbrStride of the block, a
+// warp's m-th entries one 64-byte half line. Otherwise the warp's base is
+// kNbrWide and its entries are whole slots, word nbr_col(k) + m * kNbrStride.
 constexpr uint32_t kNbrStride = 32;
+constexpr uint32_t kNbrWide = 0x80000000u;
 static_assert(kSegAlign % kNbrStride == 0, "a scene's segment starts on a list block");
 __host__ __device__ __forceinline__ size_t nbr_col(size_t k) {
   return (k >> 5) * (size_t)kMaxNbr * kNbrStride + (k & 31);
+}
+__host__ __device__ __forceinline__ size_t nbr16_col(size_t k) {
+  return (k >> 5) * (size_t)kMaxNbr * kNbrStride * 2 + (k & 31);
 }
 constexpr uint32_t kBlock = 256;
 constexpr uint32_t kMaxContacts = 32;  // contact pairs kept per emitting particle per substep
@@ -291,7 +299,8 @@ struct WorldView {
   uint32_t* perm;     // new slot -> id (sort output)
   uint32_t* cstart;
   uint32_t* ccount;
-  uint32_t* nbr;      // kMaxNbr * n, blocked by warp (nbr_col): slot of each neighbour (slot path)
+  uint32_t* nbr;      // kMaxNbr * n, blocked by warp: 16- or 32-bit entries (slot path)
+  uint32_t* nbr_base; // per warp of slots: base slot of its 16-bit entries, or kNbrWide
   uint16_t* nbr16;    // the same storage, kMaxNbr * n halfwords: halo index of each neighbour (tile path)
   uint32_t* ncount;
   uint32_t* slot_tile;  // tile of each slot (this substep)

@@ -3,9 +3,10 @@
 // Each thread owns one particle (slot k, cell order) and gathers its
 // neighbours' state straight from the slot arrays; particles are in cell
 // order, so a warp's gathers fall on a few hundred consecutive slots that L1
-// holds. The neighbour list stores slots (32 bits) blocked by warp (nbr_col),
-// so a warp reads its m-th entries as one coalesced line and its next
-// entries from the next line. The loops fetch the list and
+// holds. The neighbour list is blocked by warp: 16-bit offsets from a
+// per-warp base slot (32-bit slots where a warp's rows reach further), so a
+// warp reads its m-th entries as one coalesced half line (or line) and its
+// next entries from the next one. The loops fetch the list and
 // the neighbours several at a time before using them: independent loads in
 // flight per round instead of a dependent load per neighbour, with the sums
 // still formed in list order.
@@ -21,38 +22,57 @@
 namespace pf {
 
 // A list entry (read-only for the kernel). A miss fetches 256 bytes into L2:
-// with the warp-blocked layout that is the warp's next line of entries too.
+// with the warp-blocked layout that is the warp's next lines of entries too.
 __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
   uint32_t v;
   asm("ld.global.nc.L2::256B.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
+__device__ __forceinline__ uint32_t ld_entry(const uint16_t* p) {
+  unsigned short v;
+  asm("ld.global.nc.L2::256B.u16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+}
+
+// The list of slot k: its warp's base (kNbrWide: 32-bit entries) and the
+// first entry of either width.
+struct NbrList {
+  uint32_t base;
+  const uint32_t* w32;
+  const uint16_t* w16;
+  __device__ __forceinline__ bool wide() const { return (base & kNbrWide) != 0; }
+};
+__device__ __forceinline__ NbrList nbr_list(const WorldView& V, uint32_t k) {
+  NbrList L;
+  L.base = V.nbr_base[k >> 5];
+  L.w32 = V.nbr + nbr_col(k);
+  L.w16 = reinterpret_cast<const uint16_t*>(V.nbr) + nbr16_col(k);
+  return L;
+}
 
 // Before a walk: one lane of the warp has its list block's first max(cnt)
-// lines (128 bytes each, contiguous) fetched into L2 in one bulk prefetch,
-// so the later rounds' entries come from L2 instead of DRAM.
-__device__ __forceinline__ void prefetch_list(const WorldView& V, uint32_t k, uint32_t cnt) {
+// entry lines (contiguous) fetched into L2 in one bulk prefetch, so the
+// later rounds' entries come from L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_list(const NbrList& L, uint32_t cnt) {
   const uint32_t act = __activemask();
   const uint32_t most = __reduce_max_sync(act, cnt);
   if (most && (threadIdx.x & 31u) == (uint32_t)(__ffs(act) - 1)) {
-    const uint32_t* base = V.nbr + nbr_col(k & ~31u);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base), "r"(most * kNbrStride * 4u) : "memory");
+    const uint32_t lane = threadIdx.x & 31u;
+    const void* base = L.wide() ? (const void*)(L.w32 - lane) : (const void*)(L.w16 - lane);
+    const uint32_t bytes = most * kNbrStride * (L.wide() ? 4u : 2u);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base), "r"(bytes) : "memory");
   }
 }
 
-// Walks list entries [0, cnt) of one slot (its column starts at nl, entries
-// `stride` words apart), kU per round, in list order: a round gathers its neighbours'
-// records (fetch), then fetches the next round's list entries, then uses the
-// records (use). The list entries come from DRAM and the records mostly from
-// L1, so the next round's entries are in flight while this round's records
-// arrive and are used. The last partial round is one batch as well.
-// kFresh: the list was written by this same thread in this kernel, so its
-// entries are read with plain (coherent) loads.
-template <uint32_t kU, bool kFresh = false, typename Fetch, typename Use>
-__device__ __forceinline__ void walk_list(const uint32_t* __restrict__ nl, uint32_t stride, uint32_t cnt, Fetch fetch,
-                                          Use use) {
+// Walks list entries [0, cnt) (entry(m) gives the m-th neighbour's slot), kU
+// per round, in list order: a round gathers its neighbours' records (fetch),
+// then fetches the next round's list entries, then uses the records (use).
+// The list entries come from DRAM and the records mostly from L1, so the
+// next round's entries are in flight while this round's records arrive and
+// are used. The last partial round is one batch as well.
+template <uint32_t kU, typename Entry, typename Fetch, typename Use>
+__device__ __forceinline__ void walk_list(Entry entry, uint32_t cnt, Fetch fetch, Use use) {
   using Rec = decltype(fetch(0u));
-  auto entry = [&](uint32_t m) { return kFresh ? nl[m * stride] : ld_entry(nl + m * stride); };
   uint32_t jn[kU];
 #pragma unroll
   for (uint32_t q = 0; q < kU; ++q) jn[q] = q < cnt ? entry(q) : 0u;
@@ -79,6 +99,24 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ nl, uint3
 #pragma unroll
     for (uint32_t q = 0; q < kU; ++q)
       if (m + q < cnt) use(jn[q], r[q]);
+  }
+}
+
+// walk_list over slot k's list in whichever width its warp stored (a
+// warp-uniform branch). kFresh: the list was written by this same thread in
+// this kernel, so its entries are read with plain (coherent) loads.
+template <uint32_t kU, bool kFresh = false, typename Fetch, typename Use>
+__device__ __forceinline__ void walk_nbrs(const NbrList& L, uint32_t cnt, Fetch fetch, Use use) {
+  if (L.wide()) {
+    const uint32_t* p = L.w32;
+    walk_list<kU>([&](uint32_t m) { return kFresh ? p[m * kNbrStride] : ld_entry(p + m * kNbrStride); }, cnt, fetch,
+                  use);
+  } else {
+    const uint16_t* p = L.w16;
+    const uint32_t b = L.base;
+    walk_list<kU>(
+        [&](uint32_t m) { return b + (kFresh ? (uint32_t)p[m * kNbrStride] : ld_entry(p + m * kNbrStride)); }, cnt,
+        fetch, use);
   }
 }
 
@@ -159,13 +197,14 @@ __device__ __forceinline__ void lambda_terms(const DevFluid& F, f3 xi, float4 xj
 template <uint32_t kNbrUnroll, bool kDens>
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= V.n_fchunk * kSegAlign) return;
+  if (g >= V.n_fchunk * kSegAlign) return;     // whole warps
   const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
-  const uint32_t f = tag_fluid(V.cur.tag[k]);
-  if (!f) return;
   const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
-  const DevFluid& F = V.fluids[f - 1];
+  if (sub >= S.substeps) return;               // whole chunks
+  const uint32_t f = tag_fluid(V.cur.tag[k]);
+  // every lane of the warp takes part in choosing the list width; lanes of
+  // other materials (f == 0) leave after that
+  const DevFluid& F = V.fluids[f ? f - 1 : 0];
   const float4 xi4 = V.cur.xs[k];
   const f3 xi = xyz(xi4);
   const bool dens = kDens && F.rank == 0 && S.iterations > 0;
@@ -212,16 +251,39 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
     rs[r] = __ldg(V.cstart + row + a0);
     re[r] = __ldg(V.cstart + row + a1) + __ldg(V.ccount + row + a1);
   }
+  // The warp's entries are 16-bit offsets from the lowest slot its rows
+  // reach when every reachable slot lies within 65,536 of it.
+  uint32_t lo = 0xffffffffu, hi = 0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    if (!f) rs[r] = re[r] = 0;
+    if (re[r] > rs[r]) {
+      lo = min(lo, rs[r]);
+      hi = max(hi, re[r]);
+    }
+  }
+  lo = __reduce_min_sync(0xffffffffu, lo);
+  hi = __reduce_max_sync(0xffffffffu, hi);
+  const bool narrow = hi <= lo || hi - lo <= 65536u;
+  const uint32_t base = narrow ? (hi > lo ? lo : 0u) : kNbrWide;
+  if ((threadIdx.x & 31u) == 0) V.nbr_base[k >> 5] = base;
+  if (!f) return;
   // Every candidate is tested; the first kMaxNbr hits in walk order are
   // stored (as the reference's list keeps them) and any further hit only
   // marks the overflow.
   uint32_t cnt = 0;
   uint32_t* __restrict__ out = V.nbr + nbr_col(k);
+  uint16_t* __restrict__ out16 = reinterpret_cast<uint16_t*>(V.nbr) + nbr16_col(k);
   auto test = [&](uint32_t j, float4 xj) {
     if (dot_rn(xi - xyz(xj)) < hsq) {
       if (cnt < kMaxNbr) {
-        *out = j;
-        out += kNbrStride;
+        if (narrow) {
+          *out16 = (uint16_t)(j - base);
+          out16 += kNbrStride;
+        } else {
+          *out = j;
+          out += kNbrStride;
+        }
       }
       ++cnt;
     }
@@ -256,12 +318,14 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   if (kDens && dens) {
     // the density pass over the list just written (still in cache), in list
     // order, outside the divergent walk
-    const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+    NbrList L;
+    L.base = base;
+    L.w32 = V.nbr + nbr_col(k);
+    L.w16 = reinterpret_cast<const uint16_t*>(V.nbr) + nbr16_col(k);
     const float qh = -S.homog_mass;
     const bool homog = S.homog;
-    walk_list<kNbrUnroll, true>(
-        nl, kNbrStride, cnt,
-        [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), homog ? qh : __ldg(q_of + 2 * (size_t)j)}; },
+    walk_nbrs<kNbrUnroll, true>(
+        L, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), homog ? qh : __ldg(q_of + 2 * (size_t)j)}; },
         [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
     finish_lambda(V, S, F, k, xi4, rho, gs, gss);
   }
@@ -284,18 +348,18 @@ __global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it
   float rho = 0.0f, gss = 0.0f;
   f3 gs = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
-  prefetch_list(V, k, cnt);
+  const NbrList nl = nbr_list(V, k);
+  prefetch_list(nl, cnt);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y
   if (S.homog) {
     // one fluid, one mass: no mass gather
     const float qh = -S.homog_mass;
-    walk_list<kNbrUnroll>(
-        nl, kNbrStride, cnt, [&](uint32_t j) { return __ldg(V.cur.xs + j); },
+    walk_nbrs<kNbrUnroll>(
+        nl, cnt, [&](uint32_t j) { return __ldg(V.cur.xs + j); },
         [&](uint32_t, const float4& xj) { lambda_terms(F, xi, xj, qh, rho, gs, gss); });
   } else {
-    walk_list<kNbrUnroll>(
-        nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j)}; },
+    walk_nbrs<kNbrUnroll>(
+        nl, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(q_of + 2 * (size_t)j)}; },
         [&](uint32_t, const NbrXQ& r) { lambda_terms(F, xi, r.x, r.q, rho, gs, gss); });
   }
   finish_lambda(V, S, F, k, xi4, rho, gs, gss);
@@ -329,8 +393,8 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
   const bool multi = S.fluid_count > 1;
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
-  prefetch_list(V, k, cnt);
+  const NbrList nl = nbr_list(V, k);
+  prefetch_list(nl, cnt);
   auto one = [&](uint32_t j, float4 xj, float2 lq) {
     const float bvj = lq.y;
     const float lj = (multi && tag_fluid(__ldg(V.cur.tag + j)) != f) ? 0.0f : lq.x;
@@ -360,12 +424,12 @@ __global__ void __maxnreg__(kNbrUnroll == 8 ? 96 : 56) k_s_delta(WorldView V, ui
   if (S.homog) {
     // one fluid, one mass: (x*, lambda) of a neighbour in one gather
     const float qh = -S.homog_mass;
-    walk_list<kNbrUnroll>(
-        nl, kNbrStride, cnt, [&](uint32_t j) { return __ldg(V.xl + j); },
+    walk_nbrs<kNbrUnroll>(
+        nl, cnt, [&](uint32_t j) { return __ldg(V.xl + j); },
         [&](uint32_t j, const float4& xj) { one(j, xj, make_float2(xj.w, qh)); });
   } else {
-    walk_list<kNbrUnroll>(
-        nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXL{__ldg(V.cur.xs + j), __ldg(V.lm + j)}; },
+    walk_nbrs<kNbrUnroll>(
+        nl, cnt, [&](uint32_t j) { return NbrXL{__ldg(V.cur.xs + j), __ldg(V.lm + j)}; },
         [&](uint32_t j, const NbrXL& r) { one(j, r.x, r.lq); });
   }
 #ifndef PF_EXACT_ROUNDING
@@ -403,8 +467,8 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
   const f3 vi = xyz(V.cur.v[k]);
   f3 sm = mk(0.0f, 0.0f, 0.0f), curl = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
-  prefetch_list(V, k, cnt);
+  const NbrList nl = nbr_list(V, k);
+  prefetch_list(nl, cnt);
   const float* __restrict__ q_of = reinterpret_cast<const float*>(V.lm) + 1;  // lm[j].y: volume if > 0
   // without boundaries in the world every neighbour has the fluid volume
   auto one = [&](float4 xj, float4 vj, float bvj) {
@@ -421,8 +485,8 @@ __global__ void k_s_xsph(WorldView V, uint32_t rank, uint32_t sub) {
     }
 #endif
   };
-  walk_list<kNbrUnroll>(
-      nl, kNbrStride, cnt,
+  walk_nbrs<kNbrUnroll>(
+      nl, cnt,
       [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), __ldg(V.cur.v + j), kBnd ? __ldg(q_of + 2 * (size_t)j) : 0.0f}; },
       [&](uint32_t, const NbrXV& r) { one(r.x, r.v, r.q); });
 #ifndef PF_EXACT_ROUNDING
@@ -449,10 +513,10 @@ __global__ void k_s_vort_grad(WorldView V, uint32_t rank, uint32_t sub) {
   const float wi = V.vort[k].w;
   f3 eta = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
-  prefetch_list(V, k, cnt);
-  walk_list<kNbrUnroll>(
-      nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
+  const NbrList nl = nbr_list(V, k);
+  prefetch_list(nl, cnt);
+  walk_nbrs<kNbrUnroll>(
+      nl, cnt, [&](uint32_t j) { return NbrXV{__ldg(V.cur.x + j), V.vort[j], __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXV& r) {
         if (r.q > 0.0f) return;
         const f3 off = xi - xyz(r.x);
@@ -477,10 +541,10 @@ __global__ void k_s_color_normal(WorldView V, uint32_t rank, uint32_t sub) {
   const f3 xi = xyz(V.cur.xs[k]);
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
-  prefetch_list(V, k, cnt);
-  walk_list<kNbrUnroll>(
-      nl, kNbrStride, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
+  const NbrList nl = nbr_list(V, k);
+  prefetch_list(nl, cnt);
+  walk_nbrs<kNbrUnroll>(
+      nl, cnt, [&](uint32_t j) { return NbrXQ{__ldg(V.cur.xs + j), __ldg(V.cur.bv + j)}; },
       [&](uint32_t, const NbrXQ& r) {
         const f3 off = xi - xyz(r.x);
         sum = sum + spiky_vec(off, dot(off, off), F) * (r.q > 0.0f ? r.q : F.volume);
@@ -523,9 +587,9 @@ __global__ void k_s_impulses(WorldView V, uint32_t rank, uint32_t sub) {
   const float rhoi = V.cur.dens[k];
   const float dt = S.dt;
   const uint32_t cnt = V.ncount[k];
-  const uint32_t* __restrict__ nl = V.nbr + nbr_col(k);
+  const NbrList nl = nbr_list(V, k);
   for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = __ldg(nl + m * kNbrStride);
+    const uint32_t j = nl.wide() ? __ldg(nl.w32 + m * kNbrStride) : nl.base + __ldg(nl.w16 + m * kNbrStride);
     const f3 off = xi - xyz(__ldg(V.cur.xs + j));
     if (F.has_st) {
       const uint32_t idj = V.ids[j];

@@ -280,6 +280,7 @@ class ServerStats(C.Structure):
         ("max_tick_ms", C.c_float),
         ("max_swap_ms", C.c_float),
         ("max_admit_ms", C.c_float),
+        ("last_admit_ms", C.c_float),
     ]
 
 
