@@ -319,8 +319,8 @@ class BatchWorkload:
             N.check(L.pf_batch_profile_stage(batch.h, sid, 10, C.byref(st_ms), C.byref(items)))
             stages[sid] = st_ms.value
         torch.cuda.nvtx.range_pop()
-        tp, tb, tu = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
-        N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu)))
+        tp, tb, tu, tg = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+        N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu), C.byref(tg)))
         # ---- end to end: per step the scene parameters go host->device (pinned)
         # and every scene's positions come back to pinned host memory
         total = sum(r.capacity for r in recipes)
@@ -406,7 +406,7 @@ class BatchWorkload:
                 "plain_overlapped_ms_per_step": overlap_ms,
                 "batched_over_plain_overlapped": overlap_ms / ms,
                 "tuning": {"nbr_path": "tiles" if tp.value == 1 else "slots", "block": tb.value,
-                           "fetch_depth": tu.value},
+                           "fetch_depth": tu.value, "l2_group_particles": tg.value},
                 "scenes": len(recipes),
                 "particles": total,
                 "fluid_particles": int(items.value),

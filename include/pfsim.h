@@ -499,8 +499,12 @@ PF_API pf_status pf_batch_profile_stage(pf_batch* batch, uint32_t stage, uint32_
                                         uint64_t* items);
 /* The fluid neighbour-pass configuration the autotuner chose on the batch's
  * first step: path 0 = one thread per slot (block threads per block, list
- * entries fetched `unroll` at a time), 1 = warp tiles. */
-PF_API pf_status pf_batch_tuning(pf_batch* batch, uint32_t* path, uint32_t* block, uint32_t* unroll);
+ * entries fetched `unroll` at a time), 1 = warp tiles. `group` (may be NULL)
+ * receives the fluid particles per group of the scenes that hold only one
+ * fluid of one mass, stepped group by group so that a group's lists stay in
+ * L2 across its passes (0: one launch per pass over all of them). */
+PF_API pf_status pf_batch_tuning(pf_batch* batch, uint32_t* path, uint32_t* block, uint32_t* unroll,
+                                 uint32_t* group);
 
 /* ------------------------------------------------------------------------ */
 /* Mesh -> particle setup on the GPU                                          */

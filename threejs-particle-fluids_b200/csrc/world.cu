@@ -109,17 +109,29 @@ __global__ void k_grid_fit(WorldView V, uint32_t nscenes) {
   S.prune_slack = big * (1.0f / 65536.0f) + 1e-9f;
 }
 
-// integrate.ts:36-44
-__global__ void __launch_bounds__(kBlock) k_advect(WorldView V, uint32_t sub) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= V.n) return;
-  const DevScene& S = scene_at(V, k);
-  if (sub >= S.substeps) return;
+// integrate.ts:36-44 (scenes stepped by groups advect there)
+__device__ __forceinline__ void advect_slot(const WorldView& V, const DevScene& S, uint32_t k) {
   const float4 x = V.cur.x[k];
   if (!(x.w > 0.0f)) return;
   const float4 xs = V.cur.xs[k];
   V.cur.v[k] = with_w((xyz(xs) - xyz(x)) / S.dt, 0.0f);
   V.cur.x[k] = xs;
+}
+__global__ void __launch_bounds__(kBlock) k_advect(WorldView V, uint32_t sub) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= V.n) return;
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps || S.grouped) return;
+  advect_slot(V, S, k);
+}
+// The advect of one group of run_groups, over its chunks.
+__global__ void __launch_bounds__(kBlock) k_advect_chunks(WorldView V, uint32_t sub) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= V.n_fchunk * kSegAlign) return;
+  const uint32_t k = chunk_slot(V.fchunk, g);
+  const DevScene& S = scene_at(V, k);
+  if (sub >= S.substeps) return;
+  advect_slot(V, S, k);
 }
 
 // ---------------------------------------------------------------- grid ----
@@ -1639,12 +1651,36 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   std::vector<uint32_t> chunk(n_ / kSegAlign, 0);
   for (uint32_t s = 0; s < K; ++s)
     for (uint32_t c = h_scenes_[s].seg_start / kSegAlign; c < h_scenes_[s].seg_end / kSegAlign; ++c) chunk[c] = s;
+  // scenes that hold one fluid of one mass and nothing else but colliders
+  // fused into its apply: candidates for the L2-sized groups of run_groups.
+  // Their chunks lead the fluid chunk list, scene by scene.
+  std::vector<uint8_t> pure(K, 0);
+  pure_end_.clear();
+  pure_parts_.clear();
+  pure_scene_.clear();
+  for (uint32_t s = 0; s < K; ++s) {
+    const DevScene& S = h_scenes_[s];
+    if (S.fluid_count != 1 || !S.homog || S.contact || specs[s]->materials.size() != 1) continue;
+    if (S.prim_count + S.sdf_count > 0 && S.collide_rank1 != 1) continue;
+    const DevFluid& F = h_fluids_[S.fluid_first];
+    if (F.has_vort || F.has_st || F.has_ad || F.bnd_count) continue;
+    pure[s] = 1;
+  }
   std::vector<uint32_t> fchunk, cchunk;
+  for (uint32_t s = 0; s < K; ++s) {
+    if (!pure[s]) continue;
+    for (uint32_t c = h_scenes_[s].seg_start / kSegAlign; c < h_scenes_[s].seg_end / kSegAlign; ++c) fchunk.push_back(c);
+    pure_end_.push_back((uint32_t)fchunk.size());
+    pure_parts_.push_back(h_scenes_[s].cap);
+    pure_scene_.push_back(s);
+  }
+  n_pure_chunks_ = (uint32_t)fchunk.size();
   for (uint32_t c = 0; c < chunk.size(); ++c) {
     const DevScene& S = h_scenes_[chunk[c]];
-    if (S.fluid_count) fchunk.push_back(c);
+    if (S.fluid_count && !pure[chunk[c]]) fchunk.push_back(c);
     if ((S.prim_count + S.sdf_count > 0 || S.contact) && S.collide_rank1 == 0) cchunk.push_back(c);
   }
+  groups_.clear();
   std::vector<float> dens(n_, 0.0f);
   std::vector<uint32_t> tag(n_, 0);
   for (uint32_t s = 0; s < K; ++s) {
@@ -2101,10 +2137,10 @@ void World::launch_tiles_build(const WorldView& V, uint32_t s) {
 
 // One-thread-per-slot fluid kernels at a tuned block size.
 template <typename K, typename... A>
-void World::launch_fluid(uint32_t block, K kernel, A... args) {
-  const uint32_t slots = base_.n_fchunk * kSegAlign;  // the chunks of the scenes with a fluid
+void World::launch_fluid(uint32_t block, K kernel, const WorldView& V, A... args) {
+  const uint32_t slots = V.n_fchunk * kSegAlign;  // the view's chunks of scenes with a fluid
   if (!slots) return;
-  kernel<<<div_up(slots, block), block, 0, stream_>>>(args...);
+  kernel<<<div_up(slots, block), block, 0, stream_>>>(V, args...);
   ++t_launches;
 }
 
@@ -2188,6 +2224,61 @@ void World::run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s) {
   }
 }
 
+WorldView World::group_view(const WorldView& V, size_t g) const {
+  WorldView W = V;
+  W.fchunk = base_.fchunk + groups_[g].first;
+  W.n_fchunk = groups_[g].second - groups_[g].first;
+  return W;
+}
+
+WorldView World::rest_view(const WorldView& V) const {
+  if (!grouping()) return V;
+  WorldView W = V;
+  W.fchunk = base_.fchunk + n_pure_chunks_;
+  W.n_fchunk = base_.n_fchunk - n_pure_chunks_;
+  return W;
+}
+
+// Groups of consecutive single-fluid scenes of about tune_.group fluid
+// particles (whole scenes), and each scene's grouped flag.
+void World::apply_grouping() {
+  groups_.clear();
+  for (auto& S : h_scenes_) S.grouped = 0;
+  if (tune_.path != 0 || tune_.group == 0 || pure_end_.empty()) return;
+  uint32_t c0 = 0;
+  uint64_t parts = 0;
+  for (size_t i = 0; i < pure_end_.size(); ++i) {
+    parts += pure_parts_[i];
+    h_scenes_[pure_scene_[i]].grouped = 1;
+    if (parts >= tune_.group || i + 1 == pure_end_.size()) {
+      groups_.push_back({c0, pure_end_[i]});
+      c0 = pure_end_[i];
+      parts = 0;
+    }
+  }
+}
+
+// The substep of the grouped scenes, group by group: the list build, the
+// solver iterations (density + lambda, position correction with its fused
+// apply and colliders), advect, XSPH and its apply. A group's lists and
+// records stay in L2 across these passes. `apply` = 0 leaves x* and the
+// velocities alone (the autotuner's timing).
+void World::run_groups(const WorldView& V, uint32_t s, bool apply) {
+  for (size_t g = 0; g < groups_.size(); ++g) {
+    const WorldView G = group_view(V, g);
+    PF_NBR(G, s);
+    for (uint32_t it = 0; it < max_iter_; ++it) {
+      if (!(fuse_dens_ && it == 0)) PF_BY_UNROLL(kSlotLambda, k_s_lambda, G, 0u, s, it);
+      PF_DELTA(G, 0u, s, it, apply ? 1u : 0u);
+    }
+    if (apply) launch_fluid(kBlock, k_advect_chunks, G, s);
+    if (any_visc_) {
+      PF_XSPH(G, 0u, s);
+      if (apply) launch_slots(k_xsph_apply, G.n_fchunk * kSegAlign, stream_, G, 0u, s);
+    }
+  }
+}
+
 // Autotuner: on the world's own state (one grid rebuild, as the next
 // substep would do; the permutation is canonical, so no result changes),
 // time each slot kernel (list build, density + lambda, position correction,
@@ -2209,6 +2300,9 @@ pf_status World::tune() {
       tune_.block[q] = blk;
       tune_.unroll[q] = unr;
     }
+    tune_.group = 0;
+    if (const char* g = std::getenv("PFSIM_GROUP")) tune_.group = (uint32_t)std::atoi(g);
+    apply_grouping();
     return PF_OK;
   }
   run_sort_and_permute(parity_, false);
@@ -2270,6 +2364,29 @@ pf_status World::tune() {
     const uint32_t reps = kind == kSlotDelta ? iters : (kind == kSlotLambda ? iters - (fuse_dens_ ? 1u : 0u) : 1u);
     slot_total += best * reps;
   }
+  // L2-sized groups of the single-fluid scenes: time their neighbour passes
+  // group by group against one launch per pass over all of them
+  tune_.group = 0;
+  uint64_t pure_total = 0;
+  for (uint64_t p : pure_parts_) pure_total += p;
+  if (!pure_end_.empty() && !std::getenv("PFSIM_NO_GROUPS")) {
+    float best = 1e30f;
+    uint32_t best_g = 0;
+    const uint32_t cands[4] = {0u, 393216u, 786432u, 1572864u};
+    for (uint32_t gsz : cands) {
+      if (gsz && gsz >= pure_total) continue;  // one group is no grouping
+      tune_.group = gsz ? gsz : 0xffffffffu;   // 0 here: all pure scenes as one launch
+      apply_grouping();
+      float t = 0;
+      PF_TRY(timed([&] { run_groups(V, 0u, false); }, &t));
+      if (t < best) {
+        best = t;
+        best_g = gsz;
+      }
+    }
+    tune_.group = best_g;
+    apply_grouping();
+  }
   // the warp-tile path has no vorticity or surface pass and reads one shared
   // lambda buffer: worlds with those, or with a scene of several fluids,
   // stay on slots
@@ -2284,6 +2401,7 @@ pf_status World::tune() {
         },
         &t));
     tune_.path = t < slot_total ? 1u : 0u;
+    apply_grouping();  // groups are a slot-path schedule
   }
   PF_CUDA(cudaMemcpyAsync(V.cur.dens, keep, 4ull * n_, cudaMemcpyDeviceToDevice, stream_));
   return PF_OK;
@@ -2361,6 +2479,9 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   } else {
     launch_slots(k_reset_sums, n_, stream_, V);
   }
+  // the other fluid scenes' passes run over their chunks (all fluid chunks
+  // without groups); the grouped scenes run after the cloth fork below
+  const WorldView VF = rest_view(V);
   // preSolve: contacts first (loop.ts:196-223), then the materials'
   if (any_contact_) {
     const uint32_t K = (uint32_t)h_scenes_.size();
@@ -2372,7 +2493,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
   }
   launch_aero(V, 0, s);
   if (any_dyn_bnd_) launch_slots(k_boundary_volume, n_, stream_, V, 0u, s);
-  if (any_fluid_) run_fluid_neighbors(V, s);
+  if (any_fluid_) run_fluid_neighbors(VF, s);
   // FluidSystem.ts:233-255: surface tension and adhesion, once per substep
   if (any_imp_)
     for (uint32_t r = 0; r < max_rank_; ++r) {
@@ -2382,9 +2503,9 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         imp = imp || (F.rank == r && (F.has_st || F.has_ad));
       }
       if (!imp) continue;
-      if (st) PF_BY_UNROLL(kSlotVel, k_s_color_normal, V, r, s);
-      PF_BY_UNROLL(kSlotVel, k_s_impulses, V, r, s);
-      launch_slots(k_imp_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s);
+      if (st) PF_BY_UNROLL(kSlotVel, k_s_color_normal, VF, r, s);
+      PF_BY_UNROLL(kSlotVel, k_s_impulses, VF, r, s);
+      launch_slots(k_imp_apply, VF.n_fchunk * kSegAlign, stream_, VF, r, s);
     }
   launch_aero(V, 1, s);
   // pair multipliers reset every substep (buildImplicitResetPairLambdaKernel)
@@ -2407,6 +2528,8 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (any_unfused_prims_) launch_slots(k_collide, base_.n_cchunk * kSegAlign, side_stream_, V, s, it);
     }
   }
+  // the grouped single-fluid scenes' whole substep, beside the cloth sweeps
+  if (grouping()) run_groups(V, s, true);
   for (uint32_t it = 0; it < max_iter_; ++it) {
     for (uint32_t r = 0; r < max_rank_; ++r) {
       bool has_fluid = false, has_local = false, has_global = false;
@@ -2415,13 +2538,13 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         has_local = has_local || (D.rank == r && D.local);
         has_global = has_global || (D.rank == r && !D.local);
       }
-      if (has_fluid) {
-        run_fluid_lambda_delta(V, r, s, it);
+      if (has_fluid && VF.n_fchunk) {
+        run_fluid_lambda_delta(VF, r, s, it);
         // on the slot path the position pass applies homogeneous scenes itself
         const bool slot = tune_.path == 0;
         bool rest = !slot;
         for (auto& S : h_scenes_) rest = rest || (S.fluid_count && !S.homog);
-        if (rest) launch_slots(k_fluid_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s, it, slot ? 1u : 0u);
+        if (rest) launch_slots(k_fluid_apply, VF.n_fchunk * kSegAlign, stream_, VF, r, s, it, slot ? 1u : 0u);
       }
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
@@ -2454,10 +2577,10 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       has_vort = has_vort || (F.rank == r && F.has_vort);
     }
     for (auto& D : h_softs_) has_local = has_local || (D.rank == r && D.local);
-    if (has_velocity) {
-      run_fluid_xsph(V, r, s);
-      if (has_vort) PF_BY_UNROLL(kSlotVel, k_s_vort_grad, V, r, s);
-      launch_slots(k_xsph_apply, base_.n_fchunk * kSegAlign, stream_, V, r, s);
+    if (has_velocity && VF.n_fchunk) {
+      run_fluid_xsph(VF, r, s);
+      if (has_vort) PF_BY_UNROLL(kSlotVel, k_s_vort_grad, VF, r, s);
+      launch_slots(k_xsph_apply, VF.n_fchunk * kSegAlign, stream_, VF, r, s);
     }
     if (has_local) {
       launch_slots(k_rot_advect, base_.n_grp, stream_, V, s);
@@ -2490,7 +2613,10 @@ pf_status World::step(double dt) {
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
   PF_TRY(upload_params(dt));
   PF_CUDA(cudaEventRecord(ev0_, stream_));
-  if (!tuned_) PF_TRY(tune());
+  if (!tuned_) {
+    PF_TRY(tune());
+    PF_TRY(upload_params(dt));  // the scenes' grouped flags the tuner set
+  }
   if (!inited_) {
     run_init_pass();
     inited_ = true;
@@ -2882,26 +3008,36 @@ pf_status World::profile_stage(uint32_t stage, uint32_t reps, float* ms, uint64_
   uint64_t fluid = 0;
   for (uint32_t s = 0; s < specs_.size(); ++s)
     for (auto& f : specs_[s]->fluids) fluid += f.range.count;
-  auto run = [&]() {
+  auto run_on = [&](const WorldView& W) {
     switch (stage) {
       case 0:
-        if (tune_.path == 1) launch_tiled(k_t_neighbors, kSmemNbr, V, 0u);
-        else PF_NBR(V, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_neighbors, kSmemNbr, W, 0u);
+        else PF_NBR(W, 0u);
         break;
       case 1:
-        if (tune_.path == 1) launch_tiled(k_t_lambda, kSmemLambda, V, rank, 0u, 0u);
-        else PF_BY_UNROLL(kSlotLambda, k_s_lambda, V, rank, 0u, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_lambda, kSmemLambda, W, rank, 0u, 0u);
+        else PF_BY_UNROLL(kSlotLambda, k_s_lambda, W, rank, 0u, 0u);
         break;
       case 2:  // with the apply the step fuses in (it rewrites x*, which the next predict replaces)
-        if (tune_.path == 1) launch_tiled(k_t_delta, kSmemDelta, V, rank, 0u, 0u);
-        else PF_DELTA(V, rank, 0u, 0u, 1u);
+        if (tune_.path == 1) launch_tiled(k_t_delta, kSmemDelta, W, rank, 0u, 0u);
+        else PF_DELTA(W, rank, 0u, 0u, 1u);
         break;
       case 3:
-        if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, V, rank, 0u);
-        else PF_XSPH(V, rank, 0u);
+        if (tune_.path == 1) launch_tiled(k_t_xsph, kSmemXsph, W, rank, 0u);
+        else PF_XSPH(W, rank, 0u);
         break;
-      case 4: launch_slots(k_predict, n_, stream_, V, 0u); break;
+      case 4: launch_slots(k_predict, n_, stream_, W, 0u); break;
       default: break;
+    }
+  };
+  // as the step launches it: group by group, then the other fluid scenes
+  auto run = [&]() {
+    if (stage < 4 && grouping()) {
+      for (size_t g = 0; g < groups_.size(); ++g) run_on(group_view(V, g));
+      const WorldView R = rest_view(V);
+      if (R.n_fchunk) run_on(R);
+    } else {
+      run_on(V);
     }
   };
   if (stage > 4) return fail(PF_ERR_INVALID, "profile: unknown stage");

@@ -181,6 +181,10 @@ struct DevScene {
   // from xl in one load
   uint32_t homog;
   float homog_mass;
+  // a single-fluid scene of one mass with nothing else but fused colliders,
+  // stepped by the L2-sized groups of World::run_groups (the world's other
+  // passes leave it alone)
+  uint32_t grouped;
 };
 
 // One SDF collider as the kernels read it (sdf.ts:17-80 fields).
@@ -459,6 +463,10 @@ class World {
     uint32_t path = 0;
     uint32_t block[4] = {256, 256, 256, 256};
     uint32_t unroll[4] = {4, 4, 4, 4};
+    // fluid particles per group of run_groups (0: no groups): the scenes
+    // that only hold one fluid of one mass run their whole substep group by
+    // group, so a group's lists and records stay in L2 across its passes
+    uint32_t group = 0;
   };
   void tuning(uint32_t* path, uint32_t* block, uint32_t* unroll = nullptr) const {
     *path = tune_.path;
@@ -473,7 +481,8 @@ class World {
   void set_tuning(const Tuning& t) {
     tune_ = t;
     tuned_ = true;
-    drop_graphs();  // captured launches depend on the path
+    apply_grouping();  // this world's own groups of that size
+    drop_graphs();     // captured launches depend on the path
   }
   size_t device_bytes() const { return bytes_; }
 
@@ -486,10 +495,17 @@ class World {
   void run_init_pass();
   void launch_tiles_build(const WorldView& V, uint32_t s);
   template <typename K, typename... A>
-  void launch_fluid(uint32_t block, K kernel, A... args);
+  void launch_fluid(uint32_t block, K kernel, const WorldView& V, A... args);
   void run_fluid_neighbors(const WorldView& V, uint32_t s);
   void run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it);
   void run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s);
+  // L2-sized groups of the single-fluid scenes (their chunks lead fchunk):
+  // each group's substep (list build, iterations, advect, XSPH) in turn
+  void run_groups(const WorldView& V, uint32_t s, bool apply);
+  WorldView group_view(const WorldView& V, size_t g) const;
+  WorldView rest_view(const WorldView& V) const;  // the other fluid scenes' chunks
+  void apply_grouping();  // groups_ and the scenes' grouped flags from tune_.group
+  bool grouping() const { return tune_.path == 0 && !groups_.empty(); }
   pf_status tune();
   template <typename K, typename... A>
   void launch_tiled(K kernel, size_t smem, const WorldView& V, A... args);
@@ -527,6 +543,14 @@ class World {
   bool any_contact_ = false;        // a scene with particle contacts
   bool any_multi_fluid_ = false;    // a scene with two or more fluids (slot path only)
   bool fuse_dens_ = false;          // the slot list build forms the first density and lambda
+  // single-fluid scenes (DevScene::grouped candidates): their chunks are
+  // fchunk[0, n_pure_chunks_), scene by scene; per scene its end chunk and
+  // its fluid particles
+  uint32_t n_pure_chunks_ = 0;
+  std::vector<uint32_t> pure_end_;
+  std::vector<uint64_t> pure_parts_;
+  std::vector<uint32_t> pure_scene_;
+  std::vector<std::pair<uint32_t, uint32_t>> groups_;  // chunk ranges [begin, end) of fchunk
   uint32_t n_ = 0, cells_ = 0, prim_stride_ = 0;
   // device memory: one arena
   void* arena_ = nullptr;
