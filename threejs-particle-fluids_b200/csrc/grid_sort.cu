@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <set>
 #include <string>
 
 #include "grid_sort.cuh"
@@ -617,12 +619,7 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
     if (plan.passes == 0) {
       k_identity<<<div_up(n, 256), 256, 0, st>>>(perm, n);
     } else {
-      static bool attr_set = false;  // per process; the attribute is per function and device
-      if (!attr_set) {
-        cudaFuncSetAttribute(k_radix_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOsSmemBytes);
-        cudaFuncSetAttribute(k_radix_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOsSmemBytes);
-        attr_set = true;
-      }
+      if (cudaError_t e = radix_prepare(); e != cudaSuccess) return e;
       if (cudaError_t e = cudaMemsetAsync(s.counters + kCounterPass0, 0, 4 * kRadixMaxPasses, st); e != cudaSuccess)
         return e;
       k_digit_first<<<plan.passes, 1024, 0, st>>>(s.digit_count, plan.digits);
@@ -655,6 +652,25 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
   }
   if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
   return launch_exclusive_scan(count, start, nullptr, C, s.scan_status, s.counters, st);
+}
+
+cudaError_t radix_prepare() {
+  static std::mutex m;
+  static std::set<int> ready;
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(m);
+  if (ready.count(dev)) return cudaSuccess;
+  if (cudaError_t e = cudaFuncSetAttribute(k_radix_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kOsSmemBytes);
+      e != cudaSuccess)
+    return e;
+  if (cudaError_t e = cudaFuncSetAttribute(k_radix_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kOsSmemBytes);
+      e != cudaSuccess)
+    return e;
+  ready.insert(dev);
+  return cudaSuccess;
 }
 
 cudaError_t sort_run(const float4* pos, uint32_t n, const KeyFn& kf, uint64_t C, uint32_t* perm, uint32_t* start,

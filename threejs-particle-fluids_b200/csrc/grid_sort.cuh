@@ -95,6 +95,11 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
                              uint32_t* count, uint32_t* start, uint32_t* perm, const SortScratch& s,
                              cudaStream_t st);
 
+// Per device, once: the radix passes' shared-memory size above the default
+// limit. Call it outside stream capture before the first sort on a device
+// (the sort calls it itself; a world calls it when it is built).
+cudaError_t radix_prepare();
+
 // The whole standalone sort on device buffers: clears the counts and
 // counters it needs, computes keys (into `keys`) and the overflow flag, and
 // sorts. `overflow` may be null (the flag then goes to a scratch counter).

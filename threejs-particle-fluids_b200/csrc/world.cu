@@ -1883,6 +1883,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   };
   PF_CUDA(cudaMemsetAsync(arena_, 0, probe.off, stream_));
   PF_CUDA(sort_scratch_zero(sort_, stream_));
+  PF_CUDA(radix_prepare());  // before any graph capture
   PF_TRY(up(base_.scenes_rw, h_scenes_.data(), sizeof(DevScene) * K));
   {
     // empty cell bounds: the predict pass narrows them (a pageable source:
