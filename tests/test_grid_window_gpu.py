@@ -146,3 +146,22 @@ def test_too_small_window_clamps_and_keeps_every_neighbour(oracle, cuda):
     assert np.array_equal(ca, cb)
     for i in range(0, r.capacity, 7):
         assert set(la[i, :ca[i]].tolist()) == set(lb[i, :cb[i]].tolist())
+
+
+def test_wide_warps_keep_32_bit_entries(oracle, cuda):
+    """A fluid slab two cells thick and 130 cells wide: a z-layer holds about
+    135,000 particles, so a warp's 27-cell rows reach further than 65,536
+    slots and its list falls back to whole 32-bit slots. The lists still
+    equal the oracle's, element for element."""
+    s = 0.01
+    h = 2.0 * s
+    pts = W.fill_box(np.array([0.0, 0.0, 0.0]), np.array([130 * h, 130 * h, 2 * h]), s)
+    pts = pts + W.rng(25).uniform(-0.05 * s, 0.05 * s, pts.shape)
+    mass = 1000.0 * s**3
+    rho0 = W.lattice_rest_density(s, h, mass)
+    fluid = R.FluidOpts(range=(0, pts.shape[0]), rest_density=rho0, particle_spacing=(mass / rho0) ** (1 / 3),
+                        smoothing_radius=h, compliance=1e-4, viscosity=0.01)
+    r = R.Recipe(capacity=pts.shape[0], radius=s / 2, uploads=[R.Upload(0, pts.astype(np.float32))],
+                 materials=[("fluid", fluid)], loop=R.LoopOpts(substeps=1, iterations=1, gravity=(0.0, 0.0, 0.0)))
+    assert pts.shape[0] > 260_000
+    assert_same_lists(oracle, cuda, r)

@@ -2155,18 +2155,23 @@ void World::launch_fluid(uint32_t block, K kernel, const WorldView& V, A... args
   } while (0)
 // The list build, forming the first iteration's density and lambda of
 // first-material fluids when nothing moves between the two (fuse_dens_).
-#define PF_NBR(...)                                                                     \
+#define PF_NBR_FLAT(FLAT, ...)                                                          \
   do {                                                                                  \
     const uint32_t b_ = tune_.block[kSlotNbr], u_ = tune_.unroll[kSlotNbr];             \
     if (fuse_dens_) {                                                                   \
-      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, true>, __VA_ARGS__);               \
-      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, true>, __VA_ARGS__);          \
-      else launch_fluid(b_, k_s_neighbors<4, true>, __VA_ARGS__);                       \
+      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, true, FLAT>, __VA_ARGS__);         \
+      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, true, FLAT>, __VA_ARGS__);    \
+      else launch_fluid(b_, k_s_neighbors<4, true, FLAT>, __VA_ARGS__);                 \
     } else {                                                                            \
-      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, false>, __VA_ARGS__);              \
-      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, false>, __VA_ARGS__);         \
-      else launch_fluid(b_, k_s_neighbors<4, false>, __VA_ARGS__);                      \
+      if (u_ == 2) launch_fluid(b_, k_s_neighbors<2, false, FLAT>, __VA_ARGS__);        \
+      else if (u_ == 8) launch_fluid(b_, k_s_neighbors<8, false, FLAT>, __VA_ARGS__);   \
+      else launch_fluid(b_, k_s_neighbors<4, false, FLAT>, __VA_ARGS__);                \
     }                                                                                   \
+  } while (0)
+#define PF_NBR(...)                                                                     \
+  do {                                                                                  \
+    if (tune_.nbr_flat) PF_NBR_FLAT(true, __VA_ARGS__);                                 \
+    else PF_NBR_FLAT(false, __VA_ARGS__);                                               \
   } while (0)
 // XSPH, without the boundary-volume gather when the world has no boundaries.
 #define PF_XSPH(...)                                                                    \
@@ -2303,6 +2308,8 @@ pf_status World::tune() {
     }
     tune_.group = 0;
     if (const char* g = std::getenv("PFSIM_GROUP")) tune_.group = (uint32_t)std::atoi(g);
+    tune_.nbr_flat = 0;
+    if (const char* fl = std::getenv("PFSIM_NBR_FLAT")) tune_.nbr_flat = std::atoi(fl) ? 1u : 0u;
     apply_grouping();
     return PF_OK;
   }
@@ -2339,12 +2346,14 @@ pf_status World::tune() {
   for (int kind = 0; kind < 4; ++kind) {
     if (kind == kSlotVel && !vel) continue;
     float best = 1e30f;
-    uint32_t bb = 256, bu = 4;
+    uint32_t bb = 256, bu = 4, bf = 0;
+    for (uint32_t flat = 0; flat < (kind == kSlotNbr ? 2u : 1u); ++flat)
     for (uint32_t b : blocks)
       for (uint32_t u : unrolls) {
         if (u == 8 && b == 512) continue;
         tune_.block[kind] = b;
         tune_.unroll[kind] = u;
+        if (kind == kSlotNbr) tune_.nbr_flat = flat;
         float t = 0;
         PF_TRY(timed(
             [&] {
@@ -2358,10 +2367,12 @@ pf_status World::tune() {
           best = t;
           bb = b;
           bu = u;
+          bf = kind == kSlotNbr ? tune_.nbr_flat : 0u;
         }
       }
     tune_.block[kind] = bb;
     tune_.unroll[kind] = bu;
+    if (kind == kSlotNbr) tune_.nbr_flat = bf;
     const uint32_t reps = kind == kSlotDelta ? iters : (kind == kSlotLambda ? iters - (fuse_dens_ ? 1u : 0u) : 1u);
     slot_total += best * reps;
   }

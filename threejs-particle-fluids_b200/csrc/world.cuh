@@ -467,6 +467,8 @@ class World {
     // that only hold one fluid of one mass run their whole substep group by
     // group, so a group's lists and records stay in L2 across its passes
     uint32_t group = 0;
+    // the list build walks its nine rows as one sequence (k_s_neighbors kFlat)
+    uint32_t nbr_flat = 0;
   };
   void tuning(uint32_t* path, uint32_t* block, uint32_t* unroll = nullptr) const {
     *path = tune_.path;

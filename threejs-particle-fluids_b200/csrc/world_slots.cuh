@@ -194,7 +194,11 @@ __device__ __forceinline__ void lambda_terms(const DevFluid& F, f3 xi, float4 xj
 // density and lambda of its first solver iteration from the same hits, in
 // the same order (nothing moves between the list and that pass when the
 // world has no surface impulses and no late drag and lift).
-template <uint32_t kNbrUnroll, bool kDens>
+// kFlat: the nine rows are walked as one sequence, kNbrUnroll candidates
+// per round across row ends, so a warp waits for its longest walk rather
+// than, row by row, for each row's longest (the same candidates in the same
+// order; the autotuner picks the faster form).
+template <uint32_t kNbrUnroll, bool kDens, bool kFlat>
 __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= V.n_fchunk * kSegAlign) return;     // whole warps
@@ -288,27 +292,68 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
       ++cnt;
     }
   };
+  if (kFlat) {
+    // the row pointer moves on at each row's end (empty rows skipped); the
+    // rows stay in registers (constant indices after unrolling)
+    int r = 0;
+    uint32_t j = rs[0], e = re[0];
+    auto pick = [](const uint32_t(&a)[9], int q) {
+      uint32_t v = a[0];
 #pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    uint32_t j = rs[r];
-    const uint32_t e = re[r];
-    // whole rounds, then the row's last 1 to kNbrUnroll - 1 candidates as
-    // one guarded round (their loads in flight together)
-    for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
+      for (int t = 1; t < 9; ++t) v = q == t ? a[t] : v;
+      return v;
+    };
+    auto advance = [&]() {
+      while (j >= e && r < 8) {
+        ++r;
+        j = pick(rs, r);
+        e = pick(re, r);
+      }
+    };
+    advance();
+    while (j < e) {
+      uint32_t c[kNbrUnroll];
+      bool live[kNbrUnroll];
+#pragma unroll
+      for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+        live[q] = j < e;
+        c[q] = j;
+        if (live[q]) {
+          ++j;
+          if (j >= e) advance();
+        }
+      }
       float4 xj[kNbrUnroll];
 #pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
+      for (uint32_t q = 0; q < kNbrUnroll; ++q)
+        if (live[q]) xj[q] = __ldg(V.cur.xs + c[q]);
 #pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
+      for (uint32_t q = 0; q < kNbrUnroll; ++q)
+        if (live[q]) test(c[q], xj[q]);
     }
-    if (j < e) {
-      float4 xj[kNbrUnroll];
+  } else {
 #pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q)
-        if (j + q < e) xj[q] = __ldg(V.cur.xs + j + q);
+    for (int r = 0; r < 9; ++r) {
+      uint32_t j = rs[r];
+      const uint32_t e = re[r];
+      // whole rounds, then the row's last 1 to kNbrUnroll - 1 candidates as
+      // one guarded round (their loads in flight together)
+      for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
+        float4 xj[kNbrUnroll];
 #pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q)
-        if (j + q < e) test(j + q, xj[q]);
+        for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
+      }
+      if (j < e) {
+        float4 xj[kNbrUnroll];
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q)
+          if (j + q < e) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q)
+          if (j + q < e) test(j + q, xj[q]);
+      }
     }
   }
   const bool over = cnt > kMaxNbr;
