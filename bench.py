@@ -199,9 +199,9 @@ class SortWorkload:
             "ms": ms,
             "units_per_step": self.n,
             "kernel_ms": ms,
-            "kernel_name": "grid sort pipeline (keys+hist, look-back scan, scatter, fix-up)",
+            "kernel_name": "grid sort pipeline (keys + digit counts, LSD radix passes with look-back, run counts, start scan)",
             "algorithmic_bytes": self.algorithmic_bytes(),
-            "gpu_launches_per_step": 10,
+            "gpu_launches_per_step": 6,  # keys + digit counts, digit starts, 2 radix passes, run counts, start scan
             "clocks": clk,
             "e2e_ms": e2e_ms,
             "h2d": 16 * self.n,

@@ -104,7 +104,7 @@ PF_API pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* gr
 /* pf_sort that allocates no device memory (no counterpart in the reference;
  * added for callers that cannot allocate, such as hosts whose own pool owns
  * the device memory or loops where an allocation would stall the frame).
- * Same arguments and results as pf_sort. Its scratch is one fixed 27 MiB
+ * Same arguments and results as pf_sort. Its scratch is one fixed 23 MiB
  * block compiled into the library, so n <= 1,048,576 particles and at most
  * 2,097,152 cells per call; larger sizes return PF_ERR_INVALID. The runtime
  * loads that block lazily: the first call on a device reserves it there

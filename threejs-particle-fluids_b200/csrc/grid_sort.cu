@@ -6,18 +6,19 @@
 //   * keys with every radix pass's digit counts, from shared-memory
 //     histograms (one global atomic per digit per block);
 //   * one least-significant-digit radix pass per 11 key bits (two for a
-//     128^3 grid), each a single kernel: tiles rank their elements by digit
-//     in element order with warp-aggregated ranks (__match_any_sync), find
-//     each digit's output position by a decoupled look-back over the tiles
-//     before them, and write their elements run by run through shared memory
-//     (Adinets and Merrill's "Onesweep" structure). The passes are stable,
-//     unlike the reference's atomic write cursor (sort.ts:187-192), so the
-//     permutation lists each cell's particles in ascending index;
+//     128^3 grid), each three steps: every tile of 4096 elements counts its
+//     digits; the counts are scanned over the tiles per digit (in chunks of
+//     32 tiles, then over the chunks); every tile ranks its elements by digit
+//     in element order with warp-aggregated ranks (__match_any_sync) and
+//     writes them out run by run through shared memory. The passes are
+//     stable, unlike the reference's atomic write cursor (sort.ts:187-192),
+//     so the permutation lists each cell's particles in ascending index;
 //   * cell counts from the sorted keys (one atomic per run of equal keys in a
 //     warp) and a single-pass decoupled look-back scan to the cell starts,
 //     so the bucket count is not capped at 1024^2 as in the two-level
 //     workgroup scan (sort.ts:22-28).
-// Every spin-wait is bounded and reports DEV_ERR_LOOKBACK_TIMEOUT.
+// The one spin-wait (the start scan's look-back) is bounded and reports
+// DEV_ERR_LOOKBACK_TIMEOUT.
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -52,11 +53,6 @@ constexpr uint32_t kOsPer = kRadixMaxDigits / kOsThreads;  // digits per thread 
 constexpr uint32_t kOsStageWords = 2 * kRadixTile;
 static_assert(kOsWarps * kRadixMaxDigits / 2 <= kOsStageWords, "histograms fit the staging area");
 constexpr size_t kOsSmemBytes = 4ull * (kOsStageWords + 2 * kRadixMaxDigits);
-// look-back status word: bits 31..30 flag (1 tile count, 2 inclusive
-// prefix), bits 29..0 the value (so n < 2^30)
-constexpr uint32_t kStAgg = 1u << 30;
-constexpr uint32_t kStInc = 2u << 30;
-constexpr uint32_t kStVal = (1u << 30) - 1u;
 constexpr uint32_t kMortonBias = 512;
 constexpr int32_t kCellCoordMax = 1 << 30;
 
@@ -281,41 +277,104 @@ __global__ void __launch_bounds__(1024) k_digit_first(uint32_t* __restrict__ dc,
 }
 
 // ------------------------------------------------------------ radix pass ----
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// A pass over digit (key >> shift) & (digits - 1) runs as three kernels: each
+// tile of kRadixTile elements counts its digits (k_tile_counts); the counts
+// are scanned over the tiles per digit, in chunks of kScanChunk tiles
+// (k_tile_scan_chunk, k_tile_scan_chunks), giving each tile its first output
+// position per digit; each tile then ranks its elements by digit in element
+// order and writes them out digit run by digit run (k_radix_scatter). No
+// kernel waits on another block.
+constexpr uint32_t kScanChunk = 32;  // tiles per chunk of the tile-count scan
+
+// Digit counts of tile blockIdx.x: row tile of `tcount` (digits entries).
+__global__ void __launch_bounds__(kOsThreads)
+k_tile_counts(const uint32_t* __restrict__ kin, uint32_t n, uint32_t shift, uint32_t digits,
+              uint32_t* __restrict__ tcount) {
+  __shared__ uint32_t h[kRadixMaxDigits];
+  for (uint32_t d = threadIdx.x; d < digits; d += kOsThreads) h[d] = 0u;
+  __syncthreads();
+  const uint32_t mask = digits - 1u;
+  const size_t base = (size_t)blockIdx.x * kRadixTile;
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < kRadixTile; i += kOsThreads) {
+    const size_t e = base + i;
+    if (e < n) atomicAdd(h + ((__ldg(kin + e) >> shift) & mask), 1u);
+  }
+  __syncthreads();
+  uint32_t* row = tcount + (size_t)blockIdx.x * digits;
+  for (uint32_t d = threadIdx.x; d < digits; d += kOsThreads) row[d] = h[d];
 }
 
-// One stable LSD pass over digit (key >> shift) & (digits - 1). Tiles are
-// numbered in launch order by a ticket, so every tile's predecessors have
-// started and its look-back ends. kFirst: the values are the element indices.
-// `status` holds this pass's look-back words (clear on entry); `clear`, when
-// given, is the next pass's region, whose row of this tile is cleared here.
+// Per digit (one thread each), the exclusive running sum over the tiles of
+// chunk blockIdx.x, in place, and the chunk's total into `csum`.
+__global__ void __launch_bounds__(256)
+k_tile_scan_chunk(uint32_t* __restrict__ tcount, uint32_t tiles, uint32_t digits, uint32_t* __restrict__ csum) {
+  const uint32_t d = blockIdx.y * blockDim.x + threadIdx.x;
+  if (d >= digits) return;
+  const uint32_t t0 = blockIdx.x * kScanChunk, t1 = min(t0 + kScanChunk, tiles);
+  uint32_t v[kScanChunk];
+#pragma unroll
+  for (uint32_t q = 0; q < kScanChunk; ++q) v[q] = t0 + q < t1 ? tcount[(size_t)(t0 + q) * digits + d] : 0u;
+  uint32_t run = 0;
+#pragma unroll
+  for (uint32_t q = 0; q < kScanChunk; ++q) {
+    if (t0 + q < t1) tcount[(size_t)(t0 + q) * digits + d] = run;
+    run += v[q];
+  }
+  csum[(size_t)blockIdx.x * digits + d] = run;
+}
+
+// Per digit, the chunk totals -> each chunk's first output position
+// (the digit's first position plus the counts of the chunks before), in place.
+__global__ void __launch_bounds__(256)
+k_tile_scan_chunks(uint32_t* __restrict__ csum, uint32_t chunks, uint32_t digits, const uint32_t* __restrict__ first) {
+  const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= digits) return;
+  uint32_t run = first[d];
+  uint32_t c = 0;
+  for (; c + 8 <= chunks; c += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (uint32_t q = 0; q < 8; ++q) v[q] = csum[(size_t)(c + q) * digits + d];
+#pragma unroll
+    for (uint32_t q = 0; q < 8; ++q) {
+      csum[(size_t)(c + q) * digits + d] = run;
+      run += v[q];
+    }
+  }
+  for (; c < chunks; ++c) {
+    const uint32_t v = csum[(size_t)c * digits + d];
+    csum[(size_t)c * digits + d] = run;
+    run += v;
+  }
+}
+
+// The scatter of one stable LSD pass: tile blockIdx.x ranks its elements by
+// digit in element order, stages them in digit order in shared memory and
+// writes each digit's run to the run's first output position (the tile's
+// scanned count plus its chunk's base). kFirst: the values are the element
+// indices.
 template <bool kFirst>
 __global__ void __launch_bounds__(kOsThreads, 2)
-k_radix_pass(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
-             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
-             const uint32_t* __restrict__ first, uint32_t* __restrict__ status, uint32_t* __restrict__ clear,
-             uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
+k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
+                uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
+                const uint32_t* __restrict__ tcount, const uint32_t* __restrict__ csum) {
   extern __shared__ uint32_t sm[];
   uint16_t* whist = reinterpret_cast<uint16_t*>(sm);  // [warp][digit], then the staged tile
   uint32_t* stage_k = sm;
   uint32_t* stage_v = sm + kRadixTile;
-  uint32_t* lstart = sm + kOsStageWords;     // first tile position of each digit
+  uint32_t* lstart = sm + kOsStageWords;        // first tile position of each digit
   uint32_t* gstart = lstart + kRadixMaxDigits;  // first output position of each digit
-  __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wsum[kOsWarps];
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  const uint32_t tile = blockIdx.x;
   for (uint32_t w = tid; w < kOsWarps * digits / 2; w += kOsThreads) sm[w] = 0u;
+  {
+    const uint32_t* trow = tcount + (size_t)tile * digits;
+    const uint32_t* crow = csum + (size_t)(tile / kScanChunk) * digits;
+    for (uint32_t d = tid; d < digits; d += kOsThreads) gstart[d] = __ldg(trow + d) + __ldg(crow + d);
+  }
   __syncthreads();
-  const uint32_t tile = s_tile;
-  if (clear)
-    for (uint32_t d = tid; d < kRadixMaxDigits; d += kOsThreads) clear[(size_t)tile * kRadixMaxDigits + d] = 0u;
   const uint32_t mask = digits - 1u;
   const uint32_t base = tile * kRadixTile + warp * kOsStripe;
   uint32_t key[kOsItems], val[kOsItems], pos[kOsItems];
@@ -383,66 +442,6 @@ k_radix_pass(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
       }
   }
   __syncthreads();
-  // publish this tile's digit counts, then look back over the preceding
-  // tiles for each digit's output position (all of a thread's digits at once)
-  const uint32_t tile_valid = min(kRadixTile, n - tile * kRadixTile);
-  uint32_t* row = status + (size_t)tile * kRadixMaxDigits;
-  uint32_t cnt[kOsPer], excl[kOsPer];
-  int32_t pred[kOsPer];
-  uint32_t pending = 0;
-#pragma unroll
-  for (uint32_t j = 0; j < kOsPer; ++j) {
-    const uint32_t d = tid + j * kOsThreads;
-    cnt[j] = 0;
-    excl[j] = 0;
-    pred[j] = (int32_t)tile - 1;
-    if (d < digits) {
-      cnt[j] = (d + 1 < digits ? lstart[d + 1] : tile_valid) - lstart[d];
-      if (tile == 0) {
-        excl[j] = first[d];
-        st_relaxed(row + d, kStInc | (excl[j] + cnt[j]));
-      } else {
-        st_relaxed(row + d, kStAgg | cnt[j]);
-        pending |= 1u << j;
-      }
-    }
-  }
-  uint32_t spins = 0;
-  while (pending) {
-    bool waiting = false;
-#pragma unroll
-    for (uint32_t j = 0; j < kOsPer; ++j) {
-      if (!((pending >> j) & 1u)) continue;
-      const uint32_t d = tid + j * kOsThreads;
-      const uint32_t s = ld_relaxed(status + (size_t)pred[j] * kRadixMaxDigits + d);
-      const uint32_t f = s >> 30;
-      if (f == 0) {
-        waiting = true;
-        continue;
-      }
-      excl[j] += s & kStVal;
-      if (f == 2) {
-        pending &= ~(1u << j);
-        st_relaxed(row + d, kStInc | (excl[j] + cnt[j]));
-      } else {
-        --pred[j];
-      }
-    }
-    if (waiting && ++spins >= kLookbackSpinLimit) {
-      // give up: report, and publish what we have so that no later tile waits
-      atomicOr(err, DEV_ERR_LOOKBACK_TIMEOUT);
-#pragma unroll
-      for (uint32_t j = 0; j < kOsPer; ++j)
-        if ((pending >> j) & 1u) st_relaxed(row + tid + j * kOsThreads, kStInc | ((excl[j] + cnt[j]) & kStVal));
-      break;
-    }
-    if (waiting) __nanosleep(32);
-  }
-#pragma unroll
-  for (uint32_t j = 0; j < kOsPer; ++j) {
-    const uint32_t d = tid + j * kOsThreads;
-    if (d < digits) gstart[d] = excl[j];
-  }
   // tile positions, then the tile staged in digit order
 #pragma unroll
   for (uint32_t i = 0; i < kOsItems; ++i) {
@@ -458,6 +457,7 @@ k_radix_pass(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
     }
   __syncthreads();
   // out run by run: consecutive threads write consecutive positions of a digit
+  const uint32_t tile_valid = min(kRadixTile, n - tile * kRadixTile);
   for (uint32_t k = tid; k < tile_valid; k += kOsThreads) {
     const uint32_t kk = stage_k[k];
     const uint32_t d = (kk >> shift) & mask;
@@ -473,16 +473,22 @@ __global__ void __launch_bounds__(256) k_identity(uint32_t* __restrict__ perm, u
   if (i < n) perm[i] = i;
 }
 
-// Cell counts from the sorted keys: one atomic per run of equal keys in a warp.
+// Cell counts from the sorted keys: one atomic per run of equal keys in a
+// warp (a run's first lane in the warp adds the run's length there).
 __global__ void __launch_bounds__(256) k_run_counts(const uint32_t* __restrict__ sk, uint32_t n,
                                                     uint32_t* __restrict__ count) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = lane_id();
   const bool valid = i < n;
-  const uint32_t key = valid ? __ldg(sk + i) : 0u;
-  const uint32_t active = __ballot_sync(0xffffffffu, valid);
-  if (!valid) return;
-  const uint32_t peers = __match_any_sync(active, key);
-  if (lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(count + key, (uint32_t)__popc(peers));
+  const uint32_t key = valid ? __ldg(sk + i) : 0xffffffffu;
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool starts = valid && (lane == 0 || key != prev);
+  const uint32_t heads = __ballot_sync(0xffffffffu, starts);
+  const uint32_t live = __ballot_sync(0xffffffffu, valid);
+  if (!starts) return;
+  const uint32_t later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
+  const uint32_t end = later ? (uint32_t)(__ffs(later) - 1) : 32u - __clz(live);
+  atomicAdd(count + key, end - lane);
 }
 
 }  // namespace
@@ -556,7 +562,8 @@ size_t sort_scratch_bytes(uint32_t n, uint64_t C) {
   size_t b = 0;
   b += 5 * align256(4ull * n);                                          // keys, ka, va, kb, vb
   b += align256(4ull * kRadixMaxPasses * kRadixMaxDigits);             // digit counts
-  b += align256(4ull * kRadixMaxPasses * radix_tiles(n) * kRadixMaxDigits);  // look-back words
+  b += align256(4ull * radix_tiles(n) * kRadixMaxDigits);                 // tile digit counts
+  b += align256(4ull * div_up(radix_tiles(n), kScanChunk) * kRadixMaxDigits);  // chunk bases
   b += align256(8ull * scan_tiles(std::max<uint64_t>(C, 1)));           // scan tile status
   b += align256(4ull * kNumCounters);                                   // counters
   return b;
@@ -576,7 +583,8 @@ void sort_scratch_carve(void* base, uint32_t n, uint64_t C, SortScratch* s) {
   s->vb = reinterpret_cast<uint32_t*>(take(4ull * n));
   s->digit_count = reinterpret_cast<uint32_t*>(take(4ull * kRadixMaxPasses * kRadixMaxDigits));
   s->tiles_cap = radix_tiles(n);
-  s->status = reinterpret_cast<uint32_t*>(take(4ull * kRadixMaxPasses * s->tiles_cap * kRadixMaxDigits));
+  s->tcount = reinterpret_cast<uint32_t*>(take(4ull * s->tiles_cap * kRadixMaxDigits));
+  s->csum = reinterpret_cast<uint32_t*>(take(4ull * div_up(s->tiles_cap, kScanChunk) * kRadixMaxDigits));
   s->scan_tiles_cap = scan_tiles(std::max<uint64_t>(C, 1));
   s->scan_status = reinterpret_cast<uint64_t*>(take(8ull * s->scan_tiles_cap));
   s->counters = reinterpret_cast<uint32_t*>(take(4ull * kNumCounters));
@@ -585,7 +593,7 @@ void sort_scratch_carve(void* base, uint32_t n, uint64_t C, SortScratch* s) {
 }
 
 cudaError_t sort_scratch_zero(const SortScratch& s, cudaStream_t st) {
-  // the look-back words, digit counts, scan status and counters
+  // the digit counts, tile counts, chunk bases, scan status and counters
   const char* a = reinterpret_cast<const char*>(s.digit_count);
   const char* b = reinterpret_cast<const char*>(s.counters) + 4ull * kNumCounters;
   return cudaMemsetAsync(const_cast<char*>(a), 0, (size_t)(b - a), st);
@@ -620,10 +628,8 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
       k_identity<<<div_up(n, 256), 256, 0, st>>>(perm, n);
     } else {
       if (cudaError_t e = radix_prepare(); e != cudaSuccess) return e;
-      if (cudaError_t e = cudaMemsetAsync(s.counters + kCounterPass0, 0, 4 * kRadixMaxPasses, st); e != cudaSuccess)
-        return e;
       k_digit_first<<<plan.passes, 1024, 0, st>>>(s.digit_count, plan.digits);
-      const size_t region = (size_t)s.tiles_cap * kRadixMaxDigits;
+      const uint32_t chunks = div_up(tiles, kScanChunk);
       const uint32_t* kin = keys;
       const uint32_t* vin = nullptr;
       for (uint32_t p = 0; p < plan.passes; ++p) {
@@ -631,22 +637,22 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
         // pass outputs: 0 -> (ka, va), 1 -> (kb, vb), the last -> (sorted keys, perm)
         uint32_t* kout = last ? (p == 2 ? s.ka : s.kb) : (p == 0 ? s.ka : s.kb);
         uint32_t* vout = last ? perm : (p == 0 ? s.va : s.vb);
-        uint32_t* clear = plan.passes >= 2 ? s.status + ((p + 1) % plan.passes) * region : nullptr;
+        const uint32_t shift = p * plan.width;
+        k_tile_counts<<<tiles, kOsThreads, 0, st>>>(kin, n, shift, plan.digits, s.tcount);
+        k_tile_scan_chunk<<<dim3(chunks, div_up(plan.digits, 256)), 256, 0, st>>>(s.tcount, tiles, plan.digits,
+                                                                                   s.csum);
+        k_tile_scan_chunks<<<div_up(plan.digits, 256), 256, 0, st>>>(s.csum, chunks, plan.digits,
+                                                                   s.digit_count + p * kRadixMaxDigits);
         if (p == 0)
-          k_radix_pass<true><<<tiles, kOsThreads, kOsSmemBytes, st>>>(
-              kin, vin, n, kout, vout, p * plan.width, plan.digits, s.digit_count + p * kRadixMaxDigits,
-              s.status + p * region, clear, s.counters + kCounterPass0 + p, s.counters + kCounterError);
+          k_radix_scatter<true><<<tiles, kOsThreads, kOsSmemBytes, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
+                                                                        s.tcount, s.csum);
         else
-          k_radix_pass<false><<<tiles, kOsThreads, kOsSmemBytes, st>>>(
-              kin, vin, n, kout, vout, p * plan.width, plan.digits, s.digit_count + p * kRadixMaxDigits,
-              s.status + p * region, clear, s.counters + kCounterPass0 + p, s.counters + kCounterError);
+          k_radix_scatter<false><<<tiles, kOsThreads, kOsSmemBytes, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
+                                                                         s.tcount, s.csum);
         kin = kout;
         vin = vout;
       }
       sorted = kin;
-      // one pass: nothing clears its look-back words for the next call
-      if (plan.passes == 1)
-        if (cudaError_t e = cudaMemsetAsync(s.status, 0, 4ull * tiles * kRadixMaxDigits, st); e != cudaSuccess) return e;
     }
     k_run_counts<<<div_up(n, 256), 256, 0, st>>>(sorted, n, count);
   }
@@ -661,11 +667,11 @@ cudaError_t radix_prepare() {
   if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
   std::lock_guard<std::mutex> g(m);
   if (ready.count(dev)) return cudaSuccess;
-  if (cudaError_t e = cudaFuncSetAttribute(k_radix_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaError_t e = cudaFuncSetAttribute(k_radix_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kOsSmemBytes);
       e != cudaSuccess)
     return e;
-  if (cudaError_t e = cudaFuncSetAttribute(k_radix_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaError_t e = cudaFuncSetAttribute(k_radix_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kOsSmemBytes);
       e != cudaSuccess)
     return e;

@@ -6,12 +6,12 @@
 //                histograms flushed once per block
 //   digit scan   the counts of each pass turned into each digit's first
 //                output position
-//   passes       one LSD radix pass per 11 (or fewer) key bits: each tile of
-//                4096 elements ranks its elements by digit in element order
-//                (warp-aggregated with __match_any_sync), publishes its digit
-//                counts and finds its digit offsets by a decoupled look-back
-//                over the preceding tiles (bounded spins), then writes its
-//                elements out digit run by digit run through shared memory
+//   passes       one LSD radix pass per 11 (or fewer) key bits, each three
+//                steps: every tile of 4096 elements counts its digits; the
+//                tile counts are scanned per digit over the tiles; every tile
+//                ranks its elements by digit in element order (warp-aggregated
+//                with __match_any_sync) and writes them out digit run by
+//                digit run through shared memory
 //   runs         the count of every cell from the sorted keys (one atomic per
 //                run of equal keys in a warp)
 //   scan         decoupled look-back exclusive scan counts -> start
@@ -53,8 +53,7 @@ struct RadixPlan {
 RadixPlan radix_plan(uint64_t cells);
 
 // Scratch of one sort, carved for a capacity of n_cap elements and c_cap
-// cells. The layout depends on the capacity only, so calls of any size up
-// to it find the look-back status words where earlier calls left them.
+// cells.
 struct SortScratch {
   uint32_t* keys = nullptr;      // n_cap: keys by element when the caller keeps none
   uint32_t* ka = nullptr;        // n_cap: keys after pass 0
@@ -62,14 +61,14 @@ struct SortScratch {
   uint32_t* kb = nullptr;        // n_cap: keys after pass 1 (3-pass plans), else the sorted keys
   uint32_t* vb = nullptr;        // n_cap
   uint32_t* digit_count = nullptr;  // kRadixMaxPasses x kRadixMaxDigits: counts, then first positions
-  uint32_t* status = nullptr;    // kRadixMaxPasses regions of tiles_cap x kRadixMaxDigits look-back words
+  uint32_t* tcount = nullptr;    // tiles_cap x kRadixMaxDigits: digit counts per tile, then their scan
+  uint32_t* csum = nullptr;      // tiles_cap / 32 x kRadixMaxDigits: per chunk of 32 tiles, its first positions
   uint64_t* scan_status = nullptr;  // look-back tiles of the count -> start scan
   uint32_t* counters = nullptr;  // kNumCounters words
   uint32_t n_cap = 0, c_cap = 0, tiles_cap = 0, scan_tiles_cap = 0;
 };
 
 constexpr int kCounterTicket = 0;  // scan tile ticket
-constexpr int kCounterPass0 = 1;   // radix pass tile tickets (3 words)
 constexpr int kCounterError = 4;
 constexpr int kCounterOverflow = 5;
 constexpr int kNumCounters = 8;
@@ -77,8 +76,7 @@ constexpr int kNumCounters = 8;
 // Bytes of scratch for a capacity of n elements and C cells.
 size_t sort_scratch_bytes(uint32_t n, uint64_t C);
 // Carve a scratch layout out of one device allocation of sort_scratch_bytes.
-// A fresh allocation must be zeroed once (sort_scratch_zero) before its
-// first sort: the radix passes expect their look-back words clear.
+// sort_scratch_zero clears its counters and counts (a fresh block once).
 void sort_scratch_carve(void* base, uint32_t n, uint64_t C, SortScratch* s);
 cudaError_t sort_scratch_zero(const SortScratch& s, cudaStream_t st);
 

@@ -10,7 +10,7 @@
 // fixed block of device memory that is part of the library image.
 //
 // The scratch block below is a file-scope __device__ array of
-// kNoAllocScratchBytes (27 MiB). Its size caps the problem: at most
+// kNoAllocScratchBytes (23 MiB). Its size caps the problem: at most
 // kNoAllocMaxParticles particles and kNoAllocMaxCells cells per call. The
 // CUDA runtime loads this file's device code lazily (CUDA 12 defaults to
 // lazy module loading), so the block is reserved on a device by the first
@@ -28,8 +28,7 @@
 // that device current.
 //
 // All calls share the one block and it keeps the last call's contents: each
-// call clears what must start at zero itself (the radix passes leave their
-// look-back words clear for the next call), and two calls whose GPU work
+// call clears what must start at zero itself, and two calls whose GPU work
 // overlaps (for example on two streams) race on the block and corrupt each
 // other's results. Serialise them.
 //
@@ -50,7 +49,7 @@ namespace {
 
 constexpr uint32_t kNoAllocMaxParticles = 1u << 20;  // 1,048,576
 constexpr uint64_t kNoAllocMaxCells = 1ull << 21;    // 2,097,152 (a 128^3 grid)
-constexpr size_t kNoAllocScratchBytes = 27ull << 20; // >= sort_scratch_bytes(max particles, max cells)
+constexpr size_t kNoAllocScratchBytes = 23ull << 20; // >= sort_scratch_bytes(max particles, max cells)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -103,8 +102,7 @@ extern "C" pf_status pf_sort_noalloc(const float* d_pos4, uint32_t n, const pf_g
   if (!d_start || !d_count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
 
   PF_TRY(noalloc_scratch(&base));
-  // carved for the block's limits, whatever this call's size: the look-back
-  // words stay where the previous call cleared them
+  // carved for the block's limits, whatever this call's size
   SortScratch s;
   sort_scratch_carve(base, kNoAllocMaxParticles, kNoAllocMaxCells, &s);
   cudaStream_t st = static_cast<cudaStream_t>(stream);

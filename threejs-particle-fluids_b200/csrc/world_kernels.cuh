@@ -47,6 +47,30 @@ __device__ __forceinline__ float4 with_w(f3 a, float w) { return make_float4(a.x
 __device__ __forceinline__ float dot_rn(f3 a) {
   return __fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z));
 }
+__device__ __forceinline__ float dot_rn(f3 a, f3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+
+// collider.ts:53-89, the static-friction cone of one contact: the slip's
+// tangential part and whether the particle sticks (the tangential
+// displacement fits the remaining budget mu_s * lambda_n - lambda_t). A
+// sticking particle returns to where it was, a sliding one keeps its slip, so
+// the decision is a step: it is formed with separately rounded products and
+// sums, as the reference's arithmetic rounds them.
+struct StickTest {
+  f3 tang;
+  float tl;
+  bool sticks;
+};
+__device__ __forceinline__ StickTest stick_test(f3 slip, f3 nrm, float w, float mu_s, float ln, float lt) {
+  const float sn = dot_rn(slip, nrm);
+  StickTest r;
+  r.tang = mk(__fsub_rn(slip.x, __fmul_rn(nrm.x, sn)), __fsub_rn(slip.y, __fmul_rn(nrm.y, sn)),
+              __fsub_rn(slip.z, __fmul_rn(nrm.z, sn)));
+  r.tl = __fsqrt_rn(dot_rn(r.tang));
+  r.sticks = r.tl > 1e-10f && (__fdiv_rn(r.tl, w) <= __fsub_rn(__fmul_rn(mu_s, ln), lt));
+  return r;
+}
 
 // ------------------------------------------------------------ SPH kernels ----
 // sph/kernels.ts:254-298
@@ -242,7 +266,7 @@ __device__ __forceinline__ void prim_sdf(const pf_primitive& p, f3 xw, float rew
     const f3 d0 = mk(p.data0[0], p.data0[1], p.data0[2]);
     const f3 d1 = mk(p.data1[0], p.data1[1], p.data1[2]);
     const f3 x = d1 + ((xw + mk(p.velocity[0], p.velocity[1], p.velocity[2]) * 0.0f) - d1);
-    const float phi = dot(d0, x - d1);
+    const float phi = dot_rn(d0, x - d1);
     const bool inv = (p.flags & PF_PRIM_INVERT) != 0;
     *phi_out = inv ? -phi : phi;
     *grad_out = inv ? neg(d0) : d0;
@@ -511,7 +535,7 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
       const float4 b = __ldg(V.plane4 + 2 * ((size_t)S.prim_base + p) + 1);
       const f3 d0 = xyz(a), d1 = xyz(b);
       const f3 x = d1 + (xstar - d1);
-      const float ph = dot(d0, x - d1);
+      const float ph = dot_rn(d0, x - d1);
       const bool inv = a.w != 0.0f;
       phi = inv ? -ph : ph;
       nrm = inv ? neg(d0) : d0;
@@ -525,11 +549,11 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     float2 lam = lam_at(p);
     const float ln = lam.x + depth / w;
     const f3 slip = disp() - coldisp;
-    const f3 tang = slip - nrm * dot(slip, nrm);
-    const float tl = len(tang);
-    const bool sticks = tl > 1e-10f && (tl / w <= P.data1[3] * ln - lam.y);
+    const StickTest st = stick_test(slip, nrm, w, P.data1[3], ln, lam.y);
+    const bool sticks = st.sticks;
+    const float tl = st.tl;
     const f3 push = nrm * depth;
-    const f3 c = sticks ? push - tang : push;
+    const f3 c = sticks ? push - st.tang : push;
     tx += (uint32_t)to_ticks(c.x, S.pos_scale);
     ty += (uint32_t)to_ticks(c.y, S.pos_scale);
     tz += (uint32_t)to_ticks(c.z, S.pos_scale);
@@ -553,12 +577,11 @@ __device__ __forceinline__ bool collide_particle(const WorldView& V, const DevSc
     const uint32_t li = S.prim_count + q;
     float2 lam = lam_at(li);
     const float ln = lam.x + depth / w;
-    const f3 dp = disp();
-    const f3 tang = dp - nrm * dot(dp, nrm);
-    const float tl = len(tang);
-    const bool sticks = tl > 1e-10f && (tl / w <= G.mu_s * ln - lam.y);
+    const StickTest st = stick_test(disp(), nrm, w, G.mu_s, ln, lam.y);
+    const bool sticks = st.sticks;
+    const float tl = st.tl;
     const f3 push = nrm * depth;
-    const f3 c = sticks ? push - tang : push;
+    const f3 c = sticks ? push - st.tang : push;
     tx += (uint32_t)to_ticks(c.x, S.pos_scale);
     ty += (uint32_t)to_ticks(c.y, S.pos_scale);
     tz += (uint32_t)to_ticks(c.z, S.pos_scale);
