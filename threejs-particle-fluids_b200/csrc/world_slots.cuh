@@ -378,7 +378,7 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
 
 // lambda.ts:41-71
 template <uint32_t kNbrUnroll>
-__global__ void k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+__global__ void __maxnreg__(kNbrUnroll == 8 ? 80 : 48) k_s_lambda(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= V.n_fchunk * kSegAlign) return;
   const uint32_t k = chunk_slot(V.fchunk, g);  // slots of the scenes with a fluid
