@@ -733,6 +733,16 @@ def max_over_ranks(values, device) -> list:
     return [float(v) for v in t.tolist()]
 
 
+def sum_over_ranks(value, device) -> float:
+    """The sum of a per-rank count (units every replica processed)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 # -------------------------------------------------------------- main ----
 def main() -> None:
     ap = argparse.ArgumentParser()
@@ -841,15 +851,15 @@ def main() -> None:
     else:
         res = wl.run_gpu(args.steps, warmup, rank, world, barrier)
     ms = res["ms"]
+    units = res["units_per_step"]  # this rank's; replicas step different scenes
     if world > 1:
-        import torch.distributed as dist
-
         ms, e2e_ms = max_over_ranks([ms, res["e2e_ms"]], "cuda")
+        units = sum_over_ranks(units, "cuda")
     else:
         e2e_ms = res["e2e_ms"]
     peak, peak_kind = hbm_peak()
     achieved = res["algorithmic_bytes"] / (res["kernel_ms"] * 1e-3) / 1e9
-    value = res["units_per_step"] * world / (ms * 1e-3)
+    value = units / (ms * 1e-3)
     line = {
         "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
         "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -858,7 +868,7 @@ def main() -> None:
         "roofline": {"bound": "hbm", "kernel": res["kernel_name"], "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": res.get("traffic")},
-        "e2e": {"value": res["units_per_step"] * world / (e2e_ms * 1e-3), "unit": wl.unit,
+        "e2e": {"value": units / (e2e_ms * 1e-3), "unit": wl.unit,
                 "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": res["gpu_launches_per_step"] * args.steps,
         "clocks": res["clocks"],

@@ -29,10 +29,14 @@ def _rank(rank: int, world: int, port: int, out):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         ms = bench.max_over_ranks([10.0 + rank, 5.0 - rank], "cpu")
-        names = [r.name for r in W.batch_stream(6, seed=bench.replica_seed(rank))]
+        recipes = W.batch_stream(6, seed=bench.replica_seed(rank))
+        names = [r.name for r in recipes]
         gathered = [None] * world
         dist.all_gather_object(gathered, names)
-        out.put((rank, ms, gathered))
+        # the job's units are every replica's own (its scenes differ)
+        mine = sum(r.particle_substeps for r in recipes)
+        total = bench.sum_over_ranks(mine, "cpu")
+        out.put((rank, ms, gathered, mine, total))
     finally:
         dist.destroy_process_group()
 
@@ -48,6 +52,8 @@ def test_two_replicas_over_gloo():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, ms, gathered in res:
+    mine = {rank: m for rank, _, _, m, _ in res}
+    for rank, ms, gathered, _, total in res:
         assert ms == [11.0, 5.0]  # max over ranks, element-wise
         assert gathered[0] != gathered[1]  # each rank its own scenes
+        assert total == mine[0] + mine[1]
