@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <set>
 
 #include "world.cuh"
 #include "world_kernels.cuh"
@@ -1022,6 +1024,41 @@ void launch_slots(K kernel, uint32_t n, cudaStream_t st, A... args) {
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// The slot neighbour passes use no shared memory and gather their
+// neighbours' records through L1: each asks for the largest L1 (a hint the
+// runtime may round), once per device, outside any stream capture.
+template <typename K>
+cudaError_t prefer_l1(K kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxL1);
+}
+template <uint32_t U>
+cudaError_t prefer_l1_depth() {
+  cudaError_t e = cudaSuccess;
+  auto on = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  on(prefer_l1(k_s_neighbors<U, false, false>));
+  on(prefer_l1(k_s_neighbors<U, true, false>));
+  on(prefer_l1(k_s_neighbors<U, false, true>));
+  on(prefer_l1(k_s_neighbors<U, true, true>));
+  on(prefer_l1(k_s_lambda<U>));
+  on(prefer_l1(k_s_delta<U, false>));
+  on(prefer_l1(k_s_delta<U, true>));
+  on(prefer_l1(k_s_xsph<U, false>));
+  on(prefer_l1(k_s_xsph<U, true>));
+  return e;
+}
+cudaError_t slot_kernels_prepare() {
+  static std::mutex m;
+  static std::set<int> ready;
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(m);
+  if (ready.count(dev)) return cudaSuccess;
+  for (cudaError_t e : {prefer_l1_depth<2>(), prefer_l1_depth<4>(), prefer_l1_depth<8>()})
+    if (e != cudaSuccess) return e;
+  ready.insert(dev);
+  return cudaSuccess;
+}
+
 }  // namespace
 
 // ================================================================ World ====
@@ -1884,6 +1921,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   PF_CUDA(cudaMemsetAsync(arena_, 0, probe.off, stream_));
   PF_CUDA(sort_scratch_zero(sort_, stream_));
   PF_CUDA(radix_prepare());  // before any graph capture
+  PF_CUDA(slot_kernels_prepare());
   PF_TRY(up(base_.scenes_rw, h_scenes_.data(), sizeof(DevScene) * K));
   {
     // empty cell bounds: the predict pass narrows them (a pageable source:
