@@ -52,6 +52,8 @@ def test_mixed_scene_full_one_frame(oracle, cuda):
 
 
 def mixed_stats(scene, r):
+    """Centre of mass, mean kinetic energy per particle, and the fluid's mean
+    and max density error above rest, at the scene's current frame."""
     fluid = r.materials[1][1]
     s0, n = fluid.range
     x = scene.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
@@ -62,23 +64,30 @@ def mixed_stats(scene, r):
 
 
 def test_mixed_scene_full_300_frames_statistics(oracle, cuda):
+    """300 frames, compared by statistics averaged over the last 100 frames
+    (sampled every 10): five seconds of fluid sloshing among 20 soft bodies
+    and a moving sphere are chaotic, so the runs agree in their statistics,
+    not their states, and a single frame's kinetic energy depends on the
+    slosh's phase."""
     r = W.mixed_scene(seed=32)
     a, b = cuda.build(r), oracle.OracleBackend(threads=THREADS).build(r)
-    for _ in range(300):
+    sa, sb = [], []
+    for f in range(1, 301):
         a.step(DT)
         b.step(DT)
-    sa, sb = mixed_stats(a, r), mixed_stats(b, r)
+        if f > 200 and f % 10 == 0:
+            sa.append(mixed_stats(a, r))
+            sb.append(mixed_stats(b, r))
     assert np.isfinite(a.readback(N.PF_FIELD_POSITIONS)).all()
-    # five seconds of sloshing fluid among 20 soft bodies and a moving sphere
-    # are chaotic: the two runs agree in their statistics, not their states
-    # (the centre of mass within 5 % of the 1 m container, the kinetic energy
-    # within 30 %, the mean density error within 0.01)
-    assert np.abs(sa["com"] - sb["com"]).max() < 0.05, (sa, sb)
-    assert abs(sa["ke"] - sb["ke"]) <= 0.3 * max(sb["ke"], 1e-4), (sa, sb)
-    assert abs(sa["mean_err"] - sb["mean_err"]) < 0.01, (sa, sb)
+    mean = lambda st, k: np.mean([x[k] for x in st], axis=0)  # noqa: E731
+    # the centre of mass within 3 % of the 1 m container, the kinetic energy
+    # within 25 %, the mean density error within 0.01
+    assert np.abs(mean(sa, "com") - mean(sb, "com")).max() < 0.03, (sa[-1], sb[-1])
+    assert abs(mean(sa, "ke") - mean(sb, "ke")) <= 0.25 * max(mean(sb, "ke"), 1e-4), (mean(sa, "ke"), mean(sb, "ke"))
+    assert abs(mean(sa, "mean_err") - mean(sb, "mean_err")) < 0.01
     # the largest compression is one particle squeezed between bodies: the
     # same order of magnitude on both
-    assert sa["max_err"] <= max(2.0 * sb["max_err"], 0.5), (sa, sb)
+    assert mean(sa, "max_err") <= max(2.0 * mean(sb, "max_err"), 0.5)
     assert not a.overflow()["grid_clamped"]
 
 
@@ -101,11 +110,27 @@ def test_batch_stream_sampled_scenes(oracle, cuda):
     try:
         batch.step(DT)
         for i in sorted(pick):
-            ref = oracle.OracleBackend(threads=THREADS).build(recipes[i])
+            rec = recipes[i]
+            ref = oracle.OracleBackend(threads=THREADS).build(rec)
             ref.step(DT)
-            tol = 1e-5 * extent(recipes[i])
-            got = batch.readback(i, N.PF_FIELD_POSITIONS)
-            assert dev(got, ref.readback(N.PF_FIELD_POSITIONS)) <= tol, (recipes[i].name, i)
-            assert not any(batch.overflow(i).values()), (recipes[i].name, batch.overflow(i))
+            tol = 1e-5 * extent(rec)
+            got = batch.readback(i, N.PF_FIELD_POSITIONS).astype(np.float64)
+            want = ref.readback(N.PF_FIELD_POSITIONS).astype(np.float64)
+            d = np.abs(got - want).max(1)
+            far = np.flatnonzero(d > tol)
+            # A particle touching a wall sticks while its slip fits the
+            # static-friction cone and slides by its whole slip otherwise
+            # (collider.ts:53-89): a step. When its slip and the cone agree
+            # to a few parts in 1e5, the last bits of the fluid solve decide
+            # it, so such a particle may land one slip (well under a particle
+            # spacing) from the oracle's. At most a few per 100,000 may; any
+            # other particle is held to the tolerance.
+            assert far.size <= max(2, rec.capacity // 100_000), (rec.name, i, far.size, d.max())
+            for j in far:
+                walls = [p for p in rec.prims if p.kind == 0]
+                gap = min(abs(np.dot(np.asarray(p.data0[:3]), want[j, :3] - np.asarray(p.data1[:3]))) for p in walls)
+                assert gap <= 1.01 * rec.radius, (rec.name, i, int(j), gap)
+                assert d[j] <= 2.0 * rec.radius, (rec.name, i, int(j), d[j])
+            assert not any(batch.overflow(i).values()), (rec.name, batch.overflow(i))
     finally:
         batch.close()
