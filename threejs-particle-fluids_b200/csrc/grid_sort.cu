@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <set>
 #include <string>
@@ -46,7 +47,6 @@ constexpr uint32_t kOsItems = 16;
 constexpr uint32_t kOsWarps = kOsThreads / 32;
 constexpr uint32_t kOsStripe = kOsItems * 32;
 static_assert(kOsThreads * kOsItems == kRadixTile, "tile size");
-constexpr uint32_t kOsPer = kRadixMaxDigits / kOsThreads;  // digits per thread in the look-back
 // shared memory of a pass, in words: warp histograms (u16) or the staged
 // tile (keys then element indices), then each digit's first tile position
 // and first output position
@@ -537,11 +537,21 @@ pf_status validate_sort(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_
   return PF_OK;
 }
 
+uint32_t radix_digit_bits() {
+  static const uint32_t b = [] {
+    const char* e = std::getenv("PFSIM_RADIX_BITS");
+    const int v = e ? std::atoi(e) : 8;
+    return (uint32_t)std::min(std::max(v, 4), (int)kRadixMaxBits);
+  }();
+  return b;
+}
+
 RadixPlan radix_plan(uint64_t cells) {
   uint32_t bits = 0;
   while (bits < 40 && (1ull << bits) < cells) ++bits;
+  const uint32_t dbits = radix_digit_bits();
   RadixPlan p;
-  p.passes = (bits + kRadixMaxBits - 1) / kRadixMaxBits;
+  p.passes = (bits + dbits - 1) / dbits;
   p.width = p.passes ? (bits + p.passes - 1) / p.passes : 0;
   p.digits = 1u << p.width;
   return p;
@@ -634,9 +644,12 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
       const uint32_t* vin = nullptr;
       for (uint32_t p = 0; p < plan.passes; ++p) {
         const bool last = p + 1 == plan.passes;
-        // pass outputs: 0 -> (ka, va), 1 -> (kb, vb), the last -> (sorted keys, perm)
-        uint32_t* kout = last ? (p == 2 ? s.ka : s.kb) : (p == 0 ? s.ka : s.kb);
-        uint32_t* vout = last ? perm : (p == 0 ? s.va : s.vb);
+        // pass outputs: even passes -> (ka, va), odd -> (kb, vb); the last
+        // writes perm and the sorted keys into whichever of ka, kb it does
+        // not read
+        uint32_t* kout = last ? (kin == s.ka ? s.kb : s.ka) : ((p & 1u) ? s.kb : s.ka);
+        if (last && plan.passes == 1) kout = s.kb;
+        uint32_t* vout = last ? perm : ((p & 1u) ? s.vb : s.va);
         const uint32_t shift = p * plan.width;
         k_tile_counts<<<tiles, kOsThreads, 0, st>>>(kin, n, shift, plan.digits, s.tcount);
         k_tile_scan_chunk<<<dim3(chunks, div_up(plan.digits, 256)), 256, 0, st>>>(s.tcount, tiles, plan.digits,

@@ -42,11 +42,13 @@ bool make_key_fn(const pf_grid_desc& g, KeyFn* out, uint64_t* cells);
 // resolves its key function; the reference's error text on failure.
 pf_status validate_sort(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_t* cells);
 
-// Radix plan for keys in [0, C): `passes` LSD passes of `width` bits.
+// Radix plan for keys in [0, C): `passes` LSD passes of `width` bits, at
+// most radix_digit_bits() bits each (8 unless PFSIM_RADIX_BITS sets 4 to 11).
 constexpr uint32_t kRadixMaxBits = 11;
 constexpr uint32_t kRadixMaxDigits = 1u << kRadixMaxBits;  // 2048
-constexpr uint32_t kRadixMaxPasses = 3;                     // 33 bits >= any key below 2^31
+constexpr uint32_t kRadixMaxPasses = 4;                     // 32 bits of 8 >= any key below 2^31
 constexpr uint32_t kRadixTile = 4096;                       // elements per tile (256 threads x 16)
+uint32_t radix_digit_bits();
 struct RadixPlan {
   uint32_t passes = 0, width = 0, digits = 1;
 };
@@ -58,7 +60,7 @@ struct SortScratch {
   uint32_t* keys = nullptr;      // n_cap: keys by element when the caller keeps none
   uint32_t* ka = nullptr;        // n_cap: keys after pass 0
   uint32_t* va = nullptr;        // n_cap: element indices after pass 0
-  uint32_t* kb = nullptr;        // n_cap: keys after pass 1 (3-pass plans), else the sorted keys
+  uint32_t* kb = nullptr;        // n_cap: keys after odd passes, or the sorted keys
   uint32_t* vb = nullptr;        // n_cap
   uint32_t* digit_count = nullptr;  // kRadixMaxPasses x kRadixMaxDigits: counts, then first positions
   uint32_t* tcount = nullptr;    // tiles_cap x kRadixMaxDigits: digit counts per tile, then their scan
