@@ -42,17 +42,21 @@ constexpr uint32_t kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096
 // radix passes: 256 threads x 16 elements per tile, elements warp-striped
 // (warp w ranks elements [512 w, 512 w + 512) of its tile, 32 per round)
-constexpr uint32_t kOsThreads = 256;
-constexpr uint32_t kOsItems = 16;
+constexpr uint32_t kOsThreads = 512;
+constexpr uint32_t kOsItems = 8;
 constexpr uint32_t kOsWarps = kOsThreads / 32;
 constexpr uint32_t kOsStripe = kOsItems * 32;
 static_assert(kOsThreads * kOsItems == kRadixTile, "tile size");
-// shared memory of a pass, in words: warp histograms (u16) or the staged
-// tile (keys then element indices), then each digit's first tile position
-// and first output position
-constexpr uint32_t kOsStageWords = 2 * kRadixTile;
-static_assert(kOsWarps * kRadixMaxDigits / 2 <= kOsStageWords, "histograms fit the staging area");
-constexpr size_t kOsSmemBytes = 4ull * (kOsStageWords + 2 * kRadixMaxDigits);
+// shared memory of a scatter, in words: the warp histograms (u16) or the
+// staged tile (keys then element indices), whichever is larger, then each
+// digit's first tile position and first output position
+__host__ __device__ constexpr uint32_t scatter_stage_words(uint32_t digits) {
+  return 2 * kRadixTile > kOsWarps * digits / 2 ? 2 * kRadixTile : kOsWarps * digits / 2;
+}
+__host__ __device__ constexpr size_t scatter_smem_bytes(uint32_t digits) {
+  return 4ull * (scatter_stage_words(digits) + 2ull * digits);
+}
+constexpr size_t kOsSmemBytes = scatter_smem_bytes(kRadixMaxDigits);  // the largest
 constexpr uint32_t kMortonBias = 512;
 constexpr int32_t kCellCoordMax = 1 << 30;
 
@@ -363,8 +367,8 @@ k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ v
   uint16_t* whist = reinterpret_cast<uint16_t*>(sm);  // [warp][digit], then the staged tile
   uint32_t* stage_k = sm;
   uint32_t* stage_v = sm + kRadixTile;
-  uint32_t* lstart = sm + kOsStageWords;        // first tile position of each digit
-  uint32_t* gstart = lstart + kRadixMaxDigits;  // first output position of each digit
+  uint32_t* lstart = sm + scatter_stage_words(digits);  // first tile position of each digit
+  uint32_t* gstart = lstart + digits;                    // first output position of each digit
   __shared__ uint32_t s_wsum[kOsWarps];
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   const uint32_t tile = blockIdx.x;
@@ -657,10 +661,10 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
         k_tile_scan_chunks<<<div_up(plan.digits, 256), 256, 0, st>>>(s.csum, chunks, plan.digits,
                                                                    s.digit_count + p * kRadixMaxDigits);
         if (p == 0)
-          k_radix_scatter<true><<<tiles, kOsThreads, kOsSmemBytes, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
+          k_radix_scatter<true><<<tiles, kOsThreads, scatter_smem_bytes(plan.digits), st>>>(kin, vin, n, kout, vout, shift, plan.digits,
                                                                         s.tcount, s.csum);
         else
-          k_radix_scatter<false><<<tiles, kOsThreads, kOsSmemBytes, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
+          k_radix_scatter<false><<<tiles, kOsThreads, scatter_smem_bytes(plan.digits), st>>>(kin, vin, n, kout, vout, shift, plan.digits,
                                                                          s.tcount, s.csum);
         kin = kout;
         vin = vout;
