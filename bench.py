@@ -252,10 +252,14 @@ class BatchWorkload:
               2: ("position correction + apply", 36), 3: ("XSPH", 48)}
     # DRAM bytes per fluid particle of one launch of a stage, from a one-pass
     # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of that
-    # stage's pf_batch_profile_stage launch on this workload at the frame the
-    # bench profiles it (after 3 warm-up and 20 timed frames); the command
-    # and the figures are in profiles/batch256_stage_traffic.md
-    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {}
+    # stage's pf_batch_profile_stage launches on this workload at the frame the
+    # bench profiles it (after 3 warm-up and 20 timed frames; mean of 11
+    # launches, 9,441,833 fluid particles), taken with
+    #   ncu --nvtx --nvtx-include "stage_profile/" --metrics dram__bytes_read.sum,
+    #       dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
+    #       -k regex:k_s_ -c 44 --csv python bench.py --steps 20 --warmup 3
+    #       --no-cpu-baseline --no-plain --no-serve
+    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {0: 158.9, 1: 123.3, 2: 164.9, 3: 136.0}
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -382,7 +386,8 @@ class BatchWorkload:
             table[label] = {"ms_per_launch": stages[sid], "launches_per_step": per_step[sid],
                             "ms_per_step": stages[sid] * per_step[sid],
                             "share_of_step": stages[sid] * per_step[sid] / ms,
-                            "bytes_per_fluid_particle": bpp, "achieved_gbs": gbs, "frac": gbs / peak}
+                            "bytes_per_fluid_particle": bpp, "achieved_gbs": gbs, "frac": gbs / peak,
+                            "dram_bytes_per_fluid_particle": self.STAGE_TRAFFIC_PER_PARTICLE.get(sid)}
         dom = max(self.STAGES, key=lambda sid: stages[sid] * per_step[sid])
         tpp = self.STAGE_TRAFFIC_PER_PARTICLE.get(dom)
         return {

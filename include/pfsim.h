@@ -95,6 +95,9 @@ PF_API uint64_t pf_grid_cells(const pf_grid_desc* grid);
  *   d_overflow device, 1 entry or NULL: 1 if a cell coordinate left the
  *             Morton range or was clamped (HashGrid.overflowFlag)
  *   stream    cudaStream_t or NULL for the legacy default stream
+ * d_pos4 must be 16-byte aligned (float4 elements); the other buffers need
+ * 4-byte alignment. Missing or misaligned buffers return PF_ERR_INVALID
+ * before any device work.
  * Scratch memory comes from a per-device workspace owned by the library.
  */
 PF_API pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* grid,

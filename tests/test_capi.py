@@ -81,3 +81,27 @@ def test_api_validation_is_host_side():
         A.SoftbodySystem(A.ParticleSystem(4, 0.01), [], shape_matching="x")
     with pytest.raises(N.PfError, match="SDFCollider: resolution"):
         A.SDFCollider(A.ParticleSystem(4, 0.01), np.zeros((2, 4, 4)), (0, 0, 0), (1, 1, 1))
+
+
+def test_sort_buffers_are_checked_before_device_work():
+    """pf_sort and pf_sort_noalloc refuse missing and misaligned device
+    buffers with an error (positions are read as float4, so they must be
+    16-byte aligned) before they touch the device. The pointers here are
+    never dereferenced."""
+    import pytest
+
+    from pfsim import hashgrid as H
+    from pfsim import workloads as W
+
+    L = N.lib()
+    g = H.GridOptions(cell_size=W.SORT_CELL, kind="linear", dims=(8, 8, 8))
+    n = 100
+    d = g.desc(n)
+    p = lambda a: C.c_void_p(a)  # noqa: E731
+    for entry in (L.pf_sort, L.pf_sort_noalloc):
+        with pytest.raises(N.PfError, match="16-byte aligned"):
+            N.check(entry(p(0x10004), n, C.byref(d), p(0x20000), p(0x30000), p(0x40000), None, None, None))
+        with pytest.raises(N.PfError, match="4-byte aligned"):
+            N.check(entry(p(0x10000), n, C.byref(d), p(0x20002), p(0x30000), p(0x40000), None, None, None))
+        with pytest.raises(N.PfError, match="NULL start or count"):
+            N.check(entry(p(0x10000), n, C.byref(d), p(0x20000), None, p(0x40000), None, None, None))

@@ -138,3 +138,43 @@ def test_sizes_shrink_and_grow(oracle, pfsim):
     for n in (300_000, 5_000, 2_000_000, 4_097, 1_000_000):
         pos = W.sort_blobs(n, 400 + n)
         assert_same(H.sort(pos, g), oracle_sort(oracle, pos, g))
+
+
+@pytest.mark.parametrize("n", [4_097, 300_001])
+def test_unaligned_caller_buffers(oracle, pfsim, n):
+    """pf_sort on caller buffers that are 4-byte but not 16-byte aligned (the
+    keys buffer is also the first radix pass's input, which is then copied
+    element by element instead of 16 bytes at a time): the same results as
+    the oracle."""
+    import ctypes as C
+
+    import torch
+
+    pos_h = W.sort_blobs(n, 500 + n)
+    g = linear_grid()
+    desc = g.desc(n)
+    cells = int(N.lib().pf_grid_cells(C.byref(desc)))
+    pos = torch.from_numpy(pos_h).cuda()
+    # each buffer one element into a larger allocation
+    perm = torch.full((n + 1,), -1, dtype=torch.int32, device="cuda")
+    keys = torch.full((n + 1,), -1, dtype=torch.int32, device="cuda")
+    start = torch.full((cells + 1,), -1, dtype=torch.int32, device="cuda")
+    count = torch.full((cells + 1,), -1, dtype=torch.int32, device="cuda")
+    ovf = torch.zeros(2, dtype=torch.int32, device="cuda")
+
+    def at1(t):
+        return C.c_void_p(t.data_ptr() + 4)
+
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    N.check(N.lib().pf_sort(C.c_void_p(pos.data_ptr()), n, C.byref(desc), at1(perm), at1(start), at1(count),
+                            at1(keys), at1(ovf), stream))
+    torch.cuda.synchronize()
+    ref = oracle_sort(oracle, pos_h, g)
+    u32 = lambda t: t.cpu().numpy().view(np.uint32)[1:]  # noqa: E731
+    assert np.array_equal(u32(keys), ref["keys"])
+    assert np.array_equal(u32(perm), ref["perm"])
+    assert np.array_equal(u32(start), ref["start"])
+    assert np.array_equal(u32(count), ref["count"])
+    assert int(u32(ovf)[0]) == int(ref["overflow"][0])
+    for t in (perm, keys, start, count):
+        assert int(t[0]) == -1  # nothing written before the buffers

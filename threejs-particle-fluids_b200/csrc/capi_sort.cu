@@ -132,8 +132,7 @@ pf_status pf_sort(const float* d_pos4, uint32_t n, const pf_grid_desc* grid, uin
   KeyFn kf;
   uint64_t C = 0;
   PF_TRY(validate_sort(n, grid, &kf, &C));
-  if (n > 0 && (!d_pos4 || !d_perm)) return fail(PF_ERR_INVALID, "HashGrid: NULL positions or perm");
-  if (!d_start || !d_count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
+  PF_TRY(validate_sort_buffers(n, d_pos4, d_perm, d_start, d_count, d_keys, d_overflow));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> g(g_ws_mutex);
   Workspace& ws = workspace_for(st);

@@ -37,26 +37,25 @@ namespace pf {
 namespace {
 
 constexpr uint32_t kHistThreads = 256;
+constexpr uint32_t kKeysUnroll = 4;
 constexpr uint32_t kScanThreads = 256;
 constexpr uint32_t kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096
-// radix passes: 256 threads x 16 elements per tile, elements warp-striped
-// (warp w ranks elements [512 w, 512 w + 512) of its tile, 32 per round)
+// radix scatter: 512 threads x 8 elements per tile, elements warp-striped
+// (warp w ranks elements [256 w, 256 w + 256) of its tile, 32 per round)
 constexpr uint32_t kOsThreads = 512;
 constexpr uint32_t kOsItems = 8;
 constexpr uint32_t kOsWarps = kOsThreads / 32;
 constexpr uint32_t kOsStripe = kOsItems * 32;
 static_assert(kOsThreads * kOsItems == kRadixTile, "tile size");
-// shared memory of a scatter, in words: the warp histograms (u16) or the
-// staged tile (keys then element indices), whichever is larger, then each
-// digit's first tile position and first output position
-__host__ __device__ constexpr uint32_t scatter_stage_words(uint32_t digits) {
-  return 2 * kRadixTile > kOsWarps * digits / 2 ? 2 * kRadixTile : kOsWarps * digits / 2;
+// shared memory of a scatter, in words: two tile buffers of keys (and two of
+// values unless the values are the element indices); the staged tile (keys
+// then values); the warp histograms (u16); each digit's first tile position
+// and first output position
+__host__ __device__ constexpr size_t scatter_smem_bytes(uint32_t digits, bool first) {
+  return 4ull * ((first ? 2ull : 4ull) * kRadixTile + 2ull * kRadixTile + kOsWarps * digits / 2 + 2ull * digits);
 }
-__host__ __device__ constexpr size_t scatter_smem_bytes(uint32_t digits) {
-  return 4ull * (scatter_stage_words(digits) + 2ull * digits);
-}
-constexpr size_t kOsSmemBytes = scatter_smem_bytes(kRadixMaxDigits);  // the largest
+constexpr size_t kOsSmemBytes = scatter_smem_bytes(kRadixMaxDigits, false);  // the largest
 constexpr uint32_t kMortonBias = 512;
 constexpr int32_t kCellCoordMax = 1 << 30;
 
@@ -122,7 +121,7 @@ __device__ __forceinline__ void store_status(uint64_t* p, uint64_t v) {
 
 __global__ void __launch_bounds__(kScanThreads)
 k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t* __restrict__ zero_out,
-       uint64_t n, uint64_t* __restrict__ status, uint32_t* __restrict__ counters) {
+       uint64_t n, uint64_t* __restrict__ status, uint32_t* __restrict__ counters, uint32_t vec) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_prefix;
@@ -131,7 +130,8 @@ k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t* __
   const uint32_t tile = s_tile;
   const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
-  const bool full = base + kScanItems <= n;
+  // 16-byte loads and stores when every array is 16-byte aligned
+  const bool full = vec && base + kScanItems <= n;
   if (full) {
     const uint4* src = reinterpret_cast<const uint4*>(in + base);
 #pragma unroll
@@ -244,13 +244,23 @@ k_keys_digits(const float4* __restrict__ pos, uint32_t n, KeyFn kf, DigitHist h,
   digit_hist_zero(sh, h);
   __syncthreads();
   uint32_t over_any = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float4 p = __ldg(pos + i);
-    uint32_t over = 0;
-    const uint32_t key = cell_key(kf, p.x, p.y, p.z, &over);
-    keys[i] = key;
-    over_any |= over;
-    digit_hist_add(sh, h, key);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // kKeysUnroll positions in flight per thread before their keys
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kKeysUnroll * stride) {
+    float4 p[kKeysUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kKeysUnroll; ++q)
+      if (i0 + q * stride < n) p[q] = __ldg(pos + i0 + q * stride);
+#pragma unroll
+    for (uint32_t q = 0; q < kKeysUnroll; ++q) {
+      const uint32_t i = i0 + q * stride;
+      if (i >= n) break;
+      uint32_t over = 0;
+      const uint32_t key = cell_key(kf, p[q].x, p[q].y, p[q].z, &over);
+      keys[i] = key;
+      over_any |= over;
+      digit_hist_add(sh, h, key);
+    }
   }
   if (__any_sync(0xffffffffu, over_any) && lane_id() == 0) atomicOr(overflow, 1u);
   __syncthreads();
@@ -289,24 +299,42 @@ __global__ void __launch_bounds__(1024) k_digit_first(uint32_t* __restrict__ dc,
 // order and writes them out digit run by digit run (k_radix_scatter). No
 // kernel waits on another block.
 constexpr uint32_t kScanChunk = 32;  // tiles per chunk of the tile-count scan
+constexpr uint32_t kCountThreads = 256;
+constexpr uint32_t kCountItems = kRadixTile / kCountThreads;  // 16: four 16-byte loads
+static_assert(kCountItems % 4 == 0, "tile count loads");
 
 // Digit counts of tile blockIdx.x: row tile of `tcount` (digits entries).
-__global__ void __launch_bounds__(kOsThreads)
+// `vec`: kin is 16-byte aligned (whole tiles load four keys at a time).
+__global__ void __launch_bounds__(kCountThreads)
 k_tile_counts(const uint32_t* __restrict__ kin, uint32_t n, uint32_t shift, uint32_t digits,
-              uint32_t* __restrict__ tcount) {
+              uint32_t* __restrict__ tcount, uint32_t vec) {
   __shared__ uint32_t h[kRadixMaxDigits];
-  for (uint32_t d = threadIdx.x; d < digits; d += kOsThreads) h[d] = 0u;
+  for (uint32_t d = threadIdx.x; d < digits; d += kCountThreads) h[d] = 0u;
   __syncthreads();
   const uint32_t mask = digits - 1u;
   const size_t base = (size_t)blockIdx.x * kRadixTile;
+  if (vec && base + kRadixTile <= n) {
+    const uint4* src = reinterpret_cast<const uint4*>(kin + base);
+    uint4 v[kCountItems / 4];
+#pragma unroll
+    for (uint32_t q = 0; q < kCountItems / 4; ++q) v[q] = __ldg(src + threadIdx.x + q * kCountThreads);
+#pragma unroll
+    for (uint32_t q = 0; q < kCountItems / 4; ++q) {
+      atomicAdd(h + ((v[q].x >> shift) & mask), 1u);
+      atomicAdd(h + ((v[q].y >> shift) & mask), 1u);
+      atomicAdd(h + ((v[q].z >> shift) & mask), 1u);
+      atomicAdd(h + ((v[q].w >> shift) & mask), 1u);
+    }
+  } else {
 #pragma unroll 4
-  for (uint32_t i = threadIdx.x; i < kRadixTile; i += kOsThreads) {
-    const size_t e = base + i;
-    if (e < n) atomicAdd(h + ((__ldg(kin + e) >> shift) & mask), 1u);
+    for (uint32_t i = threadIdx.x; i < kRadixTile; i += kCountThreads) {
+      const size_t e = base + i;
+      if (e < n) atomicAdd(h + ((__ldg(kin + e) >> shift) & mask), 1u);
+    }
   }
   __syncthreads();
   uint32_t* row = tcount + (size_t)blockIdx.x * digits;
-  for (uint32_t d = threadIdx.x; d < digits; d += kOsThreads) row[d] = h[d];
+  for (uint32_t d = threadIdx.x; d < digits; d += kCountThreads) row[d] = h[d];
 }
 
 // Per digit (one thread each), the exclusive running sum over the tiles of
@@ -328,146 +356,234 @@ k_tile_scan_chunk(uint32_t* __restrict__ tcount, uint32_t tiles, uint32_t digits
   csum[(size_t)blockIdx.x * digits + d] = run;
 }
 
-// Per digit, the chunk totals -> each chunk's first output position
-// (the digit's first position plus the counts of the chunks before), in place.
+// Per digit (one warp each, 32 chunks per round), the chunk totals -> each
+// chunk's first output position (the digit's first position plus the counts
+// of the chunks before), in place.
 __global__ void __launch_bounds__(256)
 k_tile_scan_chunks(uint32_t* __restrict__ csum, uint32_t chunks, uint32_t digits, const uint32_t* __restrict__ first) {
-  const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= digits) return;
+  const uint32_t d = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const uint32_t lane = lane_id();
+  if (d >= digits) return;  // whole warps
   uint32_t run = first[d];
-  uint32_t c = 0;
-  for (; c + 8 <= chunks; c += 8) {
-    uint32_t v[8];
-#pragma unroll
-    for (uint32_t q = 0; q < 8; ++q) v[q] = csum[(size_t)(c + q) * digits + d];
-#pragma unroll
-    for (uint32_t q = 0; q < 8; ++q) {
-      csum[(size_t)(c + q) * digits + d] = run;
-      run += v[q];
-    }
-  }
-  for (; c < chunks; ++c) {
-    const uint32_t v = csum[(size_t)c * digits + d];
-    csum[(size_t)c * digits + d] = run;
-    run += v;
-  }
-}
-
-// The scatter of one stable LSD pass: tile blockIdx.x ranks its elements by
-// digit in element order, stages them in digit order in shared memory and
-// writes each digit's run to the run's first output position (the tile's
-// scanned count plus its chunk's base). kFirst: the values are the element
-// indices.
-template <bool kFirst>
-__global__ void __launch_bounds__(kOsThreads, 2)
-k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
-                uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
-                const uint32_t* __restrict__ tcount, const uint32_t* __restrict__ csum) {
-  extern __shared__ uint32_t sm[];
-  uint16_t* whist = reinterpret_cast<uint16_t*>(sm);  // [warp][digit], then the staged tile
-  uint32_t* stage_k = sm;
-  uint32_t* stage_v = sm + kRadixTile;
-  uint32_t* lstart = sm + scatter_stage_words(digits);  // first tile position of each digit
-  uint32_t* gstart = lstart + digits;                    // first output position of each digit
-  __shared__ uint32_t s_wsum[kOsWarps];
-  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  const uint32_t tile = blockIdx.x;
-  for (uint32_t w = tid; w < kOsWarps * digits / 2; w += kOsThreads) sm[w] = 0u;
-  {
-    const uint32_t* trow = tcount + (size_t)tile * digits;
-    const uint32_t* crow = csum + (size_t)(tile / kScanChunk) * digits;
-    for (uint32_t d = tid; d < digits; d += kOsThreads) gstart[d] = __ldg(trow + d) + __ldg(crow + d);
-  }
-  __syncthreads();
-  const uint32_t mask = digits - 1u;
-  const uint32_t base = tile * kRadixTile + warp * kOsStripe;
-  uint32_t key[kOsItems], val[kOsItems], pos[kOsItems];
-#pragma unroll
-  for (uint32_t i = 0; i < kOsItems; ++i) {
-    const uint32_t e = base + i * 32u + lane;
-    const bool valid = e < n;
-    key[i] = valid ? __ldg(kin + e) : 0u;
-    val[i] = kFirst ? e : (valid ? __ldg(vin + e) : 0u);
-  }
-  // rank in element order inside the warp's stripe: a round's equal digits
-  // by lane, after the counts of the warp's earlier rounds
-  uint16_t* wh = whist + warp * digits;
-#pragma unroll
-  for (uint32_t i = 0; i < kOsItems; ++i) {
-    const uint32_t e = base + i * 32u + lane;
-    const uint32_t vm = __ballot_sync(0xffffffffu, e < n);
-    pos[i] = 0;
-    if (!vm) continue;  // warp-uniform
-    const uint32_t d = (key[i] >> shift) & mask;
-    uint32_t peers = 0, old = 0;
-    if (e < n) {
-      peers = __match_any_sync(vm, d);
-      old = wh[d];
-      pos[i] = old + __popc(peers & lanemask_lt());
-    }
-    __syncwarp();
-    if (e < n && lane == (uint32_t)(__ffs(peers) - 1)) wh[d] = (uint16_t)(old + __popc(peers));
-    __syncwarp();
-  }
-  __syncthreads();
-  // per digit: the warps' counts -> exclusive offsets over warps; the tile's count
-  for (uint32_t d = tid; d < digits; d += kOsThreads) {
-    uint32_t sum = 0;
-#pragma unroll
-    for (uint32_t w = 0; w < kOsWarps; ++w) {
-      const uint32_t c = whist[w * digits + d];
-      whist[w * digits + d] = (uint16_t)sum;
-      sum += c;
-    }
-    lstart[d] = sum;
-  }
-  __syncthreads();
-  // exclusive scan of the tile's digit counts (a run of digits per thread)
-  {
-    const uint32_t per = (digits + kOsThreads - 1) / kOsThreads, d0 = tid * per;
-    uint32_t run = 0;
-    for (uint32_t q = 0; q < per; ++q)
-      if (d0 + q < digits) run += lstart[d0 + q];
-    uint32_t x = run;
+  for (uint32_t c0 = 0; c0 < chunks; c0 += 32) {
+    const uint32_t c = c0 + lane;
+    const uint32_t v = c < chunks ? csum[(size_t)c * digits + d] : 0u;
+    uint32_t x = v;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
       if (lane >= (uint32_t)off) x += y;
     }
-    if (lane == 31) s_wsum[warp] = x;
-    __syncthreads();
-    uint32_t acc = x - run;
-    for (uint32_t w = 0; w < warp; ++w) acc += s_wsum[w];
-    for (uint32_t q = 0; q < per; ++q)
-      if (d0 + q < digits) {
-        const uint32_t c = lstart[d0 + q];
-        lstart[d0 + q] = acc;
-        acc += c;
-      }
+    if (c < chunks) csum[(size_t)c * digits + d] = run + x - v;
+    run += __shfl_sync(0xffffffffu, x, 31);
   }
-  __syncthreads();
-  // tile positions, then the tile staged in digit order
+}
+
+// Asynchronous global -> shared copies (cp.async): 16 bytes with zero fill
+// past src_bytes, or one 4-byte element.
+__device__ __forceinline__ void cp_async16(uint32_t* dst, const uint32_t* src, uint32_t src_bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Copy tile `tile` of `src` (its elements below n) into dst[0, kRadixTile):
+// 16-byte copies when src is 16-byte aligned, else element by element.
+__device__ __forceinline__ void tile_fetch(uint32_t* dst, const uint32_t* __restrict__ src, uint32_t tile,
+                                           uint32_t n, bool vec) {
+  const uint32_t base = tile * kRadixTile;  // n < 2^30
+  const uint32_t valid = min(kRadixTile, n - base);
+  if (vec) {
 #pragma unroll
-  for (uint32_t i = 0; i < kOsItems; ++i) {
-    const uint32_t d = (key[i] >> shift) & mask;
-    if (base + i * 32u + lane < n) pos[i] += lstart[d] + whist[warp * digits + d];
-  }
-  __syncthreads();
-#pragma unroll
-  for (uint32_t i = 0; i < kOsItems; ++i)
-    if (base + i * 32u + lane < n) {
-      stage_k[pos[i]] = key[i];
-      stage_v[pos[i]] = val[i];
+    for (uint32_t c = threadIdx.x; c < kRadixTile / 4; c += kOsThreads) {
+      const uint32_t e = 4 * c;
+      if (e < valid) cp_async16(dst + e, src + base + e, 4 * min(4u, valid - e));
     }
-  __syncthreads();
-  // out run by run: consecutive threads write consecutive positions of a digit
-  const uint32_t tile_valid = min(kRadixTile, n - tile * kRadixTile);
-  for (uint32_t k = tid; k < tile_valid; k += kOsThreads) {
-    const uint32_t kk = stage_k[k];
-    const uint32_t d = (kk >> shift) & mask;
-    const uint32_t dst = gstart[d] + (k - lstart[d]);
-    kout[dst] = kk;
-    vout[dst] = stage_v[k];
+  } else {
+    for (uint32_t e = threadIdx.x; e < valid; e += kOsThreads) cp_async4(dst + e, src + base + e);
+  }
+}
+
+// The lanes of `active` whose digit d (of `bits` bits) equals this lane's:
+// one ballot per digit bit, each keeping the lanes that agree on that bit.
+// Called by every lane of `active` together.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t bits, uint32_t active) {
+  uint32_t m = active;
+#pragma unroll
+  for (uint32_t b = 0; b < kRadixMaxBits; ++b)
+    if (b < bits) {  // uniform over the warp
+      const bool set = (d >> b) & 1u;
+      const uint32_t v = __ballot_sync(active, set);
+      m &= set ? v : ~v;
+    }
+  return m;
+}
+
+// The scatter of one stable LSD pass, a persistent kernel: each block takes
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ... and copies the next tile's
+// keys (and values) into shared memory while it ranks the current one. A
+// tile ranks its elements by digit in element order (warp-striped rounds of
+// 32: equal digits found by digit_peers (kBallot) or __match_any_sync, ranked
+// against a per-warp digit histogram; then the warps' counts scanned per
+// digit), stages them in digit order in shared
+// memory and writes each digit's run to the run's first output position (the
+// tile's scanned count plus its chunk's base).
+// kFirst: the values are the element indices (no value input).
+// kLast: the keys are not written out; instead the staged tile, which is in
+// key order, adds the length of every run of equal keys in a warp's 32
+// entries to count[key] (the cell counts of the sort).
+template <bool kFirst, bool kLast, bool kBallot>
+__global__ void __launch_bounds__(kOsThreads, 2)
+k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
+                uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
+                const uint32_t* __restrict__ tcount, const uint32_t* __restrict__ csum,
+                uint32_t* __restrict__ count, uint32_t vec) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint32_t* in_k = sm;                                                  // [2][kRadixTile]
+  uint32_t* in_v = sm + 2 * kRadixTile;                                 // [2][kRadixTile], not with kFirst
+  uint32_t* stage_k = sm + (kFirst ? 2 : 4) * kRadixTile;                    // the tile in digit order
+  uint32_t* stage_v = stage_k + kRadixTile;
+  uint16_t* whist = reinterpret_cast<uint16_t*>(stage_v + kRadixTile);       // [warp][digit]
+  uint32_t* lstart = stage_v + kRadixTile + kOsWarps * digits / 2;           // first tile position of each digit
+  uint32_t* gstart = lstart + digits;                                        // first output position of each digit
+  __shared__ uint32_t s_wsum[kOsWarps];
+  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  const uint32_t tiles = div_up(n, kRadixTile);
+  const uint32_t mask = digits - 1u;
+  const uint32_t width = 31u - __clz(digits);
+  uint32_t tile = blockIdx.x, buf = 0;
+  if (tile < tiles) {
+    tile_fetch(in_k, kin, tile, n, vec);
+    if (!kFirst) tile_fetch(in_v, vin, tile, n, vec);
+  }
+  cp_async_commit();
+  for (; tile < tiles; tile += gridDim.x, buf ^= 1u) {
+    // the next tile's copies go out first; the buffer they fill was last
+    // read before the previous iteration's closing barrier
+    const uint32_t next = tile + gridDim.x;
+    if (next < tiles) {
+      tile_fetch(in_k + (buf ^ 1u) * kRadixTile, kin, next, n, vec);
+      if (!kFirst) tile_fetch(in_v + (buf ^ 1u) * kRadixTile, vin, next, n, vec);
+    }
+    cp_async_commit();
+    {
+      const uint32_t* trow = tcount + (size_t)tile * digits;
+      const uint32_t* crow = csum + (size_t)(tile / kScanChunk) * digits;
+      for (uint32_t d = tid; d < digits; d += kOsThreads) gstart[d] = __ldg(trow + d) + __ldg(crow + d);
+    }
+    uint32_t* wrow = reinterpret_cast<uint32_t*>(whist + warp * digits);  // digits is even
+    for (uint32_t w = lane; w < digits / 2; w += 32) wrow[w] = 0u;
+    cp_async_wait_prev();  // this thread's copies of this tile have landed
+    __syncthreads();       // and everyone's
+    const uint32_t* ik = in_k + buf * kRadixTile;
+    const uint32_t tbase = tile * kRadixTile;
+    const uint32_t valid = min(kRadixTile, n - tbase);
+    const uint32_t wbase = warp * kOsStripe;
+    // rank in element order inside the warp's stripe: a round's equal digits
+    // by lane, after the counts of the warp's earlier rounds
+    uint32_t key[kOsItems], pos[kOsItems];
+    uint16_t* wh = whist + warp * digits;
+#pragma unroll
+    for (uint32_t i = 0; i < kOsItems; ++i) {
+      const uint32_t l = wbase + i * 32u + lane;
+      const bool ok = l < valid;
+      key[i] = ok ? ik[l] : 0u;
+      const uint32_t vm = __ballot_sync(0xffffffffu, ok);
+      pos[i] = 0;
+      if (!vm) continue;  // warp-uniform
+      const uint32_t d = (key[i] >> shift) & mask;
+      uint32_t peers = 0, old = 0;
+      if (ok) {
+        peers = kBallot ? digit_peers(d, width, vm) : __match_any_sync(vm, d);
+        old = wh[d];
+        pos[i] = old + __popc(peers & lanemask_lt());
+      }
+      __syncwarp();
+      if (ok && lane == (uint32_t)(__ffs(peers) - 1)) wh[d] = (uint16_t)(old + __popc(peers));
+      __syncwarp();
+    }
+    __syncthreads();
+    // per digit: the warps' counts -> exclusive offsets over warps; the tile's count
+    for (uint32_t d = tid; d < digits; d += kOsThreads) {
+      uint32_t sum = 0;
+#pragma unroll
+      for (uint32_t w = 0; w < kOsWarps; ++w) {
+        const uint32_t c = whist[w * digits + d];
+        whist[w * digits + d] = (uint16_t)sum;
+        sum += c;
+      }
+      lstart[d] = sum;
+    }
+    __syncthreads();
+    // exclusive scan of the tile's digit counts (a run of digits per thread)
+    {
+      const uint32_t per = (digits + kOsThreads - 1) / kOsThreads, d0 = tid * per;
+      uint32_t run = 0;
+      for (uint32_t q = 0; q < per; ++q)
+        if (d0 + q < digits) run += lstart[d0 + q];
+      uint32_t x = run;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= (uint32_t)off) x += y;
+      }
+      if (lane == 31) s_wsum[warp] = x;
+      __syncthreads();
+      uint32_t acc = x - run;
+      for (uint32_t w = 0; w < warp; ++w) acc += s_wsum[w];
+      for (uint32_t q = 0; q < per; ++q)
+        if (d0 + q < digits) {
+          const uint32_t c = lstart[d0 + q];
+          lstart[d0 + q] = acc;
+          acc += c;
+        }
+    }
+    __syncthreads();
+    // tile positions, and the tile staged in digit order (the stage holds
+    // nothing else)
+    const uint32_t* iv = in_v + buf * kRadixTile;
+#pragma unroll
+    for (uint32_t i = 0; i < kOsItems; ++i) {
+      const uint32_t l = wbase + i * 32u + lane;
+      if (l < valid) {
+        const uint32_t d = (key[i] >> shift) & mask;
+        const uint32_t p = pos[i] + lstart[d] + whist[warp * digits + d];
+        stage_k[p] = key[i];
+        stage_v[p] = kFirst ? tbase + l : iv[l];
+      }
+    }
+    __syncthreads();
+    // out run by run: consecutive threads write consecutive positions of a digit
+#pragma unroll 2
+    for (uint32_t k0 = 0; k0 < valid; k0 += kOsThreads) {  // uniform over the block
+      const uint32_t k = k0 + tid;
+      const bool ok = k < valid;
+      const uint32_t kk = ok ? stage_k[k] : 0xffffffffu;
+      if (ok) {
+        const uint32_t d = (kk >> shift) & mask;
+        const uint32_t dst = gstart[d] + (k - lstart[d]);
+        if (!kLast) kout[dst] = kk;
+        vout[dst] = stage_v[k];
+      }
+      if (kLast) {
+        // one atomic per run of equal keys in the warp's 32 entries
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, kk, 1);
+        const bool starts = ok && (lane == 0 || kk != prev);
+        const uint32_t heads = __ballot_sync(0xffffffffu, starts);
+        const uint32_t live = __ballot_sync(0xffffffffu, ok);
+        if (starts) {
+          const uint32_t later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
+          const uint32_t end = later ? (uint32_t)(__ffs(later) - 1) : 32u - __clz(live);
+          atomicAdd(count + kk, end - lane);
+        }
+      }
+    }
+    __syncthreads();  // the stage, histograms and this tile's buffer are free again
   }
 }
 
@@ -538,6 +654,19 @@ pf_status validate_sort(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_
     return fail(PF_ERR_INVALID, "HashGrid: invalid grid descriptor");
   }
   if (n >= (1u << 30)) return fail(PF_ERR_INVALID, "HashGrid: too many particles (at most 2^30 - 1)");
+  return PF_OK;
+}
+
+pf_status validate_sort_buffers(uint32_t n, const void* pos4, const void* perm, const void* start, const void* count,
+                                const void* keys, const void* overflow) {
+  if (n > 0 && (!pos4 || !perm)) return fail(PF_ERR_INVALID, "HashGrid: NULL positions or perm");
+  if (!start || !count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
+  if (reinterpret_cast<uintptr_t>(pos4) & 15u)
+    return fail(PF_ERR_INVALID, "HashGrid: positions must be 16-byte aligned (float4 elements)");
+  const uintptr_t words = reinterpret_cast<uintptr_t>(perm) | reinterpret_cast<uintptr_t>(start) |
+                          reinterpret_cast<uintptr_t>(count) | reinterpret_cast<uintptr_t>(keys) |
+                          reinterpret_cast<uintptr_t>(overflow);
+  if (words & 3u) return fail(PF_ERR_INVALID, "HashGrid: perm, start, count, keys and overflow must be 4-byte aligned");
   return PF_OK;
 }
 
@@ -627,8 +756,64 @@ cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* z
   const uint32_t tiles = scan_tiles(n);
   if (cudaError_t e = cudaMemsetAsync(tile_status, 0, 8ull * tiles, st); e != cudaSuccess) return e;
   if (cudaError_t e = cudaMemsetAsync(counters + kCounterTicket, 0, 4, st); e != cudaSuccess) return e;
-  k_scan<<<tiles, kScanThreads, 0, st>>>(in, out, zero_out, n, tile_status, counters);
+  const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out) |
+                     reinterpret_cast<uintptr_t>(zero_out)) & 15u) == 0;
+  k_scan<<<tiles, kScanThreads, 0, st>>>(in, out, zero_out, n, tile_status, counters, vec ? 1u : 0u);
   return cudaGetLastError();
+}
+
+namespace {
+// Per device: shared memory per SM, for the blocks per SM of the persistent
+// scatter (two by its launch bounds when shared memory allows).
+int g_smem_per_sm[64];
+
+// Equal digits in a warp round by ballots (default) or by __match_any_sync
+// (PFSIM_RADIX_RANK=match); the results are the same.
+bool radix_rank_ballot() {
+  static const bool b = [] {
+    const char* e = std::getenv("PFSIM_RADIX_RANK");
+    return !(e && std::string(e) == "match");
+  }();
+  return b;
+}
+
+template <bool kFirst, bool kLast, bool kBallot>
+cudaError_t launch_scatter_as(const uint32_t* kin, const uint32_t* vin, uint32_t n, uint32_t* kout, uint32_t* vout,
+                              uint32_t shift, const RadixPlan& plan, const SortScratch& s, uint32_t* count,
+                              cudaStream_t st) {
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
+  const size_t smem = scatter_smem_bytes(plan.digits, kFirst);
+  const int per_sm = dev < 64 ? g_smem_per_sm[dev] : 0;
+  const uint32_t blocks = per_sm > 0 ? (uint32_t)std::min<size_t>(2, std::max<size_t>(1, per_sm / (smem + 1024))) : 1u;
+  const uint32_t grid = std::min<uint32_t>(radix_tiles(n), blocks * (uint32_t)sm_count());
+  const bool vec = (reinterpret_cast<uintptr_t>(kin) & 15u) == 0 &&
+                   (kFirst || (reinterpret_cast<uintptr_t>(vin) & 15u) == 0);
+  k_radix_scatter<kFirst, kLast, kBallot><<<grid, kOsThreads, smem, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
+                                                                          s.tcount, s.csum, count, vec ? 1u : 0u);
+  return cudaGetLastError();
+}
+
+template <bool kFirst, bool kLast>
+cudaError_t launch_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t n, uint32_t* kout, uint32_t* vout,
+                           uint32_t shift, const RadixPlan& plan, const SortScratch& s, uint32_t* count,
+                           cudaStream_t st) {
+  return radix_rank_ballot()
+             ? launch_scatter_as<kFirst, kLast, true>(kin, vin, n, kout, vout, shift, plan, s, count, st)
+             : launch_scatter_as<kFirst, kLast, false>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+}
+
+template <bool kFirst, bool kLast, bool kBallot>
+cudaError_t scatter_allow_smem() {
+  return cudaFuncSetAttribute(k_radix_scatter<kFirst, kLast, kBallot>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kOsSmemBytes);
+}
+}  // namespace
+
+uint32_t grid_sort_launches(const RadixPlan& plan, uint32_t n) {
+  if (n == 0) return 1;                        // the start scan
+  if (plan.passes == 0) return 3;              // identity, run counts, start scan
+  return 1 + 4 * plan.passes + 1;              // digit scan, per pass four, start scan
 }
 
 cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const RadixPlan& plan, uint32_t* count,
@@ -637,41 +822,43 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
   if (cudaError_t e = cudaMemsetAsync(count, 0, 4ull * C, st); e != cudaSuccess) return e;
   if (n > 0) {
     const uint32_t tiles = radix_tiles(n);
-    const uint32_t* sorted = keys;
     if (plan.passes == 0) {
       k_identity<<<div_up(n, 256), 256, 0, st>>>(perm, n);
+      k_run_counts<<<div_up(n, 256), 256, 0, st>>>(keys, n, count);
     } else {
       if (cudaError_t e = radix_prepare(); e != cudaSuccess) return e;
       k_digit_first<<<plan.passes, 1024, 0, st>>>(s.digit_count, plan.digits);
       const uint32_t chunks = div_up(tiles, kScanChunk);
+      const bool kvec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
       const uint32_t* kin = keys;
       const uint32_t* vin = nullptr;
       for (uint32_t p = 0; p < plan.passes; ++p) {
-        const bool last = p + 1 == plan.passes;
+        const bool first = p == 0, last = p + 1 == plan.passes;
         // pass outputs: even passes -> (ka, va), odd -> (kb, vb); the last
-        // writes perm and the sorted keys into whichever of ka, kb it does
-        // not read
-        uint32_t* kout = last ? (kin == s.ka ? s.kb : s.ka) : ((p & 1u) ? s.kb : s.ka);
-        if (last && plan.passes == 1) kout = s.kb;
+        // writes the permutation and the cell counts, no keys
+        uint32_t* kout = last ? nullptr : ((p & 1u) ? s.kb : s.ka);
         uint32_t* vout = last ? perm : ((p & 1u) ? s.vb : s.va);
         const uint32_t shift = p * plan.width;
-        k_tile_counts<<<tiles, kOsThreads, 0, st>>>(kin, n, shift, plan.digits, s.tcount);
+        k_tile_counts<<<tiles, kCountThreads, 0, st>>>(kin, n, shift, plan.digits, s.tcount,
+                                                       (first ? kvec : true) ? 1u : 0u);
         k_tile_scan_chunk<<<dim3(chunks, div_up(plan.digits, 256)), 256, 0, st>>>(s.tcount, tiles, plan.digits,
                                                                                    s.csum);
-        k_tile_scan_chunks<<<div_up(plan.digits, 256), 256, 0, st>>>(s.csum, chunks, plan.digits,
-                                                                   s.digit_count + p * kRadixMaxDigits);
-        if (p == 0)
-          k_radix_scatter<true><<<tiles, kOsThreads, scatter_smem_bytes(plan.digits), st>>>(kin, vin, n, kout, vout, shift, plan.digits,
-                                                                        s.tcount, s.csum);
+        k_tile_scan_chunks<<<div_up(plan.digits, 8), 256, 0, st>>>(s.csum, chunks, plan.digits,
+                                                                 s.digit_count + p * kRadixMaxDigits);
+        cudaError_t e;
+        if (first && last)
+          e = launch_scatter<true, true>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+        else if (first)
+          e = launch_scatter<true, false>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+        else if (last)
+          e = launch_scatter<false, true>(kin, vin, n, kout, vout, shift, plan, s, count, st);
         else
-          k_radix_scatter<false><<<tiles, kOsThreads, scatter_smem_bytes(plan.digits), st>>>(kin, vin, n, kout, vout, shift, plan.digits,
-                                                                         s.tcount, s.csum);
+          e = launch_scatter<false, false>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+        if (e != cudaSuccess) return e;
         kin = kout;
         vin = vout;
       }
-      sorted = kin;
     }
-    k_run_counts<<<div_up(n, 256), 256, 0, st>>>(sorted, n, count);
   }
   if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
   return launch_exclusive_scan(count, start, nullptr, C, s.scan_status, s.counters, st);
@@ -684,14 +871,17 @@ cudaError_t radix_prepare() {
   if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
   std::lock_guard<std::mutex> g(m);
   if (ready.count(dev)) return cudaSuccess;
-  if (cudaError_t e = cudaFuncSetAttribute(k_radix_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kOsSmemBytes);
+  for (cudaError_t e : {scatter_allow_smem<true, true, true>(), scatter_allow_smem<true, false, true>(),
+                        scatter_allow_smem<false, true, true>(), scatter_allow_smem<false, false, true>(),
+                        scatter_allow_smem<true, true, false>(), scatter_allow_smem<true, false, false>(),
+                        scatter_allow_smem<false, true, false>(), scatter_allow_smem<false, false, false>()})
+    if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if (cudaError_t e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
       e != cudaSuccess)
     return e;
-  if (cudaError_t e = cudaFuncSetAttribute(k_radix_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kOsSmemBytes);
-      e != cudaSuccess)
-    return e;
+  if (dev < 64) g_smem_per_sm[dev] = per_sm;
+  (void)sm_count();  // cached outside any stream capture
   ready.insert(dev);
   return cudaSuccess;
 }

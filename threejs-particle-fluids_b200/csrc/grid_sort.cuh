@@ -6,14 +6,16 @@
 //                histograms flushed once per block
 //   digit scan   the counts of each pass turned into each digit's first
 //                output position
-//   passes       one LSD radix pass per 11 (or fewer) key bits, each three
-//                steps: every tile of 4096 elements counts its digits; the
-//                tile counts are scanned per digit over the tiles; every tile
-//                ranks its elements by digit in element order (warp-aggregated
-//                with __match_any_sync) and writes them out digit run by
-//                digit run through shared memory
-//   runs         the count of every cell from the sorted keys (one atomic per
-//                run of equal keys in a warp)
+//   passes       one LSD radix pass per 8 (or fewer; PFSIM_RADIX_BITS) key
+//                bits, each three steps: every tile of 4096 elements counts
+//                its digits; the tile counts are scanned per digit over the
+//                tiles; a persistent scatter ranks each tile's elements by
+//                digit in element order (warp-aggregated with
+//                __match_any_sync), copying the next tile into shared memory
+//                meanwhile, and writes them out digit run by digit run
+//   runs         the last pass writes no keys: it counts every cell from its
+//                staged tiles, which are in key order (one atomic per run of
+//                equal keys in a warp)
 //   scan         decoupled look-back exclusive scan counts -> start
 // LSD passes are stable, so the result equals a stable counting sort of the
 // elements 0..n-1: within a cell, elements appear in ascending index.
@@ -41,13 +43,19 @@ bool make_key_fn(const pf_grid_desc& g, KeyFn* out, uint64_t* cells);
 // Checks a sort request as HashGrid's constructor and rebuild do and
 // resolves its key function; the reference's error text on failure.
 pf_status validate_sort(uint32_t n, const pf_grid_desc* grid, KeyFn* kf, uint64_t* cells);
+// Checks the device buffers of a standalone sort: positions and perm present
+// unless n is 0, start and count present, positions 16-byte aligned (they are
+// read as float4), the other buffers (keys and overflow may be NULL) 4-byte
+// aligned. Other alignments are handled inside the sort.
+pf_status validate_sort_buffers(uint32_t n, const void* pos4, const void* perm, const void* start, const void* count,
+                                const void* keys, const void* overflow);
 
 // Radix plan for keys in [0, C): `passes` LSD passes of `width` bits, at
 // most radix_digit_bits() bits each (8 unless PFSIM_RADIX_BITS sets 4 to 11).
 constexpr uint32_t kRadixMaxBits = 11;
 constexpr uint32_t kRadixMaxDigits = 1u << kRadixMaxBits;  // 2048
 constexpr uint32_t kRadixMaxPasses = 4;                     // 32 bits of 8 >= any key below 2^31
-constexpr uint32_t kRadixTile = 4096;                       // elements per tile (256 threads x 16)
+constexpr uint32_t kRadixTile = 4096;                       // elements per tile of a radix pass
 uint32_t radix_digit_bits();
 struct RadixPlan {
   uint32_t passes = 0, width = 0, digits = 1;
@@ -94,6 +102,9 @@ void launch_keys_digits(const float4* pos, uint32_t n, const KeyFn& kf, const Ra
 cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const RadixPlan& plan,
                              uint32_t* count, uint32_t* start, uint32_t* perm, const SortScratch& s,
                              cudaStream_t st);
+
+// Kernel launches of launch_grid_sort for a plan and element count.
+uint32_t grid_sort_launches(const RadixPlan& plan, uint32_t n);
 
 // Per device, once: the radix passes' shared-memory size above the default
 // limit. Call it outside stream capture before the first sort on a device

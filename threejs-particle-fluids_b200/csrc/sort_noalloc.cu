@@ -98,8 +98,7 @@ extern "C" pf_status pf_sort_noalloc(const float* d_pos4, uint32_t n, const pf_g
   void* base = nullptr;
   // set-up only: the block's address on this device (see the file comment)
   if (n == 0 && !d_start && !d_count) return noalloc_scratch(&base);
-  if (n > 0 && (!d_pos4 || !d_perm)) return fail(PF_ERR_INVALID, "HashGrid: NULL positions or perm");
-  if (!d_start || !d_count) return fail(PF_ERR_INVALID, "HashGrid: NULL start or count");
+  PF_TRY(validate_sort_buffers(n, d_pos4, d_perm, d_start, d_count, d_keys, d_overflow));
 
   PF_TRY(noalloc_scratch(&base));
   // carved for the block's limits, whatever this call's size

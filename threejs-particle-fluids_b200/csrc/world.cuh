@@ -39,6 +39,8 @@ constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts
 // m-th entry is halfword nbr16_col(k) + m * kNbrStride of the block, a
 // warp's m-th entries one 64-byte half line. Otherwise the warp's base is
 // kNbrWide and its entries are whole slots, word nbr_col(k) + m * kNbrStride.
+// The 16-bit entries fill half the block; the list build stores hits past
+// the kMaxNbr-th in entry kMaxNbr, which no reader reads.
 constexpr uint32_t kNbrStride = 32;
 constexpr uint32_t kNbrWide = 0x80000000u;
 static_assert(kSegAlign % kNbrStride == 0, "a scene's segment starts on a list block");

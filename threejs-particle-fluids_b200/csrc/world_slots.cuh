@@ -17,6 +17,8 @@
 // (world_tiles.cuh) per world.
 #pragma once
 
+#include <type_traits>
+
 #include "world_kernels.cuh"
 
 namespace pf {
@@ -274,88 +276,94 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   if (!f) return;
   // Every candidate is tested; the first kMaxNbr hits in walk order are
   // stored (as the reference's list keeps them) and any further hit only
-  // marks the overflow.
+  // marks the overflow. The walk is compiled once per entry width (the width
+  // is uniform over the warp), and a 16-bit entry is stored without a branch
+  // on the count: hits past the kMaxNbr-th land in entry kMaxNbr of the
+  // block, which the 16-bit layout leaves unused (a 16-bit block has room
+  // for 2 kMaxNbr entries per slot).
   uint32_t cnt = 0;
   uint32_t* __restrict__ out = V.nbr + nbr_col(k);
   uint16_t* __restrict__ out16 = reinterpret_cast<uint16_t*>(V.nbr) + nbr16_col(k);
-  auto test = [&](uint32_t j, float4 xj) {
-    if (dot_rn(xi - xyz(xj)) < hsq) {
-      if (cnt < kMaxNbr) {
-        if (narrow) {
-          *out16 = (uint16_t)(j - base);
-          out16 += kNbrStride;
-        } else {
-          *out = j;
-          out += kNbrStride;
+  auto walk = [&](auto narrow_tag) {
+    constexpr bool kNarrow = decltype(narrow_tag)::value;
+    auto test = [&](uint32_t j, float4 xj) {
+      const bool hit = dot_rn(xi - xyz(xj)) < hsq;
+      if (kNarrow) {
+        if (hit) out16[min(cnt, kMaxNbr) * kNbrStride] = (uint16_t)(j - base);
+      } else {
+        if (hit && cnt < kMaxNbr) out[cnt * kNbrStride] = j;
+      }
+      cnt += hit ? 1u : 0u;
+    };
+    if (kFlat) {
+      // the row pointer moves on at each row's end (empty rows skipped); the
+      // rows stay in registers (constant indices after unrolling)
+      int r = 0;
+      uint32_t j = rs[0], e = re[0];
+      auto pick = [](const uint32_t(&a)[9], int q) {
+        uint32_t v = a[0];
+#pragma unroll
+        for (int t = 1; t < 9; ++t) v = q == t ? a[t] : v;
+        return v;
+      };
+      auto advance = [&]() {
+        while (j >= e && r < 8) {
+          ++r;
+          j = pick(rs, r);
+          e = pick(re, r);
+        }
+      };
+      advance();
+      while (j < e) {
+        uint32_t c[kNbrUnroll];
+        bool live[kNbrUnroll];
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q) {
+          live[q] = j < e;
+          c[q] = j;
+          if (live[q]) {
+            ++j;
+            if (j >= e) advance();
+          }
+        }
+        float4 xj[kNbrUnroll];
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q)
+          if (live[q]) xj[q] = __ldg(V.cur.xs + c[q]);
+#pragma unroll
+        for (uint32_t q = 0; q < kNbrUnroll; ++q)
+          if (live[q]) test(c[q], xj[q]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        uint32_t j = rs[r];
+        const uint32_t e = re[r];
+        // whole rounds, then the row's last 1 to kNbrUnroll - 1 candidates as
+        // one guarded round (their loads in flight together)
+        for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
+          float4 xj[kNbrUnroll];
+#pragma unroll
+          for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+          for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
+        }
+        if (j < e) {
+          float4 xj[kNbrUnroll];
+#pragma unroll
+          for (uint32_t q = 0; q < kNbrUnroll; ++q)
+            if (j + q < e) xj[q] = __ldg(V.cur.xs + j + q);
+#pragma unroll
+          for (uint32_t q = 0; q < kNbrUnroll; ++q)
+            if (j + q < e) test(j + q, xj[q]);
         }
       }
-      ++cnt;
     }
   };
-  if (kFlat) {
-    // the row pointer moves on at each row's end (empty rows skipped); the
-    // rows stay in registers (constant indices after unrolling)
-    int r = 0;
-    uint32_t j = rs[0], e = re[0];
-    auto pick = [](const uint32_t(&a)[9], int q) {
-      uint32_t v = a[0];
-#pragma unroll
-      for (int t = 1; t < 9; ++t) v = q == t ? a[t] : v;
-      return v;
-    };
-    auto advance = [&]() {
-      while (j >= e && r < 8) {
-        ++r;
-        j = pick(rs, r);
-        e = pick(re, r);
-      }
-    };
-    advance();
-    while (j < e) {
-      uint32_t c[kNbrUnroll];
-      bool live[kNbrUnroll];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q) {
-        live[q] = j < e;
-        c[q] = j;
-        if (live[q]) {
-          ++j;
-          if (j >= e) advance();
-        }
-      }
-      float4 xj[kNbrUnroll];
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q)
-        if (live[q]) xj[q] = __ldg(V.cur.xs + c[q]);
-#pragma unroll
-      for (uint32_t q = 0; q < kNbrUnroll; ++q)
-        if (live[q]) test(c[q], xj[q]);
-    }
-  } else {
-#pragma unroll
-    for (int r = 0; r < 9; ++r) {
-      uint32_t j = rs[r];
-      const uint32_t e = re[r];
-      // whole rounds, then the row's last 1 to kNbrUnroll - 1 candidates as
-      // one guarded round (their loads in flight together)
-      for (; j + kNbrUnroll <= e; j += kNbrUnroll) {
-        float4 xj[kNbrUnroll];
-#pragma unroll
-        for (uint32_t q = 0; q < kNbrUnroll; ++q) xj[q] = __ldg(V.cur.xs + j + q);
-#pragma unroll
-        for (uint32_t q = 0; q < kNbrUnroll; ++q) test(j + q, xj[q]);
-      }
-      if (j < e) {
-        float4 xj[kNbrUnroll];
-#pragma unroll
-        for (uint32_t q = 0; q < kNbrUnroll; ++q)
-          if (j + q < e) xj[q] = __ldg(V.cur.xs + j + q);
-#pragma unroll
-        for (uint32_t q = 0; q < kNbrUnroll; ++q)
-          if (j + q < e) test(j + q, xj[q]);
-      }
-    }
-  }
+  if (narrow)
+    walk(std::true_type{});
+  else
+    walk(std::false_type{});
   const bool over = cnt > kMaxNbr;
   cnt = min(cnt, kMaxNbr);
   V.ncount[k] = cnt;
