@@ -359,13 +359,16 @@ typedef struct pf_loop_desc {
   uint32_t iterations;
   float gravity[3];
   float hash_origin[3];
-  /* Size and first placement of the neighbour grid window in metres. The
+  /* First size and placement of the neighbour grid window in metres. The
    * grid is a window over the reference's cell lattice (cell = the widest
    * query radius, aligned to hash_origin) that moves with the particles
-   * each substep; only particles spread wider than the window are clamped
-   * into its border cells (pf_overflow.grid_clamped). min >= max on any
-   * axis selects a window four times the extent of the uploaded particles
-   * (at least 16 cells more), centred on them. */
+   * each substep, and grows between steps (to twice their spread on an
+   * axis, up to 2^27 cells) when they come close to its size. Particles
+   * spread wider than the window before it has grown (on the first step,
+   * or past that limit) are clamped into its border cells
+   * (pf_overflow.grid_clamped). min >= max on any axis selects a window
+   * four times the extent of the uploaded particles (at least 16 cells
+   * more), centred on them. */
   float grid_min[3];
   float grid_max[3];
   /* SimLoopOptions.contact (loop.ts:20-30, 347-417; src/core/contact/):
@@ -433,8 +436,9 @@ PF_API pf_status pf_write(pf_scene* scene, uint32_t field, const void* src_host,
  *                 wider than its grid window, so some were clamped into the
  *                 window's border cells: neighbour sets stay complete, but
  *                 their order can depart from the reference's walk. The window
- *                 follows the particles each substep; it is sized by
- *                 pf_loop_desc.grid_min/max, or four times the initial extent. */
+ *                 follows the particles each substep and grows between steps
+ *                 (see pf_loop_desc.grid_min/max), so this fires only when a
+ *                 step outruns it. */
 typedef struct pf_overflow {
   uint32_t positions;
   uint32_t velocities;

@@ -412,11 +412,13 @@ __device__ __forceinline__ void tile_fetch(uint32_t* dst, const uint32_t* __rest
 // The lanes of `active` whose digit d (of `bits` bits) equals this lane's:
 // one ballot per digit bit, each keeping the lanes that agree on that bit.
 // Called by every lane of `active` together.
+// kW > 0: the digits have exactly kW bits (bits is then ignored).
+template <uint32_t kW>
 __device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t bits, uint32_t active) {
   uint32_t m = active;
 #pragma unroll
-  for (uint32_t b = 0; b < kRadixMaxBits; ++b)
-    if (b < bits) {  // uniform over the warp
+  for (uint32_t b = 0; b < (kW ? kW : kRadixMaxBits); ++b)
+    if (kW || b < bits) {  // uniform over the warp
       const bool set = (d >> b) & 1u;
       const uint32_t v = __ballot_sync(active, set);
       m &= set ? v : ~v;
@@ -434,10 +436,11 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t bits, uint3
 // memory and writes each digit's run to the run's first output position (the
 // tile's scanned count plus its chunk's base).
 // kFirst: the values are the element indices (no value input).
+// kW: the digit width when it is fixed at compile time (0: any width).
 // kLast: the keys are not written out; instead the staged tile, which is in
 // key order, adds the length of every run of equal keys in a warp's 32
 // entries to count[key] (the cell counts of the sort).
-template <bool kFirst, bool kLast, bool kBallot>
+template <bool kFirst, bool kLast, bool kBallot, uint32_t kW>
 __global__ void __launch_bounds__(kOsThreads, 2)
 k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
                 uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t shift, uint32_t digits,
@@ -485,27 +488,50 @@ k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ v
     const uint32_t valid = min(kRadixTile, n - tbase);
     const uint32_t wbase = warp * kOsStripe;
     // rank in element order inside the warp's stripe: a round's equal digits
-    // by lane, after the counts of the warp's earlier rounds
-    uint32_t key[kOsItems], pos[kOsItems];
+    // by lane, after the counts of the warp's earlier rounds. The rounds'
+    // peer masks depend on nothing in shared memory, so they are all formed
+    // first (their latencies overlap); then the rounds run through the warp's
+    // histogram in order.
+    uint32_t key[kOsItems], pos[kOsItems], peers[kOsItems];
     uint16_t* wh = whist + warp * digits;
+    const uint32_t lt = lanemask_lt();
+    if (valid == kRadixTile) {  // a whole tile (uniform over the block)
 #pragma unroll
-    for (uint32_t i = 0; i < kOsItems; ++i) {
-      const uint32_t l = wbase + i * 32u + lane;
-      const bool ok = l < valid;
-      key[i] = ok ? ik[l] : 0u;
-      const uint32_t vm = __ballot_sync(0xffffffffu, ok);
-      pos[i] = 0;
-      if (!vm) continue;  // warp-uniform
-      const uint32_t d = (key[i] >> shift) & mask;
-      uint32_t peers = 0, old = 0;
-      if (ok) {
-        peers = kBallot ? digit_peers(d, width, vm) : __match_any_sync(vm, d);
-        old = wh[d];
-        pos[i] = old + __popc(peers & lanemask_lt());
+      for (uint32_t i = 0; i < kOsItems; ++i) key[i] = ik[wbase + i * 32u + lane];
+#pragma unroll
+      for (uint32_t i = 0; i < kOsItems; ++i) {
+        const uint32_t d = (key[i] >> shift) & mask;
+        peers[i] = kBallot ? digit_peers<kW>(d, width, 0xffffffffu) : __match_any_sync(0xffffffffu, d);
       }
-      __syncwarp();
-      if (ok && lane == (uint32_t)(__ffs(peers) - 1)) wh[d] = (uint16_t)(old + __popc(peers));
-      __syncwarp();
+#pragma unroll
+      for (uint32_t i = 0; i < kOsItems; ++i) {
+        const uint32_t d = (key[i] >> shift) & mask;
+        const uint32_t old = wh[d];
+        pos[i] = old + __popc(peers[i] & lt);
+        __syncwarp();
+        if (lane == (uint32_t)(__ffs(peers[i]) - 1)) wh[d] = (uint16_t)(old + __popc(peers[i]));
+        __syncwarp();
+      }
+    } else {
+#pragma unroll
+      for (uint32_t i = 0; i < kOsItems; ++i) {
+        const uint32_t l = wbase + i * 32u + lane;
+        const bool ok = l < valid;
+        key[i] = ok ? ik[l] : 0u;
+        const uint32_t vm = __ballot_sync(0xffffffffu, ok);
+        pos[i] = 0;
+        if (!vm) continue;  // warp-uniform
+        const uint32_t d = (key[i] >> shift) & mask;
+        uint32_t pm = 0, old = 0;
+        if (ok) {
+          pm = kBallot ? digit_peers<kW>(d, width, vm) : __match_any_sync(vm, d);
+          old = wh[d];
+          pos[i] = old + __popc(pm & lt);
+        }
+        __syncwarp();
+        if (ok && lane == (uint32_t)(__ffs(pm) - 1)) wh[d] = (uint16_t)(old + __popc(pm));
+        __syncwarp();
+      }
     }
     __syncthreads();
     // per digit: the warps' counts -> exclusive offsets over warps; the tile's count
@@ -544,6 +570,8 @@ k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ v
         }
     }
     __syncthreads();
+    // each digit's output position for tile position 0 of its run
+    for (uint32_t d = tid; d < digits; d += kOsThreads) gstart[d] -= lstart[d];
     // tile positions, and the tile staged in digit order (the stage holds
     // nothing else)
     const uint32_t* iv = in_v + buf * kRadixTile;
@@ -565,8 +593,7 @@ k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ v
       const bool ok = k < valid;
       const uint32_t kk = ok ? stage_k[k] : 0xffffffffu;
       if (ok) {
-        const uint32_t d = (kk >> shift) & mask;
-        const uint32_t dst = gstart[d] + (k - lstart[d]);
+        const uint32_t dst = gstart[(kk >> shift) & mask] + k;
         if (!kLast) kout[dst] = kk;
         vout[dst] = stage_v[k];
       }
@@ -777,7 +804,7 @@ bool radix_rank_ballot() {
   return b;
 }
 
-template <bool kFirst, bool kLast, bool kBallot>
+template <bool kFirst, bool kLast, bool kBallot, uint32_t kW>
 cudaError_t launch_scatter_as(const uint32_t* kin, const uint32_t* vin, uint32_t n, uint32_t* kout, uint32_t* vout,
                               uint32_t shift, const RadixPlan& plan, const SortScratch& s, uint32_t* count,
                               cudaStream_t st) {
@@ -789,24 +816,45 @@ cudaError_t launch_scatter_as(const uint32_t* kin, const uint32_t* vin, uint32_t
   const uint32_t grid = std::min<uint32_t>(radix_tiles(n), blocks * (uint32_t)sm_count());
   const bool vec = (reinterpret_cast<uintptr_t>(kin) & 15u) == 0 &&
                    (kFirst || (reinterpret_cast<uintptr_t>(vin) & 15u) == 0);
-  k_radix_scatter<kFirst, kLast, kBallot><<<grid, kOsThreads, smem, st>>>(kin, vin, n, kout, vout, shift, plan.digits,
-                                                                          s.tcount, s.csum, count, vec ? 1u : 0u);
+  k_radix_scatter<kFirst, kLast, kBallot, kW><<<grid, kOsThreads, smem, st>>>(
+      kin, vin, n, kout, vout, shift, plan.digits, s.tcount, s.csum, count, vec ? 1u : 0u);
   return cudaGetLastError();
 }
+
+// The digit widths of the common plans get their own ballot kernels.
+#define PF_SCATTER_WIDTHS(X) X(6) X(7) X(8)
 
 template <bool kFirst, bool kLast>
 cudaError_t launch_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t n, uint32_t* kout, uint32_t* vout,
                            uint32_t shift, const RadixPlan& plan, const SortScratch& s, uint32_t* count,
                            cudaStream_t st) {
-  return radix_rank_ballot()
-             ? launch_scatter_as<kFirst, kLast, true>(kin, vin, n, kout, vout, shift, plan, s, count, st)
-             : launch_scatter_as<kFirst, kLast, false>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+  if (!radix_rank_ballot())
+    return launch_scatter_as<kFirst, kLast, false, 0>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+  switch (plan.width) {
+#define PF_CASE(w) \
+  case w:          \
+    return launch_scatter_as<kFirst, kLast, true, w>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+    PF_SCATTER_WIDTHS(PF_CASE)
+#undef PF_CASE
+    default:
+      return launch_scatter_as<kFirst, kLast, true, 0>(kin, vin, n, kout, vout, shift, plan, s, count, st);
+  }
 }
 
-template <bool kFirst, bool kLast, bool kBallot>
+template <bool kFirst, bool kLast, bool kBallot, uint32_t kW>
 cudaError_t scatter_allow_smem() {
-  return cudaFuncSetAttribute(k_radix_scatter<kFirst, kLast, kBallot>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_radix_scatter<kFirst, kLast, kBallot, kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)kOsSmemBytes);
+}
+template <bool kFirst, bool kLast>
+cudaError_t scatter_allow_smem_all() {
+  for (cudaError_t e : {scatter_allow_smem<kFirst, kLast, false, 0>(), scatter_allow_smem<kFirst, kLast, true, 0>()
+#define PF_ALLOW(w) , scatter_allow_smem<kFirst, kLast, true, w>()
+                            PF_SCATTER_WIDTHS(PF_ALLOW)
+#undef PF_ALLOW
+       })
+    if (e != cudaSuccess) return e;
+  return cudaSuccess;
 }
 }  // namespace
 
@@ -871,10 +919,8 @@ cudaError_t radix_prepare() {
   if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) return e;
   std::lock_guard<std::mutex> g(m);
   if (ready.count(dev)) return cudaSuccess;
-  for (cudaError_t e : {scatter_allow_smem<true, true, true>(), scatter_allow_smem<true, false, true>(),
-                        scatter_allow_smem<false, true, true>(), scatter_allow_smem<false, false, true>(),
-                        scatter_allow_smem<true, true, false>(), scatter_allow_smem<true, false, false>(),
-                        scatter_allow_smem<false, true, false>(), scatter_allow_smem<false, false, false>()})
+  for (cudaError_t e : {scatter_allow_smem_all<true, true>(), scatter_allow_smem_all<true, false>(),
+                        scatter_allow_smem_all<false, true>(), scatter_allow_smem_all<false, false>()})
     if (e != cudaSuccess) return e;
   int per_sm = 0;
   if (cudaError_t e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);

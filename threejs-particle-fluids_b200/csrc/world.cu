@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(kBlock) k_bbox(WorldView V) {
 // Places each grid scene's window for this substep: the least move of the
 // build-time window (lo0) that covers the scene's cell bounds, or lo0 where
 // the bounds are wider than the window (the keys then clamp and flag). The
-// bounds are reset for the next substep.
+// bounds are kept in bbox_last (the host widens windows between steps from
+// them) and reset for the next substep.
 __global__ void k_grid_fit(WorldView V, uint32_t nscenes) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nscenes) return;
@@ -95,6 +96,10 @@ __global__ void k_grid_fit(WorldView V, uint32_t nscenes) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int64_t mn = b[a], mx = b[a + 3], d = S.dims[a];
+    if (mn <= mx) {  // scenes past their substeps keep their last bounds
+      V.bbox_last[6 * s + a] = b[a];
+      V.bbox_last[6 * s + a + 3] = b[a + 3];
+    }
     int64_t lo = S.lo0[a];
     if (mn <= mx && mx - mn + 1 <= d) {
       if (lo > mn) lo = mn;
@@ -1090,6 +1095,10 @@ World::~World() {
   drop_graphs();
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (ev_bbox_) cudaEventDestroy(ev_bbox_);
+  if (ev_params_) cudaEventDestroy(ev_params_);
+  if (h_pinned_bbox_) cudaFreeHost(h_pinned_bbox_);
+  if (grid_arena_) cudaFree(grid_arena_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   if (side_stream_) cudaStreamDestroy(side_stream_);
@@ -1758,8 +1767,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     if (!S.has_grid || S.fluid_count == 0) continue;
     grid_scene.push_back(s);
     row_base.push_back(row_base.back() + S.dims[1] * S.dims[2]);
-    // every tile holds at least one particle and one cell
-    max_tiles += std::min<uint64_t>(S.cells, S.cap);
+    // every tile holds at least one particle (and one cell, whatever the
+    // window's size once it has grown)
+    max_tiles += S.cap;
   }
   max_tiles = std::min<uint64_t>(max_tiles, 0xffffffffull);
   // ---- allocate one arena ----------------------------------------------
@@ -1781,6 +1791,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.n_cchunk = (uint32_t)cchunk.size();
     base_.flags = cv.take<uint32_t>(K * kNumFlags);
     base_.bbox = cv.take<int32_t>(6 * K);
+    base_.bbox_last = cv.take<int32_t>(6 * K);
     base_.clocks = cv.take<float>(K);
     base_.fluids = cv.take<DevFluid>(h_fluids_.size());
     base_.bnds = cv.take<DevBoundary>(h_bnds_.size());
@@ -1902,6 +1913,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   layout(cv);
   sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, cells_, &sort_);
   radix_ = radix_plan(cells_);
+  cells_cap_ = cells_;
+  grow_prev_ext_.assign(3 * K, 0);
   base_.scenes = base_.scenes_rw;
   base_.n = n_;
   base_.prim_stride = prim_stride_;
@@ -1922,6 +1935,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   PF_CUDA(cudaEventCreate(&ev0_));
   PF_CUDA(cudaEventCreate(&ev1_));
+  PF_CUDA(cudaEventCreateWithFlags(&ev_bbox_, cudaEventDisableTiming));
+  PF_CUDA(cudaEventCreateWithFlags(&ev_params_, cudaEventDisableTiming));
+  PF_CUDA(cudaMallocHost(&h_pinned_bbox_, sizeof(int32_t) * 6 * std::max<size_t>(1, K)));
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_plane4_, sizeof(float4) * 2 * std::max<size_t>(1, h_prims_.size())));
@@ -2150,6 +2166,9 @@ pf_status World::upload_params(double dt) {
   // where this step's density passes leave lambda (read back by PF_FIELD_LAMBDA)
   lam_in_xl_.resize(K);
   for (uint32_t s = 0; s < K; ++s) lam_in_xl_[s] = h_scenes_[s].homog != 0;
+  // the previous step's copies may still wait behind earlier work: their
+  // pinned sources are written only once those copies have run
+  if (params_pending_) PF_CUDA(cudaEventSynchronize(ev_params_));
   std::memcpy(h_pinned_scenes_, h_scenes_.data(), sizeof(DevScene) * K);
   PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, h_pinned_scenes_, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
   if (sdfs_dirty_ && !h_sdfs_.empty()) {
@@ -2173,6 +2192,8 @@ pf_status World::upload_params(double dt) {
                             sizeof(pf_primitive) * h_prims_.size(), cudaMemcpyHostToDevice, stream_));
     prims_dirty_ = false;
   }
+  PF_CUDA(cudaEventRecord(ev_params_, stream_));
+  params_pending_ = true;
   return PF_OK;
 }
 
@@ -2675,6 +2696,7 @@ void World::run_substep(uint32_t s, uint32_t parity) {
 pf_status World::step(double dt) {
   if (!(dt > 0) || !std::isfinite(dt))
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
+  PF_TRY(maybe_grow_windows());
   PF_TRY(upload_params(dt));
   PF_CUDA(cudaEventRecord(ev0_, stream_));
   if (!tuned_) {
@@ -2700,18 +2722,33 @@ pf_status World::step(double dt) {
   if (use_graph_) {
     // Both start parities are captured on the first step, so later steps
     // only launch (no capture runs while a host thread builds another world).
-    for (uint32_t p : {parity_, parity_ ^ flips}) {
+    // After the grid windows grew, the captured steps are captured again
+    // and, where the launches keep their shape, updated in place (cheaper
+    // than a new instantiation).
+    const uint32_t parities[2] = {parity_, parity_ ^ flips};
+    for (uint32_t i = 0; i < (flips ? 2u : 1u); ++i) {
+      const uint32_t p = parities[i];
       cudaGraphExec_t& g = graph_[p];
-      if (g) continue;
+      if (g && !graphs_stale_) continue;
       cudaGraph_t graph;
       PF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       body(p);
       launches_per_step_ = t_launches;
       PF_CUDA(cudaStreamEndCapture(stream_, &graph));
-      const cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+      if (g) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(g, graph, &info) != cudaSuccess) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+      }
+      cudaError_t e = cudaSuccess;
+      if (!g) e = cudaGraphInstantiate(&g, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) return fail(PF_ERR_CUDA, std::string("SimLoop: graph instantiate: ") + cudaGetErrorString(e));
     }
+    graphs_stale_ = false;
     PF_CUDA(cudaGraphLaunch(graph_[parity_], stream_));
   } else {
     body(parity_);
@@ -2719,7 +2756,115 @@ pf_status World::step(double dt) {
   }
   parity_ ^= flips;
   PF_CUDA(cudaEventRecord(ev1_, stream_));
+  if (any_grid_) {
+    PF_CUDA(cudaMemcpyAsync(h_pinned_bbox_, base_.bbox_last, sizeof(int32_t) * 6 * h_scenes_.size(),
+                            cudaMemcpyDeviceToHost, stream_));
+    PF_CUDA(cudaEventRecord(ev_bbox_, stream_));
+    bbox_pending_ = true;
+  }
   PF_CUDA(cudaGetLastError());
+  return PF_OK;
+}
+
+// Between steps: a grid scene whose particles' cell bounds (as the last
+// window fit saw them) come within a margin of its window's size on some
+// axis gets a window twice their spread there, centred on them, so it never
+// has to clamp (the reference's hash grid is unbounded). Windows past 2^27
+// cells stay as they are (their keys clamp and flag).
+pf_status World::maybe_grow_windows() {
+  if (!bbox_pending_) return PF_OK;
+  const cudaError_t q = cudaEventQuery(ev_bbox_);
+  if (q == cudaErrorNotReady) return PF_OK;  // the last step still runs: look before the next one
+  PF_CUDA(q);
+  bbox_pending_ = false;
+  bool any = false;
+  for (uint32_t s = 0; s < h_scenes_.size(); ++s) {
+    DevScene& S = h_scenes_[s];
+    if (!S.has_grid) continue;
+    const int32_t* b = h_pinned_bbox_ + 6 * s;
+    int64_t lo[3], dims[3];
+    bool grow = false;
+    for (int a = 0; a < 3; ++a) {
+      const int64_t mn = b[a], mx = b[a + 3], d = S.dims[a];
+      lo[a] = S.lo0[a];
+      dims[a] = d;
+      if (mn > mx) continue;  // no particle
+      // within two cells of clamping, plus twice the spread's growth since
+      // the last look (a fluid that walls hold stops growing there)
+      const int64_t ext = mx - mn + 1;
+      int32_t& prev = grow_prev_ext_[3 * s + a];
+      const int64_t rate = prev > 0 ? std::max<int64_t>(0, ext - prev) : 0;
+      prev = (int32_t)ext;
+      if (ext + 2 * rate + 4 <= d) continue;
+      dims[a] = std::max<int64_t>(d, 2 * ext + 8);
+      lo[a] = ((mn + mx) >> 1) - dims[a] / 2;
+      grow = true;
+    }
+    if (!grow) continue;
+    const uint64_t cells = (uint64_t)dims[0] * dims[1] * dims[2];
+    if (cells > (1ull << 27)) continue;
+    for (int a = 0; a < 3; ++a) grow_prev_ext_[3 * s + a] = 0;
+    bool fits = true;
+    for (int a = 0; a < 3; ++a) fits = fits && lo[a] > INT32_MIN / 2 && lo[a] + dims[a] < INT32_MAX / 2;
+    if (!fits) continue;
+    const float org[3] = {S.ox, S.oy, S.oz};
+    double big = 0;
+    for (int a = 0; a < 3; ++a) {
+      S.lo0[a] = S.lo[a] = (int32_t)lo[a];
+      S.dims[a] = (uint32_t)dims[a];
+      big = std::max(big, std::fabs((double)org[a]) + std::max(std::fabs((double)lo[a]),
+                                                               std::fabs((double)(lo[a] + dims[a]))) * S.cell);
+    }
+    S.cells = (uint32_t)cells;
+    S.prune_slack = f32(big * (1.0 / 65536.0) + 1e-9);
+    any = true;
+  }
+  if (!any) return PF_OK;
+  return relayout_grid();
+}
+
+// The cell layout after windows changed size: key bases, the fluid grid
+// rows, the cell arrays and sort scratch (a new block when the arena's are
+// too small), the radix plan; graphs are captured again on the next step.
+pf_status World::relayout_grid() {
+  PF_CUDA(cudaStreamSynchronize(stream_));
+  if (side_stream_) PF_CUDA(cudaStreamSynchronize(side_stream_));
+  uint64_t cell = 0;
+  for (auto& S : h_scenes_) {
+    S.cell_base = (uint32_t)cell;
+    cell += (uint64_t)S.cells + 1;
+  }
+  if (cell > 0x7fffffffull) return fail(PF_ERR_INVALID, "SimLoop: grid windows over 2^31 cells");
+  cells_ = (uint32_t)cell;
+  std::vector<uint32_t> row_base(1, 0);
+  for (auto& S : h_scenes_)
+    if (S.has_grid && S.fluid_count) row_base.push_back(row_base.back() + S.dims[1] * S.dims[2]);
+  PF_CUDA(cudaMemcpy(const_cast<uint32_t*>(base_.row_base), row_base.data(), 4 * row_base.size(),
+                     cudaMemcpyHostToDevice));
+  base_.n_rows = row_base.back();
+  if (cells_ > cells_cap_) {
+    const uint64_t cap = std::min<uint64_t>(0x7fffffffull, (uint64_t)cells_ + cells_ / 4);
+    const size_t cell_bytes = al256(4ull * cap);
+    const size_t bytes = 2 * cell_bytes + al256(sort_scratch_bytes(n_, cap));
+    void* g = nullptr;
+    if (const cudaError_t e = cudaMalloc(&g, bytes); e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,
+                  "SimLoop: growing the grid windows needs " + std::to_string(bytes) + " more bytes");
+    }
+    char* p = static_cast<char*>(g);
+    base_.cstart = reinterpret_cast<uint32_t*>(p);
+    base_.ccount = reinterpret_cast<uint32_t*>(p + cell_bytes);
+    sort_scratch_carve(p + 2 * cell_bytes, n_, cap, &sort_);
+    if (grid_arena_) cudaFree(grid_arena_);
+    grid_arena_ = g;
+    bytes_ += bytes;
+    cells_cap_ = cap;
+  }
+  radix_ = radix_plan(cells_);
+  PF_CUDA(sort_scratch_zero(sort_, stream_));
+  ++regrowths_;
+  graphs_stale_ = true;
   return PF_OK;
 }
 
@@ -2904,7 +3049,7 @@ pf_status World::readback(uint32_t scene, uint32_t field, void* dst, size_t byte
             const uint32_t wb = wbase[k / 32];
             // a slot of the same scene's segment
             const uint32_t j = (wb & kNbrWide) ? all[nbr_col(k) + (size_t)m * kNbrStride]
-                                               : wb + all16[nbr16_col(k) + (size_t)m * kNbrStride];
+                                               : wb + all16[nbr16_at(k, m)];
             o[(size_t)id * kMaxNbr + m] = (j >= S.seg_start && j < S.seg_end) ? seg_ids[j - S.seg_start] - S.seg_start
                                                                                : 0xfffffffeu;
           }

@@ -35,21 +35,28 @@ constexpr uint32_t kMaxNbr = 64;  // NeighborList MAX_NEIGHBORS (neighborList.ts
 // The slot path's neighbour list is blocked by warp: each warp of slots owns
 // an 8 KB block. Entries are 16-bit offsets from a per-warp base slot
 // (nbr_base[k / 32]) when every slot the warp's 27-cell rows reach lies
-// within 65,536 slots of the lowest, which is the common case; then slot k's
-// m-th entry is halfword nbr16_col(k) + m * kNbrStride of the block, a
-// warp's m-th entries one 64-byte half line. Otherwise the warp's base is
-// kNbrWide and its entries are whole slots, word nbr_col(k) + m * kNbrStride.
-// The 16-bit entries fill half the block; the list build stores hits past
-// the kMaxNbr-th in entry kMaxNbr, which no reader reads.
+// within 65,536 slots of the lowest, which is the common case. Then the
+// entries go in groups of kNbrGroup (16 bytes) per slot: group g of the
+// warp's 32 slots is 512 contiguous bytes, slot k's 16 bytes at lane k % 32
+// (nbr16_at), so a warp reads a group as one coalesced 16-byte load per
+// lane. Otherwise the warp's base is kNbrWide and its entries are whole
+// slots, word nbr_col(k) + m * kNbrStride (a warp's m-th entries one line).
+// The 16-bit groups fill half the block; the list build stores hits past
+// the kMaxNbr-th in group kMaxNbr / kNbrGroup, which no reader reads.
 constexpr uint32_t kNbrStride = 32;
+constexpr uint32_t kNbrGroup = 8;
 constexpr uint32_t kNbrWide = 0x80000000u;
 static_assert(kSegAlign % kNbrStride == 0, "a scene's segment starts on a list block");
+static_assert(kMaxNbr % kNbrGroup == 0, "whole groups");
 __host__ __device__ __forceinline__ size_t nbr_col(size_t k) {
   return (k >> 5) * (size_t)kMaxNbr * kNbrStride + (k & 31);
 }
-__host__ __device__ __forceinline__ size_t nbr16_col(size_t k) {
-  return (k >> 5) * (size_t)kMaxNbr * kNbrStride * 2 + (k & 31);
+// halfword index of slot k's 16-bit entry m
+__host__ __device__ __forceinline__ size_t nbr16_at(size_t k, uint32_t m) {
+  return (k >> 5) * (size_t)kMaxNbr * kNbrStride * 2 + (size_t)(m / kNbrGroup) * (kNbrStride * kNbrGroup) +
+         (k & 31) * kNbrGroup + (m % kNbrGroup);
 }
+__host__ __device__ __forceinline__ size_t nbr16_col(size_t k) { return nbr16_at(k, 0); }
 constexpr uint32_t kBlock = 256;
 constexpr uint32_t kMaxContacts = 32;  // contact pairs kept per emitting particle per substep
 
@@ -291,6 +298,7 @@ struct WorldView {
   DevScene* scenes_rw;
   uint32_t* flags;              // kNumFlags per scene
   int32_t* bbox;                // per scene: lowest and highest cell of the predicted positions (6 words)
+  int32_t* bbox_last;           // per scene: the bounds the last window fit used (6 words; read between steps)
   float* clocks;                // collider sweep clock per scene (PrimitiveSet.motionClock)
   const DevFluid* fluids;
   const DevBoundary* bnds;
@@ -596,6 +604,27 @@ class World {
   uint64_t* prefix_dev_ = nullptr;
   uint64_t launches_per_step_ = 0;
   std::vector<uint64_t> prefix_;   // particle offset of each scene in read_positions
+  // Grid windows grow with their particles: after each step the last window
+  // fit's cell bounds come back to pinned memory, and before the next step
+  // any window they have nearly outgrown is widened and the cell arrays laid
+  // out again (outside any graph).
+  int32_t* h_pinned_bbox_ = nullptr;
+  cudaEvent_t ev_bbox_ = nullptr;
+  bool bbox_pending_ = false;
+  // the previous parameter upload, waited on before its pinned staging is
+  // written again
+  cudaEvent_t ev_params_ = nullptr;
+  bool params_pending_ = false;
+  void* grid_arena_ = nullptr;  // cell arrays and sort scratch once the windows outgrow the arena's
+  uint64_t cells_cap_ = 0;      // cells the current cell arrays and sort scratch hold
+  std::vector<int32_t> grow_prev_ext_;  // per scene and axis: the spread in cells at the last look
+  uint32_t regrowths_ = 0;
+  bool graphs_stale_ = false;  // the windows grew: capture the graphs again before launching one
+  pf_status maybe_grow_windows();
+  pf_status relayout_grid();
+
+ public:
+  uint32_t window_regrowths() const { return regrowths_; }
 };
 
 }  // namespace pf

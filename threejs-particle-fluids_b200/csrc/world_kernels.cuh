@@ -50,6 +50,20 @@ __device__ __forceinline__ float dot_rn(f3 a) {
 __device__ __forceinline__ float dot_rn(f3 a, f3 b) {
   return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
 }
+// dot_rn(xi - xj) with the x and y lanes in packed f32x2 operations (each
+// lane rounded as its scalar form, so the result is the same bits): the
+// list build's acceptance test.
+__device__ __forceinline__ float dist2_rn(f3 xi, float4 xj) {
+  float r;
+  asm("{\n\t.reg .b64 a, b, d;\n\t.reg .f32 sx, sy, dz;\n\t"
+      "mov.b64 a, {%1, %2};\n\tmov.b64 b, {%4, %5};\n\t"
+      "sub.rn.f32x2 d, a, b;\n\tmul.rn.f32x2 d, d, d;\n\t"
+      "mov.b64 {sx, sy}, d;\n\tadd.rn.f32 sx, sx, sy;\n\t"
+      "sub.rn.f32 dz, %3, %6;\n\tmul.rn.f32 dz, dz, dz;\n\tadd.rn.f32 %0, sx, dz;\n\t}"
+      : "=f"(r)
+      : "f"(xi.x), "f"(xi.y), "f"(xi.z), "f"(xj.x), "f"(xj.y), "f"(xj.z));
+  return r;
+}
 
 // collider.ts:53-89, the static-friction cone of one contact: the slip's
 // tangential part and whether the particle sticks (the tangential

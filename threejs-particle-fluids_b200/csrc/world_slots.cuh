@@ -4,9 +4,10 @@
 // neighbours' state straight from the slot arrays; particles are in cell
 // order, so a warp's gathers fall on a few hundred consecutive slots that L1
 // holds. The neighbour list is blocked by warp: 16-bit offsets from a
-// per-warp base slot (32-bit slots where a warp's rows reach further), so a
-// warp reads its m-th entries as one coalesced half line (or line) and its
-// next entries from the next one. The loops fetch the list and
+// per-warp base slot in groups of eight per slot, so a warp reads a round of
+// 2, 4 or 8 entries per slot as one coalesced vector load per lane (32-bit
+// slots, one line per entry index, where a warp's rows reach further). The
+// loops fetch the list and
 // the neighbours several at a time before using them: independent loads in
 // flight per round instead of a dependent load per neighbour, with the sums
 // still formed in list order.
@@ -23,26 +24,38 @@
 
 namespace pf {
 
-// A list entry (read-only for the kernel). A miss fetches 256 bytes into L2:
-// with the warp-blocked layout that is the warp's next lines of entries too.
+// A list entry, or 2, 4 or 8 16-bit entries of one group (read-only for the
+// kernel). A miss fetches 256 bytes into L2: with the warp-blocked layout
+// that is the warp's neighbouring entries too.
 __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
   uint32_t v;
   asm("ld.global.nc.L2::256B.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
-__device__ __forceinline__ uint32_t ld_entry(const uint16_t* p) {
-  unsigned short v;
-  asm("ld.global.nc.L2::256B.u16 %0, [%1];" : "=h"(v) : "l"(p));
-  return v;
+template <uint32_t kN>
+__device__ __forceinline__ void ld_group(const uint16_t* p, uint32_t (&w)[kN / 2]) {
+  static_assert(kN == 2 || kN == 4 || kN == 8, "2, 4 or 8 entries");
+  if constexpr (kN == 8)
+    asm("ld.global.nc.L2::256B.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+        : "l"(p));
+  else if constexpr (kN == 4)
+    asm("ld.global.nc.L2::256B.v2.u32 {%0, %1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "l"(p));
+  else
+    asm("ld.global.nc.L2::256B.u32 %0, [%1];" : "=r"(w[0]) : "l"(p));
 }
 
 // The list of slot k: its warp's base (kNbrWide: 32-bit entries) and the
 // first entry of either width.
 struct NbrList {
   uint32_t base;
-  const uint32_t* w32;
-  const uint16_t* w16;
+  const uint32_t* w32;  // entry m at w32[m * kNbrStride]
+  const uint16_t* w16;  // entry m at w16[(m / 8) * 256 + m % 8]
   __device__ __forceinline__ bool wide() const { return (base & kNbrWide) != 0; }
+  __device__ __forceinline__ uint32_t entry(uint32_t m) const {
+    return wide() ? __ldg(w32 + m * kNbrStride)
+                  : base + __ldg(w16 + (m / kNbrGroup) * (kNbrStride * kNbrGroup) + m % kNbrGroup);
+  }
 };
 __device__ __forceinline__ NbrList nbr_list(const WorldView& V, uint32_t k) {
   NbrList L;
@@ -60,24 +73,24 @@ __device__ __forceinline__ void prefetch_list(const NbrList& L, uint32_t cnt) {
   const uint32_t most = __reduce_max_sync(act, cnt);
   if (most && (threadIdx.x & 31u) == (uint32_t)(__ffs(act) - 1)) {
     const uint32_t lane = threadIdx.x & 31u;
-    const void* base = L.wide() ? (const void*)(L.w32 - lane) : (const void*)(L.w16 - lane);
-    const uint32_t bytes = most * kNbrStride * (L.wide() ? 4u : 2u);
+    const void* base = L.wide() ? (const void*)(L.w32 - lane) : (const void*)(L.w16 - lane * kNbrGroup);
+    const uint32_t bytes = L.wide() ? most * kNbrStride * 4u : div_up(most, kNbrGroup) * kNbrStride * kNbrGroup * 2u;
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base), "r"(bytes) : "memory");
   }
 }
 
-// Walks list entries [0, cnt) (entry(m) gives the m-th neighbour's slot), kU
-// per round, in list order: a round gathers its neighbours' records (fetch),
-// then fetches the next round's list entries, then uses the records (use).
-// The list entries come from DRAM and the records mostly from L1, so the
-// next round's entries are in flight while this round's records arrive and
-// are used. The last partial round is one batch as well.
-template <uint32_t kU, typename Entry, typename Fetch, typename Use>
-__device__ __forceinline__ void walk_list(Entry entry, uint32_t cnt, Fetch fetch, Use use) {
+// Walks list entries [0, cnt) (entries(m, j) gives the slots of entries m
+// to m + kU - 1, m a multiple of kU), kU per round, in list order: a round
+// gathers its neighbours' records (fetch), then fetches the next round's
+// list entries, then uses the records (use). The list entries come from
+// DRAM and the records mostly from L1, so the next round's entries are in
+// flight while this round's records arrive and are used. The last partial
+// round is one batch as well (its entries past cnt are read, not used).
+template <uint32_t kU, typename Entries, typename Fetch, typename Use>
+__device__ __forceinline__ void walk_list(Entries entries, uint32_t cnt, Fetch fetch, Use use) {
   using Rec = decltype(fetch(0u));
   uint32_t jn[kU];
-#pragma unroll
-  for (uint32_t q = 0; q < kU; ++q) jn[q] = q < cnt ? entry(q) : 0u;
+  if (cnt) entries(0u, jn);
   uint32_t m = 0;
   for (; m + kU <= cnt; m += kU) {
     uint32_t j[kU];
@@ -87,9 +100,7 @@ __device__ __forceinline__ void walk_list(Entry entry, uint32_t cnt, Fetch fetch
       j[q] = jn[q];
       r[q] = fetch(j[q]);
     }
-#pragma unroll
-    for (uint32_t q = 0; q < kU; ++q)
-      if (m + kU + q < cnt) jn[q] = entry(m + kU + q);
+    if (m + kU < cnt) entries(m + kU, jn);
 #pragma unroll
     for (uint32_t q = 0; q < kU; ++q) use(j[q], r[q]);
   }
@@ -105,20 +116,40 @@ __device__ __forceinline__ void walk_list(Entry entry, uint32_t cnt, Fetch fetch
 }
 
 // walk_list over slot k's list in whichever width its warp stored (a
-// warp-uniform branch). kFresh: the list was written by this same thread in
-// this kernel, so its entries are read with plain (coherent) loads.
+// warp-uniform branch): 16-bit entries a group at a time. kFresh: the list
+// was written by this same thread in this kernel, so its entries are read
+// with plain (coherent) loads.
 template <uint32_t kU, bool kFresh = false, typename Fetch, typename Use>
 __device__ __forceinline__ void walk_nbrs(const NbrList& L, uint32_t cnt, Fetch fetch, Use use) {
+  static_assert(kNbrGroup % kU == 0, "a round lies in one group");
   if (L.wide()) {
     const uint32_t* p = L.w32;
-    walk_list<kU>([&](uint32_t m) { return kFresh ? p[m * kNbrStride] : ld_entry(p + m * kNbrStride); }, cnt, fetch,
-                  use);
+    walk_list<kU>(
+        [&](uint32_t m, uint32_t(&j)[kU]) {
+#pragma unroll
+          for (uint32_t q = 0; q < kU; ++q) j[q] = kFresh ? p[(m + q) * kNbrStride] : ld_entry(p + (m + q) * kNbrStride);
+        },
+        cnt, fetch, use);
   } else {
     const uint16_t* p = L.w16;
     const uint32_t b = L.base;
     walk_list<kU>(
-        [&](uint32_t m) { return b + (kFresh ? (uint32_t)p[m * kNbrStride] : ld_entry(p + m * kNbrStride)); }, cnt,
-        fetch, use);
+        [&](uint32_t m, uint32_t(&j)[kU]) {
+          const uint16_t* g = p + (m / kNbrGroup) * (kNbrStride * kNbrGroup) + m % kNbrGroup;
+          uint32_t w[kU / 2];
+          if (kFresh) {
+#pragma unroll
+            for (uint32_t q = 0; q < kU / 2; ++q) w[q] = reinterpret_cast<const uint32_t*>(g)[q];
+          } else {
+            ld_group<kU>(g, w);
+          }
+#pragma unroll
+          for (uint32_t q = 0; q < kU / 2; ++q) {
+            j[2 * q] = b + (w[q] & 0xffffu);
+            j[2 * q + 1] = b + (w[q] >> 16);
+          }
+        },
+        cnt, fetch, use);
   }
 }
 
@@ -278,18 +309,19 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   // stored (as the reference's list keeps them) and any further hit only
   // marks the overflow. The walk is compiled once per entry width (the width
   // is uniform over the warp), and a 16-bit entry is stored without a branch
-  // on the count: hits past the kMaxNbr-th land in entry kMaxNbr of the
-  // block, which the 16-bit layout leaves unused (a 16-bit block has room
-  // for 2 kMaxNbr entries per slot).
+  // on the count: hits past the kMaxNbr-th land in the group after the last,
+  // which the 16-bit layout leaves unused (a block has room for 2 kMaxNbr
+  // entries per slot).
   uint32_t cnt = 0;
   uint32_t* __restrict__ out = V.nbr + nbr_col(k);
   uint16_t* __restrict__ out16 = reinterpret_cast<uint16_t*>(V.nbr) + nbr16_col(k);
   auto walk = [&](auto narrow_tag) {
     constexpr bool kNarrow = decltype(narrow_tag)::value;
     auto test = [&](uint32_t j, float4 xj) {
-      const bool hit = dot_rn(xi - xyz(xj)) < hsq;
+      const bool hit = dist2_rn(xi, xj) < hsq;
       if (kNarrow) {
-        if (hit) out16[min(cnt, kMaxNbr) * kNbrStride] = (uint16_t)(j - base);
+        if (hit)
+          out16[(min(cnt, kMaxNbr) / kNbrGroup) * (kNbrStride * kNbrGroup) + cnt % kNbrGroup] = (uint16_t)(j - base);
       } else {
         if (hit && cnt < kMaxNbr) out[cnt * kNbrStride] = j;
       }
@@ -642,7 +674,7 @@ __global__ void k_s_impulses(WorldView V, uint32_t rank, uint32_t sub) {
   const uint32_t cnt = V.ncount[k];
   const NbrList nl = nbr_list(V, k);
   for (uint32_t m = 0; m < cnt; ++m) {
-    const uint32_t j = nl.wide() ? __ldg(nl.w32 + m * kNbrStride) : nl.base + __ldg(nl.w16 + m * kNbrStride);
+    const uint32_t j = nl.entry(m);
     const f3 off = xi - xyz(__ldg(V.cur.xs + j));
     if (F.has_st) {
       const uint32_t idj = V.ids[j];
