@@ -113,7 +113,7 @@ def test_auto_bounds_step_time_matches_explicit_bounds(cuda):
     assert mb <= 1.10 * ma, (ma, mb)
 
 
-def test_window_grows_instead_of_clamping(cuda):
+def test_window_grows_instead_of_clamping(cuda, monkeypatch):
     """A dam break whose explicit window holds only the fluid block, which
     the fluid outgrows within frames (and whose splash leaves through the
     open top), widens its window between steps instead of clamping: no
@@ -123,8 +123,7 @@ def test_window_grows_instead_of_clamping(cuda):
     autotuner could otherwise pick the warp-tile path for one window size
     and not the other, and the two paths agree within tolerance, not bit
     for bit."""
-    import os
-
+    monkeypatch.setenv("PFSIM_NBR_PATH", "0")
     r = W.dam_break(20000, seed=25)
     h = r.materials[0][1].smoothing_radius
     small, big = copy.deepcopy(r), copy.deepcopy(r)
@@ -132,18 +131,10 @@ def test_window_grows_instead_of_clamping(cuda):
     small.loop.grid_max = (-0.1 + 2 * h, 0.5 + 2 * h, 0.3 + 2 * h)
     big.loop.grid_min = (-0.5 - 2 * h, -2 * h, -0.3 - 2 * h)
     big.loop.grid_max = (0.5 + 2 * h, 12.0, 0.3 + 2 * h)
-    old = os.environ.get("PFSIM_NBR_PATH")
-    os.environ["PFSIM_NBR_PATH"] = "0"
-    try:
-        a, b = cuda.build(small), cuda.build(big)
-        for _ in range(60):
-            a.step(DT)
-            b.step(DT)
-    finally:
-        if old is None:
-            del os.environ["PFSIM_NBR_PATH"]
-        else:
-            os.environ["PFSIM_NBR_PATH"] = old
+    a, b = cuda.build(small), cuda.build(big)
+    for _ in range(60):
+        a.step(DT)
+        b.step(DT)
     assert not a.overflow()["grid_clamped"] and not b.overflow()["grid_clamped"]
     assert np.array_equal(a.readback(N.PF_FIELD_POSITIONS), b.readback(N.PF_FIELD_POSITIONS))
     assert np.array_equal(a.readback(N.PF_FIELD_VELOCITIES), b.readback(N.PF_FIELD_VELOCITIES))
