@@ -115,6 +115,22 @@ class SortWorkload:
 
         return W.sort_uniform(self.n, seed) if self.dist == "uniform" else W.sort_blobs(self.n, seed)
 
+    # DRAM bytes per particle of one sort of this workload (uniform), the sum
+    # of dram__bytes_read.sum + dram__bytes_write.sum over a sort's launches
+    # from a one-pass ncu capture:
+    #   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,
+    #       dram__bytes_write.sum --clock-control none -s 40 -c 60 --csv
+    #       python bench.py --workload sort --steps 3 --warmup 3
+    #       --no-cpu-baseline
+    TRAFFIC_PER_PARTICLE = 63.4
+
+    def launches(self) -> int:
+        """Kernel launches of one sort: keys with digit counts, digit starts,
+        per radix pass (digits of at most 8 bits) tile counts, two tile-count
+        scans and the scatter, then the start scan."""
+        bits = max(1, (self.cells - 1).bit_length())
+        return 2 + 4 * -(-bits // 8) + 1
+
     def algorithmic_bytes(self) -> int:
         # read x (16 B) + write perm (4 B) per particle; start + count (8 B) per cell
         return 20 * self.n + 8 * self.cells
@@ -199,9 +215,12 @@ class SortWorkload:
             "ms": ms,
             "units_per_step": self.n,
             "kernel_ms": ms,
-            "kernel_name": "grid sort pipeline (keys + digit counts, LSD radix passes with look-back, run counts, start scan)",
+            "kernel_name": "grid sort pipeline (keys with digit counts, digit starts, LSD radix passes of "
+                           "tile counts + two tile-count scans + scatter, the last also counting the cells, "
+                           "start scan)",
             "algorithmic_bytes": self.algorithmic_bytes(),
-            "gpu_launches_per_step": 6,  # keys + digit counts, digit starts, 2 radix passes, run counts, start scan
+            "traffic": self.TRAFFIC_PER_PARTICLE * self.n if self.dist == "uniform" else None,
+            "gpu_launches_per_step": self.launches(),
             "clocks": clk,
             "e2e_ms": e2e_ms,
             "h2d": 16 * self.n,
@@ -259,7 +278,7 @@ class BatchWorkload:
     #       dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
     #       -k regex:k_s_ -c 44 --csv python bench.py --steps 20 --warmup 3
     #       --no-cpu-baseline --no-plain --no-serve
-    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {0: 158.9, 1: 123.3, 2: 164.9, 3: 136.0}
+    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {0: 151.1, 1: 127.6, 2: 168.9, 3: 140.0}
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes

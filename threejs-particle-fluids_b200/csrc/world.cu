@@ -150,40 +150,25 @@ __global__ void __launch_bounds__(kBlock) k_keys(WorldView V, DigitHist h) {
   extern __shared__ uint32_t sh[];
   digit_hist_zero(sh, h);
   __syncthreads();
-  constexpr uint32_t kU = 4;  // slots in flight per thread before their keys
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < V.n; k0 += kU * stride) {
-    float4 xs[kU];
-    uint32_t ids[kU];
-#pragma unroll
-    for (uint32_t q = 0; q < kU; ++q)
-      if (k0 + q * stride < V.n) {
-        xs[q] = V.cur.xs[k0 + q * stride];
-        ids[q] = V.ids[k0 + q * stride];
-      }
-#pragma unroll
-    for (uint32_t q = 0; q < kU; ++q) {
-      const uint32_t k = k0 + q * stride;
-      if (k >= V.n) break;
-      const uint32_t s = scene_index(V, k);
-      const DevScene& S = V.scenes[s];
-      const uint32_t id = ids[q];
-      uint32_t key;
-      bool clamped = false, ref_over = false;
-      if (id >= S.seg_start + S.cap) {
-        key = S.cell_base + S.cells;
-      } else if (S.has_grid) {
-        int32_t cx, cy, cz;
-        local_cell(S, xyz(xs[q]), &cx, &cy, &cz, &clamped, &ref_over);
-        key = S.cell_base + (uint32_t)cx + S.dims[0] * ((uint32_t)cy + S.dims[1] * (uint32_t)cz);
-      } else {
-        key = S.cell_base + (id - S.seg_start);
-      }
-      V.keys[id] = key;
-      digit_hist_add(sh, h, key);
-      if (clamped) atomicOr(V.flags + s * kNumFlags + FLAG_CLAMP, 1u);
-      if (ref_over) atomicOr(V.flags + s * kNumFlags + FLAG_GRID, 1u);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < V.n; k += gridDim.x * blockDim.x) {
+    const uint32_t s = scene_index(V, k);
+    const DevScene& S = V.scenes[s];
+    const uint32_t id = V.ids[k];
+    uint32_t key;
+    bool clamped = false, ref_over = false;
+    if (id >= S.seg_start + S.cap) {
+      key = S.cell_base + S.cells;
+    } else if (S.has_grid) {
+      int32_t cx, cy, cz;
+      local_cell(S, xyz(V.cur.xs[k]), &cx, &cy, &cz, &clamped, &ref_over);
+      key = S.cell_base + (uint32_t)cx + S.dims[0] * ((uint32_t)cy + S.dims[1] * (uint32_t)cz);
+    } else {
+      key = S.cell_base + (id - S.seg_start);
     }
+    V.keys[id] = key;
+    digit_hist_add(sh, h, key);
+    if (clamped) atomicOr(V.flags + s * kNumFlags + FLAG_CLAMP, 1u);
+    if (ref_over) atomicOr(V.flags + s * kNumFlags + FLAG_GRID, 1u);
   }
   __syncthreads();
   digit_hist_flush(sh, h);
