@@ -344,8 +344,8 @@ class BatchWorkload:
             N.check(L.pf_batch_profile_stage(batch.h, sid, 10, C.byref(st_ms), C.byref(items)))
             stages[sid] = st_ms.value
         torch.cuda.nvtx.range_pop()
-        tp, tb, tu, tg = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
-        N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu), C.byref(tg)))
+        tp, tb, tu, tg, te = (C.c_uint32(0) for _ in range(5))
+        N.check(L.pf_batch_tuning(batch.h, C.byref(tp), C.byref(tb), C.byref(tu), C.byref(tg), C.byref(te)))
         # ---- end to end: per step the scene parameters go host->device (pinned)
         # and every scene's positions come back to pinned host memory
         total = sum(r.capacity for r in recipes)
@@ -406,7 +406,8 @@ class BatchWorkload:
                             "ms_per_step": stages[sid] * per_step[sid],
                             "share_of_step": stages[sid] * per_step[sid] / ms,
                             "bytes_per_fluid_particle": bpp, "achieved_gbs": gbs, "frac": gbs / peak,
-                            "dram_bytes_per_fluid_particle": self.STAGE_TRAFFIC_PER_PARTICLE.get(sid)}
+                            "dram_bytes_per_fluid_particle": (self.STAGE_TRAFFIC_PER_PARTICLE.get(sid)
+                                                              if te.value == 16 else None)}
         dom = max(self.STAGES, key=lambda sid: stages[sid] * per_step[sid])
         tpp = self.STAGE_TRAFFIC_PER_PARTICLE.get(dom)
         return {
@@ -415,7 +416,8 @@ class BatchWorkload:
             "kernel_ms": stages[dom],
             "kernel_name": self.STAGES[dom][0] + (" (warp-tile path)" if tp.value == 1 else " (slot path)"),
             "algorithmic_bytes": self.STAGES[dom][1] * items.value,
-            "traffic": tpp * items.value if (tpp is not None and tp.value == 0) else None,
+            # the captured figures are of the slot path with 16-bit list entries
+            "traffic": tpp * items.value if (tpp is not None and tp.value == 0 and te.value == 16) else None,
             "stages": table,
             "gpu_launches_per_step": launches,
             "clocks": clk,
@@ -432,7 +434,7 @@ class BatchWorkload:
                 "plain_overlapped_ms_per_step": overlap_ms,
                 "batched_over_plain_overlapped": overlap_ms / ms,
                 "tuning": {"nbr_path": "tiles" if tp.value == 1 else "slots", "block": tb.value,
-                           "fetch_depth": tu.value, "l2_group_particles": tg.value},
+                           "fetch_depth": tu.value, "l2_group_particles": tg.value, "list_entry_bits": te.value},
                 "scenes": len(recipes),
                 "particles": total,
                 "fluid_particles": int(items.value),

@@ -509,9 +509,12 @@ PF_API pf_status pf_batch_profile_stage(pf_batch* batch, uint32_t stage, uint32_
  * entries fetched `unroll` at a time), 1 = warp tiles. `group` (may be NULL)
  * receives the fluid particles per group of the scenes that hold only one
  * fluid of one mass, stepped group by group so that a group's lists stay in
- * L2 across its passes (0: one launch per pass over all of them). */
+ * L2 across its passes (0: one launch per pass over all of them).
+ * `entry_bits` (may be NULL) receives the width of the list entries: 16
+ * (offsets from a per-warp base where a warp's rows allow it) or 32 (whole
+ * slots in every warp). */
 PF_API pf_status pf_batch_tuning(pf_batch* batch, uint32_t* path, uint32_t* block, uint32_t* unroll,
-                                 uint32_t* group);
+                                 uint32_t* group, uint32_t* entry_bits);
 
 /* ------------------------------------------------------------------------ */
 /* Mesh -> particle setup on the GPU                                          */

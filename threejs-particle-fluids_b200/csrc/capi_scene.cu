@@ -983,10 +983,12 @@ pf_status pf_batch_read_positions(pf_batch* b, float* dst_host, size_t bytes) {
   return b->world->read_positions(dst_host, bytes);
 }
 
-pf_status pf_batch_tuning(pf_batch* b, uint32_t* path, uint32_t* block, uint32_t* unroll, uint32_t* group) {
+pf_status pf_batch_tuning(pf_batch* b, uint32_t* path, uint32_t* block, uint32_t* unroll, uint32_t* group,
+                          uint32_t* entry_bits) {
   if (!b || !path || !block || !unroll) return fail(PF_ERR_INVALID, "batch: NULL");
   b->world->tuning(path, block, unroll);
   if (group) *group = b->world->tuning_all().group;
+  if (entry_bits) *entry_bits = b->world->tuning_all().nbr_wide ? 32u : 16u;
   return PF_OK;
 }
 

@@ -338,9 +338,12 @@ k_tile_counts(const uint32_t* __restrict__ kin, uint32_t n, uint32_t shift, uint
 }
 
 // Per digit (one thread each), the exclusive running sum over the tiles of
-// chunk blockIdx.x, in place, and the chunk's total into `csum`.
+// chunk blockIdx.x, in place, and the chunk's total into `csum`. With
+// `first` (a pass of one chunk), csum gets the digit's first output position
+// instead, so no scan over the chunks is needed.
 __global__ void __launch_bounds__(256)
-k_tile_scan_chunk(uint32_t* __restrict__ tcount, uint32_t tiles, uint32_t digits, uint32_t* __restrict__ csum) {
+k_tile_scan_chunk(uint32_t* __restrict__ tcount, uint32_t tiles, uint32_t digits, uint32_t* __restrict__ csum,
+                  const uint32_t* __restrict__ first) {
   const uint32_t d = blockIdx.y * blockDim.x + threadIdx.x;
   if (d >= digits) return;
   const uint32_t t0 = blockIdx.x * kScanChunk, t1 = min(t0 + kScanChunk, tiles);
@@ -353,7 +356,7 @@ k_tile_scan_chunk(uint32_t* __restrict__ tcount, uint32_t tiles, uint32_t digits
     if (t0 + q < t1) tcount[(size_t)(t0 + q) * digits + d] = run;
     run += v[q];
   }
-  csum[(size_t)blockIdx.x * digits + d] = run;
+  csum[(size_t)blockIdx.x * digits + d] = first ? first[d] : run;
 }
 
 // Per digit (one warp each, 32 chunks per round), the chunk totals -> each
@@ -861,7 +864,9 @@ cudaError_t scatter_allow_smem_all() {
 uint32_t grid_sort_launches(const RadixPlan& plan, uint32_t n) {
   if (n == 0) return 1;                        // the start scan
   if (plan.passes == 0) return 3;              // identity, run counts, start scan
-  return 1 + 4 * plan.passes + 1;              // digit scan, per pass four, start scan
+  // digit scan, per pass four (three when the tiles form one chunk), start scan
+  const uint32_t per_pass = div_up(radix_tiles(n), kScanChunk) > 1 ? 4u : 3u;
+  return 1 + per_pass * plan.passes + 1;
 }
 
 cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const RadixPlan& plan, uint32_t* count,
@@ -889,10 +894,11 @@ cudaError_t launch_grid_sort(const uint32_t* keys, uint32_t n, uint64_t C, const
         const uint32_t shift = p * plan.width;
         k_tile_counts<<<tiles, kCountThreads, 0, st>>>(kin, n, shift, plan.digits, s.tcount,
                                                        (first ? kvec : true) ? 1u : 0u);
-        k_tile_scan_chunk<<<dim3(chunks, div_up(plan.digits, 256)), 256, 0, st>>>(s.tcount, tiles, plan.digits,
-                                                                                   s.csum);
-        k_tile_scan_chunks<<<div_up(plan.digits, 8), 256, 0, st>>>(s.csum, chunks, plan.digits,
-                                                                 s.digit_count + p * kRadixMaxDigits);
+        const uint32_t* first_pos = s.digit_count + p * kRadixMaxDigits;
+        k_tile_scan_chunk<<<dim3(chunks, div_up(plan.digits, 256)), 256, 0, st>>>(
+            s.tcount, tiles, plan.digits, s.csum, chunks == 1 ? first_pos : nullptr);
+        if (chunks > 1)
+          k_tile_scan_chunks<<<div_up(plan.digits, 8), 256, 0, st>>>(s.csum, chunks, plan.digits, first_pos);
         cudaError_t e;
         if (first && last)
           e = launch_scatter<true, true>(kin, vin, n, kout, vout, shift, plan, s, count, st);

@@ -384,6 +384,8 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
   uint32_t s = 0, mask = 0;
   int4 start = make_int4(0, 0, 0, 0);
   if (k < V.n) {
+    // the slot's contact mask goes out with the scene lookup, not after it
+    const uint32_t m = V.cmask[k];
     s = scene_index(V, k);
     const DevScene& S0 = V.scenes[s];
     if ((S0.prim_count + S0.sdf_count > 0 || S0.contact) && sub < S0.substeps) {
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(kBlock) k_friction(WorldView V, uint32_t sub) 
         start = V.acc_con[k];
         if (start.x | start.y | start.z) V.acc_con[k] = make_int4(0, 0, 0, 0);
       }
-      mask = V.cmask[k];
+      mask = m;
       work = mask || S0.prim_count + S0.sdf_count > 32 || (start.x | start.y | start.z);
     }
   }
@@ -1080,7 +1082,6 @@ World::~World() {
   drop_graphs();
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
-  if (ev_bbox_) cudaEventDestroy(ev_bbox_);
   if (ev_params_) cudaEventDestroy(ev_params_);
   if (h_pinned_bbox_) cudaFreeHost(h_pinned_bbox_);
   if (grid_arena_) cudaFree(grid_arena_);
@@ -1098,6 +1099,7 @@ World::~World() {
 
 WorldView World::view(uint32_t parity) const {
   WorldView v = base_;
+  v.nbr_wide_only = tune_.nbr_wide;
   v.cur = buf_[parity & 1];
   v.nxt = buf_[(parity & 1) ^ 1];
   return v;
@@ -1920,9 +1922,8 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   PF_CUDA(cudaEventCreate(&ev0_));
   PF_CUDA(cudaEventCreate(&ev1_));
-  PF_CUDA(cudaEventCreateWithFlags(&ev_bbox_, cudaEventDisableTiming));
   PF_CUDA(cudaEventCreateWithFlags(&ev_params_, cudaEventDisableTiming));
-  PF_CUDA(cudaMallocHost(&h_pinned_bbox_, sizeof(int32_t) * 6 * std::max<size_t>(1, K)));
+  PF_CUDA(cudaMallocHost(&h_pinned_bbox_, sizeof(int32_t) * 12 * std::max<size_t>(1, K)));  // two steps
   PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_plane4_, sizeof(float4) * 2 * std::max<size_t>(1, h_prims_.size())));
@@ -2348,9 +2349,12 @@ void World::run_groups(const WorldView& V, uint32_t s, bool apply) {
 // substep would do; the permutation is canonical, so no result changes),
 // time each slot kernel (list build, density + lambda, position correction,
 // XSPH) at every block size and fetch depth and keep each kernel's fastest;
-// then time one substep's worth of the warp-tile path against the tuned slot
-// path and keep the faster. The passes write only per-substep scratch (lists,
-// lambda, density, deltas), which every substep rebuilds.
+// then one substep's slot passes with 16-bit and with 32-bit list entries,
+// and keep the faster; then time one substep's worth of the warp-tile path
+// against the tuned slot path and keep the faster. The passes write only
+// per-substep scratch (lists, lambda, density, deltas), which every substep
+// rebuilds; none moves a predicted position (the warp-tile trial needs them
+// where the sort saw them).
 pf_status World::tune() {
   tuned_ = true;
   if (!any_fluid_ || n_ == 0) return PF_OK;
@@ -2369,6 +2373,8 @@ pf_status World::tune() {
     if (const char* g = std::getenv("PFSIM_GROUP")) tune_.group = (uint32_t)std::atoi(g);
     tune_.nbr_flat = 0;
     if (const char* fl = std::getenv("PFSIM_NBR_FLAT")) tune_.nbr_flat = std::atoi(fl) ? 1u : 0u;
+    tune_.nbr_wide = 0;
+    if (const char* nw = std::getenv("PFSIM_NBR_WIDE")) tune_.nbr_wide = std::atoi(nw) ? 1u : 0u;
     apply_grouping();
     return PF_OK;
   }
@@ -2457,6 +2463,30 @@ pf_status World::tune() {
     }
     tune_.group = best_g;
     apply_grouping();
+  }
+  // the list's entry width: one substep's slot passes timed with 16-bit
+  // offsets (where a warp's rows allow them) and with 32-bit slots. As in
+  // the trials above, the position pass only forms its corrections (no
+  // apply): the tuner leaves the predicted positions as the sort saw them,
+  // which the warp-tile trial below relies on (its halo rows come from the
+  // sorted cells).
+  {
+    auto substep = [&] {
+      const WorldView W = view(parity_);
+      PF_NBR(W, 0u);
+      for (uint32_t it = 0; it < iters; ++it) {
+        if (!(fuse_dens_ && it == 0)) PF_BY_UNROLL(kSlotLambda, k_s_lambda, W, rank, 0u, 0u);
+        PF_DELTA(W, rank, 0u, 0u, 0u);
+      }
+      if (vel) PF_XSPH(W, rank, 0u);
+    };
+    float t16 = 0, t32 = 0;
+    tune_.nbr_wide = 0;
+    PF_TRY(timed(substep, &t16));
+    tune_.nbr_wide = 1;
+    PF_TRY(timed(substep, &t32));
+    tune_.nbr_wide = t32 < t16 ? 1u : 0u;
+    slot_total = std::min(t16, t32);
   }
   // the warp-tile path has no vorticity or surface pass and reads one shared
   // lambda buffer: worlds with those, or with a scene of several fluids,
@@ -2681,6 +2711,9 @@ void World::run_substep(uint32_t s, uint32_t parity) {
 pf_status World::step(double dt) {
   if (!(dt > 0) || !std::isfinite(dt))
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
+  // the previous step's parameter copies have run, so everything queued
+  // before them has too (the bounds maybe_grow_windows reads among it)
+  if (params_pending_) PF_CUDA(cudaEventSynchronize(ev_params_));
   PF_TRY(maybe_grow_windows());
   PF_TRY(upload_params(dt));
   PF_CUDA(cudaEventRecord(ev0_, stream_));
@@ -2742,31 +2775,32 @@ pf_status World::step(double dt) {
   parity_ ^= flips;
   PF_CUDA(cudaEventRecord(ev1_, stream_));
   if (any_grid_) {
-    PF_CUDA(cudaMemcpyAsync(h_pinned_bbox_, base_.bbox_last, sizeof(int32_t) * 6 * h_scenes_.size(),
+    // this step's bounds, into the buffer of its parity; the step two later
+    // reads them (by then they have surely arrived)
+    const size_t K6 = 6 * h_scenes_.size();
+    PF_CUDA(cudaMemcpyAsync(h_pinned_bbox_ + K6 * (steps_done_ & 1), base_.bbox_last, sizeof(int32_t) * K6,
                             cudaMemcpyDeviceToHost, stream_));
-    PF_CUDA(cudaEventRecord(ev_bbox_, stream_));
-    bbox_pending_ = true;
   }
+  ++steps_done_;
   PF_CUDA(cudaGetLastError());
   return PF_OK;
 }
 
-// Between steps: a grid scene whose particles' cell bounds (as the last
-// window fit saw them) come within a margin of its window's size on some
-// axis gets a window twice their spread there, centred on them, so it never
-// has to clamp (the reference's hash grid is unbounded). Windows past 2^27
-// cells stay as they are (their keys clamp and flag).
+// Before a step: a grid scene whose particles' cell bounds (as the window
+// fit of the step two before saw them: the wait on the last parameter upload
+// has made sure they arrived) come within a margin of its window's size on
+// some axis gets a window twice their spread there, centred on them, so it
+// never has to clamp (the reference's hash grid is unbounded). The margin
+// covers the two steps since those bounds. Windows past 2^27 cells stay as
+// they are (their keys clamp and flag).
 pf_status World::maybe_grow_windows() {
-  if (!bbox_pending_) return PF_OK;
-  const cudaError_t q = cudaEventQuery(ev_bbox_);
-  if (q == cudaErrorNotReady) return PF_OK;  // the last step still runs: look before the next one
-  PF_CUDA(q);
-  bbox_pending_ = false;
+  if (!any_grid_ || steps_done_ < 2) return PF_OK;
+  const int32_t* seen = h_pinned_bbox_ + 6 * h_scenes_.size() * (steps_done_ & 1);  // step steps_done_ - 2
   bool any = false;
   for (uint32_t s = 0; s < h_scenes_.size(); ++s) {
     DevScene& S = h_scenes_[s];
     if (!S.has_grid) continue;
-    const int32_t* b = h_pinned_bbox_ + 6 * s;
+    const int32_t* b = seen + 6 * s;
     int64_t lo[3], dims[3];
     bool grow = false;
     for (int a = 0; a < 3; ++a) {
@@ -2774,13 +2808,14 @@ pf_status World::maybe_grow_windows() {
       lo[a] = S.lo0[a];
       dims[a] = d;
       if (mn > mx) continue;  // no particle
-      // within two cells of clamping, plus twice the spread's growth since
-      // the last look (a fluid that walls hold stops growing there)
+      // within two cells of clamping, plus three times the spread's growth
+      // per step (the two steps since these bounds, and one more); a fluid
+      // that walls hold stops growing there
       const int64_t ext = mx - mn + 1;
       int32_t& prev = grow_prev_ext_[3 * s + a];
       const int64_t rate = prev > 0 ? std::max<int64_t>(0, ext - prev) : 0;
       prev = (int32_t)ext;
-      if (ext + 2 * rate + 4 <= d) continue;
+      if (ext + 3 * rate + 4 <= d) continue;
       dims[a] = std::max<int64_t>(d, 2 * ext + 8);
       lo[a] = ((mn + mx) >> 1) - dims[a] / 2;
       grow = true;

@@ -315,6 +315,7 @@ struct WorldView {
   uint32_t* ccount;
   uint32_t* nbr;      // kMaxNbr * n, blocked by warp: 16- or 32-bit entries (slot path)
   uint32_t* nbr_base; // per warp of slots: base slot of its 16-bit entries, or kNbrWide
+  uint32_t nbr_wide_only;  // the list build stores whole 32-bit slots for every warp (a tuned choice)
   uint16_t* nbr16;    // the same storage, kMaxNbr * n halfwords: halo index of each neighbour (tile path)
   uint32_t* ncount;
   uint32_t* slot_tile;  // tile of each slot (this substep)
@@ -479,6 +480,9 @@ class World {
     uint32_t group = 0;
     // the list build walks its nine rows as one sequence (k_s_neighbors kFlat)
     uint32_t nbr_flat = 0;
+    // list entries as whole 32-bit slots in every warp instead of 16-bit
+    // offsets where they fit: fewer bytes against fewer decode instructions
+    uint32_t nbr_wide = 0;
   };
   void tuning(uint32_t* path, uint32_t* block, uint32_t* unroll = nullptr) const {
     *path = tune_.path;
@@ -605,12 +609,11 @@ class World {
   uint64_t launches_per_step_ = 0;
   std::vector<uint64_t> prefix_;   // particle offset of each scene in read_positions
   // Grid windows grow with their particles: after each step the last window
-  // fit's cell bounds come back to pinned memory, and before the next step
-  // any window they have nearly outgrown is widened and the cell arrays laid
-  // out again (outside any graph).
-  int32_t* h_pinned_bbox_ = nullptr;
-  cudaEvent_t ev_bbox_ = nullptr;
-  bool bbox_pending_ = false;
+  // fit's cell bounds come back to pinned memory, and two steps later any
+  // window they have nearly outgrown is widened and the cell arrays laid out
+  // again (outside any graph).
+  int32_t* h_pinned_bbox_ = nullptr;  // two buffers of 6 words per scene, by step parity
+  uint64_t steps_done_ = 0;
   // the previous parameter upload, waited on before its pinned staging is
   // written again
   cudaEvent_t ev_params_ = nullptr;

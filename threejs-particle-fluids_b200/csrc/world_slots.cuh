@@ -301,7 +301,7 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   }
   lo = __reduce_min_sync(0xffffffffu, lo);
   hi = __reduce_max_sync(0xffffffffu, hi);
-  const bool narrow = hi <= lo || hi - lo <= 65536u;
+  const bool narrow = !V.nbr_wide_only && (hi <= lo || hi - lo <= 65536u);
   const uint32_t base = narrow ? (hi > lo ? lo : 0u) : kNbrWide;
   if ((threadIdx.x & 31u) == 0) V.nbr_base[k >> 5] = base;
   if (!f) return;

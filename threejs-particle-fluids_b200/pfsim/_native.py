@@ -324,7 +324,7 @@ SIGNATURES = {
     "pf_batch_create": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(BatchOpts), C.POINTER(_P)]),
     "pf_add_sdf_collider": (C.c_int, [_P, C.POINTER(SdfDesc), _u32p]),
     "pf_set_sdf_transform": (C.c_int, [_P, C.c_uint32, _f32p, _f32p, C.c_float]),
-    "pf_batch_tuning": (C.c_int, [_P, _u32p, _u32p, _u32p, _u32p]),
+    "pf_batch_tuning": (C.c_int, [_P, _u32p, _u32p, _u32p, _u32p, _u32p]),
     "pf_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(_P)]),
     "pf_server_destroy": (None, [_P]),
     "pf_server_submit": (C.c_int, [_P, _P, C.POINTER(LoopDesc), C.c_uint32, C.POINTER(C.c_uint64)]),
