@@ -278,7 +278,12 @@ class BatchWorkload:
     #       dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
     #       -k regex:k_s_ -c 44 --csv python bench.py --steps 20 --warmup 3
     #       --no-cpu-baseline --no-plain --no-serve
-    STAGE_TRAFFIC_PER_PARTICLE: dict[int, float] = {0: 151.1, 1: 127.6, 2: 168.9, 3: 140.0}
+    # (PFSIM_NBR_WIDE=0 or 1 fixes the list entry width the autotuner would
+    # pick, for the figures of the other width). Keyed by that width in bits.
+    STAGE_TRAFFIC_PER_PARTICLE: dict[int, dict[int, float]] = {
+        16: {0: 151.1, 1: 127.6, 2: 168.9, 3: 140.0},
+        32: {0: 286.6, 1: 207.6, 2: 248.8, 3: 216.1},
+    }
 
     def __init__(self, n_scenes: int = 256):
         self.n_scenes = n_scenes
@@ -400,24 +405,24 @@ class BatchWorkload:
         plain = None
         peak, _ = hbm_peak()
         table = {}
+        traffic = self.STAGE_TRAFFIC_PER_PARTICLE.get(te.value, {})
         for sid, (label, bpp) in self.STAGES.items():
             gbs = bpp * items.value / (stages[sid] * 1e-3) / 1e9
             table[label] = {"ms_per_launch": stages[sid], "launches_per_step": per_step[sid],
                             "ms_per_step": stages[sid] * per_step[sid],
                             "share_of_step": stages[sid] * per_step[sid] / ms,
                             "bytes_per_fluid_particle": bpp, "achieved_gbs": gbs, "frac": gbs / peak,
-                            "dram_bytes_per_fluid_particle": (self.STAGE_TRAFFIC_PER_PARTICLE.get(sid)
-                                                              if te.value == 16 else None)}
+                            "dram_bytes_per_fluid_particle": traffic.get(sid)}
         dom = max(self.STAGES, key=lambda sid: stages[sid] * per_step[sid])
-        tpp = self.STAGE_TRAFFIC_PER_PARTICLE.get(dom)
+        tpp = traffic.get(dom)
         return {
             "ms": ms,
             "units_per_step": psub,
             "kernel_ms": stages[dom],
             "kernel_name": self.STAGES[dom][0] + (" (warp-tile path)" if tp.value == 1 else " (slot path)"),
             "algorithmic_bytes": self.STAGES[dom][1] * items.value,
-            # the captured figures are of the slot path with 16-bit list entries
-            "traffic": tpp * items.value if (tpp is not None and tp.value == 0 and te.value == 16) else None,
+            # the captured figures are of the slot path
+            "traffic": tpp * items.value if (tpp is not None and tp.value == 0) else None,
             "stages": table,
             "gpu_launches_per_step": launches,
             "clocks": clk,

@@ -2485,8 +2485,10 @@ pf_status World::tune() {
     PF_TRY(timed(substep, &t16));
     tune_.nbr_wide = 1;
     PF_TRY(timed(substep, &t32));
-    tune_.nbr_wide = t32 < t16 ? 1u : 0u;
-    slot_total = std::min(t16, t32);
+    // 32-bit entries move half again as many bytes, so they must win
+    // clearly (a few per cent can be the noise of two timings)
+    tune_.nbr_wide = t32 < 0.97f * t16 ? 1u : 0u;
+    slot_total = tune_.nbr_wide ? t32 : t16;
   }
   // the warp-tile path has no vorticity or surface pass and reads one shared
   // lambda buffer: worlds with those, or with a scene of several fluids,
