@@ -12,6 +12,9 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cstdio>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -1031,6 +1034,13 @@ void launch_slots(K kernel, uint32_t n, cudaStream_t st, A... args) {
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// PFSIM_VERBOSE set: host-side events (grid window growth, graph captures)
+// and their times go to stderr.
+bool verbose() {
+  static const bool v = std::getenv("PFSIM_VERBOSE") != nullptr;
+  return v;
+}
+
 // The slot neighbour passes use no shared memory and gather their
 // neighbours' records through L1: each asks for the largest L1 (a hint the
 // runtime may round), once per device, outside any stream capture.
@@ -1085,6 +1095,7 @@ World::~World() {
   if (ev_params_) cudaEventDestroy(ev_params_);
   if (h_pinned_bbox_) cudaFreeHost(h_pinned_bbox_);
   if (grid_arena_) cudaFree(grid_arena_);
+  if (sort_arena_) cudaFree(sort_arena_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   if (side_stream_) cudaStreamDestroy(side_stream_);
@@ -1769,6 +1780,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     prefix_[s] = total_real;
     total_real += h_scenes_[s].cap;
   }
+  const uint64_t cell_room = std::min<uint64_t>(kSortCellCap, 2ull * cells_);
   auto layout = [&](Carver& cv) {
     base_.scenes_rw = cv.take<DevScene>(K);
     base_.chunk_scene = cv.take<uint32_t>(chunk.size());
@@ -1798,8 +1810,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.inv = cv.take<uint32_t>(N);
     base_.keys = cv.take<uint32_t>(N);
     base_.perm = cv.take<uint32_t>(N);
-    base_.cstart = cv.take<uint32_t>(cells_);
-    base_.ccount = cv.take<uint32_t>(cells_);
+    // room for the windows to double before the cell arrays move
+    base_.cstart = cv.take<uint32_t>(cell_room);
+    base_.ccount = cv.take<uint32_t>(cell_room);
     base_.nbr = any_fluid_ ? cv.take<uint32_t>(N * kMaxNbr) : nullptr;
     base_.nbr_base = any_fluid_ ? cv.take<uint32_t>(N / 32) : nullptr;
     base_.nbr16 = reinterpret_cast<uint16_t*>(base_.nbr);
@@ -1885,7 +1898,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   };
   Carver probe{nullptr};
   layout(probe);
-  const size_t sort_bytes = sort_scratch_bytes(n_, cells_);
+  // the sort scratch is carved for 64 times the cells (its cell-sized part
+  // is 1/512 byte per cell), so growing windows seldom re-allocate it
+  const uint64_t sort_cells = std::min<uint64_t>(kSortCellCap, std::max<uint64_t>(64ull * cells_, 1ull << 20));
+  const size_t sort_bytes = sort_scratch_bytes(n_, sort_cells);
   bytes_ = probe.off + al256(sort_bytes);
   if (plan_only) return PF_OK;
   (void)sm_count();  // cache the SM count outside any stream capture
@@ -1898,9 +1914,9 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   Carver cv{static_cast<char*>(arena_)};
   layout(cv);
-  sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, cells_, &sort_);
+  sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, sort_cells, &sort_);
   radix_ = radix_plan(cells_);
-  cells_cap_ = cells_;
+  cells_cap_ = cell_room;
   grow_prev_ext_.assign(3 * K, 0);
   base_.scenes = base_.scenes_rw;
   base_.n = n_;
@@ -2750,6 +2766,8 @@ pf_status World::step(double dt) {
       const uint32_t p = parities[i];
       cudaGraphExec_t& g = graph_[p];
       if (g && !graphs_stale_) continue;
+      const auto t_cap = std::chrono::steady_clock::now();
+      const bool updating = g != nullptr;
       cudaGraph_t graph;
       PF_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       body(p);
@@ -2763,10 +2781,15 @@ pf_status World::step(double dt) {
           g = nullptr;
         }
       }
+      const bool updated = updating && g;
       cudaError_t e = cudaSuccess;
       if (!g) e = cudaGraphInstantiate(&g, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) return fail(PF_ERR_CUDA, std::string("SimLoop: graph instantiate: ") + cudaGetErrorString(e));
+      if (verbose())
+        std::fprintf(stderr, "pfsim: step graph %s: %.2f ms\n",
+                     updated ? "updated" : (updating ? "instantiated again (update refused)" : "instantiated"),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_cap).count());
     }
     graphs_stale_ = false;
     PF_CUDA(cudaGraphLaunch(graph_[parity_], stream_));
@@ -2849,6 +2872,8 @@ pf_status World::maybe_grow_windows() {
 // rows, the cell arrays and sort scratch (a new block when the arena's are
 // too small), the radix plan; graphs are captured again on the next step.
 pf_status World::relayout_grid() {
+  const auto t_start = std::chrono::steady_clock::now();
+  const uint32_t cells_before = cells_;
   PF_CUDA(cudaStreamSynchronize(stream_));
   if (side_stream_) PF_CUDA(cudaStreamSynchronize(side_stream_));
   uint64_t cell = 0;
@@ -2856,7 +2881,7 @@ pf_status World::relayout_grid() {
     S.cell_base = (uint32_t)cell;
     cell += (uint64_t)S.cells + 1;
   }
-  if (cell > 0x7fffffffull) return fail(PF_ERR_INVALID, "SimLoop: grid windows over 2^31 cells");
+  if (cell > kSortCellCap) return fail(PF_ERR_INVALID, "SimLoop: grid windows over 2^31 - 1 cells");
   cells_ = (uint32_t)cell;
   std::vector<uint32_t> row_base(1, 0);
   for (auto& S : h_scenes_)
@@ -2865,28 +2890,46 @@ pf_status World::relayout_grid() {
                      cudaMemcpyHostToDevice));
   base_.n_rows = row_base.back();
   if (cells_ > cells_cap_) {
-    const uint64_t cap = std::min<uint64_t>(0x7fffffffull, (uint64_t)cells_ + cells_ / 4);
+    // new cell arrays with twice the room
+    const uint64_t cap = std::min<uint64_t>(kSortCellCap, 2ull * cells_);
     const size_t cell_bytes = al256(4ull * cap);
-    const size_t bytes = 2 * cell_bytes + al256(sort_scratch_bytes(n_, cap));
+    void* g = nullptr;
+    if (const cudaError_t e = cudaMalloc(&g, 2 * cell_bytes); e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,
+                  "SimLoop: growing the grid windows needs " + std::to_string(2 * cell_bytes) + " more bytes");
+    }
+    char* p = static_cast<char*>(g);
+    base_.cstart = reinterpret_cast<uint32_t*>(p);
+    base_.ccount = reinterpret_cast<uint32_t*>(p + cell_bytes);
+    if (grid_arena_) cudaFree(grid_arena_);
+    grid_arena_ = g;
+    bytes_ += 2 * cell_bytes;
+    cells_cap_ = cap;
+  }
+  if (cells_ > sort_.c_cap) {
+    // new sort scratch only once the windows pass the 64 times the cells the
+    // old one was carved for
+    const uint64_t sort_cells = std::min<uint64_t>(kSortCellCap, 64ull * cells_);
+    const size_t bytes = sort_scratch_bytes(n_, sort_cells);
     void* g = nullptr;
     if (const cudaError_t e = cudaMalloc(&g, bytes); e != cudaSuccess) {
       cudaGetLastError();
       return fail(e == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,
                   "SimLoop: growing the grid windows needs " + std::to_string(bytes) + " more bytes");
     }
-    char* p = static_cast<char*>(g);
-    base_.cstart = reinterpret_cast<uint32_t*>(p);
-    base_.ccount = reinterpret_cast<uint32_t*>(p + cell_bytes);
-    sort_scratch_carve(p + 2 * cell_bytes, n_, cap, &sort_);
-    if (grid_arena_) cudaFree(grid_arena_);
-    grid_arena_ = g;
+    sort_scratch_carve(g, n_, sort_cells, &sort_);
+    PF_CUDA(sort_scratch_zero(sort_, stream_));
+    if (sort_arena_) cudaFree(sort_arena_);
+    sort_arena_ = g;
     bytes_ += bytes;
-    cells_cap_ = cap;
   }
   radix_ = radix_plan(cells_);
-  PF_CUDA(sort_scratch_zero(sort_, stream_));
   ++regrowths_;
   graphs_stale_ = true;
+  if (verbose())
+    std::fprintf(stderr, "pfsim: grid windows grew: %u -> %u cells, %.2f ms\n", cells_before, cells_,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
   return PF_OK;
 }
 

@@ -58,6 +58,7 @@ __host__ __device__ __forceinline__ size_t nbr16_at(size_t k, uint32_t m) {
 }
 __host__ __device__ __forceinline__ size_t nbr16_col(size_t k) { return nbr16_at(k, 0); }
 constexpr uint32_t kBlock = 256;
+constexpr uint64_t kSortCellCap = 0x7fffffffull;  // keys of a world's sort stay below this
 constexpr uint32_t kMaxContacts = 32;  // contact pairs kept per emitting particle per substep
 
 // ------------------------------------------------------------- host spec ----
@@ -618,7 +619,8 @@ class World {
   // written again
   cudaEvent_t ev_params_ = nullptr;
   bool params_pending_ = false;
-  void* grid_arena_ = nullptr;  // cell arrays and sort scratch once the windows outgrow the arena's
+  void* grid_arena_ = nullptr;  // cell arrays once the windows outgrow the arena's
+  void* sort_arena_ = nullptr;  // sort scratch once the windows pass the cells it was carved for
   uint64_t cells_cap_ = 0;      // cells the current cell arrays and sort scratch hold
   std::vector<int32_t> grow_prev_ext_;  // per scene and axis: the spread in cells at the last look
   uint32_t regrowths_ = 0;

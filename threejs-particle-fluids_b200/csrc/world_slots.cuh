@@ -290,19 +290,24 @@ __global__ void k_s_neighbors(WorldView V, uint32_t sub) {
   }
   // The warp's entries are 16-bit offsets from the lowest slot its rows
   // reach when every reachable slot lies within 65,536 of it.
-  uint32_t lo = 0xffffffffu, hi = 0;
+  // (No reduction when the world keeps whole slots in every warp.)
+  bool narrow = false;
+  uint32_t base = kNbrWide;
+  if (!V.nbr_wide_only) {  // uniform over the launch
+    uint32_t lo = 0xffffffffu, hi = 0;
 #pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    if (!f) rs[r] = re[r] = 0;
-    if (re[r] > rs[r]) {
-      lo = min(lo, rs[r]);
-      hi = max(hi, re[r]);
+    for (int r = 0; r < 9; ++r) {
+      if (!f) rs[r] = re[r] = 0;
+      if (re[r] > rs[r]) {
+        lo = min(lo, rs[r]);
+        hi = max(hi, re[r]);
+      }
     }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    narrow = hi <= lo || hi - lo <= 65536u;
+    base = narrow ? (hi > lo ? lo : 0u) : kNbrWide;
   }
-  lo = __reduce_min_sync(0xffffffffu, lo);
-  hi = __reduce_max_sync(0xffffffffu, hi);
-  const bool narrow = !V.nbr_wide_only && (hi <= lo || hi - lo <= 65536u);
-  const uint32_t base = narrow ? (hi > lo ? lo : 0u) : kNbrWide;
   if ((threadIdx.x & 31u) == 0) V.nbr_base[k >> 5] = base;
   if (!f) return;
   // Every candidate is tested; the first kMaxNbr hits in walk order are
