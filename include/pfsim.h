@@ -497,6 +497,17 @@ PF_API void* pf_scene_stream(pf_scene* scene);
  * order (w = 0), scenes concatenated in batch order: one device gather and
  * one device-to-host copy (pinned host memory makes it fastest). Synchronous. */
 PF_API pf_status pf_batch_read_positions(pf_batch* batch, float* dst_host, size_t bytes);
+/* pf_batch_read_positions without the wait, as the reference's readback
+ * returns a promise (particles.ts:200-227): the gather is queued on the
+ * batch's stream behind its work so far, and the copy to dst_host runs on a
+ * second stream, beside the steps that follow. dst_host holds the positions
+ * once pf_batch_wait_reads returns; until then leave it alone and keep it
+ * alive. Use pinned host memory (a pageable destination makes the copy
+ * synchronous). Two reads can be in flight; a third first waits for the
+ * oldest. */
+PF_API pf_status pf_batch_read_positions_async(pf_batch* batch, float* dst_host, size_t bytes);
+/* Waits until every pf_batch_read_positions_async of the batch has landed. */
+PF_API pf_status pf_batch_wait_reads(pf_batch* batch);
 /* Average device milliseconds of one solver stage launched `reps` times on the
  * batch's current state: 0 neighbour lists, 1 density + lambda, 2 position
  * correction, 3 XSPH, 4 predict. `items` receives the particles the stage

@@ -117,6 +117,37 @@ def test_batched_equals_plain(cuda, use_graph):
         assert np.array_equal(s.readback(N.PF_FIELD_VELOCITIES), batch.readback(i, N.PF_FIELD_VELOCITIES))
 
 
+def test_async_batch_reads_equal_sync_reads(cuda):
+    """pf_batch_read_positions_async, one read per step into two pinned
+    buffers in turn while the next steps run, delivers every step's positions
+    bit for bit as the synchronous read of a twin batch does."""
+    import ctypes as C
+
+    import torch
+
+    recipes = [W.dam_break(3000, seed=14), W.dam_break(6000, seed=15, scale=1.3, offset=(3.0, 0.0, 0.0))]
+    a = R.Batch([cuda.build(r) for r in recipes])
+    b = R.Batch([cuda.build(r) for r in recipes])
+    total = sum(r.capacity for r in recipes)
+    L = N.lib()
+    want = []
+    for _ in range(5):
+        a.step(DT)
+        buf = np.empty(total * 4, np.float32)
+        N.check(L.pf_batch_read_positions(a.h, buf.ctypes.data_as(C.POINTER(C.c_float)), buf.nbytes))
+        want.append(buf)
+    pinned = [torch.empty(total * 4, dtype=torch.float32).pin_memory() for _ in range(5)]
+    for k in range(5):
+        b.step(DT)
+        N.check(L.pf_batch_read_positions_async(b.h, C.cast(C.c_void_p(pinned[k].data_ptr()), C.POINTER(C.c_float)),
+                                                pinned[k].numel() * 4))
+    N.check(L.pf_batch_wait_reads(b.h))
+    for k in range(5):
+        assert np.array_equal(pinned[k].numpy(), want[k]), k
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("seed", [4, 9])
 def test_vorticity_confinement_one_frame(oracle, cuda, seed):
     """FluidSystem with vorticity (velocity.ts:36-120): curl in the XSPH walk,

@@ -983,6 +983,16 @@ pf_status pf_batch_read_positions(pf_batch* b, float* dst_host, size_t bytes) {
   return b->world->read_positions(dst_host, bytes);
 }
 
+pf_status pf_batch_read_positions_async(pf_batch* b, float* dst_host, size_t bytes) {
+  if (!b || !dst_host) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->read_positions_async(dst_host, bytes);
+}
+
+pf_status pf_batch_wait_reads(pf_batch* b) {
+  if (!b) return fail(PF_ERR_INVALID, "batch: NULL");
+  return b->world->wait_reads();
+}
+
 pf_status pf_batch_tuning(pf_batch* b, uint32_t* path, uint32_t* block, uint32_t* unroll, uint32_t* group,
                           uint32_t* entry_bits) {
   if (!b || !path || !block || !unroll) return fail(PF_ERR_INVALID, "batch: NULL");

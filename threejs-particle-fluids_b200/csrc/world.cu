@@ -1090,6 +1090,14 @@ void World::drop_graphs() {
 
 World::~World() {
   drop_graphs();
+  if (read_stream_) {
+    cudaStreamSynchronize(read_stream_);
+    cudaStreamDestroy(read_stream_);
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (ev_gathered_[b]) cudaEventDestroy(ev_gathered_[b]);
+    if (ev_read_[b]) cudaEventDestroy(ev_read_[b]);
+  }
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (ev_params_) cudaEventDestroy(ev_params_);
@@ -1894,6 +1902,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.acc_con = any_contact_ ? cv.take<int4>(N) : nullptr;
     base_.con_stat = any_contact_ ? cv.take<uint2>(K) : nullptr;
     stage_pos_ = cv.take<float4>(total_real);
+    stage_pos2_ = cv.take<float4>(total_real);
     prefix_dev_ = cv.take<uint64_t>(K);
   };
   Carver probe{nullptr};
@@ -3270,9 +3279,45 @@ uint64_t World::total_particles() const {
 pf_status World::read_positions(float* dst, size_t bytes) {
   const uint64_t total = total_particles();
   if (bytes < 16ull * total) return fail(PF_ERR_INVALID, "readback: destination too small");
+  PF_TRY(wait_reads());  // an async read may still copy out of stage_pos_
   launch_slots(k_gather_positions, n_, stream_, view(parity_), (const uint64_t*)prefix_dev_, stage_pos_);
   PF_CUDA(cudaMemcpyAsync(dst, stage_pos_, 16ull * total, cudaMemcpyDeviceToHost, stream_));
   PF_CUDA(cudaStreamSynchronize(stream_));
+  return PF_OK;
+}
+
+pf_status World::read_positions_async(float* dst, size_t bytes) {
+  const uint64_t total = total_particles();
+  if (bytes < 16ull * total) return fail(PF_ERR_INVALID, "readback: destination too small");
+  if (!read_stream_) {
+    PF_CUDA(cudaStreamCreateWithFlags(&read_stream_, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      PF_CUDA(cudaEventCreateWithFlags(&ev_gathered_[b], cudaEventDisableTiming));
+      PF_CUDA(cudaEventCreateWithFlags(&ev_read_[b], cudaEventDisableTiming));
+    }
+  }
+  const uint32_t b = read_next_;
+  read_next_ ^= 1u;
+  if (read_pending_[b]) {  // the read two calls back still copies out of this staging buffer
+    PF_CUDA(cudaEventSynchronize(ev_read_[b]));
+    read_pending_[b] = false;
+  }
+  float4* stage = b ? stage_pos2_ : stage_pos_;
+  launch_slots(k_gather_positions, n_, stream_, view(parity_), (const uint64_t*)prefix_dev_, stage);
+  PF_CUDA(cudaEventRecord(ev_gathered_[b], stream_));
+  PF_CUDA(cudaStreamWaitEvent(read_stream_, ev_gathered_[b], 0));
+  PF_CUDA(cudaMemcpyAsync(dst, stage, 16ull * total, cudaMemcpyDeviceToHost, read_stream_));
+  PF_CUDA(cudaEventRecord(ev_read_[b], read_stream_));
+  read_pending_[b] = true;
+  return PF_OK;
+}
+
+pf_status World::wait_reads() {
+  for (int b = 0; b < 2; ++b)
+    if (read_pending_[b]) {
+      PF_CUDA(cudaEventSynchronize(ev_read_[b]));
+      read_pending_[b] = false;
+    }
   return PF_OK;
 }
 

@@ -459,6 +459,12 @@ class World {
   // Positions of every scene, each in particle order, w = 0, concatenated in
   // scene order, into host memory (one gather kernel + one copy).
   pf_status read_positions(float* dst_host, size_t bytes);
+  // read_positions queued behind the work so far: the gather on the world's
+  // stream, the copy on a second stream beside the next steps (two staging
+  // buffers, so at most two reads in flight); dst_host is written once
+  // wait_reads returns.
+  pf_status read_positions_async(float* dst_host, size_t bytes);
+  pf_status wait_reads();
   uint64_t total_particles() const;
   uint64_t launches_per_step() const { return launches_per_step_; }
   size_t step_upload_bytes() const { return sizeof(DevScene) * h_scenes_.size(); }
@@ -606,6 +612,11 @@ class World {
   bool prims_dirty_ = true;
   size_t pair_entries_ = 0;
   float4* stage_pos_ = nullptr;  // gather buffer of read_positions
+  float4* stage_pos2_ = nullptr;  // the second one of read_positions_async
+  cudaStream_t read_stream_ = nullptr;  // copies of read_positions_async (made on first use)
+  cudaEvent_t ev_gathered_[2] = {nullptr, nullptr}, ev_read_[2] = {nullptr, nullptr};
+  bool read_pending_[2] = {false, false};
+  uint32_t read_next_ = 0;
   uint64_t* prefix_dev_ = nullptr;
   uint64_t launches_per_step_ = 0;
   std::vector<uint64_t> prefix_;   // particle offset of each scene in read_positions

@@ -349,6 +349,8 @@ SIGNATURES = {
     "pf_batch_step_upload_bytes": (C.c_uint64, [_P]),
     "pf_scene_stream": (_P, [_P]),
     "pf_batch_read_positions": (C.c_int, [_P, _f32p, C.c_size_t]),
+    "pf_batch_read_positions_async": (C.c_int, [_P, _f32p, C.c_size_t]),
+    "pf_batch_wait_reads": (C.c_int, [_P]),
     "pf_batch_profile_stage": (C.c_int, [_P, C.c_uint32, C.c_uint32, _f32p, C.POINTER(C.c_uint64)]),
 }
 
