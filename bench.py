@@ -56,6 +56,9 @@ class ClockSampler:
         self.proc = None
 
     def start(self):
+        """Starts sampling and returns once the first sample is out, so that
+        nvidia-smi's own start-up (NVML initialisation, which can hold up the
+        driver for tens of milliseconds) is over before the timed region."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
@@ -63,6 +66,12 @@ class ClockSampler:
             )
         except Exception:
             self.proc = None
+            return
+        import select
+
+        ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+        if ready:
+            self.proc.stdout.readline()  # taken before the timed region: not counted
 
     def stop(self) -> dict:
         if self.proc is None:
