@@ -1100,7 +1100,10 @@ World::~World() {
   }
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
-  if (ev_params_) cudaEventDestroy(ev_params_);
+  for (auto& e : ev_params_)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ev_bounds_)
+    if (e) cudaEventDestroy(e);
   if (h_pinned_bbox_) cudaFreeHost(h_pinned_bbox_);
   if (grid_arena_) cudaFree(grid_arena_);
   if (sort_arena_) cudaFree(sort_arena_);
@@ -1947,9 +1950,10 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   }
   PF_CUDA(cudaEventCreate(&ev0_));
   PF_CUDA(cudaEventCreate(&ev1_));
-  PF_CUDA(cudaEventCreateWithFlags(&ev_params_, cudaEventDisableTiming));
-  PF_CUDA(cudaMallocHost(&h_pinned_bbox_, sizeof(int32_t) * 12 * std::max<size_t>(1, K)));  // two steps
-  PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * K));
+  for (uint32_t q = 0; q < kParamRing; ++q) PF_CUDA(cudaEventCreateWithFlags(&ev_params_[q], cudaEventDisableTiming));
+  for (uint32_t q = 0; q < kBoundsRing; ++q) PF_CUDA(cudaEventCreateWithFlags(&ev_bounds_[q], cudaEventDisableTiming));
+  PF_CUDA(cudaMallocHost(&h_pinned_bbox_, sizeof(int32_t) * 6 * kBoundsRing * std::max<size_t>(1, K)));
+  PF_CUDA(cudaMallocHost(&h_pinned_scenes_, sizeof(DevScene) * kParamRing * std::max<size_t>(1, K)));
   PF_CUDA(cudaMallocHost(&h_pinned_prims_, sizeof(pf_primitive) * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_plane4_, sizeof(float4) * 2 * std::max<size_t>(1, h_prims_.size())));
   PF_CUDA(cudaMallocHost(&h_pinned_sdfs_, sizeof(DevSdf) * std::max<size_t>(1, h_sdfs_.size())));
@@ -2177,11 +2181,20 @@ pf_status World::upload_params(double dt) {
   // where this step's density passes leave lambda (read back by PF_FIELD_LAMBDA)
   lam_in_xl_.resize(K);
   for (uint32_t s = 0; s < K; ++s) lam_in_xl_[s] = h_scenes_[s].homog != 0;
-  // the previous step's copies may still wait behind earlier work: their
-  // pinned sources are written only once those copies have run
-  if (params_pending_) PF_CUDA(cudaEventSynchronize(ev_params_));
-  std::memcpy(h_pinned_scenes_, h_scenes_.data(), sizeof(DevScene) * K);
-  PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, h_pinned_scenes_, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
+  // Earlier steps' copies may still wait behind earlier work: a ring slot's
+  // pinned source is written only once its last copy has run, and the
+  // single-buffer tables (rewritten only after a setter) once every copy has.
+  const uint32_t slot = (uint32_t)(uploads_ % kParamRing);
+  if (params_pending_[slot]) {
+    PF_CUDA(cudaEventSynchronize(ev_params_[slot]));
+    params_pending_[slot] = false;
+  }
+  if ((sdfs_dirty_ && !h_sdfs_.empty()) || (cloth_par_dirty_ && !h_cloth_par_.empty()) ||
+      (prims_dirty_ && !h_prims_.empty()))
+    PF_TRY(wait_uploads());
+  DevScene* staged = h_pinned_scenes_ + (size_t)slot * K;
+  std::memcpy(staged, h_scenes_.data(), sizeof(DevScene) * K);
+  PF_CUDA(cudaMemcpyAsync(base_.scenes_rw, staged, sizeof(DevScene) * K, cudaMemcpyHostToDevice, stream_));
   if (sdfs_dirty_ && !h_sdfs_.empty()) {
     std::memcpy(h_pinned_sdfs_, h_sdfs_.data(), sizeof(DevSdf) * h_sdfs_.size());
     PF_CUDA(cudaMemcpyAsync(const_cast<DevSdf*>(base_.sdfs), h_pinned_sdfs_, sizeof(DevSdf) * h_sdfs_.size(),
@@ -2203,8 +2216,18 @@ pf_status World::upload_params(double dt) {
                             sizeof(pf_primitive) * h_prims_.size(), cudaMemcpyHostToDevice, stream_));
     prims_dirty_ = false;
   }
-  PF_CUDA(cudaEventRecord(ev_params_, stream_));
-  params_pending_ = true;
+  PF_CUDA(cudaEventRecord(ev_params_[slot], stream_));
+  params_pending_[slot] = true;
+  ++uploads_;
+  return PF_OK;
+}
+
+pf_status World::wait_uploads() {
+  for (uint32_t q = 0; q < kParamRing; ++q)
+    if (params_pending_[q]) {
+      PF_CUDA(cudaEventSynchronize(ev_params_[q]));
+      params_pending_[q] = false;
+    }
   return PF_OK;
 }
 
@@ -2738,9 +2761,6 @@ void World::run_substep(uint32_t s, uint32_t parity) {
 pf_status World::step(double dt) {
   if (!(dt > 0) || !std::isfinite(dt))
     return fail(PF_ERR_INVALID, "SimLoop: step dt must be a positive finite number, got " + std::to_string(dt));
-  // the previous step's parameter copies have run, so everything queued
-  // before them has too (the bounds maybe_grow_windows reads among it)
-  if (params_pending_) PF_CUDA(cudaEventSynchronize(ev_params_));
   PF_TRY(maybe_grow_windows());
   PF_TRY(upload_params(dt));
   PF_CUDA(cudaEventRecord(ev0_, stream_));
@@ -2809,11 +2829,14 @@ pf_status World::step(double dt) {
   parity_ ^= flips;
   PF_CUDA(cudaEventRecord(ev1_, stream_));
   if (any_grid_) {
-    // this step's bounds, into the buffer of its parity; the step two later
-    // reads them (by then they have surely arrived)
+    // this step's bounds, into its ring buffer, with an event a later step
+    // queries (the host reads a buffer only once its copy has landed, and
+    // only before queueing the copy that reuses it)
     const size_t K6 = 6 * h_scenes_.size();
-    PF_CUDA(cudaMemcpyAsync(h_pinned_bbox_ + K6 * (steps_done_ & 1), base_.bbox_last, sizeof(int32_t) * K6,
-                            cudaMemcpyDeviceToHost, stream_));
+    const uint32_t q = (uint32_t)(steps_done_ % kBoundsRing);
+    PF_CUDA(cudaMemcpyAsync(h_pinned_bbox_ + K6 * q, base_.bbox_last, sizeof(int32_t) * K6, cudaMemcpyDeviceToHost,
+                            stream_));
+    PF_CUDA(cudaEventRecord(ev_bounds_[q], stream_));
   }
   ++steps_done_;
   PF_CUDA(cudaGetLastError());
@@ -2821,15 +2844,35 @@ pf_status World::step(double dt) {
 }
 
 // Before a step: a grid scene whose particles' cell bounds (as the window
-// fit of the step two before saw them: the wait on the last parameter upload
-// has made sure they arrived) come within a margin of its window's size on
-// some axis gets a window twice their spread there, centred on them, so it
-// never has to clamp (the reference's hash grid is unbounded). The margin
-// covers the two steps since those bounds. Windows past 2^27 cells stay as
-// they are (their keys clamp and flag).
+// fit of the newest step whose bounds have arrived saw them) come within a
+// margin of its window's size on some axis gets a window twice their spread
+// there, centred on them, so it never has to clamp (the reference's hash
+// grid is unbounded). The margin covers the spread's growth over the steps
+// from those bounds to the end of the one about to be queued, and one more.
+// Windows past 2^27 cells stay as they are (their keys clamp and flag).
 pf_status World::maybe_grow_windows() {
-  if (!any_grid_ || steps_done_ < 2) return PF_OK;
-  const int32_t* seen = h_pinned_bbox_ + 6 * h_scenes_.size() * (steps_done_ & 1);  // step steps_done_ - 2
+  if (!any_grid_ || steps_done_ == 0) return PF_OK;
+  // the newest step whose bounds have landed (the ring holds the last
+  // kBoundsRing steps; one that is still queued is skipped, not waited for)
+  uint64_t seen_step = 0;
+  bool found = false;
+  const uint64_t oldest = steps_done_ > kBoundsRing ? steps_done_ - kBoundsRing : 0;
+  for (uint64_t t = steps_done_; t-- > oldest;) {
+    if (t + 1 <= bounds_seen_) break;  // looked at already
+    const cudaError_t e = cudaEventQuery(ev_bounds_[t % kBoundsRing]);
+    if (e == cudaSuccess) {
+      seen_step = t;
+      found = true;
+      break;
+    }
+    if (e != cudaErrorNotReady) PF_CUDA(e);
+  }
+  if (!found) return PF_OK;
+  // steps from those bounds to the end of the step about to be queued
+  const uint64_t ahead = steps_done_ - seen_step;
+  const uint64_t since = bounds_seen_ ? seen_step + 1 - bounds_seen_ : 1;  // steps since the last look
+  bounds_seen_ = seen_step + 1;
+  const int32_t* seen = h_pinned_bbox_ + 6 * h_scenes_.size() * (seen_step % kBoundsRing);
   bool any = false;
   for (uint32_t s = 0; s < h_scenes_.size(); ++s) {
     DevScene& S = h_scenes_[s];
@@ -2842,14 +2885,14 @@ pf_status World::maybe_grow_windows() {
       lo[a] = S.lo0[a];
       dims[a] = d;
       if (mn > mx) continue;  // no particle
-      // within two cells of clamping, plus three times the spread's growth
-      // per step (the two steps since these bounds, and one more); a fluid
-      // that walls hold stops growing there
+      // within two cells of clamping, plus the spread's growth per step
+      // over the steps from these bounds to the end of the next one, and
+      // one step more; a fluid that walls hold stops growing there
       const int64_t ext = mx - mn + 1;
       int32_t& prev = grow_prev_ext_[3 * s + a];
-      const int64_t rate = prev > 0 ? std::max<int64_t>(0, ext - prev) : 0;
+      const int64_t rate = prev > 0 ? (std::max<int64_t>(0, ext - prev) + (int64_t)since - 1) / (int64_t)since : 0;
       prev = (int32_t)ext;
-      if (ext + 3 * rate + 4 <= d) continue;
+      if (ext + (int64_t)(ahead + 1) * rate + 4 <= d) continue;
       dims[a] = std::max<int64_t>(d, 2 * ext + 8);
       lo[a] = ((mn + mx) >> 1) - dims[a] / 2;
       grow = true;

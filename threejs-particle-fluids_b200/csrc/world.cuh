@@ -621,15 +621,23 @@ class World {
   uint64_t launches_per_step_ = 0;
   std::vector<uint64_t> prefix_;   // particle offset of each scene in read_positions
   // Grid windows grow with their particles: after each step the last window
-  // fit's cell bounds come back to pinned memory, and two steps later any
-  // window they have nearly outgrown is widened and the cell arrays laid out
-  // again (outside any graph).
-  int32_t* h_pinned_bbox_ = nullptr;  // two buffers of 6 words per scene, by step parity
+  // fit's cell bounds come back to pinned memory (a ring of kBoundsRing
+  // buffers, each with an event), and before a later step any window they
+  // have nearly outgrown is widened and the cell arrays laid out again
+  // (outside any graph), from the newest bounds that have arrived.
+  static constexpr uint32_t kBoundsRing = 4;
+  int32_t* h_pinned_bbox_ = nullptr;  // kBoundsRing buffers of 6 words per scene
+  cudaEvent_t ev_bounds_[kBoundsRing] = {};
   uint64_t steps_done_ = 0;
-  // the previous parameter upload, waited on before its pinned staging is
-  // written again
-  cudaEvent_t ev_params_ = nullptr;
-  bool params_pending_ = false;
+  uint64_t bounds_seen_ = 0;  // steps_done_ of the last bounds looked at, plus one (0: none yet)
+  // Per-step parameters go through a ring of kParamRing pinned staging
+  // buffers, so the host can queue that many steps ahead; a buffer is
+  // written again once the event of its last upload has passed.
+  static constexpr uint32_t kParamRing = 3;
+  cudaEvent_t ev_params_[kParamRing] = {};
+  bool params_pending_[kParamRing] = {};
+  uint64_t uploads_ = 0;
+  pf_status wait_uploads();  // every upload queued so far (before rewriting the single-buffer tables)
   void* grid_arena_ = nullptr;  // cell arrays once the windows outgrow the arena's
   void* sort_arena_ = nullptr;  // sort scratch once the windows pass the cells it was carved for
   uint64_t cells_cap_ = 0;      // cells the current cell arrays and sort scratch hold
