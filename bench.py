@@ -611,6 +611,7 @@ class ServeWorkload:
                 "plain_with_builds_p99_tick_ms": p["p99"] if p else None,
                 "requests": len(stream), "cohort_builds": b["stats"]["rebuilds"],
                 "max_swap_ms": b["stats"]["max_swap_ms"], "max_admit_ms": b["stats"]["max_admit_ms"],
+                "max_step_ms": b["stats"]["max_step_ms"], "max_free_ms": b["stats"]["max_free_ms"],
                 "plain_max_admit_ms": p["stats"]["max_admit_ms"] if p else None,
                 "live_at_end": b["stats"]["live"], "queued_at_end": b["stats"]["queued"],
             },
@@ -938,6 +939,8 @@ def main() -> None:
             "plain_with_builds_value": ex["plain_with_builds_value"],
             "plain_with_builds_p99_tick_ms": ex["plain_with_builds_p99_tick_ms"],
             "timing": "host wall clock per tick; the plain arm's ticks without its world builds",
+            "cohort_builds": ex["cohort_builds"], "max_swap_ms": ex["max_swap_ms"],
+            "max_step_ms": ex["max_step_ms"], "max_free_ms": ex["max_free_ms"],
             "clocks": sres["clocks"],
         }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

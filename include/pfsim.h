@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define PFSIM_ABI_VERSION 2
+#define PFSIM_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PF_API __attribute__((visibility("default")))
@@ -53,6 +53,12 @@ typedef enum pf_status {
 PF_API const char* pf_last_error(void);
 /* PFSIM_ABI_VERSION of the loaded library. */
 PF_API int pf_abi_version(void);
+/* Worlds (SimLoops, batches, server cohorts) take their device memory from
+ * a pool of the current device that keeps what destroyed worlds and grown
+ * grids free, for the next world of the process. This waits for the device
+ * and hands the pool's unused memory back (for other allocators of the
+ * process, or other processes). No reference counterpart. */
+PF_API pf_status pf_trim_device_memory(void);
 
 /* ------------------------------------------------------------------------ */
 /* Neighbour grid: standalone stable counting sort                          */
@@ -618,6 +624,9 @@ typedef struct pf_server_stats {
   float max_admit_ms;         /* longest admission (synchronous builds included) */
   float last_admit_ms;        /* admission inside the last tick (PLAIN: its world builds);
                                  last_tick_ms minus this is that tick's stepping */
+  float max_step_ms;          /* longest stepping inside a tick: every cohort's launches and
+                                 the wait for them (a fresh cohort's graph capture included) */
+  float max_free_ms;          /* longest release of emptied cohorts inside a tick */
 } pf_server_stats;
 
 /* Request states reported by pf_server_request_state. */

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_text():
     lib = N.lib()
-    assert lib.pf_abi_version() == 2
+    assert lib.pf_abi_version() == 3
     # An invalid descriptor is rejected on the host before any device work.
     d = N.GridDesc()
     d.key_kind = N.PF_KEY_MORTON

@@ -148,6 +148,98 @@ def test_async_batch_reads_equal_sync_reads(cuda):
     b.close()
 
 
+def _tuning(batch):
+    import ctypes as C
+
+    v = [C.c_uint32() for _ in range(5)]
+    N.check(N.lib().pf_batch_tuning(batch.h, *[C.byref(x) for x in v]))
+    return [x.value for x in v]  # path, block, unroll (density pass), group, entry bits
+
+
+def test_tuning_cache_file(cuda, tmp_path, monkeypatch):
+    """PFSIM_TUNE_CACHE: a world that times its candidates appends one line
+    keyed by GPU, configuration and particle count; a world of the same
+    configuration takes the last matching line's choices and times nothing
+    (a planted line with other slot-path choices is what pf_batch_tuning then
+    reports, and nothing is appended); a world of another particle count
+    appends its own line. The planted choices (512-thread blocks, fetch depth
+    2, 32-bit entries) step to the same bits as the fixed default ones."""
+    monkeypatch.delenv("PFSIM_NBR_PATH", raising=False)
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("PFSIM_TUNE_CACHE", str(cache))
+
+    def recipes(n0=3000):
+        return [W.dam_break(n0, seed=21), W.dam_break(5000, seed=22, scale=1.2, offset=(3.0, 0.0, 0.0))]
+
+    a = R.Batch([cuda.build(r) for r in recipes()])
+    a.step(DT)
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1
+    f = lines[0].split()
+    assert f[0] == "pfsim-tune-1" and len(f) == 17
+    assert int(f[4]) >= sum(r.capacity for r in recipes())  # slots, scenes padded to whole chunks
+    assert _tuning(a)[:4] == [int(f[5]), int(f[7]), int(f[11]), int(f[14])]
+    a.close()
+
+    planted = f[:5] + ["0"] + ["512"] * 4 + ["2"] * 4 + ["0", "0", "1"]
+    cache.write_text(lines[0] + "\nnot a tuning line\n" + " ".join(planted) + "\n")
+    b = R.Batch([cuda.build(r) for r in recipes()])
+    b.step(DT)
+    assert _tuning(b) == [0, 512, 2, 0, 32]
+    assert len(cache.read_text().splitlines()) == 3
+
+    monkeypatch.setenv("PFSIM_NBR_PATH", "0")  # slot path, 256-thread blocks, depth 4, 16-bit entries
+    c = R.Batch([cuda.build(r) for r in recipes()])
+    c.step(DT)
+    assert _tuning(c) == [0, 256, 4, 0, 16]
+    for _ in range(4):
+        b.step(DT)
+        c.step(DT)
+    for i in range(2):
+        assert np.array_equal(b.readback(i, N.PF_FIELD_POSITIONS), c.readback(i, N.PF_FIELD_POSITIONS))
+        assert np.array_equal(b.readback(i, N.PF_FIELD_VELOCITIES), c.readback(i, N.PF_FIELD_VELOCITIES))
+    b.close()
+    c.close()
+
+    monkeypatch.delenv("PFSIM_NBR_PATH")
+    d = R.Batch([cuda.build(r) for r in recipes(4000)])
+    d.step(DT)
+    d.close()
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 4 and int(lines[3].split()[4]) > int(f[4])
+
+
+def test_worlds_reuse_pooled_device_memory(cuda):
+    """A destroyed world's device memory stays in the library's pool, the
+    next world of the same size takes it from there (the device's free
+    memory does not move), and pf_trim_device_memory hands it back; the
+    second world steps to the same bits as the first."""
+    import torch
+
+    L = N.lib()
+    N.check(L.pf_trim_device_memory())
+    free0 = torch.cuda.mem_get_info()[0]
+    r = W.dam_break(200_000, seed=31)
+    a = cuda.build(r)
+    a.step(DT)
+    xa = a.readback(N.PF_FIELD_POSITIONS)
+    free1 = torch.cuda.mem_get_info()[0]
+    held = free0 - free1
+    assert held > 0
+    a.close()
+    free2 = torch.cuda.mem_get_info()[0]
+    assert free2 - free1 < 0.25 * held  # kept by the pool
+    b = cuda.build(r)
+    b.step(DT)
+    free3 = torch.cuda.mem_get_info()[0]
+    assert abs(free3 - free2) < 0.25 * held  # taken from the pool
+    assert np.array_equal(b.readback(N.PF_FIELD_POSITIONS), xa)
+    b.close()
+    N.check(L.pf_trim_device_memory())
+    free4 = torch.cuda.mem_get_info()[0]
+    assert free4 - free1 > 0.75 * held  # handed back
+
+
 @pytest.mark.parametrize("seed", [4, 9])
 def test_vorticity_confinement_one_frame(oracle, cuda, seed):
     """FluidSystem with vorticity (velocity.ts:36-120): curl in the XSPH walk,

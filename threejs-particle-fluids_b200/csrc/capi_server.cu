@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <future>
@@ -94,6 +95,7 @@ struct pf_server {
   double busy_ms = 0;
   std::vector<float> tick_ms;
   float max_swap_ms = 0, max_admit_ms = 0;
+  float max_step_ms = 0, max_free_ms = 0;
   float last_admit_ms = 0;  // admission (and synchronous builds) inside the last tick
   bool blocked = false;  // the last build ran out of memory: wait for a cohort to free
   std::string last_error;
@@ -369,9 +371,11 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   if (!S) return fail(PF_ERR_INVALID, "server: NULL");
   if (!(dt > 0)) return fail(PF_ERR_INVALID, "server: dt must be positive");
   const auto t0 = Clock::now();
+  double swap_ms = 0;
   if (build_ready(S)) {
     PF_TRY(swap_in(S));
-    S->max_swap_ms = std::max(S->max_swap_ms, (float)ms_since(t0));
+    swap_ms = ms_since(t0);
+    S->max_swap_ms = std::max(S->max_swap_ms, (float)swap_ms);
   }
   S->last_admit_ms = 0;
   if (!S->opts.async_build || S->opts.mode == PF_SERVER_PLAIN) {
@@ -383,9 +387,14 @@ pf_status pf_server_tick(pf_server* S, double dt) {
   }
   bool stepped = false;
   const bool plain = S->opts.mode == PF_SERVER_PLAIN;
-  for (auto& c : S->cohorts)
+  const auto ts = Clock::now();
+  std::vector<float> host_ms(S->cohorts.size(), 0.0f);  // per cohort, for the verbose log
+  for (size_t ci = 0; ci < S->cohorts.size(); ++ci) {
+    auto& c = S->cohorts[ci];
     if (c->live) {
+      const auto th = Clock::now();
       PF_TRY(c->world->step(dt));
+      host_ms[ci] = (float)ms_since(th);
       if (!S->have_tuning && c->world->tuned() && c->world->has_fluid()) {
         S->tuning = c->world->tuning_all();
         S->have_tuning = true;
@@ -394,9 +403,23 @@ pf_status pf_server_tick(pf_server* S, double dt) {
       if (plain) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
       stepped = true;
     }
+  }
   if (!plain)
     for (auto& c : S->cohorts)
       if (c->live) PF_CUDA(cudaStreamSynchronize(c->world->stream()));
+  const double step_ms = ms_since(ts);
+  S->max_step_ms = std::max(S->max_step_ms, (float)step_ms);
+  if (verbose() && !plain)
+    // each stepped cohort: its step call on the host and its step on the
+    // device (the cohorts' steps overlap there); printed before this tick's
+    // line
+    for (size_t ci = 0; ci < S->cohorts.size(); ++ci) {
+      float gpu = 0;
+      if (host_ms[ci] > 0 && S->cohorts[ci]->world->elapsed_ms(&gpu) == PF_OK)
+        std::fprintf(stderr, "pfsim:   cohort %zu: %u live, step call %.2f ms, device %.2f ms\n", ci,
+                     S->cohorts[ci]->live, host_ms[ci], gpu);
+    }
+  const auto tr = Clock::now();
   bool freed = false;
   for (auto& c : S->cohorts) {
     for (uint32_t j = 0; j < c->members.size(); ++j) {
@@ -421,6 +444,8 @@ pf_status pf_server_tick(pf_server* S, double dt) {
       }
     }
   }
+  const double retire_ms = ms_since(tr);
+  const auto tf = Clock::now();
   for (size_t i = 0; i < S->cohorts.size();) {
     Cohort* c = S->cohorts[i].get();
     if (c->live == 0 && !c->folding) {
@@ -432,6 +457,8 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     }
   }
   if (freed) S->blocked = false;
+  const double free_ms = ms_since(tf);
+  S->max_free_ms = std::max(S->max_free_ms, (float)free_ms);
   // An asynchronous build starts after this tick's steps (and their first-step
   // graph captures), and runs on the worker thread while the next ticks go on.
   if (S->opts.async_build && S->opts.mode != PF_SERVER_PLAIN) {
@@ -442,10 +469,17 @@ pf_status pf_server_tick(pf_server* S, double dt) {
     S->max_admit_ms = std::max(S->max_admit_ms, ms);
   }
   S->ticks++;
+  const double ms = ms_since(t0);
   if (stepped) {  // latency statistics cover ticks that stepped at least one scene
-    const double ms = ms_since(t0);
     S->busy_ms += ms;
     S->tick_ms.push_back((float)ms);
+  }
+  if (verbose()) {
+    std::fprintf(stderr,
+                 "pfsim: tick %llu %.2f ms: swap %.2f, admit %.2f, step %.2f, retire %.2f, free %.2f; %zu cohorts, "
+                 "%u live\n",
+                 (unsigned long long)S->ticks, ms, swap_ms, (double)S->last_admit_ms, step_ms, retire_ms, free_ms,
+                 S->cohorts.size(), live_count(S));
   }
   return PF_OK;
 }
@@ -492,6 +526,8 @@ pf_status pf_server_stats_read(pf_server* S, pf_server_stats* o) {
   o->max_swap_ms = S->max_swap_ms;
   o->max_admit_ms = S->max_admit_ms;
   o->last_admit_ms = S->last_admit_ms;
+  o->max_step_ms = S->max_step_ms;
+  o->max_free_ms = S->max_free_ms;
   return PF_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
 #include <string>
 
 #include "pfsim.h"
@@ -14,6 +15,13 @@ namespace pf {
 // Thread-local error text behind pf_last_error().
 void set_error(const std::string& msg);
 const std::string& get_error();
+
+// PFSIM_VERBOSE set: host-side events (grid window growth, graph captures,
+// the phases of a serving tick) and their times go to stderr.
+inline bool verbose() {
+  static const bool v = std::getenv("PFSIM_VERBOSE") != nullptr;
+  return v;
+}
 
 // Returns a pf_status and records msg.
 inline pf_status fail(pf_status s, const std::string& msg) {

@@ -22,6 +22,7 @@
 #include <mutex>
 #include <set>
 
+#include "devmem.cuh"
 #include "world.cuh"
 #include "world_kernels.cuh"
 #include "world_slots.cuh"
@@ -1034,13 +1035,6 @@ void launch_slots(K kernel, uint32_t n, cudaStream_t st, A... args) {
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// PFSIM_VERBOSE set: host-side events (grid window growth, graph captures)
-// and their times go to stderr.
-bool verbose() {
-  static const bool v = std::getenv("PFSIM_VERBOSE") != nullptr;
-  return v;
-}
-
 // The slot neighbour passes use no shared memory and gather their
 // neighbours' records through L1: each asks for the largest L1 (a hint the
 // runtime may round), once per device, outside any stream capture.
@@ -1105,13 +1099,17 @@ World::~World() {
   for (auto& e : ev_bounds_)
     if (e) cudaEventDestroy(e);
   if (h_pinned_bbox_) cudaFreeHost(h_pinned_bbox_);
-  if (grid_arena_) cudaFree(grid_arena_);
-  if (sort_arena_) cudaFree(sort_arena_);
+  // the device memory goes back to the pool in stream order, once this
+  // world's streams are idle: no other stream touches it after that
+  if (side_stream_) cudaStreamSynchronize(side_stream_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  dev_free(grid_arena_, stream_);
+  dev_free(sort_arena_, stream_);
+  dev_free(arena_, stream_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   if (side_stream_) cudaStreamDestroy(side_stream_);
   if (stream_) cudaStreamDestroy(stream_);
-  if (arena_) cudaFree(arena_);
   if (h_pinned_scenes_) cudaFreeHost(h_pinned_scenes_);
   if (h_pinned_prims_) cudaFreeHost(h_pinned_prims_);
   if (h_pinned_plane4_) cudaFreeHost(h_pinned_plane4_);
@@ -1917,13 +1915,16 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   bytes_ = probe.off + al256(sort_bytes);
   if (plan_only) return PF_OK;
   (void)sm_count();  // cache the SM count outside any stream capture
-  if (const cudaError_t e = cudaMalloc(&arena_, bytes_); e != cudaSuccess) {
-    cudaGetLastError();
+  PF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  if (const cudaError_t e = dev_alloc(&arena_, bytes_, stream_); e != cudaSuccess) {
     arena_ = nullptr;
     if (e == cudaErrorMemoryAllocation)
       return fail(PF_ERR_OOM, "SimLoop: out of device memory (" + std::to_string(bytes_) + " bytes)");
     return fail(PF_ERR_CUDA, std::string("SimLoop: device allocation failed: ") + cudaGetErrorString(e));
   }
+  // the pool's allocation is ordered on stream_: wait for it, so copies on
+  // any stream may use the arena
+  PF_CUDA(cudaStreamSynchronize(stream_));
   Carver cv{static_cast<char*>(arena_)};
   layout(cv);
   sort_scratch_carve(static_cast<char*>(arena_) + probe.off, n_, sort_cells, &sort_);
@@ -1942,7 +1943,6 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
   base_.n_grid_scenes = (uint32_t)grid_scene.size();
   base_.n_rows = row_base.back();
   pair_entries_ = any_soft_local_ ? csr_idx.size() : 0;
-  PF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   if (side_ok_) {
     PF_CUDA(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking));
     PF_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
@@ -2393,6 +2393,116 @@ void World::run_groups(const WorldView& V, uint32_t s, bool apply) {
   }
 }
 
+// Tuning cache. With PFSIM_TUNE_CACHE naming a file, the tuner first looks
+// there for a line
+//   pfsim-tune-1 <gpu> <sms> <config> <n> <path> <block x4> <unroll x4> <group> <flat> <wide>
+// keyed by the GPU (its name, blanks as '_', and its SM count), the world's
+// configuration (a 64-bit FNV-1a hash, in hex, of its scenes' capacities,
+// substeps, iterations, build-time grid windows, fluids and contacts, and
+// of the world's feature flags) and its particle count. A world whose key
+// is there takes the last such line's choices and times nothing; a world
+// that times its candidates appends its line. A line that does not parse,
+// or whose choices this world cannot run, is passed over. The choices set
+// the speed: both paths build the same neighbour lists, and on the slot
+// path every block size, fetch depth, group size and entry width steps to
+// the same bits.
+std::string World::tune_key() const {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      h ^= (v >> (8 * b)) & 0xffu;
+      h *= 1099511628211ull;
+    }
+  };
+  mix(h_scenes_.size());
+  for (const DevScene& S : h_scenes_) {
+    mix(S.cap);
+    mix(S.seg_end - S.seg_start);
+    mix(S.substeps);
+    mix(S.iterations);
+    mix(S.has_grid);
+    for (int a = 0; a < 3; ++a) mix(S.dims[a]);
+    mix(S.fluid_count);
+    mix(S.contact);
+  }
+  mix(h_fluids_.size());
+  for (const DevFluid& F : h_fluids_) mix(F.rank);
+  mix((uint64_t)any_visc_ | (uint64_t)any_vort_ << 1 | (uint64_t)any_imp_ << 2 | (uint64_t)any_multi_fluid_ << 3 |
+      (uint64_t)fuse_dens_ << 4 | (uint64_t)any_contact_ << 5);
+  mix(pure_parts_.size());
+  for (uint64_t p : pure_parts_) mix(p);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop{};
+  std::string gpu = "unknown";
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+    gpu.assign(prop.name, strnlen(prop.name, sizeof(prop.name)));
+    for (char& c : gpu)
+      if (c == ' ' || c == '\t') c = '_';
+    if (gpu.empty()) gpu = "unknown";
+  }
+  char buf[320];
+  std::snprintf(buf, sizeof buf, "%s %d %016llx %u", gpu.c_str(), sm_count(), (unsigned long long)h, n_);
+  return buf;
+}
+
+bool World::load_tuning(const char* file, const std::string& key) {
+  FILE* f = std::fopen(file, "r");
+  if (!f) return false;
+  uint64_t pure_total = 0;
+  for (uint64_t p : pure_parts_) pure_total += p;
+  auto valid = [&](const Tuning& t) {
+    if (t.path > 1 || t.nbr_flat > 1 || t.nbr_wide > 1) return false;
+    if (t.path == 1 && (any_vort_ || any_imp_ || any_multi_fluid_)) return false;
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t b = t.block[q], u = t.unroll[q];
+      if (b != 128 && b != 256 && b != 512) return false;
+      if (u != 2 && u != 4 && u != 8) return false;
+      if (u == 8 && b == 512) return false;  // never a candidate
+    }
+    return t.group == 0 || (!pure_end_.empty() && t.group < pure_total);
+  };
+  bool found = false;
+  Tuning hit;
+  char line[512];
+  while (std::fgets(line, sizeof line, f)) {
+    char tag[32], gpu[256], cfg[32];
+    int sms = 0;
+    unsigned n = 0;
+    Tuning t;
+    const int got = std::sscanf(line, "%31s %255s %d %31s %u %u %u %u %u %u %u %u %u %u %u %u %u", tag, gpu, &sms, cfg, &n,
+                                &t.path, &t.block[0], &t.block[1], &t.block[2], &t.block[3], &t.unroll[0], &t.unroll[1],
+                                &t.unroll[2], &t.unroll[3], &t.group, &t.nbr_flat, &t.nbr_wide);
+    if (got != 17 || std::strcmp(tag, "pfsim-tune-1") != 0) continue;
+    char k[320];
+    std::snprintf(k, sizeof k, "%s %d %s %u", gpu, sms, cfg, n);
+    if (key != k || !valid(t)) continue;
+    hit = t;
+    found = true;
+  }
+  std::fclose(f);
+  if (found) tune_ = hit;
+  return found;
+}
+
+void World::store_tuning(const char* file, const std::string& key) const {
+  char line[512];
+  const Tuning& t = tune_;
+  const int len = std::snprintf(line, sizeof line, "pfsim-tune-1 %s %u %u %u %u %u %u %u %u %u %u %u %u\n", key.c_str(),
+                                t.path, t.block[0], t.block[1], t.block[2], t.block[3], t.unroll[0], t.unroll[1],
+                                t.unroll[2], t.unroll[3], t.group, t.nbr_flat, t.nbr_wide);
+  if (len <= 0 || len >= (int)sizeof line) return;
+  // one short line written at once in append mode: lines of worlds tuned at
+  // the same time by other processes do not interleave
+  FILE* f = std::fopen(file, "a");
+  if (!f) {
+    if (verbose()) std::fprintf(stderr, "pfsim: tuning cache %s not writable\n", file);
+    return;
+  }
+  std::fwrite(line, 1, (size_t)len, f);
+  std::fclose(f);
+}
+
 // Autotuner: on the world's own state (one grid rebuild, as the next
 // substep would do; the permutation is canonical, so no result changes),
 // time each slot kernel (list build, density + lambda, position correction,
@@ -2426,6 +2536,20 @@ pf_status World::tune() {
     apply_grouping();
     return PF_OK;
   }
+  const char* cache = std::getenv("PFSIM_TUNE_CACHE");
+  if (cache && !*cache) cache = nullptr;
+  const std::string key = cache ? tune_key() : std::string();
+  if (cache && load_tuning(cache, key)) {
+    apply_grouping();
+    if (verbose()) std::fprintf(stderr, "pfsim: tuning of %s from %s\n", key.c_str(), cache);
+    return PF_OK;
+  }
+  PF_TRY(tune_trials());
+  if (cache) store_tuning(cache, key);
+  return PF_OK;
+}
+
+pf_status World::tune_trials() {
   run_sort_and_permute(parity_, false);
   parity_ ^= 1;
   const WorldView V = view(parity_);
@@ -2946,15 +3070,14 @@ pf_status World::relayout_grid() {
     const uint64_t cap = std::min<uint64_t>(kSortCellCap, 2ull * cells_);
     const size_t cell_bytes = al256(4ull * cap);
     void* g = nullptr;
-    if (const cudaError_t e = cudaMalloc(&g, 2 * cell_bytes); e != cudaSuccess) {
-      cudaGetLastError();
+    if (const cudaError_t e = dev_alloc(&g, 2 * cell_bytes, stream_); e != cudaSuccess) {
       return fail(e == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,
                   "SimLoop: growing the grid windows needs " + std::to_string(2 * cell_bytes) + " more bytes");
     }
     char* p = static_cast<char*>(g);
     base_.cstart = reinterpret_cast<uint32_t*>(p);
     base_.ccount = reinterpret_cast<uint32_t*>(p + cell_bytes);
-    if (grid_arena_) cudaFree(grid_arena_);
+    dev_free(grid_arena_, stream_);  // the streams are idle (synchronized above)
     grid_arena_ = g;
     bytes_ += 2 * cell_bytes;
     cells_cap_ = cap;
@@ -2965,17 +3088,17 @@ pf_status World::relayout_grid() {
     const uint64_t sort_cells = std::min<uint64_t>(kSortCellCap, 64ull * cells_);
     const size_t bytes = sort_scratch_bytes(n_, sort_cells);
     void* g = nullptr;
-    if (const cudaError_t e = cudaMalloc(&g, bytes); e != cudaSuccess) {
-      cudaGetLastError();
+    if (const cudaError_t e = dev_alloc(&g, bytes, stream_); e != cudaSuccess) {
       return fail(e == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,
                   "SimLoop: growing the grid windows needs " + std::to_string(bytes) + " more bytes");
     }
     sort_scratch_carve(g, n_, sort_cells, &sort_);
     PF_CUDA(sort_scratch_zero(sort_, stream_));
-    if (sort_arena_) cudaFree(sort_arena_);
+    dev_free(sort_arena_, stream_);
     sort_arena_ = g;
     bytes_ += bytes;
   }
+  PF_CUDA(cudaStreamSynchronize(stream_));  // new blocks usable from every stream
   radix_ = radix_plan(cells_);
   ++regrowths_;
   graphs_stale_ = true;

@@ -530,6 +530,12 @@ class World {
   void apply_grouping();  // groups_ and the scenes' grouped flags from tune_.group
   bool grouping() const { return tune_.path == 0 && !groups_.empty(); }
   pf_status tune();
+  pf_status tune_trials();  // time the candidates on this world's state
+  // tuning cache file (PFSIM_TUNE_CACHE): the key of this world on this GPU,
+  // and the lookup (true: tune_ holds a valid cached choice) and append
+  std::string tune_key() const;
+  bool load_tuning(const char* file, const std::string& key);
+  void store_tuning(const char* file, const std::string& key) const;
   template <typename K, typename... A>
   void launch_tiled(K kernel, size_t smem, const WorldView& V, A... args);
   void launch_frame_start_at(uint32_t parity);

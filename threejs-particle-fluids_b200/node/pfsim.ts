@@ -639,3 +639,12 @@ export class Simulation {
     this.loop?.particles.dispose();
   }
 }
+
+/**
+ * Hands back the device memory the library keeps from destroyed simulations
+ * (pf_trim_device_memory). No reference counterpart: the reference's buffers
+ * belong to the WebGPU device.
+ */
+export function trimDeviceMemory(): void {
+  addon.trimDeviceMemory();
+}

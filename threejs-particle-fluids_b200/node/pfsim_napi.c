@@ -1010,11 +1010,20 @@ static napi_value abi_version(napi_env env, napi_callback_info info) {
   return v;
 }
 
+/* trimDeviceMemory(): hand the device memory the library's pool keeps from
+ * destroyed worlds back to the device. */
+static napi_value trim_device_memory(napi_env env, napi_callback_info info) {
+  (void)info;
+  if (pf_trim_device_memory() != PF_OK) return throw_last(env);
+  return undefined(env);
+}
+
 /* ------------------------------------------------------------ module --- */
 
 NAPI_MODULE_INIT() {
   napi_property_descriptor p[] = {
       {"abiVersion", 0, abi_version, 0, 0, 0, napi_default, 0},
+      {"trimDeviceMemory", 0, trim_device_memory, 0, 0, 0, napi_default, 0},
       {"createScene", 0, create_scene, 0, 0, 0, napi_default, 0},
       {"destroyScene", 0, destroy_scene, 0, 0, 0, napi_default, 0},
       {"uploadParticles", 0, upload, 0, 0, 0, napi_default, 0},

@@ -281,6 +281,8 @@ class ServerStats(C.Structure):
         ("max_swap_ms", C.c_float),
         ("max_admit_ms", C.c_float),
         ("last_admit_ms", C.c_float),
+        ("max_step_ms", C.c_float),
+        ("max_free_ms", C.c_float),
     ]
 
 
@@ -292,6 +294,7 @@ _f32p = C.POINTER(C.c_float)
 SIGNATURES = {
     "pf_last_error": (C.c_char_p, []),
     "pf_abi_version": (C.c_int, []),
+    "pf_trim_device_memory": (C.c_int, []),
     "pf_grid_cells": (C.c_uint64, [C.POINTER(GridDesc)]),
     "pf_sort": (C.c_int, [_P, C.c_uint32, C.POINTER(GridDesc), _P, _P, _P, _P, _P, _P]),
     "pf_sort_device_errors": (C.c_int, [_P, _u32p]),

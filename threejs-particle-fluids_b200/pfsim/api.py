@@ -697,3 +697,9 @@ class Simulation:
     def dispose(self) -> None:
         if self.loop is not None:
             self.loop.dispose()
+
+
+def trim_device_memory() -> None:
+    """Hand back the device memory the library keeps from destroyed
+    simulations (pf_trim_device_memory). No reference counterpart."""
+    N.check(N.lib().pf_trim_device_memory())
