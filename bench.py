@@ -549,6 +549,8 @@ class ServeWorkload:
                 torch.cuda.synchronize()
                 ps0 = srv.stats()["particle_substeps"]
                 clocks.start()
+                # an ncu launch list can select the timed ticks' launches
+                torch.cuda.nvtx.range_push("plain_ticks" if plain else "served_ticks")
             for rec, life in by_tick.get(t + 1, []):
                 srv.submit(rec, life)
             t0 = time.perf_counter()
@@ -560,6 +562,7 @@ class ServeWorkload:
                 # admitted request's world inside the tick, the batched one
                 # only starts a cohort build there (it runs on a worker thread)
                 step_ms.append(max(ms - srv.stats()["last_admit_ms"], 0.0))
+        torch.cuda.nvtx.range_pop()
         clk = clocks.stop()
         st = srv.stats()
         srv.close()
