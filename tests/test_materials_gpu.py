@@ -198,3 +198,32 @@ def test_cloth_bending_batch_matches_plain(cuda):
         batch.step(DT)
     for i, s in enumerate(plain):
         assert np.array_equal(s.readback(N.PF_FIELD_POSITIONS), batch.readback(i, N.PF_FIELD_POSITIONS)), i
+
+
+@pytest.mark.parametrize("lanes", ["1", "2", "4", "8", "16", "32"])
+def test_shape_matching_gather_lanes_same_bits(oracle, cuda, monkeypatch, lanes):
+    """The shape-matching gather gives each cluster member a group of 4, 8, 16
+    or 32 lanes (the world picks one from how many clusters hold its
+    particles). The corrections are fixed-point ticks summed across the group,
+    so every width steps to the same bits: two frames of a soft-body pile and
+    of the mixed scene against the world's own choice, and the pile's first
+    frame against the oracle."""
+    recipes = [W.softbody_pile(8_000, seed=4, per_body=500), W.mixed_scene(n_budget=12_000, n_fluid=8_000, n_bodies=4, seed=1)]
+    out = []
+    for fixed in ("", lanes):
+        if fixed:
+            monkeypatch.setenv("PFSIM_MEMBER_LANES", fixed)
+        scenes = [cuda.build(r) for r in recipes]
+        frames = []
+        for _ in range(2):
+            for sc in scenes:
+                sc.step(DT)
+            frames.append([(sc.readback(N.PF_FIELD_POSITIONS), sc.readback(N.PF_FIELD_VELOCITIES)) for sc in scenes])
+        out.append(frames)
+    for f in range(2):
+        for i in range(len(recipes)):
+            assert np.array_equal(out[0][f][i][0], out[1][f][i][0]), (f, i)
+            assert np.array_equal(out[0][f][i][1], out[1][f][i][1]), (f, i)
+    ref = oracle.OracleBackend().build(recipes[0])
+    ref.step(DT)
+    assert np.abs(out[1][0][0][0] - ref.readback(N.PF_FIELD_POSITIONS)).max() <= TOL

@@ -762,65 +762,97 @@ __global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank
   if (e == s) {
     r[0] = 1; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 1; r[5] = 0; r[6] = 0; r[7] = 0; r[8] = 1;
   }
-  V.rot3[3 * (size_t)i + 0] = make_float4(r[0], r[1], r[2], 0.0f);
-  V.rot3[3 * (size_t)i + 1] = make_float4(r[3], r[4], r[5], 0.0f);
-  V.rot3[3 * (size_t)i + 2] = make_float4(r[6], r[7], r[8], 0.0f);
+  V.rot4[4 * (size_t)i + 0] = make_float4(r[0], r[1], r[2], c.x);
+  V.rot4[4 * (size_t)i + 1] = make_float4(r[3], r[4], r[5], c.y);
+  V.rot4[4 * (size_t)i + 2] = make_float4(r[6], r[7], r[8], c.z);
+  V.rot4[4 * (size_t)i + 3] = make_float4(cb.x, cb.y, cb.z, V.rest[i].w);
 }
 
 // shapeMatchImplicit.ts:248-308 taken by member, with the accumulator's
 // apply (accumulator.ts:148-178) for the particle. The reference scatters
 // each cluster's corrections to its members as fixed-point ticks, integer
-// sums whose order does not matter. Here one warp takes one particle (by id,
-// from the list of cluster members): each lane forms the corrections of
-// clusters that hold it, term for term as the cluster would, and updates
-// those pairs' multipliers (each pair belongs to one member); the lanes' tick
-// sums are added across the warp, and one lane applies them to the
-// particle's predicted position. No other warp reads that position in this
-// pass: the clusters' centres and rotations come from the passes before.
-__global__ void __launch_bounds__(kBlock) k_sm_gather(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t w = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31u;
-  if (w >= V.n_mem_ids) return;  // whole warps
-  const uint32_t j = __ldg(V.mem_ids + w);
-  const DevSoft& D = V.softs[V.mem_soft[j]];
-  const DevScene& S = V.scenes[D.scene];
-  if (D.rank != rank || sub >= S.substeps || it >= S.iterations) return;
-  const uint32_t b = V.mem_off[j], e = V.mem_off[j + 1];
-  const uint32_t sj = V.inv[j];
-  const float4 xj = V.cur.xs[sj];
-  const f3 rj = xyz(V.rest[j]);
-  const float wj = xj.w;
-  const float mj = fmaxf((float)(V.csr_off[j + 1] - V.csr_off[j]), 1.0f);
-  const float dt2 = S.dt * S.dt;
-  uint32_t tx = 0, ty = 0, tz = 0;
-  for (uint32_t q = b + lane; q < e; q += 32) {
-    const uint2 im = __ldg(V.mem + q);
-    const uint32_t i = im.x, m = im.y;
-    const f3 R0 = xyz(V.rot3[3 * (size_t)i]), R1 = xyz(V.rot3[3 * (size_t)i + 1]), R2 = xyz(V.rot3[3 * (size_t)i + 2]);
-    const f3 c = xyz(V.centers[i]);
-    const f3 cb = xyz(V.rest_c[i]);
-    const float at = V.rest[i].w / dt2;
-    const f3 lo = xyz(V.pair_lambda[m]);
-    const f3 rr = rj - cb;
-    const f3 goal = mk(dot(R0, rr), dot(R1, rr), dot(R2, rr)) + c;
-    const f3 C = xyz(xj) - goal;
-    const float denom = wj + at;
-    const f3 dl = (neg(C) - lo * at) / denom;
-    V.pair_lambda[m] = with_w(lo + dl, 0.0f);
-    const f3 dx = (dl * wj) / mj;
-    const float sc = sqrtf(D.maxc2 / fmaxf(dot(dx, dx), D.maxc2));
-    const f3 v = dx * sc;
-    tx += (uint32_t)to_ticks(v.x, S.sb_scale);
-    ty += (uint32_t)to_ticks(v.y, S.sb_scale);
-    tz += (uint32_t)to_ticks(v.z, S.sb_scale);
+// sums whose order does not matter. Here a group of L lanes takes one
+// particle (by id, from the list of cluster members; 32 / L particles per
+// warp, L chosen per world from how many clusters hold a particle): each lane
+// forms the corrections of clusters that hold it, term for term as the
+// cluster would, and updates those pairs' multipliers (each pair belongs to
+// one member); the lanes' tick sums are added across the group, and its first
+// lane applies them to the particle's predicted position. No other group
+// reads that position in this pass: the clusters' centres and rotations come
+// from the passes before. Every lane of a warp reaches the shuffles: a lane
+// past the last member, or whose member's body skips this pass, adds zero.
+template <uint32_t L>
+__global__ void __launch_bounds__(kBlock, 5) k_sm_gather(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+  static_assert(L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32,
+                "lanes per member: a power of two dividing the warp");
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x % L;
+  bool act = t / L < V.n_mem_ids;
+  const DevSoft* D = nullptr;
+  const DevScene* S = nullptr;
+  uint32_t tx = 0, ty = 0, tz = 0, sj = 0;
+  float4 xj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  uint32_t j = 0, b = 0, e = 0, c0 = 0, c1 = 0;
+  float4 rest4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (act) {
+    // the member's own records are loaded beside its body and scene (they
+    // do not depend on them), so the chains of dependent loads overlap
+    j = __ldg(V.mem_ids + t / L);
+    const uint32_t soft = V.mem_soft[j];
+    b = V.mem_off[j];
+    e = V.mem_off[j + 1];
+    sj = V.inv[j];
+    rest4 = V.rest[j];
+    c0 = V.csr_off[j];
+    c1 = V.csr_off[j + 1];
+    D = &V.softs[soft];
+    xj = V.cur.xs[sj];
+    S = &V.scenes[D->scene];
+    act = D->rank == rank && sub < S->substeps && it < S->iterations;
   }
-  tx = __reduce_add_sync(0xffffffffu, tx);
-  ty = __reduce_add_sync(0xffffffffu, ty);
-  tz = __reduce_add_sync(0xffffffffu, tz);
-  if (lane != 0 || !(tx | ty | tz)) return;
+  if (act) {
+    const f3 rj = xyz(rest4);
+    const float wj = xj.w;
+    const float mj = fmaxf((float)(c1 - c0), 1.0f);
+    const float dt2 = S->dt * S->dt;
+    const float maxc2 = D->maxc2, scale = S->sb_scale;
+    for (uint32_t q = b + lane; q < e; q += L) {
+      const uint2 im = __ldg(V.mem + q);
+      const uint32_t i = im.x, m = im.y;
+      // the cluster's record: rotation rows with the centre, then the rest
+      // centre and compliance (written by k_sm_moment this iteration)
+      const float4 a0 = V.rot4[4 * (size_t)i], a1 = V.rot4[4 * (size_t)i + 1], a2 = V.rot4[4 * (size_t)i + 2],
+                   a3 = V.rot4[4 * (size_t)i + 3];
+      const f3 R0 = xyz(a0), R1 = xyz(a1), R2 = xyz(a2);
+      const f3 c = mk(a0.w, a1.w, a2.w);
+      const f3 cb = xyz(a3);
+      const float at = a3.w / dt2;
+      const f3 lo = xyz(V.pair_lambda[m]);
+      const f3 rr = rj - cb;
+      const f3 goal = mk(dot(R0, rr), dot(R1, rr), dot(R2, rr)) + c;
+      const f3 C = xyz(xj) - goal;
+      const float denom = wj + at;
+      const f3 dl = (neg(C) - lo * at) / denom;
+      V.pair_lambda[m] = with_w(lo + dl, 0.0f);
+      const f3 dx = (dl * wj) / mj;
+      const float sc = sqrtf(maxc2 / fmaxf(dot(dx, dx), maxc2));
+      const f3 v = dx * sc;
+      tx += (uint32_t)to_ticks(v.x, scale);
+      ty += (uint32_t)to_ticks(v.y, scale);
+      tz += (uint32_t)to_ticks(v.z, scale);
+    }
+  }
+#pragma unroll
+  for (uint32_t o = L / 2; o > 0; o >>= 1) {
+    tx += __shfl_xor_sync(0xffffffffu, tx, o);
+    ty += __shfl_xor_sync(0xffffffffu, ty, o);
+    tz += __shfl_xor_sync(0xffffffffu, tz, o);
+  }
+  if (!act || lane != 0 || !(tx | ty | tz)) return;
   bool sat = false;
-  const f3 ch = ticks_change((int)tx, (int)ty, (int)tz, S.sb_inv, &sat);
-  V.cur.xs[sj] = with_w(xyz(xj) + ch, wj);
-  if (sat) atomicOr(V.flags + D.scene * kNumFlags + FLAG_SOFT, 1u);
+  const f3 ch = ticks_change((int)tx, (int)ty, (int)tz, S->sb_inv, &sat);
+  V.cur.xs[sj] = with_w(xyz(xj) + ch, xj.w);
+  if (sat) atomicOr(V.flags + D->scene * kNumFlags + FLAG_SOFT, 1u);
 }
 
 // shapeMatchImplicit.ts:325-401
@@ -832,7 +864,7 @@ __global__ void __launch_bounds__(kBlock) k_sm_qp(WorldView V, uint32_t rank, ui
   if (!group_active(V, g, rank, sub, it, &D, &S)) return;
   const uint32_t i = V.grp[g];
   if (V.csr_off[i + 1] <= V.csr_off[i]) return;
-  const float4 r0 = V.rot3[3 * (size_t)i], r1 = V.rot3[3 * (size_t)i + 1], r2 = V.rot3[3 * (size_t)i + 2];
+  const float4 r0 = V.rot4[4 * (size_t)i], r1 = V.rot4[4 * (size_t)i + 1], r2 = V.rot4[4 * (size_t)i + 2];
   const float m00 = r0.x, m01 = r0.y, m02 = r0.z, m10 = r1.x, m11 = r1.y, m12 = r1.z, m20 = r2.x, m21 = r2.y,
               m22 = r2.z;
   const float tr = m00 + m11 + m22;
@@ -1706,9 +1738,32 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
         ++mem_off[csr_idx[m] + 1];
         mem_soft[csr_idx[m]] = grp_soft[g];
       }
+    std::vector<uint32_t> held;  // clusters holding each member
     for (uint32_t i = 0; i < n_; ++i) {
-      if (mem_off[i + 1]) mem_ids.push_back(i);
+      if (mem_off[i + 1]) {
+        mem_ids.push_back(i);
+        held.push_back(mem_off[i + 1]);
+      }
       mem_off[i + 1] += mem_off[i];
+    }
+    // lanes per member in k_sm_gather: the smallest power of two that takes
+    // the clusters of nine members in ten in at most sixteen rounds. Each
+    // member starts with a chain of dependent loads (its id, body, scene,
+    // slot and position), so more members per warp keep more of those chains
+    // in flight; some rounds per member cost less than idle chains. On the
+    // serving stream's soft bodies (27 clusters per member) one served tick
+    // took 15.8, 13.2, 11.8, 10.7, 10.4 and 10.9 ms with 32, 16, 8, 4, 2 and
+    // 1 lanes.
+    mem_lanes_ = 1;
+    if (!held.empty()) {
+      const size_t at = (held.size() * 9) / 10;
+      std::nth_element(held.begin(), held.begin() + at, held.end());
+      const uint32_t p90 = held[at];
+      while (mem_lanes_ < 32 && mem_lanes_ * 16 < p90) mem_lanes_ *= 2;
+    }
+    if (const char* e = std::getenv("PFSIM_MEMBER_LANES")) {  // fixed choice for measurements and tests
+      const uint32_t l = (uint32_t)std::atoi(e);
+      if (l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32) mem_lanes_ = l;
     }
     mem.assign(std::max<uint32_t>(1, mem_off[n_]), make_uint2(0, 0));
     std::vector<uint32_t> at(mem_off.begin(), mem_off.end() - 1);
@@ -1852,7 +1907,7 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.rest_c = need_soft ? cv.take<float4>(N) : nullptr;
     base_.weights = need_soft ? cv.take<float>(N) : nullptr;
     base_.centers = need_soft ? cv.take<float4>(N) : nullptr;
-    base_.rot3 = need_soft ? cv.take<float4>(3 * N) : nullptr;
+    base_.rot4 = need_soft ? cv.take<float4>(4 * N) : nullptr;
     base_.q = need_soft ? cv.take<float4>(N) : nullptr;
     base_.qp = need_soft ? cv.take<float4>(N) : nullptr;
     base_.omega = need_soft ? cv.take<float4>(N) : nullptr;
@@ -2823,8 +2878,14 @@ void World::run_substep(uint32_t s, uint32_t parity) {
       if (has_local) {
         launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
         launch_slots(k_sm_moment, base_.n_grp, stream_, V, r, s, it);
-        if (base_.n_mem_ids) {  // one warp per cluster member
-          k_sm_gather<<<(uint32_t)((32ull * base_.n_mem_ids + kBlock - 1) / kBlock), kBlock, 0, stream_>>>(V, r, s, it);
+        if (base_.n_mem_ids) {  // mem_lanes_ lanes per cluster member
+          const uint32_t grid = (uint32_t)(((uint64_t)mem_lanes_ * base_.n_mem_ids + kBlock - 1) / kBlock);
+          if (mem_lanes_ == 1) k_sm_gather<1><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
+          else if (mem_lanes_ == 2) k_sm_gather<2><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
+          else if (mem_lanes_ == 4) k_sm_gather<4><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
+          else if (mem_lanes_ == 8) k_sm_gather<8><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
+          else if (mem_lanes_ == 16) k_sm_gather<16><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
+          else k_sm_gather<32><<<grid, kBlock, 0, stream_>>>(V, r, s, it);
           ++t_launches;
         }
         launch_slots(k_sm_qp, base_.n_grp, stream_, V, r, s, it);

@@ -353,7 +353,10 @@ struct WorldView {
   const float4* rest_c;      // neighbourhood rest centres
   const float* weights;
   float4* centers;
-  float4* rot3;              // 3 rows per id
+  // 4 rows per cluster id: the rotation's rows with the cluster centre's
+  // x, y, z in w, then (rest centre, compliance); the record the
+  // shape-matching gather reads per (member, cluster) pair, 64 aligned bytes
+  float4* rot4;
   float4* q;                 // orientation
   float4* qp;                // predicted orientation
   float4* omega;             // angular velocity
@@ -519,6 +522,7 @@ class World {
   void launch_tiles_build(const WorldView& V, uint32_t s);
   template <typename K, typename... A>
   void launch_fluid(uint32_t block, K kernel, const WorldView& V, A... args);
+  uint32_t mem_lanes_ = 32;  // lanes per cluster member in the shape-matching gather
   void run_fluid_neighbors(const WorldView& V, uint32_t s);
   void run_fluid_lambda_delta(const WorldView& V, uint32_t r, uint32_t s, uint32_t it);
   void run_fluid_xsph(const WorldView& V, uint32_t r, uint32_t s);
