@@ -702,8 +702,12 @@ __global__ void __launch_bounds__(kBlock) k_rot_advect(WorldView V, uint32_t sub
   V.q[i] = qp;
 }
 
-// shapeMatchImplicit.ts:46-71
-__global__ void __launch_bounds__(kBlock) k_sm_center(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
+// shapeMatchImplicit.ts:46-71 (the cluster's centre) and 100-217 (its moment
+// matrix and rotation), one thread per cluster. The moment of a cluster reads
+// only its own centre, so the thread forms the centre first, in CSR order as
+// the reference's centre pass does, and keeps it in registers; the members'
+// positions come back from cache for the moment.
+__global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= V.n_grp) return;
   const DevSoft* D;
@@ -713,22 +717,9 @@ __global__ void __launch_bounds__(kBlock) k_sm_center(WorldView V, uint32_t rank
   const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
   f3 sum = mk(0.0f, 0.0f, 0.0f);
   for (uint32_t m = s; m < e; ++m) sum = sum + xyz(V.cur.xs[V.inv[V.csr_idx[m]]]);
-  const uint32_t cnt = e - s;
-  const float inv = 1.0f / (float)max(cnt, 1u);
-  V.centers[i] = cnt == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : with_w(sum * inv, 0.0f);
-}
-
-// shapeMatchImplicit.ts:100-217
-__global__ void __launch_bounds__(kBlock) k_sm_moment(WorldView V, uint32_t rank, uint32_t sub, uint32_t it) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= V.n_grp) return;
-  const DevSoft* D;
-  const DevScene* S;
-  if (!group_active(V, g, rank, sub, it, &D, &S)) return;
-  const uint32_t i = V.grp[g];
-  const uint32_t s = V.csr_off[i], e = V.csr_off[i + 1];
+  const float inv_cnt = 1.0f / (float)max(e - s, 1u);
+  const f3 c = e == s ? mk(0.0f, 0.0f, 0.0f) : sum * inv_cnt;
   float a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  const f3 c = xyz(V.centers[i]);
   const f3 cb = xyz(V.rest_c[i]);
   const float ai = D->ai;
   for (uint32_t m = s; m < e; ++m) {
@@ -1906,7 +1897,6 @@ pf_status World::build(const std::vector<SceneSpec*>& specs, bool use_graph, boo
     base_.rest = need_soft ? cv.take<float4>(N) : nullptr;
     base_.rest_c = need_soft ? cv.take<float4>(N) : nullptr;
     base_.weights = need_soft ? cv.take<float>(N) : nullptr;
-    base_.centers = need_soft ? cv.take<float4>(N) : nullptr;
     base_.rot4 = need_soft ? cv.take<float4>(4 * N) : nullptr;
     base_.q = need_soft ? cv.take<float4>(N) : nullptr;
     base_.qp = need_soft ? cv.take<float4>(N) : nullptr;
@@ -2876,7 +2866,6 @@ void World::run_substep(uint32_t s, uint32_t parity) {
         if (rest) launch_slots(k_fluid_apply, VF.n_fchunk * kSegAlign, stream_, VF, r, s, it, slot ? 1u : 0u);
       }
       if (has_local) {
-        launch_slots(k_sm_center, base_.n_grp, stream_, V, r, s, it);
         launch_slots(k_sm_moment, base_.n_grp, stream_, V, r, s, it);
         if (base_.n_mem_ids) {  // mem_lanes_ lanes per cluster member
           const uint32_t grid = (uint32_t)(((uint64_t)mem_lanes_ * base_.n_mem_ids + kBlock - 1) / kBlock);

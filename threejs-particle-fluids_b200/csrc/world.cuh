@@ -352,7 +352,6 @@ struct WorldView {
   const float4* rest;        // rest offsets, w = compliance
   const float4* rest_c;      // neighbourhood rest centres
   const float* weights;
-  float4* centers;
   // 4 rows per cluster id: the rotation's rows with the cluster centre's
   // x, y, z in w, then (rest centre, compliance); the record the
   // shape-matching gather reads per (member, cluster) pair, 64 aligned bytes
