@@ -37,3 +37,16 @@ def test_reference_arm_line(workload):
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_other_ranks_do_nothing():
+    """Under torchrun with N > 1 only rank 0 runs the reference arm and prints
+    its line; every other rank exits 0 at once, printing nothing."""
+    import os
+
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT="29555")
+    out = subprocess.run(
+        [sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--workload", "dam", "--steps", "1",
+         "--warmup", "3"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == ""
