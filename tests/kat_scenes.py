@@ -442,3 +442,48 @@ def sample_field(data: np.ndarray, origin, voxel, p) -> float:
     c0 = L(L(c(0, 0, 0), c(1, 0, 0), t[0]), L(c(0, 1, 0), c(1, 1, 0), t[0]), t[1])
     c1 = L(L(c(0, 0, 1), c(1, 0, 1), t[0]), L(c(0, 1, 1), c(1, 1, 1), t[0]), t[1])
     return L(c0, c1, t[2])
+
+
+# ---------------------------------------------------------------- soft bodies
+SM_DT = 1.0 / 240.0  # softbody-pass3-apply.gpu.test.ts:34
+
+
+def unit_cube_rest() -> np.ndarray:
+    """softbody-pass3-apply.gpu.test.ts:51-62: the eight corners of a unit cube
+    about the origin (rest centre of mass 0)."""
+    return np.array([[x, y, z] for z in (-0.5, 0.5) for y in (-0.5, 0.5) for x in (-0.5, 0.5)], np.float32)
+
+
+def shape_match_body(rest: np.ndarray, start: np.ndarray, compliance: float, iterations: int,
+                     inv_mass: float = 1.0) -> R.Recipe:
+    """softbody-pass3-apply.gpu.test.ts:115-161 at the scene level: one body
+    with global shape matching over `rest`, its particles at `start` with no
+    velocity and no gravity, one substep of `iterations` iterations. The
+    predicted positions are then `start`, and the step's positions are the
+    predicted positions after the shape-matching iterations (what the test
+    reads back)."""
+    n = rest.shape[0]
+    body = R.BodyDef(range=(0, n), compliance=compliance, rest_positions=np.asarray(rest, np.float32))
+    return R.Recipe(
+        capacity=n,
+        radius=0.05,
+        uploads=[R.Upload(0, np.asarray(start, np.float32), np.zeros((n, 3), np.float32),
+                          np.full(n, inv_mass, np.float32))],
+        materials=[("soft", R.SoftbodyOpts([body], "global"))],
+        loop=R.LoopOpts(substeps=1, iterations=iterations, gravity=(0.0, 0.0, 0.0)),
+        name="shape-match-cube",
+    )
+
+
+def shape_match_goal(rest: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """goal_i = R r_i + c for the frame fitted to positions x (equal masses):
+    c the mean of x, R the rotation of the polar decomposition of
+    sum (x_i - c)(r_i - r_c)^T (shapeMatch.ts, the test's CPU check)."""
+    x = np.asarray(x, np.float64)
+    r = np.asarray(rest, np.float64)
+    c, rc = x.mean(0), r.mean(0)
+    a = (x - c).T @ (r - rc)
+    u, _, vt = np.linalg.svd(a)
+    d = np.sign(np.linalg.det(u @ vt))
+    rot = u @ np.diag([1.0, 1.0, d]) @ vt
+    return (r - rc) @ rot.T + c

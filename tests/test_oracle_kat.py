@@ -3,8 +3,10 @@
 Each test restates one reference test's scene, expected value and tolerance
 (tests/analytical/...), runs it on the oracle, and so pins the oracle's
 integrator, PBF density, XPBD distance constraint, collider contact, greedy
-colouring and polar decomposition to the reference's own expectations.
-The same scenes run on the CUDA path in test_kat_gpu.py.
+colouring, polar decomposition and global shape matching to the reference's
+own expectations. The same scenes, but for the shape-matching ones, run on
+the CUDA path in test_kat_gpu.py; the CUDA path's shape matching is held to
+this oracle scene by scene.
 """
 
 import numpy as np
@@ -170,3 +172,60 @@ def test_bending_drives_toward_rest(cpu):
         s.step(K.DT)
         smallest = min(smallest, abs(K.signed_dihedral(s.readback(N.PF_FIELD_POSITIONS))))
     assert smallest < 0.5 * a0
+
+
+def _shape_match(cpu, start, compliance=1e-12, iterations=1, inv_mass=1.0):
+    rest = K.unit_cube_rest()
+    s = cpu.build(K.shape_match_body(rest, start, compliance, iterations, inv_mass))
+    s.step(K.SM_DT)
+    return rest, s.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
+
+
+def _max_dist(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64), axis=1).max())
+
+
+def test_shape_match_rest_is_still(cpu):
+    """softbody-pass3-apply.gpu.test.ts:188-196: at rest, dx = 0 (< 1e-5)."""
+    rest = K.unit_cube_rest()
+    _, x = _shape_match(cpu, rest)
+    assert _max_dist(x, rest) < 1e-5
+
+
+def test_shape_match_rigid_translation_and_rotation(cpu):
+    """softbody-pass3-apply.gpu.test.ts:198-229 (and pass2-rotation's rotated
+    cases): a rigidly translated body, and one rotated by pi/4 about z, stay
+    where they are (< 1e-4): the fitted frame is the rigid motion."""
+    rest = K.unit_cube_rest()
+    moved = rest + np.array([3.0, -1.0, 2.0], np.float32)
+    _, x = _shape_match(cpu, moved)
+    assert _max_dist(x, moved) < 1e-4
+    rotated = (rest.astype(np.float64) @ K.rot_z(np.pi / 4).T).astype(np.float32)
+    _, x = _shape_match(cpu, rotated)
+    assert _max_dist(x, rotated) < 1e-4
+
+
+def test_shape_match_perturbed_particle(cpu):
+    """softbody-pass3-apply.gpu.test.ts:231-307: one corner moved by 0.5 in x.
+    At compliance 1e-12 one iteration takes every particle to its goal under
+    the frame fitted to the perturbed positions (< 1e-4); at compliance 1e-2
+    (alpha / dt^2 = 576) the corner moves by under 0.05; ten iterations at
+    1e-12 end at a fixed point of the fit (< 1e-5)."""
+    rest = K.unit_cube_rest()
+    start = rest.copy()
+    start[0, 0] += 0.5
+    _, x = _shape_match(cpu, start, 1e-12, 1)
+    assert _max_dist(x, K.shape_match_goal(rest, start)) < 1e-4
+    _, x = _shape_match(cpu, start, 1e-2, 1)
+    assert abs(x[0, 0] - start[0, 0]) < 0.05
+    _, x = _shape_match(cpu, start, 1e-12, 10)
+    assert _max_dist(x, K.shape_match_goal(rest, x)) < 1e-5
+
+
+def test_shape_match_kinematic_body(cpu):
+    """softbody-pass3-apply.gpu.test.ts:309-322: particles of inverse mass 0
+    are never corrected (< 1e-5), even at compliance 1e-12."""
+    rest = K.unit_cube_rest()
+    moved = rest + np.array([1.0, 0.0, 0.0], np.float32)
+    _, x = _shape_match(cpu, moved, inv_mass=0.0)
+    assert _max_dist(x, moved) < 1e-5
