@@ -455,7 +455,7 @@ def unit_cube_rest() -> np.ndarray:
 
 
 def shape_match_body(rest: np.ndarray, start: np.ndarray, compliance: float, iterations: int,
-                     inv_mass: float = 1.0) -> R.Recipe:
+                     inv_mass=1.0) -> R.Recipe:
     """softbody-pass3-apply.gpu.test.ts:115-161 at the scene level: one body
     with global shape matching over `rest`, its particles at `start` with no
     velocity and no gravity, one substep of `iterations` iterations. The
@@ -468,21 +468,34 @@ def shape_match_body(rest: np.ndarray, start: np.ndarray, compliance: float, ite
         capacity=n,
         radius=0.05,
         uploads=[R.Upload(0, np.asarray(start, np.float32), np.zeros((n, 3), np.float32),
-                          np.full(n, inv_mass, np.float32))],
+                          np.broadcast_to(np.asarray(inv_mass, np.float32), (n,)).copy())],
         materials=[("soft", R.SoftbodyOpts([body], "global"))],
         loop=R.LoopOpts(substeps=1, iterations=iterations, gravity=(0.0, 0.0, 0.0)),
         name="shape-match-cube",
     )
 
 
-def shape_match_goal(rest: np.ndarray, x: np.ndarray) -> np.ndarray:
-    """goal_i = R r_i + c for the frame fitted to positions x (equal masses):
-    c the mean of x, R the rotation of the polar decomposition of
-    sum (x_i - c)(r_i - r_c)^T (shapeMatch.ts, the test's CPU check)."""
+def shape_match_weights(inv_mass: np.ndarray) -> np.ndarray:
+    """SoftbodySystem.ts:366-372: each dynamic particle weighs its mass over the
+    body's mean mass (all 1 when the masses are equal), a kinematic one 1."""
+    inv_mass = np.asarray(inv_mass, np.float64)
+    m = np.where(inv_mass > 0, 1.0 / np.where(inv_mass > 0, inv_mass, 1.0), 0.0)
+    dyn = m[m > 0]
+    if dyn.size == 0 or np.all(dyn == dyn[0]):
+        return np.ones_like(m)
+    return np.where(m > 0, m / dyn.mean(), 1.0)
+
+
+def shape_match_goal(rest: np.ndarray, x: np.ndarray, weights=None) -> np.ndarray:
+    """goal_i = R r_i + c for the frame fitted to positions x: c the weighted
+    mean of x, r_i the rest positions less their weighted centre, R the
+    rotation of the polar decomposition of sum w_i (x_i - c) r_i^T
+    (shapeMatch.ts:49-135, SoftbodySystem.ts:181-189, the test's CPU check)."""
     x = np.asarray(x, np.float64)
     r = np.asarray(rest, np.float64)
-    c, rc = x.mean(0), r.mean(0)
-    a = (x - c).T @ (r - rc)
+    w = np.ones(len(x)) if weights is None else np.asarray(weights, np.float64)
+    c, rc = (w[:, None] * x).sum(0) / w.sum(), (w[:, None] * r).sum(0) / w.sum()
+    a = (w[:, None] * (x - c)).T @ (r - rc)
     u, _, vt = np.linalg.svd(a)
     d = np.sign(np.linalg.det(u @ vt))
     rot = u @ np.diag([1.0, 1.0, d]) @ vt

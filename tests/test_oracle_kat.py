@@ -229,3 +229,19 @@ def test_shape_match_kinematic_body(cpu):
     moved = rest + np.array([1.0, 0.0, 0.0], np.float32)
     _, x = _shape_match(cpu, moved, inv_mass=0.0)
     assert _max_dist(x, moved) < 1e-5
+
+
+def test_shape_match_weights_by_mass(cpu):
+    """softbody-center-of-mass.gpu.test.ts case (d) through the correction of
+    softbody-pass3-apply.gpu.test.ts:231-259: with unequal masses the frame
+    is fitted with mass weights (SoftbodySystem.ts:366-372), so one iteration
+    at compliance 1e-12 takes the perturbed cube to the goal of the weighted
+    fit (< 1e-4), and not to that of the unweighted one."""
+    rest = K.unit_cube_rest()
+    start = rest.copy()
+    start[0, 0] += 0.5
+    inv_mass = np.array([1.0, 0.5, 2.0, 1.0, 1.0, 0.25, 1.0, 1.0], np.float32)
+    _, x = _shape_match(cpu, start, 1e-12, 1, inv_mass)
+    weighted = K.shape_match_goal(rest, start, K.shape_match_weights(inv_mass))
+    assert _max_dist(x, weighted) < 1e-4
+    assert _max_dist(x, K.shape_match_goal(rest, start)) > 1e-2
