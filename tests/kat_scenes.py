@@ -500,3 +500,29 @@ def shape_match_goal(rest: np.ndarray, x: np.ndarray, weights=None) -> np.ndarra
     d = np.sign(np.linalg.det(u @ vt))
     rot = u @ np.diag([1.0, 1.0, d]) @ vt
     return (r - rc) @ rot.T + c
+
+
+# ------------------------------------------------------------- non-penetration
+def non_penetration() -> R.Recipe:
+    """tests/analytical/collider/collider-non-penetration.gpu.test.ts:46-81:
+    three particles (r = 0.05) and one PrimitiveSet of a plane at y = 0, a
+    solid sphere below it and an inverted box (a container) around (1, 0, 0),
+    each with muS 0.3 and muK 0.2; 4 substeps, 4 iterations, gravity -9.81."""
+    pos = np.array([[-1.0, 0.5, 0.0], [0.0, 0.0, 0.0], [1.0, 0.0, 0.0]], np.float32)
+    prims = [R.plane((0, 1, 0), (-1.0, 0.0, 0.0), 0.3, 0.2),
+             R.sphere((0.0, -0.5, 0.0), 0.3, mu_s=0.3, mu_k=0.2),
+             R.box((1.0, 0.0, 0.0), (0.3, 0.3, 0.3), invert=True, mu_s=0.3, mu_k=0.2)]
+    return R.Recipe(capacity=3, radius=0.05,
+                    uploads=[R.Upload(0, pos, np.zeros_like(pos), np.ones(3, np.float32))],
+                    prims=prims, loop=R.LoopOpts(substeps=4, iterations=4), name="non-penetration")
+
+
+def non_penetration_phis(x: np.ndarray) -> np.ndarray:
+    """The test's CPU SDFs (collider-non-penetration.gpu.test.ts:23-44) of
+    each particle against the plane, the sphere and the inverted box."""
+    x = np.asarray(x, np.float64)[:, :3]
+    plane = x[:, 1] - 0.0
+    sphere = np.linalg.norm(x - np.array([0.0, -0.5, 0.0]), axis=1) - 0.3
+    q = np.abs(x - np.array([1.0, 0.0, 0.0])) - 0.3
+    box = np.linalg.norm(np.maximum(q, 0.0), axis=1) + np.minimum(q.max(1), 0.0)
+    return np.stack([plane, sphere, -box], axis=1)

@@ -245,3 +245,19 @@ def test_shape_match_weights_by_mass(cpu):
     weighted = K.shape_match_goal(rest, start, K.shape_match_weights(inv_mass))
     assert _max_dist(x, weighted) < 1e-4
     assert _max_dist(x, K.shape_match_goal(rest, start)) > 1e-2
+
+
+def test_collider_non_penetration(cpu):
+    """collider-non-penetration.gpu.test.ts:46-126: over 120 frames of 1/60 s
+    no particle ends a frame with phi < -r - 5e-3 against any of the three
+    colliders (the container pulls two particles into itself on the first
+    substep, then all three settle on the plane inside it)."""
+    s = cpu.build(K.non_penetration())
+    worst = np.inf
+    for _ in range(120):
+        s.step(K.DT)
+        worst = min(worst, float(K.non_penetration_phis(s.readback(N.PF_FIELD_POSITIONS)).min()))
+    assert worst > -0.05 - 5e-3
+    # and the particles did end inside the box, on the plane
+    x = s.readback(N.PF_FIELD_POSITIONS)[:, :3]
+    assert np.all(np.abs(x[:, 0] - 1.0) < 0.3) and np.all(np.abs(x[:, 1] - 0.05) < 0.01)
