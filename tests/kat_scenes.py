@@ -526,3 +526,44 @@ def non_penetration_phis(x: np.ndarray) -> np.ndarray:
     q = np.abs(x - np.array([1.0, 0.0, 0.0])) - 0.3
     box = np.linalg.norm(np.maximum(q, 0.0), axis=1) + np.minimum(q.max(1), 0.0)
     return np.stack([plane, sphere, -box], axis=1)
+
+
+def axis_angle_quat(axis, angle: float) -> tuple:
+    """(x, y, z, w) of a rotation by `angle` about the unit `axis`."""
+    s = math.sin(angle / 2.0)
+    return (axis[0] * s, axis[1] * s, axis[2] * s, math.cos(angle / 2.0))
+
+
+ROTATED_BOXES = [  # collider-rotated-box-non-penetration.gpu.test.ts:67-95: centre, half extents, rotation, invert
+    ((-1.0, 0.0, 0.0), (0.4, 0.05, 0.4), axis_angle_quat((0, 0, 1), math.pi / 6), False),
+    ((0.0, 0.0, 0.0), (0.4, 0.05, 0.4), axis_angle_quat((1, 0, 0), math.pi / 4), False),
+    ((1.0, 0.0, 0.0), (0.3, 0.3, 0.3), axis_angle_quat((0, 1, 0), math.pi / 5), True),
+]
+
+
+def rotated_boxes() -> R.Recipe:
+    """collider-rotated-box-non-penetration.gpu.test.ts:52-104: three
+    particles (r = 0.05) above two tilted slabs and inside a rotated
+    container, muS 0.3 and muK 0.2; 4 substeps, 4 iterations, gravity -9.81."""
+    pos = np.array([[-1.0, 0.8, 0.0], [0.0, 0.8, 0.0], [1.0, 0.0, 0.0]], np.float32)
+    prims = [R.box(c, h, rotation=q, invert=inv, mu_s=0.3, mu_k=0.2) for c, h, q, inv in ROTATED_BOXES]
+    return R.Recipe(capacity=3, radius=0.05,
+                    uploads=[R.Upload(0, pos, np.zeros_like(pos), np.ones(3, np.float32))],
+                    prims=prims, loop=R.LoopOpts(substeps=4, iterations=4), name="rotated-boxes")
+
+
+def rotated_box_phis(x: np.ndarray) -> np.ndarray:
+    """The test's CPU oriented-box SDF (lines 30-49): the point in the box's
+    frame by the inverse rotation, then the axis-aligned box distance."""
+    x = np.asarray(x, np.float64)[:, :3]
+    out = []
+    for c, h, q, inv in ROTATED_BOXES:
+        qx, qy, qz, qw = q
+        rot = np.array([[1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)],
+                        [2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)],
+                        [2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)]])
+        local = (x - np.asarray(c)) @ rot  # rows: rot^T (x - c)
+        d = np.abs(local) - np.asarray(h)
+        dist = np.linalg.norm(np.maximum(d, 0.0), axis=1) + np.minimum(d.max(1), 0.0)
+        out.append(-dist if inv else dist)
+    return np.stack(out, axis=1)

@@ -261,3 +261,16 @@ def test_collider_non_penetration(cpu):
     # and the particles did end inside the box, on the plane
     x = s.readback(N.PF_FIELD_POSITIONS)[:, :3]
     assert np.all(np.abs(x[:, 0] - 1.0) < 0.3) and np.all(np.abs(x[:, 1] - 0.05) < 0.01)
+
+
+def test_rotated_box_non_penetration(cpu):
+    """collider-rotated-box-non-penetration.gpu.test.ts:52-150: over 120
+    frames no particle ends a frame with phi < -r - 5e-3 against the two
+    tilted slabs and the rotated container (the rotated SDF and its gradient
+    rotated back to world space)."""
+    s = cpu.build(K.rotated_boxes())
+    worst = np.inf
+    for _ in range(120):
+        s.step(K.DT)
+        worst = min(worst, float(K.rotated_box_phis(s.readback(N.PF_FIELD_POSITIONS)).min()))
+    assert worst > -0.05 - 5e-3
