@@ -567,3 +567,20 @@ def rotated_box_phis(x: np.ndarray) -> np.ndarray:
         dist = np.linalg.norm(np.maximum(d, 0.0), axis=1) + np.minimum(d.max(1), 0.0)
         out.append(-dist if inv else dist)
     return np.stack(out, axis=1)
+
+
+def sphere_bowl(n: int = 100) -> R.Recipe:
+    """collider-sphere-bowl-rest.gpu.test.ts:34-88: 100 particles (r = 0.05)
+    in a cloud above the centre of an inverted unit sphere (muS 0.5, muK 0.4),
+    placed by the test's LCG from seed 0xc0ffee; particle contacts on
+    (maxContacts 8N, muS 0.5, muK 0.4); 4 substeps, 4 iterations."""
+    rand = lcg_js(0xC0FFEE)
+    pos = []
+    for _ in range(n):
+        x = 0.3 * (rand() * 2 - 1)
+        y = 0.3 + 0.3 * abs(rand() * 2 - 1)
+        z = 0.3 * (rand() * 2 - 1)
+        pos.append((x, y, z))
+    return particles(pos, 0.05, 4, 4, vel=np.zeros((n, 3), np.float32), inv_mass=np.ones(n, np.float32),
+                     contact=(8 * n, 0.5, 0.4), prims=[R.sphere((0.0, 0.0, 0.0), 1.0, invert=True, mu_s=0.5, mu_k=0.4)],
+                     name="sphere-bowl")

@@ -274,3 +274,17 @@ def test_rotated_box_non_penetration(cpu):
         s.step(K.DT)
         worst = min(worst, float(K.rotated_box_phis(s.readback(N.PF_FIELD_POSITIONS)).min()))
     assert worst > -0.05 - 5e-3
+
+
+def test_sphere_bowl_rest(cpu):
+    """collider-sphere-bowl-rest.gpu.test.ts:90-131: after 300 frames (5 s)
+    every particle is inside the bowl (|x| < R - r + 5e-3), the pile has
+    settled (every speed < 0.5 m/s) and no overflow flag is set."""
+    s = cpu.build(K.sphere_bowl())
+    for _ in range(300):
+        s.step(K.DT)
+    x = s.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
+    v = s.readback(N.PF_FIELD_VELOCITIES)[:, :3].astype(np.float64)
+    assert np.linalg.norm(x, axis=1).max() < 1.0 - 0.05 + 5e-3
+    assert np.linalg.norm(v, axis=1).max() < 0.5
+    assert not any(s.overflow().values())
