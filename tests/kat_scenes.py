@@ -584,3 +584,34 @@ def sphere_bowl(n: int = 100) -> R.Recipe:
     return particles(pos, 0.05, 4, 4, vel=np.zeros((n, 3), np.float32), inv_mass=np.ones(n, np.float32),
                      contact=(8 * n, 0.5, 0.4), prims=[R.sphere((0.0, 0.0, 0.0), 1.0, invert=True, mu_s=0.5, mu_k=0.4)],
                      name="sphere-bowl")
+
+
+def spring_pair(compliance: float, substeps: int, iterations: int, offset: float = 0.05) -> R.Recipe:
+    """xpbd-frequency.gpu.test.ts:66-106: particle 0 pinned at the origin,
+    particle 1 (mass 1) released at (0, -(1 + offset), 0), one distance
+    constraint of rest length 1 and compliance alpha, no gravity."""
+    pos = np.array([[0.0, 0.0, 0.0], [0.0, -(1.0 + offset), 0.0]], np.float32)
+    w = np.array([0.0, 1.0], np.float32)
+    r = R.Recipe(capacity=2, radius=0.02,
+                 loop=R.LoopOpts(substeps=substeps, iterations=iterations, gravity=(0.0, 0.0, 0.0)),
+                 name=f"spring-{compliance:g}")
+    r.materials.append(("cloth", R.ClothOpts(offset=0, positions=pos, inv_mass=w,
+                                             pairs=np.array([[0, 1]], np.uint32),
+                                             rest_lengths=np.array([1.0], np.float32),
+                                             stretch_compliance=compliance)))
+    return r
+
+
+def spring_period(scene, frame_dt: float, frames: int) -> float:
+    """The test's period estimate (lines 126-157): upward zero crossings of
+    y + 1, interpolated within the frame, averaged gap."""
+    from pfsim import _native as N
+
+    disp = []
+    for _ in range(frames):
+        scene.step(frame_dt)
+        disp.append(float(scene.readback(N.PF_FIELD_POSITIONS)[1, 1]) + 1.0)
+    t = [(i - 1 + (0.0 if disp[i - 1] == disp[i] else -disp[i - 1] / (disp[i] - disp[i - 1]))) * frame_dt
+         for i in range(1, frames) if disp[i - 1] <= 0 < disp[i]]
+    assert len(t) >= 3, t
+    return float(np.mean(np.diff(t)))

@@ -288,3 +288,17 @@ def test_sphere_bowl_rest(cpu):
     assert np.linalg.norm(x, axis=1).max() < 1.0 - 0.05 + 5e-3
     assert np.linalg.norm(v, axis=1).max() < 0.5
     assert not any(s.overflow().values())
+
+
+@pytest.mark.parametrize("alpha", [1e-2, 1e-4, 1e-6])
+def test_xpbd_spring_frequency(cpu, alpha):
+    """xpbd-frequency.gpu.test.ts:40-176: a pinned particle and a free one of
+    mass 1 on a distance constraint of compliance alpha oscillate with period
+    2 pi sqrt(alpha) within 2 %, at 20 frames per period over 10 periods, 4
+    substeps and 2 iterations (8 at alpha <= 1e-5)."""
+    period = 2.0 * np.pi * np.sqrt(alpha)
+    frame_dt = period / 20.0
+    iterations = 8 if alpha <= 1e-5 else 2
+    s = cpu.build(K.spring_pair(alpha, 4, iterations))
+    measured = K.spring_period(s, frame_dt, 200)
+    assert abs(measured - period) / period < 0.02
