@@ -615,3 +615,24 @@ def spring_period(scene, frame_dt: float, frames: int) -> float:
          for i in range(1, frames) if disp[i - 1] <= 0 < disp[i]]
     assert len(t) >= 3, t
     return float(np.mean(np.diff(t)))
+
+
+def energy_drift_cloud(n: int = 1000):
+    """integrate-energy-drift.gpu.test.ts:26-48: 1000 particles from the
+    test's LCG (seed 0xc0ffee), positions in [-5, 5] x [10, 50] x [-5, 5] and
+    velocities in [-2, 2]^3 drawn particle by particle; no material, no
+    collider, one substep. Returns the recipe and the initial state."""
+    rand = lcg_js(0xC0FFEE)
+    pos, vel = [], []
+    for _ in range(n):
+        pos.append([-5 + 10 * rand(), 10 + 40 * rand(), -5 + 10 * rand()])
+        vel.append([-2 + 4 * rand(), -2 + 4 * rand(), -2 + 4 * rand()])
+    pos, vel = np.array(pos, np.float32), np.array(vel, np.float32)
+    rec = particles(pos, 0.05, 1, 2, vel=vel, inv_mass=np.ones(n, np.float32), name="energy-drift")
+    return rec, pos, vel
+
+
+def mean_energy(pos, vel) -> float:
+    """The test's mean energy per particle, 1/2 |v|^2 + g y."""
+    pos, vel = np.asarray(pos, np.float64), np.asarray(vel, np.float64)
+    return float((0.5 * (vel[:, :3] ** 2).sum(1) + G * pos[:, 1]).mean())
