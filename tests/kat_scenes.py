@@ -636,3 +636,25 @@ def mean_energy(pos, vel) -> float:
     """The test's mean energy per particle, 1/2 |v|^2 + g y."""
     pos, vel = np.asarray(pos, np.float64), np.asarray(vel, np.float64)
     return float((0.5 * (vel[:, :3] ** 2).sum(1) + G * pos[:, 1]).mean())
+
+
+def sealed_tank():
+    """mass-conservation.gpu.test.ts:24-77: 8 x 12 x 8 = 768 fluid particles
+    at spacing 0.025 (r = spacing / 2, h = 0.05, rest density 1000,
+    compliance 1e-4, mass rest density x spacing^3) in an open-top tank of
+    five planes at +-0.15 in x and z; 4 substeps, 2 iterations."""
+    s, nx, ny, nz = 0.025, 8, 12, 8
+    pos = [[-(nx * s) / 2 + s * 0.5 + i * s, s * 0.5 + j * s, -(nz * s) / 2 + s * 0.5 + k * s]
+           for j in range(ny) for k in range(nz) for i in range(nx)]
+    pos = np.array(pos, np.float32)
+    n = len(pos)
+    w = np.full(n, np.float32(1.0 / (1000.0 * s ** 3)), np.float32)
+    half = 0.15
+    prims = [R.plane((0, 1, 0), (0.0, 0.0, 0.0)), R.plane((1, 0, 0), (-half, 0.0, 0.0)),
+             R.plane((-1, 0, 0), (half, 0.0, 0.0)), R.plane((0, 0, 1), (0.0, 0.0, -half)),
+             R.plane((0, 0, -1), (0.0, 0.0, half))]
+    r = R.Recipe(capacity=n, radius=s * 0.5, uploads=[R.Upload(0, pos, np.zeros_like(pos), w)], prims=prims,
+                 loop=R.LoopOpts(substeps=4, iterations=2), name="sealed-tank")
+    r.materials.append(("fluid", R.FluidOpts(range=(0, n), rest_density=1000.0, particle_spacing=s,
+                                             smoothing_radius=0.05, compliance=1e-4)))
+    return r

@@ -317,3 +317,17 @@ def test_integrator_energy_drift(cpu):
     expected = -0.5 * K.G * K.G * K.DT * K.DT * 300
     assert e1 - e0 < 0
     assert abs((e1 - e0) - expected) < 0.5
+
+
+def test_fluid_stays_in_sealed_tank(cpu):
+    """mass-conservation.gpu.test.ts:79-130: after 600 frames (10 s) of the
+    768-particle tank no position is NaN and none has escaped: inside the
+    walls (+-0.15) and above the floor with 2r of slack, below y = 10."""
+    s = cpu.build(K.sealed_tank())
+    for _ in range(600):
+        s.step(K.DT)
+    x = s.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
+    assert np.isfinite(x).all()
+    tol = 2 * 0.0125
+    assert np.all(np.abs(x[:, 0]) <= 0.15 + tol) and np.all(np.abs(x[:, 2]) <= 0.15 + tol)
+    assert np.all(x[:, 1] >= -tol) and np.all(x[:, 1] <= 10.0)
