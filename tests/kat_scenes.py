@@ -658,3 +658,21 @@ def sealed_tank():
     r.materials.append(("fluid", R.FluidOpts(range=(0, n), rest_density=1000.0, particle_spacing=s,
                                              smoothing_radius=0.05, compliance=1e-4)))
     return r
+
+
+def box_container(n: int = 1000) -> R.Recipe:
+    """collider-box-container.gpu.test.ts:24-73: 1000 particles (r = 0.02)
+    from the test's LCG (seed 0xdecafbad) in x, z in [-0.4, 0.4], y in [0.2,
+    0.45], dropped in an inverted unit box (muS 0.5, muK 0.4); particle
+    contacts on (maxContacts 8N, default friction); 4 substeps, 4 iterations."""
+    rand = lcg_js(0xDECAFBAD)
+    pos = []
+    for _ in range(n):
+        x = (rand() * 2 - 1) * 0.4
+        y = 0.2 + rand() * 0.25
+        z = (rand() * 2 - 1) * 0.4
+        pos.append((x, y, z))
+    return particles(pos, 0.02, 4, 4, vel=np.zeros((n, 3), np.float32), inv_mass=np.ones(n, np.float32),
+                     contact=(8 * n, -1.0, -1.0),
+                     prims=[R.box((0.0, 0.0, 0.0), (0.5, 0.5, 0.5), invert=True, mu_s=0.5, mu_k=0.4)],
+                     name="box-container")

@@ -331,3 +331,19 @@ def test_fluid_stays_in_sealed_tank(cpu):
     tol = 2 * 0.0125
     assert np.all(np.abs(x[:, 0]) <= 0.15 + tol) and np.all(np.abs(x[:, 2]) <= 0.15 + tol)
     assert np.all(x[:, 1] >= -tol) and np.all(x[:, 1] <= 10.0)
+
+
+def test_box_container_holds_particles(cpu):
+    """collider-box-container.gpu.test.ts:74-121: after 120 frames every
+    particle is inside the inverted box less its radius (overrun < 2e-3),
+    the pile has settled (every speed < 0.5 m/s) and no overflow flag is
+    set."""
+    s = cpu.build(K.box_container())
+    for _ in range(120):
+        s.step(K.DT)
+    x = s.readback(N.PF_FIELD_POSITIONS)[:, :3].astype(np.float64)
+    v = s.readback(N.PF_FIELD_VELOCITIES)[:, :3].astype(np.float64)
+    overrun = np.maximum((np.abs(x) - (0.5 - 0.02)).max(1), 0.0)
+    assert overrun.max() < 2e-3
+    assert np.linalg.norm(v, axis=1).max() < 0.5
+    assert not any(s.overflow().values())
