@@ -347,3 +347,32 @@ def test_box_container_holds_particles(cpu):
     assert overrun.max() < 2e-3
     assert np.linalg.norm(v, axis=1).max() < 0.5
     assert not any(s.overflow().values())
+
+
+def test_hydrostatic_column(cpu):
+    """hydrostatic-column.gpu.test.ts:43-262: the 768-particle column of the
+    sealed tank settles for 300 frames (5 s); its density excess over rest
+    grows with depth. Over ten height bins, the middle eight's mean density
+    excess against depth has a positive slope with r^2 > 0.5, and no density
+    exceeds 1.1 rest density."""
+    s = cpu.build(K.sealed_tank())
+    for _ in range(300):
+        s.step(K.DT)
+    y = s.readback(N.PF_FIELD_POSITIONS)[:, 1].astype(np.float64)
+    rho = s.readback(N.PF_FIELD_DENSITY).astype(np.float64)
+    assert np.isfinite(y).all() and np.isfinite(rho).all()
+    y0, y1 = y.min(), y.max()
+    assert y1 - y0 > 0.025
+    bins = 10
+    idx = np.clip(np.floor((y - y0) / (y1 - y0) * bins).astype(int), 0, bins - 1)
+    edges = y0 + (y1 - y0) * np.arange(bins + 1) / bins
+    depth = y1 - 0.5 * (edges[:-1] + edges[1:])
+    mid = [b for b in range(1, bins - 1) if np.any(idx == b)]
+    assert len(mid) >= 6
+    xs = depth[mid]
+    ex = np.array([rho[idx == b].mean() for b in mid]) - 1000.0
+    dx, dy = xs - xs.mean(), ex - ex.mean()
+    sxx, sxy, syy = (dx * dx).sum(), (dx * dy).sum(), (dy * dy).sum()
+    assert sxy / sxx > 0
+    assert sxy * sxy / (sxx * syy) > 0.5
+    assert rho.max() < 1100.0
